@@ -1,0 +1,241 @@
+"""ctypes binding of libbanana_b200.so (the C ABI declared in include/banana_b200.h).
+
+This is the reference-facing surface the tests and the benchmark drive.  It loads the
+in-tree CUDA library and raises if it is missing: there is no CPU path behind it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libbanana_b200.so"
+
+BNN_OK = 0
+STATUS = {0: "OK", 1: "INVALID_ARGUMENT", 2: "OUT_OF_MEMORY", 3: "PCG_NOT_CONVERGED", 4: "DEVICE_CHECK",
+          5: "TIMEOUT", 6: "CUDA", 7: "NOT_SUPPORTED", 8: "CAPACITY"}
+SOLVER_KIND = {"FLIP": 0, "APIC": 1, "AFLIP": 2}
+PCG_MODE = {"fp32": 0, "fp64": 1, "refined": 2}
+FIELD = {"u": 0, "v": 1, "w": 2, "phi": 3, "pressure": 4, "old_u": 5, "old_v": 6, "old_w": 7, "active": 8}
+
+# Exported symbols of the C ABI (every one is declared in include/banana_b200.h)
+EXPORTS = [
+    "bnn_flip_create", "bnn_flip_destroy", "bnn_flip_grid_dims", "bnn_flip_set_particles", "bnn_flip_get_particles",
+    "bnn_flip_num_particles", "bnn_flip_get_grid", "bnn_flip_step", "bnn_flip_advance_frame",
+    "bnn_flip_device_particles", "bnn_flip_step_host", "bnn_cell_sort", "bnn_z_sort", "bnn_neighbors",
+    "bnn_pcg_solve_7pt", "bnn_version", "bnn_last_error",
+]
+
+
+class BnnError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        super().__init__(f"{what} failed: {STATUS.get(code, code)} ({code}) {last_error()}")
+        self.code = code
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("box_min", C.c_float * 3), ("box_max", C.c_float * 3), ("cell_size", C.c_float),
+        ("n_expand_cells", C.c_uint32), ("cfl_factor", C.c_float), ("min_timestep", C.c_float),
+        ("max_timestep", C.c_float), ("frame_duration", C.c_float), ("pic_flip_ratio", C.c_float),
+        ("cg_relative_tolerance", C.c_float), ("max_cg_iteration", C.c_uint32), ("advection_steps", C.c_uint32),
+        ("solver_kind", C.c_int32), ("pcg_mode", C.c_int32), ("preconditioner", C.c_int32),
+        ("refine_tolerance", C.c_float), ("refine_inner_tolerance", C.c_float), ("apply_gravity", C.c_int32),
+        ("max_particles", C.c_uint32),
+    ]
+
+
+class StepStats(C.Structure):
+    _fields_ = [
+        ("dt", C.c_double), ("frame_time", C.c_double), ("frame_finished", C.c_uint32),
+        ("pcg_iterations", C.c_uint32), ("pcg_residual", C.c_double), ("pcg_success", C.c_uint32),
+        ("n_active", C.c_uint32), ("outer_iterations", C.c_uint32), ("zero_phi_cells", C.c_uint32),
+        ("stage_ms", C.c_float * 10), ("device_flags", C.c_uint32),
+    ]
+
+
+class PcgStats(C.Structure):
+    _fields_ = [("iterations", C.c_uint32), ("outer_iterations", C.c_uint32), ("residual", C.c_double),
+                ("success", C.c_uint32), ("ms", C.c_float)]
+
+
+STAGES = ["move", "sort", "p2g", "extrapolate", "fluid_sdf", "system", "pcg", "update", "g2p", "step"]
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load the in-tree CUDA library (fails loudly when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} is missing: run banana_b200.build.build() first (no CPU fallback exists)")
+    L = C.CDLL(str(LIB_PATH))
+    vp = C.c_void_p
+    fp = C.POINTER(C.c_float)
+    dp = C.POINTER(C.c_double)
+    u32p = C.POINTER(C.c_uint32)
+    i32p = C.POINTER(C.c_int32)
+    u64p = C.POINTER(C.c_uint64)
+    L.bnn_flip_create.argtypes = [C.POINTER(Params), C.POINTER(vp)]
+    L.bnn_flip_destroy.argtypes = [vp]
+    L.bnn_flip_grid_dims.argtypes = [vp, i32p]
+    L.bnn_flip_set_particles.argtypes = [vp, fp, fp, C.c_uint32]
+    L.bnn_flip_get_particles.argtypes = [vp, fp, fp]
+    L.bnn_flip_num_particles.argtypes = [vp, u32p]
+    L.bnn_flip_get_grid.argtypes = [vp, C.c_int32, fp, C.c_size_t]
+    L.bnn_flip_step.argtypes = [vp, C.POINTER(StepStats)]
+    L.bnn_flip_advance_frame.argtypes = [vp, u32p]
+    L.bnn_flip_device_particles.argtypes = [vp, C.POINTER(fp), C.POINTER(u32p)]
+    L.bnn_flip_step_host.argtypes = [vp, fp, fp, C.POINTER(StepStats)]
+    L.bnn_cell_sort.argtypes = [vp, C.c_uint32, fp, C.c_float, i32p, vp, vp, vp, u32p, vp]
+    L.bnn_z_sort.argtypes = [vp, C.c_uint32, C.c_float, vp, vp, vp]
+    L.bnn_neighbors.argtypes = [vp, C.c_uint32, C.c_float, vp, vp, C.c_uint64, u64p, vp]
+    L.bnn_pcg_solve_7pt.argtypes = [C.c_uint32, fp, i32p, C.c_float, fp, C.c_float, C.c_uint32, C.c_int32, C.c_float,
+                                    dp, C.POINTER(PcgStats)]
+    L.bnn_version.restype = C.c_char_p
+    L.bnn_last_error.restype = C.c_char_p
+    for name in EXPORTS:
+        if name not in ("bnn_version", "bnn_last_error"):
+            getattr(L, name).restype = C.c_int
+    _lib = L
+    return L
+
+
+def last_error() -> str:
+    try:
+        return (load().bnn_last_error() or b"").decode()
+    except Exception:
+        return ""
+
+
+def check(code: int, what: str) -> None:
+    if code != BNN_OK:
+        raise BnnError(code, what)
+
+
+def _p(a: np.ndarray, t):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+def make_params(cfg: dict) -> Params:
+    p = Params()
+    p.box_min[:] = cfg.get("box_min", (0.0, 0.0, 0.0))
+    p.box_max[:] = cfg.get("box_max", (1.0, 1.0, 1.0))
+    p.cell_size = cfg["cell_size"]
+    p.n_expand_cells = cfg.get("n_expand_cells", 2)
+    p.cfl_factor = cfg.get("cfl_factor", 1.0)
+    p.min_timestep = cfg.get("min_timestep", 1e-6)
+    p.max_timestep = cfg.get("max_timestep", float(np.float32(1.0) / np.float32(30.0)))
+    p.frame_duration = cfg.get("frame_duration", float(np.float32(1.0 / 30.0)))
+    p.pic_flip_ratio = cfg.get("pic_flip_ratio", 0.97)
+    p.cg_relative_tolerance = cfg.get("cg_relative_tolerance", 1e-6)
+    p.max_cg_iteration = cfg.get("max_cg_iteration", 5000)
+    p.advection_steps = cfg.get("advection_steps", 1)
+    p.solver_kind = cfg.get("solver_kind", 0)
+    p.pcg_mode = cfg.get("pcg_mode", 0)
+    p.preconditioner = cfg.get("preconditioner", 0)
+    p.refine_tolerance = cfg.get("refine_tolerance", 1e-8)
+    p.refine_inner_tolerance = cfg.get("refine_inner_tolerance", 1e-3)
+    p.apply_gravity = cfg.get("apply_gravity", 1)
+    p.max_particles = cfg.get("max_particles", 0)
+    return p
+
+
+class FlipSolver:
+    """One device-resident FLIP/APIC/AFLIP scene behind the C ABI."""
+
+    def __init__(self, cfg: dict):
+        self.L = load()
+        self.cfg = dict(cfg)
+        self.params = make_params(cfg)
+        h = C.c_void_p()
+        check(self.L.bnn_flip_create(C.byref(self.params), C.byref(h)), "bnn_flip_create")
+        self.h = h
+        g = np.zeros(3, np.int32)
+        check(self.L.bnn_flip_grid_dims(self.h, _p(g, C.c_int32)), "bnn_flip_grid_dims")
+        self.G = tuple(int(x) for x in g)
+        self.n = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.bnn_flip_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def face_shape(self, d: int):
+        G = list(self.G)
+        G[d] += 1
+        return tuple(G)
+
+    def set_particles(self, pos: np.ndarray, vel: np.ndarray):
+        pos = np.ascontiguousarray(pos, np.float32)
+        vel = np.ascontiguousarray(vel, np.float32)
+        self.n = len(pos)
+        check(self.L.bnn_flip_set_particles(self.h, _p(pos, C.c_float), _p(vel, C.c_float), self.n),
+              "bnn_flip_set_particles")
+
+    def get_particles(self):
+        pos = np.zeros((self.n, 3), np.float32)
+        vel = np.zeros((self.n, 3), np.float32)
+        check(self.L.bnn_flip_get_particles(self.h, _p(pos, C.c_float), _p(vel, C.c_float)), "bnn_flip_get_particles")
+        return pos, vel
+
+    def grid(self, field) -> np.ndarray:
+        which = FIELD[field] if isinstance(field, str) else int(field)
+        if which in (0, 1, 2):
+            shape = self.face_shape(which)
+        elif which in (5, 6, 7):
+            shape = self.face_shape(which - 5)
+        else:
+            shape = self.G
+        out = np.zeros(int(np.prod(shape)), np.float32)
+        check(self.L.bnn_flip_get_grid(self.h, which, _p(out, C.c_float), out.size), "bnn_flip_get_grid")
+        return out.reshape(shape[::-1])
+
+    def step(self, allow_fail: bool = False) -> dict:
+        st = StepStats()
+        rc = self.L.bnn_flip_step(self.h, C.byref(st))
+        d = {f: getattr(st, f) for f, _ in StepStats._fields_ if f != "stage_ms"}
+        d["stage_ms"] = dict(zip(STAGES, list(st.stage_ms)))
+        d["status"] = rc
+        if rc != BNN_OK and not allow_fail:
+            raise BnnError(rc, "bnn_flip_step")
+        return d
+
+    def step_host(self, pos: np.ndarray, vel: np.ndarray) -> dict:
+        st = StepStats()
+        check(self.L.bnn_flip_step_host(self.h, _p(pos, C.c_float), _p(vel, C.c_float), C.byref(st)),
+              "bnn_flip_step_host")
+        d = {f: getattr(st, f) for f, _ in StepStats._fields_ if f != "stage_ms"}
+        d["stage_ms"] = dict(zip(STAGES, list(st.stage_ms)))
+        return d
+
+    def advance_frame(self) -> int:
+        k = C.c_uint32()
+        check(self.L.bnn_flip_advance_frame(self.h, C.byref(k)), "bnn_flip_advance_frame")
+        return k.value
+
+
+def pcg_solve_7pt(diag, nbr, offdiag, rhs, tol, max_iter, mode="fp32", inner_tol=1e-3):
+    L = load()
+    n = len(rhs)
+    d = np.ascontiguousarray(diag, np.float32)
+    nb = np.ascontiguousarray(nbr, np.int32).reshape(-1)
+    b = np.ascontiguousarray(rhs, np.float32)
+    x = np.zeros(max(n, 1), np.float64)
+    st = PcgStats()
+    m = PCG_MODE[mode] if isinstance(mode, str) else int(mode)
+    rc = L.bnn_pcg_solve_7pt(n, _p(d, C.c_float), _p(nb, C.c_int32), offdiag, _p(b, C.c_float), tol, max_iter, m,
+                             inner_tol, _p(x, C.c_double), C.byref(st))
+    if rc not in (BNN_OK, 3):
+        raise BnnError(rc, "bnn_pcg_solve_7pt")
+    return x[:n], {f: getattr(st, f) for f, _ in PcgStats._fields_}

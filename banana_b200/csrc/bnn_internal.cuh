@@ -1,0 +1,195 @@
+// Internal declarations shared by the CUDA translation units of libbanana_b200.
+//
+// Arithmetic rule for every kernel here: the library is compiled with -fmad=false and
+// IEEE division / square root, so each float operation rounds once, in the order it is
+// written.  The expressions below follow the reference's own evaluation order (each
+// device function cites the reference lines it computes), which is what lets the FLIP
+// step agree bit for bit with a serial run of the reference's CPU code.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <cfloat>
+
+#include "banana_b200.h"
+
+namespace bnn {
+
+// ----------------------------------------------------------------------------------
+// Canonical reduction layout: a vector is cut into 2048-element chunks, one 256-thread
+// block per chunk, thread t sums elements t, t+256, ... t+1792 of its chunk in FP64,
+// then a halving tree (128, 64, ..., 1).  Chunk partials are reduced the same way by
+// one block.  The result therefore depends only on n, never on the launch shape.
+// ----------------------------------------------------------------------------------
+constexpr int kLanes = 256;
+constexpr int kPerLane = 8;
+constexpr int kChunk = kLanes * kPerLane;
+
+__device__ __forceinline__ double block_sum_256(double v, double* sm) {
+    const int t = threadIdx.x;
+    sm[t] = v;
+    __syncthreads();
+#pragma unroll
+    for(int off = 128; off >= 32; off >>= 1) {
+        if(t < off) sm[t] = sm[t] + sm[t + off];
+        __syncthreads();
+    }
+    double r = 0.0;
+    if(t < 32) {
+        r = sm[t];
+#pragma unroll
+        for(int off = 16; off > 0; off >>= 1) r = r + __shfl_down_sync(0xffffffffu, r, off);
+    }
+    __syncthreads();
+    return r; // valid in thread 0
+}
+
+__device__ __forceinline__ float block_max_256(float v, float* sm) {
+    const int t = threadIdx.x;
+    sm[t] = v;
+    __syncthreads();
+    for(int off = 128; off >= 32; off >>= 1) {
+        if(t < off) { float o = sm[t + off]; sm[t] = sm[t] > o ? sm[t] : o; }
+        __syncthreads();
+    }
+    float r = 0.f;
+    if(t < 32) {
+        r = sm[t];
+        for(int off = 16; off > 0; off >>= 1) {
+            float o = __shfl_down_sync(0xffffffffu, r, off);
+            r = r > o ? r : o;
+        }
+    }
+    __syncthreads();
+    return r;
+}
+
+// Last-block-done: every block publishes its partial, then the block that arrives last
+// reduces all partials in the fixed order.  The counter is reset by that block.
+__device__ __forceinline__ bool last_block(unsigned* counter) {
+    __shared__ bool amLast;
+    __threadfence();
+    __syncthreads();
+    if(threadIdx.x == 0) {
+        unsigned prev = atomicAdd(counter, 1u);
+        amLast = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    return amLast;
+}
+
+// Final pass over chunk partials in the canonical order (called by one whole block)
+__device__ __forceinline__ double reduce_partials(const double* part, int nch, double* sm) {
+    double acc = 0.0;
+    for(int c = threadIdx.x; c < nch; c += kLanes) acc = acc + __ldcg(part + c);
+    return block_sum_256(acc, sm);
+}
+__device__ __forceinline__ float reduce_partials_max(const float* part, int nch, float* sm) {
+    float acc = 0.f;
+    for(int c = threadIdx.x; c < nch; c += kLanes) { float o = __ldcg(part + c); acc = acc > o ? acc : o; }
+    return block_max_256(acc, sm);
+}
+
+// ----------------------------------------------------------------------------------
+// Scalar helpers, same semantics as the reference's MathHelpers
+// ----------------------------------------------------------------------------------
+__device__ __forceinline__ float smin(float a, float b) { return (b < a) ? b : a; } // std::min
+__device__ __forceinline__ float smax(float a, float b) { return (a < b) ? b : a; } // std::max
+
+// MathHelpers::get_barycentric(x, i, f, 0, i_high) (MathHelpers.h:516-530)
+__device__ __forceinline__ void bary(float x, int& i, float& f, int i_high) {
+    float s = floorf(x);
+    i = (int)s;
+    if(i < 0) { i = 0; f = 0.f; }
+    else if(i > i_high - 2) { i = i_high - 2; f = 1.f; }
+    else { f = x - s; }
+}
+// MathHelpers::lerp (MathHelpers.h:549-551)
+__device__ __forceinline__ float lerpf(float v0, float v1, float f) { return (1.0f - f) * v0 + f * v1; }
+// MathHelpers::fraction_inside(left, right) (MathHelpers.h:823-838)
+__device__ __forceinline__ float fraction_inside(float l, float r) {
+    if(l < 0.f && r < 0.f) return 1.0f;
+    if(l < 0.f && r >= 0.f) return l / (l - r);
+    if(l >= 0.f && r < 0.f) return r / (r - l);
+    return 0.f;
+}
+__device__ __forceinline__ float length2f(float x, float y, float z) { return (x * x + y * y) + z * z; }
+
+// Grid description passed by value to kernels
+struct GridDesc {
+    int G[3];          // cells per axis (after padding)
+    float dx;          // cell size
+    float bmin[3];     // padded domain min
+    float boxMin[3];   // domain box (constraint) min
+    float boxMax[3];   // domain box max
+    float sdfRadius;   // PIC_Parameters::sdfRadius
+};
+
+__host__ __device__ __forceinline__ int face_sx(const GridDesc& g, int d) { return g.G[0] + (d == 0); }
+__host__ __device__ __forceinline__ int face_sy(const GridDesc& g, int d) { return g.G[1] + (d == 1); }
+__host__ __device__ __forceinline__ int face_sz(const GridDesc& g, int d) { return g.G[2] + (d == 2); }
+
+// Device-side state of one solver: PCG scalars, reduction counters and check flags
+struct DevState {
+    // PCG
+    double rho, tmp, dotv;
+    double alpha64, beta64;
+    float alpha, beta, resid, tol;
+    double resid64, tol64;
+    unsigned iter, done, success, max_iter;
+    unsigned counter0, counter1, counter2, counter3;
+    // step
+    unsigned maxvel_bits;   // max |u| over faces as float bits (non-negative)
+    unsigned flags;         // BNN device flags
+    unsigned n_active;
+    unsigned zero_phi;
+    unsigned out_of_range;
+    unsigned pad0;
+    double outer_res, outer_bmax;
+};
+
+#define BNN_FLAG_OUT_OF_GRID   1u
+#define BNN_FLAG_RING_FLUID    2u
+#define BNN_FLAG_PCG_MAXITER   4u
+#define BNN_FLAG_SCRATCH_LIMIT 8u
+
+// ----------------------------------------------------------------------------------
+// Host-side launchers (defined in the .cu files)
+// ----------------------------------------------------------------------------------
+// scan.cu
+size_t scan_workspace_bytes(size_t n);
+// exclusive scan of n uint32 into out[0..n], out[n] = total; ws from scan_workspace_bytes
+cudaError_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, size_t n, void* ws, cudaStream_t s);
+
+// pcg.cu
+struct PcgWork {
+    int cap = 0;
+    float *x = nullptr, *r = nullptr, *z = nullptr, *s0 = nullptr, *s1 = nullptr, *q = nullptr, *d32 = nullptr,
+          *r32 = nullptr;
+    double *x64 = nullptr, *r64 = nullptr, *z64 = nullptr, *s064 = nullptr, *s164 = nullptr, *q64 = nullptr,
+           *inv64 = nullptr;
+    double* part = nullptr;
+    float* partMaxF = nullptr;
+    double* partMaxD = nullptr;
+};
+struct PcgOutcome {
+    unsigned iterations = 0, outer = 0, success = 0;
+    double residual = 0;
+};
+int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const float* invd, const int32_t* nbr, float dt,
+              int mode, float tol, unsigned maxIter, float innerTol, float outerTol, float* pressure, double* x64out,
+              DevState* dst, DevState* hst, cudaStream_t s, PcgOutcome& out);
+void pcg_release(PcgWork& w);
+
+} // namespace bnn
+
+extern "C" void bnn_set_error(const char* msg);
+
+#define BNN_CUDA_CHECK(expr)                                                                 \
+    do {                                                                                     \
+        cudaError_t _e = (expr);                                                             \
+        if(_e != cudaSuccess) {                                                              \
+            bnn_set_error(cudaGetErrorString(_e));                                           \
+            return _e == cudaErrorMemoryAllocation ? BNN_ERR_OUT_OF_MEMORY : BNN_ERR_CUDA;   \
+        }                                                                                    \
+    } while(0)

@@ -1,0 +1,537 @@
+// C ABI of libbanana_b200: solver handle, memory, and the host-side order of one
+// FLIP / APIC / AFLIP sub-step (PIC_Solver::advanceFrame, PIC_Solver.cpp:267-311, and
+// FLIP_Solver::advanceVelocity, FLIP_Solver.cpp:42-53).
+#include "bnn_internal.cuh"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+static thread_local std::string g_lastError;
+extern "C" void bnn_set_error(const char* msg) { g_lastError = msg ? msg : ""; }
+extern "C" const char* bnn_last_error(void) { return g_lastError.c_str(); }
+extern "C" const char* bnn_version(void) { return "banana_b200 0.1 (sm_100a)"; }
+
+namespace bnn {
+// flip_kernels.cu
+void launch_advect(int n, float* p6, size_t stride, const float* const* U, const GridDesc& g, float sub, int steps,
+                   uint32_t* cellOf, uint32_t* slot, uint32_t* count, DevState* st, cudaStream_t s);
+void launch_cell_histogram(int n, const float* p6, size_t stride, const GridDesc& g, uint32_t* cellOf, uint32_t* slot,
+                           uint32_t* count, DevState* st, cudaStream_t s);
+void launch_sort_finish(int n, size_t ncells, const uint32_t* cellOf, const uint32_t* slot, const uint32_t* cellStart,
+                        uint32_t* order, uint32_t* count, const float* src6, float* dst6, const uint32_t* idSrc,
+                        uint32_t* idDst, const float* cSrc, float* cDst, float* g3, const GridDesc& g, size_t stride,
+                        cudaStream_t s);
+void launch_p2g(const GridDesc& g, const uint32_t* cellStart, const float* g3, const float* p6, const float* C9,
+                size_t stride, float* const* out, uint8_t* const* valid, bool affine, cudaStream_t s);
+void launch_extrapolate(const GridDesc& g, float* const* A, uint8_t* const* VA, float* const* B, uint8_t* const* VB,
+                        int lastMode, float* const* oldOut, float gravityDt, DevState* st, cudaStream_t s);
+void launch_fluid_sdf(const GridDesc& g, const uint32_t* cellStart, const float* g3, const float* p6, size_t stride,
+                      float* phi, cudaStream_t s);
+void launch_active_flags(const GridDesc& g, const float* phi, uint32_t* flag, DevState* st, cudaStream_t s);
+void launch_active_rows(size_t nc, const uint32_t* flag, const uint32_t* idx, uint32_t* rowCell, cudaStream_t s);
+void launch_build_rows(const GridDesc& g, int nrows, const uint32_t* rowCell, const float* phi, const uint32_t* aidx,
+                       const float* const* U, float dt, float* rhs, float* diag, float* invdiag, int32_t* nbr,
+                       DevState* st, cudaStream_t s);
+void launch_update_velocity(const GridDesc& g, const float* phi, const uint32_t* aidx, const float* pressure, float dt,
+                            float* const* U, uint8_t* const* V, cudaStream_t s);
+void launch_g2p(int n, const GridDesc& g, float* p6, size_t stride, const float* const* U, const float* const* O,
+                float ratio, int kind, float* C9, cudaStream_t s);
+void launch_aos_to_soa(int n, const float* pos, const float* vel, float* soa6, uint32_t* ids, size_t stride,
+                       cudaStream_t s);
+void launch_soa_to_aos(int n, const float* soa6, const uint32_t* ids, float* pos, float* vel, size_t stride,
+                       cudaStream_t s);
+void launch_cells_from_rows(size_t nc, const float* phi, const uint32_t* aidx, const float* pr, float* out, int active,
+                            cudaStream_t s);
+void launch_add_scalar(float* a, size_t n, float v, cudaStream_t s);
+void launch_step_reset(DevState* st, cudaStream_t s);
+
+// pcg.cu
+} // namespace bnn
+
+using namespace bnn;
+
+struct bnn_flip {
+    bnn_params P{};
+    GridDesc g{};
+    size_t C = 0;      // cells
+    size_t F[3] = {};  // faces per component
+    float frameDuration = 0.f, frameTime = 0.f;
+    uint32_t n = 0, cap = 0;
+    cudaStream_t s = nullptr;
+    // particles: SoA (x,y,z,vx,vy,vz) with stride cap; ping-pong for the sort
+    float* p6[2] = {nullptr, nullptr};
+    uint32_t* ids[2] = {nullptr, nullptr};
+    float* C9[2] = {nullptr, nullptr};
+    int cur = 0;
+    float* g3 = nullptr;
+    uint32_t *cellOf = nullptr, *slot = nullptr, *order = nullptr;
+    uint32_t *count = nullptr, *cellStart = nullptr;
+    void* scanWs = nullptr;
+    float* aosStage = nullptr;
+    // faces
+    float* U[3] = {};
+    float* B[3] = {};
+    float* O[3] = {};
+    uint8_t* VA[3] = {};
+    uint8_t* VB[3] = {};
+    // cells
+    float* phi = nullptr;
+    uint32_t* flag = nullptr;
+    uint32_t* aidx = nullptr; // C+1
+    float* cellTmp = nullptr;
+    // rows
+    int rowCap = 0;
+    uint32_t nRows = 0;
+    uint32_t* rowCell = nullptr;
+    float *rhs = nullptr, *diag = nullptr, *invd = nullptr, *pressure = nullptr;
+    int32_t* nbr = nullptr;
+    PcgWork pcg;
+    DevState* dst = nullptr;
+    DevState* hst = nullptr;
+    cudaEvent_t ev[11] = {};
+    unsigned maxvelBits = 0; // max|u| of the current grid (for the next CFL)
+};
+
+static void free_particles(bnn_flip* h) {
+    for(int b = 0; b < 2; ++b) {
+        cudaFree(h->p6[b]); cudaFree(h->ids[b]); cudaFree(h->C9[b]);
+        h->p6[b] = nullptr; h->ids[b] = nullptr; h->C9[b] = nullptr;
+    }
+    cudaFree(h->g3); cudaFree(h->cellOf); cudaFree(h->slot); cudaFree(h->order); cudaFree(h->aosStage);
+    h->g3 = nullptr; h->cellOf = h->slot = h->order = nullptr; h->aosStage = nullptr;
+    h->cap = 0;
+}
+
+static int reserve_particles(bnn_flip* h, uint32_t n) {
+    if(n <= h->cap) return BNN_OK;
+    free_particles(h);
+    uint32_t cap = n;
+    size_t st = cap;
+    for(int b = 0; b < 2; ++b) {
+        BNN_CUDA_CHECK(cudaMalloc(&h->p6[b], 6 * st * sizeof(float)));
+        BNN_CUDA_CHECK(cudaMalloc(&h->ids[b], st * sizeof(uint32_t)));
+        if(h->P.solver_kind == BNN_SOLVER_APIC || h->P.solver_kind == BNN_SOLVER_AFLIP)
+            BNN_CUDA_CHECK(cudaMalloc(&h->C9[b], 9 * st * sizeof(float)));
+    }
+    BNN_CUDA_CHECK(cudaMalloc(&h->g3, 3 * st * sizeof(float)));
+    BNN_CUDA_CHECK(cudaMalloc(&h->cellOf, st * sizeof(uint32_t)));
+    BNN_CUDA_CHECK(cudaMalloc(&h->slot, st * sizeof(uint32_t)));
+    BNN_CUDA_CHECK(cudaMalloc(&h->order, st * sizeof(uint32_t)));
+    BNN_CUDA_CHECK(cudaMalloc(&h->aosStage, 6 * st * sizeof(float)));
+    h->cap = cap;
+    return BNN_OK;
+}
+
+static int reserve_rows(bnn_flip* h, uint32_t n) {
+    if((int)n <= h->rowCap) return BNN_OK;
+    cudaFree(h->rowCell); cudaFree(h->rhs); cudaFree(h->diag); cudaFree(h->invd); cudaFree(h->pressure); cudaFree(h->nbr);
+    int cap = (int)(n * 1.25) + 1024;
+    if((size_t)cap > h->C) cap = (int)h->C;
+    BNN_CUDA_CHECK(cudaMalloc(&h->rowCell, cap * sizeof(uint32_t)));
+    BNN_CUDA_CHECK(cudaMalloc(&h->rhs, cap * sizeof(float)));
+    BNN_CUDA_CHECK(cudaMalloc(&h->diag, cap * sizeof(float)));
+    BNN_CUDA_CHECK(cudaMalloc(&h->invd, cap * sizeof(float)));
+    BNN_CUDA_CHECK(cudaMalloc(&h->pressure, cap * sizeof(float)));
+    BNN_CUDA_CHECK(cudaMalloc(&h->nbr, 6 * (size_t)cap * sizeof(int32_t)));
+    h->rowCap = cap;
+    return BNN_OK;
+}
+
+static void destroy_all(bnn_flip* h) {
+    if(!h) return;
+    free_particles(h);
+    for(int d = 0; d < 3; ++d) {
+        cudaFree(h->U[d]); cudaFree(h->B[d]); cudaFree(h->O[d]); cudaFree(h->VA[d]); cudaFree(h->VB[d]);
+    }
+    cudaFree(h->count); cudaFree(h->cellStart); cudaFree(h->scanWs); cudaFree(h->phi); cudaFree(h->flag);
+    cudaFree(h->aidx); cudaFree(h->cellTmp);
+    cudaFree(h->rowCell); cudaFree(h->rhs); cudaFree(h->diag); cudaFree(h->invd); cudaFree(h->pressure); cudaFree(h->nbr);
+    pcg_release(h->pcg);
+    cudaFree(h->dst);
+    if(h->hst) cudaFreeHost(h->hst);
+    for(auto& e : h->ev) if(e) cudaEventDestroy(e);
+    if(h->s) cudaStreamDestroy(h->s);
+    delete h;
+}
+
+extern "C" int bnn_flip_create(const bnn_params* params, bnn_flip** out) {
+    if(!params || !out) return BNN_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    const bnn_params& P = *params;
+    if(!(P.cell_size > 0.f) || P.advection_steps == 0) return BNN_ERR_INVALID_ARGUMENT;
+    if(P.solver_kind < 0 || P.solver_kind > 2) return BNN_ERR_NOT_SUPPORTED;
+    if(P.pcg_mode < 0 || P.pcg_mode > 2 || P.preconditioner != BNN_PRECOND_JACOBI) return BNN_ERR_NOT_SUPPORTED;
+    for(int d = 0; d < 3; ++d) if(!(P.box_max[d] > P.box_min[d])) return BNN_ERR_INVALID_ARGUMENT;
+    auto* h = new bnn_flip();
+    h->P = P;
+    // SimulationParameters::makeReady (ParticleSolverData.cpp:229-272), Grid::setCellSize
+    // (Grid.cpp:38-55), PIC_Parameters::makeReady (PIC_Data.cpp:41-44)
+    const float dx = P.cell_size;
+    const float pad = dx * (float)P.n_expand_cells;
+    h->g.dx = dx;
+    for(int d = 0; d < 3; ++d) {
+        h->g.boxMin[d] = P.box_min[d];
+        h->g.boxMax[d] = P.box_max[d];
+        h->g.bmin[d] = P.box_min[d] - pad;
+        const float bmax = P.box_max[d] + pad;
+        h->g.G[d] = (int)(uint32_t)std::ceil((bmax - h->g.bmin[d]) / dx);
+        if(h->g.G[d] < 3) { delete h; return BNN_ERR_INVALID_ARGUMENT; }
+    }
+    h->g.sdfRadius = dx * (float)(1.01 * std::sqrt(3.0) / 2.0);
+    h->frameDuration = P.frame_duration;
+    h->frameTime = P.frame_duration;
+    h->C = (size_t)h->g.G[0] * h->g.G[1] * h->g.G[2];
+    if(h->C >= (size_t)0x7fffffff) { delete h; return BNN_ERR_NOT_SUPPORTED; }
+    for(int d = 0; d < 3; ++d) h->F[d] = (size_t)face_sx(h->g, d) * face_sy(h->g, d) * face_sz(h->g, d);
+    cudaError_t e = cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking);
+    if(e != cudaSuccess) { bnn_set_error(cudaGetErrorString(e)); delete h; return BNN_ERR_CUDA; }
+    int rc = BNN_OK;
+    auto ok = [&](cudaError_t err) {
+        if(err != cudaSuccess && rc == BNN_OK) {
+            bnn_set_error(cudaGetErrorString(err));
+            rc = err == cudaErrorMemoryAllocation ? BNN_ERR_OUT_OF_MEMORY : BNN_ERR_CUDA;
+        }
+    };
+    for(int d = 0; d < 3; ++d) {
+        ok(cudaMalloc(&h->U[d], h->F[d] * sizeof(float)));
+        ok(cudaMalloc(&h->B[d], h->F[d] * sizeof(float)));
+        ok(cudaMalloc(&h->O[d], h->F[d] * sizeof(float)));
+        ok(cudaMalloc(&h->VA[d], h->F[d]));
+        ok(cudaMalloc(&h->VB[d], h->F[d]));
+    }
+    ok(cudaMalloc(&h->count, h->C * sizeof(uint32_t)));
+    ok(cudaMalloc(&h->cellStart, (h->C + 1) * sizeof(uint32_t)));
+    size_t ws = scan_workspace_bytes(h->C);
+    if(ws) ok(cudaMalloc(&h->scanWs, ws));
+    ok(cudaMalloc(&h->phi, h->C * sizeof(float)));
+    ok(cudaMalloc(&h->flag, h->C * sizeof(uint32_t)));
+    ok(cudaMalloc(&h->aidx, (h->C + 1) * sizeof(uint32_t)));
+    ok(cudaMalloc(&h->dst, sizeof(DevState)));
+    ok(cudaHostAlloc(&h->hst, sizeof(DevState), cudaHostAllocDefault));
+    for(auto& ev : h->ev) ok(cudaEventCreate(&ev));
+    if(rc != BNN_OK) { destroy_all(h); return rc; }
+    for(int d = 0; d < 3; ++d) {
+        ok(cudaMemsetAsync(h->U[d], 0, h->F[d] * sizeof(float), h->s));
+        ok(cudaMemsetAsync(h->O[d], 0, h->F[d] * sizeof(float), h->s));
+        ok(cudaMemsetAsync(h->VA[d], 0, h->F[d], h->s));
+    }
+    ok(cudaMemsetAsync(h->count, 0, h->C * sizeof(uint32_t), h->s));
+    ok(cudaMemsetAsync(h->phi, 0, h->C * sizeof(float), h->s));
+    ok(cudaMemsetAsync(h->aidx, 0, (h->C + 1) * sizeof(uint32_t), h->s));
+    ok(cudaMemsetAsync(h->dst, 0, sizeof(DevState), h->s));
+    ok(cudaStreamSynchronize(h->s));
+    std::memset(h->hst, 0, sizeof(DevState));
+    if(rc == BNN_OK && P.max_particles) rc = reserve_particles(h, P.max_particles);
+    if(rc != BNN_OK) { destroy_all(h); return rc; }
+    *out = h;
+    return BNN_OK;
+}
+
+extern "C" int bnn_flip_destroy(bnn_flip* h) {
+    if(!h) return BNN_ERR_INVALID_ARGUMENT;
+    if(h->s) cudaStreamSynchronize(h->s);
+    destroy_all(h);
+    return BNN_OK;
+}
+
+extern "C" int bnn_flip_grid_dims(bnn_flip* h, int32_t g[3]) {
+    if(!h || !g) return BNN_ERR_INVALID_ARGUMENT;
+    for(int d = 0; d < 3; ++d) g[d] = h->g.G[d];
+    return BNN_OK;
+}
+
+extern "C" int bnn_flip_num_particles(bnn_flip* h, uint32_t* n) {
+    if(!h || !n) return BNN_ERR_INVALID_ARGUMENT;
+    *n = h->n;
+    return BNN_OK;
+}
+
+// Upload into the current SoA buffers in caller order (ids = 0..n-1)
+static int upload_particles(bnn_flip* h, const float* pos, const float* vel, uint32_t n) {
+    BNN_CUDA_CHECK(cudaMemcpyAsync(h->aosStage, pos, 3 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice, h->s));
+    BNN_CUDA_CHECK(cudaMemcpyAsync(h->aosStage + 3 * (size_t)h->cap, vel, 3 * (size_t)n * sizeof(float),
+                                   cudaMemcpyHostToDevice, h->s));
+    launch_aos_to_soa((int)n, h->aosStage, h->aosStage + 3 * (size_t)h->cap, h->p6[h->cur], h->ids[h->cur], h->cap, h->s);
+    return BNN_OK;
+}
+
+extern "C" int bnn_flip_set_particles(bnn_flip* h, const float* pos, const float* vel, uint32_t n) {
+    if(!h || (n && (!pos || !vel))) return BNN_ERR_INVALID_ARGUMENT;
+    if((size_t)n >= (size_t)0x7fffffff) return BNN_ERR_INVALID_ARGUMENT;
+    int rc = reserve_particles(h, n);
+    if(rc != BNN_OK) return rc;
+    h->n = n;
+    h->cur = 0;
+    if(n) {
+        rc = upload_particles(h, pos, vel, n);
+        if(rc != BNN_OK) return rc;
+    }
+    if(h->C9[0]) BNN_CUDA_CHECK(cudaMemsetAsync(h->C9[0], 0, 9 * (size_t)h->cap * sizeof(float), h->s));
+    for(int d = 0; d < 3; ++d) {
+        BNN_CUDA_CHECK(cudaMemsetAsync(h->U[d], 0, h->F[d] * sizeof(float), h->s));
+        BNN_CUDA_CHECK(cudaMemsetAsync(h->O[d], 0, h->F[d] * sizeof(float), h->s));
+        BNN_CUDA_CHECK(cudaMemsetAsync(h->VA[d], 0, h->F[d], h->s));
+    }
+    BNN_CUDA_CHECK(cudaMemsetAsync(h->count, 0, h->C * sizeof(uint32_t), h->s));
+    BNN_CUDA_CHECK(cudaStreamSynchronize(h->s));
+    h->maxvelBits = 0;
+    h->frameTime = h->frameDuration;
+    h->nRows = 0;
+    return BNN_OK;
+}
+
+extern "C" int bnn_flip_get_particles(bnn_flip* h, float* pos, float* vel) {
+    if(!h || (h->n && (!pos || !vel))) return BNN_ERR_INVALID_ARGUMENT;
+    if(!h->n) return BNN_OK;
+    launch_soa_to_aos((int)h->n, h->p6[h->cur], h->ids[h->cur], h->aosStage, h->aosStage + 3 * (size_t)h->cap, h->cap,
+                      h->s);
+    BNN_CUDA_CHECK(cudaMemcpyAsync(pos, h->aosStage, 3 * (size_t)h->n * sizeof(float), cudaMemcpyDeviceToHost, h->s));
+    BNN_CUDA_CHECK(cudaMemcpyAsync(vel, h->aosStage + 3 * (size_t)h->cap, 3 * (size_t)h->n * sizeof(float),
+                                   cudaMemcpyDeviceToHost, h->s));
+    BNN_CUDA_CHECK(cudaStreamSynchronize(h->s));
+    return BNN_OK;
+}
+
+extern "C" int bnn_flip_device_particles(bnn_flip* h, float** p6, uint32_t** ids) {
+    if(!h) return BNN_ERR_INVALID_ARGUMENT;
+    if(p6) *p6 = h->p6[h->cur];
+    if(ids) *ids = h->ids[h->cur];
+    return BNN_OK;
+}
+
+extern "C" int bnn_flip_get_grid(bnn_flip* h, int32_t field, float* out, size_t count) {
+    if(!h || !out) return BNN_ERR_INVALID_ARGUMENT;
+    const float* src = nullptr;
+    size_t need = 0;
+    if(field >= BNN_FIELD_U && field <= BNN_FIELD_W) { src = h->U[field]; need = h->F[field]; }
+    else if(field >= BNN_FIELD_OLD_U && field <= BNN_FIELD_OLD_W) { src = h->O[field - 5]; need = h->F[field - 5]; }
+    else if(field == BNN_FIELD_PHI) { src = h->phi; need = h->C; }
+    else if(field == BNN_FIELD_PRESSURE || field == BNN_FIELD_ACTIVE) {
+        need = h->C;
+        if(count < need) return BNN_ERR_INVALID_ARGUMENT;
+        if(!h->cellTmp) BNN_CUDA_CHECK(cudaMalloc(&h->cellTmp, h->C * sizeof(float)));
+        if(h->nRows == 0 && field == BNN_FIELD_PRESSURE) {
+            BNN_CUDA_CHECK(cudaMemsetAsync(h->cellTmp, 0, h->C * sizeof(float), h->s));
+        } else {
+            launch_cells_from_rows(h->C, h->phi, h->aidx, h->pressure, h->cellTmp, field == BNN_FIELD_ACTIVE, h->s);
+        }
+        src = h->cellTmp;
+    } else {
+        return BNN_ERR_INVALID_ARGUMENT;
+    }
+    if(count < need) return BNN_ERR_INVALID_ARGUMENT;
+    BNN_CUDA_CHECK(cudaMemcpyAsync(out, src, need * sizeof(float), cudaMemcpyDeviceToHost, h->s));
+    BNN_CUDA_CHECK(cudaStreamSynchronize(h->s));
+    return BNN_OK;
+}
+
+// PIC_Solver::timestepCFL (PIC_Solver.cpp:342-349) from max|u| of the current grid
+static float timestep_cfl(const bnn_flip* h) {
+    float m;
+    std::memcpy(&m, &h->maxvelBits, 4);
+    float maxVel = FLT_MIN;
+    maxVel = (maxVel < m) ? m : maxVel;
+    float ts = maxVel > FLT_MIN ? h->P.cfl_factor * (h->g.dx / maxVel) : FLT_MAX;
+    if(ts < h->P.min_timestep) return h->P.min_timestep;
+    if(ts > h->P.max_timestep) return h->P.max_timestep;
+    return ts;
+}
+
+static int run_substep(bnn_flip* h, bnn_step_stats* st) {
+    cudaStream_t s = h->s;
+    const GridDesc& g = h->g;
+    if(h->frameTime >= h->frameDuration) h->frameTime = 0.f;
+    // PIC_Solver::advanceFrame sub-step size (PIC_Solver.cpp:284-290)
+    float substep = timestep_cfl(h);
+    const float remaining = h->frameDuration - h->frameTime;
+    if(h->frameTime + substep >= h->frameDuration) substep = remaining;
+    else if(h->frameTime + 1.5f * substep >= h->frameDuration) substep = remaining * 0.5f;
+    const float sub = substep / (float)h->P.advection_steps;
+    const int kind = h->P.solver_kind;
+    const bool affine = kind == BNN_SOLVER_APIC || kind == BNN_SOLVER_AFLIP;
+    const int n = (int)h->n;
+
+    cudaEventRecord(h->ev[0], s);
+    launch_step_reset(h->dst, s);
+    // moveParticles + counting sort (histogram while advecting)
+    launch_advect(n, h->p6[h->cur], h->cap, h->U, g, sub, (int)h->P.advection_steps, h->cellOf, h->slot, h->count,
+                  h->dst, s);
+    cudaEventRecord(h->ev[1], s);
+    BNN_CUDA_CHECK(exclusive_scan_u32(h->count, h->cellStart, h->C, h->scanWs, s));
+    const int nxt = 1 - h->cur;
+    launch_sort_finish(n, h->C, h->cellOf, h->slot, h->cellStart, h->order, h->count, h->p6[h->cur], h->p6[nxt],
+                       h->ids[h->cur], h->ids[nxt], affine ? h->C9[h->cur] : nullptr, affine ? h->C9[nxt] : nullptr,
+                       h->g3, g, h->cap, s);
+    h->cur = nxt;
+    cudaEventRecord(h->ev[2], s);
+    // P2G
+    launch_p2g(g, h->cellStart, h->g3, h->p6[h->cur], affine ? h->C9[h->cur] : nullptr, h->cap, h->U, h->VA, affine, s);
+    cudaEventRecord(h->ev[3], s);
+    const float gdt = h->P.apply_gravity ? 9.81f * substep : 0.f;
+    if(kind == BNN_SOLVER_APIC) {
+        // APIC_Solver::advanceVelocity: P2G then gravity, no extrapolation / backup
+        if(h->P.apply_gravity) launch_add_scalar(h->U[1], h->F[1], -gdt, s);
+    } else {
+        // extrapolate, backup oldVels, Earth gravity (FLIP_Solver.cpp:44-47)
+        launch_extrapolate(g, h->U, h->VA, h->B, h->VB, 1, h->O, gdt, h->dst, s);
+    }
+    cudaEventRecord(h->ev[4], s);
+    // pressure projection (PIC_Solver.cpp:533-539)
+    launch_fluid_sdf(g, h->cellStart, h->g3, h->p6[h->cur], h->cap, h->phi, s);
+    cudaEventRecord(h->ev[5], s);
+    launch_active_flags(g, h->phi, h->flag, h->dst, s);
+    BNN_CUDA_CHECK(exclusive_scan_u32(h->flag, h->aidx, h->C, h->scanWs, s));
+    uint32_t nrows = 0;
+    BNN_CUDA_CHECK(cudaMemcpyAsync(&h->hst->n_active, h->aidx + h->C, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    BNN_CUDA_CHECK(cudaStreamSynchronize(s));
+    nrows = h->hst->n_active;
+    int rc = reserve_rows(h, nrows);
+    if(rc != BNN_OK) return rc;
+    h->nRows = nrows;
+    launch_active_rows(h->C, h->flag, h->aidx, h->rowCell, s);
+    launch_build_rows(g, (int)nrows, h->rowCell, h->phi, h->aidx, h->U, substep, h->rhs, h->diag, h->invd, h->nbr,
+                      h->dst, s);
+    cudaEventRecord(h->ev[6], s);
+    PcgOutcome po;
+    rc = pcg_solve(h->pcg, (int)nrows, h->rhs, h->diag, h->invd, h->nbr, substep, h->P.pcg_mode,
+                   h->P.cg_relative_tolerance, h->P.max_cg_iteration, h->P.refine_inner_tolerance,
+                   h->P.refine_tolerance, h->pressure, nullptr, h->dst, h->hst, s, po);
+    if(rc != BNN_OK) return rc;
+    cudaEventRecord(h->ev[7], s);
+    launch_update_velocity(g, h->phi, h->aidx, h->pressure, substep, h->U, h->VA, s);
+    launch_extrapolate(g, h->U, h->VA, h->B, h->VB, 2, nullptr, 0.f, h->dst, s);
+    cudaEventRecord(h->ev[8], s);
+    launch_g2p(n, g, h->p6[h->cur], h->cap, h->U, h->O, h->P.pic_flip_ratio, kind, affine ? h->C9[h->cur] : nullptr, s);
+    cudaEventRecord(h->ev[9], s);
+    BNN_CUDA_CHECK(cudaGetLastError());
+    BNN_CUDA_CHECK(cudaMemcpyAsync(h->hst, h->dst, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+    BNN_CUDA_CHECK(cudaStreamSynchronize(s));
+    h->maxvelBits = h->hst->maxvel_bits;
+    h->frameTime += substep;
+    if(st) {
+        st->dt = substep;
+        st->frame_time = h->frameTime;
+        st->frame_finished = h->frameTime >= h->frameDuration ? 1u : 0u;
+        st->pcg_iterations = po.iterations;
+        st->pcg_residual = po.residual;
+        st->pcg_success = po.success;
+        st->n_active = nrows;
+        st->outer_iterations = po.outer;
+        st->zero_phi_cells = h->hst->zero_phi;
+        st->device_flags = h->hst->flags;
+        const int map[10][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 4}, {4, 5}, {5, 6}, {6, 7}, {7, 8}, {8, 9}, {0, 9}};
+        for(int q = 0; q < 10; ++q) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, h->ev[map[q][0]], h->ev[map[q][1]]);
+            st->stage_ms[q] = ms;
+        }
+    }
+    if(h->hst->flags & BNN_FLAG_OUT_OF_GRID) return BNN_ERR_DEVICE_CHECK;
+    if(!po.success) return BNN_ERR_PCG_NOT_CONVERGED;
+    return BNN_OK;
+}
+
+extern "C" int bnn_flip_step(bnn_flip* h, bnn_step_stats* st) {
+    if(!h) return BNN_ERR_INVALID_ARGUMENT;
+    if(st) std::memset(st, 0, sizeof(*st));
+    return run_substep(h, st);
+}
+
+extern "C" int bnn_flip_step_host(bnn_flip* h, float* pos, float* vel, bnn_step_stats* st) {
+    if(!h || (h->n && (!pos || !vel))) return BNN_ERR_INVALID_ARGUMENT;
+    if(st) std::memset(st, 0, sizeof(*st));
+    if(h->n) {
+        // The caller's arrays are in caller order: the ids restart at 0..n-1.  The sort is
+        // by (cell, id), so the step computes the same result as the resident path.
+        int rc = upload_particles(h, pos, vel, h->n);
+        if(rc != BNN_OK) return rc;
+    }
+    int rc = run_substep(h, st);
+    int rc2 = bnn_flip_get_particles(h, pos, vel);
+    return rc != BNN_OK ? rc : rc2;
+}
+
+extern "C" int bnn_flip_advance_frame(bnn_flip* h, uint32_t* substeps) {
+    if(!h) return BNN_ERR_INVALID_ARGUMENT;
+    uint32_t k = 0;
+    bnn_step_stats st;
+    do {
+        int rc = bnn_flip_step(h, &st);
+        ++k;
+        if(rc != BNN_OK) { if(substeps) *substeps = k; return rc; }
+    } while(!st.frame_finished);
+    if(substeps) *substeps = k;
+    return BNN_OK;
+}
+
+// ---------------------------------------------------------------------------------
+// Standalone PCG on a 7-point system
+// ---------------------------------------------------------------------------------
+extern "C" int bnn_pcg_solve_7pt(uint32_t n, const float* diag, const int32_t* nbr, float offdiag, const float* rhs,
+                                 float tol, uint32_t max_iter, int32_t mode, float inner_tol, double* x_out,
+                                 bnn_pcg_stats* stats) {
+    if(!diag || !nbr || !rhs || !x_out || mode < 0 || mode > 2) return BNN_ERR_INVALID_ARGUMENT;
+    if(!(offdiag <= 0.f)) return BNN_ERR_INVALID_ARGUMENT;
+    cudaStream_t s;
+    BNN_CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    float *dDiag = nullptr, *dInv = nullptr, *dRhs = nullptr, *dP = nullptr;
+    int32_t* dNbr = nullptr;
+    double* dX = nullptr;
+    DevState *dst = nullptr, *hst = nullptr;
+    PcgWork w;
+    int rc = BNN_OK;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    std::vector<float> inv(n);
+    std::vector<int32_t> planes(6 * (size_t)n);
+    for(uint32_t r = 0; r < n; ++r) {
+        inv[r] = diag[r] != 0.f ? 1.0f / diag[r] : 0.f;
+        for(int q = 0; q < 6; ++q) planes[(size_t)q * n + r] = nbr[6 * (size_t)r + q];
+    }
+    // the system stores -dt as the off-diagonal; recover dt so the kernels form -(1*dt)
+    const float dt = -offdiag;
+    size_t nn = n ? n : 1;
+    auto chk = [&](cudaError_t e) { if(e != cudaSuccess && rc == BNN_OK) { bnn_set_error(cudaGetErrorString(e)); rc = BNN_ERR_CUDA; } };
+    chk(cudaMalloc(&dDiag, nn * 4)); chk(cudaMalloc(&dInv, nn * 4)); chk(cudaMalloc(&dRhs, nn * 4));
+    chk(cudaMalloc(&dP, nn * 4)); chk(cudaMalloc(&dNbr, 6 * nn * 4)); chk(cudaMalloc(&dX, nn * 8));
+    chk(cudaMalloc(&dst, sizeof(DevState))); chk(cudaHostAlloc(&hst, sizeof(DevState), cudaHostAllocDefault));
+    if(rc == BNN_OK && n) {
+        chk(cudaMemcpyAsync(dDiag, diag, n * 4, cudaMemcpyHostToDevice, s));
+        chk(cudaMemcpyAsync(dInv, inv.data(), n * 4, cudaMemcpyHostToDevice, s));
+        chk(cudaMemcpyAsync(dRhs, rhs, n * 4, cudaMemcpyHostToDevice, s));
+        chk(cudaMemcpyAsync(dNbr, planes.data(), 6 * (size_t)n * 4, cudaMemcpyHostToDevice, s));
+    }
+    if(rc == BNN_OK) chk(cudaMemsetAsync(dst, 0, sizeof(DevState), s));
+    if(rc == BNN_OK) chk(cudaStreamSynchronize(s));
+    PcgOutcome po;
+    if(rc == BNN_OK) {
+        cudaEventRecord(e0, s);
+        rc = pcg_solve(w, (int)n, dRhs, dDiag, dInv, dNbr, dt, mode, tol, max_iter, inner_tol, tol, dP, dX, dst, hst, s,
+                       po);
+        cudaEventRecord(e1, s);
+    }
+    if(rc == BNN_OK && n) chk(cudaMemcpyAsync(x_out, dX, n * 8, cudaMemcpyDeviceToHost, s));
+    if(rc == BNN_OK) chk(cudaStreamSynchronize(s));
+    if(stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->iterations = po.iterations;
+        stats->outer_iterations = po.outer;
+        stats->residual = po.residual;
+        stats->success = po.success;
+        float ms = 0.f;
+        if(rc == BNN_OK) cudaEventElapsedTime(&ms, e0, e1);
+        stats->ms = ms;
+    }
+    pcg_release(w);
+    cudaFree(dDiag); cudaFree(dInv); cudaFree(dRhs); cudaFree(dP); cudaFree(dNbr); cudaFree(dX); cudaFree(dst);
+    if(hst) cudaFreeHost(hst);
+    cudaEventDestroy(e0); cudaEventDestroy(e1);
+    cudaStreamDestroy(s);
+    if(rc == BNN_OK && !po.success) return BNN_ERR_PCG_NOT_CONVERGED;
+    return rc;
+}

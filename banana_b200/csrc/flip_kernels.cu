@@ -1,0 +1,780 @@
+// Kernels of one FLIP / APIC / AFLIP sub-step on a single B200.
+//
+// Layout in HBM (one solver):
+//   particles  SoA float x[], y[], z[], vx[], vy[], vz[] + uint32 id[] (original index),
+//              kept physically sorted by cell (stable counting sort every step), plus the
+//              grid coordinates gx[], gy[], gz[] of the sorted particles;
+//   faces      u (G+1)GG, v G(G+1)G, w GG(G+1) floats in the reference's (k*Sy+j)*Sx+i
+//              order, with uint8 valid flags and a ping-pong buffer for extrapolation;
+//   cells      fluid SDF (float), cell histogram / start offsets (uint32), active index;
+//   rows       the pressure system compacted to fluid cells (see pcg.cu).
+//
+// Every kernel is a gather: each output element is produced by exactly one thread, in
+// the order the reference's serial loop would produce it, so no float atomics are used
+// and results are bit-reproducible.
+#include "bnn_internal.cuh"
+
+namespace bnn {
+
+// ----------------------------------------------------------------------------------
+// Staggered-grid sampling
+// ----------------------------------------------------------------------------------
+// ArrayHelpers::interpolateValueLinear 3D (ArrayHelpers.cpp:91-102) with trilerp
+// (MathHelpers.h:564-573)
+__device__ __forceinline__ float interp_face(const float* __restrict__ a, int sx, int sy, int sz, float px, float py,
+                                             float pz) {
+    int i, j, k;
+    float fi, fj, fk;
+    bary(px, i, fi, sx);
+    bary(py, j, fj, sy);
+    bary(pz, k, fk, sz);
+    const size_t sxy = (size_t)sx * sy;
+    const size_t b = (size_t)k * sxy + (size_t)j * sx + i;
+    float v000 = __ldg(a + b), v100 = __ldg(a + b + 1), v010 = __ldg(a + b + sx), v110 = __ldg(a + b + sx + 1);
+    float v001 = __ldg(a + b + sxy), v101 = __ldg(a + b + sxy + 1), v011 = __ldg(a + b + sxy + sx),
+          v111 = __ldg(a + b + sxy + sx + 1);
+    return lerpf(lerpf(lerpf(v000, v100, fi), lerpf(v010, v110, fi), fj),
+                 lerpf(lerpf(v001, v101, fi), lerpf(v011, v111, fi), fj), fk);
+}
+
+// Same trilinear sample of (a - b), the FLIP velocity change dVels = velocities - oldVels
+// (FLIP_Solver.cpp:115-121) formed tap by tap, as if the difference array existed.
+__device__ __forceinline__ float interp_face_diff(const float* __restrict__ a, const float* __restrict__ o, int sx,
+                                                  int sy, int sz, float px, float py, float pz) {
+    int i, j, k;
+    float fi, fj, fk;
+    bary(px, i, fi, sx);
+    bary(py, j, fj, sy);
+    bary(pz, k, fk, sz);
+    const size_t sxy = (size_t)sx * sy;
+    const size_t b = (size_t)k * sxy + (size_t)j * sx + i;
+#define D_(off) (__ldg(a + b + (off)) - __ldg(o + b + (off)))
+    float v000 = D_(0), v100 = D_(1), v010 = D_(sx), v110 = D_(sx + 1);
+    float v001 = D_(sxy), v101 = D_(sxy + 1), v011 = D_(sxy + sx), v111 = D_(sxy + sx + 1);
+#undef D_
+    return lerpf(lerpf(lerpf(v000, v100, fi), lerpf(v010, v110, fi), fj),
+                 lerpf(lerpf(v001, v101, fi), lerpf(v011, v111, fi), fj), fk);
+}
+
+// PIC_Solver::getVelocityFromGrid(gridPos) (PIC_Solver.cpp:1119-1133)
+__device__ __forceinline__ void vel_from_grid(const GridDesc& g, const float* u, const float* v, const float* w,
+                                              float gx, float gy, float gz, float out[3]) {
+    out[0] = interp_face(u, g.G[0] + 1, g.G[1], g.G[2], gx, gy - 0.5f, gz - 0.5f);
+    out[1] = interp_face(v, g.G[0], g.G[1] + 1, g.G[2], gx - 0.5f, gy, gz - 0.5f);
+    out[2] = interp_face(w, g.G[0], g.G[1], g.G[2] + 1, gx - 0.5f, gy - 0.5f, gz);
+}
+
+// ----------------------------------------------------------------------------------
+// Domain-box boundary (negative outside the box)
+// ----------------------------------------------------------------------------------
+// BoxObject::signedDistance with bNegativeInside = false (GeometryObjects.cpp:246-268)
+__device__ __forceinline__ float box_sdf(const GridDesc& g, float x, float y, float z) {
+    const float p[3] = {x, y, z};
+    bool inside = true;
+#pragma unroll
+    for(int d = 0; d < 3; ++d)
+        if(p[d] < g.boxMin[d] || p[d] > g.boxMax[d]) inside = false;
+    float mind = FLT_MAX;
+    if(inside) {
+#pragma unroll
+        for(int d = 0; d < 3; ++d) mind = smin(mind, smin(p[d] - g.boxMin[d], g.boxMax[d] - p[d]));
+        mind = -mind;
+    } else {
+        float c[3];
+#pragma unroll
+        for(int d = 0; d < 3; ++d) c[d] = smax(smin(p[d], g.boxMax[d]), g.boxMin[d]);
+        mind = sqrtf(length2f(p[0] - c[0], p[1] - c[1], p[2] - c[2]));
+    }
+    mind = -mind;
+    return 1.0f * mind;
+}
+
+// BoundaryObject::constrainToBoundary (BoundaryObject.cpp:72-90) with the 8-point
+// finite-difference gradient of GeometryObject::gradSignedDistance (GeometryObjects.cpp:37-85)
+__device__ __forceinline__ void constrain_to_box(const GridDesc& g, float& x, float& y, float& z) {
+    const float phiVal = box_sdf(g, x, y, z);
+    if(phiVal < 0.f) {
+        const float e = 1e-4f;
+        float v000 = box_sdf(g, x - e, y - e, z - e), v001 = box_sdf(g, x - e, y - e, z + e);
+        float v010 = box_sdf(g, x - e, y + e, z - e), v011 = box_sdf(g, x - e, y + e, z + e);
+        float v100 = box_sdf(g, x + e, y - e, z - e), v101 = box_sdf(g, x + e, y - e, z + e);
+        float v110 = box_sdf(g, x + e, y + e, z - e), v111 = box_sdf(g, x + e, y + e, z + e);
+        float gx = ((((v100 - v000) + (v101 - v001)) + (v110 - v010)) + (v111 - v011)) * 0.25f;
+        float gy = ((((v010 - v000) + (v011 - v001)) + (v110 - v100)) + (v111 - v101)) * 0.25f;
+        float gz = ((((v001 - v000) + (v011 - v010)) + (v101 - v100)) + (v111 - v110)) * 0.25f;
+        float m2 = length2f(gx, gy, gz);
+        if(m2 > FLT_MIN) {
+            float s = sqrtf(m2);
+            gx = gx / s; gy = gy / s; gz = gz / s;
+            x = x - phiVal * gx;
+            y = y - phiVal * gy;
+            z = z - phiVal * gz;
+        }
+    }
+}
+
+__device__ __forceinline__ uint32_t cell_linear(const GridDesc& g, float gx, float gy, float gz, bool& outside) {
+    // Grid::getCellIdx<Int> (Grid.h:156-162): truncation of (p - bMin)/cellSize
+    int c[3] = {(int)gx, (int)gy, (int)gz};
+    outside = false;
+#pragma unroll
+    for(int d = 0; d < 3; ++d) {
+        if(c[d] < 0) { c[d] = 0; outside = true; }
+        if(c[d] > g.G[d] - 1) { c[d] = g.G[d] - 1; outside = true; }
+    }
+    return (uint32_t)(((size_t)c[2] * g.G[1] + c[1]) * g.G[0] + c[0]);
+}
+
+// ----------------------------------------------------------------------------------
+// moveParticles + cell histogram
+// ----------------------------------------------------------------------------------
+// PIC_Solver::moveParticles (PIC_Solver.cpp:353-373) with trace_rk2 (:1137-1144), then the
+// particle's cell id and its arrival slot in the cell histogram (the first half of the
+// counting sort).
+__global__ void __launch_bounds__(256) k_advect(int n, float* __restrict__ px, float* __restrict__ py,
+                                                float* __restrict__ pz, const float* __restrict__ u,
+                                                const float* __restrict__ v, const float* __restrict__ w, GridDesc g,
+                                                float sub, int steps, uint32_t* __restrict__ cellOf,
+                                                uint32_t* __restrict__ slot, uint32_t* __restrict__ count,
+                                                DevState* st) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if(p >= n) return;
+    float x = px[p], y = py[p], z = pz[p];
+    for(int s = 0; s < steps; ++s) {
+        float gv[3];
+        float gx = (x - g.bmin[0]) / g.dx, gy = (y - g.bmin[1]) / g.dx, gz = (z - g.bmin[2]) / g.dx;
+        vel_from_grid(g, u, v, w, gx, gy, gz, gv);
+        const float h = 0.5f * sub;
+        float mx = x + h * gv[0], my = y + h * gv[1], mz = z + h * gv[2];
+        gx = (mx - g.bmin[0]) / g.dx; gy = (my - g.bmin[1]) / g.dx; gz = (mz - g.bmin[2]) / g.dx;
+        vel_from_grid(g, u, v, w, gx, gy, gz, gv);
+        x = x + sub * gv[0];
+        y = y + sub * gv[1];
+        z = z + sub * gv[2];
+        constrain_to_box(g, x, y, z);
+    }
+    px[p] = x; py[p] = y; pz[p] = z;
+    bool outside;
+    uint32_t c = cell_linear(g, (x - g.bmin[0]) / g.dx, (y - g.bmin[1]) / g.dx, (z - g.bmin[2]) / g.dx, outside);
+    if(outside) atomicOr(&st->flags, BNN_FLAG_OUT_OF_GRID);
+    cellOf[p] = c;
+    slot[p] = atomicAdd(count + c, 1u);
+}
+
+// Cell id + histogram without moving (first sort of freshly loaded particles)
+__global__ void k_cell_histogram(int n, const float* __restrict__ px, const float* __restrict__ py,
+                                 const float* __restrict__ pz, GridDesc g, uint32_t* __restrict__ cellOf,
+                                 uint32_t* __restrict__ slot, uint32_t* __restrict__ count, DevState* st) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if(p >= n) return;
+    bool outside;
+    uint32_t c = cell_linear(g, (px[p] - g.bmin[0]) / g.dx, (py[p] - g.bmin[1]) / g.dx, (pz[p] - g.bmin[2]) / g.dx,
+                             outside);
+    if(outside) atomicOr(&st->flags, BNN_FLAG_OUT_OF_GRID);
+    cellOf[p] = c;
+    slot[p] = atomicAdd(count + c, 1u);
+}
+
+// Counting-sort scatter: position of particle p = cellStart[cell] + arrival slot
+__global__ void k_scatter_index(int n, const uint32_t* __restrict__ cellOf, const uint32_t* __restrict__ slot,
+                                const uint32_t* __restrict__ cellStart, uint32_t* __restrict__ order) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if(p >= n) return;
+    order[cellStart[cellOf[p]] + slot[p]] = (uint32_t)p;
+}
+
+// Arrival slots come from atomics, so each cell's bucket is put back into ascending
+// particle-id order here: particles end up sorted by (cell, id), the order
+// Grid::collectIndexToCells + getParticleIdxSortedByCell produce on one thread for
+// particles stored in id order (Grid.cpp:92-114,299-309), whatever order they are stored
+// in now.  The histogram is cleared for the next step on the way.
+__global__ void k_sort_buckets(int ncells, const uint32_t* __restrict__ cellStart, uint32_t* __restrict__ order,
+                               const uint32_t* __restrict__ ids, uint32_t* __restrict__ count) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if(c >= ncells) return;
+    const uint32_t b = cellStart[c], e = cellStart[c + 1];
+    count[c] = 0u;
+    for(uint32_t i = b + 1; i < e; ++i) {
+        const uint32_t src = order[i];
+        const uint32_t key = ids[src];
+        uint32_t j = i;
+        while(j > b && ids[order[j - 1]] > key) { order[j] = order[j - 1]; --j; }
+        order[j] = src;
+    }
+}
+
+// Apply the permutation to the particle arrays; also emits grid coordinates
+// (Grid::getGridCoordinate, Grid.h:197) used by P2G and the fluid SDF.
+__global__ void k_gather_particles(int n, const uint32_t* __restrict__ order, const float* __restrict__ src6,
+                                   float* __restrict__ dst6, const uint32_t* __restrict__ idSrc,
+                                   uint32_t* __restrict__ idDst, const float* __restrict__ cSrc,
+                                   float* __restrict__ cDst, float* __restrict__ g3, GridDesc g, size_t stride) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n) return;
+    const uint32_t s = order[i];
+#pragma unroll
+    for(int q = 0; q < 6; ++q) dst6[q * stride + i] = src6[q * stride + s];
+    idDst[i] = idSrc[s];
+    if(cSrc) {
+#pragma unroll
+        for(int q = 0; q < 9; ++q) cDst[q * stride + i] = cSrc[q * stride + s];
+    }
+    g3[i] = (dst6[i] - g.bmin[0]) / g.dx;
+    g3[stride + i] = (dst6[stride + i] - g.bmin[1]) / g.dx;
+    g3[2 * stride + i] = (dst6[2 * stride + i] - g.bmin[2]) / g.dx;
+}
+
+// ----------------------------------------------------------------------------------
+// P2G
+// ----------------------------------------------------------------------------------
+// FLIP_Solver::mapParticles2Grid (FLIP_Solver.cpp:57-95) as a gather: the thread of face
+// f walks the particles of the cells whose particles can reach f (2 cells along the
+// component's axis, 3 along the others), in sorted-array order, keeps those whose
+// trilinear stencil (ArrayHelpers::getCoordinatesAndWeights, ArrayHelpers.cpp:50-76)
+// contains f, and sums w*v and w in that order -- the sums a serial run of the reference
+// P2G over the sorted particle array produces.  APIC/AFLIP add the affine momentum term
+// w * dot(C_d, x_f - x_p) (APIC_Solver.cpp:53-91).
+template<int D, bool AFFINE>
+__global__ void __launch_bounds__(256) k_p2g(GridDesc g, const uint32_t* __restrict__ cellStart,
+                                             const float* __restrict__ gxs, const float* __restrict__ gys,
+                                             const float* __restrict__ gzs, const float* __restrict__ pxs,
+                                             const float* __restrict__ pys, const float* __restrict__ pzs,
+                                             const float* __restrict__ vd, const float* __restrict__ Cd,
+                                             size_t cstride, float* __restrict__ out,
+                                             uint8_t* __restrict__ valid) {
+    const int sx = g.G[0] + (D == 0), sy = g.G[1] + (D == 1), sz = g.G[2] + (D == 2);
+    const size_t nf = (size_t)sx * sy * sz;
+    const size_t f = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if(f >= nf) return;
+    const int i = (int)(f % sx);
+    const int j = (int)((f / sx) % sy);
+    const int k = (int)(f / ((size_t)sx * sy));
+    const int xlo = max(i - 1, 0), xhi = min(D == 0 ? i : i + 1, g.G[0] - 1);
+    const int ylo = max(j - 1, 0), yhi = min(D == 1 ? j : j + 1, g.G[1] - 1);
+    const int zlo = max(k - 1, 0), zhi = min(D == 2 ? k : k + 1, g.G[2] - 1);
+    // world position of the face (Grid::getWorldCoordinate(VecN(idx) + extra), Grid.h:181-184)
+    float fxw = 0.f, fyw = 0.f, fzw = 0.f;
+    if(AFFINE) {
+        fxw = ((float)i + (D == 0 ? 0.f : 0.5f)) * g.dx + g.bmin[0];
+        fyw = ((float)j + (D == 1 ? 0.f : 0.5f)) * g.dx + g.bmin[1];
+        fzw = ((float)k + (D == 2 ? 0.f : 0.5f)) * g.dx + g.bmin[2];
+    }
+    float S = 0.f, W = 0.f;
+    if(xlo <= xhi) {
+        for(int kk = zlo; kk <= zhi; ++kk) {
+            for(int jj = ylo; jj <= yhi; ++jj) {
+                const size_t row = ((size_t)kk * g.G[1] + jj) * g.G[0];
+                const uint32_t b = __ldg(cellStart + row + xlo), e = __ldg(cellStart + row + xhi + 1);
+                for(uint32_t q = b; q < e; ++q) {
+                    const float ax = __ldg(gxs + q) - (D == 0 ? 0.f : 0.5f);
+                    const float ay = __ldg(gys + q) - (D == 1 ? 0.f : 0.5f);
+                    const float az = __ldg(gzs + q) - (D == 2 ? 0.f : 0.5f);
+                    int si, sj, sk;
+                    float fi, fj, fk;
+                    bary(ax, si, fi, sx);
+                    if(si != i && si != i - 1) continue;
+                    bary(ay, sj, fj, sy);
+                    if(sj != j && sj != j - 1) continue;
+                    bary(az, sk, fk, sz);
+                    if(sk != k && sk != k - 1) continue;
+                    const float wx = (si == i) ? (1.0f - fi) : fi;
+                    const float wy = (sj == j) ? (1.0f - fj) : fj;
+                    const float wz = (sk == k) ? (1.0f - fk) : fk;
+                    const float wgt = wx * wy * wz;
+                    float m;
+                    if(AFFINE) {
+                        const float c0 = __ldg(Cd + q), c1 = __ldg(Cd + cstride + q), c2 = __ldg(Cd + 2 * cstride + q);
+                        const float dxp = fxw - __ldg(pxs + q), dyp = fyw - __ldg(pys + q), dzp = fzw - __ldg(pzs + q);
+                        const float dotv = (c0 * dxp + c1 * dyp) + c2 * dzp;
+                        m = wgt * (__ldg(vd + q) + dotv);
+                    } else {
+                        m = wgt * __ldg(vd + q);
+                    }
+                    S = S + m;
+                    W = W + wgt;
+                }
+            }
+        }
+    }
+    const bool ok = W > FLT_MIN;
+    out[f] = ok ? S / W : S;
+    valid[f] = ok ? 1 : 0;
+}
+
+// ----------------------------------------------------------------------------------
+// Velocity extrapolation (one layer)
+// ----------------------------------------------------------------------------------
+// One layer of PIC_Solver::extrapolateVelocity (PIC_Solver.cpp:998-1089): an interior
+// face that was not valid takes the mean of its valid 6-neighbours (+x,-x,+y,-y,+z,-z
+// summation order) and becomes valid; everything reads the previous layer.
+// mode 0: plain layer.  mode 1 (last layer after P2G): also writes the FLIP backup
+// oldVels (FLIP_Data.h:48-52) and applies Earth gravity v -= 9.81*dt (PIC_Solver.cpp:
+// 505-511) to the v component.  mode 2 (last layer after projection): folds max|u| into
+// the CFL reduction (PIC_Solver.cpp:342-349).
+__global__ void __launch_bounds__(256) k_extrapolate(int sx, int sy, int sz, const float* __restrict__ gin,
+                                                     const uint8_t* __restrict__ vin, float* __restrict__ gout,
+                                                     uint8_t* __restrict__ vout, int mode, float* __restrict__ oldOut,
+                                                     float gravityDt, DevState* st) {
+    const size_t nf = (size_t)sx * sy * sz;
+    const size_t f = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    float val = 0.f;
+    if(f < nf) {
+        const int i = (int)(f % sx);
+        const int j = (int)((f / sx) % sy);
+        const int k = (int)(f / ((size_t)sx * sy));
+        val = gin[f];
+        uint8_t vv = vin[f];
+        if(!vv && i > 0 && i < sx - 1 && j > 0 && j < sy - 1 && k > 0 && k < sz - 1) {
+            const size_t sxy = (size_t)sx * sy;
+            float sum = 0.f;
+            unsigned count = 0;
+            if(vin[f + 1]) { sum += gin[f + 1]; ++count; }
+            if(vin[f - 1]) { sum += gin[f - 1]; ++count; }
+            if(vin[f + sx]) { sum += gin[f + sx]; ++count; }
+            if(vin[f - sx]) { sum += gin[f - sx]; ++count; }
+            if(vin[f + sxy]) { sum += gin[f + sxy]; ++count; }
+            if(vin[f - sxy]) { sum += gin[f - sxy]; ++count; }
+            if(count > 0) { val = sum / (float)count; vv = 1; }
+        }
+        vout[f] = vv;
+        if(mode == 1) {
+            oldOut[f] = val;
+            gout[f] = val - gravityDt;
+        } else {
+            gout[f] = val;
+        }
+    }
+    if(mode == 2) {
+        __shared__ float sm[256];
+        float m = block_max_256(f < nf ? fabsf(val) : 0.f, sm);
+        if(threadIdx.x == 0 && m > 0.f) atomicMax(&st->maxvel_bits, __float_as_uint(m));
+    }
+}
+
+// ----------------------------------------------------------------------------------
+// Fluid SDF
+// ----------------------------------------------------------------------------------
+// PIC_Solver::computeFluidSDF (PIC_Solver.cpp:601-652) as a gather per cell over the
+// particles of the 3x3x3 neighbouring cells: phi = min(3 dx, min_p |x_c - x_p| - r_sdf),
+// with the particle's own clamped 3x3x3 range test.  min is exact, so this equals the
+// reference's scatter with locks.
+__global__ void __launch_bounds__(256) k_fluid_sdf(GridDesc g, const uint32_t* __restrict__ cellStart,
+                                                   const float* __restrict__ gxs, const float* __restrict__ gys,
+                                                   const float* __restrict__ gzs, const float* __restrict__ pxs,
+                                                   const float* __restrict__ pys, const float* __restrict__ pzs,
+                                                   float* __restrict__ phi) {
+    const size_t nc = (size_t)g.G[0] * g.G[1] * g.G[2];
+    const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if(c >= nc) return;
+    const int i = (int)(c % g.G[0]);
+    const int j = (int)((c / g.G[0]) % g.G[1]);
+    const int k = (int)(c / ((size_t)g.G[0] * g.G[1]));
+    // Grid::getWorldCoordinate(i + 0.5, j + 0.5, k + 0.5) (Grid.h:186-194)
+    const float sxw = ((float)i + 0.5f) * g.dx + g.bmin[0];
+    const float syw = ((float)j + 0.5f) * g.dx + g.bmin[1];
+    const float szw = ((float)k + 0.5f) * g.dx + g.bmin[2];
+    float ph = g.dx * 3.0f;
+    const int xlo = max(i - 1, 0), xhi = min(i + 1, g.G[0] - 1);
+    for(int kk = max(k - 1, 0); kk <= min(k + 1, g.G[2] - 1); ++kk) {
+        for(int jj = max(j - 1, 0); jj <= min(j + 1, g.G[1] - 1); ++jj) {
+            const size_t row = ((size_t)kk * g.G[1] + jj) * g.G[0];
+            const uint32_t b = __ldg(cellStart + row + xlo), e = __ldg(cellStart + row + xhi + 1);
+            for(uint32_t q = b; q < e; ++q) {
+                // the particle's own cell and its clamped 3x3x3 range (PIC_Solver.cpp:633-635)
+                const int ci = (int)__ldg(gxs + q), cj = (int)__ldg(gys + q), ck = (int)__ldg(gzs + q);
+                if(i < max(ci - 1, 0) || i > min(ci + 1, g.G[0] - 1)) continue;
+                if(j < max(cj - 1, 0) || j > min(cj + 1, g.G[1] - 1)) continue;
+                if(k < max(ck - 1, 0) || k > min(ck + 1, g.G[2] - 1)) continue;
+                const float d = sqrtf(length2f(sxw - __ldg(pxs + q), syw - __ldg(pys + q), szw - __ldg(pzs + q)));
+                const float val = d - g.sdfRadius;
+                if(val < ph) ph = val;
+            }
+        }
+    }
+    phi[c] = ph;
+}
+
+// ----------------------------------------------------------------------------------
+// Pressure system
+// ----------------------------------------------------------------------------------
+// Active-cell flags for PIC_Solver::computeSystem's numbering loop (PIC_Solver.cpp:706-712)
+__global__ void k_active_flags(GridDesc g, const float* __restrict__ phi, uint32_t* __restrict__ flag,
+                               DevState* st) {
+    const size_t nc = (size_t)g.G[0] * g.G[1] * g.G[2];
+    const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if(c >= nc) return;
+    const float p = phi[c];
+    flag[c] = p < 0.f ? 1u : 0u;
+    if(p == 0.f) {
+        const int i = (int)(c % g.G[0]);
+        const int j = (int)((c / g.G[0]) % g.G[1]);
+        const int k = (int)(c / ((size_t)g.G[0] * g.G[1]));
+        if(i > 0 && i < g.G[0] - 1 && j > 0 && j < g.G[1] - 1 && k > 0 && k < g.G[2] - 1) atomicAdd(&st->zero_phi, 1u);
+    }
+}
+
+__global__ void k_active_rows(size_t nc, const uint32_t* __restrict__ flag, const uint32_t* __restrict__ idx,
+                              uint32_t* __restrict__ rowCell) {
+    const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if(c >= nc) return;
+    if(flag[c]) rowCell[idx[c]] = (uint32_t)c;
+}
+
+// One row of PIC_Solver::computeSystem (PIC_Solver.cpp:794-891) for a static scene
+// (face weights 1): rhs = -div u, diagonal accumulated in the order right, left, top,
+// bottom, far, near with the ghost-fluid 1/theta terms, neighbour rows for fluid
+// neighbours.  Neighbours are stored in ascending column order (-z,-y,-x,+x,+y,+z), the
+// order FixedSparseMatrix::multiply sums them in (SparseMatrix.cpp:222-235).
+__global__ void k_build_rows(GridDesc g, int nrows, const uint32_t* __restrict__ rowCell,
+                             const float* __restrict__ phi, const uint32_t* __restrict__ aidx,
+                             const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w,
+                             float dt, float* __restrict__ rhs, float* __restrict__ diag, float* __restrict__ invdiag,
+                             int32_t* __restrict__ nbr, DevState* st) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if(r >= nrows) return;
+    const uint32_t c = rowCell[r];
+    const int G0 = g.G[0], G1 = g.G[1], G2 = g.G[2];
+    const int i = (int)(c % G0);
+    const int j = (int)((c / G0) % G1);
+    const int k = (int)(c / ((size_t)G0 * G1));
+    int32_t nb[6] = {-1, -1, -1, -1, -1, -1};
+    if(i < 1 || i > G0 - 2 || j < 1 || j > G1 - 2 || k < 1 || k > G2 - 2) {
+        // fluid in the outer cell ring: the reference numbers it but never writes its row
+        atomicOr(&st->flags, BNN_FLAG_RING_FLUID);
+        rhs[r] = 0.f; diag[r] = 0.f; invdiag[r] = 0.f;
+#pragma unroll
+        for(int q = 0; q < 6; ++q) nbr[(size_t)q * nrows + r] = -1;
+        return;
+    }
+    const size_t sxu = G0 + 1, sxv = G0, sxw = G0;
+    const size_t sxyu = sxu * G1, sxyv = (size_t)G0 * (G1 + 1), sxyw = (size_t)G0 * G1;
+    const float pc = phi[c];
+    const size_t GG = (size_t)G0 * G1;
+    const float pr = phi[c + 1], pl = phi[c - 1], pt = phi[c + G0], pb = phi[c - G0], pf = phi[c + GG], pn = phi[c - GG];
+    float rv = 0.f;
+    const float term = 1.0f * dt;
+    rv -= 1.0f * u[(size_t)k * sxyu + (size_t)j * sxu + i + 1];
+    rv += 1.0f * u[(size_t)k * sxyu + (size_t)j * sxu + i];
+    rv -= 1.0f * v[(size_t)k * sxyv + (size_t)(j + 1) * sxv + i];
+    rv += 1.0f * v[(size_t)k * sxyv + (size_t)j * sxv + i];
+    rv -= 1.0f * w[(size_t)(k + 1) * sxyw + (size_t)j * sxw + i];
+    rv += 1.0f * w[(size_t)k * sxyw + (size_t)j * sxw + i];
+    rhs[r] = rv;
+    float center = 0.f;
+    // right, left, top, bottom, far, near
+    const float phn[6] = {pr, pl, pt, pb, pf, pn};
+    const size_t nc_[6] = {c + 1, c - 1, c + G0, c - G0, c + GG, c - GG};
+    const int slotOf[6] = {3, 2, 4, 1, 5, 0};
+#pragma unroll
+    for(int q = 0; q < 6; ++q) {
+        if(phn[q] < 0.f) {
+            center += term;
+            nb[slotOf[q]] = (int32_t)aidx[nc_[q]];
+        } else {
+            const float th = smax(0.01f, fraction_inside(pc, phn[q]));
+            center += term / th;
+        }
+    }
+    diag[r] = center;
+    invdiag[r] = 1.0f / center;
+#pragma unroll
+    for(int q = 0; q < 6; ++q) nbr[(size_t)q * nrows + r] = nb[q];
+}
+
+// ----------------------------------------------------------------------------------
+// Pressure update
+// ----------------------------------------------------------------------------------
+// PIC_Solver::updateProjectedVelocity (PIC_Solver.cpp:911-981), weights 1: face (i,j,k)
+// of component D between cells c- and c gets u -= dt*(p_c - p_c-)/max(0.01, theta) when
+// either cell is fluid and is marked valid; every other face is set to 0.
+template<int D>
+__global__ void __launch_bounds__(256) k_update_velocity(GridDesc g, const float* __restrict__ phi,
+                                                         const uint32_t* __restrict__ aidx,
+                                                         const float* __restrict__ pressure, float dt,
+                                                         float* __restrict__ vel, uint8_t* __restrict__ valid) {
+    const int sx = g.G[0] + (D == 0), sy = g.G[1] + (D == 1), sz = g.G[2] + (D == 2);
+    const size_t nf = (size_t)sx * sy * sz;
+    const size_t f = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if(f >= nf) return;
+    const int i = (int)(f % sx);
+    const int j = (int)((f / sx) % sy);
+    const int k = (int)(f / ((size_t)sx * sy));
+    const int a = D == 0 ? i : (D == 1 ? j : k);
+    const int amax = g.G[D];
+    float out = 0.f;
+    uint8_t vv = 0;
+    if(a > 0 && a < amax) {
+        const size_t c = ((size_t)k * g.G[1] + j) * g.G[0] + i;
+        const size_t step = D == 0 ? 1 : (D == 1 ? (size_t)g.G[0] : (size_t)g.G[0] * g.G[1]);
+        const size_t cm = c - step;
+        const float pc = phi[c], pm = phi[cm];
+        if(pc < 0.f || pm < 0.f) {
+            const float prc = pc < 0.f ? pressure[aidx[c]] : 0.f;
+            const float prm = pm < 0.f ? pressure[aidx[cm]] : 0.f;
+            const float th = smax(0.01f, fraction_inside(pm, pc));
+            out = vel[f] - dt * (prc - prm) / th;
+            vv = 1;
+        }
+    }
+    vel[f] = out;
+    valid[f] = vv;
+}
+
+// ----------------------------------------------------------------------------------
+// G2P
+// ----------------------------------------------------------------------------------
+// FLIP_Solver::mapGrid2Particles (FLIP_Solver.cpp:99-111): v = lerp(v_grid, v_p + dv_grid,
+// PIC_FLIP_ratio); APIC takes v_grid and C = grad v (APIC_Solver.cpp:95-117); AFLIP blends
+// both (AFLIP_Solver.cpp:94-132).  kind: 0 FLIP, 1 APIC, 2 AFLIP.
+template<bool DIFF>
+__device__ __forceinline__ void grad_value_t(const float* __restrict__ a, const float* __restrict__ o, int sx, int sy,
+                                             int sz, float px, float py, float pz, float cellSize, float out[3]) {
+    // ArrayHelpers::interpolateGradientValue 3D (ArrayHelpers.cpp:275-302)
+    int i, j, k;
+    float fi, fj, fk;
+    bary(px, i, fi, sx);
+    bary(py, j, fj, sy);
+    bary(pz, k, fk, sz);
+    const size_t sxy = (size_t)sx * sy;
+    const size_t b = (size_t)k * sxy + (size_t)j * sx + i;
+    const size_t offs[8] = {0, sxy, (size_t)sx, sxy + sx, 1, sxy + 1, (size_t)sx + 1, sxy + sx + 1};
+    float vv[8]; // v000, v001, v010, v011, v100, v101, v110, v111
+#pragma unroll
+    for(int q = 0; q < 8; ++q) vv[q] = DIFF ? a[b + offs[q]] - o[b + offs[q]] : a[b + offs[q]];
+    const float one = 1.0f;
+    const float wx[8] = {-(one - fj) * (one - fk), -(one - fj) * fk, -fj * (one - fk), -fj * fk,
+                         (one - fj) * (one - fk), (one - fj) * fk, fj * (one - fk), fj * fk};
+    const float wy[8] = {-(one - fi) * (one - fk), -(one - fi) * fk, (one - fi) * (one - fk), (one - fi) * fk,
+                         -fi * (one - fk), -fi * fk, fi * (one - fk), fi * fk};
+    const float wz[8] = {-(one - fi) * (one - fj), (one - fi) * (one - fj), -(one - fi) * fj, (one - fi) * fj,
+                         -fi * (one - fj), fi * (one - fj), -fi * fj, fi * fj};
+    float s0 = vv[0] * wx[0], s1 = vv[0] * wy[0], s2 = vv[0] * wz[0];
+#pragma unroll
+    for(int q = 1; q < 8; ++q) { s0 = s0 + vv[q] * wx[q]; s1 = s1 + vv[q] * wy[q]; s2 = s2 + vv[q] * wz[q]; }
+    out[0] = s0 / cellSize; out[1] = s1 / cellSize; out[2] = s2 / cellSize;
+}
+__device__ __forceinline__ void grad_value(const float* a, int sx, int sy, int sz, float px, float py, float pz,
+                                           float cellSize, float out[3]) {
+    grad_value_t<false>(a, nullptr, sx, sy, sz, px, py, pz, cellSize, out);
+}
+__device__ __forceinline__ void grad_value_diff(const float* a, const float* o, int sx, int sy, int sz, float px,
+                                                float py, float pz, float cellSize, float out[3]) {
+    grad_value_t<true>(a, o, sx, sy, sz, px, py, pz, cellSize, out);
+}
+
+__global__ void __launch_bounds__(256) k_g2p(int n, GridDesc g, const float* __restrict__ pos6, float* __restrict__ vel3,
+                                             size_t stride, const float* __restrict__ u, const float* __restrict__ v,
+                                             const float* __restrict__ w, const float* __restrict__ ou,
+                                             const float* __restrict__ ov, const float* __restrict__ ow, float ratio,
+                                             int kind, float* __restrict__ C9) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if(p >= n) return;
+    const float gx = (pos6[p] - g.bmin[0]) / g.dx;
+    const float gy = (pos6[stride + p] - g.bmin[1]) / g.dx;
+    const float gz = (pos6[2 * stride + p] - g.bmin[2]) / g.dx;
+    const int G0 = g.G[0], G1 = g.G[1], G2 = g.G[2];
+    float gv[3];
+    vel_from_grid(g, u, v, w, gx, gy, gz, gv);
+    if(kind == 1) {
+#pragma unroll
+        for(int d = 0; d < 3; ++d) vel3[d * stride + p] = gv[d];
+    } else {
+        float dg[3];
+        dg[0] = interp_face_diff(u, ou, G0 + 1, G1, G2, gx, gy - 0.5f, gz - 0.5f);
+        dg[1] = interp_face_diff(v, ov, G0, G1 + 1, G2, gx - 0.5f, gy, gz - 0.5f);
+        dg[2] = interp_face_diff(w, ow, G0, G1, G2 + 1, gx - 0.5f, gy - 0.5f, gz);
+#pragma unroll
+        for(int d = 0; d < 3; ++d) {
+            const float pv = vel3[d * stride + p];
+            vel3[d * stride + p] = (1.0f - ratio) * gv[d] + ratio * (pv + dg[d]);
+        }
+    }
+    if(kind == 1 || kind == 2) {
+        const float* arrs[3] = {u, v, w};
+        const float* olds[3] = {ou, ov, ow};
+        const int dims[3][3] = {{G0 + 1, G1, G2}, {G0, G1 + 1, G2}, {G0, G1, G2 + 1}};
+        for(int d = 0; d < 3; ++d) {
+            const float ptx = d == 0 ? gx : gx - 0.5f, pty = d == 1 ? gy : gy - 0.5f, ptz = d == 2 ? gz : gz - 0.5f;
+            float gc[3];
+            grad_value(arrs[d], dims[d][0], dims[d][1], dims[d][2], ptx, pty, ptz, g.dx, gc);
+            if(kind == 1) {
+#pragma unroll
+                for(int c = 0; c < 3; ++c) C9[(size_t)(d * 3 + c) * stride + p] = gc[c];
+            } else {
+                // dGridC = interpolateGradientValue of dVels = velocities - oldVels
+                // (AFLIP_Solver.cpp:121-130), differences formed tap by tap
+                float dc[3];
+                grad_value_diff(arrs[d], olds[d], dims[d][0], dims[d][1], dims[d][2], ptx, pty, ptz, g.dx, dc);
+#pragma unroll
+                for(int c = 0; c < 3; ++c) {
+                    const size_t o_ = (size_t)(d * 3 + c) * stride + p;
+                    C9[o_] = (1.0f - ratio) * gc[c] + ratio * (C9[o_] + dc[c]);
+                }
+            }
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------------
+// Particle I/O
+// ----------------------------------------------------------------------------------
+__global__ void k_aos_to_soa(int n, const float* __restrict__ pos, const float* __restrict__ vel,
+                             float* __restrict__ soa6, uint32_t* __restrict__ ids, size_t stride) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if(p >= n) return;
+#pragma unroll
+    for(int d = 0; d < 3; ++d) {
+        soa6[d * stride + p] = pos[3 * (size_t)p + d];
+        soa6[(3 + d) * stride + p] = vel[3 * (size_t)p + d];
+    }
+    ids[p] = (uint32_t)p;
+}
+
+// back to AoS in the caller's original order
+__global__ void k_soa_to_aos(int n, const float* __restrict__ soa6, const uint32_t* __restrict__ ids,
+                             float* __restrict__ pos, float* __restrict__ vel, size_t stride) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if(p >= n) return;
+    const uint32_t id = ids[p];
+#pragma unroll
+    for(int d = 0; d < 3; ++d) {
+        pos[3 * (size_t)id + d] = soa6[d * stride + p];
+        vel[3 * (size_t)id + d] = soa6[(3 + d) * stride + p];
+    }
+}
+
+// pressure scattered onto cells for BNN_FIELD_PRESSURE / BNN_FIELD_ACTIVE
+__global__ void k_cells_from_rows(size_t nc, const float* __restrict__ phi, const uint32_t* __restrict__ aidx,
+                                  const float* __restrict__ pr, float* __restrict__ out, int activeField) {
+    const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if(c >= nc) return;
+    if(activeField) out[c] = phi[c] < 0.f ? (float)(aidx[c] + 1) : 0.f;
+    else out[c] = phi[c] < 0.f ? pr[aidx[c]] : 0.f;
+}
+
+__global__ void k_add_scalar(float* __restrict__ a, size_t n, float v) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if(i < n) a[i] = a[i] + v;
+}
+
+__global__ void k_step_reset(DevState* st) {
+    st->flags = 0u;
+    st->zero_phi = 0u;
+    st->maxvel_bits = 0u;
+}
+
+// ----------------------------------------------------------------------------------
+// Launchers
+// ----------------------------------------------------------------------------------
+static inline unsigned nblk(size_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
+
+void launch_advect(int n, float* p6, size_t stride, const float* const* U, const GridDesc& g, float sub, int steps,
+                   uint32_t* cellOf, uint32_t* slot, uint32_t* count, DevState* st, cudaStream_t s) {
+    if(n == 0) return;
+    k_advect<<<nblk(n), 256, 0, s>>>(n, p6, p6 + stride, p6 + 2 * stride, U[0], U[1], U[2], g, sub, steps, cellOf, slot,
+                                     count, st);
+}
+void launch_cell_histogram(int n, const float* p6, size_t stride, const GridDesc& g, uint32_t* cellOf, uint32_t* slot,
+                           uint32_t* count, DevState* st, cudaStream_t s) {
+    if(n == 0) return;
+    k_cell_histogram<<<nblk(n), 256, 0, s>>>(n, p6, p6 + stride, p6 + 2 * stride, g, cellOf, slot, count, st);
+}
+void launch_sort_finish(int n, size_t ncells, const uint32_t* cellOf, const uint32_t* slot, const uint32_t* cellStart,
+                        uint32_t* order, uint32_t* count, const float* src6, float* dst6, const uint32_t* idSrc,
+                        uint32_t* idDst, const float* cSrc, float* cDst, float* g3, const GridDesc& g, size_t stride,
+                        cudaStream_t s) {
+    if(n > 0) k_scatter_index<<<nblk(n), 256, 0, s>>>(n, cellOf, slot, cellStart, order);
+    k_sort_buckets<<<nblk(ncells), 256, 0, s>>>((int)ncells, cellStart, order, idSrc, count);
+    if(n > 0)
+        k_gather_particles<<<nblk(n), 256, 0, s>>>(n, order, src6, dst6, idSrc, idDst, cSrc, cDst, g3, g, stride);
+}
+void launch_p2g(const GridDesc& g, const uint32_t* cellStart, const float* g3, const float* p6, const float* C9,
+                size_t stride, float* const* out, uint8_t* const* valid, bool affine, cudaStream_t s) {
+    const float *gx = g3, *gy = g3 + stride, *gz = g3 + 2 * stride;
+    const float *px = p6, *py = p6 + stride, *pz = p6 + 2 * stride;
+    for(int d = 0; d < 3; ++d) {
+        size_t nf = (size_t)face_sx(g, d) * face_sy(g, d) * face_sz(g, d);
+        const float* vd = p6 + (3 + d) * stride;
+        const float* Cd = C9 ? C9 + (size_t)(3 * d) * stride : nullptr;
+        if(affine) {
+            if(d == 0) k_p2g<0, true><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[0], valid[0]);
+            if(d == 1) k_p2g<1, true><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[1], valid[1]);
+            if(d == 2) k_p2g<2, true><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[2], valid[2]);
+        } else {
+            if(d == 0) k_p2g<0, false><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[0], valid[0]);
+            if(d == 1) k_p2g<1, false><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[1], valid[1]);
+            if(d == 2) k_p2g<2, false><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[2], valid[2]);
+        }
+    }
+}
+// 4 layers per component; A holds the input and receives the result (4 is even)
+void launch_extrapolate(const GridDesc& g, float* const* A, uint8_t* const* VA, float* const* B, uint8_t* const* VB,
+                        int lastMode, float* const* oldOut, float gravityDt, DevState* st, cudaStream_t s) {
+    for(int d = 0; d < 3; ++d) {
+        int sx = face_sx(g, d), sy = face_sy(g, d), sz = face_sz(g, d);
+        size_t nf = (size_t)sx * sy * sz;
+        for(int layer = 0; layer < 4; ++layer) {
+            const float* gin = (layer % 2 == 0) ? A[d] : B[d];
+            const uint8_t* vin = (layer % 2 == 0) ? VA[d] : VB[d];
+            float* gout = (layer % 2 == 0) ? B[d] : A[d];
+            uint8_t* vout = (layer % 2 == 0) ? VB[d] : VA[d];
+            int mode = layer == 3 ? lastMode : 0;
+            float gdt = (mode == 1 && d == 1) ? gravityDt : 0.f;
+            k_extrapolate<<<nblk(nf), 256, 0, s>>>(sx, sy, sz, gin, vin, gout, vout, mode, oldOut ? oldOut[d] : nullptr,
+                                                   gdt, st);
+        }
+    }
+}
+void launch_fluid_sdf(const GridDesc& g, const uint32_t* cellStart, const float* g3, const float* p6, size_t stride,
+                      float* phi, cudaStream_t s) {
+    size_t nc = (size_t)g.G[0] * g.G[1] * g.G[2];
+    k_fluid_sdf<<<nblk(nc), 256, 0, s>>>(g, cellStart, g3, g3 + stride, g3 + 2 * stride, p6, p6 + stride,
+                                         p6 + 2 * stride, phi);
+}
+void launch_active_flags(const GridDesc& g, const float* phi, uint32_t* flag, DevState* st, cudaStream_t s) {
+    size_t nc = (size_t)g.G[0] * g.G[1] * g.G[2];
+    k_active_flags<<<nblk(nc), 256, 0, s>>>(g, phi, flag, st);
+}
+void launch_active_rows(size_t nc, const uint32_t* flag, const uint32_t* idx, uint32_t* rowCell, cudaStream_t s) {
+    k_active_rows<<<nblk(nc), 256, 0, s>>>(nc, flag, idx, rowCell);
+}
+void launch_build_rows(const GridDesc& g, int nrows, const uint32_t* rowCell, const float* phi, const uint32_t* aidx,
+                       const float* const* U, float dt, float* rhs, float* diag, float* invdiag, int32_t* nbr,
+                       DevState* st, cudaStream_t s) {
+    if(nrows == 0) return;
+    k_build_rows<<<nblk(nrows), 256, 0, s>>>(g, nrows, rowCell, phi, aidx, U[0], U[1], U[2], dt, rhs, diag, invdiag,
+                                             nbr, st);
+}
+void launch_update_velocity(const GridDesc& g, const float* phi, const uint32_t* aidx, const float* pressure, float dt,
+                            float* const* U, uint8_t* const* V, cudaStream_t s) {
+    size_t n0 = (size_t)face_sx(g, 0) * face_sy(g, 0) * face_sz(g, 0);
+    size_t n1 = (size_t)face_sx(g, 1) * face_sy(g, 1) * face_sz(g, 1);
+    size_t n2 = (size_t)face_sx(g, 2) * face_sy(g, 2) * face_sz(g, 2);
+    k_update_velocity<0><<<nblk(n0), 256, 0, s>>>(g, phi, aidx, pressure, dt, U[0], V[0]);
+    k_update_velocity<1><<<nblk(n1), 256, 0, s>>>(g, phi, aidx, pressure, dt, U[1], V[1]);
+    k_update_velocity<2><<<nblk(n2), 256, 0, s>>>(g, phi, aidx, pressure, dt, U[2], V[2]);
+}
+void launch_g2p(int n, const GridDesc& g, float* p6, size_t stride, const float* const* U, const float* const* O,
+                float ratio, int kind, float* C9, cudaStream_t s) {
+    if(n == 0) return;
+    k_g2p<<<nblk(n), 256, 0, s>>>(n, g, p6, p6 + 3 * stride, stride, U[0], U[1], U[2], O[0], O[1], O[2], ratio, kind,
+                                  C9);
+}
+void launch_aos_to_soa(int n, const float* pos, const float* vel, float* soa6, uint32_t* ids, size_t stride,
+                       cudaStream_t s) {
+    if(n == 0) return;
+    k_aos_to_soa<<<nblk(n), 256, 0, s>>>(n, pos, vel, soa6, ids, stride);
+}
+void launch_soa_to_aos(int n, const float* soa6, const uint32_t* ids, float* pos, float* vel, size_t stride,
+                       cudaStream_t s) {
+    if(n == 0) return;
+    k_soa_to_aos<<<nblk(n), 256, 0, s>>>(n, soa6, ids, pos, vel, stride);
+}
+void launch_add_scalar(float* a, size_t n, float v, cudaStream_t s) { k_add_scalar<<<nblk(n), 256, 0, s>>>(a, n, v); }
+void launch_step_reset(DevState* st, cudaStream_t s) { k_step_reset<<<1, 1, 0, s>>>(st); }
+void launch_cells_from_rows(size_t nc, const float* phi, const uint32_t* aidx, const float* pr, float* out, int active,
+                            cudaStream_t s) {
+    k_cells_from_rows<<<nblk(nc), 256, 0, s>>>(nc, phi, aidx, pr, out, active);
+}
+
+} // namespace bnn

@@ -1,0 +1,407 @@
+// Uniform-grid cell sort, Morton z-sort and neighbour search (BananaCore/Banana/Grid,
+// BananaCore/Banana/NeighborSearch) as standalone device entry points.
+//
+// Sorting is a stable LSD radix sort (8-bit digits, passes only over the key bits that
+// vary): per 2048-item tile a 256-bin histogram, a digit-major exclusive scan over all
+// tiles, then a scatter that ranks equal digits in input order with warp match masks.
+// Stability gives the canonical order of equal keys (input order), which is what the
+// reference's one-thread bucket fill produces.
+#include "bnn_internal.cuh"
+
+#include <vector>
+
+namespace bnn {
+cudaError_t exclusive_scan_u32_to_u64(const uint32_t* in, unsigned long long* out, size_t n, void* ws, cudaStream_t s);
+size_t scan_workspace_bytes_u64(size_t n);
+
+namespace {
+constexpr int kRT = 256;           // threads per radix tile
+constexpr int kRPer = 8;           // rounds per tile
+constexpr int kRTile = kRT * kRPer;
+constexpr int kWarps = kRT / 32;
+
+template<class K> __global__ void __launch_bounds__(kRT) k_radix_hist(const K* __restrict__ keys, size_t n, int shift,
+                                                                      uint32_t* __restrict__ hist, unsigned ntiles) {
+    __shared__ uint32_t h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const size_t base = (size_t)blockIdx.x * kRTile;
+    for(int r = 0; r < kRPer; ++r) {
+        size_t e = base + (size_t)r * kRT + threadIdx.x;
+        if(e < n) atomicAdd(&h[(unsigned)((keys[e] >> shift) & 0xFF)], 1u);
+    }
+    __syncthreads();
+    hist[(size_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
+}
+
+template<class K> __global__ void __launch_bounds__(kRT) k_radix_scatter(const K* __restrict__ kin,
+                                                                         const uint32_t* __restrict__ vin,
+                                                                         K* __restrict__ kout, uint32_t* __restrict__ vout,
+                                                                         size_t n, int shift,
+                                                                         const uint32_t* __restrict__ offs,
+                                                                         unsigned ntiles) {
+    __shared__ uint32_t runBase[256];
+    __shared__ uint32_t cnt[kWarps][256];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    runBase[t] = offs[(size_t)t * ntiles + blockIdx.x];
+    const size_t base = (size_t)blockIdx.x * kRTile;
+    const unsigned lt = (1u << lane) - 1u;
+    for(int r = 0; r < kRPer; ++r) {
+#pragma unroll
+        for(int q = 0; q < kWarps; ++q) cnt[q][t] = 0;
+        __syncthreads();
+        const size_t e = base + (size_t)r * kRT + t;
+        const bool valid = e < n;
+        K key = valid ? kin[e] : K(0);
+        const unsigned d = valid ? (unsigned)((key >> shift) & 0xFF) : 256u;
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const unsigned rank = __popc(peers & lt);
+        if(valid && rank == 0) cnt[w][d] = __popc(peers);
+        __syncthreads();
+        if(valid) {
+            uint32_t off = 0;
+            for(int q = 0; q < w; ++q) off += cnt[q][d];
+            const uint32_t dst = runBase[d] + off + rank;
+            kout[dst] = key;
+            vout[dst] = vin ? vin[e] : (uint32_t)e;
+        }
+        __syncthreads();
+        uint32_t tot = 0;
+#pragma unroll
+        for(int q = 0; q < kWarps; ++q) tot += cnt[q][t];
+        runBase[t] += tot;
+        __syncthreads();
+    }
+}
+
+template<class K> __global__ void k_key_bits(const K* __restrict__ keys, size_t n, unsigned long long* orv,
+                                             unsigned long long* andv) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long o = 0, a = ~0ull;
+    for(; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        unsigned long long k = (unsigned long long)keys[i];
+        o |= k;
+        a &= k;
+    }
+    for(int off = 16; off > 0; off >>= 1) {
+        o |= __shfl_xor_sync(0xffffffffu, o, off);
+        a &= __shfl_xor_sync(0xffffffffu, a, off);
+    }
+    if((threadIdx.x & 31) == 0) { atomicOr(orv, o); atomicAnd(andv, a); }
+}
+
+__global__ void k_iota(uint32_t* v, size_t n) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if(i < n) v[i] = (uint32_t)i;
+}
+
+// Grid::getCellIdx + getCellLinearizedIndex (Grid.h:108-111,156-162), clamped to the grid
+__global__ void k_grid_cell_ids(const float* __restrict__ pos, uint32_t n, float b0, float b1, float b2, float cs,
+                                int n0, int n1, int n2, uint32_t* __restrict__ cid, unsigned* oor) {
+    const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if(p >= n) return;
+    int c[3] = {(int)((pos[3 * p] - b0) / cs), (int)((pos[3 * p + 1] - b1) / cs), (int)((pos[3 * p + 2] - b2) / cs)};
+    const int nn[3] = {n0, n1, n2};
+    bool out = false;
+#pragma unroll
+    for(int d = 0; d < 3; ++d) {
+        if(c[d] < 0) { c[d] = 0; out = true; }
+        if(c[d] >= nn[d]) { c[d] = nn[d] - 1; out = true; }
+    }
+    if(out) atomicAdd(oor, 1u);
+    cid[p] = (uint32_t)(((size_t)c[2] * n1 + c[1]) * n0 + c[0]);
+}
+
+__global__ void k_histogram(const uint32_t* __restrict__ keys, size_t n, uint32_t* __restrict__ count) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if(i < n) atomicAdd(count + keys[i], 1u);
+}
+
+// NeighborSearch::cell_index (NeighborSearch.cpp:44-52) with SHIFT_POSITION 1.2345
+// (DataStructures.h:32) and inv_cell_size = float(1.0 / r)
+__device__ __forceinline__ void ns_key(float x, float y, float z, float inv, int k[3]) {
+    const float sh = 1.2345f;
+    const float t[3] = {x - sh, y - sh, z - sh};
+#pragma unroll
+    for(int d = 0; d < 3; ++d) k[d] = t[d] >= 0.f ? (int)(inv * t[d]) : (int)(inv * t[d]) - 1;
+}
+
+// Morton code as m3D_e_sLUT<uint_fast64_t, uint_fast32_t> (Morton/Morton3D.h:54-66):
+// 8 byte groups, each x/y/z byte bit-interleaved and shifted in by 24 bits, so only the
+// three low bytes of each coordinate survive in the 64-bit code.
+__device__ __forceinline__ unsigned long long spread8(unsigned b) {
+    unsigned long long r = 0;
+#pragma unroll
+    for(int i = 0; i < 8; ++i) r |= (unsigned long long)((b >> i) & 1u) << (3 * i);
+    return r;
+}
+__device__ __forceinline__ unsigned long long morton3d(unsigned long long x, unsigned long long y,
+                                                       unsigned long long z) {
+    unsigned long long ans = 0;
+#pragma unroll
+    for(int i = 8; i > 0; --i) {
+        const unsigned sh = (unsigned)(i - 1) * 8;
+        ans = (ans << 24) | (spread8((unsigned)((z >> sh) & 0xFF)) << 2) | (spread8((unsigned)((y >> sh) & 0xFF)) << 1) |
+              spread8((unsigned)((x >> sh) & 0xFF));
+    }
+    return ans;
+}
+
+// NeighborSearch::z_value (NeighborSearch.cpp:57-67)
+__global__ void k_zvalues(const float* __restrict__ pos, uint32_t n, float inv, unsigned long long* __restrict__ z) {
+    const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if(p >= n) return;
+    int k[3];
+    ns_key(pos[3 * p], pos[3 * p + 1], pos[3 * p + 2], inv, k);
+    unsigned long long c[3];
+#pragma unroll
+    for(int d = 0; d < 3; ++d) c[d] = (unsigned long long)((long long)k[d] - ((long long)INT_MIN + 1));
+    z[p] = morton3d(c[0], c[1], c[2]);
+}
+
+__global__ void k_ns_keys(const float* __restrict__ pos, uint32_t n, float inv, int* __restrict__ keys3,
+                          int* __restrict__ kmin, int* __restrict__ kmax) {
+    const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int k[3] = {INT_MAX, INT_MAX, INT_MAX}, km[3] = {INT_MIN, INT_MIN, INT_MIN};
+    if(p < n) {
+        ns_key(pos[3 * p], pos[3 * p + 1], pos[3 * p + 2], inv, k);
+#pragma unroll
+        for(int d = 0; d < 3; ++d) { keys3[3 * p + d] = k[d]; km[d] = k[d]; }
+    }
+#pragma unroll
+    for(int d = 0; d < 3; ++d) {
+        int a = k[d], b = km[d];
+        for(int off = 16; off > 0; off >>= 1) {
+            a = min(a, __shfl_xor_sync(0xffffffffu, a, off));
+            b = max(b, __shfl_xor_sync(0xffffffffu, b, off));
+        }
+        if((threadIdx.x & 31) == 0) { atomicMin(kmin + d, a); atomicMax(kmax + d, b); }
+    }
+}
+
+__global__ void k_dense_cell(const int* __restrict__ keys3, uint32_t n, const int* __restrict__ kmin, int d0, int d1,
+                             uint32_t* __restrict__ cid) {
+    const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if(p >= n) return;
+    const int x = keys3[3 * p] - kmin[0] + 1, y = keys3[3 * p + 1] - kmin[1] + 1, z = keys3[3 * p + 2] - kmin[2] + 1;
+    cid[p] = (uint32_t)(((size_t)z * d1 + y) * d0 + x);
+}
+
+__global__ void k_gather_pos(const float* __restrict__ pos, const uint32_t* __restrict__ order, uint32_t n,
+                             float4* __restrict__ out) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n) return;
+    const uint32_t p = order[i];
+    out[i] = make_float4(pos[3 * (size_t)p], pos[3 * (size_t)p + 1], pos[3 * (size_t)p + 2], __uint_as_float(p));
+}
+
+// NeighborSearch::query3D (NeighborSearch.cpp:530-692) per point: every other point of the
+// 27 hash cells with (dx*dx + dy*dy) + dz*dz < r^2.  One thread per point in cell-sorted
+// order, so a warp shares its candidate cells.  pass 0 counts, pass 1 writes.
+template<bool WRITE>
+__global__ void __launch_bounds__(256) k_ns_query(const float4* __restrict__ sp, const uint32_t* __restrict__ scid,
+                                                  uint32_t n, const uint32_t* __restrict__ cellStart, int d0, int d1,
+                                                  float r2, uint32_t* __restrict__ counts,
+                                                  const unsigned long long* __restrict__ offsets,
+                                                  uint32_t* __restrict__ idx) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n) return;
+    const float4 a = sp[i];
+    const uint32_t self = __float_as_uint(a.w);
+    const uint32_t c = scid[i];
+    const size_t plane = (size_t)d0 * d1;
+    uint32_t cnt = 0;
+    unsigned long long o = WRITE ? offsets[self] : 0ull;
+    for(int dz = -1; dz <= 1; ++dz)
+        for(int dy = -1; dy <= 1; ++dy) {
+            const size_t row = (size_t)((long long)c + dz * (long long)plane + dy * (long long)d0);
+            const uint32_t b = cellStart[row - 1], e = cellStart[row + 2];
+            for(uint32_t j = b; j < e; ++j) {
+                const float4 q = sp[j];
+                const uint32_t other = __float_as_uint(q.w);
+                if(other == self) continue;
+                const float t0 = a.x - q.x, t1 = a.y - q.y, t2 = a.z - q.z;
+                const float l2 = t0 * t0 + t1 * t1 + t2 * t2;
+                if(l2 < r2) {
+                    if(WRITE) idx[o + cnt] = other;
+                    ++cnt;
+                }
+            }
+        }
+    if(!WRITE) counts[self] = cnt;
+}
+} // namespace
+
+// ---- host helpers -------------------------------------------------------------------
+namespace {
+struct DevBuf {
+    void* p = nullptr;
+    ~DevBuf() { if(p) cudaFree(p); }
+    cudaError_t alloc(size_t b) { return cudaMalloc(&p, b ? b : 1); }
+    template<class T> T* as() { return (T*)p; }
+};
+
+// stable sort of keys (input order for ties); returns permutation in permOut and sorted
+// keys in keysOut.  Uses only the key bits that vary.
+template<class K>
+int radix_sort(const K* keys, size_t n, K* keysOut, uint32_t* permOut, cudaStream_t s) {
+    if(n == 0) return BNN_OK;
+    DevBuf bits, k2, v2, hist, ws;
+    BNN_CUDA_CHECK(bits.alloc(2 * sizeof(unsigned long long)));
+    unsigned long long init[2] = {0ull, ~0ull};
+    BNN_CUDA_CHECK(cudaMemcpyAsync(bits.p, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    k_key_bits<K><<<(unsigned)std::min<size_t>((n + 255) / 256, 4096), 256, 0, s>>>(keys, n, bits.as<unsigned long long>(),
+                                                                                   bits.as<unsigned long long>() + 1);
+    unsigned long long hb[2];
+    BNN_CUDA_CHECK(cudaMemcpyAsync(hb, bits.p, sizeof(hb), cudaMemcpyDeviceToHost, s));
+    BNN_CUDA_CHECK(cudaStreamSynchronize(s));
+    const unsigned long long vary = hb[0] ^ hb[1];
+    int lo = 0, hi = -1;
+    if(vary) {
+        lo = __builtin_ctzll(vary) & ~7;
+        hi = 63 - __builtin_clzll(vary);
+    }
+    const unsigned ntiles = (unsigned)((n + kRTile - 1) / kRTile);
+    BNN_CUDA_CHECK(k2.alloc(n * sizeof(K)));
+    BNN_CUDA_CHECK(v2.alloc(n * sizeof(uint32_t)));
+    BNN_CUDA_CHECK(hist.alloc(((size_t)256 * ntiles + 1) * sizeof(uint32_t)));
+    size_t wsb = scan_workspace_bytes((size_t)256 * ntiles);
+    if(wsb) BNN_CUDA_CHECK(ws.alloc(wsb));
+    std::vector<int> shifts;
+    for(int sh = lo; sh <= hi; sh += 8) shifts.push_back(sh);
+    // ping-pong so that the last pass lands in keysOut / permOut
+    const K* kin = keys;
+    const uint32_t* vin = nullptr;
+    const int np = (int)shifts.size();
+    if(np == 0) {
+        BNN_CUDA_CHECK(cudaMemcpyAsync(keysOut, keys, n * sizeof(K), cudaMemcpyDeviceToDevice, s));
+        k_iota<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(permOut, n);
+        return BNN_OK;
+    }
+    for(int pi = 0; pi < np; ++pi) {
+        const bool toOut = ((np - 1 - pi) % 2) == 0;
+        K* kout = toOut ? keysOut : k2.as<K>();
+        uint32_t* vout = toOut ? permOut : v2.as<uint32_t>();
+        k_radix_hist<K><<<ntiles, kRT, 0, s>>>(kin, n, shifts[pi], hist.as<uint32_t>(), ntiles);
+        BNN_CUDA_CHECK(exclusive_scan_u32(hist.as<uint32_t>(), hist.as<uint32_t>(), (size_t)256 * ntiles, ws.p, s));
+        k_radix_scatter<K><<<ntiles, kRT, 0, s>>>(kin, vin, kout, vout, n, shifts[pi], hist.as<uint32_t>(), ntiles);
+        BNN_CUDA_CHECK(cudaGetLastError());
+        kin = kout;
+        vin = vout;
+    }
+    return BNN_OK;
+}
+} // namespace
+} // namespace bnn
+
+using namespace bnn;
+
+extern "C" int bnn_cell_sort(const float* pos_dev, uint32_t n, const float bmin[3], float cell_size,
+                             const int32_t ncells[3], uint32_t* cell_id_dev, uint32_t* sorted_idx_dev,
+                             uint32_t* cell_start_dev, uint32_t* out_of_range, void* stream) {
+    if((n && (!pos_dev || !cell_id_dev || !sorted_idx_dev)) || !bmin || !ncells || !(cell_size > 0.f))
+        return BNN_ERR_INVALID_ARGUMENT;
+    for(int d = 0; d < 3; ++d) if(ncells[d] <= 0) return BNN_ERR_INVALID_ARGUMENT;
+    const size_t C = (size_t)ncells[0] * ncells[1] * ncells[2];
+    if(C >= 0xffffffffull) return BNN_ERR_NOT_SUPPORTED;
+    cudaStream_t s = (cudaStream_t)stream;
+    DevBuf oor, keysSorted;
+    BNN_CUDA_CHECK(oor.alloc(sizeof(unsigned)));
+    BNN_CUDA_CHECK(cudaMemsetAsync(oor.p, 0, sizeof(unsigned), s));
+    if(n) {
+        k_grid_cell_ids<<<(n + 255) / 256, 256, 0, s>>>(pos_dev, n, bmin[0], bmin[1], bmin[2], cell_size, ncells[0],
+                                                         ncells[1], ncells[2], cell_id_dev, oor.as<unsigned>());
+        BNN_CUDA_CHECK(keysSorted.alloc((size_t)n * sizeof(uint32_t)));
+        int rc = radix_sort<uint32_t>(cell_id_dev, n, keysSorted.as<uint32_t>(), sorted_idx_dev, s);
+        if(rc != BNN_OK) return rc;
+    }
+    if(cell_start_dev) {
+        DevBuf cnt, ws;
+        BNN_CUDA_CHECK(cnt.alloc(C * sizeof(uint32_t)));
+        BNN_CUDA_CHECK(cudaMemsetAsync(cnt.p, 0, C * sizeof(uint32_t), s));
+        if(n) k_histogram<<<(n + 255) / 256, 256, 0, s>>>(cell_id_dev, n, cnt.as<uint32_t>());
+        size_t wsb = scan_workspace_bytes(C);
+        if(wsb) BNN_CUDA_CHECK(ws.alloc(wsb));
+        BNN_CUDA_CHECK(exclusive_scan_u32(cnt.as<uint32_t>(), cell_start_dev, C, ws.p, s));
+    }
+    unsigned h = 0;
+    BNN_CUDA_CHECK(cudaMemcpyAsync(&h, oor.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    BNN_CUDA_CHECK(cudaStreamSynchronize(s));
+    if(out_of_range) *out_of_range = h;
+    return BNN_OK;
+}
+
+extern "C" int bnn_z_sort(const float* pos_dev, uint32_t n, float radius, uint64_t* zvalue_dev, uint32_t* perm_dev,
+                          void* stream) {
+    if((n && (!pos_dev || !zvalue_dev || !perm_dev)) || !(radius > 0.f)) return BNN_ERR_INVALID_ARGUMENT;
+    if(n == 0) return BNN_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    const float inv = (float)(1.0 / (double)radius);
+    k_zvalues<<<(n + 255) / 256, 256, 0, s>>>(pos_dev, n, inv, (unsigned long long*)zvalue_dev);
+    DevBuf sorted;
+    BNN_CUDA_CHECK(sorted.alloc((size_t)n * sizeof(unsigned long long)));
+    int rc = radix_sort<unsigned long long>((const unsigned long long*)zvalue_dev, n, sorted.as<unsigned long long>(),
+                                            perm_dev, s);
+    if(rc != BNN_OK) return rc;
+    BNN_CUDA_CHECK(cudaStreamSynchronize(s));
+    return BNN_OK;
+}
+
+extern "C" int bnn_neighbors(const float* pos_dev, uint32_t n, float radius, uint64_t* offsets_dev, uint32_t* idx_dev,
+                             uint64_t capacity, uint64_t* total, void* stream) {
+    if((n && (!pos_dev || !offsets_dev)) || !(radius > 0.f)) return BNN_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = (cudaStream_t)stream;
+    if(n == 0) {
+        BNN_CUDA_CHECK(cudaMemsetAsync(offsets_dev, 0, sizeof(uint64_t), s));
+        if(total) *total = 0;
+        return BNN_OK;
+    }
+    const float inv = (float)(1.0 / (double)radius);
+    const float r2 = radius * radius;
+    DevBuf keys3, kmm, cid, cidSorted, order, sp, cnt, start, ws, counts, ws64;
+    BNN_CUDA_CHECK(keys3.alloc((size_t)n * 3 * sizeof(int)));
+    BNN_CUDA_CHECK(kmm.alloc(6 * sizeof(int)));
+    int init[6] = {INT_MAX, INT_MAX, INT_MAX, INT_MIN, INT_MIN, INT_MIN};
+    BNN_CUDA_CHECK(cudaMemcpyAsync(kmm.p, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    k_ns_keys<<<(n + 255) / 256, 256, 0, s>>>(pos_dev, n, inv, keys3.as<int>(), kmm.as<int>(), kmm.as<int>() + 3);
+    int hk[6];
+    BNN_CUDA_CHECK(cudaMemcpyAsync(hk, kmm.p, sizeof(hk), cudaMemcpyDeviceToHost, s));
+    BNN_CUDA_CHECK(cudaStreamSynchronize(s));
+    // dense key box with one empty cell of padding on every side
+    const long long d0 = (long long)hk[3] - hk[0] + 3, d1 = (long long)hk[4] - hk[1] + 3, d2 = (long long)hk[5] - hk[2] + 3;
+    const long long V = d0 * d1 * d2;
+    if(V > (1ll << 30)) return BNN_ERR_NOT_SUPPORTED;
+    BNN_CUDA_CHECK(cid.alloc((size_t)n * sizeof(uint32_t)));
+    k_dense_cell<<<(n + 255) / 256, 256, 0, s>>>(keys3.as<int>(), n, kmm.as<int>(), (int)d0, (int)d1, cid.as<uint32_t>());
+    BNN_CUDA_CHECK(cidSorted.alloc((size_t)n * sizeof(uint32_t)));
+    BNN_CUDA_CHECK(order.alloc((size_t)n * sizeof(uint32_t)));
+    int rc = radix_sort<uint32_t>(cid.as<uint32_t>(), n, cidSorted.as<uint32_t>(), order.as<uint32_t>(), s);
+    if(rc != BNN_OK) return rc;
+    BNN_CUDA_CHECK(sp.alloc((size_t)n * sizeof(float4)));
+    k_gather_pos<<<(n + 255) / 256, 256, 0, s>>>(pos_dev, order.as<uint32_t>(), n, sp.as<float4>());
+    BNN_CUDA_CHECK(cnt.alloc((size_t)V * sizeof(uint32_t)));
+    BNN_CUDA_CHECK(start.alloc(((size_t)V + 1) * sizeof(uint32_t)));
+    BNN_CUDA_CHECK(cudaMemsetAsync(cnt.p, 0, (size_t)V * sizeof(uint32_t), s));
+    k_histogram<<<(n + 255) / 256, 256, 0, s>>>(cid.as<uint32_t>(), n, cnt.as<uint32_t>());
+    size_t wsb = scan_workspace_bytes((size_t)V);
+    if(wsb) BNN_CUDA_CHECK(ws.alloc(wsb));
+    BNN_CUDA_CHECK(exclusive_scan_u32(cnt.as<uint32_t>(), start.as<uint32_t>(), (size_t)V, ws.p, s));
+    BNN_CUDA_CHECK(counts.alloc((size_t)n * sizeof(uint32_t)));
+    k_ns_query<false><<<(n + 255) / 256, 256, 0, s>>>(sp.as<float4>(), cidSorted.as<uint32_t>(), n, start.as<uint32_t>(),
+                                                       (int)d0, (int)d1, r2, counts.as<uint32_t>(), nullptr, nullptr);
+    size_t wsb64 = scan_workspace_bytes_u64(n);
+    if(wsb64) BNN_CUDA_CHECK(ws64.alloc(wsb64));
+    BNN_CUDA_CHECK(exclusive_scan_u32_to_u64(counts.as<uint32_t>(), (unsigned long long*)offsets_dev, n, ws64.p, s));
+    uint64_t tot = 0;
+    BNN_CUDA_CHECK(cudaMemcpyAsync(&tot, offsets_dev + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    BNN_CUDA_CHECK(cudaStreamSynchronize(s));
+    if(total) *total = tot;
+    if(tot > capacity) return BNN_ERR_CAPACITY;
+    if(tot && !idx_dev) return BNN_ERR_INVALID_ARGUMENT;
+    k_ns_query<true><<<(n + 255) / 256, 256, 0, s>>>(sp.as<float4>(), cidSorted.as<uint32_t>(), n, start.as<uint32_t>(),
+                                                      (int)d0, (int)d1, r2, nullptr,
+                                                      (const unsigned long long*)offsets_dev, idx_dev);
+    BNN_CUDA_CHECK(cudaGetLastError());
+    BNN_CUDA_CHECK(cudaStreamSynchronize(s));
+    return BNN_OK;
+}

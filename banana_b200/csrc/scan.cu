@@ -1,0 +1,109 @@
+// Device-wide exclusive prefix sums (cell histograms, active-cell numbering, neighbour
+// list offsets).  Integer addition is exact, so the result does not depend on the
+// block layout.
+#include "bnn_internal.cuh"
+
+namespace bnn {
+
+namespace {
+constexpr int kScanThreads = 256;
+constexpr int kScanPer = 8;
+constexpr int kScanTile = kScanThreads * kScanPer;
+
+template<class T> __device__ __forceinline__ T warp_incl_scan(T v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for(int off = 1; off < 32; off <<= 1) {
+        T o = __shfl_up_sync(0xffffffffu, v, off);
+        if(lane >= off) v += o;
+    }
+    return v;
+}
+
+// Exclusive scan of one 2048-element tile; writes the tile total to sums[blockIdx.x] and,
+// for a single-tile scan, also out[n].
+template<class TI, class TO>
+__global__ void __launch_bounds__(kScanThreads) k_scan_tile(const TI* __restrict__ in, TO* __restrict__ out,
+                                                             TO* __restrict__ sums, size_t n) {
+    __shared__ TO warpTot[kScanThreads / 32];
+    const size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanPer;
+    TO v[kScanPer];
+    TO local = 0;
+#pragma unroll
+    for(int j = 0; j < kScanPer; ++j) {
+        size_t e = base + j;
+        v[j] = e < n ? (TO)in[e] : (TO)0;
+        local += v[j];
+    }
+    TO incl = warp_incl_scan(local);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if(lane == 31) warpTot[warp] = incl;
+    __syncthreads();
+    if(warp == 0) {
+        TO w = lane < kScanThreads / 32 ? warpTot[lane] : (TO)0;
+        TO wi = warp_incl_scan(w);
+        if(lane < kScanThreads / 32) warpTot[lane] = wi - w;
+    }
+    __syncthreads();
+    TO run = warpTot[warp] + incl - local;
+#pragma unroll
+    for(int j = 0; j < kScanPer; ++j) {
+        size_t e = base + j;
+        if(e < n) out[e] = run;
+        run += v[j];
+    }
+    if(threadIdx.x == kScanThreads - 1) {
+        if(sums) sums[blockIdx.x] = run;
+        if(gridDim.x == 1) out[n] = run;
+    }
+}
+
+template<class TO> __global__ void k_scan_add(TO* __restrict__ out, const TO* __restrict__ offs, size_t n) {
+    const TO o = offs[blockIdx.x];
+    const size_t base = (size_t)blockIdx.x * kScanTile;
+    for(int j = threadIdx.x; j < kScanTile; j += kScanThreads) {
+        size_t e = base + j;
+        if(e < n) out[e] += o;
+    }
+}
+
+template<class TO> __global__ void k_copy_total(TO* out, size_t n, const TO* sumsScan, size_t nb) { out[n] = sumsScan[nb]; }
+
+template<class TO> size_t ws_bytes(size_t n) {
+    size_t nb = (n + kScanTile - 1) / kScanTile;
+    if(nb <= 1) return 0;
+    size_t here = ((nb + 1) * 2 * sizeof(TO) + 255) & ~size_t(255);
+    return here + ws_bytes<TO>(nb);
+}
+
+template<class TI, class TO> cudaError_t scan_impl(const TI* in, TO* out, size_t n, void* ws, cudaStream_t s) {
+    size_t nb = (n + kScanTile - 1) / kScanTile;
+    if(n == 0) return cudaMemsetAsync(out, 0, sizeof(TO), s);
+    if(nb == 1) {
+        k_scan_tile<TI, TO><<<1, kScanThreads, 0, s>>>(in, out, nullptr, n);
+        return cudaGetLastError();
+    }
+    TO* sums = (TO*)ws;
+    TO* sumsScan = sums + (nb + 1);
+    size_t here = ((nb + 1) * 2 * sizeof(TO) + 255) & ~size_t(255);
+    void* rest = (char*)ws + here;
+    k_scan_tile<TI, TO><<<(unsigned)nb, kScanThreads, 0, s>>>(in, out, sums, n);
+    cudaError_t e = scan_impl<TO, TO>(sums, sumsScan, nb, rest, s);
+    if(e != cudaSuccess) return e;
+    k_scan_add<TO><<<(unsigned)nb, kScanThreads, 0, s>>>(out, sumsScan, n);
+    k_copy_total<TO><<<1, 1, 0, s>>>(out, n, sumsScan, nb);
+    return cudaGetLastError();
+}
+} // namespace
+
+size_t scan_workspace_bytes(size_t n) { return ws_bytes<uint32_t>(n); }
+size_t scan_workspace_bytes_u64(size_t n) { return ws_bytes<unsigned long long>(n); }
+
+cudaError_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, size_t n, void* ws, cudaStream_t s) {
+    return scan_impl<uint32_t, uint32_t>(in, out, n, ws, s);
+}
+cudaError_t exclusive_scan_u32_to_u64(const uint32_t* in, unsigned long long* out, size_t n, void* ws, cudaStream_t s) {
+    return scan_impl<uint32_t, unsigned long long>(in, out, n, ws, s);
+}
+
+} // namespace bnn

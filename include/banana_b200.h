@@ -1,0 +1,182 @@
+/*
+ * banana_b200 -- C ABI of the B200-native FLIP / APIC / AFLIP fluid step, pressure PCG,
+ * uniform-grid cell sort and neighbour search.
+ *
+ * This is the drop-in boundary.  The reference (ttnghia/Banana) drives the hot path
+ * through its solver plugin API:
+ *   ParticleSolver<N,Real>              Simulation/ParticleSolvers/ParticleSolver.h:39-105
+ *   ParticleSolverFactory / Registered   Simulation/ParticleSolvers/ParticleSolverFactory.h:32-60
+ *   PIC_Solver::advanceFrame             Simulation/ParticleSolvers/PICFluid/PIC_Solver.cpp:267-311
+ *   FLIP_Solver::advanceVelocity         Simulation/ParticleSolvers/PICFluid/FLIP_Solver.cpp:42-53
+ * A host C++ class registered in that factory (banana_b200/host/FLIP_GPU_Solver.h) owns one
+ * bnn_flip handle and forwards advanceFrame / particle I/O to the functions below.
+ *
+ * Conventions: every function returns an int status (BNN_OK = 0).  Arrays are HOST
+ * pointers unless the parameter name ends in _dev.  Particle arrays are AoS float3
+ * (x,y,z per particle), the layout of glm::vec3 in ParticleSimulationData::positions
+ * (ParticleSolverData.h:197).  Grid arrays use the reference Array<3,T> layout
+ * (k*Sy + j)*Sx + i (BananaCore/Banana/Array/Array.h:276).  A handle is driven by one
+ * host thread at a time; distinct handles may be used from distinct threads.
+ * No function calls exit(): failures that the reference turns into exit(EXIT_FAILURE)
+ * (__BNN_REQUIRE, Macros.h:225-233, and ExitIfPressureProjectionFailed,
+ * PIC_Solver.cpp:901-906) come back as status codes.
+ */
+#ifndef BANANA_B200_H
+#define BANANA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------- */
+#define BNN_OK                    0
+#define BNN_ERR_INVALID_ARGUMENT  1  /* __BNN_REQUIRE failures in the reference */
+#define BNN_ERR_OUT_OF_MEMORY     2
+#define BNN_ERR_PCG_NOT_CONVERGED 3  /* PCGSolver::solve_precond returned false */
+#define BNN_ERR_DEVICE_CHECK      4  /* a kernel's own range / state check failed */
+#define BNN_ERR_TIMEOUT           5  /* a bounded device-side wait gave up */
+#define BNN_ERR_CUDA              6
+#define BNN_ERR_NOT_SUPPORTED     7
+#define BNN_ERR_CAPACITY          8  /* output buffer too small (neighbour lists) */
+
+/* ---- enums ----------------------------------------------------------------------- */
+#define BNN_SOLVER_FLIP   0  /* FLIP_3DSolver  (FLIP_Solver.cpp)  */
+#define BNN_SOLVER_APIC   1  /* APIC_3DSolver  (APIC_Solver.cpp)  */
+#define BNN_SOLVER_AFLIP  2  /* AFLIP_3DSolver (AFLIP_Solver.cpp) */
+
+#define BNN_PCG_FP32      0  /* FP32 vectors, FP64 dot/norm reductions */
+#define BNN_PCG_FP64      1  /* FP64 vectors and reductions */
+#define BNN_PCG_REFINED   2  /* FP32 inner PCG + FP64 outer residual (iterative refinement) */
+
+#define BNN_PRECOND_JACOBI 0 /* PCGSolver::JACOBI (PCGSolver.cpp:232-237,273-284) */
+
+#define BNN_FIELD_U        0 /* face velocities, sizes (G+1)GG, G(G+1)G, GG(G+1) */
+#define BNN_FIELD_V        1
+#define BNN_FIELD_W        2
+#define BNN_FIELD_PHI      3 /* fluid SDF on cells (PIC_Data.h fluidSDF) */
+#define BNN_FIELD_PRESSURE 4 /* pressure scattered onto cells, 0 where not fluid */
+#define BNN_FIELD_OLD_U    5 /* FLIP backup velocities (FLIP_Data.h oldVels) */
+#define BNN_FIELD_OLD_V    6
+#define BNN_FIELD_OLD_W    7
+#define BNN_FIELD_ACTIVE   8 /* active cell index + 1 on cells, 0 = not fluid */
+
+/* Values of SimulationParameters / PIC_Parameters / GlobalParameters the step reads
+ * (ParticleSolverData.h:87-175, PIC_Data.h:31-40, ParticleSolverData.h:37-75). */
+typedef struct bnn_params {
+    float    box_min[3];             /* SimulationDomainBox BoxMin (before NExpandCells padding) */
+    float    box_max[3];             /* SimulationDomainBox BoxMax */
+    float    cell_size;              /* CellSize */
+    uint32_t n_expand_cells;         /* NExpandCells (default 2) */
+    float    cfl_factor;             /* CFLFactor (default 1) */
+    float    min_timestep;           /* MinTimestep (default 1e-6) */
+    float    max_timestep;           /* MaxTimestep (default 1/30) */
+    float    frame_duration;         /* FrameDuration (default 1/30) */
+    float    pic_flip_ratio;         /* PIC_FLIP_ratio (default 0.97) */
+    float    cg_relative_tolerance;  /* CGRelativeTolerance */
+    uint32_t max_cg_iteration;       /* MaxCGIteration */
+    uint32_t advection_steps;        /* AdvectionSteps (default 1) */
+    int32_t  solver_kind;            /* BNN_SOLVER_* */
+    int32_t  pcg_mode;               /* BNN_PCG_* */
+    int32_t  preconditioner;         /* BNN_PRECOND_* */
+    float    refine_tolerance;       /* BNN_PCG_REFINED: outer max-norm relative tolerance */
+    float    refine_inner_tolerance; /* BNN_PCG_REFINED: inner FP32 relative tolerance */
+    int32_t  apply_gravity;          /* GlobalParameters ApplyGravity (default 1) */
+    uint32_t max_particles;          /* particle capacity; 0 = size to the first set_particles */
+} bnn_params;
+
+/* What one call of bnn_flip_step did.  stage_ms are CUDA-event times of the stages:
+ * 0 move, 1 sort, 2 p2g, 3 extrapolate+backup+gravity, 4 fluid sdf, 5 system, 6 pcg,
+ * 7 update+extrapolate, 8 g2p, 9 whole step. */
+typedef struct bnn_step_stats {
+    double   dt;               /* sub-step size used (PIC_Solver.cpp:284-290) */
+    double   frame_time;       /* frameLocalTime after the sub-step */
+    uint32_t frame_finished;   /* 1 when frame_time reached FrameDuration */
+    uint32_t pcg_iterations;   /* PCGSolver::iterations() (inner total for refinement) */
+    double   pcg_residual;     /* PCGSolver::residual(): max|r| of the last iterate */
+    uint32_t pcg_success;
+    uint32_t n_active;         /* rows of the pressure system */
+    uint32_t outer_iterations; /* refinement sweeps (BNN_PCG_REFINED) */
+    uint32_t zero_phi_cells;   /* interior cells with fluid SDF exactly 0 (left out) */
+    float    stage_ms[10];
+    uint32_t device_flags;     /* bit 0: particle outside the grid, bit 1: fluid in the
+                                  outer cell ring, bit 2: PCG hit MaxCGIteration */
+} bnn_step_stats;
+
+typedef struct bnn_flip bnn_flip;
+
+/* Create a solver: grid setup as SimulationParameters::makeReady + PIC_Data::makeReady
+ * (ParticleSolverData.cpp:229-272, PIC_Data.cpp:128-144). */
+int bnn_flip_create(const bnn_params* params, bnn_flip** out);
+int bnn_flip_destroy(bnn_flip* h);
+/* Grid cell counts G (after padding) */
+int bnn_flip_grid_dims(bnn_flip* h, int32_t g[3]);
+/* Replace all particles (PIC_ParticleData::addParticles, PIC_Data.cpp:73-82, into an
+ * empty solver); grid velocities are reset to 0 as after makeReady. */
+int bnn_flip_set_particles(bnn_flip* h, const float* pos, const float* vel, uint32_t n);
+/* Particles in the order they were given (ParticleSolverInterface.h:128-149 reads
+ * positions / velocities as raw host arrays between frames). */
+int bnn_flip_get_particles(bnn_flip* h, float* pos, float* vel);
+int bnn_flip_num_particles(bnn_flip* h, uint32_t* n);
+/* Copy one grid field (BNN_FIELD_*) of `count` floats to host. */
+int bnn_flip_get_grid(bnn_flip* h, int32_t field, float* out, size_t count);
+/* One iteration of PIC_Solver::advanceFrame's sub-step loop (CFL, moveParticles,
+ * advanceVelocity; PIC_Solver.cpp:277-305).  A new frame starts when the previous one
+ * finished. */
+int bnn_flip_step(bnn_flip* h, bnn_step_stats* stats);
+/* PIC_Solver::advanceFrame: sub-steps until FrameDuration is reached. */
+int bnn_flip_advance_frame(bnn_flip* h, uint32_t* substeps);
+/* Device pointers of the particle arrays (SoA x,y,z,vx,vy,vz, current sorted order),
+ * valid until the next step; lets a caller keep data on the device. */
+int bnn_flip_device_particles(bnn_flip* h, float** xyz_vxyz_dev, uint32_t** ids_dev);
+/* Same sub-step as bnn_flip_step, but the particles come from pinned host AoS arrays and
+ * are written back to them: upload, step, download in one stream (end-to-end timing). */
+int bnn_flip_step_host(bnn_flip* h, float* pos, float* vel, bnn_step_stats* stats);
+
+/* ---- standalone kernels (device pointers, stream = cudaStream_t or NULL) ---------- */
+
+/* Grid::getCellIdx + getCellLinearizedIndex (Grid.h:108-111,156-162) for every point and
+ * the canonical sorted index (stable: by linear cell id, ties in input order), i.e.
+ * Grid::getParticleIdxSortedByCell (Grid.cpp:299-309) of a one-thread collectIndexToCells.
+ * cell_start_dev (optional) receives the C+1 bucket offsets.  Points outside the grid
+ * are clamped onto its border and counted in *out_of_range. */
+int bnn_cell_sort(const float* pos_dev, uint32_t n, const float bmin[3], float cell_size, const int32_t ncells[3],
+                  uint32_t* cell_id_dev, uint32_t* sorted_idx_dev, uint32_t* cell_start_dev, uint32_t* out_of_range,
+                  void* stream);
+
+/* NeighborSearch::z_sort (NeighborSearch.cpp:57-86): Morton code of each point's hash key
+ * and the permutation sorting by it (ties in input order). */
+int bnn_z_sort(const float* pos_dev, uint32_t n, float radius, uint64_t* zvalue_dev, uint32_t* perm_dev, void* stream);
+
+/* NeighborSearch::find_neighbors for one self-searching point set (NeighborSearch.cpp:
+ * 219-226, query3D :530-692): neighbours of each point are all other points with
+ * |x-y|^2 < r^2.  Output CSR: offsets_dev (n+1), idx_dev (capacity entries), each list
+ * sorted ascending.  *total receives the entry count; BNN_ERR_CAPACITY when it exceeds
+ * capacity (offsets are still written). */
+int bnn_neighbors(const float* pos_dev, uint32_t n, float radius, uint64_t* offsets_dev, uint32_t* idx_dev,
+                  uint64_t capacity, uint64_t* total, void* stream);
+
+/* Standalone Jacobi PCG (PCGSolver::solve_precond, PCGSolver.cpp:143-199) on a 7-point
+ * system given in host memory: diag[n], nbr[6n] neighbour rows in column order
+ * (-z,-y,-x,+x,+y,+z; -1 = none), one off-diagonal value for every neighbour, rhs[n].
+ * mode BNN_PCG_*.  x_out receives the solution in FP64. */
+typedef struct bnn_pcg_stats {
+    uint32_t iterations;
+    uint32_t outer_iterations;
+    double   residual;
+    uint32_t success;
+    float    ms;
+} bnn_pcg_stats;
+int bnn_pcg_solve_7pt(uint32_t n, const float* diag, const int32_t* nbr, float offdiag, const float* rhs, float tol,
+                      uint32_t max_iter, int32_t mode, float inner_tol, double* x_out, bnn_pcg_stats* stats);
+
+/* Library version / last CUDA error text for diagnostics */
+const char* bnn_version(void);
+const char* bnn_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BANANA_B200_H */

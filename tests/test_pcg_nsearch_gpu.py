@@ -1,0 +1,146 @@
+"""Standalone PCG, cell sort, z-sort and neighbour search through the C ABI, against the
+oracle (restatements of PCGSolver.cpp, Grid.cpp and NeighborSearch.cpp)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+from banana_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _system(oracle_mod, n=32, steps=3):
+    cfg = scenes.dam_break_params(n)
+    pos, vel = scenes.dam_break(n)
+    o = oracle_mod.Oracle(cfg)
+    o.set_particles(pos, vel)
+    for _ in range(steps):
+        o.step()
+    rs, ci, va, rhs = o.system()
+    nrow = len(rhs)
+    diag = np.zeros(nrow, np.float32)
+    nbr = -np.ones((nrow, 6), np.int32)
+    off = None
+    for r in range(nrow):
+        cols = ci[rs[r]:rs[r + 1]]
+        vals = va[rs[r]:rs[r + 1]]
+        lo = [c for c in cols if c < r]
+        hi = [c for c in cols if c > r]
+        for c, v in zip(cols, vals):
+            if c == r:
+                diag[r] = v
+            else:
+                off = v
+        nbr[r, 3 - len(lo):3] = lo
+        nbr[r, 3:3 + len(hi)] = hi
+    return (rs, ci, va, rhs), diag, nbr, off
+
+
+@pytest.mark.parametrize("mode,omode", [("fp32", 0), ("fp64", 1), ("refined", 2)])
+def test_pcg_7pt_matches_oracle(bnn, oracle_mod, mode, omode):
+    (rs, ci, va, rhs), diag, nbr, off = _system(oracle_mod)
+    tol = 1e-8 if mode == "refined" else 1e-6
+    x, st = bnn.pcg_solve_7pt(diag, nbr, off, rhs, tol, 5000, mode=mode, inner_tol=1e-3)
+    xo, so = oracle_mod.pcg(rs, ci, va, rhs, tol, 5000, omode, inner_tol=1e-3)
+    assert st["success"] == 1 and so["success"]
+    assert st["iterations"] == so["iterations"]
+    if mode == "fp32":
+        assert np.array_equal(x.astype(np.float32), xo.astype(np.float32))
+    else:
+        assert np.array_equal(x, xo)
+
+
+def test_refined_reaches_1e8_fp64_checked(bnn, oracle_mod):
+    """Refined FP32 PCG: max|b - A x| (FP64) < 1e-8 max|b|"""
+    (rs, ci, va, rhs), diag, nbr, off = _system(oracle_mod, n=32, steps=4)
+    x, st = bnn.pcg_solve_7pt(diag, nbr, off, rhs, 1e-8, 5000, mode="refined", inner_tol=1e-3)
+    n = len(rhs)
+    ax = np.zeros(n)
+    for r in range(n):
+        for j in range(rs[r], rs[r + 1]):
+            ax[r] += float(va[j]) * x[ci[j]]
+    res = np.abs(rhs.astype(np.float64) - ax).max()
+    assert res < 1e-8 * np.abs(rhs).max()
+
+
+def _dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def test_cell_sort_bitexact(bnn, oracle_mod):
+    pts = scenes.point_cloud(200_000, seed=7)
+    bmin = np.zeros(3, np.float32)
+    nc = np.array([100, 100, 100], np.int32)
+    cid, srt, start, oor = oracle_mod.cell_sort(pts, bmin, np.float32(0.01), nc)
+    L = bnn.load()
+    p = _dev(pts)
+    n = len(pts)
+    gc = torch.zeros(n, dtype=torch.int32, device="cuda")
+    gs = torch.zeros(n, dtype=torch.int32, device="cuda")
+    gst = torch.zeros(int(nc.prod()) + 1, dtype=torch.int32, device="cuda")
+    o = C.c_uint32()
+    rc = L.bnn_cell_sort(C.c_void_p(p.data_ptr()), n, bmin.ctypes.data_as(C.POINTER(C.c_float)), 0.01,
+                         nc.ctypes.data_as(C.POINTER(C.c_int32)), C.c_void_p(gc.data_ptr()), C.c_void_p(gs.data_ptr()),
+                         C.c_void_p(gst.data_ptr()), C.byref(o), None)
+    torch.cuda.synchronize()
+    assert rc == 0
+    assert o.value == oor
+    assert np.array_equal(gc.cpu().numpy().view(np.uint32), cid)
+    assert np.array_equal(gs.cpu().numpy().view(np.uint32), srt)
+    assert np.array_equal(gst.cpu().numpy().view(np.uint32), start)
+
+
+def test_z_sort_bitexact(bnn, oracle_mod):
+    pts = scenes.point_cloud(100_000, seed=3)
+    z, perm = oracle_mod.z_sort(pts, np.float32(0.01))
+    L = bnn.load()
+    p = _dev(pts)
+    n = len(pts)
+    gz = torch.zeros(n, dtype=torch.int64, device="cuda")
+    gp = torch.zeros(n, dtype=torch.int32, device="cuda")
+    rc = L.bnn_z_sort(C.c_void_p(p.data_ptr()), n, 0.01, C.c_void_p(gz.data_ptr()), C.c_void_p(gp.data_ptr()), None)
+    assert rc == 0
+    assert np.array_equal(gz.cpu().numpy().view(np.uint64), z)
+    assert np.array_equal(gp.cpu().numpy().view(np.uint32), perm)
+
+
+def _lists(off, idx, n):
+    return [np.sort(idx[off[i]:off[i + 1]]) for i in range(n)]
+
+
+@pytest.mark.parametrize("n,seed", [(30_000, 7), (60_000, 1)])
+def test_neighbors_set_equal(bnn, oracle_mod, n, seed):
+    pts = scenes.point_cloud(n, seed=seed)
+    r = np.float32(0.01)
+    off_o, idx_o = oracle_mod.neighbors(pts, r)
+    L = bnn.load()
+    p = _dev(pts)
+    goff = torch.zeros(n + 1, dtype=torch.int64, device="cuda")
+    cap = int(off_o[-1]) + 16
+    gidx = torch.zeros(max(cap, 1), dtype=torch.int32, device="cuda")
+    tot = C.c_uint64()
+    rc = L.bnn_neighbors(C.c_void_p(p.data_ptr()), n, r, C.c_void_p(goff.data_ptr()), C.c_void_p(gidx.data_ptr()),
+                         cap, C.byref(tot), None)
+    assert rc == 0
+    assert tot.value == off_o[-1]
+    go = goff.cpu().numpy().view(np.uint64)
+    gi = gidx.cpu().numpy().view(np.uint32)[: tot.value]
+    assert np.array_equal(go, off_o)
+    # set equality per point (the reference's list order depends on its thread schedule)
+    owner = np.repeat(np.arange(n), np.diff(go).astype(np.int64))
+    a = np.lexsort((gi, owner))
+    assert np.array_equal(gi[a], idx_o)
+
+
+def test_neighbors_capacity_error(bnn):
+    pts = scenes.point_cloud(5_000, seed=2)
+    L = bnn.load()
+    p = _dev(pts)
+    goff = torch.zeros(len(pts) + 1, dtype=torch.int64, device="cuda")
+    gidx = torch.zeros(4, dtype=torch.int32, device="cuda")
+    tot = C.c_uint64()
+    rc = L.bnn_neighbors(C.c_void_p(p.data_ptr()), len(pts), 0.05, C.c_void_p(goff.data_ptr()),
+                         C.c_void_p(gidx.data_ptr()), 4, C.byref(tot), None)
+    assert rc == 8 and tot.value > 4
