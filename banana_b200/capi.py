@@ -6,12 +6,13 @@ in-tree CUDA library and raises if it is missing: there is no CPU path behind it
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 import numpy as np
 
 PKG = Path(__file__).resolve().parent
-LIB_PATH = PKG / "libbanana_b200.so"
+LIB_PATH = Path(os.environ.get("BNN_LIB", str(PKG / "libbanana_b200.so")))
 
 BNN_OK = 0
 STATUS = {0: "OK", 1: "INVALID_ARGUMENT", 2: "OUT_OF_MEMORY", 3: "PCG_NOT_CONVERGED", 4: "DEVICE_CHECK",
@@ -24,8 +25,8 @@ FIELD = {"u": 0, "v": 1, "w": 2, "phi": 3, "pressure": 4, "old_u": 5, "old_v": 6
 EXPORTS = [
     "bnn_flip_create", "bnn_flip_destroy", "bnn_flip_grid_dims", "bnn_flip_set_particles", "bnn_flip_get_particles",
     "bnn_flip_num_particles", "bnn_flip_get_grid", "bnn_flip_step", "bnn_flip_advance_frame",
-    "bnn_flip_device_particles", "bnn_flip_step_host", "bnn_cell_sort", "bnn_z_sort", "bnn_neighbors",
-    "bnn_pcg_solve_7pt", "bnn_version", "bnn_last_error",
+    "bnn_flip_device_particles", "bnn_flip_step_host", "bnn_flip_stream", "bnn_cell_sort", "bnn_z_sort", "bnn_neighbors",
+    "bnn_pcg_solve_7pt", "bnn_version", "bnn_last_error", "bnn_launch_count",
 ]
 
 
@@ -91,18 +92,26 @@ def load() -> C.CDLL:
     L.bnn_flip_advance_frame.argtypes = [vp, u32p]
     L.bnn_flip_device_particles.argtypes = [vp, C.POINTER(fp), C.POINTER(u32p)]
     L.bnn_flip_step_host.argtypes = [vp, fp, fp, C.POINTER(StepStats)]
+    L.bnn_flip_stream.argtypes = [vp, C.POINTER(vp)]
     L.bnn_cell_sort.argtypes = [vp, C.c_uint32, fp, C.c_float, i32p, vp, vp, vp, u32p, vp]
     L.bnn_z_sort.argtypes = [vp, C.c_uint32, C.c_float, vp, vp, vp]
     L.bnn_neighbors.argtypes = [vp, C.c_uint32, C.c_float, vp, vp, C.c_uint64, u64p, vp]
     L.bnn_pcg_solve_7pt.argtypes = [C.c_uint32, fp, i32p, C.c_float, fp, C.c_float, C.c_uint32, C.c_int32, C.c_float,
                                     dp, C.POINTER(PcgStats)]
+    L.bnn_launch_count.argtypes = []
+    L.bnn_launch_count.restype = C.c_uint64
     L.bnn_version.restype = C.c_char_p
     L.bnn_last_error.restype = C.c_char_p
     for name in EXPORTS:
-        if name not in ("bnn_version", "bnn_last_error"):
+        if name not in ("bnn_version", "bnn_last_error", "bnn_launch_count"):
             getattr(L, name).restype = C.c_int
     _lib = L
     return L
+
+
+def launch_count() -> int:
+    """Kernels launched by libbanana_b200 so far in this process."""
+    return int(load().bnn_launch_count())
 
 
 def last_error() -> str:
@@ -215,6 +224,21 @@ class FlipSolver:
         st = StepStats()
         check(self.L.bnn_flip_step_host(self.h, _p(pos, C.c_float), _p(vel, C.c_float), C.byref(st)),
               "bnn_flip_step_host")
+        d = {f: getattr(st, f) for f, _ in StepStats._fields_ if f != "stage_ms"}
+        d["stage_ms"] = dict(zip(STAGES, list(st.stage_ms)))
+        return d
+
+    def stream_ptr(self) -> int:
+        """cudaStream_t of this handle (all its kernels run on it)"""
+        s = C.c_void_p()
+        check(self.L.bnn_flip_stream(self.h, C.byref(s)), "bnn_flip_stream")
+        return int(s.value or 0)
+
+    def step_host_ptr(self, pos_ptr: int, vel_ptr: int) -> dict:
+        """bnn_flip_step_host on raw (pinned) host pointers"""
+        st = StepStats()
+        check(self.L.bnn_flip_step_host(self.h, C.cast(pos_ptr, C.POINTER(C.c_float)),
+                                        C.cast(vel_ptr, C.POINTER(C.c_float)), C.byref(st)), "bnn_flip_step_host")
         d = {f: getattr(st, f) for f, _ in StepStats._fields_ if f != "stage_ms"}
         d["stage_ms"] = dict(zip(STAGES, list(st.stage_ms)))
         return d

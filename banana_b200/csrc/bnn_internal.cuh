@@ -78,11 +78,17 @@ __device__ __forceinline__ bool last_block(unsigned* counter) {
     return amLast;
 }
 
-// Final pass over chunk partials in the canonical order (called by one whole block)
+// Final pass over chunk partials in the canonical order (called by one whole block);
+// the result is returned to every thread of the block.
 __device__ __forceinline__ double reduce_partials(const double* part, int nch, double* sm) {
     double acc = 0.0;
     for(int c = threadIdx.x; c < nch; c += kLanes) acc = acc + __ldcg(part + c);
-    return block_sum_256(acc, sm);
+    const double r = block_sum_256(acc, sm);
+    if(threadIdx.x == 0) sm[0] = r;
+    __syncthreads();
+    const double b = sm[0];
+    __syncthreads();
+    return b;
 }
 __device__ __forceinline__ float reduce_partials_max(const float* part, int nch, float* sm) {
     float acc = 0.f;
@@ -152,6 +158,7 @@ struct DevState {
 #define BNN_FLAG_RING_FLUID    2u
 #define BNN_FLAG_PCG_MAXITER   4u
 #define BNN_FLAG_SCRATCH_LIMIT 8u
+#define BNN_FLAG_TIMEOUT       16u
 
 // ----------------------------------------------------------------------------------
 // Host-side launchers (defined in the .cu files)
@@ -162,8 +169,14 @@ size_t scan_workspace_bytes(size_t n);
 cudaError_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, size_t n, void* ws, cudaStream_t s);
 
 // pcg.cu
+struct GridSync {
+    unsigned count;  // blocks arrived at the current barrier
+    unsigned gen;    // barrier generation
+};
 struct PcgWork {
     int cap = 0;
+    int nchCap = 0;
+    GridSync* gs = nullptr;
     float *x = nullptr, *r = nullptr, *z = nullptr, *s0 = nullptr, *s1 = nullptr, *q = nullptr, *d32 = nullptr,
           *r32 = nullptr;
     double *x64 = nullptr, *r64 = nullptr, *z64 = nullptr, *s064 = nullptr, *s164 = nullptr, *q64 = nullptr,
@@ -184,6 +197,10 @@ void pcg_release(PcgWork& w);
 } // namespace bnn
 
 extern "C" void bnn_set_error(const char* msg);
+
+// Every kernel launch of the library is followed by bnn_note_launch(): the running total
+// is what bnn_launch_count() reports.
+void bnn_note_launch();
 
 #define BNN_CUDA_CHECK(expr)                                                                 \
     do {                                                                                     \

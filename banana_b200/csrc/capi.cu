@@ -10,7 +10,12 @@
 #include <string>
 #include <vector>
 
+#include <atomic>
+
 static thread_local std::string g_lastError;
+static std::atomic<unsigned long long> g_launches{0};
+void bnn_note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+extern "C" uint64_t bnn_launch_count(void) { return g_launches.load(); }
 extern "C" void bnn_set_error(const char* msg) { g_lastError = msg ? msg : ""; }
 extern "C" const char* bnn_last_error(void) { return g_lastError.c_str(); }
 extern "C" const char* bnn_version(void) { return "banana_b200 0.1 (sm_100a)"; }
@@ -235,6 +240,12 @@ extern "C" int bnn_flip_destroy(bnn_flip* h) {
     if(!h) return BNN_ERR_INVALID_ARGUMENT;
     if(h->s) cudaStreamSynchronize(h->s);
     destroy_all(h);
+    return BNN_OK;
+}
+
+extern "C" int bnn_flip_stream(bnn_flip* h, void** stream) {
+    if(!h || !stream) return BNN_ERR_INVALID_ARGUMENT;
+    *stream = (void*)h->s;
     return BNN_OK;
 }
 

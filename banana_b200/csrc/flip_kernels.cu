@@ -671,22 +671,22 @@ static inline unsigned nblk(size_t n, int t = 256) { return (unsigned)((n + t - 
 void launch_advect(int n, float* p6, size_t stride, const float* const* U, const GridDesc& g, float sub, int steps,
                    uint32_t* cellOf, uint32_t* slot, uint32_t* count, DevState* st, cudaStream_t s) {
     if(n == 0) return;
-    k_advect<<<nblk(n), 256, 0, s>>>(n, p6, p6 + stride, p6 + 2 * stride, U[0], U[1], U[2], g, sub, steps, cellOf, slot,
-                                     count, st);
+    { k_advect<<<nblk(n), 256, 0, s>>>(n, p6, p6 + stride, p6 + 2 * stride, U[0], U[1], U[2], g, sub, steps, cellOf, slot,
+                                     count, st); bnn_note_launch(); }
 }
 void launch_cell_histogram(int n, const float* p6, size_t stride, const GridDesc& g, uint32_t* cellOf, uint32_t* slot,
                            uint32_t* count, DevState* st, cudaStream_t s) {
     if(n == 0) return;
-    k_cell_histogram<<<nblk(n), 256, 0, s>>>(n, p6, p6 + stride, p6 + 2 * stride, g, cellOf, slot, count, st);
+    { k_cell_histogram<<<nblk(n), 256, 0, s>>>(n, p6, p6 + stride, p6 + 2 * stride, g, cellOf, slot, count, st); bnn_note_launch(); }
 }
 void launch_sort_finish(int n, size_t ncells, const uint32_t* cellOf, const uint32_t* slot, const uint32_t* cellStart,
                         uint32_t* order, uint32_t* count, const float* src6, float* dst6, const uint32_t* idSrc,
                         uint32_t* idDst, const float* cSrc, float* cDst, float* g3, const GridDesc& g, size_t stride,
                         cudaStream_t s) {
-    if(n > 0) k_scatter_index<<<nblk(n), 256, 0, s>>>(n, cellOf, slot, cellStart, order);
-    k_sort_buckets<<<nblk(ncells), 256, 0, s>>>((int)ncells, cellStart, order, idSrc, count);
+    if(n > 0) { k_scatter_index<<<nblk(n), 256, 0, s>>>(n, cellOf, slot, cellStart, order); bnn_note_launch(); }
+    { k_sort_buckets<<<nblk(ncells), 256, 0, s>>>((int)ncells, cellStart, order, idSrc, count); bnn_note_launch(); }
     if(n > 0)
-        k_gather_particles<<<nblk(n), 256, 0, s>>>(n, order, src6, dst6, idSrc, idDst, cSrc, cDst, g3, g, stride);
+        { k_gather_particles<<<nblk(n), 256, 0, s>>>(n, order, src6, dst6, idSrc, idDst, cSrc, cDst, g3, g, stride); bnn_note_launch(); }
 }
 void launch_p2g(const GridDesc& g, const uint32_t* cellStart, const float* g3, const float* p6, const float* C9,
                 size_t stride, float* const* out, uint8_t* const* valid, bool affine, cudaStream_t s) {
@@ -697,13 +697,13 @@ void launch_p2g(const GridDesc& g, const uint32_t* cellStart, const float* g3, c
         const float* vd = p6 + (3 + d) * stride;
         const float* Cd = C9 ? C9 + (size_t)(3 * d) * stride : nullptr;
         if(affine) {
-            if(d == 0) k_p2g<0, true><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[0], valid[0]);
-            if(d == 1) k_p2g<1, true><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[1], valid[1]);
-            if(d == 2) k_p2g<2, true><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[2], valid[2]);
+            if(d == 0) { k_p2g<0, true><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[0], valid[0]); bnn_note_launch(); }
+            if(d == 1) { k_p2g<1, true><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[1], valid[1]); bnn_note_launch(); }
+            if(d == 2) { k_p2g<2, true><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[2], valid[2]); bnn_note_launch(); }
         } else {
-            if(d == 0) k_p2g<0, false><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[0], valid[0]);
-            if(d == 1) k_p2g<1, false><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[1], valid[1]);
-            if(d == 2) k_p2g<2, false><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[2], valid[2]);
+            if(d == 0) { k_p2g<0, false><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[0], valid[0]); bnn_note_launch(); }
+            if(d == 1) { k_p2g<1, false><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[1], valid[1]); bnn_note_launch(); }
+            if(d == 2) { k_p2g<2, false><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[2], valid[2]); bnn_note_launch(); }
         }
     }
 }
@@ -720,61 +720,61 @@ void launch_extrapolate(const GridDesc& g, float* const* A, uint8_t* const* VA, 
             uint8_t* vout = (layer % 2 == 0) ? VB[d] : VA[d];
             int mode = layer == 3 ? lastMode : 0;
             float gdt = (mode == 1 && d == 1) ? gravityDt : 0.f;
-            k_extrapolate<<<nblk(nf), 256, 0, s>>>(sx, sy, sz, gin, vin, gout, vout, mode, oldOut ? oldOut[d] : nullptr,
-                                                   gdt, st);
+            { k_extrapolate<<<nblk(nf), 256, 0, s>>>(sx, sy, sz, gin, vin, gout, vout, mode, oldOut ? oldOut[d] : nullptr,
+                                                   gdt, st); bnn_note_launch(); }
         }
     }
 }
 void launch_fluid_sdf(const GridDesc& g, const uint32_t* cellStart, const float* g3, const float* p6, size_t stride,
                       float* phi, cudaStream_t s) {
     size_t nc = (size_t)g.G[0] * g.G[1] * g.G[2];
-    k_fluid_sdf<<<nblk(nc), 256, 0, s>>>(g, cellStart, g3, g3 + stride, g3 + 2 * stride, p6, p6 + stride,
-                                         p6 + 2 * stride, phi);
+    { k_fluid_sdf<<<nblk(nc), 256, 0, s>>>(g, cellStart, g3, g3 + stride, g3 + 2 * stride, p6, p6 + stride,
+                                         p6 + 2 * stride, phi); bnn_note_launch(); }
 }
 void launch_active_flags(const GridDesc& g, const float* phi, uint32_t* flag, DevState* st, cudaStream_t s) {
     size_t nc = (size_t)g.G[0] * g.G[1] * g.G[2];
-    k_active_flags<<<nblk(nc), 256, 0, s>>>(g, phi, flag, st);
+    { k_active_flags<<<nblk(nc), 256, 0, s>>>(g, phi, flag, st); bnn_note_launch(); }
 }
 void launch_active_rows(size_t nc, const uint32_t* flag, const uint32_t* idx, uint32_t* rowCell, cudaStream_t s) {
-    k_active_rows<<<nblk(nc), 256, 0, s>>>(nc, flag, idx, rowCell);
+    { k_active_rows<<<nblk(nc), 256, 0, s>>>(nc, flag, idx, rowCell); bnn_note_launch(); }
 }
 void launch_build_rows(const GridDesc& g, int nrows, const uint32_t* rowCell, const float* phi, const uint32_t* aidx,
                        const float* const* U, float dt, float* rhs, float* diag, float* invdiag, int32_t* nbr,
                        DevState* st, cudaStream_t s) {
     if(nrows == 0) return;
-    k_build_rows<<<nblk(nrows), 256, 0, s>>>(g, nrows, rowCell, phi, aidx, U[0], U[1], U[2], dt, rhs, diag, invdiag,
-                                             nbr, st);
+    { k_build_rows<<<nblk(nrows), 256, 0, s>>>(g, nrows, rowCell, phi, aidx, U[0], U[1], U[2], dt, rhs, diag, invdiag,
+                                             nbr, st); bnn_note_launch(); }
 }
 void launch_update_velocity(const GridDesc& g, const float* phi, const uint32_t* aidx, const float* pressure, float dt,
                             float* const* U, uint8_t* const* V, cudaStream_t s) {
     size_t n0 = (size_t)face_sx(g, 0) * face_sy(g, 0) * face_sz(g, 0);
     size_t n1 = (size_t)face_sx(g, 1) * face_sy(g, 1) * face_sz(g, 1);
     size_t n2 = (size_t)face_sx(g, 2) * face_sy(g, 2) * face_sz(g, 2);
-    k_update_velocity<0><<<nblk(n0), 256, 0, s>>>(g, phi, aidx, pressure, dt, U[0], V[0]);
-    k_update_velocity<1><<<nblk(n1), 256, 0, s>>>(g, phi, aidx, pressure, dt, U[1], V[1]);
-    k_update_velocity<2><<<nblk(n2), 256, 0, s>>>(g, phi, aidx, pressure, dt, U[2], V[2]);
+    { k_update_velocity<0><<<nblk(n0), 256, 0, s>>>(g, phi, aidx, pressure, dt, U[0], V[0]); bnn_note_launch(); }
+    { k_update_velocity<1><<<nblk(n1), 256, 0, s>>>(g, phi, aidx, pressure, dt, U[1], V[1]); bnn_note_launch(); }
+    { k_update_velocity<2><<<nblk(n2), 256, 0, s>>>(g, phi, aidx, pressure, dt, U[2], V[2]); bnn_note_launch(); }
 }
 void launch_g2p(int n, const GridDesc& g, float* p6, size_t stride, const float* const* U, const float* const* O,
                 float ratio, int kind, float* C9, cudaStream_t s) {
     if(n == 0) return;
-    k_g2p<<<nblk(n), 256, 0, s>>>(n, g, p6, p6 + 3 * stride, stride, U[0], U[1], U[2], O[0], O[1], O[2], ratio, kind,
-                                  C9);
+    { k_g2p<<<nblk(n), 256, 0, s>>>(n, g, p6, p6 + 3 * stride, stride, U[0], U[1], U[2], O[0], O[1], O[2], ratio, kind,
+                                  C9); bnn_note_launch(); }
 }
 void launch_aos_to_soa(int n, const float* pos, const float* vel, float* soa6, uint32_t* ids, size_t stride,
                        cudaStream_t s) {
     if(n == 0) return;
-    k_aos_to_soa<<<nblk(n), 256, 0, s>>>(n, pos, vel, soa6, ids, stride);
+    { k_aos_to_soa<<<nblk(n), 256, 0, s>>>(n, pos, vel, soa6, ids, stride); bnn_note_launch(); }
 }
 void launch_soa_to_aos(int n, const float* soa6, const uint32_t* ids, float* pos, float* vel, size_t stride,
                        cudaStream_t s) {
     if(n == 0) return;
-    k_soa_to_aos<<<nblk(n), 256, 0, s>>>(n, soa6, ids, pos, vel, stride);
+    { k_soa_to_aos<<<nblk(n), 256, 0, s>>>(n, soa6, ids, pos, vel, stride); bnn_note_launch(); }
 }
-void launch_add_scalar(float* a, size_t n, float v, cudaStream_t s) { k_add_scalar<<<nblk(n), 256, 0, s>>>(a, n, v); }
-void launch_step_reset(DevState* st, cudaStream_t s) { k_step_reset<<<1, 1, 0, s>>>(st); }
+void launch_add_scalar(float* a, size_t n, float v, cudaStream_t s) { { k_add_scalar<<<nblk(n), 256, 0, s>>>(a, n, v); bnn_note_launch(); } }
+void launch_step_reset(DevState* st, cudaStream_t s) { { k_step_reset<<<1, 1, 0, s>>>(st); bnn_note_launch(); } }
 void launch_cells_from_rows(size_t nc, const float* phi, const uint32_t* aidx, const float* pr, float* out, int active,
                             cudaStream_t s) {
-    k_cells_from_rows<<<nblk(nc), 256, 0, s>>>(nc, phi, aidx, pr, out, active);
+    { k_cells_from_rows<<<nblk(nc), 256, 0, s>>>(nc, phi, aidx, pr, out, active); bnn_note_launch(); }
 }
 
 } // namespace bnn

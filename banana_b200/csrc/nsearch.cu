@@ -250,8 +250,8 @@ int radix_sort(const K* keys, size_t n, K* keysOut, uint32_t* permOut, cudaStrea
     BNN_CUDA_CHECK(bits.alloc(2 * sizeof(unsigned long long)));
     unsigned long long init[2] = {0ull, ~0ull};
     BNN_CUDA_CHECK(cudaMemcpyAsync(bits.p, init, sizeof(init), cudaMemcpyHostToDevice, s));
-    k_key_bits<K><<<(unsigned)std::min<size_t>((n + 255) / 256, 4096), 256, 0, s>>>(keys, n, bits.as<unsigned long long>(),
-                                                                                   bits.as<unsigned long long>() + 1);
+    { k_key_bits<K><<<(unsigned)std::min<size_t>((n + 255) / 256, 4096), 256, 0, s>>>(keys, n, bits.as<unsigned long long>(),
+                                                                                   bits.as<unsigned long long>() + 1); bnn_note_launch(); }
     unsigned long long hb[2];
     BNN_CUDA_CHECK(cudaMemcpyAsync(hb, bits.p, sizeof(hb), cudaMemcpyDeviceToHost, s));
     BNN_CUDA_CHECK(cudaStreamSynchronize(s));
@@ -275,16 +275,16 @@ int radix_sort(const K* keys, size_t n, K* keysOut, uint32_t* permOut, cudaStrea
     const int np = (int)shifts.size();
     if(np == 0) {
         BNN_CUDA_CHECK(cudaMemcpyAsync(keysOut, keys, n * sizeof(K), cudaMemcpyDeviceToDevice, s));
-        k_iota<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(permOut, n);
+        { k_iota<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(permOut, n); bnn_note_launch(); }
         return BNN_OK;
     }
     for(int pi = 0; pi < np; ++pi) {
         const bool toOut = ((np - 1 - pi) % 2) == 0;
         K* kout = toOut ? keysOut : k2.as<K>();
         uint32_t* vout = toOut ? permOut : v2.as<uint32_t>();
-        k_radix_hist<K><<<ntiles, kRT, 0, s>>>(kin, n, shifts[pi], hist.as<uint32_t>(), ntiles);
+        { k_radix_hist<K><<<ntiles, kRT, 0, s>>>(kin, n, shifts[pi], hist.as<uint32_t>(), ntiles); bnn_note_launch(); }
         BNN_CUDA_CHECK(exclusive_scan_u32(hist.as<uint32_t>(), hist.as<uint32_t>(), (size_t)256 * ntiles, ws.p, s));
-        k_radix_scatter<K><<<ntiles, kRT, 0, s>>>(kin, vin, kout, vout, n, shifts[pi], hist.as<uint32_t>(), ntiles);
+        { k_radix_scatter<K><<<ntiles, kRT, 0, s>>>(kin, vin, kout, vout, n, shifts[pi], hist.as<uint32_t>(), ntiles); bnn_note_launch(); }
         BNN_CUDA_CHECK(cudaGetLastError());
         kin = kout;
         vin = vout;
@@ -309,8 +309,8 @@ extern "C" int bnn_cell_sort(const float* pos_dev, uint32_t n, const float bmin[
     BNN_CUDA_CHECK(oor.alloc(sizeof(unsigned)));
     BNN_CUDA_CHECK(cudaMemsetAsync(oor.p, 0, sizeof(unsigned), s));
     if(n) {
-        k_grid_cell_ids<<<(n + 255) / 256, 256, 0, s>>>(pos_dev, n, bmin[0], bmin[1], bmin[2], cell_size, ncells[0],
-                                                         ncells[1], ncells[2], cell_id_dev, oor.as<unsigned>());
+        { k_grid_cell_ids<<<(n + 255) / 256, 256, 0, s>>>(pos_dev, n, bmin[0], bmin[1], bmin[2], cell_size, ncells[0],
+                                                         ncells[1], ncells[2], cell_id_dev, oor.as<unsigned>()); bnn_note_launch(); }
         BNN_CUDA_CHECK(keysSorted.alloc((size_t)n * sizeof(uint32_t)));
         int rc = radix_sort<uint32_t>(cell_id_dev, n, keysSorted.as<uint32_t>(), sorted_idx_dev, s);
         if(rc != BNN_OK) return rc;
@@ -319,7 +319,7 @@ extern "C" int bnn_cell_sort(const float* pos_dev, uint32_t n, const float bmin[
         DevBuf cnt, ws;
         BNN_CUDA_CHECK(cnt.alloc(C * sizeof(uint32_t)));
         BNN_CUDA_CHECK(cudaMemsetAsync(cnt.p, 0, C * sizeof(uint32_t), s));
-        if(n) k_histogram<<<(n + 255) / 256, 256, 0, s>>>(cell_id_dev, n, cnt.as<uint32_t>());
+        if(n) { k_histogram<<<(n + 255) / 256, 256, 0, s>>>(cell_id_dev, n, cnt.as<uint32_t>()); bnn_note_launch(); }
         size_t wsb = scan_workspace_bytes(C);
         if(wsb) BNN_CUDA_CHECK(ws.alloc(wsb));
         BNN_CUDA_CHECK(exclusive_scan_u32(cnt.as<uint32_t>(), cell_start_dev, C, ws.p, s));
@@ -337,7 +337,7 @@ extern "C" int bnn_z_sort(const float* pos_dev, uint32_t n, float radius, uint64
     if(n == 0) return BNN_OK;
     cudaStream_t s = (cudaStream_t)stream;
     const float inv = (float)(1.0 / (double)radius);
-    k_zvalues<<<(n + 255) / 256, 256, 0, s>>>(pos_dev, n, inv, (unsigned long long*)zvalue_dev);
+    { k_zvalues<<<(n + 255) / 256, 256, 0, s>>>(pos_dev, n, inv, (unsigned long long*)zvalue_dev); bnn_note_launch(); }
     DevBuf sorted;
     BNN_CUDA_CHECK(sorted.alloc((size_t)n * sizeof(unsigned long long)));
     int rc = radix_sort<unsigned long long>((const unsigned long long*)zvalue_dev, n, sorted.as<unsigned long long>(),
@@ -363,7 +363,7 @@ extern "C" int bnn_neighbors(const float* pos_dev, uint32_t n, float radius, uin
     BNN_CUDA_CHECK(kmm.alloc(6 * sizeof(int)));
     int init[6] = {INT_MAX, INT_MAX, INT_MAX, INT_MIN, INT_MIN, INT_MIN};
     BNN_CUDA_CHECK(cudaMemcpyAsync(kmm.p, init, sizeof(init), cudaMemcpyHostToDevice, s));
-    k_ns_keys<<<(n + 255) / 256, 256, 0, s>>>(pos_dev, n, inv, keys3.as<int>(), kmm.as<int>(), kmm.as<int>() + 3);
+    { k_ns_keys<<<(n + 255) / 256, 256, 0, s>>>(pos_dev, n, inv, keys3.as<int>(), kmm.as<int>(), kmm.as<int>() + 3); bnn_note_launch(); }
     int hk[6];
     BNN_CUDA_CHECK(cudaMemcpyAsync(hk, kmm.p, sizeof(hk), cudaMemcpyDeviceToHost, s));
     BNN_CUDA_CHECK(cudaStreamSynchronize(s));
@@ -372,23 +372,23 @@ extern "C" int bnn_neighbors(const float* pos_dev, uint32_t n, float radius, uin
     const long long V = d0 * d1 * d2;
     if(V > (1ll << 30)) return BNN_ERR_NOT_SUPPORTED;
     BNN_CUDA_CHECK(cid.alloc((size_t)n * sizeof(uint32_t)));
-    k_dense_cell<<<(n + 255) / 256, 256, 0, s>>>(keys3.as<int>(), n, kmm.as<int>(), (int)d0, (int)d1, cid.as<uint32_t>());
+    { k_dense_cell<<<(n + 255) / 256, 256, 0, s>>>(keys3.as<int>(), n, kmm.as<int>(), (int)d0, (int)d1, cid.as<uint32_t>()); bnn_note_launch(); }
     BNN_CUDA_CHECK(cidSorted.alloc((size_t)n * sizeof(uint32_t)));
     BNN_CUDA_CHECK(order.alloc((size_t)n * sizeof(uint32_t)));
     int rc = radix_sort<uint32_t>(cid.as<uint32_t>(), n, cidSorted.as<uint32_t>(), order.as<uint32_t>(), s);
     if(rc != BNN_OK) return rc;
     BNN_CUDA_CHECK(sp.alloc((size_t)n * sizeof(float4)));
-    k_gather_pos<<<(n + 255) / 256, 256, 0, s>>>(pos_dev, order.as<uint32_t>(), n, sp.as<float4>());
+    { k_gather_pos<<<(n + 255) / 256, 256, 0, s>>>(pos_dev, order.as<uint32_t>(), n, sp.as<float4>()); bnn_note_launch(); }
     BNN_CUDA_CHECK(cnt.alloc((size_t)V * sizeof(uint32_t)));
     BNN_CUDA_CHECK(start.alloc(((size_t)V + 1) * sizeof(uint32_t)));
     BNN_CUDA_CHECK(cudaMemsetAsync(cnt.p, 0, (size_t)V * sizeof(uint32_t), s));
-    k_histogram<<<(n + 255) / 256, 256, 0, s>>>(cid.as<uint32_t>(), n, cnt.as<uint32_t>());
+    { k_histogram<<<(n + 255) / 256, 256, 0, s>>>(cid.as<uint32_t>(), n, cnt.as<uint32_t>()); bnn_note_launch(); }
     size_t wsb = scan_workspace_bytes((size_t)V);
     if(wsb) BNN_CUDA_CHECK(ws.alloc(wsb));
     BNN_CUDA_CHECK(exclusive_scan_u32(cnt.as<uint32_t>(), start.as<uint32_t>(), (size_t)V, ws.p, s));
     BNN_CUDA_CHECK(counts.alloc((size_t)n * sizeof(uint32_t)));
-    k_ns_query<false><<<(n + 255) / 256, 256, 0, s>>>(sp.as<float4>(), cidSorted.as<uint32_t>(), n, start.as<uint32_t>(),
-                                                       (int)d0, (int)d1, r2, counts.as<uint32_t>(), nullptr, nullptr);
+    { k_ns_query<false><<<(n + 255) / 256, 256, 0, s>>>(sp.as<float4>(), cidSorted.as<uint32_t>(), n, start.as<uint32_t>(),
+                                                       (int)d0, (int)d1, r2, counts.as<uint32_t>(), nullptr, nullptr); bnn_note_launch(); }
     size_t wsb64 = scan_workspace_bytes_u64(n);
     if(wsb64) BNN_CUDA_CHECK(ws64.alloc(wsb64));
     BNN_CUDA_CHECK(exclusive_scan_u32_to_u64(counts.as<uint32_t>(), (unsigned long long*)offsets_dev, n, ws64.p, s));
@@ -398,9 +398,9 @@ extern "C" int bnn_neighbors(const float* pos_dev, uint32_t n, float radius, uin
     if(total) *total = tot;
     if(tot > capacity) return BNN_ERR_CAPACITY;
     if(tot && !idx_dev) return BNN_ERR_INVALID_ARGUMENT;
-    k_ns_query<true><<<(n + 255) / 256, 256, 0, s>>>(sp.as<float4>(), cidSorted.as<uint32_t>(), n, start.as<uint32_t>(),
+    { k_ns_query<true><<<(n + 255) / 256, 256, 0, s>>>(sp.as<float4>(), cidSorted.as<uint32_t>(), n, start.as<uint32_t>(),
                                                       (int)d0, (int)d1, r2, nullptr,
-                                                      (const unsigned long long*)offsets_dev, idx_dev);
+                                                      (const unsigned long long*)offsets_dev, idx_dev); bnn_note_launch(); }
     BNN_CUDA_CHECK(cudaGetLastError());
     BNN_CUDA_CHECK(cudaStreamSynchronize(s));
     return BNN_OK;

@@ -16,6 +16,7 @@
 // the host can queue iterations in batches and only look at `done` between batches.
 #include "bnn_internal.cuh"
 
+#include <cstdio>
 #include <vector>
 
 namespace bnn {
@@ -60,167 +61,356 @@ template<class VT> __device__ __forceinline__ VT reduce_max_t(const VT* part, in
     return block_max_t(acc, sm);
 }
 
-// r = rhs, x = 0, z = D^-1 r, rho = z.r, resid = max|r|, tol = tolFactor * resid
+// ---------------------------------------------------------------------------------
+// Persistent PCG: one cooperative launch per solve.  Blocks own fixed 2048-row chunks
+// (c = blockIdx.x, +gridDim.x, ...), every phase writes one FP64 partial per chunk, and
+// after each grid barrier EVERY block reduces the partials in the canonical order, so all
+// blocks hold bit-identical scalars and take the same branch without a broadcast.  Data
+// written by other blocks is read with ld.global.cg (L2), never through a stale L1 line.
+// ---------------------------------------------------------------------------------
+constexpr unsigned kSpinLimit = 1u << 24;  // ~seconds of polling before a barrier gives up
+#ifndef BNN_BARRIER_SLEEP_NS
+#define BNN_BARRIER_SLEEP_NS 0
+#endif
+#ifndef BNN_PCG_UNROLL_A
+#define BNN_PCG_UNROLL_A 4
+#endif
+constexpr int kUnrollA = BNN_PCG_UNROLL_A;
+#ifndef BNN_PCG_ROW_GROUP
+#define BNN_PCG_ROW_GROUP 4
+#endif
+constexpr int kRowGroup = BNN_PCG_ROW_GROUP;  // rows whose loads are in flight together
+
+// Canonical 256-lane tree (lane t of the chunk owns v; levels 128, 64, 32 then a warp
+// shuffle tree), with one shared-memory staging step: warp 0 forms the three upper
+// levels in registers in the same association as the level-by-level tree.  The sum is
+// valid in thread 0.  `m` (optional) is max-reduced alongside.
 template<class VT>
-__global__ void __launch_bounds__(kLanes) k_pcg_init(int n, const float* __restrict__ rhsF, const VT* __restrict__ rhsV,
-                                                     VT* __restrict__ x, VT* __restrict__ r, VT* __restrict__ z,
-                                                     const VT* __restrict__ invd, double* __restrict__ part,
-                                                     VT* __restrict__ partMax, DevState* st, VT tolFactor,
-                                                     unsigned maxIter) {
-    __shared__ double smd[kLanes];
-    __shared__ VT smv[kLanes];
-    const size_t base = (size_t)blockIdx.x * kChunk + threadIdx.x;
+__device__ __forceinline__ void block_sum_max_256(double v, VT m, double* sm, VT* smm, double& sum, VT& mx,
+                                                  bool withMax) {
+    const int t = threadIdx.x;
+    sm[t] = v;
+    if(withMax) smm[t] = m;
+    __syncthreads();
+    if(t < 32) {
+        const double a0 = sm[t] + sm[t + 128];
+        const double a1 = sm[t + 64] + sm[t + 192];
+        const double a2 = sm[t + 32] + sm[t + 160];
+        const double a3 = sm[t + 96] + sm[t + 224];
+        double c = (a0 + a1) + (a2 + a3);
+#pragma unroll
+        for(int off = 16; off > 0; off >>= 1) c = c + __shfl_down_sync(0xffffffffu, c, off);
+        sum = c;
+        if(withMax) {
+            VT x = smm[t];
+#pragma unroll
+            for(int q = 1; q < 8; ++q) { const VT o = smm[t + 32 * q]; x = x > o ? x : o; }
+#pragma unroll
+            for(int off = 16; off > 0; off >>= 1) { const VT o = __shfl_down_sync(0xffffffffu, x, off); x = x > o ? x : o; }
+            mx = x;
+        }
+    }
+    __syncthreads();
+}
+
+// Reduce the chunk partials (sum in canonical order, and max) and give the result to
+// every thread of the block.
+template<class VT>
+__device__ __forceinline__ void reduce_partials_bcast(const double* part, const VT* pmax, int nch, double* sm, VT* smm,
+                                                      double& sum, VT& mx) {
     double acc = 0.0;
     VT m = VT(0);
-#pragma unroll
-    for(int j = 0; j < kPerLane; ++j) {
-        const size_t e = base + (size_t)j * kLanes;
-        if(e < (size_t)n) {
-            const VT rv = rhsV ? rhsV[e] : (VT)rhsF[e];
-            r[e] = rv;
-            x[e] = VT(0);
-            const VT a = vabs(rv);
-            m = m > a ? m : a;
-            const VT zv = invd[e] * rv;
-            z[e] = zv;
-            acc = acc + (double)zv * (double)rv;
-        }
+    for(int c = threadIdx.x; c < nch; c += kLanes) {
+        acc = acc + __ldcg(part + c);
+        if(pmax) { const VT o = __ldcg(pmax + c); m = m > o ? m : o; }
     }
-    const double bs = block_sum_256(acc, smd);
-    const VT bm = block_max_t(m, smv);
-    if(threadIdx.x == 0) { part[blockIdx.x] = bs; partMax[blockIdx.x] = bm; }
-    if(last_block(&st->counter0)) {
-        const int nch = gridDim.x;
-        const double rho = reduce_partials(part, nch, smd);
-        const VT resid = reduce_max_t(partMax, nch, smv);
-        if(threadIdx.x == 0) {
-            st->counter0 = 0;
-            st->iter = 0;
-            st->max_iter = maxIter;
-            st->done = 0;
-            st->success = 0;
-            Sc<VT>::set_resid(st, resid);
-            tolFactor = fmax(tolFactor, VT(1e-30));
-            if(resid < (VT)FLT_MIN) {
-                st->done = 1; st->success = 1;
-            } else {
-                Sc<VT>::set_tol(st, tolFactor * resid);
-                if(rho < (double)FLT_MIN || isnan(rho)) { st->done = 1; st->success = 0; }
-                st->rho = rho;
+    double s = 0.0;
+    VT x = VT(0);
+    block_sum_max_256<VT>(acc, m, sm, smm, s, x, pmax != nullptr);
+    if(threadIdx.x == 0) { sm[0] = s; smm[0] = x; }
+    __syncthreads();
+    sum = sm[0];
+    mx = smm[0];
+    __syncthreads();
+}
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ unsigned atom_add_release_u32(unsigned* p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
+// Grid-wide barrier with a bounded wait (sense reversal on one word): block 0 adds
+// 2^31 - (nblocks - 1), every other block adds 1, so the word's top bit flips exactly
+// when the last block arrives and its low bits return to where they were.  Arrival is a
+// release, the poll an acquire, so each block's writes before the barrier are visible to
+// every block after it.  Returns false (and sets the timeout flag) when the wait gave up.
+__device__ __forceinline__ bool grid_barrier(GridSync* gs, unsigned nblocks, unsigned& gen, unsigned* flags) {
+    __shared__ int sOk;
+    (void)gen;
+    __syncthreads();
+    if(threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned add = blockIdx.x == 0 ? 0x80000000u - (nblocks - 1u) : 1u;
+        const unsigned old = atom_add_release_u32(&gs->count, add);
+        unsigned spins = 0;
+        while(((ld_acquire_u32(&gs->count) ^ old) & 0x80000000u) == 0u) {
+            if(++spins > kSpinLimit) {
+                ok = 0;
+                atomicOr(flags, BNN_FLAG_TIMEOUT);
+                break;
             }
-            if(maxIter == 0 && !st->done) { st->done = 1; st->success = 0; }
+            if(BNN_BARRIER_SLEEP_NS) __nanosleep(BNN_BARRIER_SLEEP_NS);
         }
+        sOk = ok;
     }
+    __syncthreads();
+    return sOk != 0;
+}
+
+template<class VT> struct PcgArgs {
+    int n;
+    const float* rhsF;
+    const float* diag;
+    const VT* invd;
+    const int32_t* nbr;
+    VT negoff;
+    VT tolFactor;
+    unsigned maxIter;
+    VT *x, *r, *z, *s0, *s1, *q;
+    double *part0, *part1, *part2;
+    VT* partMax;
+    DevState* st;
+    GridSync* gs;
+};
+
+template<class VT>
+__device__ __forceinline__ VT s_val(const VT* z, const VT* sOld, VT beta, bool first, size_t e) {
+    return first ? __ldcg(z + e) : __ldcg(z + e) + beta * __ldcg(sOld + e);
 }
 
 template<class VT>
-__device__ __forceinline__ VT s_of(const VT* __restrict__ z, const VT* __restrict__ sOld, VT beta, bool first, int e) {
-    return first ? z[e] : z[e] + beta * sOld[e];
-}
-
-// s = z + beta*s_old; q = A s (column-ordered sum); partial s.q; last block: alpha
-template<class VT>
-__global__ void __launch_bounds__(kLanes) k_pcg_spmv(int n, const VT* __restrict__ z, const VT* __restrict__ sOld,
-                                                     VT* __restrict__ sNew, VT* __restrict__ q,
-                                                     const float* __restrict__ diag, const int32_t* __restrict__ nbr,
-                                                     VT negoff, double* __restrict__ part, DevState* st, int first) {
-    __shared__ double smd[kLanes];
-    if(*(volatile unsigned*)&st->done) return;
-    const VT beta = first ? VT(0) : Sc<VT>::beta(st);
-    const bool fst = first != 0;
-    const size_t base = (size_t)blockIdx.x * kChunk + threadIdx.x;
-    double acc = 0.0;
-#pragma unroll 2
-    for(int j = 0; j < kPerLane; ++j) {
-        const size_t e = base + (size_t)j * kLanes;
-        if(e < (size_t)n) {
-            const int32_t n0 = nbr[e], n1 = nbr[(size_t)n + e], n2 = nbr[2 * (size_t)n + e];
-            const int32_t n3 = nbr[3 * (size_t)n + e], n4 = nbr[4 * (size_t)n + e], n5 = nbr[5 * (size_t)n + e];
-            const float dg = diag[e];
-            const VT se = s_of(z, sOld, beta, fst, (int)e);
-            VT t = VT(0);
-            if(n0 >= 0) t += negoff * s_of(z, sOld, beta, fst, n0);
-            if(n1 >= 0) t += negoff * s_of(z, sOld, beta, fst, n1);
-            if(n2 >= 0) t += negoff * s_of(z, sOld, beta, fst, n2);
-            if(dg != 0.f) t += (VT)dg * se;
-            if(n3 >= 0) t += negoff * s_of(z, sOld, beta, fst, n3);
-            if(n4 >= 0) t += negoff * s_of(z, sOld, beta, fst, n4);
-            if(n5 >= 0) t += negoff * s_of(z, sOld, beta, fst, n5);
-            sNew[e] = se;
-            q[e] = t;
-            acc = acc + (double)se * (double)t;
-        }
-    }
-    const double bs = block_sum_256(acc, smd);
-    if(threadIdx.x == 0) part[blockIdx.x] = bs;
-    if(last_block(&st->counter1)) {
-        const double tmp = reduce_partials(part, gridDim.x, smd);
-        if(threadIdx.x == 0) {
-            st->counter1 = 0;
-            st->tmp = tmp;
-            if(tmp < (double)FLT_MIN) {
-                st->iter = st->iter + 1;
-                st->done = 1;
-                st->success = 1;
-            } else {
-                Sc<VT>::set_alpha(st, st->rho / tmp);
-            }
-        }
-    }
-}
-
-// x += alpha s; r -= alpha q; max|r|; z = D^-1 r; partial z.r; last block: test and beta
-template<class VT>
-__global__ void __launch_bounds__(kLanes) k_pcg_update(int n, VT* __restrict__ x, VT* __restrict__ r,
-                                                       VT* __restrict__ z, const VT* __restrict__ sNew,
-                                                       const VT* __restrict__ q, const VT* __restrict__ invd,
-                                                       double* __restrict__ part, VT* __restrict__ partMax,
-                                                       DevState* st) {
+__global__ void __launch_bounds__(kLanes) k_pcg_persistent(PcgArgs<VT> a) {
     __shared__ double smd[kLanes];
     __shared__ VT smv[kLanes];
-    if(*(volatile unsigned*)&st->done) return;
-    const VT alpha = Sc<VT>::alpha(st);
-    const size_t base = (size_t)blockIdx.x * kChunk + threadIdx.x;
-    double acc = 0.0;
-    VT m = VT(0);
+    const int n = a.n;
+    const int nch = (n + kChunk - 1) / kChunk;
+    const unsigned nb = gridDim.x;
+    unsigned gen = ld_acquire_u32(&a.gs->gen);
+    unsigned* flags = &a.st->flags;
+    VT* __restrict__ xR = a.x;
+    VT* __restrict__ rR = a.r;
+    VT* __restrict__ zR = a.z;
+    VT* __restrict__ qR = a.q;
+    const VT* __restrict__ invdR = a.invd;
+    const float* __restrict__ diagR = a.diag;
+    const int32_t* __restrict__ nbrR = a.nbr;
+    const VT negoff = a.negoff;
+
+    // ---- init: r = rhs, x = 0, z = D^-1 r; partial z.r and max|r| (PCGSolver.cpp:151-168)
+    for(int c = blockIdx.x; c < nch; c += nb) {
+        double acc = 0.0;
+        VT m = VT(0);
+        const size_t base = (size_t)c * kChunk + threadIdx.x;
 #pragma unroll
-    for(int j = 0; j < kPerLane; ++j) {
-        const size_t e = base + (size_t)j * kLanes;
-        if(e < (size_t)n) {
-            x[e] += alpha * sNew[e];
-            const VT rv = r[e] + (-alpha) * q[e];
-            r[e] = rv;
-            const VT a = vabs(rv);
-            m = m > a ? m : a;
-            const VT zv = invd[e] * rv;
-            z[e] = zv;
-            acc = acc + (double)zv * (double)rv;
+        for(int j = 0; j < kPerLane; ++j) {
+            const size_t e = base + (size_t)j * kLanes;
+            if(e < (size_t)n) {
+                const VT rv = (VT)a.rhsF[e];
+                a.r[e] = rv;
+                a.x[e] = VT(0);
+                const VT ab = vabs(rv);
+                m = m > ab ? m : ab;
+                const VT zv = __ldg(a.invd + e) * rv;
+                a.z[e] = zv;
+                acc = acc + (double)zv * (double)rv;
+            }
         }
+        double bs;
+        VT bm;
+        block_sum_max_256<VT>(acc, m, smd, smv, bs, bm, true);
+        if(threadIdx.x == 0) { a.part0[c] = bs; a.partMax[c] = bm; }
     }
-    const double bs = block_sum_256(acc, smd);
-    const VT bm = block_max_t(m, smv);
-    if(threadIdx.x == 0) { part[blockIdx.x] = bs; partMax[blockIdx.x] = bm; }
-    if(last_block(&st->counter2)) {
-        const int nch = gridDim.x;
-        const double rhoNew = reduce_partials(part, nch, smd);
-        const VT resid = reduce_max_t(partMax, nch, smv);
-        if(threadIdx.x == 0) {
-            st->counter2 = 0;
-            st->iter = st->iter + 1;
-            Sc<VT>::set_resid(st, resid);
-            if(resid < Sc<VT>::tol(st)) {
-                st->done = 1;
-                st->success = 1;
-            } else {
-                Sc<VT>::set_beta(st, rhoNew / st->rho);
-                st->rho = rhoNew;
-                if(st->iter >= st->max_iter) {
-                    st->done = 1;
-                    st->success = 0;
-                    atomicOr(&st->flags, BNN_FLAG_PCG_MAXITER);
+    if(!grid_barrier(a.gs, nb, gen, flags)) return;
+    double rho;
+    VT resid;
+    reduce_partials_bcast<VT>(a.part0, a.partMax, nch, smd, smv, rho, resid);
+    const VT tolFactor = fmax(a.tolFactor, VT(1e-30));
+    unsigned iter = 0, success = 0;
+    bool done = false;
+    VT tol = VT(0);
+    if(resid < (VT)FLT_MIN) {
+        done = true;
+        success = 1;
+    } else {
+        tol = tolFactor * resid;
+        if(rho < (double)FLT_MIN || isnan(rho)) done = true;
+    }
+    if(a.maxIter == 0) done = true;
+
+    VT beta = VT(0);
+    bool first = true;
+#ifdef BNN_PCG_TIMING
+    unsigned long long tc[6] = {0, 0, 0, 0, 0, 0};
+    long long t0_ = clock64();
+#define TMARK(k) do { long long t1_ = clock64(); tc[k] += (unsigned long long)(t1_ - t0_); t0_ = t1_; } while(0)
+#else
+#define TMARK(k) do {} while(0)
+#endif
+    VT* sOld = a.s1;
+    VT* sNew = a.s0;
+    while(!done) {
+        // ---- phase A: s = z + beta s_old, q = A s, partial s.q (PCGSolver.cpp:173-174,192-193)
+        // Every load of a chunk is issued before any store (missing neighbours read the
+        // row itself and are masked afterwards), so the chunk costs a few L2 round trips
+        // instead of one per row and neighbour.
+        for(int c = blockIdx.x; c < nch; c += nb) {
+            const size_t base = (size_t)c * kChunk + threadIdx.x;
+            VT sOut[kPerLane], qOut[kPerLane];
+#pragma unroll
+            for(int g0 = 0; g0 < kPerLane; g0 += kRowGroup) {
+                int32_t id[kRowGroup][7];
+                bool has[kRowGroup][7];
+                float dg[kRowGroup];
+#pragma unroll
+                for(int u = 0; u < kRowGroup; ++u) {
+                    const size_t e = base + (size_t)(g0 + u) * kLanes;
+                    const size_t ee = e < (size_t)n ? e : 0;
+#pragma unroll
+                    for(int q = 0; q < 6; ++q) {
+                        const int32_t v = __ldg(nbrR + (size_t)q * n + ee);
+                        const int slot = q < 3 ? q : q + 1;
+                        has[u][slot] = v >= 0;
+                        id[u][slot] = v >= 0 ? v : (int32_t)ee;
+                    }
+                    id[u][3] = (int32_t)ee;
+                    has[u][3] = true;
+                    dg[u] = __ldg(diagR + ee);
+                }
+                VT zv[kRowGroup][7], sv[kRowGroup][7];
+#pragma unroll
+                for(int u = 0; u < kRowGroup; ++u)
+#pragma unroll
+                    for(int q = 0; q < 7; ++q) {
+                        zv[u][q] = __ldcg(zR + id[u][q]);
+                        sv[u][q] = first ? VT(0) : __ldcg(sOld + id[u][q]);
+                    }
+#pragma unroll
+                for(int u = 0; u < kRowGroup; ++u) {
+                    VT s7[7];
+#pragma unroll
+                    for(int q = 0; q < 7; ++q) s7[q] = first ? zv[u][q] : zv[u][q] + beta * sv[u][q];
+                    VT t = VT(0);
+#pragma unroll
+                    for(int q = 0; q < 3; ++q) if(has[u][q]) t += negoff * s7[q];
+                    if(dg[u] != 0.f) t += (VT)dg[u] * s7[3];
+#pragma unroll
+                    for(int q = 4; q < 7; ++q) if(has[u][q]) t += negoff * s7[q];
+                    sOut[g0 + u] = s7[3];
+                    qOut[g0 + u] = t;
                 }
             }
+            double acc = 0.0;
+#pragma unroll
+            for(int j = 0; j < kPerLane; ++j) {
+                const size_t e = base + (size_t)j * kLanes;
+                if(e < (size_t)n) {
+                    sNew[e] = sOut[j];
+                    qR[e] = qOut[j];
+                    acc = acc + (double)sOut[j] * (double)qOut[j];
+                }
+            }
+            double bs;
+            VT unused;
+            block_sum_max_256<VT>(acc, VT(0), smd, smv, bs, unused, false);
+            if(threadIdx.x == 0) a.part1[c] = bs;
         }
+        TMARK(0);
+        if(!grid_barrier(a.gs, nb, gen, flags)) return;
+        TMARK(1);
+        double tmp;
+        VT unused2;
+        reduce_partials_bcast<VT>(a.part1, (const VT*)nullptr, nch, smd, smv, tmp, unused2);
+        if(tmp < (double)FLT_MIN) {
+            ++iter;
+            success = 1;
+            break;
+        }
+        const VT alpha = (VT)(rho / tmp);
+        TMARK(2);
+        // ---- phase B: x += alpha s, r -= alpha q, max|r|, z = D^-1 r, partial z.r
+        for(int c = blockIdx.x; c < nch; c += nb) {
+            const size_t base = (size_t)c * kChunk + threadIdx.x;
+            VT xs[kPerLane], ss[kPerLane], rs[kPerLane], qs[kPerLane], is[kPerLane];
+#pragma unroll
+            for(int j = 0; j < kPerLane; ++j) {
+                const size_t e = base + (size_t)j * kLanes;
+                const size_t ee = e < (size_t)n ? e : 0;
+                xs[j] = __ldcg(xR + ee);
+                ss[j] = __ldcg(sNew + ee);
+                rs[j] = __ldcg(rR + ee);
+                qs[j] = __ldcg(qR + ee);
+                is[j] = __ldg(invdR + ee);
+            }
+            double acc = 0.0;
+            VT m = VT(0);
+#pragma unroll
+            for(int j = 0; j < kPerLane; ++j) {
+                const size_t e = base + (size_t)j * kLanes;
+                if(e < (size_t)n) {
+                    xR[e] = xs[j] + alpha * ss[j];
+                    const VT rv = rs[j] + (-alpha) * qs[j];
+                    rR[e] = rv;
+                    const VT ab = vabs(rv);
+                    m = m > ab ? m : ab;
+                    const VT zv = is[j] * rv;
+                    zR[e] = zv;
+                    acc = acc + (double)zv * (double)rv;
+                }
+            }
+            double bs;
+            VT bm;
+            block_sum_max_256<VT>(acc, m, smd, smv, bs, bm, true);
+            if(threadIdx.x == 0) { a.part2[c] = bs; a.partMax[c] = bm; }
+        }
+        TMARK(3);
+        if(!grid_barrier(a.gs, nb, gen, flags)) return;
+        TMARK(4);
+        double rhoNew;
+        reduce_partials_bcast<VT>(a.part2, a.partMax, nch, smd, smv, rhoNew, resid);
+        TMARK(5);
+        ++iter;
+        if(resid < tol) {
+            success = 1;
+            break;
+        }
+        beta = (VT)(rhoNew / rho);
+        rho = rhoNew;
+        if(iter >= a.maxIter) {
+            if(blockIdx.x == 0 && threadIdx.x == 0) atomicOr(flags, BNN_FLAG_PCG_MAXITER);
+            break;
+        }
+        VT* t = sOld;
+        sOld = sNew;
+        sNew = t;
+        first = false;
+    }
+#ifdef BNN_PCG_TIMING
+    if(threadIdx.x == 0 && blockIdx.x < 2)
+        printf("blk %d iters %u  cycles/iter: phaseA %.0f bar1 %.0f red1 %.0f phaseB %.0f bar2 %.0f red2 %.0f\n", (int)blockIdx.x, iter,
+               tc[0] / (double)iter, tc[1] / (double)iter, tc[2] / (double)iter, tc[3] / (double)iter, tc[4] / (double)iter, tc[5] / (double)iter);
+#endif
+    if(blockIdx.x == 0 && threadIdx.x == 0) {
+        a.st->iter = iter;
+        a.st->success = success;
+        a.st->done = 1;
+        Sc<VT>::set_resid(a.st, resid);
     }
 }
 
@@ -316,6 +506,7 @@ int pcg_reserve(PcgWork& w, int n, bool fp64) {
         pcg_release(w);
         const int cap = (int)(n * 1.25) + 4096;
         const size_t nch = ((size_t)cap + kChunk - 1) / kChunk + 1;
+        w.nchCap = (int)nch;
         BNN_CUDA_CHECK(cudaMalloc(&w.x, cap * sizeof(float)));
         BNN_CUDA_CHECK(cudaMalloc(&w.r, cap * sizeof(float)));
         BNN_CUDA_CHECK(cudaMalloc(&w.z, cap * sizeof(float)));
@@ -324,7 +515,9 @@ int pcg_reserve(PcgWork& w, int n, bool fp64) {
         BNN_CUDA_CHECK(cudaMalloc(&w.q, cap * sizeof(float)));
         BNN_CUDA_CHECK(cudaMalloc(&w.d32, cap * sizeof(float)));
         BNN_CUDA_CHECK(cudaMalloc(&w.r32, cap * sizeof(float)));
-        BNN_CUDA_CHECK(cudaMalloc(&w.part, nch * sizeof(double)));
+        BNN_CUDA_CHECK(cudaMalloc(&w.part, 3 * nch * sizeof(double)));
+        BNN_CUDA_CHECK(cudaMalloc(&w.gs, sizeof(GridSync)));
+        BNN_CUDA_CHECK(cudaMemset(w.gs, 0, sizeof(GridSync)));
         BNN_CUDA_CHECK(cudaMalloc(&w.partMaxF, nch * sizeof(float)));
         BNN_CUDA_CHECK(cudaMalloc(&w.partMaxD, nch * sizeof(double)));
         w.cap = cap;
@@ -344,37 +537,46 @@ int pcg_reserve(PcgWork& w, int n, bool fp64) {
 void pcg_release(PcgWork& w) {
     for(void* p : {(void*)w.x, (void*)w.r, (void*)w.z, (void*)w.s0, (void*)w.s1, (void*)w.q, (void*)w.d32, (void*)w.r32,
                    (void*)w.part, (void*)w.partMaxF, (void*)w.partMaxD, (void*)w.x64, (void*)w.r64, (void*)w.z64,
-                   (void*)w.s064, (void*)w.s164, (void*)w.q64, (void*)w.inv64})
+                   (void*)w.s064, (void*)w.s164, (void*)w.q64, (void*)w.inv64, (void*)w.gs})
         if(p) cudaFree(p);
     w = PcgWork();
 }
 
-// Runs one PCG solve (VT vectors).  Iterations are queued in batches; between batches the
-// host reads `done` from pinned memory.  Returns BNN status; solution in x (VT).
+// Runs one PCG solve (VT vectors) as a single cooperative launch.  Returns BNN status;
+// the solution is left in x.
 template<class VT>
-static int pcg_solve_t(int n, const float* rhsF, const VT* rhsV, const float* diag, const VT* invd,
-                       const int32_t* nbr, VT negoff, VT tolFactor, unsigned maxIter, VT* x, VT* r, VT* z, VT* s0,
-                       VT* s1, VT* q, double* part, VT* partMax, DevState* dst, DevState* hst, cudaStream_t s,
-                       PcgOutcome& out) {
-    const unsigned nch = (unsigned)((n + kChunk - 1) / kChunk);
-    if(n == 0) { out = PcgOutcome(); out.success = 1; return BNN_OK; }
-    k_pcg_init<VT><<<nch, kLanes, 0, s>>>(n, rhsF, rhsV, x, r, z, invd, part, partMax, dst, tolFactor, maxIter);
-    BNN_CUDA_CHECK(cudaGetLastError());
-    unsigned it = 0;
-    unsigned batch = 4;
-    for(;;) {
-        for(unsigned b = 0; b < batch && it < maxIter; ++b, ++it) {
-            VT* sOld = (it % 2 == 0) ? s1 : s0;
-            VT* sNew = (it % 2 == 0) ? s0 : s1;
-            k_pcg_spmv<VT><<<nch, kLanes, 0, s>>>(n, z, sOld, sNew, q, diag, nbr, negoff, part, dst, it == 0 ? 1 : 0);
-            k_pcg_update<VT><<<nch, kLanes, 0, s>>>(n, x, r, z, sNew, q, invd, part, partMax, dst);
-        }
-        BNN_CUDA_CHECK(cudaGetLastError());
-        BNN_CUDA_CHECK(cudaMemcpyAsync(hst, dst, sizeof(DevState), cudaMemcpyDeviceToHost, s));
-        BNN_CUDA_CHECK(cudaStreamSynchronize(s));
-        if(hst->done || it >= maxIter) break;
-        if(batch < 32) batch *= 2;
+static int pcg_solve_t(PcgWork& w, int n, const float* rhsF, const float* diag, const VT* invd, const int32_t* nbr,
+                       VT negoff, VT tolFactor, unsigned maxIter, VT* x, VT* r, VT* z, VT* s0, VT* s1, VT* q,
+                       VT* partMax, DevState* dst, DevState* hst, cudaStream_t s, PcgOutcome& out) {
+    out = PcgOutcome();
+    if(n == 0) { out.success = 1; return BNN_OK; }
+    const int nch = (n + kChunk - 1) / kChunk;
+    static int numSM = 0, perSM[2] = {0, 0};
+    const int ti = sizeof(VT) == 8 ? 1 : 0;
+    if(!numSM) {
+        int dev = 0;
+        BNN_CUDA_CHECK(cudaGetDevice(&dev));
+        BNN_CUDA_CHECK(cudaDeviceGetAttribute(&numSM, cudaDevAttrMultiProcessorCount, dev));
     }
+    if(!perSM[ti]) {
+        BNN_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM[ti], k_pcg_persistent<VT>, kLanes, 0));
+        if(perSM[ti] < 1) { bnn_set_error("persistent PCG kernel cannot be resident"); return BNN_ERR_CUDA; }
+    }
+    const int cap = numSM * perSM[ti];
+    const int perBlock = (nch + cap - 1) / cap;           // chunks per block
+    const int grid = (nch + perBlock - 1) / perBlock;     // balanced: every block the same count
+    PcgArgs<VT> a;
+    a.n = n; a.rhsF = rhsF; a.diag = diag; a.invd = invd; a.nbr = nbr; a.negoff = negoff; a.tolFactor = tolFactor;
+    a.maxIter = maxIter; a.x = x; a.r = r; a.z = z; a.s0 = s0; a.s1 = s1; a.q = q;
+    a.part0 = w.part; a.part1 = w.part + w.nchCap; a.part2 = w.part + 2 * (size_t)w.nchCap; a.partMax = partMax;
+    a.st = dst; a.gs = w.gs;
+    BNN_CUDA_CHECK(cudaMemsetAsync(&w.gs->count, 0, sizeof(unsigned), s));
+    void* args[] = {&a};
+    BNN_CUDA_CHECK(cudaLaunchCooperativeKernel((const void*)k_pcg_persistent<VT>, dim3(grid), dim3(kLanes), args, 0, s));
+    bnn_note_launch();
+    BNN_CUDA_CHECK(cudaMemcpyAsync(hst, dst, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+    BNN_CUDA_CHECK(cudaStreamSynchronize(s));
+    if(hst->flags & BNN_FLAG_TIMEOUT) { bnn_set_error("PCG grid barrier timed out"); return BNN_ERR_TIMEOUT; }
     out.iterations = hst->iter;
     out.success = hst->success;
     out.residual = sizeof(VT) == 8 ? hst->resid64 : (double)hst->resid;
@@ -391,26 +593,26 @@ int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const floa
     const unsigned nch = (unsigned)((n + kChunk - 1) / kChunk);
     out = PcgOutcome();
     if(mode == BNN_PCG_FP32) {
-        rc = pcg_solve_t<float>(n, rhs, nullptr, diag, invd, nbr, -(1.0f * dt), tol, maxIter, w.x, w.r, w.z, w.s0,
-                                w.s1, w.q, w.part, w.partMaxF, dst, hst, s, out);
+        rc = pcg_solve_t<float>(w, n, rhs, diag, invd, nbr, -(1.0f * dt), tol, maxIter, w.x, w.r, w.z, w.s0, w.s1,
+                                w.q, w.partMaxF, dst, hst, s, out);
         if(rc != BNN_OK) return rc;
         if(n > 0) BNN_CUDA_CHECK(cudaMemcpyAsync(pressure, w.x, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
-        if(x64out && n > 0) k_f32_to_f64<<<nb, 256, 0, s>>>(n, w.x, x64out);
+        if(x64out && n > 0) { k_f32_to_f64<<<nb, 256, 0, s>>>(n, w.x, x64out); bnn_note_launch(); }
         return BNN_OK;
     }
     if(mode == BNN_PCG_FP64) {
-        if(n > 0) k_inv_diag64<<<nb, 256, 0, s>>>(n, diag, w.inv64);
-        rc = pcg_solve_t<double>(n, rhs, nullptr, diag, w.inv64, nbr, -(double)(1.0f * dt), (double)tol, maxIter,
-                                 w.x64, w.r64, w.z64, w.s064, w.s164, w.q64, w.part, w.partMaxD, dst, hst, s, out);
+        if(n > 0) { k_inv_diag64<<<nb, 256, 0, s>>>(n, diag, w.inv64); bnn_note_launch(); }
+        rc = pcg_solve_t<double>(w, n, rhs, diag, w.inv64, nbr, -(double)(1.0f * dt), (double)tol, maxIter, w.x64,
+                                 w.r64, w.z64, w.s064, w.s164, w.q64, w.partMaxD, dst, hst, s, out);
         if(rc != BNN_OK) return rc;
-        if(n > 0) k_d64_to_f32<<<nb, 256, 0, s>>>(n, w.x64, pressure);
+        if(n > 0) { k_d64_to_f32<<<nb, 256, 0, s>>>(n, w.x64, pressure); bnn_note_launch(); }
         if(x64out && n > 0)
             BNN_CUDA_CHECK(cudaMemcpyAsync(x64out, w.x64, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
         return BNN_OK;
     }
     // refined: FP64 outer residual and solution, FP32 inner solves
     if(n == 0) { out.success = 1; return BNN_OK; }
-    k_ir_init<<<nch, kLanes, 0, s>>>(n, rhs, w.x64, w.r64, w.partMaxD, dst);
+    { k_ir_init<<<nch, kLanes, 0, s>>>(n, rhs, w.x64, w.r64, w.partMaxD, dst); bnn_note_launch(); }
     BNN_CUDA_CHECK(cudaMemcpyAsync(hst, dst, sizeof(DevState), cudaMemcpyDeviceToHost, s));
     BNN_CUDA_CHECK(cudaStreamSynchronize(s));
     const double bmax = hst->outer_bmax;
@@ -420,14 +622,14 @@ int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const floa
     bool ok = bmax < (double)FLT_MIN;
     while(!ok && outer < maxOuter) {
         if(res < (double)outerTol * bmax) { ok = true; break; }
-        k_ir_to_f32<<<nb, 256, 0, s>>>(n, w.r64, w.r32);
+        { k_ir_to_f32<<<nb, 256, 0, s>>>(n, w.r64, w.r32); bnn_note_launch(); }
         PcgOutcome inner;
-        rc = pcg_solve_t<float>(n, w.r32, nullptr, diag, invd, nbr, -(1.0f * dt), innerTol, maxIter, w.d32, w.r, w.z,
-                                w.s0, w.s1, w.q, w.part, w.partMaxF, dst, hst, s, inner);
+        rc = pcg_solve_t<float>(w, n, w.r32, diag, invd, nbr, -(1.0f * dt), innerTol, maxIter, w.d32, w.r, w.z, w.s0,
+                                w.s1, w.q, w.partMaxF, dst, hst, s, inner);
         if(rc != BNN_OK) return rc;
         total += inner.iterations;
-        k_ir_accumulate<<<nb, 256, 0, s>>>(n, w.x64, w.d32);
-        k_ir_residual<<<nch, kLanes, 0, s>>>(n, rhs, w.x64, w.r64, diag, nbr, (double)(-(1.0f * dt)), w.partMaxD, dst);
+        { k_ir_accumulate<<<nb, 256, 0, s>>>(n, w.x64, w.d32); bnn_note_launch(); }
+        { k_ir_residual<<<nch, kLanes, 0, s>>>(n, rhs, w.x64, w.r64, diag, nbr, (double)(-(1.0f * dt)), w.partMaxD, dst); bnn_note_launch(); }
         BNN_CUDA_CHECK(cudaMemcpyAsync(hst, dst, sizeof(DevState), cudaMemcpyDeviceToHost, s));
         BNN_CUDA_CHECK(cudaStreamSynchronize(s));
         res = hst->outer_res;
@@ -439,7 +641,7 @@ int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const floa
     out.outer = outer;
     out.residual = res;
     out.success = ok ? 1 : 0;
-    k_d64_to_f32<<<nb, 256, 0, s>>>(n, w.x64, pressure);
+    { k_d64_to_f32<<<nb, 256, 0, s>>>(n, w.x64, pressure); bnn_note_launch(); }
     if(x64out) BNN_CUDA_CHECK(cudaMemcpyAsync(x64out, w.x64, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
     return BNN_OK;
 }

@@ -80,18 +80,18 @@ template<class TI, class TO> cudaError_t scan_impl(const TI* in, TO* out, size_t
     size_t nb = (n + kScanTile - 1) / kScanTile;
     if(n == 0) return cudaMemsetAsync(out, 0, sizeof(TO), s);
     if(nb == 1) {
-        k_scan_tile<TI, TO><<<1, kScanThreads, 0, s>>>(in, out, nullptr, n);
+        { k_scan_tile<TI, TO><<<1, kScanThreads, 0, s>>>(in, out, nullptr, n); bnn_note_launch(); }
         return cudaGetLastError();
     }
     TO* sums = (TO*)ws;
     TO* sumsScan = sums + (nb + 1);
     size_t here = ((nb + 1) * 2 * sizeof(TO) + 255) & ~size_t(255);
     void* rest = (char*)ws + here;
-    k_scan_tile<TI, TO><<<(unsigned)nb, kScanThreads, 0, s>>>(in, out, sums, n);
+    { k_scan_tile<TI, TO><<<(unsigned)nb, kScanThreads, 0, s>>>(in, out, sums, n); bnn_note_launch(); }
     cudaError_t e = scan_impl<TO, TO>(sums, sumsScan, nb, rest, s);
     if(e != cudaSuccess) return e;
-    k_scan_add<TO><<<(unsigned)nb, kScanThreads, 0, s>>>(out, sumsScan, n);
-    k_copy_total<TO><<<1, 1, 0, s>>>(out, n, sumsScan, nb);
+    { k_scan_add<TO><<<(unsigned)nb, kScanThreads, 0, s>>>(out, sumsScan, n); bnn_note_launch(); }
+    { k_copy_total<TO><<<1, 1, 0, s>>>(out, n, sumsScan, nb); bnn_note_launch(); }
     return cudaGetLastError();
 }
 } // namespace

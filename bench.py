@@ -1,0 +1,314 @@
+#!/usr/bin/env python
+"""Benchmark: particle-steps/s of the 3D FLIP dam break at 256^3 (12,734,496 particles,
+Jacobi PCG to 1e-6 max-norm relative residual), one sub-step per step.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One process per GPU (torchrun for N > 1).  Every rank advances its own replica of the
+scene (a single scene does not shard: its pressure solve needs a global reduction every
+PCG iteration), so per-GPU work is fixed and `scaling` is "weak".  The timed region is
+bracketed by a barrier and a device synchronize on both sides and timed with CUDA events
+on the stream the solver launches on; the job time is the max over ranks.
+
+`--impl reference` times the reference's CPU algorithm (the oracle port of PIC_Solver /
+FLIP_Solver / PCGSolver, reference arithmetic order, OpenMP over all host cores) on the
+same workload; under torchrun only rank 0 runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+import numpy as np  # noqa: E402
+
+N_GRID = 256
+METRIC = "particle-steps/s at 256^3 FLIP (1e-6 rel residual)"
+UNIT = "particle-steps/s"
+WORKLOAD = "flip_dam_break_256"
+
+
+def _config(pcg_mode: str):
+    return {"workload": WORKLOAD, "grid": f"{N_GRID}^3 (+2 padding cells per side = {N_GRID + 4}^3 stored)",
+            "particles": None, "block": [0.4, 0.6, 0.4], "particles_per_cell": 8, "seed": 42,
+            "solver": "FLIP", "pic_flip_ratio": 0.97, "cfl": 1.0, "pcg": f"Jacobi, {pcg_mode}, tol 1e-6 max-norm rel",
+            "step": "one advanceFrame sub-step", "l2_policy": "inputs larger than L2 (particles 306 MB, faces 212 MB)",
+            "parallelism": "replicas"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region"""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in Path(self.f.name).read_text().strip().splitlines() if r.strip()]
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except Exception:
+                continue
+            for k, name in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_port_steps(n_grid: int, steps: int, skip: int, threads: int):
+    """Oracle port (reference order, OpenMP) on the same scene: time `steps` sub-steps after
+    `skip` untimed ones.  Returns (particle-steps/s, particles, seconds)."""
+    from banana_b200 import scenes
+    from oracle import oracle as O
+    O.set_threads(threads)
+    pos, vel = scenes.dam_break(n_grid)
+    cfg = scenes.dam_break_params(n_grid, reduce_mode=0, nthreads=threads, sort_each_step=0)
+    o = O.Oracle(cfg)
+    o.set_particles(pos, vel)
+    for _ in range(skip):
+        o.step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.step()
+    dt = time.perf_counter() - t0
+    o.close()
+    return len(pos) * steps / dt, len(pos), dt
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    # full-size sub-steps of the same scene; when one step is slow the timed count shrinks
+    # so the whole run stays within a few minutes (the line reports what was timed)
+    from banana_b200 import scenes
+    from oracle import oracle as O
+    O.set_threads(threads)
+    pos, vel = scenes.dam_break(N_GRID)
+    cfg = scenes.dam_break_params(N_GRID, reduce_mode=0, nthreads=threads, sort_each_step=0)
+    o = O.Oracle(cfg)
+    o.set_particles(pos, vel)
+    t_w = time.perf_counter()
+    w_done = 0
+    for _ in range(args.warmup):
+        o.step()
+        w_done += 1
+        if time.perf_counter() - t_w > 60:
+            break
+    per = (time.perf_counter() - t_w) / max(w_done, 1)
+    steps = args.steps
+    if per * steps > 150:
+        steps = max(1, int(150 / max(per, 1e-9)))
+    t0 = time.perf_counter()
+    iters = []
+    for _ in range(steps):
+        st = o.step()
+        iters.append(st["pcg_iterations"])
+    dt = time.perf_counter() - t0
+    o.close()
+    value = len(pos) * steps / dt
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": steps, "warmup": w_done,
+            "ms_per_step": dt * 1e3 / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded dam break, seed 42)", "impl": "reference",
+            "config": dict(_config("reference order FP32"), particles=len(pos)),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{steps} full sub-steps of the 256^3 scene after {w_done} untimed "
+                                       f"(oracle port of the reference CPU solver, OpenMP, {threads} threads)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "pcg_iterations_mean": float(np.mean(iters))}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    import torch.distributed as dist
+
+    from banana_b200 import FlipSolver, capi, scenes
+
+    torch.cuda.set_device(local)
+    if ws > 1:
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local),
+                                timeout=__import__("datetime").timedelta(seconds=120))
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+
+    pcg_mode = args.pcg_mode
+    cfg = scenes.dam_break_params(N_GRID, pcg_mode={"fp32": 0, "fp64": 1, "refined": 2}[pcg_mode])
+    pos, vel = scenes.dam_break(N_GRID)
+    npart = len(pos)
+    solver = FlipSolver(cfg)
+    solver.set_particles(pos, vel)
+    stream = torch.cuda.ExternalStream(solver.stream_ptr())
+    for _ in range(args.warmup):
+        solver.step()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = capi.launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    stats = []
+    for _ in range(args.steps):
+        stats.append(solver.step())
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    launches = capi.launch_count() - launches0
+    ms = ev0.elapsed_time(ev1)
+    t_max = ms
+    if ws > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    value = npart * ws * args.steps / (t_max * 1e-3)
+
+    # stage breakdown and roofline of the PCG iteration (spmv + update kernels)
+    stage_tot = {k: sum(s["stage_ms"][k] for s in stats) for k in capi.STAGES}
+    iters = sum(s["pcg_iterations"] for s in stats)
+    rows = [s["n_active"] for s in stats]
+    pcg_bytes = sum(76.0 * s["n_active"] * s["pcg_iterations"] for s in stats)
+    peak, peak_kind = _peaks()
+    pcg_ms = stage_tot["pcg"]
+    achieved = pcg_bytes / (pcg_ms * 1e-3) / 1e9 if pcg_ms > 0 else 0.0
+    F = 3 * (N_GRID + 5) * (N_GRID + 4) ** 2
+    C = (N_GRID + 4) ** 3
+    stage_bytes = {"move": 36.0 * npart + 0.0, "sort": 80.0 * npart + 16.0 * C, "p2g": 28.0 * npart + 5.0 * F,
+                   "extrapolate": 4 * 10.0 * F + 4.0 * F, "fluid_sdf": 24.0 * npart + 4.0 * C + 8.0 * C,
+                   "g2p": 36.0 * npart + 8.0 * F}
+    stage_gbs = {k: (stage_bytes[k] * args.steps / (stage_tot[k] * 1e-3) / 1e9 if stage_tot[k] > 0 else None)
+                 for k in stage_bytes}
+
+    # end to end: host arrays in pinned memory, H2D + step + D2H per step
+    e2e = None
+    if not args.skip_e2e:
+        hp = torch.empty((npart, 3), dtype=torch.float32, pin_memory=True)
+        hv = torch.empty((npart, 3), dtype=torch.float32, pin_memory=True)
+        p_np, v_np = solver.get_particles()
+        hp.numpy()[:] = p_np
+        hv.numpy()[:] = v_np
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            solver.step_host_ptr(hp.data_ptr(), hv.data_ptr())
+        torch.cuda.synchronize()
+        te = time.perf_counter() - t0
+        if ws > 1:
+            t = torch.tensor([te], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            te = float(t.item())
+        e2e = {"value": npart * ws * args.steps / te, "unit": UNIT, "h2d_bytes_per_step": 24 * npart,
+               "d2h_bytes_per_step": 24 * npart,
+               "api": "bnn_flip_step_host (pinned host AoS positions/velocities in and out every step), wall clock"}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, n, sec = cpu_port_steps(N_GRID, steps=2, skip=1, threads=threads)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"sub-steps 2-3 of the same 256^3 scene ({n} particles), oracle port of the reference CPU "
+                         f"solver in reference arithmetic order, OpenMP {threads} threads, {sec:.1f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded dam break, seed 42)",
+            "config": dict(_config(pcg_mode), particles=npart),
+            "roofline": {"bound": "hbm", "kernel": "PCG iteration (k_pcg_spmv + k_pcg_update)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "algorithmic_bytes": "76 B per active row per iteration", "traffic": None},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+            "clocks": clk,
+            "detail": {"pcg_iterations_per_step": iters / args.steps, "active_rows_mean": float(np.mean(rows)),
+                       "stage_ms_per_step": {k: v / args.steps for k, v in stage_tot.items()},
+                       "stage_gbs": stage_gbs},
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if ws > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    global N_GRID
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--pcg-mode", choices=["fp32", "fp64", "refined"], default="fp32")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--grid", type=int, default=N_GRID, help="fluid-domain resolution (profiling of smaller cases)")
+    args = ap.parse_args()
+    ws, rank, local = _dist()
+    N_GRID = args.grid
+    if args.impl == "reference":
+        return run_reference(args, ws, rank)
+    return run_ours(args, ws, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -131,6 +131,8 @@ int bnn_flip_advance_frame(bnn_flip* h, uint32_t* substeps);
 /* Device pointers of the particle arrays (SoA x,y,z,vx,vy,vz, current sorted order),
  * valid until the next step; lets a caller keep data on the device. */
 int bnn_flip_device_particles(bnn_flip* h, float** xyz_vxyz_dev, uint32_t** ids_dev);
+/* The cudaStream_t every kernel of this handle is launched on (for events / ordering). */
+int bnn_flip_stream(bnn_flip* h, void** stream);
 /* Same sub-step as bnn_flip_step, but the particles come from pinned host AoS arrays and
  * are written back to them: upload, step, download in one stream (end-to-end timing). */
 int bnn_flip_step_host(bnn_flip* h, float* pos, float* vel, bnn_step_stats* stats);
@@ -172,9 +174,11 @@ typedef struct bnn_pcg_stats {
 int bnn_pcg_solve_7pt(uint32_t n, const float* diag, const int32_t* nbr, float offdiag, const float* rhs, float tol,
                       uint32_t max_iter, int32_t mode, float inner_tol, double* x_out, bnn_pcg_stats* stats);
 
-/* Library version / last CUDA error text for diagnostics */
+/* Library version / last CUDA error text / number of kernels this library has launched
+ * in this process (diagnostics; no counterpart in the reference). */
 const char* bnn_version(void);
 const char* bnn_last_error(void);
+uint64_t bnn_launch_count(void);
 
 #ifdef __cplusplus
 }
