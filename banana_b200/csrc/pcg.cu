@@ -72,12 +72,8 @@ constexpr unsigned kSpinLimit = 1u << 24;  // ~seconds of polling before a barri
 #ifndef BNN_BARRIER_SLEEP_NS
 #define BNN_BARRIER_SLEEP_NS 0
 #endif
-#ifndef BNN_PCG_UNROLL_A
-#define BNN_PCG_UNROLL_A 4
-#endif
-constexpr int kUnrollA = BNN_PCG_UNROLL_A;
 #ifndef BNN_PCG_ROW_GROUP
-#define BNN_PCG_ROW_GROUP 4
+#define BNN_PCG_ROW_GROUP 2
 #endif
 constexpr int kRowGroup = BNN_PCG_ROW_GROUP;  // rows whose loads are in flight together
 
@@ -195,8 +191,11 @@ __device__ __forceinline__ VT s_val(const VT* z, const VT* sOld, VT beta, bool f
     return first ? __ldcg(z + e) : __ldcg(z + e) + beta * __ldcg(sOld + e);
 }
 
+#ifndef BNN_PCG_MIN_BLOCKS
+#define BNN_PCG_MIN_BLOCKS 4
+#endif
 template<class VT>
-__global__ void __launch_bounds__(kLanes) k_pcg_persistent(PcgArgs<VT> a) {
+__global__ void __launch_bounds__(kLanes, BNN_PCG_MIN_BLOCKS) k_pcg_persistent(PcgArgs<VT> a) {
     __shared__ double smd[kLanes];
     __shared__ VT smv[kLanes];
     const int n = a.n;
