@@ -25,7 +25,7 @@ FIELD = {"u": 0, "v": 1, "w": 2, "phi": 3, "pressure": 4, "old_u": 5, "old_v": 6
 EXPORTS = [
     "bnn_flip_create", "bnn_flip_destroy", "bnn_flip_grid_dims", "bnn_flip_set_particles", "bnn_flip_get_particles",
     "bnn_flip_num_particles", "bnn_flip_get_grid", "bnn_flip_step", "bnn_flip_advance_frame",
-    "bnn_flip_device_particles", "bnn_flip_step_host", "bnn_flip_stream", "bnn_cell_sort", "bnn_z_sort", "bnn_neighbors",
+    "bnn_flip_device_particles", "bnn_flip_step_host", "bnn_flip_stream", "bnn_cell_sort", "bnn_cell_sort_noalloc", "bnn_z_sort", "bnn_neighbors",
     "bnn_pcg_solve_7pt", "bnn_version", "bnn_last_error", "bnn_launch_count",
 ]
 
@@ -94,6 +94,7 @@ def load() -> C.CDLL:
     L.bnn_flip_step_host.argtypes = [vp, fp, fp, C.POINTER(StepStats)]
     L.bnn_flip_stream.argtypes = [vp, C.POINTER(vp)]
     L.bnn_cell_sort.argtypes = [vp, C.c_uint32, fp, C.c_float, i32p, vp, vp, vp, u32p, vp]
+    L.bnn_cell_sort_noalloc.argtypes = [vp, C.c_uint32, fp, C.c_float, i32p, vp, vp, vp, u32p, vp]
     L.bnn_z_sort.argtypes = [vp, C.c_uint32, C.c_float, vp, vp, vp]
     L.bnn_neighbors.argtypes = [vp, C.c_uint32, C.c_float, vp, vp, C.c_uint64, u64p, vp]
     L.bnn_pcg_solve_7pt.argtypes = [C.c_uint32, fp, i32p, C.c_float, fp, C.c_float, C.c_uint32, C.c_int32, C.c_float,

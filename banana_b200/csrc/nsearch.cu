@@ -8,6 +8,7 @@
 // reference's one-thread bucket fill produces.
 #include "bnn_internal.cuh"
 
+#include <mutex>
 #include <vector>
 
 namespace bnn {
@@ -403,5 +404,125 @@ extern "C" int bnn_neighbors(const float* pos_dev, uint32_t n, float radius, uin
                                                       (const unsigned long long*)offsets_dev, idx_dev); bnn_note_launch(); }
     BNN_CUDA_CHECK(cudaGetLastError());
     BNN_CUDA_CHECK(cudaStreamSynchronize(s));
+    return BNN_OK;
+}
+
+// ---------------------------------------------------------------------------------
+// Cell sort without any device allocation.
+//
+// Some callers cannot allocate device memory at the moment they need a sort: code that
+// runs while a CUDA graph is being captured (cudaMalloc is not capturable), code inside
+// a host callback or a custom allocator's hook, or an embedding application that
+// pre-reserves all device memory and forbids further allocation.  For them this entry
+// point works entirely in a fixed scratch array compiled into the library: every GPU
+// that loads the library holds kNoAllocScratchBytes (about 21 MiB) until the process
+// exits.  Limits: at most kNoAllocMaxPoints points and kNoAllocMaxCells grid cells.
+// ---------------------------------------------------------------------------------
+namespace {
+constexpr uint32_t kNoAllocMaxPoints = 1u << 20;  // 1,048,576 points
+constexpr uint32_t kNoAllocMaxCells = 1u << 21;   // 2,097,152 cells (e.g. 128^3)
+constexpr uint32_t kNoAllocTiles = (kNoAllocMaxPoints + kRTile - 1) / kRTile;
+constexpr size_t kAlign = 256;
+constexpr size_t alignUp(size_t b) { return (b + kAlign - 1) / kAlign * kAlign; }
+constexpr size_t kOffCounter = 0;                                                     // out-of-range count
+constexpr size_t kOffKeys0 = alignUp(kOffCounter + 16);                               // sorted keys
+constexpr size_t kOffKeys1 = alignUp(kOffKeys0 + sizeof(uint32_t) * kNoAllocMaxPoints);  // ping-pong keys
+constexpr size_t kOffVals1 = alignUp(kOffKeys1 + sizeof(uint32_t) * kNoAllocMaxPoints);  // ping-pong payload
+constexpr size_t kOffHist = alignUp(kOffVals1 + sizeof(uint32_t) * kNoAllocMaxPoints);   // radix histogram (+1)
+constexpr size_t kOffCells = alignUp(kOffHist + sizeof(uint32_t) * (256u * kNoAllocTiles + 1));  // cell counts
+constexpr size_t kOffScanWs = alignUp(kOffCells + sizeof(uint32_t) * kNoAllocMaxCells);  // scan workspace
+constexpr size_t kScanWsBytes = 64u * 1024u;  // >= scan_workspace_bytes of either scan, checked at run time
+constexpr size_t kNoAllocScratchBytes = alignUp(kOffScanWs + kScanWsBytes);
+} // namespace
+
+static __device__ __align__(256) unsigned char g_cellSortScratch[kNoAllocScratchBytes];
+
+namespace {
+std::mutex g_noallocMutex;
+void* g_noallocPtr[64] = {};  // device address of g_cellSortScratch, per device ordinal
+
+// First call on a device: resolve the scratch array's device address with that device
+// current.  The host-side symbol is only a stand-in and must never reach a kernel.
+int noalloc_scratch(unsigned char** out) {
+    int dev = 0;
+    BNN_CUDA_CHECK(cudaGetDevice(&dev));
+    if(dev < 0 || dev >= 64) return BNN_ERR_NOT_SUPPORTED;
+    std::lock_guard<std::mutex> lock(g_noallocMutex);
+    if(!g_noallocPtr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_cellSortScratch);
+        if(e != cudaSuccess || !p) {
+            bnn_set_error(e != cudaSuccess ? cudaGetErrorString(e) : "scratch symbol has no device address");
+            return BNN_ERR_CUDA;
+        }
+        g_noallocPtr[dev] = p;
+    }
+    *out = (unsigned char*)g_noallocPtr[dev];
+    return BNN_OK;
+}
+} // namespace
+
+extern "C" int bnn_cell_sort_noalloc(const float* pos_dev, uint32_t n, const float bmin[3], float cell_size,
+                                     const int32_t ncells[3], uint32_t* cell_id_dev, uint32_t* sorted_idx_dev,
+                                     uint32_t* cell_start_dev, uint32_t* out_of_range, void* stream) {
+    if((n && (!pos_dev || !cell_id_dev || !sorted_idx_dev)) || !bmin || !ncells || !(cell_size > 0.f))
+        return BNN_ERR_INVALID_ARGUMENT;
+    for(int d = 0; d < 3; ++d) if(ncells[d] <= 0) return BNN_ERR_INVALID_ARGUMENT;
+    const size_t C = (size_t)ncells[0] * ncells[1] * ncells[2];
+    if(n > kNoAllocMaxPoints || C > kNoAllocMaxCells) {
+        bnn_set_error("bnn_cell_sort_noalloc: more than 1,048,576 points or 2,097,152 cells does not fit the "
+                      "fixed scratch array; use bnn_cell_sort");
+        return BNN_ERR_CAPACITY;
+    }
+    if(scan_workspace_bytes((size_t)256 * kNoAllocTiles) > kScanWsBytes || scan_workspace_bytes(C) > kScanWsBytes)
+        return BNN_ERR_CAPACITY;
+    unsigned char* scratch = nullptr;
+    int rc = noalloc_scratch(&scratch);
+    if(rc != BNN_OK) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned* oor = (unsigned*)(scratch + kOffCounter);
+    uint32_t* keys0 = (uint32_t*)(scratch + kOffKeys0);
+    uint32_t* keys1 = (uint32_t*)(scratch + kOffKeys1);
+    uint32_t* vals1 = (uint32_t*)(scratch + kOffVals1);
+    uint32_t* hist = (uint32_t*)(scratch + kOffHist);
+    uint32_t* cells = (uint32_t*)(scratch + kOffCells);
+    void* scanWs = scratch + kOffScanWs;
+    // the array keeps the previous call's contents: zero what is accumulated into
+    BNN_CUDA_CHECK(cudaMemsetAsync(oor, 0, sizeof(unsigned), s));
+    if(n) {
+        { k_grid_cell_ids<<<(n + 255) / 256, 256, 0, s>>>(pos_dev, n, bmin[0], bmin[1], bmin[2], cell_size, ncells[0],
+                                                         ncells[1], ncells[2], cell_id_dev, oor); bnn_note_launch(); }
+        // stable LSD radix sort over the bits a cell id < C can have; ping-pong so the
+        // last pass writes the caller's sorted_idx_dev
+        int bits = 0;
+        while(bits < 32 && ((size_t)1 << bits) < C) ++bits;
+        const int passes = (bits + 7) / 8;
+        const unsigned ntiles = (unsigned)((n + kRTile - 1) / kRTile);
+        if(passes == 0) {
+            { k_iota<<<(n + 255) / 256, 256, 0, s>>>(sorted_idx_dev, n); bnn_note_launch(); }
+        }
+        const uint32_t* kin = cell_id_dev;
+        const uint32_t* vin = nullptr;
+        for(int pi = 0; pi < passes; ++pi) {
+            const bool toOut = ((passes - 1 - pi) % 2) == 0;
+            uint32_t* kout = toOut ? keys0 : keys1;
+            uint32_t* vout = toOut ? sorted_idx_dev : vals1;
+            { k_radix_hist<uint32_t><<<ntiles, kRT, 0, s>>>(kin, n, 8 * pi, hist, ntiles); bnn_note_launch(); }
+            BNN_CUDA_CHECK(exclusive_scan_u32(hist, hist, (size_t)256 * ntiles, scanWs, s));
+            { k_radix_scatter<uint32_t><<<ntiles, kRT, 0, s>>>(kin, vin, kout, vout, n, 8 * pi, hist, ntiles); bnn_note_launch(); }
+            kin = kout;
+            vin = vout;
+        }
+    }
+    if(cell_start_dev) {
+        BNN_CUDA_CHECK(cudaMemsetAsync(cells, 0, C * sizeof(uint32_t), s));
+        if(n) { k_histogram<<<(n + 255) / 256, 256, 0, s>>>(cell_id_dev, n, cells); bnn_note_launch(); }
+        BNN_CUDA_CHECK(exclusive_scan_u32(cells, cell_start_dev, C, scanWs, s));
+    }
+    BNN_CUDA_CHECK(cudaGetLastError());
+    unsigned h = 0;
+    BNN_CUDA_CHECK(cudaMemcpyAsync(&h, oor, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    BNN_CUDA_CHECK(cudaStreamSynchronize(s));
+    if(out_of_range) *out_of_range = h;
     return BNN_OK;
 }
