@@ -66,7 +66,10 @@ def dam_break(n: int, block=(0.4, 0.6, 0.4), ppc: int = 8, seed: int = 42, domai
     for a, c in enumerate((ci, cj, ck)):
         u = uniform01(seed, a, lin)
         cc = np.repeat(c, ppc).astype(np.float64)
-        pos[:, a] = ((cc + u) * dx).astype(np.float32)
+        p = ((cc + u) * dx).astype(np.float32)
+        # rounding to float32 may land a sample on the next cell's face: keep it inside
+        hi = ((cc + 1.0) * dx).astype(np.float32)
+        pos[:, a] = np.where(p >= hi, np.nextafter(hi, np.float32(0)), p)
     vel = np.zeros_like(pos)
     return pos, vel
 

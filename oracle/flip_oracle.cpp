@@ -1374,3 +1374,14 @@ void orc_grid_ncells(const float* bmin, const float* bmax, float cellSize, int32
 }
 
 } // extern "C"
+
+extern "C" {
+// ArrayHelpers::interpolateValueLinear of face component d at grid coordinates g (for the
+// analytic interpolation checks)
+double orc_interp_face(void* hp, int d, double gx, double gy, double gz) {
+    auto* h = (orc_handle*)hp;
+    if(h->dbl) { double g[3] = {gx, gy, gz}; return h->d->velFromGrid(g, d, h->d->u); }
+    float g[3] = {(float)gx, (float)gy, (float)gz};
+    return (double)h->f->velFromGrid(g, d, h->f->u);
+}
+} // extern "C"

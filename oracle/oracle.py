@@ -93,6 +93,8 @@ def lib() -> C.CDLL:
         L.orc_grid_neighbor_list.argtypes = [fp, C.c_uint32, fp, C.c_float, i32p, fp, C.c_float, C.c_int, u32p]
         L.orc_grid_neighbor_list.restype = C.c_uint32
         L.orc_grid_ncells.argtypes = [fp, fp, C.c_float, i32p]; L.orc_grid_ncells.restype = None
+        L.orc_interp_face.argtypes = [vp, C.c_int, C.c_double, C.c_double, C.c_double]
+        L.orc_interp_face.restype = C.c_double
         _lib = L
     return _lib
 
@@ -200,6 +202,10 @@ class Oracle:
     def set_grid(self, which: int, arr: np.ndarray):
         a = np.ascontiguousarray(arr, np.float32).ravel()
         self.L.orc_set_grid(self.h, which, _p(a, C.c_float))
+
+    def interp_face(self, d: int, gx: float, gy: float, gz: float) -> float:
+        """velocity component d sampled at grid coordinates (PIC_Solver::getVelocityFromGrid)"""
+        return self.L.orc_interp_face(self.h, d, gx, gy, gz)
 
     def step(self) -> dict:
         st = OrcStepStats()

@@ -1,0 +1,79 @@
+"""The C ABI without a GPU: the library loads, exports every function include/banana_b200.h
+declares, its struct layouts match the ctypes binding, and argument validation (the
+reference's __BNN_REQUIRE checks, Macros.h:225-233) returns status codes before any CUDA
+call."""
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import pytest
+
+from banana_b200 import build as bld
+from banana_b200 import capi
+
+ROOT = Path(__file__).resolve().parent.parent
+HEADER = ROOT / "include" / "banana_b200.h"
+
+
+@pytest.fixture(scope="module")
+def lib():
+    if not bld.LIB.exists():
+        bld.build_cuda()
+    return capi.load()
+
+
+def _declared():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(bnn_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_every_declared_symbol_is_exported(lib):
+    names = _declared()
+    assert len(names) >= 15
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(names) == set(capi.EXPORTS)
+
+
+def test_struct_layouts_match_binding(tmp_path):
+    src = tmp_path / "layout.c"
+    fields = {"bnn_params": capi.Params, "bnn_step_stats": capi.StepStats, "bnn_pcg_stats": capi.PcgStats}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "banana_b200.h"', "int main(void) {"]
+    for cname, py in fields.items():
+        lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'printf("{cname}.{f} %zu\\n", offsetof({cname}, {f}));')
+    lines.append("return 0; }")
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    out = dict(l.split() for l in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n") if l)
+    for cname, py in fields.items():
+        assert int(out[cname]) == C.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert int(out[f"{cname}.{f}"]) == getattr(py, f).offset, (cname, f)
+
+
+def test_validation_needs_no_gpu(lib):
+    assert lib.bnn_version().decode().startswith("banana_b200")
+    h = C.c_void_p()
+    p = capi.make_params({"cell_size": 0.0})
+    assert lib.bnn_flip_create(C.byref(p), C.byref(h)) == capi.STATUS_CODE["INVALID_ARGUMENT"]
+    p = capi.make_params({"cell_size": 0.1, "solver_kind": 9})
+    assert lib.bnn_flip_create(C.byref(p), C.byref(h)) == capi.STATUS_CODE["NOT_SUPPORTED"]
+    p = capi.make_params({"cell_size": 0.1, "box_max": (0.0, 1.0, 1.0)})
+    assert lib.bnn_flip_create(C.byref(p), C.byref(h)) == capi.STATUS_CODE["INVALID_ARGUMENT"]
+    assert lib.bnn_flip_create(None, C.byref(h)) == capi.STATUS_CODE["INVALID_ARGUMENT"]
+    assert lib.bnn_flip_step(None, None) == capi.STATUS_CODE["INVALID_ARGUMENT"]
+    assert lib.bnn_neighbors(None, 5, C.c_float(0.1), None, None, 0, None, None) == capi.STATUS_CODE["INVALID_ARGUMENT"]
+    assert lib.bnn_cell_sort_noalloc(None, 1 << 21, None, C.c_float(1.0), None, None, None, None, None, None) \
+        == capi.STATUS_CODE["INVALID_ARGUMENT"]
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    monkeypatch.setattr(capi, "_lib", None)
+    monkeypatch.setattr(capi, "LIB_PATH", tmp_path / "nope.so")
+    with pytest.raises(RuntimeError, match="no CPU fallback"):
+        capi.load()
