@@ -152,6 +152,7 @@ struct DevState {
     unsigned out_of_range;
     unsigned pad0;
     double outer_res, outer_bmax;
+    int bbox[6];            // min x,y,z and max x,y,z of the particles' (clamped) cells
 };
 
 #define BNN_FLAG_OUT_OF_GRID   1u

@@ -31,11 +31,11 @@ void launch_sort_finish(int n, size_t ncells, const uint32_t* cellOf, const uint
                         uint32_t* idDst, const float* cSrc, float* cDst, float* g3, const GridDesc& g, size_t stride,
                         cudaStream_t s);
 void launch_p2g(const GridDesc& g, const uint32_t* cellStart, const float* g3, const float* p6, const float* C9,
-                size_t stride, float* const* out, uint8_t* const* valid, bool affine, cudaStream_t s);
+                size_t stride, float* const* out, uint8_t* const* valid, bool affine, const DevState* st, cudaStream_t s);
 void launch_extrapolate(const GridDesc& g, float* const* A, uint8_t* const* VA, float* const* B, uint8_t* const* VB,
                         int lastMode, float* const* oldOut, float gravityDt, DevState* st, cudaStream_t s);
 void launch_fluid_sdf(const GridDesc& g, const uint32_t* cellStart, const float* g3, const float* p6, size_t stride,
-                      float* phi, cudaStream_t s);
+                      float* phi, const DevState* st, cudaStream_t s);
 void launch_active_flags(const GridDesc& g, const float* phi, uint32_t* flag, DevState* st, cudaStream_t s);
 void launch_active_rows(size_t nc, const uint32_t* flag, const uint32_t* idx, uint32_t* rowCell, cudaStream_t s);
 void launch_build_rows(const GridDesc& g, int nrows, const uint32_t* rowCell, const float* phi, const uint32_t* aidx,
@@ -380,7 +380,8 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st) {
     h->cur = nxt;
     cudaEventRecord(h->ev[2], s);
     // P2G
-    launch_p2g(g, h->cellStart, h->g3, h->p6[h->cur], affine ? h->C9[h->cur] : nullptr, h->cap, h->U, h->VA, affine, s);
+    launch_p2g(g, h->cellStart, h->g3, h->p6[h->cur], affine ? h->C9[h->cur] : nullptr, h->cap, h->U, h->VA, affine,
+               h->dst, s);
     cudaEventRecord(h->ev[3], s);
     const float gdt = h->P.apply_gravity ? 9.81f * substep : 0.f;
     if(kind == BNN_SOLVER_APIC) {
@@ -392,7 +393,7 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st) {
     }
     cudaEventRecord(h->ev[4], s);
     // pressure projection (PIC_Solver.cpp:533-539)
-    launch_fluid_sdf(g, h->cellStart, h->g3, h->p6[h->cur], h->cap, h->phi, s);
+    launch_fluid_sdf(g, h->cellStart, h->g3, h->p6[h->cur], h->cap, h->phi, h->dst, s);
     cudaEventRecord(h->ev[5], s);
     launch_active_flags(g, h->phi, h->flag, h->dst, s);
     BNN_CUDA_CHECK(exclusive_scan_u32(h->flag, h->aidx, h->C, h->scanWs, s));

@@ -113,7 +113,8 @@ __device__ __forceinline__ void constrain_to_box(const GridDesc& g, float& x, fl
     }
 }
 
-__device__ __forceinline__ uint32_t cell_linear(const GridDesc& g, float gx, float gy, float gz, bool& outside) {
+__device__ __forceinline__ uint32_t cell_linear(const GridDesc& g, float gx, float gy, float gz, bool& outside,
+                                                int* cc = nullptr) {
     // Grid::getCellIdx<Int> (Grid.h:156-162): truncation of (p - bMin)/cellSize
     int c[3] = {(int)gx, (int)gy, (int)gz};
     outside = false;
@@ -122,7 +123,33 @@ __device__ __forceinline__ uint32_t cell_linear(const GridDesc& g, float gx, flo
         if(c[d] < 0) { c[d] = 0; outside = true; }
         if(c[d] > g.G[d] - 1) { c[d] = g.G[d] - 1; outside = true; }
     }
+    if(cc) { cc[0] = c[0]; cc[1] = c[1]; cc[2] = c[2]; }
     return (uint32_t)(((size_t)c[2] * g.G[1] + c[1]) * g.G[0] + c[0]);
+}
+
+// Bounding box of occupied cells: per-thread box, reduced over the block, then one set
+// of atomics per block (the advection grid is capped, so there are few blocks).
+__device__ __forceinline__ void bbox_block_reduce(DevState* st, int mn[3], int mx[3]) {
+    __shared__ int sm[2][3][32];
+#pragma unroll
+    for(int d = 0; d < 3; ++d)
+        for(int off = 16; off > 0; off >>= 1) {
+            mn[d] = min(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], off));
+            mx[d] = max(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], off));
+        }
+    const int w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    if((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for(int d = 0; d < 3; ++d) { sm[0][d][w] = mn[d]; sm[1][d][w] = mx[d]; }
+    }
+    __syncthreads();
+    if(threadIdx.x < 3) {
+        const int d = threadIdx.x;
+        int a = INT_MAX, b = INT_MIN;
+        for(int q = 0; q < nw; ++q) { a = min(a, sm[0][d][q]); b = max(b, sm[1][d][q]); }
+        if(a != INT_MAX) atomicMin(&st->bbox[d], a);
+        if(b != INT_MIN) atomicMax(&st->bbox[3 + d], b);
+    }
 }
 
 // ----------------------------------------------------------------------------------
@@ -137,8 +164,8 @@ __global__ void __launch_bounds__(256) k_advect(int n, float* __restrict__ px, f
                                                 float sub, int steps, uint32_t* __restrict__ cellOf,
                                                 uint32_t* __restrict__ slot, uint32_t* __restrict__ count,
                                                 DevState* st) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if(p >= n) return;
+    int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {INT_MIN, INT_MIN, INT_MIN};
+    for(int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
     float x = px[p], y = py[p], z = pz[p];
     for(int s = 0; s < steps; ++s) {
         float gv[3];
@@ -155,10 +182,15 @@ __global__ void __launch_bounds__(256) k_advect(int n, float* __restrict__ px, f
     }
     px[p] = x; py[p] = y; pz[p] = z;
     bool outside;
-    uint32_t c = cell_linear(g, (x - g.bmin[0]) / g.dx, (y - g.bmin[1]) / g.dx, (z - g.bmin[2]) / g.dx, outside);
+    int cc[3];
+    uint32_t c = cell_linear(g, (x - g.bmin[0]) / g.dx, (y - g.bmin[1]) / g.dx, (z - g.bmin[2]) / g.dx, outside, cc);
     if(outside) atomicOr(&st->flags, BNN_FLAG_OUT_OF_GRID);
     cellOf[p] = c;
     slot[p] = atomicAdd(count + c, 1u);
+#pragma unroll
+    for(int d = 0; d < 3; ++d) { mn[d] = min(mn[d], cc[d]); mx[d] = max(mx[d], cc[d]); }
+    }
+    bbox_block_reduce(st, mn, mx);
 }
 
 // Cell id + histogram without moving (first sort of freshly loaded particles)
@@ -661,7 +693,9 @@ __global__ void k_step_reset(DevState* st) {
     st->flags = 0u;
     st->zero_phi = 0u;
     st->maxvel_bits = 0u;
+    for(int d = 0; d < 3; ++d) { st->bbox[d] = INT_MAX; st->bbox[3 + d] = INT_MIN; }
 }
+
 
 // ----------------------------------------------------------------------------------
 // Launchers
@@ -671,7 +705,8 @@ static inline unsigned nblk(size_t n, int t = 256) { return (unsigned)((n + t - 
 void launch_advect(int n, float* p6, size_t stride, const float* const* U, const GridDesc& g, float sub, int steps,
                    uint32_t* cellOf, uint32_t* slot, uint32_t* count, DevState* st, cudaStream_t s) {
     if(n == 0) return;
-    { k_advect<<<nblk(n), 256, 0, s>>>(n, p6, p6 + stride, p6 + 2 * stride, U[0], U[1], U[2], g, sub, steps, cellOf, slot,
+    const unsigned blocks = nblk(n) < 148u * 8u ? nblk(n) : 148u * 8u;
+    { k_advect<<<blocks, 256, 0, s>>>(n, p6, p6 + stride, p6 + 2 * stride, U[0], U[1], U[2], g, sub, steps, cellOf, slot,
                                      count, st); bnn_note_launch(); }
 }
 void launch_cell_histogram(int n, const float* p6, size_t stride, const GridDesc& g, uint32_t* cellOf, uint32_t* slot,
@@ -688,8 +723,17 @@ void launch_sort_finish(int n, size_t ncells, const uint32_t* cellOf, const uint
     if(n > 0)
         { k_gather_particles<<<nblk(n), 256, 0, s>>>(n, order, src6, dst6, idSrc, idDst, cSrc, cDst, g3, g, stride); bnn_note_launch(); }
 }
+void launch_p2g_col(const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float* g3, const float* p6,
+                    size_t stride, float* const* out, uint8_t* const* valid, cudaStream_t s);
+void launch_fluid_sdf_col(const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float* g3,
+                          const float* p6, size_t stride, float* phi, cudaStream_t s);
+
 void launch_p2g(const GridDesc& g, const uint32_t* cellStart, const float* g3, const float* p6, const float* C9,
-                size_t stride, float* const* out, uint8_t* const* valid, bool affine, cudaStream_t s) {
+                size_t stride, float* const* out, uint8_t* const* valid, bool affine, const DevState* st, cudaStream_t s) {
+    if(!affine) {
+        launch_p2g_col(g, st, cellStart, g3, p6, stride, out, valid, s);
+        return;
+    }
     const float *gx = g3, *gy = g3 + stride, *gz = g3 + 2 * stride;
     const float *px = p6, *py = p6 + stride, *pz = p6 + 2 * stride;
     for(int d = 0; d < 3; ++d) {
@@ -726,10 +770,8 @@ void launch_extrapolate(const GridDesc& g, float* const* A, uint8_t* const* VA, 
     }
 }
 void launch_fluid_sdf(const GridDesc& g, const uint32_t* cellStart, const float* g3, const float* p6, size_t stride,
-                      float* phi, cudaStream_t s) {
-    size_t nc = (size_t)g.G[0] * g.G[1] * g.G[2];
-    { k_fluid_sdf<<<nblk(nc), 256, 0, s>>>(g, cellStart, g3, g3 + stride, g3 + 2 * stride, p6, p6 + stride,
-                                         p6 + 2 * stride, phi); bnn_note_launch(); }
+                      float* phi, const DevState* st, cudaStream_t s) {
+    launch_fluid_sdf_col(g, st, cellStart, g3, p6, stride, phi, s);
 }
 void launch_active_flags(const GridDesc& g, const float* phi, uint32_t* flag, DevState* st, cudaStream_t s) {
     size_t nc = (size_t)g.G[0] * g.G[1] * g.G[2];

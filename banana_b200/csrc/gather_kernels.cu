@@ -1,0 +1,278 @@
+// Column gathers for P2G (non-affine) and the fluid SDF.
+//
+// Tuned on B200 at 256^3 (12.7M particles): 32 x 8 threads per block, columns of 4 outputs,
+// particle loads issued 2 at a time (batches of 4 or 8 and columns of 8 were slower).
+//
+// One thread owns a column of kCol consecutive outputs (faces of one component, or cells)
+// along one axis; the 32 lanes of a warp own 32 consecutive x positions, so their particle
+// loads fall on a few cache lines.  A face or cell only receives from particles of the
+// cells one step around it, so the thread walks the cell rows around its whole column
+// once (kCol + 2 rows along the column axis instead of 3 per output) and hands every
+// particle to the outputs of the column it can reach.  Rows are walked in linear cell
+// order (z outer, y inner) and particles in sorted order inside a row, so every output
+// sees its particles in exactly the order of the serial reference loop over cell-sorted
+// particles: the sums are bit-identical to the per-output gathers in flip_kernels.cu.
+//
+// The fluid SDF keeps the minimum squared distance instead of the minimum distance:
+// sqrtf (correctly rounded) and the subtraction of the particle radius are both
+// non-decreasing, so min(sqrtf(d2) - r) == sqrtf(min d2) - r exactly, and one square root
+// per cell replaces one per candidate particle.
+//
+// Thread blocks whose column box lies more than one cell away from every particle (the
+// occupied-cell bounding box is reduced during advection) only write the empty values.
+#include "bnn_internal.cuh"
+
+namespace bnn {
+
+namespace {
+#ifndef BNN_COL_LEN
+#define BNN_COL_LEN 4
+#endif
+#ifndef BNN_COL_ROWS
+#define BNN_COL_ROWS 8
+#endif
+#ifndef BNN_COL_BATCH
+#define BNN_COL_BATCH 2
+#endif
+constexpr int kCol = BNN_COL_LEN;     // outputs per thread along the column axis
+constexpr int kLx = 32;               // threads along x
+constexpr int kLr = BNN_COL_ROWS;     // threads along the row axis
+constexpr int kBatch = BNN_COL_BATCH; // particles whose loads are issued together
+
+__device__ __forceinline__ void bary_c(float x, int& i, float& f, int i_high) {
+    // get_barycentric (ArrayHelpers.h:95-112)
+    const float s = floorf(x);
+    i = (int)s;
+    if(i < 0) { i = 0; f = 0.f; }
+    else if(i > i_high - 2) { i = i_high - 2; f = 1.f; }
+    else { f = x - s; }
+}
+
+// Does [lo, hi] (per axis) meet the occupied-cell box grown by one cell?
+__device__ __forceinline__ bool near_particles(const DevState* st, const int lo[3], const int hi[3]) {
+#pragma unroll
+    for(int d = 0; d < 3; ++d) {
+        const int bl = st->bbox[d], bh = st->bbox[3 + d];
+        if(bh < bl) return false;  // no particles
+        if(hi[d] < bl - 1 || lo[d] > bh + 1) return false;
+    }
+    return true;
+}
+} // namespace
+
+// FLIP_Solver::mapParticles2Grid (FLIP_Solver.cpp:57-95) for component D.  The column axis
+// is z for u and v faces and y for w faces (never the component's own axis); the other
+// non-x axis is the thread-row axis.
+template<int D>
+__global__ void __launch_bounds__(kLx * kLr) k_p2g_col(GridDesc g, const DevState* __restrict__ st,
+                                                       const uint32_t* __restrict__ cellStart,
+                                                       const float* __restrict__ gxs, const float* __restrict__ gys,
+                                                       const float* __restrict__ gzs, const float* __restrict__ vd,
+                                                       float* __restrict__ out, uint8_t* __restrict__ valid) {
+    constexpr int A = (D == 2) ? 1 : 2;  // column axis
+    constexpr int R = (D == 2) ? 2 : 1;  // thread-row axis
+    const int sz[3] = {g.G[0] + (D == 0), g.G[1] + (D == 1), g.G[2] + (D == 2)};
+    const int i = blockIdx.x * kLx + threadIdx.x;
+    const int r = blockIdx.y * kLr + threadIdx.y;
+    const int a0 = blockIdx.z * kCol;
+    auto face_index = [&](int u) {
+        const int fy = (A == 1) ? a0 + u : r, fz = (A == 2) ? a0 + u : r;
+        return ((size_t)fz * sz[1] + fy) * sz[0] + i;
+    };
+    const bool liveIR = i < sz[0] && r < sz[R];
+    {
+        int lo[3], hi[3];
+        lo[0] = blockIdx.x * kLx; hi[0] = lo[0] + kLx - 1;
+        lo[R] = blockIdx.y * kLr; hi[R] = lo[R] + kLr - 1;
+        lo[A] = a0; hi[A] = a0 + kCol - 1;
+        if(!near_particles(st, lo, hi)) {
+            if(liveIR) {
+#pragma unroll
+                for(int u = 0; u < kCol; ++u)
+                    if(a0 + u < sz[A]) { out[face_index(u)] = 0.f; valid[face_index(u)] = 0; }
+            }
+            return;
+        }
+    }
+    float S[kCol], W[kCol];
+#pragma unroll
+    for(int u = 0; u < kCol; ++u) { S[u] = 0.f; W[u] = 0.f; }
+    const int xlo = max(i - 1, 0), xhi = min(D == 0 ? i : i + 1, g.G[0] - 1);
+    const int rlo = max(r - 1, 0), rhi = min(R == D ? r : r + 1, g.G[R] - 1);
+    const float* gR = (R == 1) ? gys : gzs;
+    const float* gA = (A == 1) ? gys : gzs;
+
+    // one cell row: A coordinate a0 - 1 + t, R coordinate rr
+    auto row = [&](int t, int rr) __attribute__((always_inline)) {
+        const int ca = a0 - 1 + t;
+        if(ca < 0 || ca > g.G[A] - 1) return;
+        const int kk = (A == 2) ? ca : rr, jj = (A == 1) ? ca : rr;
+        const size_t base = ((size_t)kk * g.G[1] + jj) * g.G[0];
+        const uint32_t b = __ldg(cellStart + base + xlo), e = __ldg(cellStart + base + xhi + 1);
+        // Particles are taken kBatch at a time: all loads first, then the arithmetic.  A
+        // particle that does not reach an output adds +0 to its sums, which leaves them
+        // unchanged (they start at +0 and can never become -0), so no branch is needed.
+        for(uint32_t q0 = b; q0 < e; q0 += kBatch) {
+            float lx[kBatch], lr[kBatch], la[kBatch], lv[kBatch];
+#pragma unroll
+            for(int w = 0; w < kBatch; ++w) {
+                const uint32_t q = min(q0 + (uint32_t)w, e - 1u);
+                lx[w] = __ldg(gxs + q);
+                lr[w] = __ldg(gR + q);
+                la[w] = __ldg(gA + q);
+                lv[w] = __ldg(vd + q);
+            }
+#pragma unroll
+            for(int w = 0; w < kBatch; ++w) {
+                int si, sr, sa;
+                float fi, fr, fa;
+                bary_c(lx[w] - (D == 0 ? 0.f : 0.5f), si, fi, sz[0]);
+                bary_c(lr[w] - (R == D ? 0.f : 0.5f), sr, fr, sz[R]);
+                bary_c(la[w] - 0.5f, sa, fa, sz[A]);
+                const bool reach = (q0 + (uint32_t)w < e) && (si == i || si == i - 1) && (sr == r || sr == r - 1);
+                const float wx = (si == i) ? (1.0f - fi) : fi;
+                const float wr = (sr == r) ? (1.0f - fr) : fr;
+                const float wxr = wx * wr;  // (wx * wy) when the column axis is z
+#pragma unroll
+                for(int du = -1; du <= 1; ++du) {
+                    const int u = t - 1 + du;
+                    if(u < 0 || u >= kCol) continue;
+                    const int fa_ = a0 + u;
+                    const bool ok = reach && (sa == fa_ || sa == fa_ - 1);
+                    const float wa = (sa == fa_) ? (1.0f - fa) : fa;
+                    // weight = wx * wy * wz, multiplied left to right
+                    const float wgt = (A == 2) ? wxr * wa : (wx * wa) * wr;
+                    const float m = wgt * lv[w];
+                    S[u] = S[u] + (ok ? m : 0.f);
+                    W[u] = W[u] + (ok ? wgt : 0.f);
+                }
+            }
+        }
+    };
+    if(A == 2) {
+#pragma unroll
+        for(int t = 0; t < kCol + 2; ++t)
+            for(int rr = rlo; rr <= rhi; ++rr) row(t, rr);
+    } else {
+        for(int rr = rlo; rr <= rhi; ++rr) {
+#pragma unroll
+            for(int t = 0; t < kCol + 2; ++t) row(t, rr);
+        }
+    }
+    if(liveIR) {
+#pragma unroll
+        for(int u = 0; u < kCol; ++u) {
+            if(a0 + u >= sz[A]) continue;
+            const bool ok = W[u] > FLT_MIN;
+            out[face_index(u)] = ok ? S[u] / W[u] : S[u];
+            valid[face_index(u)] = ok ? 1 : 0;
+        }
+    }
+}
+
+// PIC_Solver::computeFluidSDF (PIC_Solver.cpp:601-652): phi of a cell = min(3 dx,
+// min over the particles whose clamped 3x3x3 cell range holds it of |x_cell - x_p| - r).
+// The column axis is z.  The range test against the particle's own cell only matters for
+// a particle outside the grid (its own cell differs from the clamped cell it is sorted
+// into); the advection flags that case and the test is then made for every candidate.
+__global__ void __launch_bounds__(kLx * kLr) k_fluid_sdf_col(GridDesc g, const DevState* __restrict__ st,
+                                                             const uint32_t* __restrict__ cellStart,
+                                                             const float* __restrict__ gxs,
+                                                             const float* __restrict__ gys,
+                                                             const float* __restrict__ gzs,
+                                                             const float* __restrict__ pxs,
+                                                             const float* __restrict__ pys,
+                                                             const float* __restrict__ pzs, float* __restrict__ phi) {
+    const int i = blockIdx.x * kLx + threadIdx.x;
+    const int j = blockIdx.y * kLr + threadIdx.y;
+    const int k0 = blockIdx.z * kCol;
+    const bool liveIJ = i < g.G[0] && j < g.G[1];
+    const float empty = g.dx * 3.0f;
+    {
+        const int lo[3] = {(int)(blockIdx.x * kLx), (int)(blockIdx.y * kLr), k0};
+        const int hi[3] = {lo[0] + kLx - 1, lo[1] + kLr - 1, k0 + kCol - 1};
+        if(!near_particles(st, lo, hi)) {
+            if(liveIJ) {
+#pragma unroll
+                for(int u = 0; u < kCol; ++u)
+                    if(k0 + u < g.G[2]) phi[((size_t)(k0 + u) * g.G[1] + j) * g.G[0] + i] = empty;
+            }
+            return;
+        }
+    }
+    const bool exact = (st->flags & BNN_FLAG_OUT_OF_GRID) != 0u;
+    // Grid::getWorldCoordinate(i + 0.5, j + 0.5, k + 0.5) (Grid.h:186-194)
+    const float sxw = ((float)i + 0.5f) * g.dx + g.bmin[0];
+    const float syw = ((float)j + 0.5f) * g.dx + g.bmin[1];
+    float m[kCol];
+#pragma unroll
+    for(int u = 0; u < kCol; ++u) m[u] = __int_as_float(0x7f800000);  // +inf
+    const int xlo = max(i - 1, 0), xhi = min(i + 1, g.G[0] - 1);
+    const int ylo = max(j - 1, 0), yhi = min(j + 1, g.G[1] - 1);
+#pragma unroll
+    for(int t = 0; t < kCol + 2; ++t) {
+        const int kk = k0 - 1 + t;
+        if(kk < 0 || kk > g.G[2] - 1) continue;
+        for(int jj = ylo; jj <= yhi; ++jj) {
+            const size_t base = ((size_t)kk * g.G[1] + jj) * g.G[0];
+            const uint32_t b = __ldg(cellStart + base + xlo), e = __ldg(cellStart + base + xhi + 1);
+            for(uint32_t q = b; q < e; ++q) {
+                const float ddx = sxw - __ldg(pxs + q), ddy = syw - __ldg(pys + q);
+                const float pz = __ldg(pzs + q);
+                const float dxy = ddx * ddx + ddy * ddy;
+                int ck = 0;
+                if(exact) {
+                    // the particle's own cell and its clamped 3x3x3 range (PIC_Solver.cpp:633-635)
+                    const int ci = (int)__ldg(gxs + q), cj = (int)__ldg(gys + q);
+                    ck = (int)__ldg(gzs + q);
+                    if(i < max(ci - 1, 0) || i > min(ci + 1, g.G[0] - 1)) continue;
+                    if(j < max(cj - 1, 0) || j > min(cj + 1, g.G[1] - 1)) continue;
+                }
+#pragma unroll
+                for(int du = -1; du <= 1; ++du) {
+                    const int u = t - 1 + du;
+                    if(u < 0 || u >= kCol) continue;
+                    const int k = k0 + u;
+                    if(exact && (k < max(ck - 1, 0) || k > min(ck + 1, g.G[2] - 1))) continue;
+                    const float ddz = (((float)k + 0.5f) * g.dx + g.bmin[2]) - pz;
+                    const float d2 = dxy + ddz * ddz;  // glm::length2: (x*x + y*y) + z*z
+                    m[u] = fminf(m[u], d2);
+                }
+            }
+        }
+    }
+    if(liveIJ) {
+#pragma unroll
+        for(int u = 0; u < kCol; ++u) {
+            if(k0 + u >= g.G[2]) continue;
+            float ph = empty;
+            if(m[u] != __int_as_float(0x7f800000)) {
+                const float val = sqrtf(m[u]) - g.sdfRadius;
+                if(val < ph) ph = val;
+            }
+            phi[((size_t)(k0 + u) * g.G[1] + j) * g.G[0] + i] = ph;
+        }
+    }
+}
+
+static dim3 col_grid(int sx, int sr, int sa) {
+    return dim3((unsigned)((sx + kLx - 1) / kLx), (unsigned)((sr + kLr - 1) / kLr), (unsigned)((sa + kCol - 1) / kCol));
+}
+
+void launch_p2g_col(const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float* g3, const float* p6,
+                    size_t stride, float* const* out, uint8_t* const* valid, cudaStream_t s) {
+    const float *gx = g3, *gy = g3 + stride, *gz = g3 + 2 * stride;
+    const dim3 blk(kLx, kLr);
+    // u, v: rows along y, columns along z; w: rows along z, columns along y
+    { k_p2g_col<0><<<col_grid(g.G[0] + 1, g.G[1], g.G[2]), blk, 0, s>>>(g, st, cellStart, gx, gy, gz, p6 + 3 * stride, out[0], valid[0]); bnn_note_launch(); }
+    { k_p2g_col<1><<<col_grid(g.G[0], g.G[1] + 1, g.G[2]), blk, 0, s>>>(g, st, cellStart, gx, gy, gz, p6 + 4 * stride, out[1], valid[1]); bnn_note_launch(); }
+    { k_p2g_col<2><<<col_grid(g.G[0], g.G[2] + 1, g.G[1]), blk, 0, s>>>(g, st, cellStart, gx, gy, gz, p6 + 5 * stride, out[2], valid[2]); bnn_note_launch(); }
+}
+
+void launch_fluid_sdf_col(const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float* g3,
+                          const float* p6, size_t stride, float* phi, cudaStream_t s) {
+    { k_fluid_sdf_col<<<col_grid(g.G[0], g.G[1], g.G[2]), dim3(kLx, kLr), 0, s>>>(
+          g, st, cellStart, g3, g3 + stride, g3 + 2 * stride, p6, p6 + stride, p6 + 2 * stride, phi); bnn_note_launch(); }
+}
+
+} // namespace bnn

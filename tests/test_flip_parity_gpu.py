@@ -136,3 +136,17 @@ def test_advance_frame_substeps(bnn, oracle_mod):
                 break
         assert k == ko
     assert np.array_equal(g.get_particles()[0], o.get_particles()[0])
+
+
+def test_dense_scene_bitexact(bnn, oracle_mod):
+    """27 particles per cell: long cell rows in the column gathers of P2G and the fluid SDF
+    (odd row lengths end on a partial load batch); results stay identical to the oracle."""
+    n = 20
+    cfg = scenes.dam_break_params(n)
+    pos, vel = scenes.dam_break(n, ppc=27)
+    g = bnn.FlipSolver(cfg)
+    g.set_particles(pos, vel)
+    o = oracle_mod.Oracle(cfg)
+    o.set_particles(pos, vel)
+    for s in range(4):
+        _compare_step(g, o, s)
