@@ -28,14 +28,16 @@ void launch_cell_histogram(int n, const float* p6, size_t stride, const GridDesc
                            uint32_t* count, DevState* st, cudaStream_t s);
 void launch_sort_finish(int n, size_t ncells, const uint32_t* cellOf, const uint32_t* slot, const uint32_t* cellStart,
                         uint32_t* order, uint32_t* count, const float* src6, float* dst6, const uint32_t* idSrc,
-                        uint32_t* idDst, const float* cSrc, float* cDst, float* g3, const GridDesc& g, size_t stride,
+                        uint32_t* idDst, const float* cSrc, float* cDst, float* g3, float4* rec, const GridDesc& g,
+                        size_t stride,
                         cudaStream_t s);
 void launch_p2g(const GridDesc& g, const uint32_t* cellStart, const float* g3, const float* p6, const float* C9,
-                size_t stride, float* const* out, uint8_t* const* valid, bool affine, const DevState* st, cudaStream_t s);
+                const float4* rec, size_t stride, float* const* out, uint8_t* const* valid, bool affine,
+                const DevState* st, cudaStream_t s);
 void launch_extrapolate(const GridDesc& g, float* const* A, uint8_t* const* VA, float* const* B, uint8_t* const* VB,
                         int lastMode, float* const* oldOut, float gravityDt, DevState* st, cudaStream_t s);
-void launch_fluid_sdf(const GridDesc& g, const uint32_t* cellStart, const float* g3, const float* p6, size_t stride,
-                      float* phi, const DevState* st, cudaStream_t s);
+void launch_fluid_sdf(const GridDesc& g, const uint32_t* cellStart, const float4* rec, size_t stride, float* phi,
+                      const DevState* st, cudaStream_t s);
 void launch_active_flags(const GridDesc& g, const float* phi, uint32_t* flag, DevState* st, cudaStream_t s);
 void launch_active_rows(size_t nc, const uint32_t* flag, const uint32_t* idx, uint32_t* rowCell, cudaStream_t s);
 void launch_build_rows(const GridDesc& g, int nrows, const uint32_t* rowCell, const float* phi, const uint32_t* aidx,
@@ -72,7 +74,8 @@ struct bnn_flip {
     uint32_t* ids[2] = {nullptr, nullptr};
     float* C9[2] = {nullptr, nullptr};
     int cur = 0;
-    float* g3 = nullptr;
+    float* g3 = nullptr;    // grid coordinates (APIC / AFLIP P2G)
+    float4* rec = nullptr;  // per-particle gather records: 3 P2G stencil planes + positions
     uint32_t *cellOf = nullptr, *slot = nullptr, *order = nullptr;
     uint32_t *count = nullptr, *cellStart = nullptr;
     void* scanWs = nullptr;
@@ -106,8 +109,8 @@ static void free_particles(bnn_flip* h) {
         cudaFree(h->p6[b]); cudaFree(h->ids[b]); cudaFree(h->C9[b]);
         h->p6[b] = nullptr; h->ids[b] = nullptr; h->C9[b] = nullptr;
     }
-    cudaFree(h->g3); cudaFree(h->cellOf); cudaFree(h->slot); cudaFree(h->order); cudaFree(h->aosStage);
-    h->g3 = nullptr; h->cellOf = h->slot = h->order = nullptr; h->aosStage = nullptr;
+    cudaFree(h->g3); cudaFree(h->rec); cudaFree(h->cellOf); cudaFree(h->slot); cudaFree(h->order); cudaFree(h->aosStage);
+    h->g3 = nullptr; h->rec = nullptr; h->cellOf = h->slot = h->order = nullptr; h->aosStage = nullptr;
     h->cap = 0;
 }
 
@@ -123,6 +126,7 @@ static int reserve_particles(bnn_flip* h, uint32_t n) {
             BNN_CUDA_CHECK(cudaMalloc(&h->C9[b], 9 * st * sizeof(float)));
     }
     BNN_CUDA_CHECK(cudaMalloc(&h->g3, 3 * st * sizeof(float)));
+    BNN_CUDA_CHECK(cudaMalloc(&h->rec, 4 * st * sizeof(float4)));
     BNN_CUDA_CHECK(cudaMalloc(&h->cellOf, st * sizeof(uint32_t)));
     BNN_CUDA_CHECK(cudaMalloc(&h->slot, st * sizeof(uint32_t)));
     BNN_CUDA_CHECK(cudaMalloc(&h->order, st * sizeof(uint32_t)));
@@ -376,11 +380,12 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st) {
     const int nxt = 1 - h->cur;
     launch_sort_finish(n, h->C, h->cellOf, h->slot, h->cellStart, h->order, h->count, h->p6[h->cur], h->p6[nxt],
                        h->ids[h->cur], h->ids[nxt], affine ? h->C9[h->cur] : nullptr, affine ? h->C9[nxt] : nullptr,
-                       h->g3, g, h->cap, s);
+                       h->g3, h->rec, g, h->cap, s);
     h->cur = nxt;
     cudaEventRecord(h->ev[2], s);
     // P2G
-    launch_p2g(g, h->cellStart, h->g3, h->p6[h->cur], affine ? h->C9[h->cur] : nullptr, h->cap, h->U, h->VA, affine,
+    launch_p2g(g, h->cellStart, h->g3, h->p6[h->cur], affine ? h->C9[h->cur] : nullptr, h->rec, h->cap, h->U, h->VA,
+               affine,
                h->dst, s);
     cudaEventRecord(h->ev[3], s);
     const float gdt = h->P.apply_gravity ? 9.81f * substep : 0.f;
@@ -393,7 +398,7 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st) {
     }
     cudaEventRecord(h->ev[4], s);
     // pressure projection (PIC_Solver.cpp:533-539)
-    launch_fluid_sdf(g, h->cellStart, h->g3, h->p6[h->cur], h->cap, h->phi, h->dst, s);
+    launch_fluid_sdf(g, h->cellStart, h->rec, h->cap, h->phi, h->dst, s);
     cudaEventRecord(h->ev[5], s);
     launch_active_flags(g, h->phi, h->flag, h->dst, s);
     BNN_CUDA_CHECK(exclusive_scan_u32(h->flag, h->aidx, h->C, h->scanWs, s));

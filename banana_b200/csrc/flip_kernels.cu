@@ -235,25 +235,58 @@ __global__ void k_sort_buckets(int ncells, const uint32_t* __restrict__ cellStar
     }
 }
 
-// Apply the permutation to the particle arrays; also emits grid coordinates
-// (Grid::getGridCoordinate, Grid.h:197) used by P2G and the fluid SDF.
+// Apply the permutation to the particle arrays and emit what the gathers read per
+// particle (all from Grid::getGridCoordinate, Grid.h:197):
+//   g3   grid coordinates (SoA; the APIC/AFLIP P2G reads them);
+//   rec  plane D < 3: the P2G stencil record of component D, {ex, ey, ez, v_D}: e_a is the
+//        get_barycentric fraction of axis a (ArrayHelpers.h:95-112), its sign bit set when
+//        the stencil's base index is the particle's (sort) cell - 1 instead of the cell
+//        itself -- the only two cases, whatever the position, since both indices are
+//        clamped the same way and fractions are never -0;
+//        plane 3: the position {x, y, z, 0} for the fluid SDF.
+// One 16-byte load per candidate particle then replaces four scattered 4-byte loads.
 __global__ void k_gather_particles(int n, const uint32_t* __restrict__ order, const float* __restrict__ src6,
                                    float* __restrict__ dst6, const uint32_t* __restrict__ idSrc,
                                    uint32_t* __restrict__ idDst, const float* __restrict__ cSrc,
-                                   float* __restrict__ cDst, float* __restrict__ g3, GridDesc g, size_t stride) {
+                                   float* __restrict__ cDst, float* __restrict__ g3, float4* __restrict__ rec,
+                                   GridDesc g, size_t stride) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if(i >= n) return;
     const uint32_t s = order[i];
+    float v6[6];
 #pragma unroll
-    for(int q = 0; q < 6; ++q) dst6[q * stride + i] = src6[q * stride + s];
+    for(int q = 0; q < 6; ++q) { v6[q] = src6[q * stride + s]; dst6[q * stride + i] = v6[q]; }
     idDst[i] = idSrc[s];
+    float gc[3];
+#pragma unroll
+    for(int a = 0; a < 3; ++a) gc[a] = (v6[a] - g.bmin[a]) / g.dx;
     if(cSrc) {
 #pragma unroll
         for(int q = 0; q < 9; ++q) cDst[q * stride + i] = cSrc[q * stride + s];
+#pragma unroll
+        for(int a = 0; a < 3; ++a) g3[a * stride + i] = gc[a];
     }
-    g3[i] = (dst6[i] - g.bmin[0]) / g.dx;
-    g3[stride + i] = (dst6[stride + i] - g.bmin[1]) / g.dx;
-    g3[2 * stride + i] = (dst6[2 * stride + i] - g.bmin[2]) / g.dx;
+    rec[3 * stride + i] = make_float4(v6[0], v6[1], v6[2], 0.f);
+    if(!cSrc) {
+        int cell[3];
+#pragma unroll
+        for(int a = 0; a < 3; ++a) {
+            int c = (int)gc[a];
+            cell[a] = c < 0 ? 0 : (c > g.G[a] - 1 ? g.G[a] - 1 : c);
+        }
+#pragma unroll
+        for(int D = 0; D < 3; ++D) {
+            float e[3];
+#pragma unroll
+            for(int a = 0; a < 3; ++a) {
+                int si;
+                float fi;
+                bary(gc[a] - (a == D ? 0.f : 0.5f), si, fi, g.G[a] + (a == D ? 1 : 0));
+                e[a] = (si < cell[a]) ? __int_as_float(__float_as_int(fi) | (int)0x80000000) : fi;
+            }
+            rec[D * stride + i] = make_float4(e[0], e[1], e[2], v6[3 + D]);
+        }
+    }
 }
 
 // ----------------------------------------------------------------------------------
@@ -716,22 +749,23 @@ void launch_cell_histogram(int n, const float* p6, size_t stride, const GridDesc
 }
 void launch_sort_finish(int n, size_t ncells, const uint32_t* cellOf, const uint32_t* slot, const uint32_t* cellStart,
                         uint32_t* order, uint32_t* count, const float* src6, float* dst6, const uint32_t* idSrc,
-                        uint32_t* idDst, const float* cSrc, float* cDst, float* g3, const GridDesc& g, size_t stride,
-                        cudaStream_t s) {
+                        uint32_t* idDst, const float* cSrc, float* cDst, float* g3, float4* rec, const GridDesc& g,
+                        size_t stride, cudaStream_t s) {
     if(n > 0) { k_scatter_index<<<nblk(n), 256, 0, s>>>(n, cellOf, slot, cellStart, order); bnn_note_launch(); }
     { k_sort_buckets<<<nblk(ncells), 256, 0, s>>>((int)ncells, cellStart, order, idSrc, count); bnn_note_launch(); }
     if(n > 0)
-        { k_gather_particles<<<nblk(n), 256, 0, s>>>(n, order, src6, dst6, idSrc, idDst, cSrc, cDst, g3, g, stride); bnn_note_launch(); }
+        { k_gather_particles<<<nblk(n), 256, 0, s>>>(n, order, src6, dst6, idSrc, idDst, cSrc, cDst, g3, rec, g, stride); bnn_note_launch(); }
 }
-void launch_p2g_col(const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float* g3, const float* p6,
+void launch_p2g_col(const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float4* rec,
                     size_t stride, float* const* out, uint8_t* const* valid, cudaStream_t s);
-void launch_fluid_sdf_col(const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float* g3,
-                          const float* p6, size_t stride, float* phi, cudaStream_t s);
+void launch_fluid_sdf_col(const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float4* rec,
+                          size_t stride, float* phi, cudaStream_t s);
 
 void launch_p2g(const GridDesc& g, const uint32_t* cellStart, const float* g3, const float* p6, const float* C9,
-                size_t stride, float* const* out, uint8_t* const* valid, bool affine, const DevState* st, cudaStream_t s) {
+                const float4* rec, size_t stride, float* const* out, uint8_t* const* valid, bool affine,
+                const DevState* st, cudaStream_t s) {
     if(!affine) {
-        launch_p2g_col(g, st, cellStart, g3, p6, stride, out, valid, s);
+        launch_p2g_col(g, st, cellStart, rec, stride, out, valid, s);
         return;
     }
     const float *gx = g3, *gy = g3 + stride, *gz = g3 + 2 * stride;
@@ -769,9 +803,9 @@ void launch_extrapolate(const GridDesc& g, float* const* A, uint8_t* const* VA, 
         }
     }
 }
-void launch_fluid_sdf(const GridDesc& g, const uint32_t* cellStart, const float* g3, const float* p6, size_t stride,
-                      float* phi, const DevState* st, cudaStream_t s) {
-    launch_fluid_sdf_col(g, st, cellStart, g3, p6, stride, phi, s);
+void launch_fluid_sdf(const GridDesc& g, const uint32_t* cellStart, const float4* rec, size_t stride, float* phi,
+                      const DevState* st, cudaStream_t s) {
+    launch_fluid_sdf_col(g, st, cellStart, rec, stride, phi, s);
 }
 void launch_active_flags(const GridDesc& g, const float* phi, uint32_t* flag, DevState* st, cudaStream_t s) {
     size_t nc = (size_t)g.G[0] * g.G[1] * g.G[2];

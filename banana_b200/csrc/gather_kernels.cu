@@ -1,7 +1,9 @@
 // Column gathers for P2G (non-affine) and the fluid SDF.
 //
-// Tuned on B200 at 256^3 (12.7M particles): 32 x 8 threads per block, columns of 4 outputs,
-// particle loads issued 2 at a time (batches of 4 or 8 and columns of 8 were slower).
+// Both read one 16-byte record per candidate particle, written by the sort's gather
+// (flip_kernels.cu, k_gather_particles): the P2G stencil record of the component, or the
+// position.  Tuned on B200 at 256^3 (12.7M particles): 32 x 8 threads per block, columns
+// of 4 outputs, particle loads issued 2 at a time.
 //
 // One thread owns a column of kCol consecutive outputs (faces of one component, or cells)
 // along one axis; the 32 lanes of a warp own 32 consecutive x positions, so their particle
@@ -39,15 +41,6 @@ constexpr int kLx = 32;               // threads along x
 constexpr int kLr = BNN_COL_ROWS;     // threads along the row axis
 constexpr int kBatch = BNN_COL_BATCH; // particles whose loads are issued together
 
-__device__ __forceinline__ void bary_c(float x, int& i, float& f, int i_high) {
-    // get_barycentric (ArrayHelpers.h:95-112)
-    const float s = floorf(x);
-    i = (int)s;
-    if(i < 0) { i = 0; f = 0.f; }
-    else if(i > i_high - 2) { i = i_high - 2; f = 1.f; }
-    else { f = x - s; }
-}
-
 // Does [lo, hi] (per axis) meet the occupied-cell box grown by one cell?
 __device__ __forceinline__ bool near_particles(const DevState* st, const int lo[3], const int hi[3]) {
 #pragma unroll
@@ -66,8 +59,7 @@ __device__ __forceinline__ bool near_particles(const DevState* st, const int lo[
 template<int D>
 __global__ void __launch_bounds__(kLx * kLr) k_p2g_col(GridDesc g, const DevState* __restrict__ st,
                                                        const uint32_t* __restrict__ cellStart,
-                                                       const float* __restrict__ gxs, const float* __restrict__ gys,
-                                                       const float* __restrict__ gzs, const float* __restrict__ vd,
+                                                       const float4* __restrict__ rec, size_t stride,
                                                        float* __restrict__ out, uint8_t* __restrict__ valid) {
     constexpr int A = (D == 2) ? 1 : 2;  // column axis
     constexpr int R = (D == 2) ? 2 : 1;  // thread-row axis
@@ -99,8 +91,7 @@ __global__ void __launch_bounds__(kLx * kLr) k_p2g_col(GridDesc g, const DevStat
     for(int u = 0; u < kCol; ++u) { S[u] = 0.f; W[u] = 0.f; }
     const int xlo = max(i - 1, 0), xhi = min(D == 0 ? i : i + 1, g.G[0] - 1);
     const int rlo = max(r - 1, 0), rhi = min(R == D ? r : r + 1, g.G[R] - 1);
-    const float* gR = (R == 1) ? gys : gzs;
-    const float* gA = (A == 1) ? gys : gzs;
+    const float4* __restrict__ recD = rec + (size_t)D * stride;
 
     // one cell row: A coordinate a0 - 1 + t, R coordinate rr
     auto row = [&](int t, int rr) __attribute__((always_inline)) {
@@ -108,28 +99,32 @@ __global__ void __launch_bounds__(kLx * kLr) k_p2g_col(GridDesc g, const DevStat
         if(ca < 0 || ca > g.G[A] - 1) return;
         const int kk = (A == 2) ? ca : rr, jj = (A == 1) ? ca : rr;
         const size_t base = ((size_t)kk * g.G[1] + jj) * g.G[0];
+        if(xlo > xhi) return;
+        // the row segment holds cells xlo..xhi (at most 3): c1, c2 split it by cell
         const uint32_t b = __ldg(cellStart + base + xlo), e = __ldg(cellStart + base + xhi + 1);
+        const uint32_t c1 = __ldg(cellStart + base + min(xlo + 1, xhi + 1));
+        const uint32_t c2 = __ldg(cellStart + base + min(xlo + 2, xhi + 1));
+        // stencil bases on the row / column axes: the row's cell, or one less
+        const int sr0 = rr, sa0 = ca;
         // Particles are taken kBatch at a time: all loads first, then the arithmetic.  A
         // particle that does not reach an output adds +0 to its sums, which leaves them
         // unchanged (they start at +0 and can never become -0), so no branch is needed.
         for(uint32_t q0 = b; q0 < e; q0 += kBatch) {
-            float lx[kBatch], lr[kBatch], la[kBatch], lv[kBatch];
+            float4 L[kBatch];
+#pragma unroll
+            for(int w = 0; w < kBatch; ++w) L[w] = __ldg(recD + min(q0 + (uint32_t)w, e - 1u));
 #pragma unroll
             for(int w = 0; w < kBatch; ++w) {
-                const uint32_t q = min(q0 + (uint32_t)w, e - 1u);
-                lx[w] = __ldg(gxs + q);
-                lr[w] = __ldg(gR + q);
-                la[w] = __ldg(gA + q);
-                lv[w] = __ldg(vd + q);
-            }
-#pragma unroll
-            for(int w = 0; w < kBatch; ++w) {
-                int si, sr, sa;
-                float fi, fr, fa;
-                bary_c(lx[w] - (D == 0 ? 0.f : 0.5f), si, fi, sz[0]);
-                bary_c(lr[w] - (R == D ? 0.f : 0.5f), sr, fr, sz[R]);
-                bary_c(la[w] - 0.5f, sa, fa, sz[A]);
-                const bool reach = (q0 + (uint32_t)w < e) && (si == i || si == i - 1) && (sr == r || sr == r - 1);
+                const uint32_t q = q0 + (uint32_t)w;
+                const int cx = xlo + (q >= c1 ? 1 : 0) + (q >= c2 ? 1 : 0);
+                const float ex = L[w].x, ey = L[w].y, ez = L[w].z;
+                const float eR = (R == 1) ? ey : ez, eA = (A == 1) ? ey : ez;
+                // sign bit set: stencil base = cell - 1
+                const int si = cx + (__float_as_int(ex) >> 31);
+                const int sr = sr0 + (__float_as_int(eR) >> 31);
+                const int sa = sa0 + (__float_as_int(eA) >> 31);
+                const float fi = fabsf(ex), fr = fabsf(eR), fa = fabsf(eA);
+                const bool reach = (q < e) && (si == i || si == i - 1) && (sr == r || sr == r - 1);
                 const float wx = (si == i) ? (1.0f - fi) : fi;
                 const float wr = (sr == r) ? (1.0f - fr) : fr;
                 const float wxr = wx * wr;  // (wx * wy) when the column axis is z
@@ -142,7 +137,7 @@ __global__ void __launch_bounds__(kLx * kLr) k_p2g_col(GridDesc g, const DevStat
                     const float wa = (sa == fa_) ? (1.0f - fa) : fa;
                     // weight = wx * wy * wz, multiplied left to right
                     const float wgt = (A == 2) ? wxr * wa : (wx * wa) * wr;
-                    const float m = wgt * lv[w];
+                    const float m = wgt * L[w].w;
                     S[u] = S[u] + (ok ? m : 0.f);
                     W[u] = W[u] + (ok ? wgt : 0.f);
                 }
@@ -177,12 +172,7 @@ __global__ void __launch_bounds__(kLx * kLr) k_p2g_col(GridDesc g, const DevStat
 // into); the advection flags that case and the test is then made for every candidate.
 __global__ void __launch_bounds__(kLx * kLr) k_fluid_sdf_col(GridDesc g, const DevState* __restrict__ st,
                                                              const uint32_t* __restrict__ cellStart,
-                                                             const float* __restrict__ gxs,
-                                                             const float* __restrict__ gys,
-                                                             const float* __restrict__ gzs,
-                                                             const float* __restrict__ pxs,
-                                                             const float* __restrict__ pys,
-                                                             const float* __restrict__ pzs, float* __restrict__ phi) {
+                                                             const float4* __restrict__ pos, float* __restrict__ phi) {
     const int i = blockIdx.x * kLx + threadIdx.x;
     const int j = blockIdx.y * kLr + threadIdx.y;
     const int k0 = blockIdx.z * kCol;
@@ -201,12 +191,13 @@ __global__ void __launch_bounds__(kLx * kLr) k_fluid_sdf_col(GridDesc g, const D
         }
     }
     const bool exact = (st->flags & BNN_FLAG_OUT_OF_GRID) != 0u;
+    const float inf = __int_as_float(0x7f800000);
     // Grid::getWorldCoordinate(i + 0.5, j + 0.5, k + 0.5) (Grid.h:186-194)
     const float sxw = ((float)i + 0.5f) * g.dx + g.bmin[0];
     const float syw = ((float)j + 0.5f) * g.dx + g.bmin[1];
     float m[kCol];
 #pragma unroll
-    for(int u = 0; u < kCol; ++u) m[u] = __int_as_float(0x7f800000);  // +inf
+    for(int u = 0; u < kCol; ++u) m[u] = inf;
     const int xlo = max(i - 1, 0), xhi = min(i + 1, g.G[0] - 1);
     const int ylo = max(j - 1, 0), yhi = min(j + 1, g.G[1] - 1);
 #pragma unroll
@@ -215,28 +206,36 @@ __global__ void __launch_bounds__(kLx * kLr) k_fluid_sdf_col(GridDesc g, const D
         if(kk < 0 || kk > g.G[2] - 1) continue;
         for(int jj = ylo; jj <= yhi; ++jj) {
             const size_t base = ((size_t)kk * g.G[1] + jj) * g.G[0];
+            if(xlo > xhi) continue;
             const uint32_t b = __ldg(cellStart + base + xlo), e = __ldg(cellStart + base + xhi + 1);
-            for(uint32_t q = b; q < e; ++q) {
-                const float ddx = sxw - __ldg(pxs + q), ddy = syw - __ldg(pys + q);
-                const float pz = __ldg(pzs + q);
-                const float dxy = ddx * ddx + ddy * ddy;
-                int ck = 0;
-                if(exact) {
-                    // the particle's own cell and its clamped 3x3x3 range (PIC_Solver.cpp:633-635)
-                    const int ci = (int)__ldg(gxs + q), cj = (int)__ldg(gys + q);
-                    ck = (int)__ldg(gzs + q);
-                    if(i < max(ci - 1, 0) || i > min(ci + 1, g.G[0] - 1)) continue;
-                    if(j < max(cj - 1, 0) || j > min(cj + 1, g.G[1] - 1)) continue;
-                }
+            for(uint32_t q0 = b; q0 < e; q0 += kBatch) {
+                float4 L[kBatch];
 #pragma unroll
-                for(int du = -1; du <= 1; ++du) {
-                    const int u = t - 1 + du;
-                    if(u < 0 || u >= kCol) continue;
-                    const int k = k0 + u;
-                    if(exact && (k < max(ck - 1, 0) || k > min(ck + 1, g.G[2] - 1))) continue;
-                    const float ddz = (((float)k + 0.5f) * g.dx + g.bmin[2]) - pz;
-                    const float d2 = dxy + ddz * ddz;  // glm::length2: (x*x + y*y) + z*z
-                    m[u] = fminf(m[u], d2);
+                for(int w = 0; w < kBatch; ++w) L[w] = __ldg(pos + min(q0 + (uint32_t)w, e - 1u));
+#pragma unroll
+                for(int w = 0; w < kBatch; ++w) {
+                    const float ddx = sxw - L[w].x, ddy = syw - L[w].y;
+                    const float dxy = ddx * ddx + ddy * ddy;
+                    bool reach = q0 + (uint32_t)w < e;
+                    int ck = 0;
+                    if(exact) {
+                        // the particle's own cell (Grid::getGridCoordinate, truncated) and its
+                        // clamped 3x3x3 range (PIC_Solver.cpp:633-635)
+                        const int ci = (int)((L[w].x - g.bmin[0]) / g.dx), cj = (int)((L[w].y - g.bmin[1]) / g.dx);
+                        ck = (int)((L[w].z - g.bmin[2]) / g.dx);
+                        reach = reach && !(i < max(ci - 1, 0) || i > min(ci + 1, g.G[0] - 1)) &&
+                                !(j < max(cj - 1, 0) || j > min(cj + 1, g.G[1] - 1));
+                    }
+#pragma unroll
+                    for(int du = -1; du <= 1; ++du) {
+                        const int u = t - 1 + du;
+                        if(u < 0 || u >= kCol) continue;
+                        const int k = k0 + u;
+                        const bool ok = reach && !(exact && (k < max(ck - 1, 0) || k > min(ck + 1, g.G[2] - 1)));
+                        const float ddz = (((float)k + 0.5f) * g.dx + g.bmin[2]) - L[w].z;
+                        const float d2 = dxy + ddz * ddz;  // glm::length2: (x*x + y*y) + z*z
+                        m[u] = fminf(m[u], ok ? d2 : inf);
+                    }
                 }
             }
         }
@@ -246,7 +245,7 @@ __global__ void __launch_bounds__(kLx * kLr) k_fluid_sdf_col(GridDesc g, const D
         for(int u = 0; u < kCol; ++u) {
             if(k0 + u >= g.G[2]) continue;
             float ph = empty;
-            if(m[u] != __int_as_float(0x7f800000)) {
+            if(m[u] != inf) {
                 const float val = sqrtf(m[u]) - g.sdfRadius;
                 if(val < ph) ph = val;
             }
@@ -259,20 +258,19 @@ static dim3 col_grid(int sx, int sr, int sa) {
     return dim3((unsigned)((sx + kLx - 1) / kLx), (unsigned)((sr + kLr - 1) / kLr), (unsigned)((sa + kCol - 1) / kCol));
 }
 
-void launch_p2g_col(const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float* g3, const float* p6,
+void launch_p2g_col(const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float4* rec,
                     size_t stride, float* const* out, uint8_t* const* valid, cudaStream_t s) {
-    const float *gx = g3, *gy = g3 + stride, *gz = g3 + 2 * stride;
     const dim3 blk(kLx, kLr);
     // u, v: rows along y, columns along z; w: rows along z, columns along y
-    { k_p2g_col<0><<<col_grid(g.G[0] + 1, g.G[1], g.G[2]), blk, 0, s>>>(g, st, cellStart, gx, gy, gz, p6 + 3 * stride, out[0], valid[0]); bnn_note_launch(); }
-    { k_p2g_col<1><<<col_grid(g.G[0], g.G[1] + 1, g.G[2]), blk, 0, s>>>(g, st, cellStart, gx, gy, gz, p6 + 4 * stride, out[1], valid[1]); bnn_note_launch(); }
-    { k_p2g_col<2><<<col_grid(g.G[0], g.G[2] + 1, g.G[1]), blk, 0, s>>>(g, st, cellStart, gx, gy, gz, p6 + 5 * stride, out[2], valid[2]); bnn_note_launch(); }
+    { k_p2g_col<0><<<col_grid(g.G[0] + 1, g.G[1], g.G[2]), blk, 0, s>>>(g, st, cellStart, rec, stride, out[0], valid[0]); bnn_note_launch(); }
+    { k_p2g_col<1><<<col_grid(g.G[0], g.G[1] + 1, g.G[2]), blk, 0, s>>>(g, st, cellStart, rec, stride, out[1], valid[1]); bnn_note_launch(); }
+    { k_p2g_col<2><<<col_grid(g.G[0], g.G[2] + 1, g.G[1]), blk, 0, s>>>(g, st, cellStart, rec, stride, out[2], valid[2]); bnn_note_launch(); }
 }
 
-void launch_fluid_sdf_col(const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float* g3,
-                          const float* p6, size_t stride, float* phi, cudaStream_t s) {
-    { k_fluid_sdf_col<<<col_grid(g.G[0], g.G[1], g.G[2]), dim3(kLx, kLr), 0, s>>>(
-          g, st, cellStart, g3, g3 + stride, g3 + 2 * stride, p6, p6 + stride, p6 + 2 * stride, phi); bnn_note_launch(); }
+void launch_fluid_sdf_col(const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float4* rec,
+                          size_t stride, float* phi, cudaStream_t s) {
+    { k_fluid_sdf_col<<<col_grid(g.G[0], g.G[1], g.G[2]), dim3(kLx, kLr), 0, s>>>(g, st, cellStart, rec + 3 * stride,
+                                                                               phi); bnn_note_launch(); }
 }
 
 } // namespace bnn
