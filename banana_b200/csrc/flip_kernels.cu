@@ -369,50 +369,102 @@ __global__ void __launch_bounds__(256) k_p2g(GridDesc g, const uint32_t* __restr
 // ----------------------------------------------------------------------------------
 // Velocity extrapolation (one layer)
 // ----------------------------------------------------------------------------------
+// Face-index distance (Chebyshev, per axis beyond the box) of face (i,j,k) from the
+// occupied-cell bounding box; INT_MAX when there are no particles.  Faces of any component
+// that P2G or the pressure update make valid lie within distance 2: P2G reaches faces
+// c-1..c+1 of a particle's cell c, fluid cells (phi < 0) lie within one cell of a
+// particle, and a face touches the cells a and a-1 on its own axis.
+__device__ __forceinline__ int bbox_distance(const DevState* st, int i, int j, int k) {
+    const int c[3] = {i, j, k};
+    int o = 0;
+#pragma unroll
+    for(int d = 0; d < 3; ++d) {
+        const int lo = st->bbox[d], hi = st->bbox[3 + d];
+        if(hi < lo) return INT_MAX;
+        o = max(o, max(lo - c[d], c[d] - hi));
+    }
+    return o;
+}
+// Each extrapolation layer makes valid only faces next to valid ones, so after 4 layers
+// every valid face is within kExtFull of the box and faces farther than that never
+// change.  Layers therefore compute faces up to kExtFull, copy those up to kExtRegion
+// (the neighbours the computed faces read, kept defined in both ping-pong buffers) and
+// leave the rest alone: there the input is 0 and invalid and stays so.
+constexpr int kExtFull = 2 + 4;
+constexpr int kExtRegion = kExtFull + 2;
+
 // One layer of PIC_Solver::extrapolateVelocity (PIC_Solver.cpp:998-1089): an interior
 // face that was not valid takes the mean of its valid 6-neighbours (+x,-x,+y,-y,+z,-z
 // summation order) and becomes valid; everything reads the previous layer.
 // mode 0: plain layer.  mode 1 (last layer after P2G): also writes the FLIP backup
 // oldVels (FLIP_Data.h:48-52) and applies Earth gravity v -= 9.81*dt (PIC_Solver.cpp:
-// 505-511) to the v component.  mode 2 (last layer after projection): folds max|u| into
-// the CFL reduction (PIC_Solver.cpp:342-349).
+// 505-511) to the v component -- on every face, so faces beyond the region get the
+// backup 0 and the velocity 0 - gravityDt.  mode 2 (last layer after projection): folds
+// max|u| into the CFL reduction (PIC_Solver.cpp:342-349).
+// Block: 32 x 8 faces of one (x, y) slab.
 __global__ void __launch_bounds__(256) k_extrapolate(int sx, int sy, int sz, const float* __restrict__ gin,
                                                      const uint8_t* __restrict__ vin, float* __restrict__ gout,
                                                      uint8_t* __restrict__ vout, int mode, float* __restrict__ oldOut,
                                                      float gravityDt, DevState* st) {
-    const size_t nf = (size_t)sx * sy * sz;
-    const size_t f = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    float val = 0.f;
-    if(f < nf) {
-        const int i = (int)(f % sx);
-        const int j = (int)((f / sx) % sy);
-        const int k = (int)(f / ((size_t)sx * sy));
-        val = gin[f];
-        uint8_t vv = vin[f];
-        if(!vv && i > 0 && i < sx - 1 && j > 0 && j < sy - 1 && k > 0 && k < sz - 1) {
-            const size_t sxy = (size_t)sx * sy;
-            float sum = 0.f;
-            unsigned count = 0;
-            if(vin[f + 1]) { sum += gin[f + 1]; ++count; }
-            if(vin[f - 1]) { sum += gin[f - 1]; ++count; }
-            if(vin[f + sx]) { sum += gin[f + sx]; ++count; }
-            if(vin[f - sx]) { sum += gin[f - sx]; ++count; }
-            if(vin[f + sxy]) { sum += gin[f + sxy]; ++count; }
-            if(vin[f - sxy]) { sum += gin[f - sxy]; ++count; }
-            if(count > 0) { val = sum / (float)count; vv = 1; }
+    const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, k = blockIdx.z;
+    const bool live = i < sx && j < sy;
+    const size_t f = ((size_t)k * sy + j) * sx + i;
+    {
+        // the block's nearest face: per axis the nearer end of its index range
+        const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 8;
+        const int ob = max(bbox_distance(st, min(max(st->bbox[0], x0), x0 + 31), min(max(st->bbox[1], y0), y0 + 7), k),
+                           0);
+        if(ob > kExtRegion) {
+            // whole block beyond the region: only mode 1 writes anything there
+            if(mode == 1 && live) {
+                oldOut[f] = 0.f;
+                if(gravityDt != 0.f) gout[f] = 0.f - gravityDt;
+            }
+            return;
         }
-        vout[f] = vv;
-        if(mode == 1) {
-            oldOut[f] = val;
-            gout[f] = val - gravityDt;
+    }
+    float val = 0.f;
+    if(live) {
+        const int o = bbox_distance(st, i, j, k);
+        if(o > kExtRegion) {
+            if(mode == 1) {
+                oldOut[f] = 0.f;
+                if(gravityDt != 0.f) gout[f] = 0.f - gravityDt;
+            }
         } else {
-            gout[f] = val;
+            val = gin[f];
+            uint8_t vv = vin[f];
+            if(!vv && o <= kExtFull && i > 0 && i < sx - 1 && j > 0 && j < sy - 1 && k > 0 && k < sz - 1) {
+                const size_t sxy = (size_t)sx * sy;
+                float sum = 0.f;
+                unsigned count = 0;
+                if(vin[f + 1]) { sum += gin[f + 1]; ++count; }
+                if(vin[f - 1]) { sum += gin[f - 1]; ++count; }
+                if(vin[f + sx]) { sum += gin[f + sx]; ++count; }
+                if(vin[f - sx]) { sum += gin[f - sx]; ++count; }
+                if(vin[f + sxy]) { sum += gin[f + sxy]; ++count; }
+                if(vin[f - sxy]) { sum += gin[f - sxy]; ++count; }
+                if(count > 0) { val = sum / (float)count; vv = 1; }
+            }
+            vout[f] = vv;
+            if(mode == 1) {
+                oldOut[f] = val;
+                gout[f] = val - gravityDt;
+            } else {
+                gout[f] = val;
+            }
         }
     }
     if(mode == 2) {
-        __shared__ float sm[256];
-        float m = block_max_256(f < nf ? fabsf(val) : 0.f, sm);
-        if(threadIdx.x == 0 && m > 0.f) atomicMax(&st->maxvel_bits, __float_as_uint(m));
+        __shared__ float sm[8];
+        float m = fabsf(val);
+        for(int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
+        if(threadIdx.x == 0) sm[threadIdx.y] = m;
+        __syncthreads();
+        if(threadIdx.x == 0 && threadIdx.y == 0) {
+            for(int w = 1; w < 8; ++w) m = fmaxf(m, sm[w]);
+            if(m > 0.f) atomicMax(&st->maxvel_bits, __float_as_uint(m));
+        }
     }
 }
 
@@ -551,24 +603,24 @@ __global__ void k_build_rows(GridDesc g, int nrows, const uint32_t* __restrict__
 // ----------------------------------------------------------------------------------
 // PIC_Solver::updateProjectedVelocity (PIC_Solver.cpp:911-981), weights 1: face (i,j,k)
 // of component D between cells c- and c gets u -= dt*(p_c - p_c-)/max(0.01, theta) when
-// either cell is fluid and is marked valid; every other face is set to 0.
+// either cell is fluid and is marked valid; every other face is set to 0.  Fluid cells lie
+// within one cell of the occupied-cell box, so faces farther than 2 from it are set to 0
+// without reading anything.  Block: 32 x 8 faces of one (x, y) slab.
 template<int D>
-__global__ void __launch_bounds__(256) k_update_velocity(GridDesc g, const float* __restrict__ phi,
+__global__ void __launch_bounds__(256) k_update_velocity(GridDesc g, const DevState* __restrict__ st,
+                                                         const float* __restrict__ phi,
                                                          const uint32_t* __restrict__ aidx,
                                                          const float* __restrict__ pressure, float dt,
                                                          float* __restrict__ vel, uint8_t* __restrict__ valid) {
-    const int sx = g.G[0] + (D == 0), sy = g.G[1] + (D == 1), sz = g.G[2] + (D == 2);
-    const size_t nf = (size_t)sx * sy * sz;
-    const size_t f = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if(f >= nf) return;
-    const int i = (int)(f % sx);
-    const int j = (int)((f / sx) % sy);
-    const int k = (int)(f / ((size_t)sx * sy));
+    const int sx = g.G[0] + (D == 0), sy = g.G[1] + (D == 1);
+    const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, k = blockIdx.z;
+    if(i >= sx || j >= sy) return;
+    const size_t f = ((size_t)k * sy + j) * sx + i;
     const int a = D == 0 ? i : (D == 1 ? j : k);
     const int amax = g.G[D];
     float out = 0.f;
     uint8_t vv = 0;
-    if(a > 0 && a < amax) {
+    if(a > 0 && a < amax && bbox_distance(st, i, j, k) <= 2) {
         const size_t c = ((size_t)k * g.G[1] + j) * g.G[0] + i;
         const size_t step = D == 0 ? 1 : (D == 1 ? (size_t)g.G[0] : (size_t)g.G[0] * g.G[1]);
         const size_t cm = c - step;
@@ -798,8 +850,9 @@ void launch_extrapolate(const GridDesc& g, float* const* A, uint8_t* const* VA, 
             uint8_t* vout = (layer % 2 == 0) ? VB[d] : VA[d];
             int mode = layer == 3 ? lastMode : 0;
             float gdt = (mode == 1 && d == 1) ? gravityDt : 0.f;
-            { k_extrapolate<<<nblk(nf), 256, 0, s>>>(sx, sy, sz, gin, vin, gout, vout, mode, oldOut ? oldOut[d] : nullptr,
-                                                   gdt, st); bnn_note_launch(); }
+            const dim3 grid((unsigned)((sx + 31) / 32), (unsigned)((sy + 7) / 8), (unsigned)sz);
+            { k_extrapolate<<<grid, dim3(32, 8), 0, s>>>(sx, sy, sz, gin, vin, gout, vout, mode,
+                                                        oldOut ? oldOut[d] : nullptr, gdt, st); bnn_note_launch(); }
         }
     }
 }
@@ -821,14 +874,15 @@ void launch_build_rows(const GridDesc& g, int nrows, const uint32_t* rowCell, co
     { k_build_rows<<<nblk(nrows), 256, 0, s>>>(g, nrows, rowCell, phi, aidx, U[0], U[1], U[2], dt, rhs, diag, invdiag,
                                              nbr, st); bnn_note_launch(); }
 }
-void launch_update_velocity(const GridDesc& g, const float* phi, const uint32_t* aidx, const float* pressure, float dt,
-                            float* const* U, uint8_t* const* V, cudaStream_t s) {
-    size_t n0 = (size_t)face_sx(g, 0) * face_sy(g, 0) * face_sz(g, 0);
-    size_t n1 = (size_t)face_sx(g, 1) * face_sy(g, 1) * face_sz(g, 1);
-    size_t n2 = (size_t)face_sx(g, 2) * face_sy(g, 2) * face_sz(g, 2);
-    { k_update_velocity<0><<<nblk(n0), 256, 0, s>>>(g, phi, aidx, pressure, dt, U[0], V[0]); bnn_note_launch(); }
-    { k_update_velocity<1><<<nblk(n1), 256, 0, s>>>(g, phi, aidx, pressure, dt, U[1], V[1]); bnn_note_launch(); }
-    { k_update_velocity<2><<<nblk(n2), 256, 0, s>>>(g, phi, aidx, pressure, dt, U[2], V[2]); bnn_note_launch(); }
+void launch_update_velocity(const GridDesc& g, const DevState* st, const float* phi, const uint32_t* aidx,
+                            const float* pressure, float dt, float* const* U, uint8_t* const* V, cudaStream_t s) {
+    const dim3 blk(32, 8);
+    const dim3 g0((unsigned)((face_sx(g, 0) + 31) / 32), (unsigned)((face_sy(g, 0) + 7) / 8), (unsigned)face_sz(g, 0));
+    const dim3 g1((unsigned)((face_sx(g, 1) + 31) / 32), (unsigned)((face_sy(g, 1) + 7) / 8), (unsigned)face_sz(g, 1));
+    const dim3 g2((unsigned)((face_sx(g, 2) + 31) / 32), (unsigned)((face_sy(g, 2) + 7) / 8), (unsigned)face_sz(g, 2));
+    { k_update_velocity<0><<<g0, blk, 0, s>>>(g, st, phi, aidx, pressure, dt, U[0], V[0]); bnn_note_launch(); }
+    { k_update_velocity<1><<<g1, blk, 0, s>>>(g, st, phi, aidx, pressure, dt, U[1], V[1]); bnn_note_launch(); }
+    { k_update_velocity<2><<<g2, blk, 0, s>>>(g, st, phi, aidx, pressure, dt, U[2], V[2]); bnn_note_launch(); }
 }
 void launch_g2p(int n, const GridDesc& g, float* p6, size_t stride, const float* const* U, const float* const* O,
                 float ratio, int kind, float* C9, cudaStream_t s) {

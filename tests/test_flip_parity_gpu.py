@@ -36,7 +36,10 @@ def _pair(bnn, oracle_mod, n, **over):
     return g, o
 
 
-def _compare_step(g, o, step, fields=("u", "v", "w", "phi", "pressure")):
+_WHICH = {"u": 0, "v": 1, "w": 2, "phi": 3, "pressure": 4, "old_u": 5, "old_v": 6, "old_w": 7}
+
+
+def _compare_step(g, o, step, fields=("u", "v", "w", "phi", "pressure", "old_u", "old_v", "old_w")):
     sg = g.step()
     so = o.step()
     assert sg["dt"] == so["dt"], (step, sg["dt"], so["dt"])
@@ -44,8 +47,8 @@ def _compare_step(g, o, step, fields=("u", "v", "w", "phi", "pressure")):
     assert sg["pcg_iterations"] == so["pcg_iterations"], (step, sg["pcg_iterations"], so["pcg_iterations"])
     assert sg["pcg_success"] == so["pcg_success"] == 1, step
     for f in fields:
-        which = {"u": 0, "v": 1, "w": 2, "phi": 3, "pressure": 4}[f]
-        ok, err = _same(g.grid(f), o.grid(which))
+        which = _WHICH[f]
+        ok, err = _same(g.grid(which), o.grid(which))
         assert ok, f"step {step}: field {f} differs, max |diff| = {err}"
     pg, vg = g.get_particles()
     po, vo = o.get_particles()
