@@ -28,6 +28,9 @@ EXPORTS = [
     "bnn_flip_num_particles", "bnn_flip_get_grid", "bnn_flip_step", "bnn_flip_advance_frame",
     "bnn_flip_device_particles", "bnn_flip_step_host", "bnn_flip_stream", "bnn_cell_sort", "bnn_cell_sort_noalloc", "bnn_z_sort", "bnn_neighbors",
     "bnn_pcg_solve_7pt", "bnn_version", "bnn_last_error", "bnn_launch_count",
+    "bnn_flip_device_bytes", "bnn_scene_bytes_estimate",
+    "bnn_batch_create", "bnn_batch_destroy", "bnn_batch_add_scene", "bnn_batch_remove_scene", "bnn_batch_step",
+    "bnn_batch_scene_info", "bnn_batch_get_scene", "bnn_batch_memory",
 ]
 
 
@@ -56,6 +59,15 @@ class StepStats(C.Structure):
         ("n_active", C.c_uint32), ("outer_iterations", C.c_uint32), ("zero_phi_cells", C.c_uint32),
         ("stage_ms", C.c_float * 10), ("device_flags", C.c_uint32),
     ]
+
+
+class BatchParams(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("worker_threads", C.c_uint32)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("scenes", C.c_uint32), ("failed", C.c_uint32), ("particle_steps", C.c_uint64),
+                ("pcg_iterations", C.c_uint64), ("wall_ms", C.c_double), ("max_scene_ms", C.c_double)]
 
 
 class PcgStats(C.Structure):
@@ -100,6 +112,16 @@ def load() -> C.CDLL:
     L.bnn_neighbors.argtypes = [vp, C.c_uint32, C.c_float, vp, vp, C.c_uint64, u64p, vp]
     L.bnn_pcg_solve_7pt.argtypes = [C.c_uint32, fp, i32p, C.c_float, fp, C.c_float, C.c_uint32, C.c_int32, C.c_float,
                                     dp, C.POINTER(PcgStats)]
+    L.bnn_flip_device_bytes.argtypes = [vp, u64p]
+    L.bnn_scene_bytes_estimate.argtypes = [C.POINTER(Params), C.c_uint32, u64p]
+    L.bnn_batch_create.argtypes = [C.POINTER(BatchParams), C.POINTER(vp)]
+    L.bnn_batch_destroy.argtypes = [vp]
+    L.bnn_batch_add_scene.argtypes = [vp, C.POINTER(Params), fp, fp, C.c_uint32, u32p]
+    L.bnn_batch_remove_scene.argtypes = [vp, C.c_uint32]
+    L.bnn_batch_step.argtypes = [vp, C.POINTER(BatchStats)]
+    L.bnn_batch_scene_info.argtypes = [vp, C.c_uint32, u32p, u64p, C.POINTER(StepStats)]
+    L.bnn_batch_get_scene.argtypes = [vp, C.c_uint32, fp, fp]
+    L.bnn_batch_memory.argtypes = [vp, u64p, u64p]
     L.bnn_launch_count.argtypes = []
     L.bnn_launch_count.restype = C.c_uint64
     L.bnn_version.restype = C.c_char_p
@@ -265,3 +287,80 @@ def pcg_solve_7pt(diag, nbr, offdiag, rhs, tol, max_iter, mode="fp32", inner_tol
     if rc not in (BNN_OK, 3):
         raise BnnError(rc, "bnn_pcg_solve_7pt")
     return x[:n], {f: getattr(st, f) for f, _ in PcgStats._fields_}
+
+
+def scene_bytes_estimate(cfg: dict, n: int) -> int:
+    """Device bytes a scene with these parameters and n particles is expected to hold."""
+    b = C.c_uint64()
+    p = make_params(cfg)
+    check(load().bnn_scene_bytes_estimate(C.byref(p), int(n), C.byref(b)), "bnn_scene_bytes_estimate")
+    return int(b.value)
+
+
+class FlipBatch:
+    """Many independent scenes on one GPU (bnn_batch_*): every scene computes what a lone
+    FlipSolver computes; step() advances all of them by one sub-step."""
+
+    def __init__(self, hbm_budget_bytes: int = 0, worker_threads: int = 0):
+        self.L = load()
+        bp = BatchParams(int(hbm_budget_bytes), int(worker_threads))
+        h = C.c_void_p()
+        check(self.L.bnn_batch_create(C.byref(bp), C.byref(h)), "bnn_batch_create")
+        self.h = h
+        self.n = {}
+
+    def close(self):
+        if self.h:
+            self.L.bnn_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_scene(self, cfg: dict, pos, vel) -> int:
+        """Admit a scene; raises BnnError(CAPACITY) when it does not fit the budget."""
+        pos = np.ascontiguousarray(pos, np.float32)
+        vel = np.ascontiguousarray(vel, np.float32)
+        p = make_params(cfg)
+        sid = C.c_uint32()
+        check(self.L.bnn_batch_add_scene(self.h, C.byref(p), _p(pos, C.c_float), _p(vel, C.c_float), len(pos),
+                                         C.byref(sid)), "bnn_batch_add_scene")
+        self.n[sid.value] = len(pos)
+        return int(sid.value)
+
+    def remove_scene(self, sid: int) -> None:
+        check(self.L.bnn_batch_remove_scene(self.h, int(sid)), "bnn_batch_remove_scene")
+        self.n.pop(sid, None)
+
+    def step(self, allow_fail: bool = False) -> dict:
+        st = BatchStats()
+        rc = self.L.bnn_batch_step(self.h, C.byref(st))
+        if rc != BNN_OK and not allow_fail:
+            raise BnnError(rc, "bnn_batch_step")
+        return {f: getattr(st, f) for f, _ in BatchStats._fields_}
+
+    def scene_info(self, sid: int) -> dict:
+        n = C.c_uint32()
+        steps = C.c_uint64()
+        st = StepStats()
+        rc = self.L.bnn_batch_scene_info(self.h, int(sid), C.byref(n), C.byref(steps), C.byref(st))
+        d = {f: getattr(st, f) for f, _ in StepStats._fields_ if f != "stage_ms"}
+        d.update(n=int(n.value), steps=int(steps.value), status=int(rc))
+        return d
+
+    def get_scene(self, sid: int):
+        n = self.n[sid]
+        pos = np.zeros((max(n, 1), 3), np.float32)
+        vel = np.zeros((max(n, 1), 3), np.float32)
+        check(self.L.bnn_batch_get_scene(self.h, int(sid), _p(pos, C.c_float), _p(vel, C.c_float)),
+              "bnn_batch_get_scene")
+        return pos[:n], vel[:n]
+
+    def memory(self) -> tuple[int, int]:
+        a = C.c_uint64()
+        b = C.c_uint64()
+        check(self.L.bnn_batch_memory(self.h, C.byref(a), C.byref(b)), "bnn_batch_memory")
+        return int(a.value), int(b.value)

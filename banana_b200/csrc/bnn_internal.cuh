@@ -185,14 +185,18 @@ struct PcgWork {
     double* part = nullptr;
     float* partMaxF = nullptr;
     double* partMaxD = nullptr;
+    int4* rec = nullptr;  // packed grid rows
 };
 struct PcgOutcome {
     unsigned iterations = 0, outer = 0, success = 0;
     double residual = 0;
 };
-int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const float* invd, const int32_t* nbr, float dt,
-              int mode, float tol, unsigned maxIter, float innerTol, float outerTol, float* pressure, double* x64out,
-              DevState* dst, DevState* hst, cudaStream_t s, PcgOutcome& out);
+// gridRows: the x neighbours of every row are rows r-1 / r+1 (or none) and the y
+// neighbours lie within 65535 rows (rows of a grid in cell order, at most 65535 cells
+// along x); the solve then reads the packed 16-byte row records.
+int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const float* invd, const int32_t* nbr,
+              bool gridRows, float dt, int mode, float tol, unsigned maxIter, float innerTol, float outerTol,
+              float* pressure, double* x64out, DevState* dst, DevState* hst, cudaStream_t s, PcgOutcome& out);
 void pcg_release(PcgWork& w);
 
 } // namespace bnn

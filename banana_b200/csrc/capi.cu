@@ -195,6 +195,12 @@ extern "C" int bnn_flip_create(const bnn_params* params, bnn_flip** out) {
     h->frameTime = P.frame_duration;
     h->C = (size_t)h->g.G[0] * h->g.G[1] * h->g.G[2];
     if(h->C >= (size_t)0x7fffffff) { delete h; return BNN_ERR_NOT_SUPPORTED; }
+    if(h->g.G[0] > 65535) {
+        // the packed pressure rows store y-neighbour row distances in 16 bits
+        bnn_set_error("bnn_flip_create: more than 65535 cells along x");
+        delete h;
+        return BNN_ERR_NOT_SUPPORTED;
+    }
     for(int d = 0; d < 3; ++d) h->F[d] = (size_t)face_sx(h->g, d) * face_sy(h->g, d) * face_sz(h->g, d);
     cudaError_t e = cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking);
     if(e != cudaSuccess) { bnn_set_error(cudaGetErrorString(e)); delete h; return BNN_ERR_CUDA; }
@@ -237,6 +243,46 @@ extern "C" int bnn_flip_create(const bnn_params* params, bnn_flip** out) {
     if(rc == BNN_OK && P.max_particles) rc = reserve_particles(h, P.max_particles);
     if(rc != BNN_OK) { destroy_all(h); return rc; }
     *out = h;
+    return BNN_OK;
+}
+
+// Device bytes one handle holds, from its capacities (the allocations in bnn_flip_create,
+// reserve_particles, reserve_rows and pcg_reserve).
+static uint64_t device_bytes(const bnn_flip* h) {
+    uint64_t b = 0;
+    for(int d = 0; d < 3; ++d) b += (uint64_t)h->F[d] * 14u;                       // U, B, O + 2 valid
+    b += (uint64_t)h->C * 20u + 8u + scan_workspace_bytes(h->C);                   // count..aidx
+    const bool affine = h->P.solver_kind == BNN_SOLVER_APIC || h->P.solver_kind == BNN_SOLVER_AFLIP;
+    b += (uint64_t)h->cap * (168u + (affine ? 72u : 0u));                          // particle arrays
+    b += (uint64_t)h->rowCap * 44u;                                                // rows
+    b += (uint64_t)h->pcg.cap * (48u + (h->pcg.x64 ? 56u : 0u)) + (uint64_t)h->pcg.nchCap * 40u;
+    return b;
+}
+
+// Bytes a scene will hold (admission estimate before creating it): the grid arrays plus
+// the particle arrays for n particles, with one pressure row per particle (dense fluid
+// has one row per 8 particles; thin sheets and droplets approach one per particle).
+extern "C" int bnn_scene_bytes_estimate(const bnn_params* params, uint32_t n, uint64_t* bytes) {
+    if(!params || !bytes || !(params->cell_size > 0.f)) return BNN_ERR_INVALID_ARGUMENT;
+    uint64_t G[3];
+    for(int d = 0; d < 3; ++d) {
+        const float dx = params->cell_size, pad = dx * (float)params->n_expand_cells;
+        const float lo = params->box_min[d] - pad, hi = params->box_max[d] + pad;
+        G[d] = (uint64_t)std::ceil((hi - lo) / dx);
+    }
+    const uint64_t C = G[0] * G[1] * G[2];
+    const uint64_t F = (G[0] + 1) * G[1] * G[2] + G[0] * (G[1] + 1) * G[2] + G[0] * G[1] * (G[2] + 1);
+    const bool affine = params->solver_kind == BNN_SOLVER_APIC || params->solver_kind == BNN_SOLVER_AFLIP;
+    const bool fp64 = params->pcg_mode != BNN_PCG_FP32;
+    const uint64_t rows = n < C ? n : C;
+    *bytes = F * 14u + C * 24u + (uint64_t)n * (168u + (affine ? 72u : 0u)) + rows * 44u +
+             (rows * 5u / 4u + 4096u) * (48u + (fp64 ? 56u : 0u));
+    return BNN_OK;
+}
+
+extern "C" int bnn_flip_device_bytes(bnn_flip* h, uint64_t* bytes) {
+    if(!h || !bytes) return BNN_ERR_INVALID_ARGUMENT;
+    *bytes = device_bytes(h);
     return BNN_OK;
 }
 
@@ -414,7 +460,7 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st) {
                       h->dst, s);
     cudaEventRecord(h->ev[6], s);
     PcgOutcome po;
-    rc = pcg_solve(h->pcg, (int)nrows, h->rhs, h->diag, h->invd, h->nbr, substep, h->P.pcg_mode,
+    rc = pcg_solve(h->pcg, (int)nrows, h->rhs, h->diag, h->invd, h->nbr, true, substep, h->P.pcg_mode,
                    h->P.cg_relative_tolerance, h->P.max_cg_iteration, h->P.refine_inner_tolerance,
                    h->P.refine_tolerance, h->pressure, nullptr, h->dst, h->hst, s, po);
     if(rc != BNN_OK) return rc;
@@ -506,9 +552,30 @@ extern "C" int bnn_pcg_solve_7pt(uint32_t n, const float* diag, const int32_t* n
     cudaEventCreate(&e1);
     std::vector<float> inv(n);
     std::vector<int32_t> planes(6 * (size_t)n);
+    // rows of a grid in cell order (x neighbours r-1 / r+1, y neighbours within 65535 rows,
+    // z neighbours on their side) take the packed-record solve
+    bool gridRows = true;
     for(uint32_t r = 0; r < n; ++r) {
         inv[r] = diag[r] != 0.f ? 1.0f / diag[r] : 0.f;
-        for(int q = 0; q < 6; ++q) planes[(size_t)q * n + r] = nbr[6 * (size_t)r + q];
+        for(int q = 0; q < 6; ++q) {
+            const int32_t v = nbr[6 * (size_t)r + q];
+            if(v < -1 || (v >= 0 && (uint32_t)v >= n)) {
+                bnn_set_error("bnn_pcg_solve_7pt: neighbour index outside [-1, n)");
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                cudaStreamDestroy(s);
+                return BNN_ERR_INVALID_ARGUMENT;
+            }
+            planes[(size_t)q * n + r] = v;
+        }
+        const int64_t R = r;
+        const int32_t* nb = nbr + 6 * (size_t)r;
+        if(nb[2] >= 0 && nb[2] != R - 1) gridRows = false;
+        if(nb[3] >= 0 && nb[3] != R + 1) gridRows = false;
+        if(nb[1] >= 0 && !(nb[1] < R && R - nb[1] <= 65535)) gridRows = false;
+        if(nb[4] >= 0 && !(nb[4] > R && nb[4] - R <= 65535)) gridRows = false;
+        if(nb[0] >= 0 && !(nb[0] < R)) gridRows = false;
+        if(nb[5] >= 0 && !(nb[5] > R)) gridRows = false;
     }
     // the system stores -dt as the off-diagonal; recover dt so the kernels form -(1*dt)
     const float dt = -offdiag;
@@ -528,8 +595,8 @@ extern "C" int bnn_pcg_solve_7pt(uint32_t n, const float* diag, const int32_t* n
     PcgOutcome po;
     if(rc == BNN_OK) {
         cudaEventRecord(e0, s);
-        rc = pcg_solve(w, (int)n, dRhs, dDiag, dInv, dNbr, dt, mode, tol, max_iter, inner_tol, tol, dP, dX, dst, hst, s,
-                       po);
+        rc = pcg_solve(w, (int)n, dRhs, dDiag, dInv, dNbr, gridRows, dt, mode, tol, max_iter, inner_tol, tol, dP, dX,
+                       dst, hst, s, po);
         cudaEventRecord(e1, s);
     }
     if(rc == BNN_OK && n) chk(cudaMemcpyAsync(x_out, dX, n * 8, cudaMemcpyDeviceToHost, s));

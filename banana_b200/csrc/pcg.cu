@@ -6,17 +6,24 @@
 // as six planes nbr[q*n + r].  Every off-diagonal equals -dt (face weight 1), so the
 // matrix is never materialised.
 //
-// One iteration is two kernels, both in the canonical 2048-row chunk layout so their
-// FP64 dot products are bit-reproducible:
-//   spmv   : s = z + beta*s_old formed on the fly (double buffered), q = A s, partial s.q;
-//            the last block forms alpha = rho / (s.q)
-//   update : x += alpha s, r -= alpha q, max|r|, z = D^-1 r, partial z.r; the last block
-//            tests max|r| < tol*max|b| and forms beta
-// Scalars live in DevState; once `done` is set every later launch returns at once, so
-// the host can queue iterations in batches and only look at `done` between batches.
+// Rows of a grid (rows numbered in cell order) are also packed into one 16-byte record
+// each: the x neighbours are always rows r-1 / r+1, so they become two flag bits, the y
+// and z neighbours become row distances, and the diagonal rides along.  One load then
+// replaces seven, and the x neighbours' values come from the adjacent lanes by warp
+// shuffles instead of loads.  Record {y, zm, zp, diag}: y = dy- | dy+ << 16 (row distances
+// of the -y / +y neighbours, 0 = none), zm = dz- | (has -x) << 31, zp = dz+ | (has +x) << 31.
+//
+// The solve is one persistent cooperative kernel; every iteration works in the canonical
+// 2048-row chunk layout so the FP64 dot products are bit-reproducible:
+//   phase A: s = z + beta*s_old formed on the fly (double buffered), q = A s, partial s.q;
+//   grid barrier; every block reduces the partials to the same alpha;
+//   phase B: x += alpha s, r -= alpha q, max|r|, z = D^-1 r, partial z.r;
+//   grid barrier; every block reduces to the same rho, max|r| and beta.
 #include "bnn_internal.cuh"
 
+#include <condition_variable>
 #include <cstdio>
+#include <mutex>
 #include <vector>
 
 namespace bnn {
@@ -176,6 +183,7 @@ template<class VT> struct PcgArgs {
     const float* diag;
     const VT* invd;
     const int32_t* nbr;
+    const int4* rec;
     VT negoff;
     VT tolFactor;
     unsigned maxIter;
@@ -194,7 +202,7 @@ __device__ __forceinline__ VT s_val(const VT* z, const VT* sOld, VT beta, bool f
 #ifndef BNN_PCG_MIN_BLOCKS
 #define BNN_PCG_MIN_BLOCKS 4
 #endif
-template<class VT>
+template<class VT, bool PACKED>
 __global__ void __launch_bounds__(kLanes, BNN_PCG_MIN_BLOCKS) k_pcg_persistent(PcgArgs<VT> a) {
     __shared__ double smd[kLanes];
     __shared__ VT smv[kLanes];
@@ -210,7 +218,9 @@ __global__ void __launch_bounds__(kLanes, BNN_PCG_MIN_BLOCKS) k_pcg_persistent(P
     const VT* __restrict__ invdR = a.invd;
     const float* __restrict__ diagR = a.diag;
     const int32_t* __restrict__ nbrR = a.nbr;
+    const int4* __restrict__ recR = a.rec;
     const VT negoff = a.negoff;
+    const int lane = threadIdx.x & 31;
 
     // ---- init: r = rhs, x = 0, z = D^-1 r; partial z.r and max|r| (PCGSolver.cpp:151-168)
     for(int c = blockIdx.x; c < nch; c += nb) {
@@ -281,30 +291,55 @@ __global__ void __launch_bounds__(kLanes, BNN_PCG_MIN_BLOCKS) k_pcg_persistent(P
                 for(int u = 0; u < kRowGroup; ++u) {
                     const size_t e = base + (size_t)(g0 + u) * kLanes;
                     const size_t ee = e < (size_t)n ? e : 0;
+                    if constexpr(PACKED) {
+                        // a row past n reads row 0, whose neighbours are all valid rows
+                        const int4 rr = __ldg(recR + ee);
+                        const int dyM = rr.x & 0xffff, dyP = (int)((unsigned)rr.x >> 16);
+                        const int dzM = rr.y & 0x7fffffff, dzP = rr.z & 0x7fffffff;
+                        const int32_t r0 = (int32_t)ee;
+                        has[u][0] = dzM != 0; id[u][0] = r0 - dzM;
+                        has[u][1] = dyM != 0; id[u][1] = r0 - dyM;
+                        // x neighbours: lanes 0 / 31 load them, the others take a shuffle
+                        has[u][2] = rr.y < 0; id[u][2] = (lane == 0 && rr.y < 0) ? r0 - 1 : r0;
+                        has[u][3] = true; id[u][3] = r0;
+                        has[u][4] = rr.z < 0; id[u][4] = (lane == 31 && rr.z < 0) ? r0 + 1 : r0;
+                        has[u][5] = dyP != 0; id[u][5] = r0 + dyP;
+                        has[u][6] = dzP != 0; id[u][6] = r0 + dzP;
+                        dg[u] = __int_as_float(rr.w);
+                    } else {
 #pragma unroll
-                    for(int q = 0; q < 6; ++q) {
-                        const int32_t v = __ldg(nbrR + (size_t)q * n + ee);
-                        const int slot = q < 3 ? q : q + 1;
-                        has[u][slot] = v >= 0;
-                        id[u][slot] = v >= 0 ? v : (int32_t)ee;
+                        for(int q = 0; q < 6; ++q) {
+                            const int32_t v = __ldg(nbrR + (size_t)q * n + ee);
+                            const int slot = q < 3 ? q : q + 1;
+                            has[u][slot] = v >= 0;
+                            id[u][slot] = v >= 0 ? v : (int32_t)ee;
+                        }
+                        id[u][3] = (int32_t)ee;
+                        has[u][3] = true;
+                        dg[u] = __ldg(diagR + ee);
                     }
-                    id[u][3] = (int32_t)ee;
-                    has[u][3] = true;
-                    dg[u] = __ldg(diagR + ee);
                 }
                 VT zv[kRowGroup][7], sv[kRowGroup][7];
 #pragma unroll
                 for(int u = 0; u < kRowGroup; ++u)
 #pragma unroll
                     for(int q = 0; q < 7; ++q) {
-                        zv[u][q] = __ldcg(zR + id[u][q]);
-                        sv[u][q] = first ? VT(0) : __ldcg(sOld + id[u][q]);
+                        const bool load = !PACKED || (q != 2 && q != 4) || (q == 2 && lane == 0) || (q == 4 && lane == 31);
+                        zv[u][q] = load ? __ldcg(zR + id[u][q]) : VT(0);
+                        sv[u][q] = (first || !load) ? VT(0) : __ldcg(sOld + id[u][q]);
                     }
 #pragma unroll
                 for(int u = 0; u < kRowGroup; ++u) {
                     VT s7[7];
 #pragma unroll
                     for(int q = 0; q < 7; ++q) s7[q] = first ? zv[u][q] : zv[u][q] + beta * sv[u][q];
+                    if constexpr(PACKED) {
+                        // rows e-1 / e+1 belong to the neighbouring lanes of this warp
+                        const VT up = __shfl_up_sync(0xffffffffu, s7[3], 1);
+                        const VT dn = __shfl_down_sync(0xffffffffu, s7[3], 1);
+                        if(lane != 0) s7[2] = up;
+                        if(lane != 31) s7[4] = dn;
+                    }
                     VT t = VT(0);
 #pragma unroll
                     for(int q = 0; q < 3; ++q) if(has[u][q]) t += negoff * s7[q];
@@ -495,9 +530,59 @@ __global__ void k_d64_to_f32(int n, const double* __restrict__ a, float* __restr
     if(e < (size_t)n) b[e] = (float)a[e];
 }
 
+// Packs rows of a grid into the 16-byte records (layout at the top of this file).  The
+// caller guarantees the x neighbours are rows r-1 / r+1 and the y distances fit 16 bits.
+__global__ void k_pack_rows(int n, const float* __restrict__ diag, const int32_t* __restrict__ nbr,
+                            int4* __restrict__ rec) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if(r >= n) return;
+    int32_t nb[6];
+#pragma unroll
+    for(int q = 0; q < 6; ++q) nb[q] = nbr[(size_t)q * n + r];
+    const unsigned dyM = nb[1] >= 0 ? (unsigned)(r - nb[1]) : 0u, dyP = nb[4] >= 0 ? (unsigned)(nb[4] - r) : 0u;
+    const unsigned dzM = nb[0] >= 0 ? (unsigned)(r - nb[0]) : 0u, dzP = nb[5] >= 0 ? (unsigned)(nb[5] - r) : 0u;
+    int4 v;
+    v.x = (int)(dyM | (dyP << 16));
+    v.y = (int)(dzM | (nb[2] >= 0 ? 0x80000000u : 0u));
+    v.z = (int)(dzP | (nb[3] >= 0 ? 0x80000000u : 0u));
+    v.w = __float_as_int(diag[r]);
+    rec[r] = v;
+}
+
 // ---------------------------------------------------------------------------------
 // Host driver
 // ---------------------------------------------------------------------------------
+
+// Process-wide record of the cooperative PCG kernels: SM count, resident blocks per SM of
+// each variant, and the share of the GPU held by solves in flight.  A share is counted
+// in units of 1/840 SM (840 is divisible by every resident-block count 1..8).
+constexpr int kShareUnits = 840;
+struct CoopState {
+    std::mutex mu;
+    std::condition_variable cv;
+    int numSM = 0;
+    int perSM[4] = {0, 0, 0, 0};
+    long long held = 0;
+};
+static CoopState g_coop;
+
+// Holds `units` of the GPU for the lifetime of the object; waits while other solves hold
+// so much that this grid would not fit beside them.
+struct CoopShare {
+    long long units;
+    CoopShare(long long u, long long capacity) : units(u < capacity ? u : capacity) {
+        std::unique_lock<std::mutex> lk(g_coop.mu);
+        g_coop.cv.wait(lk, [&] { return g_coop.held + units <= capacity; });
+        g_coop.held += units;
+    }
+    ~CoopShare() {
+        {
+            std::lock_guard<std::mutex> lk(g_coop.mu);
+            g_coop.held -= units;
+        }
+        g_coop.cv.notify_all();
+    }
+};
 
 int pcg_reserve(PcgWork& w, int n, bool fp64) {
     if(n <= w.cap && (!fp64 || w.x64)) return BNN_OK;
@@ -514,6 +599,7 @@ int pcg_reserve(PcgWork& w, int n, bool fp64) {
         BNN_CUDA_CHECK(cudaMalloc(&w.q, cap * sizeof(float)));
         BNN_CUDA_CHECK(cudaMalloc(&w.d32, cap * sizeof(float)));
         BNN_CUDA_CHECK(cudaMalloc(&w.r32, cap * sizeof(float)));
+        BNN_CUDA_CHECK(cudaMalloc(&w.rec, cap * sizeof(int4)));
         BNN_CUDA_CHECK(cudaMalloc(&w.part, 3 * nch * sizeof(double)));
         BNN_CUDA_CHECK(cudaMalloc(&w.gs, sizeof(GridSync)));
         BNN_CUDA_CHECK(cudaMemset(w.gs, 0, sizeof(GridSync)));
@@ -534,7 +620,7 @@ int pcg_reserve(PcgWork& w, int n, bool fp64) {
 }
 
 void pcg_release(PcgWork& w) {
-    for(void* p : {(void*)w.x, (void*)w.r, (void*)w.z, (void*)w.s0, (void*)w.s1, (void*)w.q, (void*)w.d32, (void*)w.r32,
+    for(void* p : {(void*)w.rec, (void*)w.x, (void*)w.r, (void*)w.z, (void*)w.s0, (void*)w.s1, (void*)w.q, (void*)w.d32, (void*)w.r32,
                    (void*)w.part, (void*)w.partMaxF, (void*)w.partMaxD, (void*)w.x64, (void*)w.r64, (void*)w.z64,
                    (void*)w.s064, (void*)w.s164, (void*)w.q64, (void*)w.inv64, (void*)w.gs})
         if(p) cudaFree(p);
@@ -545,33 +631,42 @@ void pcg_release(PcgWork& w) {
 // the solution is left in x.
 template<class VT>
 static int pcg_solve_t(PcgWork& w, int n, const float* rhsF, const float* diag, const VT* invd, const int32_t* nbr,
-                       VT negoff, VT tolFactor, unsigned maxIter, VT* x, VT* r, VT* z, VT* s0, VT* s1, VT* q,
+                       const int4* rec, VT negoff, VT tolFactor, unsigned maxIter, VT* x, VT* r, VT* z, VT* s0, VT* s1, VT* q,
                        VT* partMax, DevState* dst, DevState* hst, cudaStream_t s, PcgOutcome& out) {
     out = PcgOutcome();
     if(n == 0) { out.success = 1; return BNN_OK; }
     const int nch = (n + kChunk - 1) / kChunk;
-    static int numSM = 0, perSM[2] = {0, 0};
-    const int ti = sizeof(VT) == 8 ? 1 : 0;
-    if(!numSM) {
-        int dev = 0;
-        BNN_CUDA_CHECK(cudaGetDevice(&dev));
-        BNN_CUDA_CHECK(cudaDeviceGetAttribute(&numSM, cudaDevAttrMultiProcessorCount, dev));
+    const int ti = (sizeof(VT) == 8 ? 1 : 0) + (rec ? 2 : 0);
+    const void* kern = rec ? (const void*)k_pcg_persistent<VT, true> : (const void*)k_pcg_persistent<VT, false>;
+    int numSM = 0, perSMv = 0;
+    {
+        std::lock_guard<std::mutex> lk(g_coop.mu);
+        if(!g_coop.numSM) {
+            int dev = 0;
+            BNN_CUDA_CHECK(cudaGetDevice(&dev));
+            BNN_CUDA_CHECK(cudaDeviceGetAttribute(&g_coop.numSM, cudaDevAttrMultiProcessorCount, dev));
+        }
+        if(!g_coop.perSM[ti]) {
+            BNN_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_coop.perSM[ti], kern, kLanes, 0));
+            if(g_coop.perSM[ti] < 1) { bnn_set_error("persistent PCG kernel cannot be resident"); return BNN_ERR_CUDA; }
+        }
+        numSM = g_coop.numSM;
+        perSMv = g_coop.perSM[ti];
     }
-    if(!perSM[ti]) {
-        BNN_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM[ti], k_pcg_persistent<VT>, kLanes, 0));
-        if(perSM[ti] < 1) { bnn_set_error("persistent PCG kernel cannot be resident"); return BNN_ERR_CUDA; }
-    }
-    const int cap = numSM * perSM[ti];
+    const int cap = numSM * perSMv;
     const int perBlock = (nch + cap - 1) / cap;           // chunks per block
     const int grid = (nch + perBlock - 1) / perBlock;     // balanced: every block the same count
     PcgArgs<VT> a;
-    a.n = n; a.rhsF = rhsF; a.diag = diag; a.invd = invd; a.nbr = nbr; a.negoff = negoff; a.tolFactor = tolFactor;
+    a.n = n; a.rhsF = rhsF; a.diag = diag; a.invd = invd; a.nbr = nbr; a.rec = rec; a.negoff = negoff; a.tolFactor = tolFactor;
     a.maxIter = maxIter; a.x = x; a.r = r; a.z = z; a.s0 = s0; a.s1 = s1; a.q = q;
     a.part0 = w.part; a.part1 = w.part + w.nchCap; a.part2 = w.part + 2 * (size_t)w.nchCap; a.partMax = partMax;
     a.st = dst; a.gs = w.gs;
     BNN_CUDA_CHECK(cudaMemsetAsync(&w.gs->count, 0, sizeof(unsigned), s));
     void* args[] = {&a};
-    BNN_CUDA_CHECK(cudaLaunchCooperativeKernel((const void*)k_pcg_persistent<VT>, dim3(grid), dim3(kLanes), args, 0, s));
+    // grids of concurrent solves (several solver handles on several host threads) must
+    // fit the GPU together, or blocks of one could wait for SMs held by another's barrier
+    CoopShare share(grid * (kShareUnits / perSMv), numSM * kShareUnits);
+    BNN_CUDA_CHECK(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kLanes), args, 0, s));
     bnn_note_launch();
     BNN_CUDA_CHECK(cudaMemcpyAsync(hst, dst, sizeof(DevState), cudaMemcpyDeviceToHost, s));
     BNN_CUDA_CHECK(cudaStreamSynchronize(s));
@@ -583,16 +678,21 @@ static int pcg_solve_t(PcgWork& w, int n, const float* rhsF, const float* diag, 
 }
 
 // mode: BNN_PCG_FP32 / FP64 / REFINED.  Pressure written to `pressure` (float, n).
-int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const float* invd, const int32_t* nbr, float dt,
-              int mode, float tol, unsigned maxIter, float innerTol, float outerTol, float* pressure, double* x64out,
-              DevState* dst, DevState* hst, cudaStream_t s, PcgOutcome& out) {
+int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const float* invd, const int32_t* nbr,
+              bool gridRows, float dt, int mode, float tol, unsigned maxIter, float innerTol, float outerTol,
+              float* pressure, double* x64out, DevState* dst, DevState* hst, cudaStream_t s, PcgOutcome& out) {
     int rc = pcg_reserve(w, n, mode != BNN_PCG_FP32);
     if(rc != BNN_OK) return rc;
     const unsigned nb = (unsigned)((n + 255) / 256);
     const unsigned nch = (unsigned)((n + kChunk - 1) / kChunk);
     out = PcgOutcome();
+    const int4* rec = nullptr;
+    if(gridRows && n > 0) {
+        { k_pack_rows<<<nb, 256, 0, s>>>(n, diag, nbr, w.rec); bnn_note_launch(); }
+        rec = w.rec;
+    }
     if(mode == BNN_PCG_FP32) {
-        rc = pcg_solve_t<float>(w, n, rhs, diag, invd, nbr, -(1.0f * dt), tol, maxIter, w.x, w.r, w.z, w.s0, w.s1,
+        rc = pcg_solve_t<float>(w, n, rhs, diag, invd, nbr, rec, -(1.0f * dt), tol, maxIter, w.x, w.r, w.z, w.s0, w.s1,
                                 w.q, w.partMaxF, dst, hst, s, out);
         if(rc != BNN_OK) return rc;
         if(n > 0) BNN_CUDA_CHECK(cudaMemcpyAsync(pressure, w.x, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
@@ -601,7 +701,7 @@ int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const floa
     }
     if(mode == BNN_PCG_FP64) {
         if(n > 0) { k_inv_diag64<<<nb, 256, 0, s>>>(n, diag, w.inv64); bnn_note_launch(); }
-        rc = pcg_solve_t<double>(w, n, rhs, diag, w.inv64, nbr, -(double)(1.0f * dt), (double)tol, maxIter, w.x64,
+        rc = pcg_solve_t<double>(w, n, rhs, diag, w.inv64, nbr, rec, -(double)(1.0f * dt), (double)tol, maxIter, w.x64,
                                  w.r64, w.z64, w.s064, w.s164, w.q64, w.partMaxD, dst, hst, s, out);
         if(rc != BNN_OK) return rc;
         if(n > 0) { k_d64_to_f32<<<nb, 256, 0, s>>>(n, w.x64, pressure); bnn_note_launch(); }
@@ -623,7 +723,7 @@ int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const floa
         if(res < (double)outerTol * bmax) { ok = true; break; }
         { k_ir_to_f32<<<nb, 256, 0, s>>>(n, w.r64, w.r32); bnn_note_launch(); }
         PcgOutcome inner;
-        rc = pcg_solve_t<float>(w, n, w.r32, diag, invd, nbr, -(1.0f * dt), innerTol, maxIter, w.d32, w.r, w.z, w.s0,
+        rc = pcg_solve_t<float>(w, n, w.r32, diag, invd, nbr, rec, -(1.0f * dt), innerTol, maxIter, w.d32, w.r, w.z, w.s0,
                                 w.s1, w.q, w.partMaxF, dst, hst, s, inner);
         if(rc != BNN_OK) return rc;
         total += inner.iterations;

@@ -138,3 +138,31 @@ def batch_scene_specs(n_scenes: int = 256, seed: int = 11, choices=(32, 48, 64, 
         frac = tuple(float(0.2 + 0.4 * r[3 + a]) for a in range(3))
         specs.append({"res": res, "block_frac": frac, "seed": seed * 100003 + s})
     return specs
+
+
+def batch_scene(spec: dict, ppc: int = 8, pcg_mode: int = 2, **over):
+    """Parameters and particles of one batch scene (batch_scene_specs / serve_requests):
+    domain [0, res/64] per axis with cell size 1/64, a dam-break block of block_frac of
+    the domain anchored at the origin, `ppc` particles per cell, refined FP32 PCG."""
+    dx = 1.0 / 64.0
+    res = spec["res"]
+    ext = tuple(r * dx for r in res)
+    block = tuple(f * e for f, e in zip(spec["block_frac"], ext))
+    cfg = dam_break_params(64, box_max=ext, pcg_mode=pcg_mode, **over)
+    pos, vel = dam_break(64, block=block, ppc=ppc, seed=spec["seed"], cell_size=dx)
+    return cfg, pos, vel
+
+
+def serve_requests(n_requests: int, rate: float = 20.0, seed: int = 13, n_min: int = 32, n_max: int = 192):
+    """Request stream of the serving workload: Poisson arrivals (exponential gaps, mean
+    1/rate seconds), each a cubic scene whose resolution is log-uniform in
+    [n_min, n_max] (rounded), block extents uniform in [0.2, 0.6] of the domain."""
+    reqs = []
+    t = 0.0
+    for q in range(n_requests):
+        r = uniform01(seed, 2, np.arange(q * 8, q * 8 + 8, dtype=np.int64))
+        t += -math.log1p(-r[0]) / rate
+        n = int(round(math.exp(math.log(n_min) + r[1] * (math.log(n_max) - math.log(n_min)))))
+        frac = tuple(float(0.2 + 0.4 * r[2 + a]) for a in range(3))
+        reqs.append({"t": t, "res": (n, n, n), "block_frac": frac, "seed": seed * 100003 + q})
+    return reqs

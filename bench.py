@@ -10,6 +10,14 @@ PCG iteration), so per-GPU work is fixed and `scaling` is "weak".  The timed reg
 bracketed by a barrier and a device synchronize on both sides and timed with CUDA events
 on the stream the solver launches on; the job time is the max over ranks.
 
+Other workloads (`--workload`, one JSON line each, not the headline):
+  batch   256 independent dam-break scenes (seed 11, 32..128 cells per axis), refined
+          FP32 PCG, one sub-step of every scene per step; scenes are split over ranks
+          (`scaling` strong).  Reports step-latency p50/p99.
+  serve   Poisson request stream (20/s, seed 13, cubic 32..192 cells), 200 sub-steps per
+          request, 150 GB admission budget; reports request- and step-latency p50/p99.
+  nsearch 4M-point cell sort + neighbour lists (r = 0.01, seed 7).
+
 `--impl reference` times the reference's CPU algorithm (the oracle port of PIC_Solver /
 FLIP_Solver / PCGSolver, reference arithmetic order, OpenMP over all host cores) on the
 same workload; under torchrun only rank 0 runs it.
@@ -35,6 +43,9 @@ N_GRID = 256
 METRIC = "particle-steps/s at 256^3 FLIP (1e-6 rel residual)"
 UNIT = "particle-steps/s"
 WORKLOAD = "flip_dam_break_256"
+# DRAM bytes (read + write) of one k_pcg_persistent launch, from the ncu capture summarised
+# in profiles/ (None until captured for the current kernel)
+PCG_TRAFFIC = None
 
 
 def _config(pcg_mode: str):
@@ -225,7 +236,7 @@ def run_ours(args, ws, rank, local):
     stage_tot = {k: sum(s["stage_ms"][k] for s in stats) for k in capi.STAGES}
     iters = sum(s["pcg_iterations"] for s in stats)
     rows = [s["n_active"] for s in stats]
-    pcg_bytes = sum(76.0 * s["n_active"] * s["pcg_iterations"] for s in stats)
+    pcg_bytes = sum(52.0 * s["n_active"] * s["pcg_iterations"] for s in stats)
     peak, peak_kind = _peaks()
     pcg_ms = stage_tot["pcg"]
     achieved = pcg_bytes / (pcg_ms * 1e-3) / 1e9 if pcg_ms > 0 else 0.0
@@ -274,10 +285,11 @@ def run_ours(args, ws, rank, local):
             "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded dam break, seed 42)",
             "config": dict(_config(pcg_mode), particles=npart),
-            "roofline": {"bound": "hbm", "kernel": "PCG iteration (k_pcg_spmv + k_pcg_update)",
+            "roofline": {"bound": "hbm", "kernel": "k_pcg_persistent (whole Jacobi PCG solve, one launch per step)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
-                         "algorithmic_bytes": "76 B per active row per iteration", "traffic": None},
+                         "algorithmic_bytes": "52 B per active row per PCG iteration (x, r, z, s, q, 1/diag and "
+                                              "the row's matrix data once each)", "traffic": PCG_TRAFFIC},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clk,
             "detail": {"pcg_iterations_per_step": iters / args.steps, "active_rows_mean": float(np.mean(rows)),
@@ -286,6 +298,221 @@ def run_ours(args, ws, rank, local):
         }
         print(json.dumps(line), flush=True)
     solver.close()
+    if ws > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def _torch_dist(ws, local):
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if ws > 1:
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local),
+                                timeout=__import__("datetime").timedelta(seconds=300))
+    return torch, dist
+
+
+def run_batch(args, ws, rank, local):
+    """256 independent scenes on the GPU(s), one sub-step of each per step."""
+    torch, dist = _torch_dist(ws, local)
+    from banana_b200 import FlipBatch, capi, dist as bdist, scenes
+
+    specs = scenes.batch_scene_specs()
+    costs = []
+    for s in specs:
+        cells = [int(np.floor(f * r + 1e-9)) for f, r in zip(s["block_frac"], s["res"])]
+        costs.append(bdist.scene_bytes_per_step(s["res"], 8 * cells[0] * cells[1] * cells[2]))
+    mine = bdist.shard_scenes(costs, ws)[rank]
+    b = FlipBatch(worker_threads=args.workers)
+    built = [scenes.batch_scene(specs[i]) for i in mine]
+    npart = sum(len(p) for _, p, _ in built)
+    t_up = time.perf_counter()
+    ids = [b.add_scene(cfg, pos, vel) for cfg, pos, vel in built]
+    t_up = time.perf_counter() - t_up
+    for _ in range(args.warmup):
+        b.step()
+    clocks = ClockSampler(local)
+    clocks.start()
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = capi.launch_count()
+    lat, ps, iters = [], 0, 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        st = b.step()
+        lat.append(st["wall_ms"])
+        ps += st["particle_steps"]
+        iters += st["pcg_iterations"]
+    torch.cuda.synchronize()
+    te = time.perf_counter() - t0
+    t_dl = time.perf_counter()
+    for sid in ids:
+        b.get_scene(sid)
+    t_dl = time.perf_counter() - t_dl
+    clk = clocks.stop()
+    launches = capi.launch_count() - launches0
+    tot_ps = ps
+    t_max = te
+    e2e_t = te + t_up + t_dl
+    if ws > 1:
+        v = torch.tensor([ps], dtype=torch.float64, device="cuda")
+        dist.all_reduce(v)
+        tot_ps = float(v.item())
+        t = torch.tensor([te, e2e_t], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max, e2e_t = (float(x) for x in t.tolist())
+    if rank == 0:
+        line = {"metric": "particle-steps/s, 256 batched dam-break scenes", "value": tot_ps / t_max,
+                "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True, "scaling": "strong",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scenes, seed 11)",
+                "config": {"workload": "batch_256_scenes", "scenes": len(specs), "scenes_rank0": len(mine),
+                           "particles_rank0": npart, "res_choices": [32, 48, 64, 96, 128], "cell_size": "1/64",
+                           "pcg": "Jacobi, refined FP32 inner / FP64 outer to 1e-8, inner 1e-3",
+                           "worker_threads": args.workers or "min(16, cores)", "parallelism": f"scenes/{ws} ranks"},
+                "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+                "e2e": {"value": tot_ps / e2e_t, "unit": UNIT, "h2d_bytes_per_step": 24 * npart / args.steps,
+                        "d2h_bytes_per_step": 24 * npart / args.steps,
+                        "api": "bnn_batch_add_scene (upload) + steps + bnn_batch_get_scene (download), wall clock"},
+                "gpu_launches": int(launches), "clocks": clk,
+                "detail": {"pcg_iterations_per_step": iters / args.steps, "timing": "host wall clock per batch step"}}
+        print(json.dumps(line), flush=True)
+    b.close()
+    if ws > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def run_serve(args, ws, rank, local):
+    """Poisson request stream: each request is a scene that runs 200 sub-steps."""
+    torch, dist = _torch_dist(ws, local)
+    from banana_b200 import BnnError, FlipBatch, capi, scenes
+
+    reqs = scenes.serve_requests(args.requests)
+    mine = [q for k, q in enumerate(reqs) if k % ws == rank]
+    budget = int(150e9)
+    b = FlipBatch(hbm_budget_bytes=budget, worker_threads=args.workers)
+    steps_per_req = args.req_steps
+    queue = list(mine)
+    live = {}
+    done_lat, step_lat = [], []
+    ps = 0
+    launches0 = capi.launch_count()
+    clocks = ClockSampler(local)
+    clocks.start()
+    t0 = time.perf_counter()
+    while queue or live:
+        now = time.perf_counter() - t0
+        if now > args.time_limit:
+            break  # bounded run: report what completed
+        while queue and queue[0]["t"] <= now:
+            q = queue[0]
+            cfg, pos, vel = scenes.batch_scene(q)
+            try:
+                sid = b.add_scene(cfg, pos, vel)
+            except BnnError as e:
+                if e.code != 8:
+                    raise
+                break  # over budget: wait for a running request to finish
+            live[sid] = q
+            queue.pop(0)
+        if not live:
+            time.sleep(max(0.0, min(queue[0]["t"] - now, 0.05)))
+            continue
+        st = b.step()
+        step_lat.append(st["wall_ms"])
+        ps += st["particle_steps"]
+        for sid in list(live):
+            if b.scene_info(sid)["steps"] >= steps_per_req:
+                b.get_scene(sid)
+                done_lat.append(time.perf_counter() - t0 - live[sid]["t"])
+                b.remove_scene(sid)
+                del live[sid]
+    te = time.perf_counter() - t0
+    clk = clocks.stop()
+    launches = capi.launch_count() - launches0
+    tot = ps
+    if ws > 1:
+        v = torch.tensor([ps], dtype=torch.float64, device="cuda")
+        dist.all_reduce(v)
+        tot = float(v.item())
+        t = torch.tensor([te], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        te = float(t.item())
+    if rank == 0:
+        line = {"metric": "served particle-steps/s, Poisson dam-break requests", "value": tot / te, "unit": UNIT,
+                "n_gpus": ws, "steps": len(step_lat), "warmup": 0, "ms_per_step": float(np.mean(step_lat)),
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded request stream, seed 13)",
+                "config": {"workload": "serve_poisson", "requests": len(reqs), "rate_per_s": 20,
+                           "res": "cubic, log-uniform 32..192", "steps_per_request": steps_per_req,
+                           "hbm_budget_gb": 150, "pcg": "refined FP32 to 1e-8", "parallelism": f"requests/{ws} ranks"},
+                "completed_requests": len(done_lat),
+                "request_latency_s": {"p50": float(np.percentile(done_lat, 50)) if done_lat else None,
+                                      "p99": float(np.percentile(done_lat, 99)) if done_lat else None},
+                "step_latency_ms": {"p50": float(np.percentile(step_lat, 50)), "p99": float(np.percentile(step_lat, 99))},
+                "gpu_launches": int(launches), "clocks": clk}
+        print(json.dumps(line), flush=True)
+    b.close()
+    if ws > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def run_nsearch(args, ws, rank, local):
+    """4M points: cell sort (bit-exact ids + sorted index) and CSR neighbour lists."""
+    import ctypes as C
+
+    torch, dist = _torch_dist(ws, local)
+    from banana_b200 import capi, scenes
+
+    L = capi.load()
+    pts = scenes.point_cloud(4_000_000, seed=7)
+    n = len(pts)
+    r = np.float32(0.01)
+    dev = torch.from_numpy(pts).cuda()
+    cid = torch.empty(n, dtype=torch.int32, device="cuda")
+    srt = torch.empty(n, dtype=torch.int32, device="cuda")
+    nc = (C.c_int32 * 3)(100, 100, 100)
+    bmin = (C.c_float * 3)(0.0, 0.0, 0.0)
+    oor = C.c_uint32()
+    off = torch.empty(n + 1, dtype=torch.int64, device="cuda")
+    total = C.c_uint64()
+    cap = 1_200_000_000
+    idx = torch.empty(cap, dtype=torch.int32, device="cuda")
+    s = torch.cuda.current_stream()
+    sp = C.c_void_p(s.cuda_stream)
+
+    def once():
+        capi.check(L.bnn_cell_sort(C.c_void_p(dev.data_ptr()), n, bmin, C.c_float(0.01), nc, C.c_void_p(cid.data_ptr()),
+                                   C.c_void_p(srt.data_ptr()), None, C.byref(oor), sp), "bnn_cell_sort")
+        capi.check(L.bnn_neighbors(C.c_void_p(dev.data_ptr()), n, C.c_float(r), C.c_void_p(off.data_ptr()),
+                                   C.c_void_p(idx.data_ptr()), cap, C.byref(total), sp), "bnn_neighbors")
+
+    for _ in range(args.warmup):
+        once()
+    torch.cuda.synchronize()
+    launches0 = capi.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(args.steps):
+        once()
+    e1.record(s)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    launches = capi.launch_count() - launches0
+    if rank == 0:
+        line = {"metric": "points/s, 4M-point cell sort + neighbour lists (r = 0.01)", "value": n / (ms * 1e-3),
+                "unit": "points/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "replicas", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (2M uniform + 2M in 16 Gaussians, sigma 0.03, seed 7)",
+                "config": {"workload": "nsearch_4m", "points": n, "radius": 0.01, "grid": "100^3"},
+                "neighbour_entries": int(total.value),
+                "entries_per_s": int(total.value) / (ms * 1e-3), "gpu_launches": int(launches)}
+        print(json.dumps(line), flush=True)
     if ws > 1:
         dist.destroy_process_group()
     return 0
@@ -302,11 +529,22 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--grid", type=int, default=N_GRID, help="fluid-domain resolution (profiling of smaller cases)")
+    ap.add_argument("--workload", choices=["flip", "batch", "serve", "nsearch"], default="flip")
+    ap.add_argument("--workers", type=int, default=0, help="batch/serve: host threads stepping scenes (0 = auto)")
+    ap.add_argument("--requests", type=int, default=100, help="serve: number of requests")
+    ap.add_argument("--req-steps", type=int, default=200, help="serve: sub-steps per request")
+    ap.add_argument("--time-limit", type=float, default=240.0, help="serve: stop after this many seconds")
     args = ap.parse_args()
     ws, rank, local = _dist()
     N_GRID = args.grid
     if args.impl == "reference":
         return run_reference(args, ws, rank)
+    if args.workload == "batch":
+        return run_batch(args, ws, rank, local)
+    if args.workload == "serve":
+        return run_serve(args, ws, rank, local)
+    if args.workload == "nsearch":
+        return run_nsearch(args, ws, rank, local)
     return run_ours(args, ws, rank, local)
 
 

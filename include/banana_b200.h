@@ -137,6 +137,47 @@ int bnn_flip_stream(bnn_flip* h, void** stream);
  * are written back to them: upload, step, download in one stream (end-to-end timing). */
 int bnn_flip_step_host(bnn_flip* h, float* pos, float* vel, bnn_step_stats* stats);
 
+/* Device bytes the handle holds now (grids, particle, row and PCG arrays). */
+int bnn_flip_device_bytes(bnn_flip* h, uint64_t* bytes);
+/* Device bytes a scene with these parameters and n particles is expected to hold (the
+ * admission test of scene batches). */
+int bnn_scene_bytes_estimate(const bnn_params* params, uint32_t n, uint64_t* bytes);
+
+/* ---- scene batches -----------------------------------------------------------------
+ * Many independent scenes on one GPU (serving).  Each scene is a full solver (same
+ * results as a lone handle); bnn_batch_step advances every scene by one sub-step,
+ * stepping scenes concurrently from worker threads on their own streams.  A batch is
+ * driven by one host thread.  No counterpart in the reference, which runs one scene per
+ * ParticleSolver object (ParticleSolver.h:39-105). */
+typedef struct bnn_batch bnn_batch;
+typedef struct bnn_batch_params {
+    uint64_t hbm_budget_bytes; /* admission budget over bnn_scene_bytes_estimate; 0 = none */
+    uint32_t worker_threads;   /* host threads stepping scenes; 0 = min(16, cores) */
+} bnn_batch_params;
+typedef struct bnn_batch_stats {
+    uint32_t scenes;           /* scenes stepped */
+    uint32_t failed;           /* scenes whose step returned an error */
+    uint64_t particle_steps;   /* particles advanced by one sub-step, summed over scenes */
+    uint64_t pcg_iterations;   /* summed over scenes */
+    double   wall_ms;          /* host wall time of the batch step */
+    double   max_scene_ms;     /* slowest scene's step */
+} bnn_batch_stats;
+int bnn_batch_create(const bnn_batch_params* params, bnn_batch** out);
+int bnn_batch_destroy(bnn_batch* b);
+/* BNN_ERR_CAPACITY when the scene's estimate does not fit the remaining budget. */
+int bnn_batch_add_scene(bnn_batch* b, const bnn_params* params, const float* pos, const float* vel, uint32_t n,
+                        uint32_t* scene_id);
+int bnn_batch_remove_scene(bnn_batch* b, uint32_t scene_id);
+/* One sub-step of every scene; returns the first failing scene's status (all scenes are
+ * stepped regardless). */
+int bnn_batch_step(bnn_batch* b, bnn_batch_stats* stats);
+/* Particle count, sub-steps done and the stats of its last sub-step; returns the status
+ * of that sub-step. */
+int bnn_batch_scene_info(bnn_batch* b, uint32_t scene_id, uint32_t* n, uint64_t* steps, bnn_step_stats* last);
+int bnn_batch_get_scene(bnn_batch* b, uint32_t scene_id, float* pos, float* vel);
+/* Sum of the admitted scenes' estimates and of the bytes they hold now. */
+int bnn_batch_memory(bnn_batch* b, uint64_t* admitted, uint64_t* held);
+
 /* ---- standalone kernels (device pointers, stream = cudaStream_t or NULL) ---------- */
 
 /* Grid::getCellIdx + getCellLinearizedIndex (Grid.h:108-111,156-162) for every point and

@@ -39,7 +39,8 @@ def test_every_declared_symbol_is_exported(lib):
 
 def test_struct_layouts_match_binding(tmp_path):
     src = tmp_path / "layout.c"
-    fields = {"bnn_params": capi.Params, "bnn_step_stats": capi.StepStats, "bnn_pcg_stats": capi.PcgStats}
+    fields = {"bnn_params": capi.Params, "bnn_step_stats": capi.StepStats, "bnn_pcg_stats": capi.PcgStats,
+              "bnn_batch_params": capi.BatchParams, "bnn_batch_stats": capi.BatchStats}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "banana_b200.h"', "int main(void) {"]
     for cname, py in fields.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')

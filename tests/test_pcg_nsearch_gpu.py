@@ -65,6 +65,72 @@ def test_refined_reaches_1e8_fp64_checked(bnn, oracle_mod):
     assert res < 1e-8 * np.abs(rhs).max()
 
 
+def _box_system(nx=40, ny=36, nz=30, holes=0.08, seed=5):
+    """A 7-point system on a box of cells with random holes (air cells), rows in cell
+    order and neighbours in their direction slots (-z,-y,-x,+x,+y,+z): the layout of a
+    grid, which the solver packs into 16-byte row records.  Returns the slot layout, the
+    same system with each row's neighbours listed compactly (the general layout), and the
+    CSR form for the oracle."""
+    rng = np.random.default_rng(seed)
+    act = rng.random((nz, ny, nx)) > holes
+    row = -np.ones((nz, ny, nx), np.int64)
+    row[act] = np.arange(int(act.sum()))
+    n = int(act.sum())
+    dt = np.float32(1.0 / 30)
+    nbr = -np.ones((n, 6), np.int32)
+    k, j, i = np.nonzero(act)
+    r = row[k, j, i]
+    for slot, (dk, dj, di) in enumerate([(-1, 0, 0), (0, -1, 0), (0, 0, -1), (0, 0, 1), (0, 1, 0), (1, 0, 0)]):
+        kk, jj, ii = k + dk, j + dj, i + di
+        ok = (kk >= 0) & (kk < nz) & (jj >= 0) & (jj < ny) & (ii >= 0) & (ii < nx)
+        nb = np.full(n, -1, np.int64)
+        nb[ok] = row[kk[ok], jj[ok], ii[ok]]
+        nbr[r, slot] = nb
+    cnt = (nbr >= 0).sum(1)
+    diag = (cnt * dt + (6 - cnt) * dt / np.float32(0.5)).astype(np.float32)
+    rhs = (rng.standard_normal(n) * 1e-3).astype(np.float32)
+    compact = -np.ones_like(nbr)
+    rs, ci, va = [0], [], []
+    for q in range(n):
+        lo = [c for c in nbr[q, :3] if c >= 0]
+        hi = [c for c in nbr[q, 3:] if c >= 0]
+        compact[q, 3 - len(lo):3] = lo
+        compact[q, 3:3 + len(hi)] = hi
+        for c in lo:
+            ci.append(c); va.append(-dt)
+        ci.append(q); va.append(diag[q])
+        for c in hi:
+            ci.append(c); va.append(-dt)
+        rs.append(len(ci))
+    return nbr, compact, diag, -dt, rhs, (np.array(rs), np.array(ci), np.array(va, np.float32))
+
+
+@pytest.mark.parametrize("mode,omode", [("fp32", 0), ("fp64", 1), ("refined", 2)])
+def test_pcg_7pt_grid_rows_packed_matches_oracle(bnn, oracle_mod, mode, omode):
+    """Grid-ordered rows take the packed-record solve (x neighbours by warp shuffle); the
+    compact layout of the same system takes the general one.  Both equal the oracle."""
+    nbr, compact, diag, off, rhs, (rs, ci, va) = _box_system()
+    tol = 1e-8 if mode == "refined" else 1e-6
+    xo, so = oracle_mod.pcg(rs, ci, va, rhs, tol, 5000, omode, inner_tol=1e-3)
+    assert so["success"]
+    for layout in (nbr, compact):
+        x, st = bnn.pcg_solve_7pt(diag, layout, off, rhs, tol, 5000, mode=mode, inner_tol=1e-3)
+        assert st["success"] == 1
+        assert st["iterations"] == so["iterations"]
+        if mode == "fp32":
+            assert np.array_equal(x.astype(np.float32), xo.astype(np.float32))
+        else:
+            assert np.array_equal(x, xo)
+
+
+def test_pcg_7pt_rejects_bad_neighbour_index(bnn):
+    nbr, _, diag, off, rhs, _ = _box_system(8, 8, 8)
+    bad = nbr.copy()
+    bad[5, 4] = len(rhs)  # one past the last row
+    with pytest.raises(bnn.BnnError):
+        bnn.pcg_solve_7pt(diag, bad, off, rhs, 1e-6, 100)
+
+
 def _dev(a):
     return torch.from_numpy(np.ascontiguousarray(a)).cuda()
 
