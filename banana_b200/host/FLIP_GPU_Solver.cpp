@@ -1,0 +1,321 @@
+// FLIP_GPU_Solver: ParticleSolver-shaped host class over the banana_b200 C ABI.
+#include "FLIP_GPU_Solver.h"
+
+#include "json_lite.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <stdexcept>
+
+namespace bnnhost {
+
+// ---------------------------------------------------------------------------------
+// seeded sampling (must match banana_b200/scenes.py: dam_break / uniform01 / splitmix64)
+// ---------------------------------------------------------------------------------
+static inline uint64_t splitmix64(uint64_t x) {
+    uint64_t z = x + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+static inline double uniform01(uint64_t seed, uint64_t stream, uint64_t counter) {
+    const uint64_t key = splitmix64(seed * 0x9E3779B97F4A7C15ull + stream * 0xD1B54A32D192ED03ull);
+    const uint64_t bits = splitmix64(counter ^ key);
+    return (double)(bits >> 11) * (1.0 / 9007199254740992.0);
+}
+
+void sample_box(const float domainMin[3], double cellSize, const double bmin[3], const double bmax[3], unsigned ppc,
+                uint64_t seed, std::vector<float>& pos, std::vector<float>& vel) {
+    int64_t c0[3], nc[3];
+    for(int a = 0; a < 3; ++a) {
+        const double lo = (bmin[a] - (double)domainMin[a]) / cellSize, hi = (bmax[a] - (double)domainMin[a]) / cellSize;
+        c0[a] = (int64_t)std::ceil(lo - 1e-9);
+        const int64_t c1 = (int64_t)std::floor(hi + 1e-9);  // one past the last cell
+        nc[a] = c1 > c0[a] ? c1 - c0[a] : 0;
+    }
+    const int64_t ncell = nc[0] * nc[1] * nc[2];
+    if(ncell <= 0) return;
+    const size_t base = pos.size();
+    pos.resize(base + (size_t)ncell * ppc * 3);
+    vel.resize(base + (size_t)ncell * ppc * 3, 0.f);
+    for(int64_t cell = 0; cell < ncell; ++cell) {
+        const int64_t ci[3] = {cell % nc[0], (cell / nc[0]) % nc[1], cell / (nc[0] * nc[1])};
+        for(unsigned k = 0; k < ppc; ++k) {
+            const uint64_t lin = (uint64_t)(cell * (int64_t)ppc + k);
+            for(int a = 0; a < 3; ++a) {
+                const double cc = (double)(c0[a] + ci[a]);
+                const double u = uniform01(seed, (uint64_t)a, lin);
+                float p = (float)((double)domainMin[a] + (cc + u) * cellSize);
+                // rounding to float may land a sample on the next cell's face: keep it inside
+                const float hi = (float)((double)domainMin[a] + (cc + 1.0) * cellSize);
+                if(p >= hi) p = std::nextafter(hi, 0.0f);
+                pos[base + ((size_t)lin) * 3 + (size_t)a] = p;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// factory
+// ---------------------------------------------------------------------------------
+std::map<std::string, ParticleSolverFactory::CreateMethod>& ParticleSolverFactory::methods() {
+    static std::map<std::string, CreateMethod> m;
+    return m;
+}
+
+bool ParticleSolverFactory::registerSolver(const std::string& name, CreateMethod create) {
+    methods()[name] = std::move(create);
+    return true;
+}
+
+std::shared_ptr<FLIP_GPU_Solver> ParticleSolverFactory::createSolver(const std::string& name) {
+    auto it = methods().find(name);
+    return it == methods().end() ? nullptr : it->second();
+}
+
+static std::string read_file(const std::string& path) {
+    std::ifstream f(path);
+    if(!f) throw std::runtime_error("cannot open scene file " + path);
+    std::stringstream ss;
+    ss << f.rdbuf();
+    return ss.str();
+}
+
+std::shared_ptr<FLIP_GPU_Solver> ParticleSolverFactory::createSolverFromJSon(const std::string& sceneFile) {
+    const Json j = JsonParser(read_file(sceneFile)).parse();
+    std::string name;
+    if(!read_string(j["GlobalParameters"], "Solver", name)) return nullptr;
+    return createSolver(name);
+}
+
+// static registration, as RegisteredInSolverFactory does (ParticleSolverFactory.h:51-60)
+static const bool s_registered = ParticleSolverFactory::registerSolver(FLIP_GPU_Solver::solverName(), [] {
+    return std::make_shared<FLIP_GPU_Solver>();
+}) && ParticleSolverFactory::registerSolver(APIC_GPU_Solver::solverName(), [] {
+    return std::static_pointer_cast<FLIP_GPU_Solver>(std::make_shared<APIC_GPU_Solver>());
+}) && ParticleSolverFactory::registerSolver(AFLIP_GPU_Solver::solverName(), [] {
+    return std::static_pointer_cast<FLIP_GPU_Solver>(std::make_shared<AFLIP_GPU_Solver>());
+});
+
+// ---------------------------------------------------------------------------------
+// solver
+// ---------------------------------------------------------------------------------
+FLIP_GPU_Solver::~FLIP_GPU_Solver() {
+    if(m_Gpu) bnn_flip_destroy(m_Gpu);
+}
+
+void FLIP_GPU_Solver::check(int status, const char* what) {
+    if(status == BNN_OK) return;
+    std::fprintf(stderr, "%s: %s failed with status %d (%s)\n", getSolverName().c_str(), what, status,
+                 bnn_last_error());
+    if(status == BNN_ERR_PCG_NOT_CONVERGED) {
+        // PIC_Solver::solveSystem logs the failure and exits only when asked to
+        if(m_SolverParams.bExitIfPressureProjectionFailed) std::exit(EXIT_FAILURE);
+        return;
+    }
+    std::exit(EXIT_FAILURE);  // __BNN_REQUIRE
+}
+
+void FLIP_GPU_Solver::loadScene(const std::string& sceneFile, bool allocate) {
+    loadSceneFromString(read_file(sceneFile), allocate);
+}
+
+// ParticleSolver::loadScene (ParticleSolver.cpp:36-130): global and simulation parameters,
+// domain box, particle generators, then the solver memory
+void FLIP_GPU_Solver::loadSceneFromString(const std::string& sceneJson, bool allocate) {
+    const Json j = JsonParser(sceneJson).parse();
+    if(!j.has("GlobalParameters") || !j.has("SimulationParameters")) {
+        std::fprintf(stderr, "scene needs GlobalParameters and SimulationParameters\n");
+        std::exit(EXIT_FAILURE);
+    }
+    const Json& g = j["GlobalParameters"];
+    auto& G = m_GlobalParams;
+    read_string(g, "Solver", G.solverName);
+    read_value(g, "FrameDuration", G.frameDuration);
+    read_value(g, "StartFrame", G.startFrame);
+    read_value(g, "FinalFrame", G.finalFrame);
+    read_bool(g, "ApplyGravity", G.bApplyGravity);
+    read_bool(g, "SaveFrameData", G.bSaveFrameData);
+    read_string(g, "DataPath", G.dataPath);
+    read_string(g, "FrameDataFolder", G.frameDataFolder);
+
+    const Json& s = j["SimulationParameters"];
+    auto& P = m_SolverParams;
+    read_value(s, "MinTimestep", P.minTimestep);
+    read_value(s, "MaxTimestep", P.maxTimestep);
+    read_value(s, "CFLFactor", P.CFLFactor);
+    read_value(s, "CellSize", P.cellSize);
+    m_CellSizeScene = (double)P.cellSize;
+    read_number(s, "CellSize", m_CellSizeScene);
+    read_value(s, "RatioCellSizePRadius", P.ratioCellSizePRadius);
+    read_value(s, "NExpandCells", P.nExpandCells);
+    read_value(s, "MaxNParticles", P.maxNParticles);
+    read_value(s, "AdvectionSteps", P.advectionSteps);
+    read_bool(s, "CorrectPosition", P.bCorrectPosition);
+    read_value(s, "CGRelativeTolerance", P.CGRelativeTolerance);
+    read_value(s, "MaxCGIteration", P.maxCGIteration);
+    read_value(s, "PIC_FLIP_ratio", P.PIC_FLIP_ratio);
+    read_bool(s, "ExitIfPressureProjectionFailed", P.bExitIfPressureProjectionFailed);
+    std::string mode;
+    if(read_string(s, "GPU_PCGPrecision", mode))
+        P.pcgMode = mode == "fp64" ? BNN_PCG_FP64 : (mode == "refined" ? BNN_PCG_REFINED : BNN_PCG_FP32);
+    read_value(s, "GPU_RefineTolerance", P.refineTolerance);
+    read_value(s, "GPU_RefineInnerTolerance", P.refineInnerTolerance);
+    if(s.has("SimulationDomainBox")) {
+        read_vec3(s["SimulationDomainBox"], "BoxMin", P.domainBMin);
+        read_vec3(s["SimulationDomainBox"], "BoxMax", P.domainBMax);
+    }
+    if(P.bCorrectPosition)
+        std::fprintf(stderr, "%s: CorrectPosition is not supported on the GPU path; running without it\n",
+                     getSolverName().c_str());
+    // SimulationParameters::makeReady (ParticleSolverData.cpp:229-272)
+    for(int d = 0; d < 3; ++d) {
+        P.movingBMin[d] = P.domainBMin[d];
+        P.movingBMax[d] = P.domainBMax[d];
+    }
+    P.particleRadius = P.cellSize / P.ratioCellSizePRadius;
+
+    generateParticles(j);
+    if(allocate) allocateSolverMemory();
+}
+
+// ParticleSolver::generateParticles (ParticleSolver.cpp:302-310) for box generators
+void FLIP_GPU_Solver::generateParticles(const Json& scene) {
+    auto& D = m_ParticleData;
+    D.positions.clear();
+    D.velocities.clear();
+    D.objectIndex.clear();
+    D.nObjects = 0;
+    const Json& gens = scene["ParticleGenerators"];
+    for(size_t q = 0; q < gens.size(); ++q) {
+        const Json& o = gens[q];
+        std::string type = "Box";
+        read_string(o, "GeometryType", type);
+        if(type != "Box") {
+            std::fprintf(stderr, "%s: particle generator geometry '%s' is not supported (Box only)\n",
+                         getSolverName().c_str(), type.c_str());
+            std::exit(EXIT_FAILURE);
+        }
+        double bmin[3] = {0, 0, 0}, bmax[3] = {0, 0, 0};
+        read_vec3(o, "BoxMin", bmin);
+        read_vec3(o, "BoxMax", bmax);
+        unsigned ppc = 8;
+        read_value(o, "ParticlesPerCell", ppc);
+        uint64_t seed = 42;
+        read_value(o, "Seed", seed);
+        const size_t before = D.positions.size() / 3;
+        sample_box(m_SolverParams.domainBMin, m_CellSizeScene, bmin, bmax, ppc, seed, D.positions, D.velocities);
+        D.objectIndex.resize(D.positions.size() / 3, (int16_t)D.nObjects);
+        (void)before;
+        ++D.nObjects;
+    }
+}
+
+void FLIP_GPU_Solver::setParticles(const std::vector<float>& pos, const std::vector<float>& vel) {
+    m_ParticleData.positions = pos;
+    m_ParticleData.velocities = vel;
+    m_ParticleData.objectIndex.assign(pos.size() / 3, 0);
+    if(m_Gpu) check(bnn_flip_set_particles(m_Gpu, pos.data(), vel.data(), (uint32_t)(pos.size() / 3)),
+                    "bnn_flip_set_particles");
+}
+
+// FLIP_Solver::allocateSolverMemory + PIC_Data::makeReady: the device solver
+void FLIP_GPU_Solver::allocateSolverMemory() {
+    const auto& P = m_SolverParams;
+    bnn_params p;
+    std::memset(&p, 0, sizeof(p));
+    for(int d = 0; d < 3; ++d) {
+        p.box_min[d] = P.domainBMin[d];
+        p.box_max[d] = P.domainBMax[d];
+    }
+    p.cell_size = P.cellSize;
+    p.n_expand_cells = P.nExpandCells;
+    p.cfl_factor = P.CFLFactor;
+    p.min_timestep = P.minTimestep;
+    p.max_timestep = P.maxTimestep;
+    p.frame_duration = m_GlobalParams.frameDuration;
+    p.pic_flip_ratio = P.PIC_FLIP_ratio;
+    p.cg_relative_tolerance = P.CGRelativeTolerance;
+    p.max_cg_iteration = P.maxCGIteration;
+    p.advection_steps = P.advectionSteps;
+    p.solver_kind = m_SolverKind;
+    p.pcg_mode = P.pcgMode;
+    p.preconditioner = BNN_PRECOND_JACOBI;
+    p.refine_tolerance = P.refineTolerance;
+    p.refine_inner_tolerance = P.refineInnerTolerance;
+    p.apply_gravity = m_GlobalParams.bApplyGravity ? 1 : 0;
+    p.max_particles = P.maxNParticles;
+    if(m_Gpu) bnn_flip_destroy(m_Gpu);
+    m_Gpu = nullptr;
+    check(bnn_flip_create(&p, &m_Gpu), "bnn_flip_create");
+    const auto& D = m_ParticleData;
+    check(bnn_flip_set_particles(m_Gpu, D.positions.data(), D.velocities.data(), D.getNParticles()),
+          "bnn_flip_set_particles");
+}
+
+// PIC_Solver::advanceFrame (PIC_Solver.cpp:267-311): sub-steps until FrameDuration; the
+// host vectors receive the particles at the end of the frame
+void FLIP_GPU_Solver::advanceFrame() {
+    FrameLog log;
+    for(;;) {
+        bnn_step_stats st;
+        const int rc = bnn_flip_step(m_Gpu, &st);
+        check(rc, "bnn_flip_step");
+        ++log.substeps;
+        log.pcgIterations += st.pcg_iterations;
+        log.lastResidual = st.pcg_residual;
+        log.gpuMs += st.stage_ms[9];
+        m_GlobalParams.frameLocalTime = (float)st.frame_time;
+        if(st.frame_finished) break;
+    }
+    auto& D = m_ParticleData;
+    check(bnn_flip_get_particles(m_Gpu, D.positions.data(), D.velocities.data()), "bnn_flip_get_particles");
+    log.frame = m_GlobalParams.finishedFrame + 1;
+    m_Logs.push_back(log);
+}
+
+// ParticleSolver::doFrameSimulation (ParticleSolver.cpp:160-186)
+void FLIP_GPU_Solver::doFrameSimulation(unsigned frame) {
+    (void)frame;
+    advanceFrame();
+    ++m_GlobalParams.finishedFrame;
+    m_GlobalParams.frameLocalTime = 0.f;
+    if(m_GlobalParams.bSaveFrameData) saveFrameData();
+}
+
+// ParticleSolver::doSimulation (ParticleSolver.cpp:134-156)
+void FLIP_GPU_Solver::doSimulation() {
+    for(unsigned frame = m_GlobalParams.startFrame; frame <= m_GlobalParams.finalFrame; ++frame)
+        doFrameSimulation(frame);
+}
+
+void FLIP_GPU_Solver::finalizeSimulation() {
+    if(m_Gpu) {
+        bnn_flip_destroy(m_Gpu);
+        m_Gpu = nullptr;
+    }
+}
+
+// Frame output: positions and velocities as raw little-endian float32 AoS with a small
+// header (n, then 3n positions, 3n velocities).  The reference's .bnn container
+// (ParticleSerialization) is not reproduced.
+int FLIP_GPU_Solver::saveFrameData() {
+    char name[64];
+    std::snprintf(name, sizeof(name), "frame.%04u.f32", m_GlobalParams.finishedFrame);
+    const std::string path = m_GlobalParams.dataPath + "/" + name;
+    std::FILE* f = std::fopen(path.c_str(), "wb");
+    if(!f) return -1;
+    const uint32_t n = m_ParticleData.getNParticles();
+    std::fwrite(&n, sizeof(n), 1, f);
+    std::fwrite(m_ParticleData.positions.data(), sizeof(float), 3 * (size_t)n, f);
+    std::fwrite(m_ParticleData.velocities.data(), sizeof(float), 3 * (size_t)n, f);
+    std::fclose(f);
+    return 0;
+}
+
+} // namespace bnnhost
