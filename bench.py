@@ -17,6 +17,12 @@ Other workloads (`--workload`, one JSON line each, not the headline):
   serve   Poisson request stream (20/s, seed 13, cubic 32..192 cells), 200 sub-steps per
           request, 150 GB admission budget; reports request- and step-latency p50/p99.
   nsearch 4M-point cell sort + neighbour lists (r = 0.01, seed 7).
+  fp64err the 256^3 scene's first `--steps` sub-steps on the GPU (FP32 PCG and refined
+          PCG) against the FP64 build of the oracle: max position error / dx, max face
+          velocity and pressure errors relative to their max magnitude.
+  pcg     standalone Jacobi PCG (bnn_pcg_solve_7pt) on the 102 x 153 x 102 box of fluid
+          cells the 256^3 dam break starts with (1,591,812 rows), a fixed number of
+          iterations (`--steps`); for profiling the solver alone.
 
 `--impl reference` times the reference's CPU algorithm (the oracle port of PIC_Solver /
 FLIP_Solver / PCGSolver, reference arithmetic order, OpenMP over all host cores) on the
@@ -43,9 +49,10 @@ N_GRID = 256
 METRIC = "particle-steps/s at 256^3 FLIP (1e-6 rel residual)"
 UNIT = "particle-steps/s"
 WORKLOAD = "flip_dam_break_256"
-# DRAM bytes (read + write) of one k_pcg_persistent launch, from the ncu capture summarised
-# in profiles/ (None until captured for the current kernel)
-PCG_TRAFFIC = None
+# DRAM bytes (read + write) per PCG iteration of k_pcg_persistent at 1.59M rows, from the ncu
+# capture summarised in profiles/k_pcg_persistent_box_1591812_rows.md (931.7 MB over 300
+# iterations); a launch's traffic is this times its iterations
+PCG_TRAFFIC_PER_ITER = 931.7e6 / 300
 
 
 def _config(pcg_mode: str):
@@ -289,7 +296,10 @@ def run_ours(args, ws, rank, local):
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "algorithmic_bytes": "52 B per active row per PCG iteration (x, r, z, s, q, 1/diag and "
-                                              "the row's matrix data once each)", "traffic": PCG_TRAFFIC},
+                                              "the row's matrix data once each)",
+                         "traffic": PCG_TRAFFIC_PER_ITER * iters / args.steps,
+                         "traffic_note": "ncu DRAM bytes per iteration of the same kernel at the same row count "
+                                         "(standalone capture) x iterations per launch; the solve is L2-resident"},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clk,
             "detail": {"pcg_iterations_per_step": iters / args.steps, "active_rows_mean": float(np.mean(rows)),
@@ -518,6 +528,107 @@ def run_nsearch(args, ws, rank, local):
     return 0
 
 
+def _box_system(nx, ny, nz, seed=1):
+    """7-point system on a full box of cells in cell order (the layout of a grid)."""
+    n = nx * ny * nz
+    dt = np.float32(1.0 / 30)
+    i = np.arange(n)
+    x, y, z = i % nx, (i // nx) % ny, i // (nx * ny)
+    nbr = -np.ones((n, 6), np.int32)
+    nbr[:, 0] = np.where(z > 0, i - nx * ny, -1)
+    nbr[:, 1] = np.where(y > 0, i - nx, -1)
+    nbr[:, 2] = np.where(x > 0, i - 1, -1)
+    nbr[:, 3] = np.where(x < nx - 1, i + 1, -1)
+    nbr[:, 4] = np.where(y < ny - 1, i + nx, -1)
+    nbr[:, 5] = np.where(z < nz - 1, i + nx * ny, -1)
+    cnt = (nbr >= 0).sum(1)
+    diag = (cnt * dt + (6 - cnt) * dt / np.float32(0.5)).astype(np.float32)
+    rhs = (np.random.default_rng(seed).standard_normal(n) * 1e-3).astype(np.float32)
+    return diag, nbr, -dt, rhs
+
+
+def run_pcg(args, ws, rank, local):
+    torch, dist = _torch_dist(ws, local)
+    from banana_b200 import capi, pcg_solve_7pt
+
+    diag, nbr, off, rhs = _box_system(102, 153, 102)
+    n = len(rhs)
+    for _ in range(args.warmup):
+        pcg_solve_7pt(diag, nbr, off, rhs, 1e-30, args.steps, mode=args.pcg_mode)
+    launches0 = capi.launch_count()
+    _, st = pcg_solve_7pt(diag, nbr, off, rhs, 1e-30, args.steps, mode=args.pcg_mode)
+    launches = capi.launch_count() - launches0
+    it = max(st["iterations"], 1)
+    us = 1e3 * st["ms"] / it
+    peak, peak_kind = _peaks()
+    achieved = 52.0 * n / (us * 1e-6) / 1e9
+    if rank == 0:
+        line = {"metric": "us per PCG iteration, 1,591,812-row 7-point system", "value": us, "unit": "us/iteration",
+                "n_gpus": 1, "steps": it, "warmup": args.warmup, "ms_per_step": st["ms"], "higher_is_better": False,
+                "scaling": "replicas", "vs_baseline": None, "dtype": args.pcg_mode,
+                "data": "synthetic (box of fluid cells, random rhs, seed 1)",
+                "config": {"workload": "pcg_box_102x153x102", "rows": n, "pcg": f"Jacobi, {args.pcg_mode}",
+                           "layout": "grid rows (packed 16-byte records)"},
+                "roofline": {"bound": "hbm", "kernel": "k_pcg_persistent", "achieved": achieved, "peak": peak,
+                             "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                             "algorithmic_bytes": "52 B per row per iteration", "traffic": None},
+                "gpu_launches": int(launches)}
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def run_fp64err(args, ws, rank, local):
+    torch, dist = _torch_dist(ws, local)
+    from banana_b200 import FlipSolver, scenes
+    from oracle import oracle as O
+
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    pos, vel = scenes.dam_break(N_GRID)
+    dx = 1.0 / N_GRID
+    ref = O.Oracle(scenes.dam_break_params(N_GRID, reduce_mode=0, nthreads=threads, sort_each_step=0, pcg_mode=1),
+                   use_double=True)
+    ref.set_particles(pos, vel)
+    gpus = {}
+    for name, mode in (("fp32", 0), ("refined", 2)):
+        s = FlipSolver(scenes.dam_break_params(N_GRID, pcg_mode=mode))
+        s.set_particles(pos, vel)
+        gpus[name] = s
+    per_step = []
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        so = ref.step()
+        row = {"step": k + 1, "dt_fp64": so["dt"]}
+        po, _ = ref.get_particles(f64=True)
+        for name, s in gpus.items():
+            sg = s.step()
+            pg, _ = s.get_particles()
+            row[name] = {"dt": sg["dt"], "pos_err_dx": float(np.abs(pg.astype(np.float64) - po).max() / dx)}
+        per_step.append(row)
+    fields = {}
+    for name, s in gpus.items():
+        e = {}
+        for f_, w in (("u", 0), ("v", 1), ("w", 2), ("pressure", 4)):
+            a = s.grid(w).astype(np.float64)
+            b = ref.grid(w, f64=True)
+            e[f_] = float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+        fields[name] = e
+    sec = time.perf_counter() - t0
+    ref.close()
+    line = {"metric": "FP64-referenced error after the first sub-steps of the 256^3 FLIP scene",
+            "value": per_step[-1]["fp32"]["pos_err_dx"], "unit": "max |x - x_fp64| / dx", "n_gpus": 1,
+            "steps": args.steps, "warmup": 0, "higher_is_better": False, "dtype": "f32 vs f64",
+            "data": "synthetic (seeded dam break, seed 42)",
+            "config": {"workload": "fp64_error_256", "reference": "oracle FP64 build (reference order, OpenMP)"},
+            "per_step": per_step, "field_rel_err_last_step": fields, "seconds": sec}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     global N_GRID
     ap = argparse.ArgumentParser()
@@ -529,7 +640,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--grid", type=int, default=N_GRID, help="fluid-domain resolution (profiling of smaller cases)")
-    ap.add_argument("--workload", choices=["flip", "batch", "serve", "nsearch"], default="flip")
+    ap.add_argument("--workload", choices=["flip", "batch", "serve", "nsearch", "pcg", "fp64err"], default="flip")
     ap.add_argument("--workers", type=int, default=0, help="batch/serve: host threads stepping scenes (0 = auto)")
     ap.add_argument("--requests", type=int, default=100, help="serve: number of requests")
     ap.add_argument("--req-steps", type=int, default=200, help="serve: sub-steps per request")
@@ -545,6 +656,10 @@ def main():
         return run_serve(args, ws, rank, local)
     if args.workload == "nsearch":
         return run_nsearch(args, ws, rank, local)
+    if args.workload == "pcg":
+        return run_pcg(args, ws, rank, local)
+    if args.workload == "fp64err":
+        return run_fp64err(args, ws, rank, local)
     return run_ours(args, ws, rank, local)
 
 
