@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <utility>
 #include <string>
 #include <vector>
 
@@ -44,7 +45,8 @@ void launch_build_rows(const GridDesc& g, int nrows, const uint32_t* rowCell, co
                        const float* const* U, float dt, float* rhs, float* diag, float* invdiag, int32_t* nbr,
                        DevState* st, cudaStream_t s);
 void launch_update_velocity(const GridDesc& g, const DevState* st, const float* phi, const uint32_t* aidx,
-                            const float* pressure, float dt, float* const* U, uint8_t* const* V, cudaStream_t s);
+                            const float* pressure, float dt, float* const* velIn, float* const* velOut,
+                            uint8_t* const* validOut, cudaStream_t s);
 void launch_g2p(int n, const GridDesc& g, float* p6, size_t stride, const float* const* U, const float* const* O,
                 float ratio, int kind, float* C9, cudaStream_t s);
 void launch_aos_to_soa(int n, const float* pos, const float* vel, float* soa6, uint32_t* ids, size_t stride,
@@ -465,8 +467,13 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st) {
                    h->P.refine_tolerance, h->pressure, nullptr, h->dst, h->hst, s, po);
     if(rc != BNN_OK) return rc;
     cudaEventRecord(h->ev[7], s);
-    launch_update_velocity(g, h->dst, h->phi, h->aidx, h->pressure, substep, h->U, h->VA, s);
-    launch_extrapolate(g, h->U, h->VA, h->B, h->VB, 2, nullptr, 0.f, h->dst, s);
+    // projected faces go to the ping-pong arrays, which then become the velocity arrays
+    launch_update_velocity(g, h->dst, h->phi, h->aidx, h->pressure, substep, h->U, h->B, h->VB, s);
+    launch_extrapolate(g, h->B, h->VB, h->U, h->VA, 2, nullptr, 0.f, h->dst, s);
+    for(int d = 0; d < 3; ++d) {
+        std::swap(h->U[d], h->B[d]);
+        std::swap(h->VA[d], h->VB[d]);
+    }
     cudaEventRecord(h->ev[8], s);
     launch_g2p(n, g, h->p6[h->cur], h->cap, h->U, h->O, h->P.pic_flip_ratio, kind, affine ? h->C9[h->cur] : nullptr, s);
     cudaEventRecord(h->ev[9], s);

@@ -393,49 +393,50 @@ __device__ __forceinline__ int bbox_distance(const DevState* st, int i, int j, i
 constexpr int kExtFull = 2 + 4;
 constexpr int kExtRegion = kExtFull + 2;
 
+// The box of faces within `reach` of the occupied-cell box, clamped to an array of size
+// S; false when it is empty (no particles).
+__device__ __forceinline__ bool reach_box(const DevState* st, int reach, const int S[3], int lo[3], int hi[3]) {
+#pragma unroll
+    for(int d = 0; d < 3; ++d) {
+        const int bl = st->bbox[d], bh = st->bbox[3 + d];
+        if(bh < bl) return false;
+        lo[d] = max(bl - reach, 0);
+        hi[d] = min(bh + reach, S[d] - 1);
+        if(hi[d] < lo[d]) return false;
+    }
+    return true;
+}
+
 // One layer of PIC_Solver::extrapolateVelocity (PIC_Solver.cpp:998-1089): an interior
 // face that was not valid takes the mean of its valid 6-neighbours (+x,-x,+y,-y,+z,-z
 // summation order) and becomes valid; everything reads the previous layer.
 // mode 0: plain layer.  mode 1 (last layer after P2G): also writes the FLIP backup
 // oldVels (FLIP_Data.h:48-52) and applies Earth gravity v -= 9.81*dt (PIC_Solver.cpp:
-// 505-511) to the v component -- on every face, so faces beyond the region get the
+// 505-511) to the v component; beyond the region the host has already written the
 // backup 0 and the velocity 0 - gravityDt.  mode 2 (last layer after projection): folds
 // max|u| into the CFL reduction (PIC_Solver.cpp:342-349).
-// Block: 32 x 8 faces of one (x, y) slab.
+// The blocks stride over 32 x 8 tiles of the region box only.
 __global__ void __launch_bounds__(256) k_extrapolate(int sx, int sy, int sz, const float* __restrict__ gin,
                                                      const uint8_t* __restrict__ vin, float* __restrict__ gout,
                                                      uint8_t* __restrict__ vout, int mode, float* __restrict__ oldOut,
                                                      float gravityDt, DevState* st) {
-    const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, k = blockIdx.z;
-    const bool live = i < sx && j < sy;
-    const size_t f = ((size_t)k * sy + j) * sx + i;
-    {
-        // the block's nearest face: per axis the nearer end of its index range
-        const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 8;
-        const int ob = max(bbox_distance(st, min(max(st->bbox[0], x0), x0 + 31), min(max(st->bbox[1], y0), y0 + 7), k),
-                           0);
-        if(ob > kExtRegion) {
-            // whole block beyond the region: only mode 1 writes anything there
-            if(mode == 1 && live) {
-                oldOut[f] = 0.f;
-                if(gravityDt != 0.f) gout[f] = 0.f - gravityDt;
-            }
-            return;
-        }
-    }
-    float val = 0.f;
-    if(live) {
-        const int o = bbox_distance(st, i, j, k);
-        if(o > kExtRegion) {
-            if(mode == 1) {
-                oldOut[f] = 0.f;
-                if(gravityDt != 0.f) gout[f] = 0.f - gravityDt;
-            }
-        } else {
-            val = gin[f];
+    const int S[3] = {sx, sy, sz};
+    int lo[3], hi[3];
+    float m = 0.f;
+    if(reach_box(st, kExtRegion, S, lo, hi)) {
+        const int tx = (hi[0] - lo[0] + 32) / 32, ty = (hi[1] - lo[1] + 8) / 8, tz = hi[2] - lo[2] + 1;
+        const long long nt = (long long)tx * ty * tz;
+        const size_t sxy = (size_t)sx * sy;
+        for(long long t = blockIdx.x; t < nt; t += gridDim.x) {
+            const int i = lo[0] + (int)(t % tx) * 32 + (int)(threadIdx.x & 31);
+            const int j = lo[1] + (int)((t / tx) % ty) * 8 + (int)(threadIdx.x >> 5);
+            const int k = lo[2] + (int)(t / ((long long)tx * ty));
+            if(i > hi[0] || j > hi[1]) continue;
+            const size_t f = ((size_t)k * sy + j) * sx + i;
+            const int o = bbox_distance(st, i, j, k);
+            float val = gin[f];
             uint8_t vv = vin[f];
             if(!vv && o <= kExtFull && i > 0 && i < sx - 1 && j > 0 && j < sy - 1 && k > 0 && k < sz - 1) {
-                const size_t sxy = (size_t)sx * sy;
                 float sum = 0.f;
                 unsigned count = 0;
                 if(vin[f + 1]) { sum += gin[f + 1]; ++count; }
@@ -453,19 +454,23 @@ __global__ void __launch_bounds__(256) k_extrapolate(int sx, int sy, int sz, con
             } else {
                 gout[f] = val;
             }
+            m = fmaxf(m, fabsf(val));
         }
     }
     if(mode == 2) {
         __shared__ float sm[8];
-        float m = fabsf(val);
         for(int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
-        if(threadIdx.x == 0) sm[threadIdx.y] = m;
+        if((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
         __syncthreads();
-        if(threadIdx.x == 0 && threadIdx.y == 0) {
+        if(threadIdx.x == 0) {
             for(int w = 1; w < 8; ++w) m = fmaxf(m, sm[w]);
             if(m > 0.f) atomicMax(&st->maxvel_bits, __float_as_uint(m));
         }
     }
+}
+
+__global__ void k_fill(float* __restrict__ a, size_t n, float v) {
+    for(size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) a[i] = v;
 }
 
 // ----------------------------------------------------------------------------------
@@ -604,37 +609,46 @@ __global__ void k_build_rows(GridDesc g, int nrows, const uint32_t* __restrict__
 // PIC_Solver::updateProjectedVelocity (PIC_Solver.cpp:911-981), weights 1: face (i,j,k)
 // of component D between cells c- and c gets u -= dt*(p_c - p_c-)/max(0.01, theta) when
 // either cell is fluid and is marked valid; every other face is set to 0.  Fluid cells lie
-// within one cell of the occupied-cell box, so faces farther than 2 from it are set to 0
-// without reading anything.  Block: 32 x 8 faces of one (x, y) slab.
+// within one cell of the occupied-cell box, so only faces within 2 of it can be valid:
+// the blocks stride over that box and the host zeroes the output arrays beforehand.
 template<int D>
 __global__ void __launch_bounds__(256) k_update_velocity(GridDesc g, const DevState* __restrict__ st,
                                                          const float* __restrict__ phi,
                                                          const uint32_t* __restrict__ aidx,
                                                          const float* __restrict__ pressure, float dt,
-                                                         float* __restrict__ vel, uint8_t* __restrict__ valid) {
-    const int sx = g.G[0] + (D == 0), sy = g.G[1] + (D == 1);
-    const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, k = blockIdx.z;
-    if(i >= sx || j >= sy) return;
-    const size_t f = ((size_t)k * sy + j) * sx + i;
-    const int a = D == 0 ? i : (D == 1 ? j : k);
+                                                         const float* __restrict__ velIn, float* __restrict__ velOut,
+                                                         uint8_t* __restrict__ validOut) {
+    const int S[3] = {g.G[0] + (D == 0), g.G[1] + (D == 1), g.G[2] + (D == 2)};
+    int lo[3], hi[3];
+    if(!reach_box(st, 2, S, lo, hi)) return;
+    const int tx = (hi[0] - lo[0] + 32) / 32, ty = (hi[1] - lo[1] + 8) / 8, tz = hi[2] - lo[2] + 1;
+    const long long nt = (long long)tx * ty * tz;
     const int amax = g.G[D];
-    float out = 0.f;
-    uint8_t vv = 0;
-    if(a > 0 && a < amax && bbox_distance(st, i, j, k) <= 2) {
-        const size_t c = ((size_t)k * g.G[1] + j) * g.G[0] + i;
-        const size_t step = D == 0 ? 1 : (D == 1 ? (size_t)g.G[0] : (size_t)g.G[0] * g.G[1]);
-        const size_t cm = c - step;
-        const float pc = phi[c], pm = phi[cm];
-        if(pc < 0.f || pm < 0.f) {
-            const float prc = pc < 0.f ? pressure[aidx[c]] : 0.f;
-            const float prm = pm < 0.f ? pressure[aidx[cm]] : 0.f;
-            const float th = smax(0.01f, fraction_inside(pm, pc));
-            out = vel[f] - dt * (prc - prm) / th;
-            vv = 1;
+    for(long long t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int i = lo[0] + (int)(t % tx) * 32 + (int)(threadIdx.x & 31);
+        const int j = lo[1] + (int)((t / tx) % ty) * 8 + (int)(threadIdx.x >> 5);
+        const int k = lo[2] + (int)(t / ((long long)tx * ty));
+        if(i > hi[0] || j > hi[1]) continue;
+        const size_t f = ((size_t)k * S[1] + j) * S[0] + i;
+        const int a = D == 0 ? i : (D == 1 ? j : k);
+        float out = 0.f;
+        uint8_t vv = 0;
+        if(a > 0 && a < amax) {
+            const size_t c = ((size_t)k * g.G[1] + j) * g.G[0] + i;
+            const size_t step = D == 0 ? 1 : (D == 1 ? (size_t)g.G[0] : (size_t)g.G[0] * g.G[1]);
+            const size_t cm = c - step;
+            const float pc = phi[c], pm = phi[cm];
+            if(pc < 0.f || pm < 0.f) {
+                const float prc = pc < 0.f ? pressure[aidx[c]] : 0.f;
+                const float prm = pm < 0.f ? pressure[aidx[cm]] : 0.f;
+                const float th = smax(0.01f, fraction_inside(pm, pc));
+                out = velIn[f] - dt * (prc - prm) / th;
+                vv = 1;
+            }
         }
+        velOut[f] = out;
+        validOut[f] = vv;
     }
-    vel[f] = out;
-    valid[f] = vv;
 }
 
 // ----------------------------------------------------------------------------------
@@ -837,7 +851,11 @@ void launch_p2g(const GridDesc& g, const uint32_t* cellStart, const float* g3, c
         }
     }
 }
-// 4 layers per component; A holds the input and receives the result (4 is even)
+static constexpr unsigned kRegionBlocks = 148u * 8u;  // resident blocks of the region kernels
+
+// 4 layers per component; A holds the input and receives the result (4 is even).  Mode 1
+// first writes the values the last layer gives every face beyond its region: backup 0,
+// and v = 0 - gravityDt (A holds 0 there).
 void launch_extrapolate(const GridDesc& g, float* const* A, uint8_t* const* VA, float* const* B, uint8_t* const* VB,
                         int lastMode, float* const* oldOut, float gravityDt, DevState* st, cudaStream_t s) {
     for(int d = 0; d < 3; ++d) {
@@ -850,9 +868,12 @@ void launch_extrapolate(const GridDesc& g, float* const* A, uint8_t* const* VA, 
             uint8_t* vout = (layer % 2 == 0) ? VB[d] : VA[d];
             int mode = layer == 3 ? lastMode : 0;
             float gdt = (mode == 1 && d == 1) ? gravityDt : 0.f;
-            const dim3 grid((unsigned)((sx + 31) / 32), (unsigned)((sy + 7) / 8), (unsigned)sz);
-            { k_extrapolate<<<grid, dim3(32, 8), 0, s>>>(sx, sy, sz, gin, vin, gout, vout, mode,
-                                                        oldOut ? oldOut[d] : nullptr, gdt, st); bnn_note_launch(); }
+            if(mode == 1) {
+                cudaMemsetAsync(oldOut[d], 0, nf * sizeof(float), s);
+                if(gdt != 0.f) { k_fill<<<kRegionBlocks, 256, 0, s>>>(gout, nf, 0.f - gdt); bnn_note_launch(); }
+            }
+            { k_extrapolate<<<kRegionBlocks, 256, 0, s>>>(sx, sy, sz, gin, vin, gout, vout, mode,
+                                                         oldOut ? oldOut[d] : nullptr, gdt, st); bnn_note_launch(); }
         }
     }
 }
@@ -874,15 +895,18 @@ void launch_build_rows(const GridDesc& g, int nrows, const uint32_t* rowCell, co
     { k_build_rows<<<nblk(nrows), 256, 0, s>>>(g, nrows, rowCell, phi, aidx, U[0], U[1], U[2], dt, rhs, diag, invdiag,
                                              nbr, st); bnn_note_launch(); }
 }
+// Reads velIn, writes the projected faces to velOut / validOut (zeroed here first).
 void launch_update_velocity(const GridDesc& g, const DevState* st, const float* phi, const uint32_t* aidx,
-                            const float* pressure, float dt, float* const* U, uint8_t* const* V, cudaStream_t s) {
-    const dim3 blk(32, 8);
-    const dim3 g0((unsigned)((face_sx(g, 0) + 31) / 32), (unsigned)((face_sy(g, 0) + 7) / 8), (unsigned)face_sz(g, 0));
-    const dim3 g1((unsigned)((face_sx(g, 1) + 31) / 32), (unsigned)((face_sy(g, 1) + 7) / 8), (unsigned)face_sz(g, 1));
-    const dim3 g2((unsigned)((face_sx(g, 2) + 31) / 32), (unsigned)((face_sy(g, 2) + 7) / 8), (unsigned)face_sz(g, 2));
-    { k_update_velocity<0><<<g0, blk, 0, s>>>(g, st, phi, aidx, pressure, dt, U[0], V[0]); bnn_note_launch(); }
-    { k_update_velocity<1><<<g1, blk, 0, s>>>(g, st, phi, aidx, pressure, dt, U[1], V[1]); bnn_note_launch(); }
-    { k_update_velocity<2><<<g2, blk, 0, s>>>(g, st, phi, aidx, pressure, dt, U[2], V[2]); bnn_note_launch(); }
+                            const float* pressure, float dt, float* const* velIn, float* const* velOut,
+                            uint8_t* const* validOut, cudaStream_t s) {
+    for(int d = 0; d < 3; ++d) {
+        const size_t nf = (size_t)face_sx(g, d) * face_sy(g, d) * face_sz(g, d);
+        cudaMemsetAsync(velOut[d], 0, nf * sizeof(float), s);
+        cudaMemsetAsync(validOut[d], 0, nf, s);
+    }
+    { k_update_velocity<0><<<kRegionBlocks, 256, 0, s>>>(g, st, phi, aidx, pressure, dt, velIn[0], velOut[0], validOut[0]); bnn_note_launch(); }
+    { k_update_velocity<1><<<kRegionBlocks, 256, 0, s>>>(g, st, phi, aidx, pressure, dt, velIn[1], velOut[1], validOut[1]); bnn_note_launch(); }
+    { k_update_velocity<2><<<kRegionBlocks, 256, 0, s>>>(g, st, phi, aidx, pressure, dt, velIn[2], velOut[2], validOut[2]); bnn_note_launch(); }
 }
 void launch_g2p(int n, const GridDesc& g, float* p6, size_t stride, const float* const* U, const float* const* O,
                 float ratio, int kind, float* C9, cudaStream_t s) {
