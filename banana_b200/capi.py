@@ -18,7 +18,7 @@ BNN_OK = 0
 STATUS = {0: "OK", 1: "INVALID_ARGUMENT", 2: "OUT_OF_MEMORY", 3: "PCG_NOT_CONVERGED", 4: "DEVICE_CHECK",
           5: "TIMEOUT", 6: "CUDA", 7: "NOT_SUPPORTED", 8: "CAPACITY"}
 STATUS_CODE = {v: k for k, v in STATUS.items()}
-SOLVER_KIND = {"FLIP": 0, "APIC": 1, "AFLIP": 2}
+SOLVER_KIND = {"FLIP": 0, "APIC": 1, "AFLIP": 2, "PIC": 3}
 PCG_MODE = {"fp32": 0, "fp64": 1, "refined": 2}
 FIELD = {"u": 0, "v": 1, "w": 2, "phi": 3, "pressure": 4, "old_u": 5, "old_v": 6, "old_w": 7, "active": 8}
 

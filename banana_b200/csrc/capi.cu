@@ -35,6 +35,7 @@ void launch_sort_finish(int n, size_t ncells, const uint32_t* cellOf, const uint
 void launch_p2g(const GridDesc& g, const uint32_t* cellStart, const float* g3, const float* p6, const float* C9,
                 const float4* rec, size_t stride, float* const* out, uint8_t* const* valid, bool affine,
                 const DevState* st, cudaStream_t s);
+void launch_advect_grid(const GridDesc& g, float** U, float** B, float dt, cudaStream_t s);
 void launch_extrapolate(const GridDesc& g, float* const* A, uint8_t* const* VA, float* const* B, uint8_t* const* VB,
                         int lastMode, float* const* oldOut, float gravityDt, DevState* st, cudaStream_t s);
 void launch_fluid_sdf(const GridDesc& g, const uint32_t* cellStart, const float4* rec, size_t stride, float* phi,
@@ -174,7 +175,7 @@ extern "C" int bnn_flip_create(const bnn_params* params, bnn_flip** out) {
     *out = nullptr;
     const bnn_params& P = *params;
     if(!(P.cell_size > 0.f) || P.advection_steps == 0) return BNN_ERR_INVALID_ARGUMENT;
-    if(P.solver_kind < 0 || P.solver_kind > 2) return BNN_ERR_NOT_SUPPORTED;
+    if(P.solver_kind < 0 || P.solver_kind > 3) return BNN_ERR_NOT_SUPPORTED;
     if(P.pcg_mode < 0 || P.pcg_mode > 2 || P.preconditioner != BNN_PRECOND_JACOBI) return BNN_ERR_NOT_SUPPORTED;
     for(int d = 0; d < 3; ++d) if(!(P.box_max[d] > P.box_min[d])) return BNN_ERR_INVALID_ARGUMENT;
     auto* h = new bnn_flip();
@@ -432,13 +433,18 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st) {
     h->cur = nxt;
     cudaEventRecord(h->ev[2], s);
     // P2G
-    launch_p2g(g, h->cellStart, h->g3, h->p6[h->cur], affine ? h->C9[h->cur] : nullptr, h->rec, h->cap, h->U, h->VA,
-               affine,
-               h->dst, s);
+    if(kind == BNN_SOLVER_PIC) {
+        // PIC_Solver::advanceVelocity (PIC_Solver.cpp:332-338): the grid velocity is advected
+        launch_advect_grid(g, h->U, h->B, substep, s);
+    } else {
+        launch_p2g(g, h->cellStart, h->g3, h->p6[h->cur], affine ? h->C9[h->cur] : nullptr, h->rec, h->cap, h->U,
+                   h->VA, affine, h->dst, s);
+    }
     cudaEventRecord(h->ev[3], s);
     const float gdt = h->P.apply_gravity ? 9.81f * substep : 0.f;
-    if(kind == BNN_SOLVER_APIC) {
-        // APIC_Solver::advanceVelocity: P2G then gravity, no extrapolation / backup
+    if(kind == BNN_SOLVER_APIC || kind == BNN_SOLVER_PIC) {
+        // APIC_Solver::advanceVelocity: P2G then gravity, no extrapolation / backup; PIC:
+        // advection then gravity
         if(h->P.apply_gravity) launch_add_scalar(h->U[1], h->F[1], -gdt, s);
     } else {
         // extrapolate, backup oldVels, Earth gravity (FLIP_Solver.cpp:44-47)
@@ -475,7 +481,10 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st) {
         std::swap(h->VA[d], h->VB[d]);
     }
     cudaEventRecord(h->ev[8], s);
-    launch_g2p(n, g, h->p6[h->cur], h->cap, h->U, h->O, h->P.pic_flip_ratio, kind, affine ? h->C9[h->cur] : nullptr, s);
+    // PIC_Solver leaves the particle velocities alone (no grid-to-particle transfer)
+    if(kind != BNN_SOLVER_PIC)
+        launch_g2p(n, g, h->p6[h->cur], h->cap, h->U, h->O, h->P.pic_flip_ratio, kind, affine ? h->C9[h->cur] : nullptr,
+                   s);
     cudaEventRecord(h->ev[9], s);
     BNN_CUDA_CHECK(cudaGetLastError());
     BNN_CUDA_CHECK(cudaMemcpyAsync(h->hst, h->dst, sizeof(DevState), cudaMemcpyDeviceToHost, s));

@@ -367,6 +367,42 @@ __global__ void __launch_bounds__(256) k_p2g(GridDesc g, const uint32_t* __restr
 }
 
 // ----------------------------------------------------------------------------------
+// PIC grid advection
+// ----------------------------------------------------------------------------------
+// PIC_Solver::advectGridVelocity + trace_rk2_grid (PIC_Solver.cpp:489-501, 1148-1154) for
+// component D: every face is traced back by RK2 through the grid velocity in grid units
+// (velocity x invCellSize) and takes component D there.  The caller swaps the output in
+// before the next component, as the reference copies each component back in turn.
+template<int D>
+__global__ void __launch_bounds__(256) k_advect_grid(GridDesc g, const float* __restrict__ u,
+                                                     const float* __restrict__ v, const float* __restrict__ w,
+                                                     float inv, float dt, float* __restrict__ out) {
+    const int sx = g.G[0] + (D == 0), sy = g.G[1] + (D == 1), sz = g.G[2] + (D == 2);
+    const size_t nf = (size_t)sx * sy * sz;
+    const size_t f = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if(f >= nf) return;
+    const int i = (int)(f % sx);
+    const int j = (int)((f / sx) % sy);
+    const int k = (int)(f / ((size_t)sx * sy));
+    const float ts = -dt;
+    const float gp[3] = {(float)i + (D == 0 ? 0.f : 0.5f), (float)j + (D == 1 ? 0.f : 0.5f),
+                         (float)k + (D == 2 ? 0.f : 0.5f)};
+    float gv[3];
+    vel_from_grid(g, u, v, w, gp[0], gp[1], gp[2], gv);
+    for(int c = 0; c < 3; ++c) gv[c] = gv[c] * inv;
+    const float h = 0.5f * ts;
+    const float mid[3] = {gp[0] + h * gv[0], gp[1] + h * gv[1], gp[2] + h * gv[2]};
+    vel_from_grid(g, u, v, w, mid[0], mid[1], mid[2], gv);
+    for(int c = 0; c < 3; ++c) gv[c] = gv[c] * inv;
+    const float bx = gp[0] + ts * gv[0], by = gp[1] + ts * gv[1], bz = gp[2] + ts * gv[2];
+    float val;
+    if(D == 0) val = interp_face(u, sx, sy, sz, bx, by - 0.5f, bz - 0.5f);
+    else if(D == 1) val = interp_face(v, sx, sy, sz, bx - 0.5f, by, bz - 0.5f);
+    else val = interp_face(w, sx, sy, sz, bx - 0.5f, by - 0.5f, bz);
+    out[f] = val;
+}
+
+// ----------------------------------------------------------------------------------
 // Velocity extrapolation (one layer)
 // ----------------------------------------------------------------------------------
 // Face-index distance (Chebyshev, per axis beyond the box) of face (i,j,k) from the
@@ -851,6 +887,20 @@ void launch_p2g(const GridDesc& g, const uint32_t* cellStart, const float* g3, c
         }
     }
 }
+// PIC grid advection of all three components; U[d] / B[d] are swapped after each one
+void launch_advect_grid(const GridDesc& g, float** U, float** B, float dt, cudaStream_t s) {
+    const float inv = 1.0f / g.dx;
+    for(int d = 0; d < 3; ++d) {
+        const size_t nf = (size_t)face_sx(g, d) * face_sy(g, d) * face_sz(g, d);
+        if(d == 0) { k_advect_grid<0><<<nblk(nf), 256, 0, s>>>(g, U[0], U[1], U[2], inv, dt, B[0]); bnn_note_launch(); }
+        if(d == 1) { k_advect_grid<1><<<nblk(nf), 256, 0, s>>>(g, U[0], U[1], U[2], inv, dt, B[1]); bnn_note_launch(); }
+        if(d == 2) { k_advect_grid<2><<<nblk(nf), 256, 0, s>>>(g, U[0], U[1], U[2], inv, dt, B[2]); bnn_note_launch(); }
+        float* t = U[d];
+        U[d] = B[d];
+        B[d] = t;
+    }
+}
+
 static constexpr unsigned kRegionBlocks = 148u * 8u;  // resident blocks of the region kernels
 
 // 4 layers per component; A holds the input and receives the result (4 is even).  Mode 1

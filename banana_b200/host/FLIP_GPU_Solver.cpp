@@ -100,6 +100,8 @@ static const bool s_registered = ParticleSolverFactory::registerSolver(FLIP_GPU_
     return std::static_pointer_cast<FLIP_GPU_Solver>(std::make_shared<APIC_GPU_Solver>());
 }) && ParticleSolverFactory::registerSolver(AFLIP_GPU_Solver::solverName(), [] {
     return std::static_pointer_cast<FLIP_GPU_Solver>(std::make_shared<AFLIP_GPU_Solver>());
+}) && ParticleSolverFactory::registerSolver(PIC_GPU_Solver::solverName(), [] {
+    return std::static_pointer_cast<FLIP_GPU_Solver>(std::make_shared<PIC_GPU_Solver>());
 });
 
 // ---------------------------------------------------------------------------------

@@ -152,6 +152,13 @@ public:
     std::string getSolverName() override { return solverName(); }
 };
 
+class PIC_GPU_Solver : public FLIP_GPU_Solver {
+public:
+    PIC_GPU_Solver() : FLIP_GPU_Solver(BNN_SOLVER_PIC) {}
+    static std::string solverName() { return "PIC_GPU_3DSolver"; }
+    std::string getSolverName() override { return solverName(); }
+};
+
 // ParticleSolverFactory (ParticleSolverFactory.h:30-60): solvers by name, and by the
 // "Solver" entry of a scene's GlobalParameters
 class ParticleSolverFactory {

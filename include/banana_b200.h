@@ -46,6 +46,8 @@ extern "C" {
 #define BNN_SOLVER_FLIP   0  /* FLIP_3DSolver  (FLIP_Solver.cpp)  */
 #define BNN_SOLVER_APIC   1  /* APIC_3DSolver  (APIC_Solver.cpp)  */
 #define BNN_SOLVER_AFLIP  2  /* AFLIP_3DSolver (AFLIP_Solver.cpp) */
+#define BNN_SOLVER_PIC    3  /* PIC_3DSolver (PIC_Solver.cpp): semi-Lagrangian grid advection,
+                                particles only mark the fluid */
 
 #define BNN_PCG_FP32      0  /* FP32 vectors, FP64 dot/norm reductions */
 #define BNN_PCG_FP64      1  /* FP64 vectors and reductions */

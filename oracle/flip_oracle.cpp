@@ -755,6 +755,36 @@ public:
     }
     void extrapolateAll() { for(int d = 0; d < 3; ++d) extrapolate(u[d], tmp[d], valid[d], oldValid[d]); }
 
+    // PIC_Solver::advectGridVelocity + trace_rk2_grid (PIC_Solver.cpp:489-501, 1148-1154):
+    // semi-Lagrangian back-trace of every face through the grid velocity, RK2 in grid
+    // units (velocity x invCellSize, Grid.cpp:38-44).  Each component is copied back before
+    // the next one is advected, so v is traced through the advected u, and w through both.
+    void advectGrid(R dt) {
+        const R inv = R(1.0) / dx;
+        const R ts = -dt;
+        for(int d = 0; d < 3; ++d) {
+            Arr3<R>& out = tmp[d];
+            const int sx = u[d].sx, sy = u[d].sy, sz = u[d].sz;
+#pragma omp parallel for schedule(static) if(nthreads() > 1)
+            for(int k = 0; k < sz; ++k)
+                for(int j = 0; j < sy; ++j)
+                    for(int i = 0; i < sx; ++i) {
+                        const R gp[3] = {(R)i + (d == 0 ? R(0) : R(0.5)), (R)j + (d == 1 ? R(0) : R(0.5)),
+                                         (R)k + (d == 2 ? R(0) : R(0.5))};
+                        R gv[3];
+                        for(int c = 0; c < 3; ++c) gv[c] = velFromGrid(gp, c, u) * inv;
+                        const R h = R(0.5) * ts;
+                        R mid[3];
+                        for(int c = 0; c < 3; ++c) mid[c] = gp[c] + h * gv[c];
+                        for(int c = 0; c < 3; ++c) gv[c] = velFromGrid(mid, c, u) * inv;
+                        R back[3];
+                        for(int c = 0; c < 3; ++c) back[c] = gp[c] + ts * gv[c];
+                        out(i, j, k) = velFromGrid(back, d, u);
+                    }
+            u[d].d = out.d;
+        }
+    }
+
     // PIC_Solver::addGravity, Earth gravity (PIC_Solver.cpp:505-511)
     void addGravity(R dt) {
         if(!P.apply_gravity) return;
@@ -998,9 +1028,12 @@ public:
         if(P.sort_each_step) sortParticlesByCell();
         double t2 = now();
         int kind = P.solver_kind;
-        mapP2G();
+        // PIC_Solver::advanceVelocity (PIC_Solver.cpp:332-338): advect the grid velocity,
+        // gravity, projection, extrapolation; the particles only carry the fluid SDF
+        if(kind == 3) advectGrid(substep);
+        else mapP2G();
         double t3 = now();
-        if(kind != 1) extrapolateAll(); // APIC goes straight to gravity (APIC_Solver.cpp:42-49)
+        if(kind != 1 && kind != 3) extrapolateAll(); // APIC goes straight to gravity (APIC_Solver.cpp:42-49)
         if(kind == 0 || kind == 2) for(int d = 0; d < 3; ++d) old[d].d = u[d].d;   // backupGridVelocity
         double t4 = now();
         addGravity(substep);
@@ -1016,7 +1049,7 @@ public:
         if(kind == 0 || kind == 2)
             for(int d = 0; d < 3; ++d)
                 for(size_t i = 0; i < u[d].size(); ++i) dV[d].d[i] = u[d].d[i] - old[d].d[i];
-        mapG2P();
+        if(kind != 3) mapG2P();
         double t9 = now();
         frameTime += substep;
         if(st) {
@@ -1182,6 +1215,15 @@ int orc_set_grid(void* hp, int which, const float* in) {
 int orc_step(void* hp, orc_step_stats* st) {
     auto* h = (orc_handle*)hp;
     if(h->dbl) h->d->step(st); else h->f->step(st);
+    return 0;
+}
+
+// The cell sort and P2G alone (FLIP_Solver::mapParticles2Grid on the current particles),
+// for analytic checks of the transfer
+int orc_p2g_only(void* hp) {
+    auto* h = (orc_handle*)hp;
+    if(h->dbl) { h->d->sortParticlesByCell(); h->d->mapP2G(); }
+    else { h->f->sortParticlesByCell(); h->f->mapP2G(); }
     return 0;
 }
 

@@ -80,6 +80,7 @@ def lib() -> C.CDLL:
         L.orc_get_grid_f64.argtypes = [vp, C.c_int, dp]; L.orc_get_grid_f64.restype = C.c_int
         L.orc_set_grid.argtypes = [vp, C.c_int, fp]; L.orc_set_grid.restype = C.c_int
         L.orc_step.argtypes = [vp, C.POINTER(OrcStepStats)]; L.orc_step.restype = C.c_int
+        L.orc_p2g_only.argtypes = [vp]; L.orc_p2g_only.restype = C.c_int
         L.orc_system_nnz.argtypes = [vp]; L.orc_system_nnz.restype = C.c_uint32
         L.orc_get_system.argtypes = [vp, u32p, u32p, fp, fp]; L.orc_get_system.restype = None
         L.orc_pcg.argtypes = [C.c_uint32, u32p, u32p, fp, fp, C.c_float, C.c_uint32, C.c_int, C.c_int, C.c_float,
@@ -211,6 +212,10 @@ class Oracle:
         st = OrcStepStats()
         self.L.orc_step(self.h, C.byref(st))
         return {f: getattr(st, f) for f, _ in OrcStepStats._fields_}
+
+    def p2g_only(self) -> None:
+        """Sort the particles by cell and run P2G alone (grid fields then hold its result)."""
+        self.L.orc_p2g_only(self.h)
 
     def system(self):
         """(rowStart, colIndex, values, rhs) of the last pressure system"""

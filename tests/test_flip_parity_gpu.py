@@ -71,9 +71,11 @@ def test_flip_64_bitexact_first_steps(bnn, oracle_mod):
         _compare_step(g, o, s)
 
 
-@pytest.mark.parametrize("kind", ["APIC", "AFLIP"])
-def test_affine_variants_bitexact(bnn, oracle_mod, kind):
-    k = {"APIC": 1, "AFLIP": 2}[kind]
+@pytest.mark.parametrize("kind", ["APIC", "AFLIP", "PIC"])
+def test_variants_bitexact(bnn, oracle_mod, kind):
+    """APIC / AFLIP (affine P2G and G2P) and PIC (semi-Lagrangian grid advection, particles
+    as fluid markers only)"""
+    k = {"APIC": 1, "AFLIP": 2, "PIC": 3}[kind]
     g, o = _pair(bnn, oracle_mod, 24, solver_kind=k)
     for s in range(12):
         _compare_step(g, o, s)
