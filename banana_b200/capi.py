@@ -28,7 +28,7 @@ EXPORTS = [
     "bnn_flip_num_particles", "bnn_flip_get_grid", "bnn_flip_step", "bnn_flip_advance_frame",
     "bnn_flip_device_particles", "bnn_flip_step_host", "bnn_flip_stream", "bnn_cell_sort", "bnn_cell_sort_noalloc", "bnn_z_sort", "bnn_neighbors",
     "bnn_pcg_solve_7pt", "bnn_version", "bnn_last_error", "bnn_launch_count",
-    "bnn_flip_device_bytes", "bnn_scene_bytes_estimate",
+    "bnn_flip_device_bytes", "bnn_scene_bytes_estimate", "bnn_flip_set_grid",
     "bnn_batch_create", "bnn_batch_destroy", "bnn_batch_add_scene", "bnn_batch_remove_scene", "bnn_batch_step",
     "bnn_batch_scene_info", "bnn_batch_get_scene", "bnn_batch_memory",
 ]
@@ -113,6 +113,7 @@ def load() -> C.CDLL:
     L.bnn_pcg_solve_7pt.argtypes = [C.c_uint32, fp, i32p, C.c_float, fp, C.c_float, C.c_uint32, C.c_int32, C.c_float,
                                     dp, C.POINTER(PcgStats)]
     L.bnn_flip_device_bytes.argtypes = [vp, u64p]
+    L.bnn_flip_set_grid.argtypes = [vp, C.c_int32, fp, C.c_size_t]
     L.bnn_scene_bytes_estimate.argtypes = [C.POINTER(Params), C.c_uint32, u64p]
     L.bnn_batch_create.argtypes = [C.POINTER(BatchParams), C.POINTER(vp)]
     L.bnn_batch_destroy.argtypes = [vp]

@@ -36,6 +36,7 @@ void launch_p2g(const GridDesc& g, const uint32_t* cellStart, const float* g3, c
                 const float4* rec, size_t stride, float* const* out, uint8_t* const* valid, bool affine,
                 const DevState* st, cudaStream_t s);
 void launch_advect_grid(const GridDesc& g, float** U, float** B, float dt, cudaStream_t s);
+void launch_maxabs(const float* a, size_t n, unsigned* maxBits, cudaStream_t s);
 void launch_extrapolate(const GridDesc& g, float* const* A, uint8_t* const* VA, float* const* B, uint8_t* const* VB,
                         int lastMode, float* const* oldOut, float gravityDt, DevState* st, cudaStream_t s);
 void launch_fluid_sdf(const GridDesc& g, const uint32_t* cellStart, const float4* rec, size_t stride, float* phi,
@@ -364,6 +365,21 @@ extern "C" int bnn_flip_device_particles(bnn_flip* h, float** p6, uint32_t** ids
     if(!h) return BNN_ERR_INVALID_ARGUMENT;
     if(p6) *p6 = h->p6[h->cur];
     if(ids) *ids = h->ids[h->cur];
+    return BNN_OK;
+}
+
+// Replace the face velocities of one component (a saved memory state, PIC_Solver::
+// loadMemoryState, PIC_Solver.cpp:158-206); the CFL maximum is taken from the new field.
+extern "C" int bnn_flip_set_grid(bnn_flip* h, int32_t field, const float* in, size_t count) {
+    if(!h || !in || field < BNN_FIELD_U || field > BNN_FIELD_W) return BNN_ERR_INVALID_ARGUMENT;
+    if(count != h->F[field]) return BNN_ERR_INVALID_ARGUMENT;
+    BNN_CUDA_CHECK(cudaMemcpyAsync(h->U[field], in, count * sizeof(float), cudaMemcpyHostToDevice, h->s));
+    BNN_CUDA_CHECK(cudaMemsetAsync(&h->dst->maxvel_bits, 0, sizeof(unsigned), h->s));
+    for(int d = 0; d < 3; ++d) launch_maxabs(h->U[d], h->F[d], &h->dst->maxvel_bits, h->s);
+    BNN_CUDA_CHECK(cudaMemcpyAsync(&h->hst->maxvel_bits, &h->dst->maxvel_bits, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                                   h->s));
+    BNN_CUDA_CHECK(cudaStreamSynchronize(h->s));
+    h->maxvelBits = h->hst->maxvel_bits;
     return BNN_OK;
 }
 

@@ -505,6 +505,22 @@ __global__ void __launch_bounds__(256) k_extrapolate(int sx, int sy, int sz, con
     }
 }
 
+// max |a| over an array, folded into *maxBits (float bits of a non-negative value order
+// like the unsigned integers)
+__global__ void __launch_bounds__(256) k_maxabs(const float* __restrict__ a, size_t n, unsigned* maxBits) {
+    float m = 0.f;
+    for(size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        m = fmaxf(m, fabsf(a[i]));
+    __shared__ float sm[8];
+    for(int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
+    if((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if(threadIdx.x == 0) {
+        for(int w = 1; w < 8; ++w) m = fmaxf(m, sm[w]);
+        if(m > 0.f) atomicMax(maxBits, __float_as_uint(m));
+    }
+}
+
 __global__ void k_fill(float* __restrict__ a, size_t n, float v) {
     for(size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) a[i] = v;
 }
@@ -901,7 +917,11 @@ void launch_advect_grid(const GridDesc& g, float** U, float** B, float dt, cudaS
     }
 }
 
-static constexpr unsigned kRegionBlocks = 148u * 8u;  // resident blocks of the region kernels
+static constexpr unsigned kRegionBlocks = 148u * 8u;
+
+void launch_maxabs(const float* a, size_t n, unsigned* maxBits, cudaStream_t s) {
+    if(n) { k_maxabs<<<kRegionBlocks, 256, 0, s>>>(a, n, maxBits); bnn_note_launch(); }
+}  // resident blocks of the region kernels
 
 // 4 layers per component; A holds the input and receives the result (4 is even).  Mode 1
 // first writes the values the last layer gives every face beyond its region: backup 0,

@@ -1,8 +1,12 @@
 // FLIP_GPU_Solver: ParticleSolver-shaped host class over the banana_b200 C ABI.
 #include "FLIP_GPU_Solver.h"
 
+#include "bnn_io.h"
 #include "json_lite.h"
 
+#include <future>
+
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -143,8 +147,17 @@ void FLIP_GPU_Solver::loadSceneFromString(const std::string& sceneJson, bool all
     read_value(g, "FinalFrame", G.finalFrame);
     read_bool(g, "ApplyGravity", G.bApplyGravity);
     read_bool(g, "SaveFrameData", G.bSaveFrameData);
+    read_bool(g, "SaveMemoryState", G.bSaveMemoryState);
+    read_bool(g, "LoadMemoryState", G.bLoadMemoryState);
+    read_value(g, "FramePerState", G.framePerState);
+    if(G.framePerState == 0) G.framePerState = 1;
     read_string(g, "DataPath", G.dataPath);
     read_string(g, "FrameDataFolder", G.frameDataFolder);
+    read_string(g, "MemoryStateDataFolder", G.memoryStateDataFolder);
+    G.SaveDataList.clear();
+    const Json& opt = g["OptionalSavingData"];
+    for(size_t q = 0; q < opt.size(); ++q)
+        if(opt[q].kind == Json::String) G.SaveDataList.push_back(opt[q].str);
 
     const Json& s = j["SimulationParameters"];
     auto& P = m_SolverParams;
@@ -183,7 +196,12 @@ void FLIP_GPU_Solver::loadSceneFromString(const std::string& sceneJson, bool all
     P.particleRadius = P.cellSize / P.ratioCellSizePRadius;
 
     generateParticles(j);
-    if(allocate) allocateSolverMemory();
+    if(!allocate) return;
+    allocateSolverMemory();
+    if(G.bLoadMemoryState) {
+        const int frame = loadMemoryState();
+        if(frame > 0) G.finishedFrame = (unsigned)frame;
+    }
 }
 
 // ParticleSolver::generateParticles (ParticleSolver.cpp:302-310) for box generators
@@ -288,36 +306,133 @@ void FLIP_GPU_Solver::doFrameSimulation(unsigned frame) {
     ++m_GlobalParams.finishedFrame;
     m_GlobalParams.frameLocalTime = 0.f;
     if(m_GlobalParams.bSaveFrameData) saveFrameData();
+    if(m_GlobalParams.bSaveMemoryState) saveMemoryState();
 }
 
-// ParticleSolver::doSimulation (ParticleSolver.cpp:134-156)
+// ParticleSolver::doSimulation (ParticleSolver.cpp:134-156); a resumed run continues
+// after the frame of its memory state
 void FLIP_GPU_Solver::doSimulation() {
-    for(unsigned frame = m_GlobalParams.startFrame; frame <= m_GlobalParams.finalFrame; ++frame)
-        doFrameSimulation(frame);
+    const unsigned first = std::max(m_GlobalParams.startFrame, m_GlobalParams.finishedFrame + 1u);
+    for(unsigned frame = first; frame <= m_GlobalParams.finalFrame; ++frame) doFrameSimulation(frame);
+    waitForFrameOutput();
 }
 
 void FLIP_GPU_Solver::finalizeSimulation() {
+    waitForFrameOutput();
     if(m_Gpu) {
         bnn_flip_destroy(m_Gpu);
         m_Gpu = nullptr;
     }
 }
 
-// Frame output: positions and velocities as raw little-endian float32 AoS with a small
-// header (n, then 3n positions, 3n velocities).  The reference's .bnn container
-// (ParticleSerialization) is not reproduced.
+void FLIP_GPU_Solver::waitForFrameOutput() {
+    if(m_FrameWriter) {
+        static_cast<std::future<void>*>(m_FrameWriter.get())->wait();
+        m_FrameWriter.reset();
+    }
+}
+
+// PIC_Solver::saveFrameData (PIC_Solver.cpp:236-263): particle_radius and compressed
+// positions, plus object indices / compressed velocities when the scene asks for them;
+// the file is written on a background thread while the next frame runs (the host arrays
+// are copied first, so the caller may keep using them).
 int FLIP_GPU_Solver::saveFrameData() {
-    char name[64];
-    std::snprintf(name, sizeof(name), "frame.%04u.f32", m_GlobalParams.finishedFrame);
-    const std::string path = m_GlobalParams.dataPath + "/" + name;
-    std::FILE* f = std::fopen(path.c_str(), "wb");
-    if(!f) return -1;
-    const uint32_t n = m_ParticleData.getNParticles();
-    std::fwrite(&n, sizeof(n), 1, f);
-    std::fwrite(m_ParticleData.positions.data(), sizeof(float), 3 * (size_t)n, f);
-    std::fwrite(m_ParticleData.velocities.data(), sizeof(float), 3 * (size_t)n, f);
-    std::fclose(f);
+    const auto& G = m_GlobalParams;
+    if(!make_output_folder(G.dataPath, G.frameDataFolder)) return -1;
+    auto file = std::make_shared<BnnFile>();
+    const auto& D = m_ParticleData;
+    file->nParticles = D.getNParticles();
+    const float radius = m_SolverParams.particleRadius;
+    file->setFixedReal("particle_radius", &radius, 1);
+    if(G.savingData("ObjectIndex")) {
+        file->setFixedUInt("NObjects", &D.nObjects, 1);
+        std::vector<uint16_t> idx(D.objectIndex.begin(), D.objectIndex.end());
+        file->setParticleUInt16("object_index", idx.data());
+    }
+    file->setParticleCompressed("particle_position", D.positions.data(), 3);
+    if(G.savingData("ParticleVelocity")) file->setParticleCompressed("particle_velocity", D.velocities.data(), 3);
+    const std::string path = bnn_file_path(G.dataPath, G.frameDataFolder, "frame", (int)G.finishedFrame);
+    waitForFrameOutput();
+    auto fut = std::make_shared<std::future<void>>(std::async(std::launch::async, [file, path] { file->write(path); }));
+    m_FrameWriter = std::static_pointer_cast<void>(fut);
     return 0;
+}
+
+// PIC_Solver::saveMemoryState (PIC_Solver.cpp:210-232): every FramePerState frames the
+// grid resolution and face velocities, the particle radius, object count and the raw
+// particle data
+int FLIP_GPU_Solver::saveMemoryState() {
+    const auto& G = m_GlobalParams;
+    if(G.finishedFrame % G.framePerState != 0) return -1;
+    if(!make_output_folder(G.dataPath, G.memoryStateDataFolder)) return -1;
+    BnnFile file;
+    int32_t gd[3];
+    check(bnn_flip_grid_dims(m_Gpu, gd), "bnn_flip_grid_dims");
+    const uint32_t res[3] = {(uint32_t)gd[0], (uint32_t)gd[1], (uint32_t)gd[2]};
+    file.setFixedUInt("grid_resolution", res, 3);
+    for(int d = 0; d < 3; ++d) {
+        const size_t nf = (size_t)(res[0] + (d == 0)) * (res[1] + (d == 1)) * (res[2] + (d == 2));
+        std::vector<float> u(nf);
+        check(bnn_flip_get_grid(m_Gpu, d, u.data(), nf), "bnn_flip_get_grid");
+        file.setFixedReal("grid_velocity_" + std::to_string(d), u.data(), (uint32_t)nf);
+    }
+    const auto& D = m_ParticleData;
+    file.nParticles = D.getNParticles();
+    file.setFixedUInt("NObjects", &D.nObjects, 1);
+    const float radius = m_SolverParams.particleRadius;
+    file.setFixedReal("particle_radius", &radius, 1);
+    file.setParticleReal("particle_position", D.positions.data(), 3);
+    file.setParticleReal("particle_velocity", D.velocities.data(), 3);
+    std::vector<uint16_t> idx(D.objectIndex.begin(), D.objectIndex.end());
+    file.setParticleUInt16("object_index", idx.data());
+    return file.write(bnn_file_path(G.dataPath, G.memoryStateDataFolder, "frame", (int)G.finishedFrame)) ? 0 : -1;
+}
+
+// PIC_Solver::loadMemoryState (PIC_Solver.cpp:158-206): the latest state file up to
+// FinalFrame; its particles and face velocities replace the generated ones
+int FLIP_GPU_Solver::loadMemoryState() {
+    const auto& G = m_GlobalParams;
+    int frame = -1;
+    BnnFile file;
+    for(int f = (int)G.finalFrame; f >= 0; --f) {
+        if(file.read(bnn_file_path(G.dataPath, G.memoryStateDataFolder, "frame", f))) {
+            frame = f;
+            break;
+        }
+    }
+    if(frame < 0) return -1;
+    std::vector<uint32_t> res;
+    int32_t gd[3];
+    check(bnn_flip_grid_dims(m_Gpu, gd), "bnn_flip_grid_dims");
+    if(!file.getUInts("grid_resolution", res) || res.size() != 3 || (int)res[0] != gd[0] || (int)res[1] != gd[1] ||
+       (int)res[2] != gd[2]) {
+        std::fprintf(stderr, "%s: memory state grid does not match the scene\n", getSolverName().c_str());
+        std::exit(EXIT_FAILURE);
+    }
+    auto& D = m_ParticleData;
+    std::vector<float> pos, vel;
+    if(!file.getFloats("particle_position", pos) || !file.getFloats("particle_velocity", vel) ||
+       pos.size() != vel.size() || pos.size() != 3 * (size_t)file.nParticles) {
+        std::fprintf(stderr, "%s: memory state without particle data\n", getSolverName().c_str());
+        std::exit(EXIT_FAILURE);
+    }
+    D.positions = pos;
+    D.velocities = vel;
+    std::vector<uint16_t> idx;
+    if(file.getUInt16("object_index", idx) && idx.size() == file.nParticles)
+        D.objectIndex.assign(idx.begin(), idx.end());
+    else
+        D.objectIndex.assign(file.nParticles, 0);
+    std::vector<uint32_t> nobj;
+    if(file.getUInts("NObjects", nobj) && !nobj.empty()) D.nObjects = nobj[0];
+    check(bnn_flip_set_particles(m_Gpu, D.positions.data(), D.velocities.data(), D.getNParticles()),
+          "bnn_flip_set_particles");
+    for(int d = 0; d < 3; ++d) {
+        std::vector<float> u;
+        if(!file.getFloats("grid_velocity_" + std::to_string(d), u)) std::exit(EXIT_FAILURE);
+        check(bnn_flip_set_grid(m_Gpu, d, u.data(), u.size()), "bnn_flip_set_grid");
+    }
+    return frame;
 }
 
 } // namespace bnnhost

@@ -36,8 +36,18 @@ struct GlobalParameters {
     float frameLocalTime = 0.0f;
     bool bApplyGravity = true;
     bool bSaveFrameData = false;
+    bool bSaveMemoryState = false;
+    bool bLoadMemoryState = false;
+    unsigned framePerState = 1u;
     std::string dataPath = ".";
-    std::string frameDataFolder = "FLIPData";
+    std::string frameDataFolder = "FrameData";
+    std::string memoryStateDataFolder = "MemoryState";
+    std::vector<std::string> SaveDataList;  // "OptionalSavingData": "ObjectIndex", "ParticleVelocity"
+    bool savingData(const std::string& name) const {
+        for(const auto& s : SaveDataList)
+            if(s == name) return true;
+        return false;
+    }
 };
 
 // SimulationParameters + PIC_Parameters (ParticleSolverData.h:87-175, PIC_Data.h:31-40),
@@ -96,7 +106,8 @@ public:
     FLIP_GPU_Solver(const FLIP_GPU_Solver&) = delete;
     FLIP_GPU_Solver& operator=(const FLIP_GPU_Solver&) = delete;
 
-    // ParticleSolver public API (ParticleSolver.cpp:36-238)
+    // ParticleSolver public API (ParticleSolver.cpp:36-238).  A scene with LoadMemoryState
+    // resumes from the latest state file; doSimulation then continues after that frame.
     // allocate = false stops after the particles are generated (no GPU needed)
     void loadScene(const std::string& sceneFile, bool allocate = true);
     void loadSceneFromString(const std::string& sceneJson, bool allocate = true);
@@ -123,7 +134,12 @@ protected:
     virtual void allocateSolverMemory();
     virtual void advanceFrame();
     virtual void sortParticles() {}  // the device sorts by cell every sub-step
+    // .bnn frame output and memory states (PIC_Solver.cpp:123-263); 0 = done, -1 = not
+    // done / failed; loadMemoryState returns the frame of the state it loaded
     virtual int saveFrameData();
+    virtual int saveMemoryState();
+    virtual int loadMemoryState();
+    void waitForFrameOutput();
 
     // A failing C ABI call: log it, and exit where the reference exits (__BNN_REQUIRE,
     // Macros.h:225-233; ExitIfPressureProjectionFailed, PIC_Solver.cpp:901-906)
@@ -136,6 +152,7 @@ protected:
     ParticleData m_ParticleData;
     bnn_flip* m_Gpu = nullptr;
     std::vector<FrameLog> m_Logs;
+    std::shared_ptr<void> m_FrameWriter;  // std::future of the frame file being written
 };
 
 class APIC_GPU_Solver : public FLIP_GPU_Solver {

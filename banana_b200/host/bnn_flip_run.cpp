@@ -49,9 +49,11 @@ int main(int argc, char** argv) {
     solver->loadScene(scene);
     auto& G = solver->globalParams();
     if(frames > 0) G.finalFrame = G.startFrame + (unsigned)frames - 1;
-    std::printf("{\"solver\": \"%s\", \"particles\": %u}\n", solver->getSolverName().c_str(),
-                solver->generalParticleData().getNParticles());
-    for(unsigned f = G.startFrame; f <= G.finalFrame; ++f) {
+    std::printf("{\"solver\": \"%s\", \"particles\": %u, \"resumed_after_frame\": %u}\n",
+                solver->getSolverName().c_str(), solver->generalParticleData().getNParticles(), G.finishedFrame);
+    // a scene that resumes from a memory state continues after the state's frame
+    const unsigned first = G.startFrame > G.finishedFrame + 1 ? G.startFrame : G.finishedFrame + 1;
+    for(unsigned f = first; f <= G.finalFrame; ++f) {
         const auto t0 = std::chrono::steady_clock::now();
         solver->doFrameSimulation(f);
         const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();

@@ -122,6 +122,10 @@ int bnn_flip_set_particles(bnn_flip* h, const float* pos, const float* vel, uint
  * positions / velocities as raw host arrays between frames). */
 int bnn_flip_get_particles(bnn_flip* h, float* pos, float* vel);
 int bnn_flip_num_particles(bnn_flip* h, uint32_t* n);
+/* Replace the face velocities of one component (BNN_FIELD_U/V/W; count = its face count),
+ * e.g. from a saved memory state (PIC_Solver::loadMemoryState, PIC_Solver.cpp:158-206);
+ * the next sub-step's CFL uses the new field. */
+int bnn_flip_set_grid(bnn_flip* h, int32_t field, const float* in, size_t count);
 /* Copy one grid field (BNN_FIELD_*) of `count` floats to host. */
 int bnn_flip_get_grid(bnn_flip* h, int32_t field, float* out, size_t count);
 /* One iteration of PIC_Solver::advanceFrame's sub-step loop (CFL, moveParticles,

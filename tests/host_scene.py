@@ -6,11 +6,14 @@ import json
 import numpy as np
 
 
-def dam_break_scene(n: int, frames: int = 2, block=(0.4, 0.6, 0.4), solver: str = "FLIP_GPU_3DSolver") -> str:
+def dam_break_scene(n: int, frames: int = 2, block=(0.4, 0.6, 0.4), solver: str = "FLIP_GPU_3DSolver",
+                    **globals_) -> str:
     f32 = lambda v: float(np.float32(v))  # noqa: E731
+    g = {"Solver": solver, "FrameDuration": f32(1.0 / 30.0), "StartFrame": 1, "FinalFrame": frames,
+         "SaveFrameData": False}
+    g.update(globals_)
     return json.dumps({
-        "GlobalParameters": {"Solver": solver, "FrameDuration": f32(1.0 / 30.0), "StartFrame": 1,
-                             "FinalFrame": frames, "SaveFrameData": False},
+        "GlobalParameters": g,
         "SimulationParameters": {
             "SimulationDomainBox": {"BoxMin": [0, 0, 0], "BoxMax": [1, 1, 1]},
             "CellSize": 1.0 / n, "NExpandCells": 2, "CFLFactor": 1, "MinTimestep": 1e-6,

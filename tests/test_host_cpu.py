@@ -7,6 +7,7 @@ import pytest
 
 from banana_b200 import build as bld
 from banana_b200 import scenes
+from tests.bnn_format import read_bnn, values
 from tests.host_scene import dam_break_scene, read_particles
 
 
@@ -36,3 +37,62 @@ def test_unknown_solver_is_refused(driver, tmp_path):
     scene.write_text(dam_break_scene(16, solver="SPH_3DSolver"))
     r = subprocess.run([str(driver), str(scene)], capture_output=True, text=True, timeout=60)
     assert r.returncode == 1 and "not supported" in r.stderr
+
+
+BNN_SELFTEST = r"""
+#include "bnn_io.h"
+#include <cstdio>
+#include <vector>
+int main(int argc, char** argv) {
+    bnnhost::BnnFile f;
+    f.nParticles = 5;
+    const float radius = 0.25f;
+    const unsigned res[3] = {7, 8, 9};
+    const unsigned nobj = 2;
+    std::vector<float> pos = {0.f, 1.f, 2.f, 0.5f, -1.f, 2.5f, 0.25f, 0.f, 2.f, 1.f, 1.f, 3.f, 0.75f, 0.5f, 2.25f};
+    std::vector<unsigned short> idx = {0, 1, 1, 0, 1};
+    f.setFixedReal("particle_radius", &radius, 1);
+    f.setFixedUInt("grid_resolution", res, 3);
+    f.setFixedUInt("NObjects", &nobj, 1);
+    f.setParticleReal("particle_velocity", pos.data(), 3);
+    f.setParticleCompressed("particle_position", pos.data(), 3);
+    f.setParticleUInt16("object_index", idx.data());
+    if(!f.write(argv[1])) return 1;
+    bnnhost::BnnFile g;
+    if(!g.read(argv[1])) return 2;
+    std::vector<float> v, c;
+    std::vector<unsigned> u;
+    if(!g.getFloats("particle_velocity", v) || v != pos) return 3;
+    if(!g.getUInts("grid_resolution", u) || u.size() != 3 || u[2] != 9) return 4;
+    if(!g.getFloats("particle_position", c) || c.size() != pos.size()) return 5;
+    for(size_t i = 0; i < c.size(); ++i) if(c[i] < pos[i] - 1e-4f || c[i] > pos[i] + 1e-4f) return 6;
+    return 0;
+}
+"""
+
+
+def test_bnn_file_format_round_trip(tmp_path):
+    """The .bnn writer / reader of the C++ class: the reference's header layout, attribute
+    order (fixed, then particle, each by name), raw and 16-bit compressed encodings."""
+    src = tmp_path / "t.cpp"
+    src.write_text(BNN_SELFTEST)
+    exe = tmp_path / "t"
+    host = bld.HOST
+    subprocess.run(["g++", "-O1", "-std=c++17", "-I", str(host), str(src), str(host / "bnn_io.cpp"), "-o", str(exe)],
+                   check=True)
+    out = tmp_path / "f.bnn"
+    subprocess.run([str(exe), str(out)], check=True)
+    n, attrs, order = read_bnn(out)
+    assert n == 5
+    assert order == ["NObjects", "grid_resolution", "particle_radius", "object_index", "particle_position",
+                     "particle_velocity"]
+    assert attrs["particle_radius"]["type"] == "real" and attrs["particle_radius"]["bytes"] == 4
+    assert list(values(attrs["grid_resolution"])) == [7, 8, 9]
+    pos = values(attrs["particle_velocity"]).reshape(5, 3)
+    dec, lo, hi, q = values(attrs["particle_position"])
+    assert attrs["particle_position"]["bytes"] == 24 + 2 * 15
+    assert np.array_equal(lo, pos.min(0)) and np.array_equal(hi, pos.max(0))
+    expect = np.trunc(np.float32(65535.0) * ((pos - lo) / np.where(hi > lo, hi - lo, 1))).astype(np.uint16)
+    assert np.array_equal(q.astype(np.uint16), expect)
+    assert np.abs(dec - pos).max() <= (hi - lo).max() / 65535 + 1e-6
+    assert list(values(attrs["object_index"])) == [0, 1, 1, 0, 1]

@@ -8,6 +8,7 @@ import pytest
 
 from banana_b200 import build as bld
 from banana_b200 import scenes
+from tests.bnn_format import read_bnn, values
 from tests.host_scene import dam_break_scene, read_particles
 
 pytestmark = pytest.mark.gpu
@@ -42,3 +43,39 @@ def test_driver_frames_match_python_and_oracle(bnn, oracle_mod, tmp_path, solver
             pass
     po, vo = o.get_particles()
     assert np.array_equal(pos, po) and np.array_equal(vel, vo)
+
+
+def test_memory_state_resume_and_bnn_frames(bnn, tmp_path):
+    """SaveMemoryState / LoadMemoryState (PIC_Solver.cpp:158-232): a run that stops after
+    frame 2 and a second run resuming from its state file reach frame 3 with exactly the
+    particles of one straight 3-frame run.  The .bnn frame files hold the frame's particles
+    (16-bit compressed positions, within one quantisation step)."""
+    exe = bld.build_host()
+    n = 16
+    data = tmp_path / "data"
+    common = {"DataPath": str(data), "FramePerState": 2, "OptionalSavingData": ["ParticleVelocity", "ObjectIndex"]}
+
+    def run(name, frames, **g):
+        sc = tmp_path / f"{name}.json"
+        sc.write_text(dam_break_scene(n, frames=frames, **dict(common, **g)))
+        out = tmp_path / f"{name}.f32"
+        r = subprocess.run([str(exe), str(sc), "--out", str(out)], capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        return read_particles(out), r.stdout
+
+    (p3, v3), _ = run("straight", 3, SaveFrameData=True, FrameDataFolder="straight")
+    (p2, _), _ = run("first", 2, SaveMemoryState=True, MemoryStateDataFolder="state")
+    assert (data / "state" / "frame.0002.bnn").exists()
+    (pr, vr), out = run("resume", 3, LoadMemoryState=True, MemoryStateDataFolder="state")
+    assert '"resumed_after_frame": 2' in out
+    assert np.array_equal(pr, p3) and np.array_equal(vr, v3)
+
+    cnt, attrs, _ = read_bnn(data / "straight" / "frame.0003.bnn")
+    assert cnt == len(p3)
+    dec, lo, hi, _ = values(attrs["particle_position"])
+    assert np.abs(dec - p3).max() <= (hi - lo).max() / 65535 * 1.01
+    assert attrs["particle_radius"]["type"] == "real"
+    assert list(values(attrs["object_index"])) == [0] * cnt
+    st_n, st, _ = read_bnn(data / "state" / "frame.0002.bnn")
+    assert np.array_equal(values(st["particle_position"]).reshape(-1, 3), p2)
+    assert list(values(st["grid_resolution"])) == [n + 4] * 3
