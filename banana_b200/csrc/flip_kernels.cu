@@ -220,12 +220,42 @@ __global__ void k_scatter_index(int n, const uint32_t* __restrict__ cellOf, cons
 // Grid::collectIndexToCells + getParticleIdxSortedByCell produce on one thread for
 // particles stored in id order (Grid.cpp:92-114,299-309), whatever order they are stored
 // in now.  The histogram is cleared for the next step on the way.
+// Buckets of up to N particles are sorted in registers: both loads of the bucket are
+// issued at once, then an odd-even transposition network (the ids are distinct, padding
+// sorts last) puts them in order; larger buckets use an insertion sort in memory.
+template<int N>
+__device__ __forceinline__ void sort_bucket_regs(uint32_t* __restrict__ order, const uint32_t* __restrict__ ids,
+                                                 uint32_t b, uint32_t cnt) {
+    uint32_t s[N], k[N];
+#pragma unroll
+    for(int q = 0; q < N; ++q) s[q] = (uint32_t)q < cnt ? order[b + q] : 0u;
+#pragma unroll
+    for(int q = 0; q < N; ++q) k[q] = (uint32_t)q < cnt ? __ldg(ids + s[q]) : 0xffffffffu;
+#pragma unroll
+    for(int round = 0; round < N; ++round) {
+#pragma unroll
+        for(int q = round & 1; q + 1 < N; q += 2) {
+            const bool sw = k[q] > k[q + 1];
+            const uint32_t k0 = sw ? k[q + 1] : k[q], k1 = sw ? k[q] : k[q + 1];
+            const uint32_t s0 = sw ? s[q + 1] : s[q], s1 = sw ? s[q] : s[q + 1];
+            k[q] = k0; k[q + 1] = k1; s[q] = s0; s[q + 1] = s1;
+        }
+    }
+#pragma unroll
+    for(int q = 0; q < N; ++q)
+        if((uint32_t)q < cnt) order[b + q] = s[q];
+}
+
 __global__ void k_sort_buckets(int ncells, const uint32_t* __restrict__ cellStart, uint32_t* __restrict__ order,
                                const uint32_t* __restrict__ ids, uint32_t* __restrict__ count) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if(c >= ncells) return;
     const uint32_t b = cellStart[c], e = cellStart[c + 1];
     count[c] = 0u;
+    const uint32_t cnt = e - b;
+    if(cnt < 2) return;
+    if(cnt <= 8) { sort_bucket_regs<8>(order, ids, b, cnt); return; }
+    if(cnt <= 16) { sort_bucket_regs<16>(order, ids, b, cnt); return; }
     for(uint32_t i = b + 1; i < e; ++i) {
         const uint32_t src = order[i];
         const uint32_t key = ids[src];
