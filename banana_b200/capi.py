@@ -48,7 +48,8 @@ class Params(C.Structure):
         ("cg_relative_tolerance", C.c_float), ("max_cg_iteration", C.c_uint32), ("advection_steps", C.c_uint32),
         ("solver_kind", C.c_int32), ("pcg_mode", C.c_int32), ("preconditioner", C.c_int32),
         ("refine_tolerance", C.c_float), ("refine_inner_tolerance", C.c_float), ("apply_gravity", C.c_int32),
-        ("max_particles", C.c_uint32),
+        ("max_particles", C.c_uint32), ("correct_position", C.c_int32), ("repulsive_force_stiffness", C.c_float),
+        ("ratio_cell_size_p_radius", C.c_float),
     ]
 
 
@@ -176,6 +177,9 @@ def make_params(cfg: dict) -> Params:
     p.refine_inner_tolerance = cfg.get("refine_inner_tolerance", 1e-3)
     p.apply_gravity = cfg.get("apply_gravity", 1)
     p.max_particles = cfg.get("max_particles", 0)
+    p.correct_position = cfg.get("correct_position", 0)
+    p.repulsive_force_stiffness = cfg.get("repulsive_force_stiffness", 50.0)
+    p.ratio_cell_size_p_radius = cfg.get("ratio_cell_size_p_radius", 2.0)
     return p
 
 

@@ -37,6 +37,11 @@ void launch_p2g(const GridDesc& g, const uint32_t* cellStart, const float* g3, c
                 const DevState* st, cudaStream_t s);
 void launch_advect_grid(const GridDesc& g, float** U, float** B, float dt, cudaStream_t s);
 void launch_maxabs(const float* a, size_t n, unsigned* maxBits, cudaStream_t s);
+void launch_correct_positions(int n, const GridDesc& g, const float* p6, size_t stride, const uint32_t* ids,
+                              const uint32_t* cellStart, float radius2, float threshold2, float jitterScale,
+                              float kSpring, int advSteps, unsigned long long step, float* out3, cudaStream_t s);
+void launch_rebin(int n, const float* p6, size_t stride, const GridDesc& g, uint32_t* cellOf, uint32_t* slot,
+                  uint32_t* count, DevState* st, cudaStream_t s);
 void launch_extrapolate(const GridDesc& g, float* const* A, uint8_t* const* VA, float* const* B, uint8_t* const* VB,
                         int lastMode, float* const* oldOut, float gravityDt, DevState* st, cudaStream_t s);
 void launch_fluid_sdf(const GridDesc& g, const uint32_t* cellStart, const float4* rec, size_t stride, float* phi,
@@ -106,6 +111,7 @@ struct bnn_flip {
     DevState* hst = nullptr;
     cudaEvent_t ev[11] = {};
     unsigned maxvelBits = 0; // max|u| of the current grid (for the next CFL)
+    unsigned long long substepIndex = 0;  // sub-steps taken (keys the position-correction jitter)
 };
 
 static void free_particles(bnn_flip* h) {
@@ -447,6 +453,26 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st) {
                        h->ids[h->cur], h->ids[nxt], affine ? h->C9[h->cur] : nullptr, affine ? h->C9[nxt] : nullptr,
                        h->g3, h->rec, g, h->cap, s);
     h->cur = nxt;
+    if(h->P.correct_position && n > 0) {
+        // PIC_Solver::advanceFrame: correctParticlePositions right after moveParticles
+        // (PIC_Solver.cpp:292-293), on the sorted particles; then they are binned again
+        const float pr = h->P.cell_size / h->P.ratio_cell_size_p_radius;
+        const float radius = 2.0f * pr / (float)std::sqrt(3.0);
+        const float threshold = 0.01f * radius;
+        const float kSpring = radius * sub * h->P.repulsive_force_stiffness;
+        launch_correct_positions(n, g, h->p6[h->cur], h->cap, h->ids[h->cur], h->cellStart, radius * radius,
+                                 threshold * threshold, threshold / substep, kSpring, (int)h->P.advection_steps,
+                                 h->substepIndex, h->aosStage, s);
+        BNN_CUDA_CHECK(cudaMemcpyAsync(h->p6[h->cur], h->aosStage, 3 * (size_t)h->cap * sizeof(float),
+                                       cudaMemcpyDeviceToDevice, s));
+        launch_rebin(n, h->p6[h->cur], h->cap, g, h->cellOf, h->slot, h->count, h->dst, s);
+        BNN_CUDA_CHECK(exclusive_scan_u32(h->count, h->cellStart, h->C, h->scanWs, s));
+        const int nxt2 = 1 - h->cur;
+        launch_sort_finish(n, h->C, h->cellOf, h->slot, h->cellStart, h->order, h->count, h->p6[h->cur], h->p6[nxt2],
+                           h->ids[h->cur], h->ids[nxt2], affine ? h->C9[h->cur] : nullptr,
+                           affine ? h->C9[nxt2] : nullptr, h->g3, h->rec, g, h->cap, s);
+        h->cur = nxt2;
+    }
     cudaEventRecord(h->ev[2], s);
     // P2G
     if(kind == BNN_SOLVER_PIC) {
@@ -507,6 +533,7 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st) {
     BNN_CUDA_CHECK(cudaStreamSynchronize(s));
     h->maxvelBits = h->hst->maxvel_bits;
     h->frameTime += substep;
+    ++h->substepIndex;
     if(st) {
         st->dt = substep;
         st->frame_time = h->frameTime;

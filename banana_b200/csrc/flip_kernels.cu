@@ -193,6 +193,107 @@ __global__ void __launch_bounds__(256) k_advect(int n, float* __restrict__ px, f
     bbox_block_reduce(st, mn, mx);
 }
 
+// ----------------------------------------------------------------------------------
+// Position correction
+// ----------------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t smix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+// PIC_Solver::correctParticlePositions (PIC_Solver.cpp:377-485), 3D, on the cell-sorted
+// particles: springs to the other particles of the 3x3x3 cells (cells z, y, x major, a
+// cell's particles in id order), MathHelpers::smooth_kernel with the cube rounded from
+// the double product, a counter-based jitter (SplitMix64 over sub-step and the two
+// particle ids, 21 bits per component) where two particles nearly coincide, then
+// AdvectionSteps moves with the box projection.  Reads the old positions, writes `o`.
+__global__ void __launch_bounds__(256) k_correct_positions(int n, GridDesc g, const float* __restrict__ px,
+                                                           const float* __restrict__ py, const float* __restrict__ pz,
+                                                           const uint32_t* __restrict__ ids,
+                                                           const uint32_t* __restrict__ cellStart, float radius2,
+                                                           float threshold2, float jitterScale, float kSpring,
+                                                           int advSteps, unsigned long long step,
+                                                           float* __restrict__ ox, float* __restrict__ oy,
+                                                           float* __restrict__ oz) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if(p >= n) return;
+    const float x0 = px[p], y0 = py[p], z0 = pz[p];
+    const int c[3] = {(int)((x0 - g.bmin[0]) / g.dx), (int)((y0 - g.bmin[1]) / g.dx), (int)((z0 - g.bmin[2]) / g.dx)};
+    float sp[3] = {0.f, 0.f, 0.f};
+    const uint32_t myId = ids[p];
+    for(int dk = -1; dk <= 1; ++dk) {
+        const int ck = c[2] + dk;
+        if(ck < 0 || ck >= g.G[2]) continue;
+        for(int dj = -1; dj <= 1; ++dj) {
+            const int cj = c[1] + dj;
+            if(cj < 0 || cj >= g.G[1]) continue;
+            const int xlo = max(c[0] - 1, 0), xhi = min(c[0] + 1, g.G[0] - 1);
+            if(xlo > xhi) continue;
+            const size_t base = ((size_t)ck * g.G[1] + cj) * g.G[0];
+            const uint32_t b = cellStart[base + xlo], e = cellStart[base + xhi + 1];
+            for(uint32_t q = b; q < e; ++q) {
+                if(q == (uint32_t)p) continue;
+                const float dx = x0 - px[q], dy = y0 - py[q], dz = z0 - pz[q];
+                const float d2 = length2f(dx, dy, dz);
+                const float x2 = d2 / radius2;
+                float w = 0.f;
+                if(!(x2 > 1.0f)) {
+                    const float t = 1.0f - x2;
+                    w = (float)(((double)t * (double)t) * (double)t);
+                }
+                if(d2 > threshold2) {
+                    const float s = sqrtf(d2);
+                    sp[0] += w * dx / s;
+                    sp[1] += w * dy / s;
+                    sp[2] += w * dz / s;
+                } else {
+                    const uint64_t h = smix64(smix64(smix64((uint64_t)step) ^ (uint64_t)myId) ^ (uint64_t)ids[q]);
+#pragma unroll
+                    for(int a = 0; a < 3; ++a) {
+                        const float u = (float)((h >> (21 * a)) & 0x1FFFFFull) * (1.0f / 2097152.0f);
+                        sp[a] += jitterScale * (2.0f * u - 1.0f);
+                    }
+                }
+            }
+        }
+    }
+    float x = x0, y = y0, z = z0;
+    for(int s = 0; s < advSteps; ++s) {
+        x += sp[0] * kSpring;
+        y += sp[1] * kSpring;
+        z += sp[2] * kSpring;
+        constrain_to_box(g, x, y, z);
+    }
+    ox[p] = x; oy[p] = y; oz[p] = z;
+}
+
+// Cell id, histogram slot and the occupied-cell box of particles that were moved since the
+// last sort (after position correction); grid-stride like k_advect
+__global__ void __launch_bounds__(256) k_rebin(int n, const float* __restrict__ px, const float* __restrict__ py,
+                                               const float* __restrict__ pz, GridDesc g,
+                                               uint32_t* __restrict__ cellOf, uint32_t* __restrict__ slot,
+                                               uint32_t* __restrict__ count, DevState* st) {
+    int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {INT_MIN, INT_MIN, INT_MIN};
+    for(int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        bool outside;
+        int cc[3];
+        const uint32_t c = cell_linear(g, (px[p] - g.bmin[0]) / g.dx, (py[p] - g.bmin[1]) / g.dx,
+                                       (pz[p] - g.bmin[2]) / g.dx, outside, cc);
+        if(outside) atomicOr(&st->flags, BNN_FLAG_OUT_OF_GRID);
+        cellOf[p] = c;
+        slot[p] = atomicAdd(count + c, 1u);
+#pragma unroll
+        for(int d = 0; d < 3; ++d) { mn[d] = min(mn[d], cc[d]); mx[d] = max(mx[d], cc[d]); }
+    }
+    bbox_block_reduce(st, mn, mx);
+}
+
+__global__ void k_bbox_reset(DevState* st) {
+    for(int d = 0; d < 3; ++d) { st->bbox[d] = INT_MAX; st->bbox[3 + d] = INT_MIN; }
+}
+
 // Cell id + histogram without moving (first sort of freshly loaded particles)
 __global__ void k_cell_histogram(int n, const float* __restrict__ px, const float* __restrict__ py,
                                  const float* __restrict__ pz, GridDesc g, uint32_t* __restrict__ cellOf,
@@ -948,6 +1049,22 @@ void launch_advect_grid(const GridDesc& g, float** U, float** B, float dt, cudaS
 }
 
 static constexpr unsigned kRegionBlocks = 148u * 8u;
+
+void launch_correct_positions(int n, const GridDesc& g, const float* p6, size_t stride, const uint32_t* ids,
+                              const uint32_t* cellStart, float radius2, float threshold2, float jitterScale,
+                              float kSpring, int advSteps, unsigned long long step, float* out3, cudaStream_t s) {
+    if(n == 0) return;
+    { k_correct_positions<<<nblk(n), 256, 0, s>>>(n, g, p6, p6 + stride, p6 + 2 * stride, ids, cellStart, radius2,
+                                                 threshold2, jitterScale, kSpring, advSteps, step, out3,
+                                                 out3 + stride, out3 + 2 * stride); bnn_note_launch(); }
+}
+void launch_rebin(int n, const float* p6, size_t stride, const GridDesc& g, uint32_t* cellOf, uint32_t* slot,
+                  uint32_t* count, DevState* st, cudaStream_t s) {
+    { k_bbox_reset<<<1, 1, 0, s>>>(st); bnn_note_launch(); }
+    if(n == 0) return;
+    const unsigned blocks = nblk(n) < kRegionBlocks ? nblk(n) : kRegionBlocks;
+    { k_rebin<<<blocks, 256, 0, s>>>(n, p6, p6 + stride, p6 + 2 * stride, g, cellOf, slot, count, st); bnn_note_launch(); }
+}
 
 void launch_maxabs(const float* a, size_t n, unsigned* maxBits, cudaStream_t s) {
     if(n) { k_maxabs<<<kRegionBlocks, 256, 0, s>>>(a, n, maxBits); bnn_note_launch(); }

@@ -172,6 +172,7 @@ void FLIP_GPU_Solver::loadSceneFromString(const std::string& sceneJson, bool all
     read_value(s, "MaxNParticles", P.maxNParticles);
     read_value(s, "AdvectionSteps", P.advectionSteps);
     read_bool(s, "CorrectPosition", P.bCorrectPosition);
+    read_value(s, "RepulsiveForceStiffness", P.repulsiveForceStiffness);
     read_value(s, "CGRelativeTolerance", P.CGRelativeTolerance);
     read_value(s, "MaxCGIteration", P.maxCGIteration);
     read_value(s, "PIC_FLIP_ratio", P.PIC_FLIP_ratio);
@@ -185,9 +186,6 @@ void FLIP_GPU_Solver::loadSceneFromString(const std::string& sceneJson, bool all
         read_vec3(s["SimulationDomainBox"], "BoxMin", P.domainBMin);
         read_vec3(s["SimulationDomainBox"], "BoxMax", P.domainBMax);
     }
-    if(P.bCorrectPosition)
-        std::fprintf(stderr, "%s: CorrectPosition is not supported on the GPU path; running without it\n",
-                     getSolverName().c_str());
     // SimulationParameters::makeReady (ParticleSolverData.cpp:229-272)
     for(int d = 0; d < 3; ++d) {
         P.movingBMin[d] = P.domainBMin[d];
@@ -270,6 +268,9 @@ void FLIP_GPU_Solver::allocateSolverMemory() {
     p.refine_inner_tolerance = P.refineInnerTolerance;
     p.apply_gravity = m_GlobalParams.bApplyGravity ? 1 : 0;
     p.max_particles = P.maxNParticles;
+    p.correct_position = P.bCorrectPosition ? 1 : 0;
+    p.repulsive_force_stiffness = P.repulsiveForceStiffness;
+    p.ratio_cell_size_p_radius = P.ratioCellSizePRadius;
     if(m_Gpu) bnn_flip_destroy(m_Gpu);
     m_Gpu = nullptr;
     check(bnn_flip_create(&p, &m_Gpu), "bnn_flip_create");

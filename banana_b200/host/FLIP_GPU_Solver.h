@@ -69,6 +69,7 @@ struct SimulationParameters {
     float PIC_FLIP_ratio = 0.97f;
     unsigned advectionSteps = 1u;
     bool bCorrectPosition = false;
+    float repulsiveForceStiffness = 50.0f;
     bool bExitIfPressureProjectionFailed = false;
     unsigned maxNParticles = 0u;
     // GPU-only choices (no reference counterpart): precision of the pressure solve

@@ -87,6 +87,11 @@ typedef struct bnn_params {
     float    refine_inner_tolerance; /* BNN_PCG_REFINED: inner FP32 relative tolerance */
     int32_t  apply_gravity;          /* GlobalParameters ApplyGravity (default 1) */
     uint32_t max_particles;          /* particle capacity; 0 = size to the first set_particles */
+    int32_t  correct_position;       /* CorrectPosition (default 0): neighbour-spring pass after
+                                        moveParticles, PIC_Solver::correctParticlePositions */
+    float    repulsive_force_stiffness; /* RepulsiveForceStiffness (default 50) */
+    float    ratio_cell_size_p_radius;  /* RatioCellSizePRadius (default 2): particle radius =
+                                           cell_size / ratio */
 } bnn_params;
 
 /* What one call of bnn_flip_step did.  stage_ms are CUDA-event times of the stages:

@@ -207,6 +207,9 @@ struct orc_params {
     int32_t  nthreads;              // 1: deterministic serial; >1: OpenMP timed mode
     int32_t  solver_kind;           // 0 FLIP, 1 APIC, 2 AFLIP, 3 PIC
     int32_t  apply_gravity;         // GlobalParameters ApplyGravity
+    int32_t  correct_position;      // CorrectPosition
+    float    repulsive_force_stiffness; // RepulsiveForceStiffness
+    float    ratio_cell_size_p_radius;  // RatioCellSizePRadius
 };
 
 struct orc_step_stats {
@@ -498,6 +501,7 @@ public:
     Arr3<uint32_t> activeIdx;
     std::vector<R> rhs, pressure;
     uint32_t nActive = 0, zeroPhiCells = 0;
+    uint64_t substepIndex = 0;  // sub-steps taken (keys the position-correction jitter)
     // last solve
     PCGResult lastSolve;
 
@@ -624,6 +628,90 @@ public:
             }
             pos[p] = pp;
         }
+    }
+
+    // Counter-based jitter replacing NumberHelpers::fRand11::vrnd (a process-global MT
+    // stream, NumberHelpers.h:155-258): three values in [-1, 1) from SplitMix64 over
+    // (sub-step, particle id, neighbour id), 21 bits each.
+    static uint64_t smix(uint64_t x) {
+        x += 0x9E3779B97F4A7C15ull;
+        x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+        x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+        return x ^ (x >> 31);
+    }
+    static void jitter(uint64_t step, uint32_t a, uint32_t b, R out[3]) {
+        const uint64_t h = smix(smix(smix(step) ^ (uint64_t)a) ^ (uint64_t)b);
+        for(int c = 0; c < 3; ++c) {
+            const float u = (float)((h >> (21 * c)) & 0x1FFFFFull) * (1.0f / 2097152.0f);
+            out[c] = (R)(2.0f * u - 1.0f);
+        }
+    }
+    // MathHelpers::smooth_kernel (MathHelpers.h:661-664): (1 - r2/h2)^3 inside h.  The cube
+    // is the rounding of the double product, the same on every platform (pow's last bit is
+    // implementation-defined).
+    static R smoothKernel(R r2, R h2) {
+        const R x2 = r2 / h2;
+        if(x2 > R(1.0)) return R(0);
+        const R t = R(1.0) - x2;
+        return (R)(((double)t * (double)t) * (double)t);
+    }
+
+    // PIC_Solver::correctParticlePositions (PIC_Solver.cpp:377-485), 3D: each particle is
+    // pushed by springs to the other particles of its 3x3x3 cells (cells z, y, x major, the
+    // particles of a cell in id order), jittered where two nearly coincide, then moved and
+    // projected into the box AdvectionSteps times; all particles read the old positions.
+    // Needs the particles sorted by (cell, id).
+    void correctPositions(R timestep) {
+        const size_t n = pos.size(), C = (size_t)G[0] * G[1] * G[2];
+        std::vector<uint32_t> start(C + 1, 0);
+        for(size_t p = 0; p < n; ++p) start[cellLinear(pos[p]) + 1]++;
+        for(size_t c = 0; c < C; ++c) start[c + 1] += start[c];
+        const R particleRadius = R(P.cell_size) / R(P.ratio_cell_size_p_radius);
+        const R radius = R(2.0) * particleRadius / R(std::sqrt(3.0));
+        const R radius2 = radius * radius;
+        const R threshold = R(0.01) * radius;
+        const R threshold2 = threshold * threshold;
+        const R substep = timestep / R(P.advection_steps);
+        const R kSpring = radius * substep * R(P.repulsive_force_stiffness);
+        std::vector<V3<R>> out(n);
+#pragma omp parallel for schedule(static) if(nthreads() > 1)
+        for(long long p = 0; p < (long long)n; ++p) {
+            const V3<R> pp = pos[p];
+            int c[3];
+            cellOf(pp, c);
+            R spring[3] = {R(0), R(0), R(0)};
+            for(int dk = -1; dk <= 1; ++dk)
+                for(int dj = -1; dj <= 1; ++dj)
+                    for(int di = -1; di <= 1; ++di) {
+                        const int ci = c[0] + di, cj = c[1] + dj, ck = c[2] + dk;
+                        if(ci < 0 || cj < 0 || ck < 0 || ci >= G[0] || cj >= G[1] || ck >= G[2]) continue;
+                        const size_t cell = ((size_t)ck * G[1] + cj) * G[0] + ci;
+                        for(uint32_t q = start[cell]; q < start[cell + 1]; ++q) {
+                            if((long long)q == p) continue;
+                            const R x[3] = {pp.x - pos[q].x, pp.y - pos[q].y, pp.z - pos[q].z};
+                            const R d2 = length2(x[0], x[1], x[2]);
+                            const R w = smoothKernel(d2, radius2);
+                            if(d2 > threshold2) {
+                                const R s = std::sqrt(d2);
+                                for(int a = 0; a < 3; ++a) spring[a] += w * x[a] / s;
+                            } else {
+                                R j[3];
+                                jitter(substepIndex, pid[p], pid[q], j);
+                                const R f = threshold / timestep;
+                                for(int a = 0; a < 3; ++a) spring[a] += f * j[a];
+                            }
+                        }
+                    }
+            V3<R> np = pp;
+            for(uint32_t s = 0; s < P.advection_steps; ++s) {
+                np.x += spring[0] * kSpring;
+                np.y += spring[1] * kSpring;
+                np.z += spring[2] * kSpring;
+                constrain(np);
+            }
+            out[p] = np;
+        }
+        pos.swap(out);
     }
 
     // Grid::getCellIdx<Int> (Grid.h:156-162) clamped into the grid, linearised (Grid.h:108-111)
@@ -1025,7 +1113,12 @@ public:
         else if(frameTime + R(1.5) * substep >= frameDuration) substep = remaining * R(0.5);
         moveParticles(substep);
         double t1 = now();
-        if(P.sort_each_step) sortParticlesByCell();
+        if(P.correct_position) {
+            // PIC_Solver::advanceFrame: moveParticles, correctParticlePositions (PIC_Solver.cpp:292-293)
+            sortParticlesByCell();
+            correctPositions(substep);
+        }
+        if(P.sort_each_step || P.correct_position) sortParticlesByCell();
         double t2 = now();
         int kind = P.solver_kind;
         // PIC_Solver::advanceVelocity (PIC_Solver.cpp:332-338): advect the grid velocity,
@@ -1052,6 +1145,7 @@ public:
         if(kind != 3) mapG2P();
         double t9 = now();
         frameTime += substep;
+        ++substepIndex;
         if(st) {
             st->dt = (double)substep; st->frame_time = (double)frameTime;
             st->frame_finished = frameTime >= frameDuration ? 1 : 0;

@@ -40,6 +40,8 @@ class OrcParams(C.Structure):
         ("reduce_mode", C.c_int32), ("pcg_mode", C.c_int32), ("preconditioner", C.c_int32),
         ("refine_tolerance", C.c_float), ("refine_inner_tolerance", C.c_float), ("sort_each_step", C.c_int32),
         ("nthreads", C.c_int32), ("solver_kind", C.c_int32), ("apply_gravity", C.c_int32),
+        ("correct_position", C.c_int32), ("repulsive_force_stiffness", C.c_float),
+        ("ratio_cell_size_p_radius", C.c_float),
     ]
 
 
@@ -131,6 +133,9 @@ def make_params(cfg: dict) -> OrcParams:
     p.nthreads = cfg.get("nthreads", 1)
     p.solver_kind = cfg.get("solver_kind", 0)
     p.apply_gravity = cfg.get("apply_gravity", 1)
+    p.correct_position = cfg.get("correct_position", 0)
+    p.repulsive_force_stiffness = cfg.get("repulsive_force_stiffness", 50.0)
+    p.ratio_cell_size_p_radius = cfg.get("ratio_cell_size_p_radius", 2.0)
     return p
 
 

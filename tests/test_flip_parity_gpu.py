@@ -155,3 +155,21 @@ def test_dense_scene_bitexact(bnn, oracle_mod):
     o.set_particles(pos, vel)
     for s in range(4):
         _compare_step(g, o, s)
+
+
+def test_position_correction_bitexact(bnn, oracle_mod):
+    """CorrectPosition (PIC_Solver::correctParticlePositions): springs between close
+    particles after every move, with the counter-based jitter where particles coincide
+    (some particles are duplicated exactly), then a second binning; identical to the oracle."""
+    n = 20
+    cfg = scenes.dam_break_params(n, correct_position=1)
+    pos, vel = scenes.dam_break(n)
+    dup = np.arange(0, len(pos), 97)
+    pos = np.concatenate([pos, pos[dup]])
+    vel = np.concatenate([vel, vel[dup]])
+    g = bnn.FlipSolver(cfg)
+    g.set_particles(pos, vel)
+    o = oracle_mod.Oracle(cfg)
+    o.set_particles(pos, vel)
+    for s in range(6):
+        _compare_step(g, o, s)

@@ -260,3 +260,24 @@ def test_floor_layer_falls_freely_under_static_box_semantics(oracle_mod):
     assert np.abs(v[:, 1] + g_t).max() < 1e-5 * g_t
     assert np.abs(v[:, [0, 2]]).max() < 1e-5 * g_t
     assert p.min() >= 0.0 and p.max() <= 1.0
+
+
+def test_position_correction_pushes_close_particles_apart(oracle_mod):
+    """Two particles closer than the spring radius (2 r / sqrt(3), r = cell / 2) in a still,
+    gravity-free box are pushed apart symmetrically by correctParticlePositions; the rest of
+    the step does not move them (zero velocity, no gravity)."""
+    n = 16
+    cfg = scenes.dam_break_params(n, correct_position=1, apply_gravity=0)
+    dx = 1.0 / n
+    c = np.array([0.5, 0.5, 0.5])
+    d = 0.2 * dx
+    pos = np.array([c - [d / 2, 0, 0], c + [d / 2, 0, 0]], np.float32)
+    vel = np.zeros_like(pos)
+    o = oracle_mod.Oracle(cfg)
+    o.set_particles(pos, vel)
+    o.step()
+    p, _ = o.get_particles()
+    gap = p[1, 0] - p[0, 0]
+    assert gap > d * 1.01
+    assert abs((p[0, 0] + p[1, 0]) / 2 - c[0]) < 1e-6
+    assert np.abs(p[:, 1:] - pos[:, 1:]).max() < 1e-6
