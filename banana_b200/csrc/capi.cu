@@ -24,7 +24,7 @@ extern "C" const char* bnn_version(void) { return "banana_b200 0.1 (sm_100a)"; }
 namespace bnn {
 // flip_kernels.cu
 void launch_advect(int n, float* p6, size_t stride, const float* const* U, const GridDesc& g, float sub, int steps,
-                   uint32_t* cellOf, uint32_t* slot, uint32_t* count, DevState* st, cudaStream_t s);
+                   uint32_t* cellOf, uint32_t* slot, uint32_t* count, DevState* st, int* bboxPart, cudaStream_t s);
 void launch_cell_histogram(int n, const float* p6, size_t stride, const GridDesc& g, uint32_t* cellOf, uint32_t* slot,
                            uint32_t* count, DevState* st, cudaStream_t s);
 void launch_sort_finish(int n, size_t ncells, const uint32_t* cellOf, const uint32_t* slot, const uint32_t* cellStart,
@@ -86,6 +86,7 @@ struct bnn_flip {
     float* g3 = nullptr;    // grid coordinates (APIC / AFLIP P2G)
     float4* rec = nullptr;  // per-particle gather records: 3 P2G stencil planes + positions
     uint32_t *cellOf = nullptr, *slot = nullptr, *order = nullptr;
+    int* bboxPart = nullptr;  // per-block occupied-cell boxes of the advection
     uint32_t *count = nullptr, *cellStart = nullptr;
     void* scanWs = nullptr;
     float* aosStage = nullptr;
@@ -119,8 +120,8 @@ static void free_particles(bnn_flip* h) {
         cudaFree(h->p6[b]); cudaFree(h->ids[b]); cudaFree(h->C9[b]);
         h->p6[b] = nullptr; h->ids[b] = nullptr; h->C9[b] = nullptr;
     }
-    cudaFree(h->g3); cudaFree(h->rec); cudaFree(h->cellOf); cudaFree(h->slot); cudaFree(h->order); cudaFree(h->aosStage);
-    h->g3 = nullptr; h->rec = nullptr; h->cellOf = h->slot = h->order = nullptr; h->aosStage = nullptr;
+    cudaFree(h->g3); cudaFree(h->rec); cudaFree(h->bboxPart); cudaFree(h->cellOf); cudaFree(h->slot); cudaFree(h->order); cudaFree(h->aosStage);
+    h->g3 = nullptr; h->rec = nullptr; h->bboxPart = nullptr; h->cellOf = h->slot = h->order = nullptr; h->aosStage = nullptr;
     h->cap = 0;
 }
 
@@ -137,6 +138,7 @@ static int reserve_particles(bnn_flip* h, uint32_t n) {
     }
     BNN_CUDA_CHECK(cudaMalloc(&h->g3, 3 * st * sizeof(float)));
     BNN_CUDA_CHECK(cudaMalloc(&h->rec, 4 * st * sizeof(float4)));
+    BNN_CUDA_CHECK(cudaMalloc(&h->bboxPart, 6 * ((st + 255) / 256) * sizeof(int)));
     BNN_CUDA_CHECK(cudaMalloc(&h->cellOf, st * sizeof(uint32_t)));
     BNN_CUDA_CHECK(cudaMalloc(&h->slot, st * sizeof(uint32_t)));
     BNN_CUDA_CHECK(cudaMalloc(&h->order, st * sizeof(uint32_t)));
@@ -445,7 +447,7 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st) {
     launch_step_reset(h->dst, s);
     // moveParticles + counting sort (histogram while advecting)
     launch_advect(n, h->p6[h->cur], h->cap, h->U, g, sub, (int)h->P.advection_steps, h->cellOf, h->slot, h->count,
-                  h->dst, s);
+                  h->dst, h->bboxPart, s);
     cudaEventRecord(h->ev[1], s);
     BNN_CUDA_CHECK(exclusive_scan_u32(h->count, h->cellStart, h->C, h->scanWs, s));
     const int nxt = 1 - h->cur;

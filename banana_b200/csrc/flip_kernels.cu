@@ -152,6 +152,40 @@ __device__ __forceinline__ void bbox_block_reduce(DevState* st, int mn[3], int m
     }
 }
 
+// The block's box written to part[6 * blockIdx.x ...] (min x,y,z, max x,y,z), no atomics
+__device__ __forceinline__ void bbox_block_partial(int* __restrict__ part, int mn[3], int mx[3]) {
+    __shared__ int sm[2][3][32];
+#pragma unroll
+    for(int d = 0; d < 3; ++d)
+        for(int off = 16; off > 0; off >>= 1) {
+            mn[d] = min(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], off));
+            mx[d] = max(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], off));
+        }
+    const int w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    if((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for(int d = 0; d < 3; ++d) { sm[0][d][w] = mn[d]; sm[1][d][w] = mx[d]; }
+    }
+    __syncthreads();
+    if(threadIdx.x < 3) {
+        const int d = threadIdx.x;
+        int a = INT_MAX, b = INT_MIN;
+        for(int q = 0; q < nw; ++q) { a = min(a, sm[0][d][q]); b = max(b, sm[1][d][q]); }
+        part[6 * blockIdx.x + d] = a;
+        part[6 * blockIdx.x + 3 + d] = b;
+    }
+}
+
+// Folds the per-block boxes into DevState::bbox
+__global__ void __launch_bounds__(256) k_bbox_final(int nparts, const int* __restrict__ part, DevState* st) {
+    int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {INT_MIN, INT_MIN, INT_MIN};
+    for(int q = blockIdx.x * blockDim.x + threadIdx.x; q < nparts; q += gridDim.x * blockDim.x) {
+#pragma unroll
+        for(int d = 0; d < 3; ++d) { mn[d] = min(mn[d], part[6 * q + d]); mx[d] = max(mx[d], part[6 * q + 3 + d]); }
+    }
+    bbox_block_reduce(st, mn, mx);
+}
+
 // ----------------------------------------------------------------------------------
 // moveParticles + cell histogram
 // ----------------------------------------------------------------------------------
@@ -163,34 +197,36 @@ __global__ void __launch_bounds__(256) k_advect(int n, float* __restrict__ px, f
                                                 const float* __restrict__ v, const float* __restrict__ w, GridDesc g,
                                                 float sub, int steps, uint32_t* __restrict__ cellOf,
                                                 uint32_t* __restrict__ slot, uint32_t* __restrict__ count,
-                                                DevState* st) {
+                                                DevState* st, int* __restrict__ bboxPart) {
     int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {INT_MIN, INT_MIN, INT_MIN};
-    for(int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
-    float x = px[p], y = py[p], z = pz[p];
-    for(int s = 0; s < steps; ++s) {
-        float gv[3];
-        float gx = (x - g.bmin[0]) / g.dx, gy = (y - g.bmin[1]) / g.dx, gz = (z - g.bmin[2]) / g.dx;
-        vel_from_grid(g, u, v, w, gx, gy, gz, gv);
-        const float h = 0.5f * sub;
-        float mx = x + h * gv[0], my = y + h * gv[1], mz = z + h * gv[2];
-        gx = (mx - g.bmin[0]) / g.dx; gy = (my - g.bmin[1]) / g.dx; gz = (mz - g.bmin[2]) / g.dx;
-        vel_from_grid(g, u, v, w, gx, gy, gz, gv);
-        x = x + sub * gv[0];
-        y = y + sub * gv[1];
-        z = z + sub * gv[2];
-        constrain_to_box(g, x, y, z);
-    }
-    px[p] = x; py[p] = y; pz[p] = z;
-    bool outside;
-    int cc[3];
-    uint32_t c = cell_linear(g, (x - g.bmin[0]) / g.dx, (y - g.bmin[1]) / g.dx, (z - g.bmin[2]) / g.dx, outside, cc);
-    if(outside) atomicOr(&st->flags, BNN_FLAG_OUT_OF_GRID);
-    cellOf[p] = c;
-    slot[p] = atomicAdd(count + c, 1u);
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if(p < n) {
+        float x = px[p], y = py[p], z = pz[p];
+        for(int s = 0; s < steps; ++s) {
+            float gv[3];
+            float gx = (x - g.bmin[0]) / g.dx, gy = (y - g.bmin[1]) / g.dx, gz = (z - g.bmin[2]) / g.dx;
+            vel_from_grid(g, u, v, w, gx, gy, gz, gv);
+            const float h = 0.5f * sub;
+            float mxp = x + h * gv[0], myp = y + h * gv[1], mzp = z + h * gv[2];
+            gx = (mxp - g.bmin[0]) / g.dx; gy = (myp - g.bmin[1]) / g.dx; gz = (mzp - g.bmin[2]) / g.dx;
+            vel_from_grid(g, u, v, w, gx, gy, gz, gv);
+            x = x + sub * gv[0];
+            y = y + sub * gv[1];
+            z = z + sub * gv[2];
+            constrain_to_box(g, x, y, z);
+        }
+        px[p] = x; py[p] = y; pz[p] = z;
+        bool outside;
+        int cc[3];
+        const uint32_t c = cell_linear(g, (x - g.bmin[0]) / g.dx, (y - g.bmin[1]) / g.dx, (z - g.bmin[2]) / g.dx,
+                                       outside, cc);
+        if(outside) atomicOr(&st->flags, BNN_FLAG_OUT_OF_GRID);
+        cellOf[p] = c;
+        slot[p] = atomicAdd(count + c, 1u);
 #pragma unroll
-    for(int d = 0; d < 3; ++d) { mn[d] = min(mn[d], cc[d]); mx[d] = max(mx[d], cc[d]); }
+        for(int d = 0; d < 3; ++d) { mn[d] = cc[d]; mx[d] = cc[d]; }
     }
-    bbox_block_reduce(st, mn, mx);
+    bbox_block_partial(bboxPart, mn, mx);
 }
 
 // ----------------------------------------------------------------------------------
@@ -985,11 +1021,13 @@ __global__ void k_step_reset(DevState* st) {
 static inline unsigned nblk(size_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
 
 void launch_advect(int n, float* p6, size_t stride, const float* const* U, const GridDesc& g, float sub, int steps,
-                   uint32_t* cellOf, uint32_t* slot, uint32_t* count, DevState* st, cudaStream_t s) {
+                   uint32_t* cellOf, uint32_t* slot, uint32_t* count, DevState* st, int* bboxPart, cudaStream_t s) {
     if(n == 0) return;
-    const unsigned blocks = nblk(n) < 148u * 8u ? nblk(n) : 148u * 8u;
+    const unsigned blocks = nblk(n);
     { k_advect<<<blocks, 256, 0, s>>>(n, p6, p6 + stride, p6 + 2 * stride, U[0], U[1], U[2], g, sub, steps, cellOf, slot,
-                                     count, st); bnn_note_launch(); }
+                                     count, st, bboxPart); bnn_note_launch(); }
+    const unsigned fb = blocks < 148u * 4u * 256u ? (blocks + 255u) / 256u : 148u * 4u;
+    { k_bbox_final<<<fb, 256, 0, s>>>((int)blocks, bboxPart, st); bnn_note_launch(); }
 }
 void launch_cell_histogram(int n, const float* p6, size_t stride, const GridDesc& g, uint32_t* cellOf, uint32_t* slot,
                            uint32_t* count, DevState* st, cudaStream_t s) {
