@@ -31,6 +31,7 @@ EXPORTS = [
     "bnn_flip_device_bytes", "bnn_scene_bytes_estimate", "bnn_flip_set_grid",
     "bnn_batch_create", "bnn_batch_destroy", "bnn_batch_add_scene", "bnn_batch_remove_scene", "bnn_batch_step",
     "bnn_batch_scene_info", "bnn_batch_get_scene", "bnn_batch_memory",
+    "bnn_aniso_default_params", "bnn_anisotropic_kernels", "bnn_flip_anisotropic_kernels",
 ]
 
 
@@ -74,6 +75,16 @@ class BatchStats(C.Structure):
 class PcgStats(C.Structure):
     _fields_ = [("iterations", C.c_uint32), ("outer_iterations", C.c_uint32), ("residual", C.c_double),
                 ("success", C.c_uint32), ("ms", C.c_float)]
+
+
+class AnisoParams(C.Structure):
+    _fields_ = [("particle_radius", C.c_float), ("kernel_ratio", C.c_float), ("default_spray_size", C.c_float),
+                ("position_blending", C.c_float), ("axis_ratio", C.c_float), ("neighbor_threshold", C.c_uint32)]
+
+
+class AnisoStats(C.Structure):
+    _fields_ = [("grid_bmin", C.c_float * 3), ("grid_cell_size", C.c_float), ("grid_dims", C.c_int32 * 3),
+                ("sprays", C.c_uint32), ("ms", C.c_float)]
 
 
 STAGES = ["move", "sort", "p2g", "extrapolate", "fluid_sdf", "system", "pcg", "update", "g2p", "step"]
@@ -124,6 +135,9 @@ def load() -> C.CDLL:
     L.bnn_batch_scene_info.argtypes = [vp, C.c_uint32, u32p, u64p, C.POINTER(StepStats)]
     L.bnn_batch_get_scene.argtypes = [vp, C.c_uint32, fp, fp]
     L.bnn_batch_memory.argtypes = [vp, u64p, u64p]
+    L.bnn_aniso_default_params.argtypes = [C.c_float, C.POINTER(AnisoParams)]
+    L.bnn_anisotropic_kernels.argtypes = [vp, C.c_uint32, C.POINTER(AnisoParams), vp, vp, C.POINTER(AnisoStats), vp]
+    L.bnn_flip_anisotropic_kernels.argtypes = [vp, C.POINTER(AnisoParams), fp, fp, C.POINTER(AnisoStats)]
     L.bnn_launch_count.argtypes = []
     L.bnn_launch_count.restype = C.c_uint64
     L.bnn_version.restype = C.c_char_p
@@ -276,6 +290,43 @@ class FlipSolver:
         k = C.c_uint32()
         check(self.L.bnn_flip_advance_frame(self.h, C.byref(k)), "bnn_flip_advance_frame")
         return k.value
+
+    def anisotropic_kernels(self, params: dict | None = None):
+        """Kernel centres (n x 3) and matrices (n x 9, column-major) of the current
+        particles, in the order they were given, plus the pass statistics."""
+        cen = np.zeros((self.n, 3), np.float32)
+        mat = np.zeros((self.n, 9), np.float32)
+        st = AnisoStats()
+        prm = aniso_params(**params) if params else None
+        check(self.L.bnn_flip_anisotropic_kernels(self.h, C.byref(prm) if prm is not None else None,
+                                                  _p(cen, C.c_float), _p(mat, C.c_float), C.byref(st)),
+              "bnn_flip_anisotropic_kernels")
+        return cen, mat, aniso_stats_dict(st)
+
+
+def aniso_params(particle_radius: float = 0.0, **kw) -> AnisoParams:
+    """AnisotropicKernelGenerator parameters: the reference defaults, overridden by kw"""
+    p = AnisoParams()
+    check(load().bnn_aniso_default_params(float(particle_radius), C.byref(p)), "bnn_aniso_default_params")
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def aniso_stats_dict(st: AnisoStats) -> dict:
+    return {"grid_bmin": list(st.grid_bmin), "grid_cell_size": st.grid_cell_size, "grid_dims": list(st.grid_dims),
+            "sprays": st.sprays, "ms": st.ms}
+
+
+def anisotropic_kernels_dev(pos_ptr: int, n: int, params: AnisoParams, cen_ptr: int, mat_ptr: int,
+                            stream: int = 0) -> dict:
+    """bnn_anisotropic_kernels on device pointers (AoS float32 points in, centres n x 3 and
+    matrices n x 9 out)."""
+    st = AnisoStats()
+    check(load().bnn_anisotropic_kernels(C.c_void_p(pos_ptr), n, C.byref(params), C.c_void_p(cen_ptr),
+                                         C.c_void_p(mat_ptr), C.byref(st), C.c_void_p(stream)),
+          "bnn_anisotropic_kernels")
+    return aniso_stats_dict(st)
 
 
 def pcg_solve_7pt(diag, nbr, offdiag, rhs, tol, max_iter, mode="fp32", inner_tol=1e-3):

@@ -198,6 +198,17 @@ int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const floa
               bool gridRows, float dt, int mode, float tol, unsigned maxIter, float innerTol, float outerTol,
               float* pressure, double* x64out, DevState* dst, DevState* hst, cudaStream_t s, PcgOutcome& out);
 int pcg_reserve(PcgWork& w, int n, bool fp64);
+// Cell grid of the anisotropic-kernel pass (aniso.cu)
+struct AnisoGrid {
+    int G[3];
+    float dx;
+    float bmin[3];
+};
+bnn_aniso_params aniso_defaults(float particleRadius);
+int aniso_check_params(const bnn_aniso_params& p);
+void launch_aniso(int n, const float4* pos, const uint32_t* ids, const uint32_t* cellStart, const AnisoGrid& g,
+                  const bnn_aniso_params& prm, float* outC, float* outM, unsigned* counters, cudaStream_t s);
+
 void pcg_release(PcgWork& w);
 
 } // namespace bnn

@@ -90,6 +90,7 @@ struct bnn_flip {
     uint32_t *count = nullptr, *cellStart = nullptr;
     void* scanWs = nullptr;
     float* aosStage = nullptr;
+    float* aniso = nullptr;  // anisotropic-kernel output: centres 3 cap, matrices 9 cap, 2 counters
     // faces
     float* U[3] = {};
     float* B[3] = {};
@@ -121,7 +122,9 @@ static void free_particles(bnn_flip* h) {
         h->p6[b] = nullptr; h->ids[b] = nullptr; h->C9[b] = nullptr;
     }
     cudaFree(h->g3); cudaFree(h->rec); cudaFree(h->bboxPart); cudaFree(h->cellOf); cudaFree(h->slot); cudaFree(h->order); cudaFree(h->aosStage);
+    cudaFree(h->aniso);
     h->g3 = nullptr; h->rec = nullptr; h->bboxPart = nullptr; h->cellOf = h->slot = h->order = nullptr; h->aosStage = nullptr;
+    h->aniso = nullptr;
     h->cap = 0;
 }
 
@@ -577,6 +580,65 @@ extern "C" int bnn_flip_step_host(bnn_flip* h, float* pos, float* vel, bnn_step_
     int rc = run_substep(h, st);
     int rc2 = bnn_flip_get_particles(h, pos, vel);
     return rc != BNN_OK ? rc : rc2;
+}
+
+// AnisotropicKernelGenerator over the solver's particles (PIC_Solver::saveFrameData,
+// PIC_Solver.cpp:248-252, constructs it with the particle positions and
+// solverParams().particleRadius).  The particles are binned and sorted first, the same
+// sort every sub-step starts from, so the pass works on any state (also before the first
+// step); the order it leaves them in does not change any later result, because each
+// sub-step sorts by (cell, id) again.
+extern "C" int bnn_flip_anisotropic_kernels(bnn_flip* h, const bnn_aniso_params* params, float* centers,
+                                            float* matrices, bnn_aniso_stats* stats) {
+    if(!h || (h->n && (!centers || !matrices))) return BNN_ERR_INVALID_ARGUMENT;
+    bnn_aniso_params prm = params ? *params : aniso_defaults(0.0f);
+    if(!(prm.particle_radius > 0.0f)) prm.particle_radius = h->P.cell_size / h->P.ratio_cell_size_p_radius;
+    int rc = aniso_check_params(prm);
+    if(rc != BNN_OK) return rc;
+    if(stats) std::memset(stats, 0, sizeof(*stats));
+    const int n = (int)h->n;
+    const GridDesc& g = h->g;
+    if(stats) {
+        for(int d = 0; d < 3; ++d) { stats->grid_bmin[d] = g.bmin[d]; stats->grid_dims[d] = g.G[d]; }
+        stats->grid_cell_size = g.dx;
+    }
+    if(n == 0) return BNN_OK;
+    cudaStream_t s = h->s;
+    const bool affine = h->P.solver_kind == BNN_SOLVER_APIC || h->P.solver_kind == BNN_SOLVER_AFLIP;
+    launch_rebin(n, h->p6[h->cur], h->cap, g, h->cellOf, h->slot, h->count, h->dst, s);
+    BNN_CUDA_CHECK(exclusive_scan_u32(h->count, h->cellStart, h->C, h->scanWs, s));
+    const int nxt = 1 - h->cur;
+    launch_sort_finish(n, h->C, h->cellOf, h->slot, h->cellStart, h->order, h->count, h->p6[h->cur], h->p6[nxt],
+                       h->ids[h->cur], h->ids[nxt], affine ? h->C9[h->cur] : nullptr, affine ? h->C9[nxt] : nullptr,
+                       h->g3, h->rec, g, h->cap, s);
+    h->cur = nxt;
+    const size_t cap = h->cap;
+    if(!h->aniso) BNN_CUDA_CHECK(cudaMalloc(&h->aniso, (12 * cap + 4) * sizeof(float)));
+    float* dC = h->aniso;
+    float* dM = h->aniso + 3 * cap;
+    unsigned* cnt = (unsigned*)(h->aniso + 12 * cap);
+    BNN_CUDA_CHECK(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned), s));
+    AnisoGrid ag;
+    for(int d = 0; d < 3; ++d) { ag.G[d] = g.G[d]; ag.bmin[d] = g.bmin[d]; }
+    ag.dx = g.dx;
+    cudaEventRecord(h->ev[0], s);
+    launch_aniso(n, h->rec + 3 * cap, h->ids[h->cur], h->cellStart, ag, prm, dC, dM, cnt, s);
+    cudaEventRecord(h->ev[1], s);
+    BNN_CUDA_CHECK(cudaMemcpyAsync(centers, dC, 3 * (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, s));
+    BNN_CUDA_CHECK(cudaMemcpyAsync(matrices, dM, 9 * (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, s));
+    unsigned hc[2] = {0u, 0u};
+    BNN_CUDA_CHECK(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, s));
+    BNN_CUDA_CHECK(cudaStreamSynchronize(s));
+    BNN_CUDA_CHECK(cudaGetLastError());
+    if(stats) {
+        stats->sprays = hc[0];
+        cudaEventElapsedTime(&stats->ms, h->ev[0], h->ev[1]);
+    }
+    if(hc[1]) {
+        bnn_set_error("bnn_flip_anisotropic_kernels: a particle lies outside the grid");
+        return BNN_ERR_DEVICE_CHECK;
+    }
+    return BNN_OK;
 }
 
 extern "C" int bnn_flip_advance_frame(bnn_flip* h, uint32_t* substeps) {

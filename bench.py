@@ -23,6 +23,9 @@ Other workloads (`--workload`, one JSON line each, not the headline):
   pcg     standalone Jacobi PCG (bnn_pcg_solve_7pt) on the 102 x 153 x 102 box of fluid
           cells the 256^3 dam break starts with (1,591,812 rows), a fixed number of
           iterations (`--steps`); for profiling the solver alone.
+  aniso   anisotropic kernels (AnisotropicKernelGenerator, the "AniKernel" frame output)
+          of the 256^3 dam break after one sub-step: particles/s of the kernel pass, and
+          end to end through bnn_flip_anisotropic_kernels into host arrays.
 
 `--impl reference` times the reference's CPU algorithm (the oracle port of PIC_Solver /
 FLIP_Solver / PCGSolver, reference arithmetic order, OpenMP over all host cores) on the
@@ -530,6 +533,67 @@ def run_nsearch(args, ws, rank, local):
     return 0
 
 
+def run_aniso(args, ws, rank, local):
+    """Anisotropic kernels of the dam break's particles (reference defaults: kernel radius
+    8 particle radii = 4 cells, threshold 25 neighbours)."""
+    torch, dist = _torch_dist(ws, local)
+    from banana_b200 import capi, scenes
+
+    cfg = scenes.dam_break_params(N_GRID)
+    pos, vel = scenes.dam_break(N_GRID)
+    g = capi.FlipSolver(cfg)
+    g.set_particles(pos, vel)
+    g.step()
+    n = len(pos)
+    for _ in range(args.warmup):
+        g.anisotropic_kernels()
+    launches0 = capi.launch_count()
+    kernel_ms, wall = [], []
+    st = None
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        _, _, st = g.anisotropic_kernels()
+        wall.append((time.perf_counter() - t0) * 1e3)
+        kernel_ms.append(st["ms"])
+    launches = capi.launch_count() - launches0
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        threads = os.cpu_count() or 1
+        O.set_threads(threads)
+        small = 64
+        sp, _ = scenes.dam_break(small)
+        sc = scenes.dam_break_params(small)
+        o = capi.FlipSolver(sc)
+        o.set_particles(sp, np.zeros_like(sp))
+        _, _, sst = o.anisotropic_kernels()
+        o.close()
+        t0 = time.perf_counter()
+        O.aniso_kernels(sp, sst["grid_bmin"], np.float32(sst["grid_cell_size"]), sst["grid_dims"],
+                        np.float32(sc["cell_size"] / 2.0))
+        dt = time.perf_counter() - t0
+        cpu = {"value": len(sp) / dt, "unit": "particles/s", "cores": threads, "kind": "port",
+               "sample": f"the oracle over all {len(sp)} particles of the {small}^3 dam break"}
+    ms = statistics.median(kernel_ms)
+    if rank == 0:
+        line = {"metric": f"particles/s, anisotropic kernels of the {N_GRID}^3 dam break", "value": n / (ms * 1e-3),
+                "unit": "particles/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "replicas", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded dam break after one sub-step)",
+                "config": {"workload": f"aniso_dam_break_{N_GRID}", "particles": n, "kernel_ratio": 8,
+                           "particle_radius": "cell / 2", "neighbor_threshold": 25},
+                "sprays": st["sprays"],
+                "e2e": {"value": n / (statistics.median(wall) * 1e-3), "unit": "particles/s",
+                        "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 48 * n,
+                        "note": "bnn_flip_anisotropic_kernels: re-sort, kernel pass, centres and matrices to host"},
+                "cpu_baseline": cpu, "gpu_launches": int(launches)}
+        print(json.dumps(line), flush=True)
+    g.close()
+    if ws > 1:
+        dist.destroy_process_group()
+    return 0
+
+
 def _box_system(nx, ny, nz, seed=1):
     """7-point system on a full box of cells in cell order (the layout of a grid)."""
     n = nx * ny * nz
@@ -649,7 +713,7 @@ def main():
     ap.add_argument("--grid", type=int, default=N_GRID, help="fluid-domain resolution (profiling of smaller cases)")
     ap.add_argument("--ref-precond", choices=["jacobi", "ic0"], default="jacobi",
                     help="reference arm: Jacobi (the configs) or the reference's default symmetric MIC(0)")
-    ap.add_argument("--workload", choices=["flip", "batch", "serve", "nsearch", "pcg", "fp64err"], default="flip")
+    ap.add_argument("--workload", choices=["flip", "batch", "serve", "nsearch", "pcg", "fp64err", "aniso"], default="flip")
     ap.add_argument("--workers", type=int, default=0, help="batch/serve: host threads stepping scenes (0 = auto)")
     ap.add_argument("--requests", type=int, default=100, help="serve: number of requests")
     ap.add_argument("--req-steps", type=int, default=200, help="serve: sub-steps per request")
@@ -669,6 +733,8 @@ def main():
         return run_pcg(args, ws, rank, local)
     if args.workload == "fp64err":
         return run_fp64err(args, ws, rank, local)
+    if args.workload == "aniso":
+        return run_aniso(args, ws, rank, local)
     return run_ours(args, ws, rank, local)
 
 

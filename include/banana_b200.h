@@ -243,6 +243,44 @@ int bnn_pcg_solve_7pt(uint32_t n, const float* diag, const int32_t* nbr, float o
 
 /* Library version / last CUDA error text / number of kernels this library has launched
  * in this process (diagnostics; no counterpart in the reference). */
+/* ---- anisotropic kernels (surface reconstruction output) -------------------------- */
+
+/* AnisotropicKernelGenerator<3, float> (Simulation/SurfaceReconstruction/
+ * AniKernelGenerator.h:35-45,51; computeAniKernels AniKernelGenerator.cpp:53-101), as
+ * PIC_Solver::saveFrameData runs it for "AniKernel" output (PIC_Solver.cpp:248-252):
+ * per particle a smoothed centre and a 3x3 kernel matrix (column-major, glm::mat3 memory
+ * order).  Neighbours are the other particles within kernel_ratio x particle_radius;
+ * particles with fewer than neighbor_threshold of them get default_spray_size x identity. */
+typedef struct bnn_aniso_params {
+    float    particle_radius;     /* kernel radius = kernel_ratio x particle_radius */
+    float    kernel_ratio;        /* 8 */
+    float    default_spray_size;  /* 0.75 */
+    float    position_blending;   /* 0.5 */
+    float    axis_ratio;          /* 8 */
+    uint32_t neighbor_threshold;  /* 25 */
+} bnn_aniso_params;
+
+typedef struct bnn_aniso_stats {
+    float    grid_bmin[3];        /* the cell grid the particles were sorted on */
+    float    grid_cell_size;
+    int32_t  grid_dims[3];
+    uint32_t sprays;              /* particles below the neighbour threshold */
+    float    ms;                  /* device time of the kernel pass */
+} bnn_aniso_stats;
+
+/* The reference defaults for one particle radius */
+int bnn_aniso_default_params(float particle_radius, bnn_aniso_params* out);
+/* Over a device array of n points (AoS x,y,z); outputs are device arrays in input order:
+ * centers n x 3, matrices n x 9.  The points are sorted on a cell grid of a quarter
+ * kernel radius spanning their bounding box (reported in stats). */
+int bnn_anisotropic_kernels(const float* pos_dev, uint32_t n, const bnn_aniso_params* params, float* centers_dev,
+                            float* matrices_dev, bnn_aniso_stats* stats, void* stream);
+/* Over the solver's current particles on its own grid; params NULL (or particle_radius
+ * <= 0) takes the solver's particle radius (CellSize / RatioCellSizePRadius).  Outputs are
+ * host arrays in the order the particles were given (as bnn_flip_get_particles). */
+int bnn_flip_anisotropic_kernels(bnn_flip* h, const bnn_aniso_params* params, float* centers, float* matrices,
+                                 bnn_aniso_stats* stats);
+
 const char* bnn_version(void);
 const char* bnn_last_error(void);
 uint64_t bnn_launch_count(void);

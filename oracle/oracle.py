@@ -15,6 +15,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 SRC = HERE / "flip_oracle.cpp"
+SRCS = [SRC, HERE / "aniso_oracle.cpp"]
 LIB = HERE / "liboracle.so"
 
 CXXFLAGS = ["-O3", "-march=x86-64-v3", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-shared",
@@ -23,8 +24,8 @@ CXXFLAGS = ["-O3", "-march=x86-64-v3", "-ffp-contract=off", "-fno-fast-math", "-
 
 def build(force: bool = False) -> Path:
     """Compile the restatement (no FMA contraction: one rounding per float operation)."""
-    if force or not LIB.exists() or LIB.stat().st_mtime < SRC.stat().st_mtime:
-        cmd = ["g++", *CXXFLAGS, "-o", str(LIB), str(SRC)]
+    if force or not LIB.exists() or any(LIB.stat().st_mtime < f.stat().st_mtime for f in SRCS):
+        cmd = ["g++", *CXXFLAGS, "-o", str(LIB), *[str(f) for f in SRCS]]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError("oracle build failed:\n" + res.stderr)
@@ -98,6 +99,11 @@ def lib() -> C.CDLL:
         L.orc_grid_ncells.argtypes = [fp, fp, C.c_float, i32p]; L.orc_grid_ncells.restype = None
         L.orc_interp_face.argtypes = [vp, C.c_int, C.c_double, C.c_double, C.c_double]
         L.orc_interp_face.restype = C.c_double
+        L.orc_aniso_kernels.argtypes = [fp, C.c_uint32, fp, C.c_float, i32p, C.c_float, C.c_float, C.c_float,
+                                        C.c_float, C.c_float, C.c_uint32, fp, fp]
+        L.orc_aniso_kernels.restype = C.c_uint32
+        L.orc_cbrt_newton.argtypes = [C.c_double]; L.orc_cbrt_newton.restype = C.c_double
+        L.orc_aniso_kernel_matrix.argtypes = [fp, C.c_float, fp]; L.orc_aniso_kernel_matrix.restype = None
         _lib = L
     return _lib
 
@@ -308,3 +314,30 @@ def grid_neighbor_list(pos, bmin, cell_size, ncells, q, d2=None):
                                      _p(qq, C.c_float), 0.0 if d2 is None else d2, 0 if d2 is None else 1,
                                      _p(out, C.c_uint32))
     return out[:n]
+
+
+def aniso_kernels(pos, bmin, cell_size, ncells, particle_radius, kernel_ratio=8.0, spray=0.75, blend=0.5,
+                  axis_ratio=8.0, threshold=25):
+    """AnisotropicKernelGenerator::computeAniKernels in the canonical order of the cell grid
+    (bmin, cell_size, ncells).  Returns (centers n x 3, matrices n x 9 column-major, sprays)."""
+    pos = np.ascontiguousarray(pos, np.float32)
+    n = len(pos)
+    cen = np.zeros((n, 3), np.float32)
+    mat = np.zeros((n, 9), np.float32)
+    sprays = lib().orc_aniso_kernels(_p(pos, C.c_float), n, _p(np.ascontiguousarray(bmin, np.float32), C.c_float),
+                                     float(cell_size), _p(np.ascontiguousarray(ncells, np.int32), C.c_int32),
+                                     float(particle_radius), float(kernel_ratio), float(spray), float(blend),
+                                     float(axis_ratio), int(threshold), _p(cen, C.c_float), _p(mat, C.c_float))
+    return cen, mat, int(sprays)
+
+
+def cbrt_newton(y: float) -> float:
+    return lib().orc_cbrt_newton(float(y))
+
+
+def aniso_kernel_matrix(cov, axis_ratio=8.0):
+    """Kernel matrix (column-major 9) of one covariance matrix (3 x 3)."""
+    c = np.ascontiguousarray(np.asarray(cov, np.float32).T.reshape(9))
+    out = np.zeros(9, np.float32)
+    lib().orc_aniso_kernel_matrix(_p(c, C.c_float), float(axis_ratio), _p(out, C.c_float))
+    return out

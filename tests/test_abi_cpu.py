@@ -40,7 +40,8 @@ def test_every_declared_symbol_is_exported(lib):
 def test_struct_layouts_match_binding(tmp_path):
     src = tmp_path / "layout.c"
     fields = {"bnn_params": capi.Params, "bnn_step_stats": capi.StepStats, "bnn_pcg_stats": capi.PcgStats,
-              "bnn_batch_params": capi.BatchParams, "bnn_batch_stats": capi.BatchStats}
+              "bnn_batch_params": capi.BatchParams, "bnn_batch_stats": capi.BatchStats,
+              "bnn_aniso_params": capi.AnisoParams, "bnn_aniso_stats": capi.AnisoStats}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "banana_b200.h"', "int main(void) {"]
     for cname, py in fields.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
@@ -71,6 +72,17 @@ def test_validation_needs_no_gpu(lib):
     assert lib.bnn_neighbors(None, 5, C.c_float(0.1), None, None, 0, None, None) == capi.STATUS_CODE["INVALID_ARGUMENT"]
     assert lib.bnn_cell_sort_noalloc(None, 1 << 21, None, C.c_float(1.0), None, None, None, None, None, None) \
         == capi.STATUS_CODE["INVALID_ARGUMENT"]
+    # anisotropic kernels: the reference defaults (AniKernelGenerator.h:41-45,51), and the
+    # argument checks that come before any CUDA call
+    ap = capi.aniso_params(0.5)
+    assert (ap.kernel_ratio, ap.default_spray_size, ap.position_blending, ap.axis_ratio, ap.neighbor_threshold) == \
+        (8.0, 0.75, 0.5, 8.0, 25)
+    assert lib.bnn_anisotropic_kernels(None, 4, C.byref(ap), None, None, None, None) == \
+        capi.STATUS_CODE["INVALID_ARGUMENT"]
+    bad = capi.aniso_params(0.0)
+    assert lib.bnn_anisotropic_kernels(None, 0, C.byref(bad), None, None, None, None) == \
+        capi.STATUS_CODE["INVALID_ARGUMENT"]
+    assert lib.bnn_flip_anisotropic_kernels(None, None, None, None, None) == capi.STATUS_CODE["INVALID_ARGUMENT"]
 
 
 def test_missing_library_fails_loudly(monkeypatch, tmp_path):
