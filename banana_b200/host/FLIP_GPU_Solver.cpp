@@ -334,7 +334,8 @@ void FLIP_GPU_Solver::waitForFrameOutput() {
 }
 
 // PIC_Solver::saveFrameData (PIC_Solver.cpp:236-263): particle_radius and compressed
-// positions, plus object indices / compressed velocities when the scene asks for them;
+// positions (the anisotropic kernel centres, with the kernel matrices, when "AniKernel"
+// is asked for), plus object indices / compressed velocities when the scene asks for them;
 // the file is written on a background thread while the next frame runs (the host arrays
 // are copied first, so the caller may keep using them).
 int FLIP_GPU_Solver::saveFrameData() {
@@ -350,7 +351,21 @@ int FLIP_GPU_Solver::saveFrameData() {
         std::vector<uint16_t> idx(D.objectIndex.begin(), D.objectIndex.end());
         file->setParticleUInt16("object_index", idx.data());
     }
-    file->setParticleCompressed("particle_position", D.positions.data(), 3);
+    if(G.savingData("AniKernel")) {
+        // AnisotropicKernelGenerator(positions, particleRadius) with its defaults; the
+        // kernel centres replace the positions in the file (PIC_Solver.cpp:248-252)
+        bnn_aniso_params ap;
+        check(bnn_aniso_default_params(radius, &ap), "bnn_aniso_default_params");
+        m_ParticleData.aniKernelCenters.resize(3 * (size_t)file->nParticles);
+        m_ParticleData.aniKernelMatrices.resize(9 * (size_t)file->nParticles);
+        check(bnn_flip_anisotropic_kernels(m_Gpu, &ap, m_ParticleData.aniKernelCenters.data(),
+                                           m_ParticleData.aniKernelMatrices.data(), nullptr),
+              "bnn_flip_anisotropic_kernels");
+        file->setParticleCompressed("particle_position", D.aniKernelCenters.data(), 3);
+        file->setParticleCompressedMatrix("anisotropic_kernel", D.aniKernelMatrices.data(), 3);
+    } else {
+        file->setParticleCompressed("particle_position", D.positions.data(), 3);
+    }
     if(G.savingData("ParticleVelocity")) file->setParticleCompressed("particle_velocity", D.velocities.data(), 3);
     const std::string path = bnn_file_path(G.dataPath, G.frameDataFolder, "frame", (int)G.finishedFrame);
     waitForFrameOutput();

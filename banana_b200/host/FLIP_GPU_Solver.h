@@ -42,7 +42,7 @@ struct GlobalParameters {
     std::string dataPath = ".";
     std::string frameDataFolder = "FrameData";
     std::string memoryStateDataFolder = "MemoryState";
-    std::vector<std::string> SaveDataList;  // "OptionalSavingData": "ObjectIndex", "ParticleVelocity"
+    std::vector<std::string> SaveDataList;  // "OptionalSavingData": "ObjectIndex", "AniKernel", "ParticleVelocity"
     bool savingData(const std::string& name) const {
         for(const auto& s : SaveDataList)
             if(s == name) return true;
@@ -84,6 +84,9 @@ struct ParticleData {
     std::vector<float> velocities;  // 3 floats per particle
     std::vector<int16_t> objectIndex;
     unsigned nObjects = 0;
+    // anisotropic kernels of the last saved frame (3 floats / 9 floats column-major each)
+    std::vector<float> aniKernelCenters;
+    std::vector<float> aniKernelMatrices;
     unsigned getNParticles() const { return (unsigned)(positions.size() / 3); }
 };
 

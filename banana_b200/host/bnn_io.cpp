@@ -64,9 +64,29 @@ void BnnFile::setParticleCompressed(const std::string& name, const float* v, uin
     for(size_t p = 0; p < nParticles; ++p)
         for(uint32_t c = 0; c < count; ++c) {
             const float diff = hi[c] - lo[c];
-            const float t = diff > 0.f ? (v[p * count + c] - lo[c]) / diff : 0.f;
-            q[p * count + c] = (uint16_t)(65535.0f * t);
+            q[p * count + c] = diff > 0.f ? (uint16_t)(65535.0f * ((v[p * count + c] - lo[c]) / diff)) : (uint16_t)0;
         }
+    put(a.data, q.data(), sizeof(uint16_t) * q.size());
+    particle[name] = std::move(a);
+}
+
+void BnnFile::setParticleCompressedMatrix(const std::string& name, const float* v, uint32_t dim) {
+    Attribute a;
+    a.type = "compressed_real";
+    a.elementBytes = 4;
+    a.count = dim * dim;
+    const size_t total = (size_t)nParticles * a.count;
+    float lo = std::numeric_limits<float>::max(), hi = -std::numeric_limits<float>::max();
+    for(size_t i = 0; i < total; ++i) {
+        lo = v[i] < lo ? v[i] : lo;
+        hi = v[i] > hi ? v[i] : hi;
+    }
+    if(total == 0) lo = hi = 0.f;
+    put(a.data, &lo, sizeof(float));
+    put(a.data, &hi, sizeof(float));
+    const float diff = hi - lo;
+    std::vector<uint16_t> q(total);
+    for(size_t i = 0; i < total; ++i) q[i] = diff > 0.f ? (uint16_t)(65535.0f * ((v[i] - lo) / diff)) : (uint16_t)0;
     put(a.data, q.data(), sizeof(uint16_t) * q.size());
     particle[name] = std::move(a);
 }
@@ -158,10 +178,28 @@ bool BnnFile::getFloats(const std::string& name, std::vector<float>& out) const 
         const uint16_t* q = (const uint16_t*)(a->data.data() + 8 * (size_t)c);
         const size_t n = (a->data.size() - 8 * (size_t)c) / 2;
         out.resize(n);
-        for(size_t i = 0; i < n; ++i) out[i] = lo[i % c] + (float)q[i] / 65535.0f * (hi[i % c] - lo[i % c]);
+        // ParticleHelpers::decompress (ParticleHelpers.cpp:183-199)
+        for(size_t i = 0; i < n; ++i) out[i] = (float)q[i] * (hi[i % c] - lo[i % c]) / 65535.0f + lo[i % c];
         return true;
     }
     return false;
+}
+
+bool BnnFile::getMatrixFloats(const std::string& name, std::vector<float>& out) const {
+    const Attribute* a = find(*this, name);
+    if(!a) return false;
+    if(a->type == "real" && a->elementBytes == 4) return getFloats(name, out);
+    if(a->type != "compressed_real" || a->data.size() < 8) return false;
+    float lo, hi;
+    std::memcpy(&lo, a->data.data(), 4);
+    std::memcpy(&hi, a->data.data() + 4, 4);
+    const uint16_t* q = (const uint16_t*)(a->data.data() + 8);
+    const size_t n = (a->data.size() - 8) / 2;
+    out.resize(n);
+    // ParticleHelpers::decompress for matrices (ParticleHelpers.cpp:234-252)
+    const float diff = hi - lo;
+    for(size_t i = 0; i < n; ++i) out[i] = (float)q[i] * diff / 65535.0f + lo;
+    return true;
 }
 
 bool BnnFile::getUInts(const std::string& name, std::vector<uint32_t>& out) const {

@@ -13,7 +13,8 @@
 // Types used by the fluid solvers: "real" (raw float), "uint" (raw uint32), "uint16", and
 // "compressed_real": float min[count], float max[count], then one uint16 per component,
 // trunc(65535 * (v - min) / (max - min)) (ParticleHelpers.cpp:46-80; a component whose
-// max equals its min is stored as 0).
+// max equals its min is stored as 0).  A matrix attribute ("anisotropic_kernel", count 9)
+// is compressed with one min and one max over all its entries (ParticleHelpers.cpp:82-114).
 #pragma once
 
 #include <cstdint>
@@ -41,6 +42,7 @@ public:
     void setFixedUInt(const std::string& name, const uint32_t* v, uint32_t count);
     void setParticleReal(const std::string& name, const float* v, uint32_t count);       // nParticles x count
     void setParticleCompressed(const std::string& name, const float* v, uint32_t count); // nParticles x count
+    void setParticleCompressedMatrix(const std::string& name, const float* v, uint32_t dim);  // nParticles x dim^2
     void setParticleUInt16(const std::string& name, const uint16_t* v);
     bool write(const std::string& path) const;
 
@@ -48,6 +50,8 @@ public:
     bool read(const std::string& path);
     // Raw floats of a "real" attribute, or the decoded values of a "compressed_real" one
     bool getFloats(const std::string& name, std::vector<float>& out) const;
+    // Decoded values of a matrix attribute (compressed with one min / max for all entries)
+    bool getMatrixFloats(const std::string& name, std::vector<float>& out) const;
     bool getUInts(const std::string& name, std::vector<uint32_t>& out) const;
     bool getUInt16(const std::string& name, std::vector<uint16_t>& out) const;
 };

@@ -1,6 +1,7 @@
 """Reader of Banana particle data files (.bnn) for the tests: text header
 (FixedAttribute / ParticleAttribute lines, NParticles, EndHeader.) then the attribute
-blobs in header order; compressed_real = float min[c], float max[c], uint16 per value."""
+blobs in header order; compressed_real = float min[c], float max[c], uint16 per value
+(a matrix attribute: one float min and one float max for all its entries)."""
 import numpy as np
 
 
@@ -46,5 +47,14 @@ def values(attr):
         lo = np.frombuffer(b[:4 * c], np.float32)
         hi = np.frombuffer(b[4 * c:8 * c], np.float32)
         q = np.frombuffer(b[8 * c:], np.uint16).reshape(-1, c).astype(np.float32)
-        return lo + q / np.float32(65535.0) * (hi - lo), lo, hi, q
+        return q * (hi - lo) / np.float32(65535.0) + lo, lo, hi, q
     raise ValueError(t)
+
+
+def matrix_values(attr):
+    """decoded matrix attribute (compressed_real with one min / max for all entries)"""
+    c, b = attr["count"], attr["raw"]
+    assert attr["type"] == "compressed_real"
+    lo, hi = np.frombuffer(b[:8], np.float32)
+    q = np.frombuffer(b[8:], np.uint16).reshape(-1, c).astype(np.float32)
+    return q * (hi - lo) / np.float32(65535.0) + lo, lo, hi, q

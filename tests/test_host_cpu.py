@@ -7,7 +7,7 @@ import pytest
 
 from banana_b200 import build as bld
 from banana_b200 import scenes
-from tests.bnn_format import read_bnn, values
+from tests.bnn_format import matrix_values, read_bnn, values
 from tests.host_scene import dam_break_scene, read_particles
 
 
@@ -57,6 +57,9 @@ int main(int argc, char** argv) {
     f.setParticleReal("particle_velocity", pos.data(), 3);
     f.setParticleCompressed("particle_position", pos.data(), 3);
     f.setParticleUInt16("object_index", idx.data());
+    std::vector<float> mats(45);
+    for(int i = 0; i < 45; ++i) mats[i] = 0.1f * (float)((i * 7) % 13) - 0.3f;
+    f.setParticleCompressedMatrix("anisotropic_kernel", mats.data(), 3);
     if(!f.write(argv[1])) return 1;
     bnnhost::BnnFile g;
     if(!g.read(argv[1])) return 2;
@@ -66,6 +69,9 @@ int main(int argc, char** argv) {
     if(!g.getUInts("grid_resolution", u) || u.size() != 3 || u[2] != 9) return 4;
     if(!g.getFloats("particle_position", c) || c.size() != pos.size()) return 5;
     for(size_t i = 0; i < c.size(); ++i) if(c[i] < pos[i] - 1e-4f || c[i] > pos[i] + 1e-4f) return 6;
+    std::vector<float> m;
+    if(!g.getMatrixFloats("anisotropic_kernel", m) || m.size() != 45) return 7;
+    for(size_t i = 0; i < m.size(); ++i) if(m[i] < mats[i] - 2e-5f || m[i] > mats[i] + 2e-5f) return 8;
     return 0;
 }
 """
@@ -84,8 +90,8 @@ def test_bnn_file_format_round_trip(tmp_path):
     subprocess.run([str(exe), str(out)], check=True)
     n, attrs, order = read_bnn(out)
     assert n == 5
-    assert order == ["NObjects", "grid_resolution", "particle_radius", "object_index", "particle_position",
-                     "particle_velocity"]
+    assert order == ["NObjects", "grid_resolution", "particle_radius", "anisotropic_kernel", "object_index",
+                     "particle_position", "particle_velocity"]
     assert attrs["particle_radius"]["type"] == "real" and attrs["particle_radius"]["bytes"] == 4
     assert list(values(attrs["grid_resolution"])) == [7, 8, 9]
     pos = values(attrs["particle_velocity"]).reshape(5, 3)
@@ -96,3 +102,11 @@ def test_bnn_file_format_round_trip(tmp_path):
     assert np.array_equal(q.astype(np.uint16), expect)
     assert np.abs(dec - pos).max() <= (hi - lo).max() / 65535 + 1e-6
     assert list(values(attrs["object_index"])) == [0, 1, 1, 0, 1]
+    # matrices: one range for all entries (ParticleHelpers.cpp:82-114)
+    mats = ((np.arange(45) * 7) % 13).astype(np.float32) * np.float32(0.1) - np.float32(0.3)
+    K, klo, khi, kq = matrix_values(attrs["anisotropic_kernel"])
+    assert attrs["anisotropic_kernel"]["count"] == 9 and attrs["anisotropic_kernel"]["bytes"] == 8 + 2 * 45
+    assert klo == mats.min() and khi == mats.max()
+    assert np.array_equal(kq.reshape(-1).astype(np.uint16),
+                          np.trunc(np.float32(65535.0) * ((mats - klo) / (khi - klo))).astype(np.uint16))
+    assert np.abs(K.reshape(-1) - mats).max() <= (khi - klo) / 65535 * 1.01

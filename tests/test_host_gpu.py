@@ -8,7 +8,7 @@ import pytest
 
 from banana_b200 import build as bld
 from banana_b200 import scenes
-from tests.bnn_format import read_bnn, values
+from tests.bnn_format import matrix_values, read_bnn, values
 from tests.host_scene import dam_break_scene, read_particles
 
 pytestmark = pytest.mark.gpu
@@ -79,3 +79,33 @@ def test_memory_state_resume_and_bnn_frames(bnn, tmp_path):
     st_n, st, _ = read_bnn(data / "state" / "frame.0002.bnn")
     assert np.array_equal(values(st["particle_position"]).reshape(-1, 3), p2)
     assert list(values(st["grid_resolution"])) == [n + 4] * 3
+
+
+def test_anikernel_frame_output(bnn, tmp_path):
+    """OptionalSavingData "AniKernel" (PIC_Solver.cpp:248-252): the frame file's positions
+    are the anisotropic kernel centres and "anisotropic_kernel" holds the 3x3 matrices
+    (16-bit compressed with one range for all entries), as the solver API computes them."""
+    exe = bld.build_host()
+    n = 16
+    data = tmp_path / "data"
+    sc = tmp_path / "ani.json"
+    sc.write_text(dam_break_scene(n, frames=1, DataPath=str(data), SaveFrameData=True, FrameDataFolder="ani",
+                                  OptionalSavingData=["AniKernel"]))
+    r = subprocess.run([str(exe), str(sc)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    cnt, attrs, order = read_bnn(data / "ani" / "frame.0001.bnn")
+    assert order == ["particle_radius", "anisotropic_kernel", "particle_position"]
+    assert attrs["anisotropic_kernel"]["count"] == 9 and attrs["anisotropic_kernel"]["bytes"] == 8 + 18 * cnt
+
+    cfg = scenes.dam_break_params(n)
+    p0, v0 = scenes.dam_break(n)
+    s = bnn.FlipSolver(cfg)
+    s.set_particles(p0, v0)
+    s.advance_frame()
+    cen, mat, st = s.anisotropic_kernels()
+    assert cnt == len(cen)
+    dec, lo, hi, _ = values(attrs["particle_position"])
+    assert np.abs(dec - cen).max() <= (hi - lo).max() / 65535 * 1.01
+    K, klo, khi, _ = matrix_values(attrs["anisotropic_kernel"])
+    assert klo == mat.min() and khi == mat.max()
+    assert np.abs(K - mat).max() <= (khi - klo) / 65535 * 1.01
