@@ -60,6 +60,10 @@ void launch_aos_to_soa(int n, const float* pos, const float* vel, float* soa6, u
                        cudaStream_t s);
 void launch_soa_to_aos(int n, const float* soa6, const uint32_t* ids, float* pos, float* vel, size_t stride,
                        cudaStream_t s);
+void launch_aos3_to_soa(int n, const float* aos, float* soa3, uint32_t* ids, size_t stride, cudaStream_t s);
+void launch_soa3_to_aos(int n, const float* soa3, const uint32_t* ids, float* aos, size_t stride, cudaStream_t s);
+void launch_scatter_planes(int n, int planes, const float* src, const uint32_t* ids, float* dst, size_t stride,
+                           cudaStream_t s);
 void launch_cells_from_rows(size_t nc, const float* phi, const uint32_t* aidx, const float* pr, float* out, int active,
                             cudaStream_t s);
 void launch_add_scalar(float* a, size_t n, float v, cudaStream_t s);
@@ -112,6 +116,10 @@ struct bnn_flip {
     DevState* dst = nullptr;
     DevState* hst = nullptr;
     cudaEvent_t ev[11] = {};
+    // host transfers of bnn_flip_step_host that overlap the step: a copy stream and its
+    // events (stream idle, velocities on the device, positions final)
+    cudaStream_t s2 = nullptr;
+    cudaEvent_t io[3] = {};
     unsigned maxvelBits = 0; // max|u| of the current grid (for the next CFL)
     unsigned long long substepIndex = 0;  // sub-steps taken (keys the position-correction jitter)
 };
@@ -178,6 +186,8 @@ static void destroy_all(bnn_flip* h) {
     cudaFree(h->dst);
     if(h->hst) cudaFreeHost(h->hst);
     for(auto& e : h->ev) if(e) cudaEventDestroy(e);
+    for(auto& e : h->io) if(e) cudaEventDestroy(e);
+    if(h->s2) cudaStreamDestroy(h->s2);
     if(h->s) cudaStreamDestroy(h->s);
     delete h;
 }
@@ -243,6 +253,8 @@ extern "C" int bnn_flip_create(const bnn_params* params, bnn_flip** out) {
     ok(cudaMalloc(&h->dst, sizeof(DevState)));
     ok(cudaHostAlloc(&h->hst, sizeof(DevState), cudaHostAllocDefault));
     for(auto& ev : h->ev) ok(cudaEventCreate(&ev));
+    for(auto& ev : h->io) ok(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    ok(cudaStreamCreateWithFlags(&h->s2, cudaStreamNonBlocking));
     if(rc != BNN_OK) { destroy_all(h); return rc; }
     for(int d = 0; d < 3; ++d) {
         ok(cudaMemsetAsync(h->U[d], 0, h->F[d] * sizeof(float), h->s));
@@ -432,7 +444,16 @@ static float timestep_cfl(const bnn_flip* h) {
     return ts;
 }
 
-static int run_substep(bnn_flip* h, bnn_step_stats* st) {
+// Host arrays of bnn_flip_step_host whose transfers overlap the step: the main stream waits
+// for the velocity upload only where the sort first gathers velocities, and the positions
+// go back to the host on the copy stream as soon as they are final (after the sort), while
+// the rest of the step runs.
+struct HostIo {
+    bool velPending = false;  // velocities still being uploaded on s2 (event io[1])
+    float* posOut = nullptr;  // host array for the final positions (caller order)
+};
+
+static int run_substep(bnn_flip* h, bnn_step_stats* st, const HostIo* io = nullptr) {
     cudaStream_t s = h->s;
     const GridDesc& g = h->g;
     if(h->frameTime >= h->frameDuration) h->frameTime = 0.f;
@@ -453,6 +474,7 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st) {
                   h->dst, h->bboxPart, s);
     cudaEventRecord(h->ev[1], s);
     BNN_CUDA_CHECK(exclusive_scan_u32(h->count, h->cellStart, h->C, h->scanWs, s));
+    if(io && io->velPending) BNN_CUDA_CHECK(cudaStreamWaitEvent(s, h->io[1], 0));
     const int nxt = 1 - h->cur;
     launch_sort_finish(n, h->C, h->cellOf, h->slot, h->cellStart, h->order, h->count, h->p6[h->cur], h->p6[nxt],
                        h->ids[h->cur], h->ids[nxt], affine ? h->C9[h->cur] : nullptr, affine ? h->C9[nxt] : nullptr,
@@ -479,6 +501,15 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st) {
         h->cur = nxt2;
     }
     cudaEventRecord(h->ev[2], s);
+    if(io && io->posOut && n > 0) {
+        // positions are final from here on (the rest of the step reads them only): back
+        // to the caller's order and to the host on the copy stream
+        BNN_CUDA_CHECK(cudaEventRecord(h->io[2], s));
+        BNN_CUDA_CHECK(cudaStreamWaitEvent(h->s2, h->io[2], 0));
+        launch_soa3_to_aos(n, h->p6[h->cur], h->ids[h->cur], h->aosStage, h->cap, h->s2);
+        BNN_CUDA_CHECK(cudaMemcpyAsync(io->posOut, h->aosStage, 3 * (size_t)n * sizeof(float), cudaMemcpyDeviceToHost,
+                                       h->s2));
+    }
     // P2G
     if(kind == BNN_SOLVER_PIC) {
         // PIC_Solver::advanceVelocity (PIC_Solver.cpp:332-338): the grid velocity is advected
@@ -568,18 +599,56 @@ extern "C" int bnn_flip_step(bnn_flip* h, bnn_step_stats* st) {
     return run_substep(h, st);
 }
 
+// The caller's arrays are in caller order (the order bnn_flip_get_particles returns): the
+// ids restart at 0..n-1 and the device-only per-particle data (APIC / AFLIP affine
+// matrices) is brought into that order.  The sort is by (cell, id), so the step computes
+// the same result as the resident path.  Positions go up
+// first on the main stream (the move needs them); velocities go up on the copy stream
+// while the particles move and are binned; the final positions come back on the copy
+// stream while the grid work runs, and the velocities after the grid-to-particle
+// transfer.
 extern "C" int bnn_flip_step_host(bnn_flip* h, float* pos, float* vel, bnn_step_stats* st) {
     if(!h || (h->n && (!pos || !vel))) return BNN_ERR_INVALID_ARGUMENT;
     if(st) std::memset(st, 0, sizeof(*st));
-    if(h->n) {
-        // The caller's arrays are in caller order: the ids restart at 0..n-1.  The sort is
-        // by (cell, id), so the step computes the same result as the resident path.
-        int rc = upload_particles(h, pos, vel, h->n);
-        if(rc != BNN_OK) return rc;
+    const int n = (int)h->n;
+    const size_t cap = h->cap;
+    HostIo io;
+    if(n) {
+        cudaStream_t s = h->s, s2 = h->s2;
+        if(h->C9[h->cur]) {
+            // the affine matrices (APIC / AFLIP) stay on the device: bring them into the
+            // caller's order, the order the ids restart in
+            launch_scatter_planes(n, 9, h->C9[h->cur], h->ids[h->cur], h->C9[1 - h->cur], cap, s);
+            std::swap(h->C9[0], h->C9[1]);
+        }
+        BNN_CUDA_CHECK(cudaEventRecord(h->io[0], s));
+        BNN_CUDA_CHECK(cudaStreamWaitEvent(s2, h->io[0], 0));
+        BNN_CUDA_CHECK(cudaMemcpyAsync(h->aosStage, pos, 3 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice, s));
+        launch_aos3_to_soa(n, h->aosStage, h->p6[h->cur], h->ids[h->cur], cap, s);
+        BNN_CUDA_CHECK(cudaMemcpyAsync(h->aosStage + 3 * cap, vel, 3 * (size_t)n * sizeof(float),
+                                       cudaMemcpyHostToDevice, s2));
+        launch_aos3_to_soa(n, h->aosStage + 3 * cap, h->p6[h->cur] + 3 * cap, nullptr, cap, s2);
+        BNN_CUDA_CHECK(cudaEventRecord(h->io[1], s2));
+        io.velPending = true;
+        io.posOut = pos;
     }
-    int rc = run_substep(h, st);
-    int rc2 = bnn_flip_get_particles(h, pos, vel);
-    return rc != BNN_OK ? rc : rc2;
+    int rc = run_substep(h, st, &io);
+    if(n) {
+        cudaStream_t s = h->s;
+        if(rc == BNN_OK || rc == BNN_ERR_PCG_NOT_CONVERGED || rc == BNN_ERR_DEVICE_CHECK) {
+            launch_soa3_to_aos(n, h->p6[h->cur] + 3 * cap, h->ids[h->cur], h->aosStage + 3 * cap, cap, s);
+            cudaError_t e = cudaMemcpyAsync(vel, h->aosStage + 3 * cap, 3 * (size_t)n * sizeof(float),
+                                            cudaMemcpyDeviceToHost, s);
+            if(e != cudaSuccess && rc == BNN_OK) { bnn_set_error(cudaGetErrorString(e)); rc = BNN_ERR_CUDA; }
+        }
+        cudaError_t e1 = cudaStreamSynchronize(h->s2);
+        cudaError_t e2 = cudaStreamSynchronize(s);
+        if((e1 != cudaSuccess || e2 != cudaSuccess) && rc == BNN_OK) {
+            bnn_set_error(cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+            rc = BNN_ERR_CUDA;
+        }
+    }
+    return rc;
 }
 
 // AnisotropicKernelGenerator over the solver's particles (PIC_Solver::saveFrameData,

@@ -993,6 +993,35 @@ __global__ void k_soa_to_aos(int n, const float* __restrict__ soa6, const uint32
     }
 }
 
+// One AoS vec3 array to / from three SoA planes (ids: written as 0..n-1 on the way in,
+// the caller's order on the way out)
+__global__ void k_aos3_to_soa(int n, const float* __restrict__ aos, float* __restrict__ soa3,
+                              uint32_t* __restrict__ ids, size_t stride) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if(p >= n) return;
+#pragma unroll
+    for(int d = 0; d < 3; ++d) soa3[d * stride + p] = aos[3 * (size_t)p + d];
+    if(ids) ids[p] = (uint32_t)p;
+}
+
+// planes of per-particle values from the current (sorted) order to the caller's order
+__global__ void k_scatter_planes(int n, int planes, const float* __restrict__ src, const uint32_t* __restrict__ ids,
+                                 float* __restrict__ dst, size_t stride) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if(p >= n) return;
+    const uint32_t id = ids[p];
+    for(int k = 0; k < planes; ++k) dst[k * stride + id] = src[k * stride + p];
+}
+
+__global__ void k_soa3_to_aos(int n, const float* __restrict__ soa3, const uint32_t* __restrict__ ids,
+                              float* __restrict__ aos, size_t stride) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if(p >= n) return;
+    const uint32_t id = ids[p];
+#pragma unroll
+    for(int d = 0; d < 3; ++d) aos[3 * (size_t)id + d] = soa3[d * stride + p];
+}
+
 // pressure scattered onto cells for BNN_FIELD_PRESSURE / BNN_FIELD_ACTIVE
 __global__ void k_cells_from_rows(size_t nc, const float* __restrict__ phi, const uint32_t* __restrict__ aidx,
                                   const float* __restrict__ pr, float* __restrict__ out, int activeField) {
@@ -1178,6 +1207,19 @@ void launch_soa_to_aos(int n, const float* soa6, const uint32_t* ids, float* pos
                        cudaStream_t s) {
     if(n == 0) return;
     { k_soa_to_aos<<<nblk(n), 256, 0, s>>>(n, soa6, ids, pos, vel, stride); bnn_note_launch(); }
+}
+void launch_aos3_to_soa(int n, const float* aos, float* soa3, uint32_t* ids, size_t stride, cudaStream_t s) {
+    if(n == 0) return;
+    { k_aos3_to_soa<<<nblk(n), 256, 0, s>>>(n, aos, soa3, ids, stride); bnn_note_launch(); }
+}
+void launch_scatter_planes(int n, int planes, const float* src, const uint32_t* ids, float* dst, size_t stride,
+                           cudaStream_t s) {
+    if(n == 0) return;
+    { k_scatter_planes<<<nblk(n), 256, 0, s>>>(n, planes, src, ids, dst, stride); bnn_note_launch(); }
+}
+void launch_soa3_to_aos(int n, const float* soa3, const uint32_t* ids, float* aos, size_t stride, cudaStream_t s) {
+    if(n == 0) return;
+    { k_soa3_to_aos<<<nblk(n), 256, 0, s>>>(n, soa3, ids, aos, stride); bnn_note_launch(); }
 }
 void launch_add_scalar(float* a, size_t n, float v, cudaStream_t s) { { k_add_scalar<<<nblk(n), 256, 0, s>>>(a, n, v); bnn_note_launch(); } }
 void launch_step_reset(DevState* st, cudaStream_t s) { { k_step_reset<<<1, 1, 0, s>>>(st); bnn_note_launch(); } }

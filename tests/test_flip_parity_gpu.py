@@ -106,10 +106,12 @@ def test_config1_100_steps_positions(bnn, oracle_mod):
     assert np.array_equal(pg, po)
 
 
-def test_step_host_matches_resident(bnn):
-    """The end-to-end entry point (host arrays in, host arrays out each step) computes the
-    same step as the device-resident one: the sort key is (cell, particle id)."""
-    cfg = scenes.dam_break_params(24)
+@pytest.mark.parametrize("over", [{}, {"solver_kind": 1}, {"solver_kind": 3}, {"correct_position": 1}])
+def test_step_host_matches_resident(bnn, over):
+    """The end-to-end entry point (host arrays in, host arrays out each step, transfers
+    overlapping the step) computes the same step as the device-resident one: the sort key
+    is (cell, particle id)."""
+    cfg = scenes.dam_break_params(24, **over)
     pos, vel = scenes.dam_break(24)
     a = bnn.FlipSolver(cfg)
     a.set_particles(pos, vel)
