@@ -20,7 +20,9 @@ STATUS = {0: "OK", 1: "INVALID_ARGUMENT", 2: "OUT_OF_MEMORY", 3: "PCG_NOT_CONVER
 STATUS_CODE = {v: k for k, v in STATUS.items()}
 SOLVER_KIND = {"FLIP": 0, "APIC": 1, "AFLIP": 2, "PIC": 3}
 PCG_MODE = {"fp32": 0, "fp64": 1, "refined": 2}
-FIELD = {"u": 0, "v": 1, "w": 2, "phi": 3, "pressure": 4, "old_u": 5, "old_v": 6, "old_w": 7, "active": 8}
+FIELD = {"u": 0, "v": 1, "w": 2, "phi": 3, "pressure": 4, "old_u": 5, "old_v": 6, "old_w": 7, "active": 8,
+         "weight_u": 9, "weight_v": 10, "weight_w": 11, "boundary_sdf": 12}
+GEOMETRY = {"box": 0, "sphere": 1}
 
 # Exported symbols of the C ABI (every one is declared in include/banana_b200.h)
 EXPORTS = [
@@ -32,6 +34,7 @@ EXPORTS = [
     "bnn_batch_create", "bnn_batch_destroy", "bnn_batch_add_scene", "bnn_batch_remove_scene", "bnn_batch_step",
     "bnn_batch_scene_info", "bnn_batch_get_scene", "bnn_batch_memory",
     "bnn_aniso_default_params", "bnn_anisotropic_kernels", "bnn_flip_anisotropic_kernels",
+    "bnn_flip_set_boundaries",
 ]
 
 
@@ -75,6 +78,46 @@ class BatchStats(C.Structure):
 class PcgStats(C.Structure):
     _fields_ = [("iterations", C.c_uint32), ("outer_iterations", C.c_uint32), ("residual", C.c_double),
                 ("success", C.c_uint32), ("ms", C.c_float)]
+
+
+class BoundaryObject(C.Structure):
+    """bnn_boundary_object: a box / sphere the fluid stays inside, with its current
+    world-to-object map (rows of a 3x4 affine matrix) and uniform scale."""
+    _fields_ = [("geometry", C.c_int32), ("dynamic", C.c_int32), ("box_min", C.c_float * 3),
+                ("box_max", C.c_float * 3), ("inv_transform", C.c_float * 12), ("uniform_scale", C.c_float),
+                ("transformed", C.c_int32)]
+
+
+def boundary_object(geometry: str, box_min=(0, 0, 0), box_max=(0, 0, 0), translation=None, axis_angle=None,
+                    scale=None, dynamic: bool = False) -> BoundaryObject:
+    """A boundary object with GeometryObject's transformation translate * rotate * scale
+    (Animation.h:199-231); axis_angle = (ax, ay, az, angle in radians)."""
+    o = BoundaryObject()
+    o.geometry = GEOMETRY[geometry]
+    o.dynamic = 1 if dynamic else 0
+    for d in range(3):
+        o.box_min[d] = float(box_min[d])
+        o.box_max[d] = float(box_max[d])
+    transformed = translation is not None or axis_angle is not None or scale is not None
+    T = np.eye(4)
+    if translation is not None:
+        T[:3, 3] = np.asarray(translation, np.float64)
+    Rm = np.eye(4)
+    if axis_angle is not None and float(axis_angle[3]) != 0.0:
+        a = np.asarray(axis_angle[:3], np.float64)
+        a = a / np.linalg.norm(a)
+        c, sn = np.cos(float(axis_angle[3])), np.sin(float(axis_angle[3]))
+        K = np.array([[0, -a[2], a[1]], [a[2], 0, -a[0]], [-a[1], a[0], 0]])
+        Rm[:3, :3] = c * np.eye(3) + sn * K + (1 - c) * np.outer(a, a)
+    sc = 1.0 if scale is None else float(scale)
+    S = np.diag([sc, sc, sc, 1.0])
+    inv = np.linalg.inv(T @ Rm @ S)
+    M = inv[:3, :4].astype(np.float32).reshape(-1)
+    for q in range(12):
+        o.inv_transform[q] = float(M[q])
+    o.uniform_scale = sc
+    o.transformed = 1 if transformed else 0
+    return o
 
 
 class AnisoParams(C.Structure):
@@ -135,6 +178,7 @@ def load() -> C.CDLL:
     L.bnn_batch_scene_info.argtypes = [vp, C.c_uint32, u32p, u64p, C.POINTER(StepStats)]
     L.bnn_batch_get_scene.argtypes = [vp, C.c_uint32, fp, fp]
     L.bnn_batch_memory.argtypes = [vp, u64p, u64p]
+    L.bnn_flip_set_boundaries.argtypes = [vp, C.POINTER(BoundaryObject), C.c_uint32]
     L.bnn_aniso_default_params.argtypes = [C.c_float, C.POINTER(AnisoParams)]
     L.bnn_anisotropic_kernels.argtypes = [vp, C.c_uint32, C.POINTER(AnisoParams), vp, vp, C.POINTER(AnisoStats), vp]
     L.bnn_flip_anisotropic_kernels.argtypes = [vp, C.POINTER(AnisoParams), fp, fp, C.POINTER(AnisoStats)]
@@ -247,6 +291,10 @@ class FlipSolver:
             shape = self.face_shape(which)
         elif which in (5, 6, 7):
             shape = self.face_shape(which - 5)
+        elif which in (9, 10, 11):
+            shape = self.face_shape(which - 9)
+        elif which == 12:
+            shape = tuple(g + 1 for g in self.G)
         else:
             shape = self.G
         out = np.zeros(int(np.prod(shape)), np.float32)
@@ -290,6 +338,11 @@ class FlipSolver:
         k = C.c_uint32()
         check(self.L.bnn_flip_advance_frame(self.h, C.byref(k)), "bnn_flip_advance_frame")
         return k.value
+
+    def set_boundaries(self, objs) -> None:
+        """Boundary objects besides the domain box (bnn_flip_set_boundaries)"""
+        arr = (BoundaryObject * max(len(objs), 1))(*objs)
+        check(self.L.bnn_flip_set_boundaries(self.h, arr, len(objs)), "bnn_flip_set_boundaries")
 
     def anisotropic_kernels(self, params: dict | None = None):
         """Kernel centres (n x 3) and matrices (n x 9, column-major) of the current

@@ -121,6 +121,19 @@ __device__ __forceinline__ float fraction_inside(float l, float r) {
 }
 __device__ __forceinline__ float length2f(float x, float y, float z) { return (x * x + y * y) + z * z; }
 
+// A boundary object (BoundaryObject over GeometryObjects::BoxObject / SphereObject,
+// Simulation/SimulationObjects/BoundaryObject.h:41-60, GeometryObjects.cpp:221-268,379-384):
+// the signed distance with bNegativeInside = false, i.e. positive inside the object,
+// which bounds the fluid.
+struct BObj {
+    int geometry;      // 0 box, 1 sphere (unit sphere in object space)
+    int transformed;   // 0: invTransform is the identity and is skipped
+    float bmin[3], bmax[3];
+    float M[12];       // world -> object: rows of a 3x4 affine map
+    float scale;       // uniform scale (multiplies the object-space distance)
+};
+constexpr int kMaxBoundaryObjects = 16;
+
 // Grid description passed by value to kernels
 struct GridDesc {
     int G[3];          // cells per axis (after padding)
@@ -129,7 +142,54 @@ struct GridDesc {
     float boxMin[3];   // domain box (constraint) min
     float boxMax[3];   // domain box max
     float sdfRadius;   // PIC_Parameters::sdfRadius
+    // Boundary objects beyond the plain domain box (nObj = 0: the domain box alone, above).
+    // obj[0, nStatic) are the static objects, the domain box first, united into one CSG
+    // object; every later object is a dynamic one of its own.
+    const BObj* obj = nullptr;
+    int nObj = 0;
+    int nStatic = 0;
 };
+
+// GeometryObject::invTransform then BoxObject / SphereObject::signedDistance(p, false)
+__device__ __forceinline__ float bobj_sdf(const BObj& o, float x, float y, float z) {
+    float q[3] = {x, y, z};
+    if(o.transformed) {
+#pragma unroll
+        for(int r = 0; r < 3; ++r) q[r] = ((o.M[4 * r] * x + o.M[4 * r + 1] * y) + o.M[4 * r + 2] * z) + o.M[4 * r + 3];
+    }
+    if(o.geometry == 0) {
+        bool inside = true;
+#pragma unroll
+        for(int d = 0; d < 3; ++d)
+            if(q[d] < o.bmin[d] || q[d] > o.bmax[d]) inside = false;
+        float mind = 3.402823466e+38f;
+        if(inside) {
+#pragma unroll
+            for(int d = 0; d < 3; ++d) mind = smin(mind, smin(q[d] - o.bmin[d], o.bmax[d] - q[d]));
+            mind = -mind;
+        } else {
+            float c[3];
+#pragma unroll
+            for(int d = 0; d < 3; ++d) c[d] = smax(smin(q[d], o.bmax[d]), o.bmin[d]);
+            mind = sqrtf(length2f(q[0] - c[0], q[1] - c[1], q[2] - c[2]));
+        }
+        mind = -mind;
+        return o.scale * mind;
+    }
+    const float d = o.scale * (sqrtf(length2f(q[0], q[1], q[2])) - 1.0f);
+    return -d;
+}
+
+// Signed distance of boundary group grp: group 0 is the CSG union of the static objects
+// (CSGObject::signedDistance, GeometryObjects.cpp:861-896: min over the members in
+// order), group g > 0 the g-th dynamic object
+__device__ __forceinline__ float group_sdf(const GridDesc& g, int grp, float x, float y, float z) {
+    const int b = grp == 0 ? 0 : g.nStatic + grp - 1;
+    const int e = grp == 0 ? g.nStatic : b + 1;
+    float sd = bobj_sdf(g.obj[b], x, y, z);
+    for(int i = b + 1; i < e; ++i) sd = smin(sd, bobj_sdf(g.obj[i], x, y, z));
+    return sd;
+}
 
 __host__ __device__ __forceinline__ int face_sx(const GridDesc& g, int d) { return g.G[0] + (d == 0); }
 __host__ __device__ __forceinline__ int face_sy(const GridDesc& g, int d) { return g.G[1] + (d == 1); }
@@ -194,9 +254,12 @@ struct PcgOutcome {
 // gridRows: the x neighbours of every row are rows r-1 / r+1 (or none) and the y
 // neighbours lie within 65535 rows (rows of a grid in cell order, at most 65535 cells
 // along x); the solve then reads the packed 16-byte row records.
+// coef (optional, compact rows only): six planes of off-diagonal values in the order of
+// nbr (face weights != 1); without it every off-diagonal is -dt.
 int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const float* invd, const int32_t* nbr,
-              bool gridRows, float dt, int mode, float tol, unsigned maxIter, float innerTol, float outerTol,
-              float* pressure, double* x64out, DevState* dst, DevState* hst, cudaStream_t s, PcgOutcome& out);
+              const float* coef, bool gridRows, float dt, int mode, float tol, unsigned maxIter, float innerTol,
+              float outerTol, float* pressure, double* x64out, DevState* dst, DevState* hst, cudaStream_t s,
+              PcgOutcome& out);
 int pcg_reserve(PcgWork& w, int n, bool fp64);
 // Cell grid of the anisotropic-kernel pass (aniso.cu)
 struct AnisoGrid {

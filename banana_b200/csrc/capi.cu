@@ -49,11 +49,11 @@ void launch_fluid_sdf(const GridDesc& g, const uint32_t* cellStart, const float4
 void launch_active_flags(const GridDesc& g, const float* phi, uint32_t* flag, DevState* st, cudaStream_t s);
 void launch_active_rows(size_t nc, const uint32_t* flag, const uint32_t* idx, uint32_t* rowCell, cudaStream_t s);
 void launch_build_rows(const GridDesc& g, int nrows, const uint32_t* rowCell, const float* phi, const uint32_t* aidx,
-                       const float* const* U, float dt, float* rhs, float* diag, float* invdiag, int32_t* nbr,
-                       DevState* st, cudaStream_t s);
+                       const float* const* U, const float* const* W, float dt, float* rhs, float* diag, float* invdiag,
+                       int32_t* nbr, float* coef, DevState* st, cudaStream_t s);
 void launch_update_velocity(const GridDesc& g, const DevState* st, const float* phi, const uint32_t* aidx,
                             const float* pressure, float dt, float* const* velIn, float* const* velOut,
-                            uint8_t* const* validOut, cudaStream_t s);
+                            uint8_t* const* validOut, const float* const* W, cudaStream_t s);
 void launch_g2p(int n, const GridDesc& g, float* p6, size_t stride, const float* const* U, const float* const* O,
                 float ratio, int kind, float* C9, cudaStream_t s);
 void launch_aos_to_soa(int n, const float* pos, const float* vel, float* soa6, uint32_t* ids, size_t stride,
@@ -61,6 +61,10 @@ void launch_aos_to_soa(int n, const float* pos, const float* vel, float* soa6, u
 void launch_soa_to_aos(int n, const float* soa6, const uint32_t* ids, float* pos, float* vel, size_t stride,
                        cudaStream_t s);
 void launch_aos3_to_soa(int n, const float* aos, float* soa3, uint32_t* ids, size_t stride, cudaStream_t s);
+void launch_boundary_grid(const GridDesc& g, float* nodeSdf, float* const* W, cudaStream_t s);
+void launch_solid_extend(const GridDesc& g, const float* nodeSdf, float* phi, cudaStream_t s);
+void launch_constrain_velocity(const GridDesc& g, const DevState* st, float* const* U, uint8_t* const* V,
+                               float* const* W, const float* nodeSdf, float* const* T, cudaStream_t s);
 void launch_soa3_to_aos(int n, const float* soa3, const uint32_t* ids, float* aos, size_t stride, cudaStream_t s);
 void launch_scatter_planes(int n, int planes, const float* src, const uint32_t* ids, float* dst, size_t stride,
                            cudaStream_t s);
@@ -95,6 +99,13 @@ struct bnn_flip {
     void* scanWs = nullptr;
     float* aosStage = nullptr;
     float* aniso = nullptr;  // anisotropic-kernel output: centres 3 cap, matrices 9 cap, 2 counters
+    // boundary objects beyond the domain box (g.obj points at objDev)
+    BObj* objDev = nullptr;
+    bool gridBoundary = false;  // a dynamic object exists: node SDF, weights, constraint
+    float* nodeSdf = nullptr;   // (G+1)^3
+    float* W[3] = {};           // face weights
+    float* coef = nullptr;      // off-diagonal values of the rows (6 planes, coefCap rows)
+    int coefCap = 0;
     // faces
     float* U[3] = {};
     float* B[3] = {};
@@ -183,6 +194,8 @@ static void destroy_all(bnn_flip* h) {
     cudaFree(h->aidx); cudaFree(h->cellTmp);
     cudaFree(h->rowCell); cudaFree(h->rhs); cudaFree(h->diag); cudaFree(h->invd); cudaFree(h->pressure); cudaFree(h->nbr);
     pcg_release(h->pcg);
+    cudaFree(h->objDev); cudaFree(h->nodeSdf); cudaFree(h->coef);
+    for(int d = 0; d < 3; ++d) cudaFree(h->W[d]);
     cudaFree(h->dst);
     if(h->hst) cudaFreeHost(h->hst);
     for(auto& e : h->ev) if(e) cudaEventDestroy(e);
@@ -413,6 +426,26 @@ extern "C" int bnn_flip_get_grid(bnn_flip* h, int32_t field, float* out, size_t 
     if(field >= BNN_FIELD_U && field <= BNN_FIELD_W) { src = h->U[field]; need = h->F[field]; }
     else if(field >= BNN_FIELD_OLD_U && field <= BNN_FIELD_OLD_W) { src = h->O[field - 5]; need = h->F[field - 5]; }
     else if(field == BNN_FIELD_PHI) { src = h->phi; need = h->C; }
+    else if(field >= BNN_FIELD_WEIGHT_U && field <= BNN_FIELD_WEIGHT_W) {
+        // weights 1 while no dynamic boundary has been set
+        const int d = field - BNN_FIELD_WEIGHT_U;
+        need = h->F[d];
+        if(count < need) return BNN_ERR_INVALID_ARGUMENT;
+        if(!h->gridBoundary) {
+            for(size_t i = 0; i < need; ++i) out[i] = 1.0f;
+            return BNN_OK;
+        }
+        src = h->W[d];
+    } else if(field == BNN_FIELD_BOUNDARY_SDF) {
+        need = (size_t)(h->g.G[0] + 1) * (h->g.G[1] + 1) * (h->g.G[2] + 1);
+        if(count < need) return BNN_ERR_INVALID_ARGUMENT;
+        if(!h->gridBoundary) {
+            // never computed for static scenes (the reference's array stays at 0)
+            for(size_t i = 0; i < need; ++i) out[i] = 0.0f;
+            return BNN_OK;
+        }
+        src = h->nodeSdf;
+    }
     else if(field == BNN_FIELD_PRESSURE || field == BNN_FIELD_ACTIVE) {
         need = h->C;
         if(count < need) return BNN_ERR_INVALID_ARGUMENT;
@@ -428,6 +461,60 @@ extern "C" int bnn_flip_get_grid(bnn_flip* h, int32_t field, float* out, size_t 
     }
     if(count < need) return BNN_ERR_INVALID_ARGUMENT;
     BNN_CUDA_CHECK(cudaMemcpyAsync(out, src, need * sizeof(float), cudaMemcpyDeviceToHost, h->s));
+    BNN_CUDA_CHECK(cudaStreamSynchronize(h->s));
+    return BNN_OK;
+}
+
+// ParticleSolver::generateBoundaries (ParticleSolver.cpp:242-295) for the domain box plus
+// the given objects: the domain box (ParticleSolver.cpp:76-82, untransformed) and the
+// static objects form one CSG union, each dynamic object stays on its own.  With a
+// dynamic object the node SDF and face weights are recomputed now.
+extern "C" int bnn_flip_set_boundaries(bnn_flip* h, const bnn_boundary_object* objs, uint32_t n) {
+    if(!h || (n && !objs) || n >= (uint32_t)kMaxBoundaryObjects) return BNN_ERR_INVALID_ARGUMENT;
+    std::vector<BObj> list;
+    BObj box{};
+    box.geometry = 0;
+    box.transformed = 0;
+    box.scale = 1.0f;
+    for(int d = 0; d < 3; ++d) { box.bmin[d] = h->g.boxMin[d]; box.bmax[d] = h->g.boxMax[d]; }
+    list.push_back(box);
+    bool anyDynamic = false;
+    for(int pass = 0; pass < 2; ++pass)
+        for(uint32_t i = 0; i < n; ++i) {
+            const bnn_boundary_object& o = objs[i];
+            if(o.geometry != BNN_GEOMETRY_BOX && o.geometry != BNN_GEOMETRY_SPHERE) return BNN_ERR_NOT_SUPPORTED;
+            if((o.dynamic != 0) != (pass == 1)) continue;
+            BObj b{};
+            b.geometry = o.geometry;
+            b.transformed = o.transformed ? 1 : 0;
+            b.scale = o.uniform_scale;
+            for(int d = 0; d < 3; ++d) { b.bmin[d] = o.box_min[d]; b.bmax[d] = o.box_max[d]; }
+            for(int q = 0; q < 12; ++q) b.M[q] = o.inv_transform[q];
+            list.push_back(b);
+            anyDynamic |= pass == 1;
+        }
+    uint32_t nStatic = 1;
+    for(uint32_t i = 0; i < n; ++i) nStatic += objs[i].dynamic ? 0u : 1u;
+    if(!h->objDev) BNN_CUDA_CHECK(cudaMalloc(&h->objDev, kMaxBoundaryObjects * sizeof(BObj)));
+    BNN_CUDA_CHECK(cudaMemcpyAsync(h->objDev, list.data(), list.size() * sizeof(BObj), cudaMemcpyHostToDevice, h->s));
+    if(n == 0) {
+        h->g.obj = nullptr;
+        h->g.nObj = 0;
+        h->g.nStatic = 0;
+    } else {
+        h->g.obj = h->objDev;
+        h->g.nObj = (int)list.size();
+        h->g.nStatic = (int)nStatic;
+    }
+    h->gridBoundary = anyDynamic;
+    if(anyDynamic) {
+        const size_t nn = (size_t)(h->g.G[0] + 1) * (h->g.G[1] + 1) * (h->g.G[2] + 1);
+        if(!h->nodeSdf) BNN_CUDA_CHECK(cudaMalloc(&h->nodeSdf, nn * sizeof(float)));
+        for(int d = 0; d < 3; ++d)
+            if(!h->W[d]) BNN_CUDA_CHECK(cudaMalloc(&h->W[d], h->F[d] * sizeof(float)));
+        launch_boundary_grid(h->g, h->nodeSdf, h->W, h->s);
+    }
+    BNN_CUDA_CHECK(cudaGetLastError());
     BNN_CUDA_CHECK(cudaStreamSynchronize(h->s));
     return BNN_OK;
 }
@@ -526,11 +613,21 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st, const HostIo* io = nullp
         if(h->P.apply_gravity) launch_add_scalar(h->U[1], h->F[1], -gdt, s);
     } else {
         // extrapolate, backup oldVels, Earth gravity (FLIP_Solver.cpp:44-47)
-        launch_extrapolate(g, h->U, h->VA, h->B, h->VB, 1, h->O, gdt, h->dst, s);
+        if(h->gridBoundary) {
+            // ... with constrainGridVelocity between the extrapolation and the backup
+            launch_extrapolate(g, h->U, h->VA, h->B, h->VB, 0, nullptr, 0.f, h->dst, s);
+            launch_constrain_velocity(g, h->dst, h->U, h->VA, h->W, h->nodeSdf, h->B, s);
+            for(int d = 0; d < 3; ++d)
+                BNN_CUDA_CHECK(cudaMemcpyAsync(h->O[d], h->U[d], h->F[d] * sizeof(float), cudaMemcpyDeviceToDevice, s));
+            if(h->P.apply_gravity) launch_add_scalar(h->U[1], h->F[1], -gdt, s);
+        } else {
+            launch_extrapolate(g, h->U, h->VA, h->B, h->VB, 1, h->O, gdt, h->dst, s);
+        }
     }
     cudaEventRecord(h->ev[4], s);
     // pressure projection (PIC_Solver.cpp:533-539)
     launch_fluid_sdf(g, h->cellStart, h->rec, h->cap, h->phi, h->dst, s);
+    if(h->gridBoundary) launch_solid_extend(g, h->nodeSdf, h->phi, s);
     cudaEventRecord(h->ev[5], s);
     launch_active_flags(g, h->phi, h->flag, h->dst, s);
     BNN_CUDA_CHECK(exclusive_scan_u32(h->flag, h->aidx, h->C, h->scanWs, s));
@@ -542,21 +639,36 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st, const HostIo* io = nullp
     if(rc != BNN_OK) return rc;
     h->nRows = nrows;
     launch_active_rows(h->C, h->flag, h->aidx, h->rowCell, s);
-    launch_build_rows(g, (int)nrows, h->rowCell, h->phi, h->aidx, h->U, substep, h->rhs, h->diag, h->invd, h->nbr,
-                      h->dst, s);
+    if(h->gridBoundary && h->coefCap < h->rowCap) {
+        cudaFree(h->coef);
+        h->coef = nullptr;
+        h->coefCap = 0;
+        BNN_CUDA_CHECK(cudaMalloc(&h->coef, 6 * (size_t)h->rowCap * sizeof(float)));
+        h->coefCap = h->rowCap;
+    }
+    launch_build_rows(g, (int)nrows, h->rowCell, h->phi, h->aidx, h->U, h->gridBoundary ? h->W : nullptr, substep,
+                      h->rhs, h->diag, h->invd, h->nbr, h->gridBoundary ? h->coef : nullptr, h->dst, s);
     cudaEventRecord(h->ev[6], s);
     PcgOutcome po;
-    rc = pcg_solve(h->pcg, (int)nrows, h->rhs, h->diag, h->invd, h->nbr, true, substep, h->P.pcg_mode,
+    rc = pcg_solve(h->pcg, (int)nrows, h->rhs, h->diag, h->invd, h->nbr, h->gridBoundary ? h->coef : nullptr,
+                   true, substep, h->P.pcg_mode,
                    h->P.cg_relative_tolerance, h->P.max_cg_iteration, h->P.refine_inner_tolerance,
                    h->P.refine_tolerance, h->pressure, nullptr, h->dst, h->hst, s, po);
     if(rc != BNN_OK) return rc;
     cudaEventRecord(h->ev[7], s);
     // projected faces go to the ping-pong arrays, which then become the velocity arrays
-    launch_update_velocity(g, h->dst, h->phi, h->aidx, h->pressure, substep, h->U, h->B, h->VB, s);
-    launch_extrapolate(g, h->B, h->VB, h->U, h->VA, 2, nullptr, 0.f, h->dst, s);
+    launch_update_velocity(g, h->dst, h->phi, h->aidx, h->pressure, substep, h->U, h->B, h->VB,
+                           h->gridBoundary ? h->W : nullptr, s);
+    launch_extrapolate(g, h->B, h->VB, h->U, h->VA, h->gridBoundary ? 0 : 2, nullptr, 0.f, h->dst, s);
     for(int d = 0; d < 3; ++d) {
         std::swap(h->U[d], h->B[d]);
         std::swap(h->VA[d], h->VB[d]);
+    }
+    if(h->gridBoundary) {
+        // constrainGridVelocity after the extrapolation (FLIP_Solver.cpp:51), then the CFL
+        // maximum over the constrained faces
+        launch_constrain_velocity(g, h->dst, h->U, h->VA, h->W, h->nodeSdf, h->B, s);
+        for(int d = 0; d < 3; ++d) launch_maxabs(h->U[d], h->F[d], &h->dst->maxvel_bits, s);
     }
     cudaEventRecord(h->ev[8], s);
     // PIC_Solver leaves the particle velocities alone (no grid-to-particle transfer)
@@ -788,7 +900,7 @@ extern "C" int bnn_pcg_solve_7pt(uint32_t n, const float* diag, const int32_t* n
     if(rc == BNN_OK) rc = pcg_reserve(w, (int)n, mode != BNN_PCG_FP32);  // outside the timed region
     if(rc == BNN_OK) {
         cudaEventRecord(e0, s);
-        rc = pcg_solve(w, (int)n, dRhs, dDiag, dInv, dNbr, gridRows, dt, mode, tol, max_iter, inner_tol, tol, dP, dX,
+        rc = pcg_solve(w, (int)n, dRhs, dDiag, dInv, dNbr, nullptr, gridRows, dt, mode, tol, max_iter, inner_tol, tol, dP, dX,
                        dst, hst, s, po);
         cudaEventRecord(e1, s);
     }

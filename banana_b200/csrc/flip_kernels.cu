@@ -113,6 +113,38 @@ __device__ __forceinline__ void constrain_to_box(const GridDesc& g, float& x, fl
     }
 }
 
+// The same projection against every boundary group in turn (the static CSG union, then
+// each dynamic object: the reference's moveParticles loops over m_BoundaryObjects,
+// PIC_Solver.cpp:353-372); the domain box alone takes the path above.
+__device__ __forceinline__ void constrain_particle(const GridDesc& g, float& x, float& y, float& z) {
+    if(g.nObj == 0) {
+        constrain_to_box(g, x, y, z);
+        return;
+    }
+    const int ng = 1 + g.nObj - g.nStatic;
+    for(int grp = 0; grp < ng; ++grp) {
+        const float phiVal = group_sdf(g, grp, x, y, z);
+        if(phiVal < 0.f) {
+            const float e = 1e-4f;
+            float v000 = group_sdf(g, grp, x - e, y - e, z - e), v001 = group_sdf(g, grp, x - e, y - e, z + e);
+            float v010 = group_sdf(g, grp, x - e, y + e, z - e), v011 = group_sdf(g, grp, x - e, y + e, z + e);
+            float v100 = group_sdf(g, grp, x + e, y - e, z - e), v101 = group_sdf(g, grp, x + e, y - e, z + e);
+            float v110 = group_sdf(g, grp, x + e, y + e, z - e), v111 = group_sdf(g, grp, x + e, y + e, z + e);
+            float gx = ((((v100 - v000) + (v101 - v001)) + (v110 - v010)) + (v111 - v011)) * 0.25f;
+            float gy = ((((v010 - v000) + (v011 - v001)) + (v110 - v100)) + (v111 - v101)) * 0.25f;
+            float gz = ((((v001 - v000) + (v011 - v010)) + (v101 - v100)) + (v111 - v110)) * 0.25f;
+            float m2 = length2f(gx, gy, gz);
+            if(m2 > FLT_MIN) {
+                float s = sqrtf(m2);
+                gx = gx / s; gy = gy / s; gz = gz / s;
+                x = x - phiVal * gx;
+                y = y - phiVal * gy;
+                z = z - phiVal * gz;
+            }
+        }
+    }
+}
+
 __device__ __forceinline__ uint32_t cell_linear(const GridDesc& g, float gx, float gy, float gz, bool& outside,
                                                 int* cc = nullptr) {
     // Grid::getCellIdx<Int> (Grid.h:156-162): truncation of (p - bMin)/cellSize
@@ -213,7 +245,7 @@ __global__ void __launch_bounds__(256) k_advect(int n, float* __restrict__ px, f
             x = x + sub * gv[0];
             y = y + sub * gv[1];
             z = z + sub * gv[2];
-            constrain_to_box(g, x, y, z);
+            constrain_particle(g, x, y, z);
         }
         px[p] = x; py[p] = y; pz[p] = z;
         bool outside;
@@ -300,7 +332,7 @@ __global__ void __launch_bounds__(256) k_correct_positions(int n, GridDesc g, co
         x += sp[0] * kSpring;
         y += sp[1] * kSpring;
         z += sp[2] * kSpring;
-        constrain_to_box(g, x, y, z);
+        constrain_particle(g, x, y, z);
     }
     ox[p] = x; oy[p] = y; oz[p] = z;
 }
@@ -648,7 +680,7 @@ __global__ void __launch_bounds__(256) k_extrapolate(int sx, int sy, int sz, con
                 if(vin[f - sx]) { sum += gin[f - sx]; ++count; }
                 if(vin[f + sxy]) { sum += gin[f + sxy]; ++count; }
                 if(vin[f - sxy]) { sum += gin[f - sxy]; ++count; }
-                if(count > 0) { val = sum / (float)count; vv = 1; }
+                if(count > 0) { val = sum / (float)count; vv = 2; }  // 2: extrapolated in this pass
             }
             vout[f] = vv;
             if(mode == 1) {
@@ -766,11 +798,13 @@ __global__ void k_active_rows(size_t nc, const uint32_t* __restrict__ flag, cons
 // bottom, far, near with the ghost-fluid 1/theta terms, neighbour rows for fluid
 // neighbours.  Neighbours are stored in ascending column order (-z,-y,-x,+x,+y,+z), the
 // order FixedSparseMatrix::multiply sums them in (SparseMatrix.cpp:222-235).
+template<bool WEIGHTED>
 __global__ void k_build_rows(GridDesc g, int nrows, const uint32_t* __restrict__ rowCell,
                              const float* __restrict__ phi, const uint32_t* __restrict__ aidx,
                              const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w,
+                             const float* __restrict__ wu, const float* __restrict__ wv, const float* __restrict__ ww,
                              float dt, float* __restrict__ rhs, float* __restrict__ diag, float* __restrict__ invdiag,
-                             int32_t* __restrict__ nbr, DevState* st) {
+                             int32_t* __restrict__ nbr, float* __restrict__ coef, DevState* st) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if(r >= nrows) return;
     const uint32_t c = rowCell[r];
@@ -785,6 +819,9 @@ __global__ void k_build_rows(GridDesc g, int nrows, const uint32_t* __restrict__
         rhs[r] = 0.f; diag[r] = 0.f; invdiag[r] = 0.f;
 #pragma unroll
         for(int q = 0; q < 6; ++q) nbr[(size_t)q * nrows + r] = -1;
+        if(WEIGHTED)
+#pragma unroll
+            for(int q = 0; q < 6; ++q) coef[(size_t)q * nrows + r] = 0.f;
         return;
     }
     const size_t sxu = G0 + 1, sxv = G0, sxw = G0;
@@ -792,42 +829,57 @@ __global__ void k_build_rows(GridDesc g, int nrows, const uint32_t* __restrict__
     const float pc = phi[c];
     const size_t GG = (size_t)G0 * G1;
     const float pr = phi[c + 1], pl = phi[c - 1], pt = phi[c + G0], pb = phi[c - G0], pf = phi[c + GG], pn = phi[c - GG];
+    // faces: right, left, top, bottom, far, near
+    const size_t fidx[6] = {(size_t)k * sxyu + (size_t)j * sxu + i + 1, (size_t)k * sxyu + (size_t)j * sxu + i,
+                            (size_t)k * sxyv + (size_t)(j + 1) * sxv + i, (size_t)k * sxyv + (size_t)j * sxv + i,
+                            (size_t)(k + 1) * sxyw + (size_t)j * sxw + i, (size_t)k * sxyw + (size_t)j * sxw + i};
+    float wt[6] = {1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f};
+    if(WEIGHTED) {
+        wt[0] = wu[fidx[0]]; wt[1] = wu[fidx[1]]; wt[2] = wv[fidx[2]];
+        wt[3] = wv[fidx[3]]; wt[4] = ww[fidx[4]]; wt[5] = ww[fidx[5]];
+    }
     float rv = 0.f;
-    const float term = 1.0f * dt;
-    rv -= 1.0f * u[(size_t)k * sxyu + (size_t)j * sxu + i + 1];
-    rv += 1.0f * u[(size_t)k * sxyu + (size_t)j * sxu + i];
-    rv -= 1.0f * v[(size_t)k * sxyv + (size_t)(j + 1) * sxv + i];
-    rv += 1.0f * v[(size_t)k * sxyv + (size_t)j * sxv + i];
-    rv -= 1.0f * w[(size_t)(k + 1) * sxyw + (size_t)j * sxw + i];
-    rv += 1.0f * w[(size_t)k * sxyw + (size_t)j * sxw + i];
+    rv -= wt[0] * u[fidx[0]];
+    rv += wt[1] * u[fidx[1]];
+    rv -= wt[2] * v[fidx[2]];
+    rv += wt[3] * v[fidx[3]];
+    rv -= wt[4] * w[fidx[4]];
+    rv += wt[5] * w[fidx[5]];
     rhs[r] = rv;
     float center = 0.f;
-    // right, left, top, bottom, far, near
     const float phn[6] = {pr, pl, pt, pb, pf, pn};
     const size_t nc_[6] = {c + 1, c - 1, c + G0, c - G0, c + GG, c - GG};
     const int slotOf[6] = {3, 2, 4, 1, 5, 0};
+    float co[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
     for(int q = 0; q < 6; ++q) {
+        const float term = wt[q] * dt;
         if(phn[q] < 0.f) {
             center += term;
             nb[slotOf[q]] = (int32_t)aidx[nc_[q]];
+            co[slotOf[q]] = -term;
         } else {
             const float th = smax(0.01f, fraction_inside(pc, phn[q]));
             center += term / th;
         }
     }
     diag[r] = center;
-    invdiag[r] = 1.0f / center;
+    // a cell closed off by zero-weight (solid) faces has a zero diagonal: Jacobi weight 0
+    invdiag[r] = center != 0.f ? 1.0f / center : 0.f;
 #pragma unroll
     for(int q = 0; q < 6; ++q) nbr[(size_t)q * nrows + r] = nb[q];
+    if(WEIGHTED)
+#pragma unroll
+        for(int q = 0; q < 6; ++q) coef[(size_t)q * nrows + r] = co[q];
 }
 
 // ----------------------------------------------------------------------------------
 // Pressure update
 // ----------------------------------------------------------------------------------
-// PIC_Solver::updateProjectedVelocity (PIC_Solver.cpp:911-981), weights 1: face (i,j,k)
-// of component D between cells c- and c gets u -= dt*(p_c - p_c-)/max(0.01, theta) when
-// either cell is fluid and is marked valid; every other face is set to 0.  Fluid cells lie
+// PIC_Solver::updateProjectedVelocity (PIC_Solver.cpp:911-981): face (i,j,k) of component
+// D between cells c- and c gets u -= dt*(p_c - p_c-)/max(0.01, theta) when either cell is
+// fluid and the face weight is positive (weights 1 without solid boundaries), and is
+// marked valid; every other face is set to 0.  Fluid cells lie
 // within one cell of the occupied-cell box, so only faces within 2 of it can be valid:
 // the blocks stride over that box and the host zeroes the output arrays beforehand.
 template<int D>
@@ -836,7 +888,8 @@ __global__ void __launch_bounds__(256) k_update_velocity(GridDesc g, const DevSt
                                                          const uint32_t* __restrict__ aidx,
                                                          const float* __restrict__ pressure, float dt,
                                                          const float* __restrict__ velIn, float* __restrict__ velOut,
-                                                         uint8_t* __restrict__ validOut) {
+                                                         uint8_t* __restrict__ validOut,
+                                                         const float* __restrict__ weight) {
     const int S[3] = {g.G[0] + (D == 0), g.G[1] + (D == 1), g.G[2] + (D == 2)};
     int lo[3], hi[3];
     if(!reach_box(st, 2, S, lo, hi)) return;
@@ -857,7 +910,7 @@ __global__ void __launch_bounds__(256) k_update_velocity(GridDesc g, const DevSt
             const size_t step = D == 0 ? 1 : (D == 1 ? (size_t)g.G[0] : (size_t)g.G[0] * g.G[1]);
             const size_t cm = c - step;
             const float pc = phi[c], pm = phi[cm];
-            if(pc < 0.f || pm < 0.f) {
+            if((pc < 0.f || pm < 0.f) && (!weight || weight[f] > 0.f)) {
                 const float prc = pc < 0.f ? pressure[aidx[c]] : 0.f;
                 const float prm = pm < 0.f ? pressure[aidx[cm]] : 0.f;
                 const float th = smax(0.01f, fraction_inside(pm, pc));
@@ -867,6 +920,183 @@ __global__ void __launch_bounds__(256) k_update_velocity(GridDesc g, const DevSt
         }
         velOut[f] = out;
         validOut[f] = vv;
+    }
+}
+
+// ----------------------------------------------------------------------------------
+// Solid boundaries (dynamic boundary objects)
+// ----------------------------------------------------------------------------------
+// MathHelpers::fraction_inside(bl, br, tl, tr) (MathHelpers.h:821-900), the area fraction
+// of a square whose corners have these signed distances that lies inside (negative); the
+// corners are walked as the cycle bl, br, tr, tl, rotated to a canonical start.
+__device__ __forceinline__ float fraction_inside4(float bl, float br, float tl, float tr) {
+    const int inside = (bl < 0.f ? 1 : 0) + (tl < 0.f ? 1 : 0) + (br < 0.f ? 1 : 0) + (tr < 0.f ? 1 : 0);
+    float l[4] = {bl, br, tr, tl};
+    auto rotate = [&l]() { const float t = l[0]; l[0] = l[1]; l[1] = l[2]; l[2] = l[3]; l[3] = t; };
+    if(inside == 4) return 1.0f;
+    if(inside == 3) {
+        for(int it = 0; it < 4 && l[0] < 0.f; ++it) rotate();
+        const float side0 = 1.0f - fraction_inside(l[0], l[3]);
+        const float side1 = 1.0f - fraction_inside(l[0], l[1]);
+        return 1.0f - 0.5f * side0 * side1;
+    }
+    if(inside == 2) {
+        for(int it = 0; it < 4 && (l[0] >= 0.f || !(l[1] < 0.f || l[2] < 0.f)); ++it) rotate();
+        if(l[1] < 0.f) {
+            const float left = fraction_inside(l[0], l[3]);
+            const float right = fraction_inside(l[1], l[2]);
+            return 0.5f * (left + right);
+        }
+        const float mid = 0.25f * (l[0] + l[1] + l[2] + l[3]);
+        if(mid < 0.f) {
+            float area = 0.f;
+            const float side1 = 1.0f - fraction_inside(l[0], l[3]);
+            const float side3 = 1.0f - fraction_inside(l[2], l[3]);
+            area += 0.5f * side1 * side3;
+            const float side2 = 1.0f - fraction_inside(l[2], l[1]);
+            const float side0 = 1.0f - fraction_inside(l[0], l[1]);
+            area += 0.5f * side0 * side2;
+            return 1.0f - area;
+        }
+        float area = 0.f;
+        const float side0 = fraction_inside(l[0], l[1]);
+        const float side1 = fraction_inside(l[0], l[3]);
+        area += 0.5f * side0 * side1;
+        const float side2 = fraction_inside(l[2], l[1]);
+        const float side3 = fraction_inside(l[2], l[3]);
+        area += 0.5f * side2 * side3;
+        return area;
+    }
+    if(inside == 1) {
+        for(int it = 0; it < 4 && l[0] >= 0.f; ++it) rotate();
+        const float side0 = fraction_inside(l[0], l[3]);
+        const float side1 = fraction_inside(l[0], l[1]);
+        return 0.5f * side0 * side1;
+    }
+    return 0.f;
+}
+
+// PIC_Solver::computeBoundarySDF (PIC_Solver.cpp:1157-1168): at every grid node the
+// minimum over the boundary objects (the static CSG union first, then the dynamic ones)
+__global__ void k_node_sdf(GridDesc g, float* __restrict__ out) {
+    const int nx = g.G[0] + 1, ny = g.G[1] + 1, nz = g.G[2] + 1;
+    const size_t total = (size_t)nx * ny * nz;
+    const int ng = 1 + g.nObj - g.nStatic;
+    for(size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(t % nx), j = (int)((t / nx) % ny), k = (int)(t / ((size_t)nx * ny));
+        const float x = g.bmin[0] + (float)i * g.dx, y = g.bmin[1] + (float)j * g.dx, z = g.bmin[2] + (float)k * g.dx;
+        float m = 3.402823466e+38f;
+        for(int grp = 0; grp < ng; ++grp) m = smin(m, group_sdf(g, grp, x, y, z));
+        out[t] = m;
+    }
+}
+
+// PIC_Solver::computeCellWeights (PIC_Solver.cpp:565-597): weight of a face = the part of
+// it outside the solid, 1 - fraction_inside of its four corner nodes, clamped to [0, 1]
+template<int D>
+__global__ void k_face_weights(GridDesc g, const float* __restrict__ nsdf, float* __restrict__ wout) {
+    const int sx = g.G[0] + (D == 0), sy = g.G[1] + (D == 1), sz = g.G[2] + (D == 2);
+    const int nx = g.G[0] + 1, ny = g.G[1] + 1;
+    const size_t total = (size_t)sx * sy * sz;
+    for(size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(t % sx), j = (int)((t / sx) % sy), k = (int)(t / ((size_t)sx * sy));
+        auto N = [&](int a, int b, int c) { return nsdf[((size_t)c * ny + b) * nx + a]; };
+        float f;
+        if(D == 0) f = fraction_inside4(N(i, j, k), N(i, j + 1, k), N(i, j, k + 1), N(i, j + 1, k + 1));
+        else if(D == 1) f = fraction_inside4(N(i, j, k), N(i, j, k + 1), N(i + 1, j, k), N(i + 1, j, k + 1));
+        else f = fraction_inside4(N(i, j, k), N(i, j + 1, k), N(i + 1, j, k), N(i + 1, j + 1, k));
+        const float tmp = 1.0f - f;
+        wout[t] = tmp < 0.f ? 0.f : (tmp > 1.0f ? 1.0f : tmp);  // MathHelpers::clamp01
+    }
+}
+
+// PIC_Solver::computeFluidSDF, solid part (PIC_Solver.cpp:671-688): a cell near the fluid
+// (phi < dx/2) whose corners average to inside the solid becomes fluid at -dx/2
+__global__ void k_solid_extend(GridDesc g, const float* __restrict__ nsdf, float* __restrict__ phi) {
+    const int nx = g.G[0] + 1, ny = g.G[1] + 1;
+    const size_t total = (size_t)g.G[0] * g.G[1] * g.G[2];
+    const float half = 0.5f * g.dx;
+    for(size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        if(!(phi[t] < half)) continue;
+        const int i = (int)(t % g.G[0]), j = (int)((t / g.G[0]) % g.G[1]), k = (int)(t / ((size_t)g.G[0] * g.G[1]));
+        auto N = [&](int a, int b, int c) { return nsdf[((size_t)c * ny + b) * nx + a]; };
+        const float solid = 0.125f * (N(i, j, k) + N(i + 1, j, k) + N(i, j + 1, k) + N(i + 1, j + 1, k) +
+                                      N(i, j, k + 1) + N(i + 1, j, k + 1) + N(i, j + 1, k + 1) + N(i + 1, j + 1, k + 1));
+        if(solid < 0.f) phi[t] = -half;
+    }
+}
+
+// ArrayHelpers::interpolateGradient 3D (ArrayHelpers.cpp:214-251) of the node SDF
+__device__ __forceinline__ void node_gradient(const float* __restrict__ a, int nx, int ny, int nz, float px, float py,
+                                              float pz, float out[3]) {
+    int i, j, k;
+    float fi, fj, fk;
+    bary(px, i, fi, nx);
+    bary(py, j, fj, ny);
+    bary(pz, k, fk, nz);
+    auto A = [&](int x, int y, int z) { return a[((size_t)z * ny + y) * nx + x]; };
+    const float v000 = A(i, j, k), v001 = A(i, j, k + 1), v010 = A(i, j + 1, k), v011 = A(i, j + 1, k + 1);
+    const float v100 = A(i + 1, j, k), v101 = A(i + 1, j, k + 1), v110 = A(i + 1, j + 1, k), v111 = A(i + 1, j + 1, k + 1);
+    // MathHelpers::bilerp(v00, v10, v01, v11, fx, fy) = lerp(lerp(v00, v10, fx), lerp(v01, v11, fx), fy)
+    auto bil = [](float v00, float v10, float v01, float v11, float fx, float fy) {
+        return lerpf(lerpf(v00, v10, fx), lerpf(v01, v11, fx), fy);
+    };
+    out[0] = bil(v100 - v000, v110 - v010, v101 - v001, v111 - v011, fj, fk);
+    out[1] = bil(v010 - v000, v110 - v100, v011 - v001, v111 - v101, fi, fk);
+    out[2] = bil(v001 - v000, v101 - v100, v011 - v010, v111 - v110, fi, fj);
+}
+
+// PIC_Solver::constrainGridVelocity (PIC_Solver.cpp:1093-1115), component D: a face that
+// the last extrapolation filled (valid flag 2) and whose weight is 0 loses the velocity
+// component along the boundary normal.  The new values go to tmp (candidate faces only)
+// and are copied back by k_constrain_apply, so every face reads the component as it was.
+template<int D>
+__global__ void __launch_bounds__(256) k_constrain_compute(GridDesc g, const DevState* __restrict__ st,
+                                                           const float* __restrict__ u, const float* __restrict__ v,
+                                                           const float* __restrict__ w,
+                                                           const uint8_t* __restrict__ valid,
+                                                           const float* __restrict__ weight,
+                                                           const float* __restrict__ nsdf, float* __restrict__ tmp) {
+    const int S[3] = {g.G[0] + (D == 0), g.G[1] + (D == 1), g.G[2] + (D == 2)};
+    int lo[3], hi[3];
+    if(!reach_box(st, kExtFull, S, lo, hi)) return;
+    const long long nx = hi[0] - lo[0] + 1, ny = hi[1] - lo[1] + 1, nz = hi[2] - lo[2] + 1;
+    for(long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nx * ny * nz;
+        t += (long long)gridDim.x * blockDim.x) {
+        const int i = lo[0] + (int)(t % nx), j = lo[1] + (int)((t / nx) % ny), k = lo[2] + (int)(t / (nx * ny));
+        const size_t f = ((size_t)k * S[1] + j) * S[0] + i;
+        if(valid[f] != 2 || !(weight[f] < FLT_MIN)) continue;
+        const float gp[3] = {(float)i + (D == 0 ? 0.f : 0.5f), (float)j + (D == 1 ? 0.f : 0.5f),
+                             (float)k + (D == 2 ? 0.f : 0.5f)};
+        float vel[3];
+        vel_from_grid(g, u, v, w, gp[0], gp[1], gp[2], vel);
+        float nrm[3];
+        node_gradient(nsdf, g.G[0] + 1, g.G[1] + 1, g.G[2] + 1, gp[0], gp[1], gp[2], nrm);
+        const float m2 = length2f(nrm[0], nrm[1], nrm[2]);
+        float out = (D == 0 ? u : (D == 1 ? v : w))[f];
+        if(m2 > FLT_MIN) {
+            const float sq = sqrtf(m2);
+            nrm[0] = nrm[0] / sq; nrm[1] = nrm[1] / sq; nrm[2] = nrm[2] / sq;
+            const float dn = (vel[0] * nrm[0] + vel[1] * nrm[1]) + vel[2] * nrm[2];
+            out = vel[D] - dn * nrm[D];
+        }
+        tmp[f] = out;
+    }
+}
+template<int D>
+__global__ void __launch_bounds__(256) k_constrain_apply(GridDesc g, const DevState* __restrict__ st,
+                                                         const uint8_t* __restrict__ valid,
+                                                         const float* __restrict__ weight,
+                                                         const float* __restrict__ tmp, float* __restrict__ vel) {
+    const int S[3] = {g.G[0] + (D == 0), g.G[1] + (D == 1), g.G[2] + (D == 2)};
+    int lo[3], hi[3];
+    if(!reach_box(st, kExtFull, S, lo, hi)) return;
+    const long long nx = hi[0] - lo[0] + 1, ny = hi[1] - lo[1] + 1, nz = hi[2] - lo[2] + 1;
+    for(long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nx * ny * nz;
+        t += (long long)gridDim.x * blockDim.x) {
+        const int i = lo[0] + (int)(t % nx), j = lo[1] + (int)((t / nx) % ny), k = lo[2] + (int)(t / (nx * ny));
+        const size_t f = ((size_t)k * S[1] + j) * S[0] + i;
+        if(valid[f] == 2 && weight[f] < FLT_MIN) vel[f] = tmp[f];
     }
 }
 
@@ -1172,25 +1402,53 @@ void launch_active_flags(const GridDesc& g, const float* phi, uint32_t* flag, De
 void launch_active_rows(size_t nc, const uint32_t* flag, const uint32_t* idx, uint32_t* rowCell, cudaStream_t s) {
     { k_active_rows<<<nblk(nc), 256, 0, s>>>(nc, flag, idx, rowCell); bnn_note_launch(); }
 }
+// W (optional): face weights of u, v, w; with them the off-diagonal values go to coef
 void launch_build_rows(const GridDesc& g, int nrows, const uint32_t* rowCell, const float* phi, const uint32_t* aidx,
-                       const float* const* U, float dt, float* rhs, float* diag, float* invdiag, int32_t* nbr,
-                       DevState* st, cudaStream_t s) {
+                       const float* const* U, const float* const* W, float dt, float* rhs, float* diag, float* invdiag,
+                       int32_t* nbr, float* coef, DevState* st, cudaStream_t s) {
     if(nrows == 0) return;
-    { k_build_rows<<<nblk(nrows), 256, 0, s>>>(g, nrows, rowCell, phi, aidx, U[0], U[1], U[2], dt, rhs, diag, invdiag,
-                                             nbr, st); bnn_note_launch(); }
+    if(W) {
+        k_build_rows<true><<<nblk(nrows), 256, 0, s>>>(g, nrows, rowCell, phi, aidx, U[0], U[1], U[2], W[0], W[1], W[2],
+                                                     dt, rhs, diag, invdiag, nbr, coef, st);
+    } else {
+        k_build_rows<false><<<nblk(nrows), 256, 0, s>>>(g, nrows, rowCell, phi, aidx, U[0], U[1], U[2], nullptr, nullptr,
+                                                      nullptr, dt, rhs, diag, invdiag, nbr, nullptr, st);
+    }
+    bnn_note_launch();
 }
 // Reads velIn, writes the projected faces to velOut / validOut (zeroed here first).
 void launch_update_velocity(const GridDesc& g, const DevState* st, const float* phi, const uint32_t* aidx,
                             const float* pressure, float dt, float* const* velIn, float* const* velOut,
-                            uint8_t* const* validOut, cudaStream_t s) {
+                            uint8_t* const* validOut, const float* const* W, cudaStream_t s) {
     for(int d = 0; d < 3; ++d) {
         const size_t nf = (size_t)face_sx(g, d) * face_sy(g, d) * face_sz(g, d);
         cudaMemsetAsync(velOut[d], 0, nf * sizeof(float), s);
         cudaMemsetAsync(validOut[d], 0, nf, s);
     }
-    { k_update_velocity<0><<<kRegionBlocks, 256, 0, s>>>(g, st, phi, aidx, pressure, dt, velIn[0], velOut[0], validOut[0]); bnn_note_launch(); }
-    { k_update_velocity<1><<<kRegionBlocks, 256, 0, s>>>(g, st, phi, aidx, pressure, dt, velIn[1], velOut[1], validOut[1]); bnn_note_launch(); }
-    { k_update_velocity<2><<<kRegionBlocks, 256, 0, s>>>(g, st, phi, aidx, pressure, dt, velIn[2], velOut[2], validOut[2]); bnn_note_launch(); }
+    { k_update_velocity<0><<<kRegionBlocks, 256, 0, s>>>(g, st, phi, aidx, pressure, dt, velIn[0], velOut[0], validOut[0], W ? W[0] : nullptr); bnn_note_launch(); }
+    { k_update_velocity<1><<<kRegionBlocks, 256, 0, s>>>(g, st, phi, aidx, pressure, dt, velIn[1], velOut[1], validOut[1], W ? W[1] : nullptr); bnn_note_launch(); }
+    { k_update_velocity<2><<<kRegionBlocks, 256, 0, s>>>(g, st, phi, aidx, pressure, dt, velIn[2], velOut[2], validOut[2], W ? W[2] : nullptr); bnn_note_launch(); }
+}
+// Node SDF of the boundary objects and the face weights it gives
+void launch_boundary_grid(const GridDesc& g, float* nodeSdf, float* const* W, cudaStream_t s) {
+    { k_node_sdf<<<kRegionBlocks, 256, 0, s>>>(g, nodeSdf); bnn_note_launch(); }
+    { k_face_weights<0><<<kRegionBlocks, 256, 0, s>>>(g, nodeSdf, W[0]); bnn_note_launch(); }
+    { k_face_weights<1><<<kRegionBlocks, 256, 0, s>>>(g, nodeSdf, W[1]); bnn_note_launch(); }
+    { k_face_weights<2><<<kRegionBlocks, 256, 0, s>>>(g, nodeSdf, W[2]); bnn_note_launch(); }
+}
+void launch_solid_extend(const GridDesc& g, const float* nodeSdf, float* phi, cudaStream_t s) {
+    { k_solid_extend<<<kRegionBlocks, 256, 0, s>>>(g, nodeSdf, phi); bnn_note_launch(); }
+}
+// constrainGridVelocity over U (components in order, each reading the ones before it as
+// already constrained); T is scratch of the face arrays' sizes
+void launch_constrain_velocity(const GridDesc& g, const DevState* st, float* const* U, uint8_t* const* V,
+                               float* const* W, const float* nodeSdf, float* const* T, cudaStream_t s) {
+    { k_constrain_compute<0><<<kRegionBlocks, 256, 0, s>>>(g, st, U[0], U[1], U[2], V[0], W[0], nodeSdf, T[0]); bnn_note_launch(); }
+    { k_constrain_apply<0><<<kRegionBlocks, 256, 0, s>>>(g, st, V[0], W[0], T[0], U[0]); bnn_note_launch(); }
+    { k_constrain_compute<1><<<kRegionBlocks, 256, 0, s>>>(g, st, U[0], U[1], U[2], V[1], W[1], nodeSdf, T[1]); bnn_note_launch(); }
+    { k_constrain_apply<1><<<kRegionBlocks, 256, 0, s>>>(g, st, V[1], W[1], T[1], U[1]); bnn_note_launch(); }
+    { k_constrain_compute<2><<<kRegionBlocks, 256, 0, s>>>(g, st, U[0], U[1], U[2], V[2], W[2], nodeSdf, T[2]); bnn_note_launch(); }
+    { k_constrain_apply<2><<<kRegionBlocks, 256, 0, s>>>(g, st, V[2], W[2], T[2], U[2]); bnn_note_launch(); }
 }
 void launch_g2p(int n, const GridDesc& g, float* p6, size_t stride, const float* const* U, const float* const* O,
                 float ratio, int kind, float* C9, cudaStream_t s) {

@@ -3,8 +3,9 @@
 //
 // Rows are the fluid cells in linear-cell order.  Per row: diag (float), 1/diag, and six
 // neighbour row indices in ascending column order (-z,-y,-x,+x,+y,+z; -1 = none), stored
-// as six planes nbr[q*n + r].  Every off-diagonal equals -dt (face weight 1), so the
-// matrix is never materialised.
+// as six planes nbr[q*n + r].  With face weights 1 every off-diagonal equals -dt, so the
+// matrix is never materialised; with solid boundaries (weights below 1) six planes of
+// off-diagonal values coef[q*n + r] ride along with the compact rows.
 //
 // Rows of a grid (rows numbered in cell order) are also packed into one 16-byte record
 // each: the x neighbours are always rows r-1 / r+1, so they become two flag bits, the y
@@ -184,6 +185,7 @@ template<class VT> struct PcgArgs {
     const VT* invd;
     const int32_t* nbr;
     const int4* rec;
+    const float* coef;  // compact rows only: off-diagonal values (nullptr: all negoff)
     VT negoff;
     VT tolFactor;
     unsigned maxIter;
@@ -219,6 +221,7 @@ __global__ void __launch_bounds__(kLanes, BNN_PCG_MIN_BLOCKS) k_pcg_persistent(P
     const float* __restrict__ diagR = a.diag;
     const int32_t* __restrict__ nbrR = a.nbr;
     const int4* __restrict__ recR = a.rec;
+    const float* __restrict__ coefR = a.coef;
     const VT negoff = a.negoff;
     const int lane = threadIdx.x & 31;
 
@@ -287,6 +290,7 @@ __global__ void __launch_bounds__(kLanes, BNN_PCG_MIN_BLOCKS) k_pcg_persistent(P
                 int32_t id[kRowGroup][7];
                 bool has[kRowGroup][7];
                 float dg[kRowGroup];
+                size_t rowE[kRowGroup];
 #pragma unroll
                 for(int u = 0; u < kRowGroup; ++u) {
                     const size_t e = base + (size_t)(g0 + u) * kLanes;
@@ -314,6 +318,7 @@ __global__ void __launch_bounds__(kLanes, BNN_PCG_MIN_BLOCKS) k_pcg_persistent(P
                             has[u][slot] = v >= 0;
                             id[u][slot] = v >= 0 ? v : (int32_t)ee;
                         }
+                        rowE[u] = ee;
                         id[u][3] = (int32_t)ee;
                         has[u][3] = true;
                         dg[u] = __ldg(diagR + ee);
@@ -341,11 +346,23 @@ __global__ void __launch_bounds__(kLanes, BNN_PCG_MIN_BLOCKS) k_pcg_persistent(P
                         if(lane != 31) s7[4] = dn;
                     }
                     VT t = VT(0);
+                    if constexpr(PACKED) {
 #pragma unroll
-                    for(int q = 0; q < 3; ++q) if(has[u][q]) t += negoff * s7[q];
-                    if(dg[u] != 0.f) t += (VT)dg[u] * s7[3];
+                        for(int q = 0; q < 3; ++q) if(has[u][q]) t += negoff * s7[q];
+                        if(dg[u] != 0.f) t += (VT)dg[u] * s7[3];
 #pragma unroll
-                    for(int q = 4; q < 7; ++q) if(has[u][q]) t += negoff * s7[q];
+                        for(int q = 4; q < 7; ++q) if(has[u][q]) t += negoff * s7[q];
+                    } else {
+                        // off-diagonal of slot q (plane q, or q - 1 above the diagonal)
+                        auto cf = [&](int q) {
+                            return coefR ? (VT)__ldg(coefR + (size_t)(q < 3 ? q : q - 1) * n + rowE[u]) : negoff;
+                        };
+#pragma unroll
+                        for(int q = 0; q < 3; ++q) if(has[u][q]) t += cf(q) * s7[q];
+                        if(dg[u] != 0.f) t += (VT)dg[u] * s7[3];
+#pragma unroll
+                        for(int q = 4; q < 7; ++q) if(has[u][q]) t += cf(q) * s7[q];
+                    }
                     sOut[g0 + u] = s7[3];
                     qOut[g0 + u] = t;
                 }
@@ -486,7 +503,8 @@ __global__ void k_ir_accumulate(int n, double* __restrict__ x64, const float* __
 __global__ void __launch_bounds__(kLanes) k_ir_residual(int n, const float* __restrict__ b,
                                                         const double* __restrict__ x64, double* __restrict__ r64,
                                                         const float* __restrict__ diag,
-                                                        const int32_t* __restrict__ nbr, double negoff,
+                                                        const int32_t* __restrict__ nbr,
+                                                        const float* __restrict__ coef, double negoff,
                                                         double* __restrict__ partMax, DevState* st) {
     __shared__ double sm[kLanes];
     const size_t base = (size_t)blockIdx.x * kChunk + threadIdx.x;
@@ -496,14 +514,17 @@ __global__ void __launch_bounds__(kLanes) k_ir_residual(int n, const float* __re
         if(e < (size_t)n) {
             const int32_t nn[6] = {nbr[e], nbr[(size_t)n + e], nbr[2 * (size_t)n + e], nbr[3 * (size_t)n + e],
                                    nbr[4 * (size_t)n + e], nbr[5 * (size_t)n + e]};
+            double co[6];
+#pragma unroll
+            for(int q = 0; q < 6; ++q) co[q] = coef ? (double)coef[(size_t)q * n + e] : negoff;
             double t = 0.0;
-            if(nn[0] >= 0) t += negoff * x64[nn[0]];
-            if(nn[1] >= 0) t += negoff * x64[nn[1]];
-            if(nn[2] >= 0) t += negoff * x64[nn[2]];
+            if(nn[0] >= 0) t += co[0] * x64[nn[0]];
+            if(nn[1] >= 0) t += co[1] * x64[nn[1]];
+            if(nn[2] >= 0) t += co[2] * x64[nn[2]];
             if(diag[e] != 0.f) t += (double)diag[e] * x64[e];
-            if(nn[3] >= 0) t += negoff * x64[nn[3]];
-            if(nn[4] >= 0) t += negoff * x64[nn[4]];
-            if(nn[5] >= 0) t += negoff * x64[nn[5]];
+            if(nn[3] >= 0) t += co[3] * x64[nn[3]];
+            if(nn[4] >= 0) t += co[4] * x64[nn[4]];
+            if(nn[5] >= 0) t += co[5] * x64[nn[5]];
             const double rv = (double)b[e] - t;
             r64[e] = rv;
             const double a = vabs(rv);
@@ -631,7 +652,7 @@ void pcg_release(PcgWork& w) {
 // the solution is left in x.
 template<class VT>
 static int pcg_solve_t(PcgWork& w, int n, const float* rhsF, const float* diag, const VT* invd, const int32_t* nbr,
-                       const int4* rec, VT negoff, VT tolFactor, unsigned maxIter, VT* x, VT* r, VT* z, VT* s0, VT* s1, VT* q,
+                       const int4* rec, const float* coef, VT negoff, VT tolFactor, unsigned maxIter, VT* x, VT* r, VT* z, VT* s0, VT* s1, VT* q,
                        VT* partMax, DevState* dst, DevState* hst, cudaStream_t s, PcgOutcome& out) {
     out = PcgOutcome();
     if(n == 0) { out.success = 1; return BNN_OK; }
@@ -657,7 +678,7 @@ static int pcg_solve_t(PcgWork& w, int n, const float* rhsF, const float* diag, 
     const int perBlock = (nch + cap - 1) / cap;           // chunks per block
     const int grid = (nch + perBlock - 1) / perBlock;     // balanced: every block the same count
     PcgArgs<VT> a;
-    a.n = n; a.rhsF = rhsF; a.diag = diag; a.invd = invd; a.nbr = nbr; a.rec = rec; a.negoff = negoff; a.tolFactor = tolFactor;
+    a.n = n; a.rhsF = rhsF; a.diag = diag; a.invd = invd; a.nbr = nbr; a.rec = rec; a.coef = coef; a.negoff = negoff; a.tolFactor = tolFactor;
     a.maxIter = maxIter; a.x = x; a.r = r; a.z = z; a.s0 = s0; a.s1 = s1; a.q = q;
     a.part0 = w.part; a.part1 = w.part + w.nchCap; a.part2 = w.part + 2 * (size_t)w.nchCap; a.partMax = partMax;
     a.st = dst; a.gs = w.gs;
@@ -679,20 +700,22 @@ static int pcg_solve_t(PcgWork& w, int n, const float* rhsF, const float* diag, 
 
 // mode: BNN_PCG_FP32 / FP64 / REFINED.  Pressure written to `pressure` (float, n).
 int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const float* invd, const int32_t* nbr,
-              bool gridRows, float dt, int mode, float tol, unsigned maxIter, float innerTol, float outerTol,
-              float* pressure, double* x64out, DevState* dst, DevState* hst, cudaStream_t s, PcgOutcome& out) {
+              const float* coef, bool gridRows, float dt, int mode, float tol, unsigned maxIter, float innerTol,
+              float outerTol, float* pressure, double* x64out, DevState* dst, DevState* hst, cudaStream_t s,
+              PcgOutcome& out) {
     int rc = pcg_reserve(w, n, mode != BNN_PCG_FP32);
     if(rc != BNN_OK) return rc;
     const unsigned nb = (unsigned)((n + 255) / 256);
     const unsigned nch = (unsigned)((n + kChunk - 1) / kChunk);
     out = PcgOutcome();
     const int4* rec = nullptr;
+    if(coef) gridRows = false;  // the packed records carry no off-diagonal values
     if(gridRows && n > 0) {
         { k_pack_rows<<<nb, 256, 0, s>>>(n, diag, nbr, w.rec); bnn_note_launch(); }
         rec = w.rec;
     }
     if(mode == BNN_PCG_FP32) {
-        rc = pcg_solve_t<float>(w, n, rhs, diag, invd, nbr, rec, -(1.0f * dt), tol, maxIter, w.x, w.r, w.z, w.s0, w.s1,
+        rc = pcg_solve_t<float>(w, n, rhs, diag, invd, nbr, rec, coef, -(1.0f * dt), tol, maxIter, w.x, w.r, w.z, w.s0, w.s1,
                                 w.q, w.partMaxF, dst, hst, s, out);
         if(rc != BNN_OK) return rc;
         if(n > 0) BNN_CUDA_CHECK(cudaMemcpyAsync(pressure, w.x, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
@@ -701,7 +724,7 @@ int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const floa
     }
     if(mode == BNN_PCG_FP64) {
         if(n > 0) { k_inv_diag64<<<nb, 256, 0, s>>>(n, diag, w.inv64); bnn_note_launch(); }
-        rc = pcg_solve_t<double>(w, n, rhs, diag, w.inv64, nbr, rec, -(double)(1.0f * dt), (double)tol, maxIter, w.x64,
+        rc = pcg_solve_t<double>(w, n, rhs, diag, w.inv64, nbr, rec, coef, -(double)(1.0f * dt), (double)tol, maxIter, w.x64,
                                  w.r64, w.z64, w.s064, w.s164, w.q64, w.partMaxD, dst, hst, s, out);
         if(rc != BNN_OK) return rc;
         if(n > 0) { k_d64_to_f32<<<nb, 256, 0, s>>>(n, w.x64, pressure); bnn_note_launch(); }
@@ -723,12 +746,12 @@ int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const floa
         if(res < (double)outerTol * bmax) { ok = true; break; }
         { k_ir_to_f32<<<nb, 256, 0, s>>>(n, w.r64, w.r32); bnn_note_launch(); }
         PcgOutcome inner;
-        rc = pcg_solve_t<float>(w, n, w.r32, diag, invd, nbr, rec, -(1.0f * dt), innerTol, maxIter, w.d32, w.r, w.z, w.s0,
+        rc = pcg_solve_t<float>(w, n, w.r32, diag, invd, nbr, rec, coef, -(1.0f * dt), innerTol, maxIter, w.d32, w.r, w.z, w.s0,
                                 w.s1, w.q, w.partMaxF, dst, hst, s, inner);
         if(rc != BNN_OK) return rc;
         total += inner.iterations;
         { k_ir_accumulate<<<nb, 256, 0, s>>>(n, w.x64, w.d32); bnn_note_launch(); }
-        { k_ir_residual<<<nch, kLanes, 0, s>>>(n, rhs, w.x64, w.r64, diag, nbr, (double)(-(1.0f * dt)), w.partMaxD, dst); bnn_note_launch(); }
+        { k_ir_residual<<<nch, kLanes, 0, s>>>(n, rhs, w.x64, w.r64, diag, nbr, coef, (double)(-(1.0f * dt)), w.partMaxD, dst); bnn_note_launch(); }
         BNN_CUDA_CHECK(cudaMemcpyAsync(hst, dst, sizeof(DevState), cudaMemcpyDeviceToHost, s));
         BNN_CUDA_CHECK(cudaStreamSynchronize(s));
         res = hst->outer_res;

@@ -64,6 +64,10 @@ extern "C" {
 #define BNN_FIELD_OLD_V    6
 #define BNN_FIELD_OLD_W    7
 #define BNN_FIELD_ACTIVE   8 /* active cell index + 1 on cells, 0 = not fluid */
+#define BNN_FIELD_WEIGHT_U 9 /* face weights (PIC_Data.h weights); 1 without dynamic boundaries */
+#define BNN_FIELD_WEIGHT_V 10
+#define BNN_FIELD_WEIGHT_W 11
+#define BNN_FIELD_BOUNDARY_SDF 12 /* boundary SDF on the (G+1)^3 nodes (PIC_Data.h boundarySDF) */
 
 /* Values of SimulationParameters / PIC_Parameters / GlobalParameters the step reads
  * (ParticleSolverData.h:87-175, PIC_Data.h:31-40, ParticleSolverData.h:37-75). */
@@ -243,6 +247,36 @@ int bnn_pcg_solve_7pt(uint32_t n, const float* diag, const int32_t* nbr, float o
 
 /* Library version / last CUDA error text / number of kernels this library has launched
  * in this process (diagnostics; no counterpart in the reference). */
+/* ---- boundary objects ------------------------------------------------------------- */
+
+#define BNN_GEOMETRY_BOX     0  /* GeometryObjects::BoxObject (GeometryObjects.cpp:246-268) */
+#define BNN_GEOMETRY_SPHERE  1  /* GeometryObjects::SphereObject, unit sphere in object space */
+
+/* One boundary object of "AdditionalBoundaryObjects" (ParticleSolver::generateBoundaries,
+ * ParticleSolver.cpp:242-295; BoundaryObject.h:41-60): the fluid stays inside it (its
+ * signed distance is taken with bNegativeInside = false).  Its current transformation is
+ * given as the world-to-object map (GeometryObject::invTransform, the inverse of
+ * translate * rotate * scale of the current animation frame) and the uniform scale. */
+typedef struct bnn_boundary_object {
+    int32_t geometry;          /* BNN_GEOMETRY_* */
+    int32_t dynamic;           /* 1: animated ("Animation" present, SimulationObject.cpp:80-82) */
+    float   box_min[3];        /* box corners in object space */
+    float   box_max[3];
+    float   inv_transform[12]; /* rows of the 3x4 world-to-object affine map */
+    float   uniform_scale;
+    int32_t transformed;       /* 0: the map is the identity and is not applied */
+} bnn_boundary_object;
+
+/* Sets the boundary objects besides the domain box (at most 15).  As in the reference,
+ * the static ones are united with the domain box into one CSG object and the dynamic
+ * ones stay separate; particles are projected out of every one after each advection.
+ * When at least one object is dynamic the grid's boundary SDF is recomputed from the
+ * objects as given (PIC_Solver::advanceScene + computeBoundarySDF, PIC_Solver.cpp:
+ * 70-118,1157-1168) and the solve uses the face weights, the solid part of the fluid SDF
+ * and constrainGridVelocity; call it again with the new transformations at the start
+ * of every frame in which an object moves.  n = 0 restores the plain domain box. */
+int bnn_flip_set_boundaries(bnn_flip* h, const bnn_boundary_object* objs, uint32_t n);
+
 /* ---- anisotropic kernels (surface reconstruction output) -------------------------- */
 
 /* AnisotropicKernelGenerator<3, float> (Simulation/SurfaceReconstruction/

@@ -487,6 +487,72 @@ static PCGResult pcg_refined(const CSR& A, const std::vector<float>& vals, const
 // ----------------------------------------------------------------------------------
 // The FLIP step
 // ----------------------------------------------------------------------------------
+// One boundary object (the layout of bnn_boundary_object): BoundaryObject over a Box or
+// Sphere geometry (Simulation/SimulationObjects/BoundaryObject.h:41-60), with its current
+// world-to-object map (GeometryObject::invTransform, GeometryObjects.cpp:231-238)
+struct orc_boundary_object {
+    int32_t geometry;          // 0 box, 1 sphere
+    int32_t dynamic;
+    float   box_min[3];
+    float   box_max[3];
+    float   inv_transform[12]; // rows of a 3x4 affine map
+    float   uniform_scale;
+    int32_t transformed;
+};
+template<class R> struct OObj {
+    int geometry = 0, transformed = 0;
+    R bmin[3] = {0, 0, 0}, bmax[3] = {0, 0, 0}, M[12] = {0}, scale = 1;
+};
+
+// MathHelpers::fraction_inside(bl, br, tl, tr) (MathHelpers.h:821-900): area fraction of a
+// square inside (negative) from its corner values, the corners walked as bl, br, tr, tl
+template<class R> static R fraction_inside4(R bl, R br, R tl, R tr) {
+    int inside = (bl < 0 ? 1 : 0) + (tl < 0 ? 1 : 0) + (br < 0 ? 1 : 0) + (tr < 0 ? 1 : 0);
+    R l[4] = {bl, br, tr, tl};
+    auto cycle = [&l]() { R t = l[0]; for(int i = 0; i < 3; ++i) l[i] = l[i + 1]; l[3] = t; };
+    if(inside == 4) return R(1.0);
+    if(inside == 3) {
+        while(l[0] < 0) cycle();
+        R side0 = R(1.0) - fraction_inside(l[0], l[3]);
+        R side1 = R(1.0) - fraction_inside(l[0], l[1]);
+        return R(1.0) - R(0.5) * side0 * side1;
+    }
+    if(inside == 2) {
+        while(l[0] >= 0 || !(l[1] < 0 || l[2] < 0)) cycle();
+        if(l[1] < 0) {
+            R left = fraction_inside(l[0], l[3]);
+            R right = fraction_inside(l[1], l[2]);
+            return R(0.5) * (left + right);
+        }
+        R mid = R(0.25) * (l[0] + l[1] + l[2] + l[3]);
+        if(mid < 0) {
+            R area = 0;
+            R side1 = R(1.0) - fraction_inside(l[0], l[3]);
+            R side3 = R(1.0) - fraction_inside(l[2], l[3]);
+            area += R(0.5) * side1 * side3;
+            R side2 = R(1.0) - fraction_inside(l[2], l[1]);
+            R side0 = R(1.0) - fraction_inside(l[0], l[1]);
+            area += R(0.5) * side0 * side2;
+            return R(1.0) - area;
+        }
+        R area = 0;
+        R side0 = fraction_inside(l[0], l[1]);
+        R side1 = fraction_inside(l[0], l[3]);
+        area += R(0.5) * side0 * side1;
+        R side2 = fraction_inside(l[2], l[1]);
+        R side3 = fraction_inside(l[2], l[3]);
+        area += R(0.5) * side2 * side3;
+        return area;
+    }
+    if(inside == 1) {
+        while(l[0] >= 0) cycle();
+        R side0 = fraction_inside(l[0], l[3]);
+        R side1 = fraction_inside(l[0], l[1]);
+        return R(0.5) * side0 * side1;
+    }
+    return R(0);
+}
+
 template<class R> class FlipOracle {
 public:
     orc_params P;
@@ -502,6 +568,12 @@ public:
     std::vector<R> rhs, pressure;
     uint32_t nActive = 0, zeroPhiCells = 0;
     uint64_t substepIndex = 0;  // sub-steps taken (keys the position-correction jitter)
+    // boundary objects beyond the domain box: [domain box, static..., dynamic...]
+    std::vector<OObj<R>> objs;
+    int nStatic = 0;
+    bool gridBoundary = false;  // a dynamic object: boundary SDF, weights, constraint
+    Arr3<R> nodeSdf, weight[3];
+    Arr3<char> extrap[3];       // PIC_Data extrapolates: faces the last extrapolation filled
     // last solve
     PCGResult lastSolve;
 
@@ -593,8 +665,65 @@ public:
         g[1] = (((ddy00 + ddy01) + ddy10) + ddy11) * R(0.25);
         g[2] = (((ddz00 + ddz01) + ddz10) + ddz11) * R(0.25);
     }
-    // BoundaryObject::constrainToBoundary(ppos, pvel) (BoundaryObject.cpp:72-90), no reflection
+    // GeometryObject::invTransform + Box / SphereObject::signedDistance(p, false)
+    // (GeometryObjects.cpp:231-268,379-384): positive inside the object
+    static R objSDF(const OObj<R>& o, R x, R y, R z) {
+        R q[3] = {x, y, z};
+        if(o.transformed)
+            for(int r = 0; r < 3; ++r) q[r] = ((o.M[4 * r] * x + o.M[4 * r + 1] * y) + o.M[4 * r + 2] * z) + o.M[4 * r + 3];
+        if(o.geometry == 0) {
+            bool inside = true;
+            for(int d = 0; d < 3; ++d) if(q[d] < o.bmin[d] || q[d] > o.bmax[d]) inside = false;
+            R mind = std::numeric_limits<R>::max();
+            if(inside) {
+                for(int d = 0; d < 3; ++d) mind = smin(mind, smin(q[d] - o.bmin[d], o.bmax[d] - q[d]));
+                mind = -mind;
+            } else {
+                R c[3];
+                for(int d = 0; d < 3; ++d) c[d] = smax(smin(q[d], o.bmax[d]), o.bmin[d]);
+                mind = std::sqrt(length2(q[0] - c[0], q[1] - c[1], q[2] - c[2]));
+            }
+            mind = -mind;
+            return o.scale * mind;
+        }
+        R d = o.scale * (std::sqrt(length2(q[0], q[1], q[2])) - R(1.0));
+        return -d;
+    }
+    // boundary group grp: 0 = CSG union of the static objects (CSGObject::signedDistance,
+    // GeometryObjects.cpp:861-896), g > 0 = the g-th dynamic object
+    R groupSDF(int grp, R x, R y, R z) const {
+        int b = grp == 0 ? 0 : nStatic + grp - 1, e = grp == 0 ? nStatic : b + 1;
+        R sd = objSDF(objs[b], x, y, z);
+        for(int i = b + 1; i < e; ++i) sd = smin(sd, objSDF(objs[i], x, y, z));
+        return sd;
+    }
+    int nGroups() const { return objs.empty() ? 0 : 1 + (int)objs.size() - nStatic; }
+
+    // BoundaryObject::constrainToBoundary(ppos, pvel) (BoundaryObject.cpp:72-90), no
+    // reflection, for every boundary object in turn (PIC_Solver.cpp:353-372)
     void constrain(V3<R>& p) const {
+        if(!objs.empty()) {
+            for(int grp = 0; grp < nGroups(); ++grp) {
+                R phiVal = groupSDF(grp, p.x, p.y, p.z);
+                if(!(phiVal < 0)) continue;
+                const R e = R(1e-4);
+                R v000 = groupSDF(grp, p.x - e, p.y - e, p.z - e), v001 = groupSDF(grp, p.x - e, p.y - e, p.z + e);
+                R v010 = groupSDF(grp, p.x - e, p.y + e, p.z - e), v011 = groupSDF(grp, p.x - e, p.y + e, p.z + e);
+                R v100 = groupSDF(grp, p.x + e, p.y - e, p.z - e), v101 = groupSDF(grp, p.x + e, p.y - e, p.z + e);
+                R v110 = groupSDF(grp, p.x + e, p.y + e, p.z - e), v111 = groupSDF(grp, p.x + e, p.y + e, p.z + e);
+                R g[3];
+                g[0] = ((((v100 - v000) + (v101 - v001)) + (v110 - v010)) + (v111 - v011)) * R(0.25);
+                g[1] = ((((v010 - v000) + (v011 - v001)) + (v110 - v100)) + (v111 - v101)) * R(0.25);
+                g[2] = ((((v001 - v000) + (v011 - v010)) + (v101 - v100)) + (v111 - v110)) * R(0.25);
+                R m2 = length2(g[0], g[1], g[2]);
+                if(m2 > std::numeric_limits<R>::min()) {
+                    R sq = std::sqrt(m2);
+                    g[0] /= sq; g[1] /= sq; g[2] /= sq;
+                    p.x -= phiVal * g[0]; p.y -= phiVal * g[1]; p.z -= phiVal * g[2];
+                }
+            }
+            return;
+        }
         R phiVal = boxSDF(p.x, p.y, p.z);
         if(phiVal < 0) {
             R g[3]; gradBoxSDF(p, g);
@@ -604,6 +733,95 @@ public:
                 g[0] /= s; g[1] /= s; g[2] /= s;
                 p.x -= phiVal * g[0]; p.y -= phiVal * g[1]; p.z -= phiVal * g[2];
             }
+        }
+    }
+
+    // ParticleSolver::generateBoundaries (ParticleSolver.cpp:242-295) + computeBoundarySDF
+    // (PIC_Solver.cpp:1157-1168) + computeCellWeights (PIC_Solver.cpp:543-598)
+    void setBoundaries(const orc_boundary_object* in, uint32_t n) {
+        objs.clear();
+        gridBoundary = false;
+        nStatic = 0;
+        if(n == 0) return;
+        OObj<R> box;
+        for(int d = 0; d < 3; ++d) { box.bmin[d] = boxMin[d]; box.bmax[d] = boxMax[d]; }
+        objs.push_back(box);
+        for(int pass = 0; pass < 2; ++pass)
+            for(uint32_t i = 0; i < n; ++i) {
+                if((in[i].dynamic != 0) != (pass == 1)) continue;
+                OObj<R> o;
+                o.geometry = in[i].geometry;
+                o.transformed = in[i].transformed ? 1 : 0;
+                o.scale = (R)in[i].uniform_scale;
+                for(int d = 0; d < 3; ++d) { o.bmin[d] = (R)in[i].box_min[d]; o.bmax[d] = (R)in[i].box_max[d]; }
+                for(int q = 0; q < 12; ++q) o.M[q] = (R)in[i].inv_transform[q];
+                objs.push_back(o);
+                if(pass == 1) gridBoundary = true;
+            }
+        nStatic = 1;
+        for(uint32_t i = 0; i < n; ++i) nStatic += in[i].dynamic ? 0 : 1;
+        if(!gridBoundary) return;
+        nodeSdf.resize(G[0] + 1, G[1] + 1, G[2] + 1, 0);
+        for(int k = 0; k <= G[2]; ++k)
+            for(int j = 0; j <= G[1]; ++j)
+                for(int i = 0; i <= G[0]; ++i) {
+                    R x = bmin[0] + (R)i * dx, y = bmin[1] + (R)j * dx, z = bmin[2] + (R)k * dx;
+                    R m = std::numeric_limits<R>::max();
+                    for(int grp = 0; grp < nGroups(); ++grp) m = smin(m, groupSDF(grp, x, y, z));
+                    nodeSdf(i, j, k) = m;
+                }
+        for(int d = 0; d < 3; ++d) {
+            weight[d].resize(u[d].sx, u[d].sy, u[d].sz, 0);
+            for(int k = 0; k < u[d].sz; ++k)
+                for(int j = 0; j < u[d].sy; ++j)
+                    for(int i = 0; i < u[d].sx; ++i) {
+                        const Arr3<R>& N = nodeSdf;
+                        R f;
+                        if(d == 0) f = fraction_inside4(N(i, j, k), N(i, j + 1, k), N(i, j, k + 1), N(i, j + 1, k + 1));
+                        else if(d == 1) f = fraction_inside4(N(i, j, k), N(i, j, k + 1), N(i + 1, j, k), N(i + 1, j, k + 1));
+                        else f = fraction_inside4(N(i, j, k), N(i, j + 1, k), N(i + 1, j, k), N(i + 1, j + 1, k));
+                        R t = R(1.0) - f;
+                        weight[d](i, j, k) = t < 0 ? R(0) : (t > R(1.0) ? R(1.0) : t);
+                    }
+        }
+    }
+    R faceWeight(int d, int i, int j, int k) const { return gridBoundary ? weight[d](i, j, k) : R(1.0); }
+
+    // ArrayHelpers::interpolateGradient 3D (ArrayHelpers.cpp:214-251)
+    static void interpGradient(const R pt[3], const Arr3<R>& a, R out[3]) {
+        int i, j, k; R fi, fj, fk;
+        get_barycentric(pt[0], i, fi, 0, a.sx);
+        get_barycentric(pt[1], j, fj, 0, a.sy);
+        get_barycentric(pt[2], k, fk, 0, a.sz);
+        R v000 = a(i, j, k), v001 = a(i, j, k + 1), v010 = a(i, j + 1, k), v011 = a(i, j + 1, k + 1);
+        R v100 = a(i + 1, j, k), v101 = a(i + 1, j, k + 1), v110 = a(i + 1, j + 1, k), v111 = a(i + 1, j + 1, k + 1);
+        out[0] = bilerp(v100 - v000, v110 - v010, v101 - v001, v111 - v011, fj, fk);
+        out[1] = bilerp(v010 - v000, v110 - v100, v011 - v001, v111 - v101, fi, fk);
+        out[2] = bilerp(v001 - v000, v101 - v100, v011 - v010, v111 - v110, fi, fj);
+    }
+
+    // PIC_Solver::constrainGridVelocity (PIC_Solver.cpp:1093-1115)
+    void constrainGridVelocity() {
+        for(int d = 0; d < 3; ++d) {
+            tmp[d].d = u[d].d;
+            for(int k = 0; k < u[d].sz; ++k)
+                for(int j = 0; j < u[d].sy; ++j)
+                    for(int i = 0; i < u[d].sx; ++i) {
+                        if(!(extrap[d](i, j, k) == 1 && weight[d](i, j, k) < std::numeric_limits<R>::min())) continue;
+                        R gp[3] = {(R)i + (d == 0 ? R(0) : R(0.5)), (R)j + (d == 1 ? R(0) : R(0.5)),
+                                   (R)k + (d == 2 ? R(0) : R(0.5))};
+                        R vel[3] = {velFromGrid(gp, 0, u), velFromGrid(gp, 1, u), velFromGrid(gp, 2, u)};
+                        R nrm[3];
+                        interpGradient(gp, nodeSdf, nrm);
+                        R m2 = length2(nrm[0], nrm[1], nrm[2]);
+                        if(m2 > std::numeric_limits<R>::min()) {
+                            R sq = std::sqrt(m2);
+                            nrm[0] /= sq; nrm[1] /= sq; nrm[2] /= sq;
+                            R dn = (vel[0] * nrm[0] + vel[1] * nrm[1]) + vel[2] * nrm[2];
+                            tmp[d](i, j, k) = vel[d] - dn * nrm[d];
+                        }
+                    }
+            u[d].d = tmp[d].d;
         }
     }
 
@@ -818,9 +1036,10 @@ public:
         }
     }
 
-    // PIC_Solver::extrapolateVelocity (PIC_Solver.cpp:985-1090); the `extrapolates` flags
-    // only feed constrainGridVelocity, a no-op for static boundaries, and are not kept.
-    void extrapolate(Arr3<R>& grid, Arr3<R>& temp, Arr3<char>& vld, Arr3<char>& ovld) {
+    // PIC_Solver::extrapolateVelocity (PIC_Solver.cpp:985-1090); `ext` marks the faces this
+    // call filled (the extrapolates flags constrainGridVelocity reads)
+    void extrapolate(Arr3<R>& grid, Arr3<R>& temp, Arr3<char>& vld, Arr3<char>& ovld, Arr3<char>& ext) {
+        ext.resize(grid.sx, grid.sy, grid.sz, 0);
         temp.d = grid.d;
         for(int layer = 0; layer < 4; ++layer) {
             ovld.d = vld.d;
@@ -836,12 +1055,12 @@ public:
                         if(ovld(i, j - 1, k)) { sum += grid(i, j - 1, k); ++count; }
                         if(ovld(i, j, k + 1)) { sum += grid(i, j, k + 1); ++count; }
                         if(ovld(i, j, k - 1)) { sum += grid(i, j, k - 1); ++count; }
-                        if(count > 0) { temp(i, j, k) = sum / static_cast<R>(count); vld(i, j, k) = 1; }
+                        if(count > 0) { temp(i, j, k) = sum / static_cast<R>(count); vld(i, j, k) = 1; ext(i, j, k) = 1; }
                     }
             grid.d = temp.d;
         }
     }
-    void extrapolateAll() { for(int d = 0; d < 3; ++d) extrapolate(u[d], tmp[d], valid[d], oldValid[d]); }
+    void extrapolateAll() { for(int d = 0; d < 3; ++d) extrapolate(u[d], tmp[d], valid[d], oldValid[d], extrap[d]); }
 
     // PIC_Solver::advectGridVelocity + trace_rk2_grid (PIC_Solver.cpp:489-501, 1148-1154):
     // semi-Lagrangian back-trace of every face through the grid velocity, RK2 in grid
@@ -912,6 +1131,18 @@ public:
         } else {
             for(size_t p = 0; p < pos.size(); ++p) body(p);
         }
+        if(!gridBoundary) return;
+        // solid part (PIC_Solver.cpp:671-688)
+        const R half = R(0.5) * dx;
+        for(int k = 0; k < G[2]; ++k)
+            for(int j = 0; j < G[1]; ++j)
+                for(int i = 0; i < G[0]; ++i) {
+                    if(!(phi(i, j, k) < half)) continue;
+                    const Arr3<R>& N = nodeSdf;
+                    R solid = R(0.125) * (N(i, j, k) + N(i + 1, j, k) + N(i, j + 1, k) + N(i + 1, j + 1, k) +
+                                          N(i, j, k + 1) + N(i + 1, j, k + 1) + N(i, j + 1, k + 1) + N(i + 1, j + 1, k + 1));
+                    if(solid < 0) phi(i, j, k) = -half;
+                }
     }
 
     // PIC_Solver::computeSystem (PIC_Solver.cpp:693-893) with static-scene weights = 1.
@@ -942,12 +1173,15 @@ public:
                     R pr = phi(i + 1, j, k), pl = phi(i - 1, j, k), pt = phi(i, j + 1, k), pb = phi(i, j - 1, k);
                     R pf = phi(i, j, k + 1), pn = phi(i, j, k - 1);
                     R rv = 0;
-                    R term_right = wgt * dt; rv -= wgt * U(i + 1, j, k);
-                    R term_left = wgt * dt;  rv += wgt * U(i, j, k);
-                    R term_top = wgt * dt;   rv -= wgt * V(i, j + 1, k);
-                    R term_bottom = wgt * dt; rv += wgt * V(i, j, k);
-                    R term_far = wgt * dt;   rv -= wgt * W(i, j, k + 1);
-                    R term_near = wgt * dt;  rv += wgt * W(i, j, k);
+                    const R wr = gridBoundary ? weight[0](i + 1, j, k) : wgt, wl = gridBoundary ? weight[0](i, j, k) : wgt;
+                    const R wt = gridBoundary ? weight[1](i, j + 1, k) : wgt, wb = gridBoundary ? weight[1](i, j, k) : wgt;
+                    const R wf = gridBoundary ? weight[2](i, j, k + 1) : wgt, wn = gridBoundary ? weight[2](i, j, k) : wgt;
+                    R term_right = wr * dt; rv -= wr * U(i + 1, j, k);
+                    R term_left = wl * dt;  rv += wl * U(i, j, k);
+                    R term_top = wt * dt;   rv -= wt * V(i, j + 1, k);
+                    R term_bottom = wb * dt; rv += wb * V(i, j, k);
+                    R term_far = wf * dt;   rv -= wf * W(i, j, k + 1);
+                    R term_near = wn * dt;  rv += wn * W(i, j, k);
                     uint32_t c = activeIdx(i, j, k);
                     rhs[c] = rv;
                     R center = 0;
@@ -1017,15 +1251,15 @@ public:
                     R prl = pl < 0 ? pressure[activeIdx(i - 1, j, k)] : R(0);
                     R prb = pb < 0 ? pressure[activeIdx(i, j - 1, k)] : R(0);
                     R prn = pn < 0 ? pressure[activeIdx(i, j, k - 1)] : R(0);
-                    if(i > 0 && (pc < 0 || pl < 0)) {
+                    if(i > 0 && (pc < 0 || pl < 0) && faceWeight(0, i, j, k) > 0) {
                         R th = smax(R(0.01), fraction_inside(pl, pc));
                         u[0](i, j, k) -= dt * (prc - prl) / th; valid[0](i, j, k) = 1;
                     }
-                    if(j > 0 && (pc < 0 || pb < 0)) {
+                    if(j > 0 && (pc < 0 || pb < 0) && faceWeight(1, i, j, k) > 0) {
                         R th = smax(R(0.01), fraction_inside(pb, pc));
                         u[1](i, j, k) -= dt * (prc - prb) / th; valid[1](i, j, k) = 1;
                     }
-                    if(k > 0 && (pc < 0 || pn < 0)) {
+                    if(k > 0 && (pc < 0 || pn < 0) && faceWeight(2, i, j, k) > 0) {
                         R th = smax(R(0.01), fraction_inside(pn, pc));
                         u[2](i, j, k) -= dt * (prc - prn) / th; valid[2](i, j, k) = 1;
                     }
@@ -1126,7 +1360,10 @@ public:
         if(kind == 3) advectGrid(substep);
         else mapP2G();
         double t3 = now();
-        if(kind != 1 && kind != 3) extrapolateAll(); // APIC goes straight to gravity (APIC_Solver.cpp:42-49)
+        if(kind != 1 && kind != 3) {
+            extrapolateAll(); // APIC goes straight to gravity (APIC_Solver.cpp:42-49)
+            if(gridBoundary) constrainGridVelocity();  // FLIP_Solver.cpp:46
+        }
         if(kind == 0 || kind == 2) for(int d = 0; d < 3; ++d) old[d].d = u[d].d;   // backupGridVelocity
         double t4 = now();
         addGravity(substep);
@@ -1138,6 +1375,7 @@ public:
         double t7 = now();
         updateVelocity(substep);
         extrapolateAll();
+        if(gridBoundary) constrainGridVelocity();
         double t8 = now();
         if(kind == 0 || kind == 2)
             for(int d = 0; d < 3; ++d)
@@ -1286,6 +1524,16 @@ template<class R, class T> static int get_grid(FlipOracle<R>& o, int which, T* o
         for(size_t i = 0; i < o.phi.size(); ++i) out[i] = o.phi.d[i] < 0 ? (T)(o.activeIdx.d[i] + 1) : (T)0;
         return 0;
     }
+    if(which >= 9 && which < 12) {
+        const int d = which - 9;
+        for(size_t i = 0; i < o.u[d].size(); ++i) out[i] = o.gridBoundary ? (T)o.weight[d].d[i] : (T)1;
+        return 0;
+    }
+    if(which == 12) {
+        const size_t nn = (size_t)(o.G[0] + 1) * (o.G[1] + 1) * (o.G[2] + 1);
+        for(size_t i = 0; i < nn; ++i) out[i] = o.gridBoundary ? (T)o.nodeSdf.d[i] : (T)0;
+        return 0;
+    }
     return -1;
 }
 extern "C" {
@@ -1303,6 +1551,13 @@ int orc_set_grid(void* hp, int which, const float* in) {
     if(which < 0 || which > 2) return -1;
     if(h->dbl) { auto& a = h->d->u[which]; for(size_t i = 0; i < a.size(); ++i) a.d[i] = in[i]; }
     else { auto& a = h->f->u[which]; for(size_t i = 0; i < a.size(); ++i) a.d[i] = in[i]; }
+    return 0;
+}
+
+// Boundary objects besides the domain box (bnn_flip_set_boundaries semantics)
+int orc_set_boundaries(void* hp, const orc_boundary_object* objs, uint32_t n) {
+    auto* h = (orc_handle*)hp;
+    if(h->dbl) h->d->setBoundaries(objs, n); else h->f->setBoundaries(objs, n);
     return 0;
 }
 

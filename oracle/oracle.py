@@ -99,6 +99,7 @@ def lib() -> C.CDLL:
         L.orc_grid_ncells.argtypes = [fp, fp, C.c_float, i32p]; L.orc_grid_ncells.restype = None
         L.orc_interp_face.argtypes = [vp, C.c_int, C.c_double, C.c_double, C.c_double]
         L.orc_interp_face.restype = C.c_double
+        L.orc_set_boundaries.argtypes = [vp, vp, C.c_uint32]; L.orc_set_boundaries.restype = C.c_int
         L.orc_aniso_kernels.argtypes = [fp, C.c_uint32, fp, C.c_float, i32p, C.c_float, C.c_float, C.c_float,
                                         C.c_float, C.c_float, C.c_uint32, fp, fp]
         L.orc_aniso_kernels.restype = C.c_uint32
@@ -200,6 +201,10 @@ class Oracle:
             shape = self.face_shape(which)
         elif which in (5, 6, 7):
             shape = self.face_shape(which - 5)
+        elif which in (9, 10, 11):
+            shape = self.face_shape(which - 9)
+        elif which == 12:
+            shape = tuple(g + 1 for g in self.G)
         else:
             shape = self.G
         n = int(np.prod(shape))
@@ -218,6 +223,14 @@ class Oracle:
     def interp_face(self, d: int, gx: float, gy: float, gz: float) -> float:
         """velocity component d sampled at grid coordinates (PIC_Solver::getVelocityFromGrid)"""
         return self.L.orc_interp_face(self.h, d, gx, gy, gz)
+
+    def set_boundaries(self, objs) -> None:
+        """Boundary objects (ctypes structures with the bnn_boundary_object layout)"""
+        if not objs:
+            lib().orc_set_boundaries(self.h, None, 0)
+            return
+        arr = (type(objs[0]) * len(objs))(*objs)
+        lib().orc_set_boundaries(self.h, C.cast(arr, C.c_void_p), len(objs))
 
     def step(self) -> dict:
         st = OrcStepStats()

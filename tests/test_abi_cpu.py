@@ -41,7 +41,8 @@ def test_struct_layouts_match_binding(tmp_path):
     src = tmp_path / "layout.c"
     fields = {"bnn_params": capi.Params, "bnn_step_stats": capi.StepStats, "bnn_pcg_stats": capi.PcgStats,
               "bnn_batch_params": capi.BatchParams, "bnn_batch_stats": capi.BatchStats,
-              "bnn_aniso_params": capi.AnisoParams, "bnn_aniso_stats": capi.AnisoStats}
+              "bnn_aniso_params": capi.AnisoParams, "bnn_aniso_stats": capi.AnisoStats,
+              "bnn_boundary_object": capi.BoundaryObject}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "banana_b200.h"', "int main(void) {"]
     for cname, py in fields.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
@@ -83,6 +84,7 @@ def test_validation_needs_no_gpu(lib):
     assert lib.bnn_anisotropic_kernels(None, 0, C.byref(bad), None, None, None, None) == \
         capi.STATUS_CODE["INVALID_ARGUMENT"]
     assert lib.bnn_flip_anisotropic_kernels(None, None, None, None, None) == capi.STATUS_CODE["INVALID_ARGUMENT"]
+    assert lib.bnn_flip_set_boundaries(None, None, 0) == capi.STATUS_CODE["INVALID_ARGUMENT"]
 
 
 def test_missing_library_fails_loudly(monkeypatch, tmp_path):
