@@ -178,7 +178,7 @@ def load() -> C.CDLL:
     L.bnn_batch_scene_info.argtypes = [vp, C.c_uint32, u32p, u64p, C.POINTER(StepStats)]
     L.bnn_batch_get_scene.argtypes = [vp, C.c_uint32, fp, fp]
     L.bnn_batch_memory.argtypes = [vp, u64p, u64p]
-    L.bnn_flip_set_boundaries.argtypes = [vp, C.POINTER(BoundaryObject), C.c_uint32]
+    L.bnn_flip_set_boundaries.argtypes = [vp, C.POINTER(BoundaryObject), C.c_uint32, C.c_int32]
     L.bnn_aniso_default_params.argtypes = [C.c_float, C.POINTER(AnisoParams)]
     L.bnn_anisotropic_kernels.argtypes = [vp, C.c_uint32, C.POINTER(AnisoParams), vp, vp, C.POINTER(AnisoStats), vp]
     L.bnn_flip_anisotropic_kernels.argtypes = [vp, C.POINTER(AnisoParams), fp, fp, C.POINTER(AnisoStats)]
@@ -339,10 +339,11 @@ class FlipSolver:
         check(self.L.bnn_flip_advance_frame(self.h, C.byref(k)), "bnn_flip_advance_frame")
         return k.value
 
-    def set_boundaries(self, objs) -> None:
+    def set_boundaries(self, objs, update_grid: bool = True) -> None:
         """Boundary objects besides the domain box (bnn_flip_set_boundaries)"""
         arr = (BoundaryObject * max(len(objs), 1))(*objs)
-        check(self.L.bnn_flip_set_boundaries(self.h, arr, len(objs)), "bnn_flip_set_boundaries")
+        check(self.L.bnn_flip_set_boundaries(self.h, arr, len(objs), 1 if update_grid else 0),
+              "bnn_flip_set_boundaries")
 
     def anisotropic_kernels(self, params: dict | None = None):
         """Kernel centres (n x 3) and matrices (n x 9, column-major) of the current

@@ -468,8 +468,10 @@ extern "C" int bnn_flip_get_grid(bnn_flip* h, int32_t field, float* out, size_t 
 // ParticleSolver::generateBoundaries (ParticleSolver.cpp:242-295) for the domain box plus
 // the given objects: the domain box (ParticleSolver.cpp:76-82, untransformed) and the
 // static objects form one CSG union, each dynamic object stays on its own.  With a
-// dynamic object the node SDF and face weights are recomputed now.
-extern "C" int bnn_flip_set_boundaries(bnn_flip* h, const bnn_boundary_object* objs, uint32_t n) {
+// dynamic object and update_grid the node SDF and face weights are recomputed now; they
+// then stay until the next update, like the reference's boundarySDF array.
+extern "C" int bnn_flip_set_boundaries(bnn_flip* h, const bnn_boundary_object* objs, uint32_t n,
+                                       int32_t update_grid) {
     if(!h || (n && !objs) || n >= (uint32_t)kMaxBoundaryObjects) return BNN_ERR_INVALID_ARGUMENT;
     std::vector<BObj> list;
     BObj box{};
@@ -506,8 +508,9 @@ extern "C" int bnn_flip_set_boundaries(bnn_flip* h, const bnn_boundary_object* o
         h->g.nObj = (int)list.size();
         h->g.nStatic = (int)nStatic;
     }
-    h->gridBoundary = anyDynamic;
-    if(anyDynamic) {
+    if(n == 0) h->gridBoundary = false;
+    if(anyDynamic && update_grid) {
+        h->gridBoundary = true;
         const size_t nn = (size_t)(h->g.G[0] + 1) * (h->g.G[1] + 1) * (h->g.G[2] + 1);
         if(!h->nodeSdf) BNN_CUDA_CHECK(cudaMalloc(&h->nodeSdf, nn * sizeof(float)));
         for(int d = 0; d < 3; ++d)

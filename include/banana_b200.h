@@ -269,13 +269,15 @@ typedef struct bnn_boundary_object {
 
 /* Sets the boundary objects besides the domain box (at most 15).  As in the reference,
  * the static ones are united with the domain box into one CSG object and the dynamic
- * ones stay separate; particles are projected out of every one after each advection.
- * When at least one object is dynamic the grid's boundary SDF is recomputed from the
- * objects as given (PIC_Solver::advanceScene + computeBoundarySDF, PIC_Solver.cpp:
- * 70-118,1157-1168) and the solve uses the face weights, the solid part of the fluid SDF
- * and constrainGridVelocity; call it again with the new transformations at the start
- * of every frame in which an object moves.  n = 0 restores the plain domain box. */
-int bnn_flip_set_boundaries(bnn_flip* h, const bnn_boundary_object* objs, uint32_t n);
+ * ones stay separate; particles are projected back inside every one after each
+ * advection.  update_grid != 0 with at least one dynamic object recomputes the grid's
+ * boundary SDF from the objects as given (PIC_Solver::advanceScene + computeBoundarySDF,
+ * PIC_Solver.cpp:70-118,1157-1168); from then on the solve uses the face weights, the
+ * solid part of the fluid SDF and constrainGridVelocity.  The reference moves dynamic
+ * objects before every sub-step after the first frame: call this then with their new
+ * transformations and update_grid = 1.  Until a first update the boundary SDF is 0
+ * everywhere (weights 1), as in the reference.  n = 0 restores the plain domain box. */
+int bnn_flip_set_boundaries(bnn_flip* h, const bnn_boundary_object* objs, uint32_t n, int32_t update_grid);
 
 /* ---- anisotropic kernels (surface reconstruction output) -------------------------- */
 

@@ -738,11 +738,11 @@ public:
 
     // ParticleSolver::generateBoundaries (ParticleSolver.cpp:242-295) + computeBoundarySDF
     // (PIC_Solver.cpp:1157-1168) + computeCellWeights (PIC_Solver.cpp:543-598)
-    void setBoundaries(const orc_boundary_object* in, uint32_t n) {
+    void setBoundaries(const orc_boundary_object* in, uint32_t n, bool updateGrid) {
         objs.clear();
-        gridBoundary = false;
         nStatic = 0;
-        if(n == 0) return;
+        if(n == 0) { gridBoundary = false; return; }
+        bool anyDynamic = false;
         OObj<R> box;
         for(int d = 0; d < 3; ++d) { box.bmin[d] = boxMin[d]; box.bmax[d] = boxMax[d]; }
         objs.push_back(box);
@@ -756,11 +756,12 @@ public:
                 for(int d = 0; d < 3; ++d) { o.bmin[d] = (R)in[i].box_min[d]; o.bmax[d] = (R)in[i].box_max[d]; }
                 for(int q = 0; q < 12; ++q) o.M[q] = (R)in[i].inv_transform[q];
                 objs.push_back(o);
-                if(pass == 1) gridBoundary = true;
+                if(pass == 1) anyDynamic = true;
             }
         nStatic = 1;
         for(uint32_t i = 0; i < n; ++i) nStatic += in[i].dynamic ? 0 : 1;
-        if(!gridBoundary) return;
+        if(!(anyDynamic && updateGrid)) return;
+        gridBoundary = true;
         nodeSdf.resize(G[0] + 1, G[1] + 1, G[2] + 1, 0);
         for(int k = 0; k <= G[2]; ++k)
             for(int j = 0; j <= G[1]; ++j)
@@ -1555,9 +1556,9 @@ int orc_set_grid(void* hp, int which, const float* in) {
 }
 
 // Boundary objects besides the domain box (bnn_flip_set_boundaries semantics)
-int orc_set_boundaries(void* hp, const orc_boundary_object* objs, uint32_t n) {
+int orc_set_boundaries(void* hp, const orc_boundary_object* objs, uint32_t n, int updateGrid) {
     auto* h = (orc_handle*)hp;
-    if(h->dbl) h->d->setBoundaries(objs, n); else h->f->setBoundaries(objs, n);
+    if(h->dbl) h->d->setBoundaries(objs, n, updateGrid != 0); else h->f->setBoundaries(objs, n, updateGrid != 0);
     return 0;
 }
 

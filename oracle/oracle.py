@@ -99,7 +99,7 @@ def lib() -> C.CDLL:
         L.orc_grid_ncells.argtypes = [fp, fp, C.c_float, i32p]; L.orc_grid_ncells.restype = None
         L.orc_interp_face.argtypes = [vp, C.c_int, C.c_double, C.c_double, C.c_double]
         L.orc_interp_face.restype = C.c_double
-        L.orc_set_boundaries.argtypes = [vp, vp, C.c_uint32]; L.orc_set_boundaries.restype = C.c_int
+        L.orc_set_boundaries.argtypes = [vp, vp, C.c_uint32, C.c_int]; L.orc_set_boundaries.restype = C.c_int
         L.orc_aniso_kernels.argtypes = [fp, C.c_uint32, fp, C.c_float, i32p, C.c_float, C.c_float, C.c_float,
                                         C.c_float, C.c_float, C.c_uint32, fp, fp]
         L.orc_aniso_kernels.restype = C.c_uint32
@@ -224,13 +224,13 @@ class Oracle:
         """velocity component d sampled at grid coordinates (PIC_Solver::getVelocityFromGrid)"""
         return self.L.orc_interp_face(self.h, d, gx, gy, gz)
 
-    def set_boundaries(self, objs) -> None:
+    def set_boundaries(self, objs, update_grid: bool = True) -> None:
         """Boundary objects (ctypes structures with the bnn_boundary_object layout)"""
         if not objs:
-            lib().orc_set_boundaries(self.h, None, 0)
+            lib().orc_set_boundaries(self.h, None, 0, 0)
             return
         arr = (type(objs[0]) * len(objs))(*objs)
-        lib().orc_set_boundaries(self.h, C.cast(arr, C.c_void_p), len(objs))
+        lib().orc_set_boundaries(self.h, C.cast(arr, C.c_void_p), len(objs), 1 if update_grid else 0)
 
     def step(self) -> dict:
         st = OrcStepStats()

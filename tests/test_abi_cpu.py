@@ -84,7 +84,7 @@ def test_validation_needs_no_gpu(lib):
     assert lib.bnn_anisotropic_kernels(None, 0, C.byref(bad), None, None, None, None) == \
         capi.STATUS_CODE["INVALID_ARGUMENT"]
     assert lib.bnn_flip_anisotropic_kernels(None, None, None, None, None) == capi.STATUS_CODE["INVALID_ARGUMENT"]
-    assert lib.bnn_flip_set_boundaries(None, None, 0) == capi.STATUS_CODE["INVALID_ARGUMENT"]
+    assert lib.bnn_flip_set_boundaries(None, None, 0, 1) == capi.STATUS_CODE["INVALID_ARGUMENT"]
 
 
 def test_missing_library_fails_loudly(monkeypatch, tmp_path):
