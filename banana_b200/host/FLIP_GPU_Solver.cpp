@@ -193,6 +193,12 @@ void FLIP_GPU_Solver::loadSceneFromString(const std::string& sceneJson, bool all
     }
     P.particleRadius = P.cellSize / P.ratioCellSizePRadius;
 
+    std::string err;
+    m_Boundaries = parse_boundary_objects(j, err);
+    if(!err.empty()) {
+        std::fprintf(stderr, "%s\n", err.c_str());
+        std::exit(EXIT_FAILURE);
+    }
     generateParticles(j);
     if(!allocate) return;
     allocateSolverMemory();
@@ -277,6 +283,16 @@ void FLIP_GPU_Solver::allocateSolverMemory() {
     const auto& D = m_ParticleData;
     check(bnn_flip_set_particles(m_Gpu, D.positions.data(), D.velocities.data(), D.getNParticles()),
           "bnn_flip_set_particles");
+    // the objects as built (their static transformation); the boundary SDF stays 0 until
+    // the scene first moves, as in the reference
+    if(!m_Boundaries.empty()) sendBoundaries(false);
+}
+
+void FLIP_GPU_Solver::sendBoundaries(bool updateGrid) {
+    std::vector<bnn_boundary_object> recs;
+    for(const auto& b : m_Boundaries) recs.push_back(b.current);
+    check(bnn_flip_set_boundaries(m_Gpu, recs.data(), (uint32_t)recs.size(), updateGrid ? 1 : 0),
+          "bnn_flip_set_boundaries");
 }
 
 // PIC_Solver::advanceFrame (PIC_Solver.cpp:267-311): sub-steps until FrameDuration; the
@@ -284,6 +300,16 @@ void FLIP_GPU_Solver::allocateSolverMemory() {
 void FLIP_GPU_Solver::advanceFrame() {
     FrameLog log;
     for(;;) {
+        // PIC_Solver::advanceFrame (PIC_Solver.cpp:280-282) + advanceScene (:70-118): after
+        // the first frame the dynamic objects move before every sub-step, and the boundary
+        // SDF is recomputed when one of them did
+        if(m_GlobalParams.finishedFrame > 0) {
+            bool changed = false;
+            const double fraction = (double)m_GlobalParams.frameLocalTime / (double)m_GlobalParams.frameDuration;
+            for(auto& b : m_Boundaries)
+                if(b.dynamic) changed |= b.update(m_GlobalParams.finishedFrame, fraction);
+            if(changed) sendBoundaries(true);
+        }
         bnn_step_stats st;
         const int rc = bnn_flip_step(m_Gpu, &st);
         check(rc, "bnn_flip_step");

@@ -15,6 +15,8 @@
 
 #include <banana_b200.h>
 
+#include "boundary_objects.h"
+
 #include <cstdint>
 #include <functional>
 #include <map>
@@ -156,6 +158,9 @@ protected:
     ParticleData m_ParticleData;
     bnn_flip* m_Gpu = nullptr;
     std::vector<FrameLog> m_Logs;
+    // "AdditionalBoundaryObjects" of the scene and their current transformations
+    std::vector<BoundaryObjectSpec> m_Boundaries;
+    void sendBoundaries(bool updateGrid);
     std::shared_ptr<void> m_FrameWriter;  // std::future of the frame file being written
 };
 

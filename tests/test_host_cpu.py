@@ -110,3 +110,116 @@ def test_bnn_file_format_round_trip(tmp_path):
     assert np.array_equal(kq.reshape(-1).astype(np.uint16),
                           np.trunc(np.float32(65535.0) * ((mats - klo) / (khi - klo))).astype(np.uint16))
     assert np.abs(K.reshape(-1) - mats).max() <= (khi - klo) / 65535 * 1.01
+
+
+ANIM_SELFTEST = r"""
+#include "boundary_objects.h"
+#include "json_lite.h"
+#include <cstdio>
+#include <fstream>
+#include <sstream>
+int main(int argc, char** argv) {
+    std::ifstream f(argv[1]);
+    std::stringstream ss;
+    ss << f.rdbuf();
+    const std::string text = ss.str();
+    bnnhost::Json j = bnnhost::JsonParser(text).parse();
+    std::string err;
+    auto objs = bnnhost::parse_boundary_objects(j, err);
+    if(!err.empty()) { std::printf("error %s\n", err.c_str()); return 0; }
+    auto dump = [&](const char* tag, double x) {
+        for(const auto& b : objs) {
+            std::printf("%s %.6f %d %d", tag, x, b.current.transformed, b.current.dynamic);
+            for(int q = 0; q < 12; ++q) std::printf(" %.9g", b.current.inv_transform[q]);
+            std::printf(" %.9g\n", b.current.uniform_scale);
+        }
+    };
+    dump("init", 0.0);
+    const double times[][2] = {{1, 0.0}, {1, 0.5}, {2, 0.25}, {4, 0.0}, {6, 0.75}, {9, 0.0}};
+    for(const auto& t : times) {
+        for(auto& b : objs) if(b.dynamic) b.update((unsigned)t[0], t[1]);
+        dump("t", t[0] + t[1]);
+    }
+    return 0;
+}
+"""
+
+
+def _inv_rows(T, axis, ang, s):
+    a = np.asarray(axis, np.float64)
+    R = np.eye(3)
+    if ang != 0.0:
+        a = a / np.linalg.norm(a)
+        K = np.array([[0, -a[2], a[1]], [a[2], 0, -a[0]], [-a[1], a[0], 0]])
+        R = np.cos(ang) * np.eye(3) + np.sin(ang) * K + (1 - np.cos(ang)) * np.outer(a, a)
+    M = np.eye(4)
+    M[:3, :3] = R * s
+    M[:3, 3] = T
+    return np.linalg.inv(M)[:3, :4].reshape(-1)
+
+
+def test_boundary_object_animation(tmp_path):
+    """Boundary-object transformations of the host scene reader: a static translated,
+    scaled sphere and a box rotating about x by linear keyframes (0 -> 180 -> 360 degrees
+    over frames 2..6, periodic from frame 2), checked against the same matrices built in
+    numpy; a translation animated by a clamped cubic spline against scipy's."""
+    import json
+    from scipy.interpolate import CubicSpline
+    scene = {"AdditionalBoundaryObjects": [
+        {"GeometryType": "Sphere", "Translation": [0.5, 0.4, 0.5], "Scale": 0.7},
+        {"GeometryType": "Box", "BoxMin": [-0.4, -0.2, -0.4], "BoxMax": [0.4, 0.2, 0.4],
+         "Translation": [0.5, 0.5, 0.5],
+         "Animation": {"Periodic": True, "StartFrame": 2, "CubicInterpolationRotation": False,
+                       "KeyFrames": [{"Frame": 2, "Translation": [0.5, 0.5, 0.5], "RotationAxisAngle": [1, 0, 0, 0]},
+                                     {"Frame": 4, "Translation": [0.5, 0.5, 0.5], "RotationAxisAngle": [1, 0, 0, 180]},
+                                     {"Frame": 6, "Translation": [0.5, 0.5, 0.5], "RotationAxisAngle": [1, 0, 0, 360]}]}},
+        {"GeometryType": "Sphere", "Scale": 0.6,
+         "Animation": {"KeyFrames": [{"Frame": 1, "Translation": [0.4, 0.5, 0.5]},
+                                     {"Frame": 3, "Translation": [0.6, 0.5, 0.5]},
+                                     {"Frame": 5, "Translation": [0.5, 0.45, 0.5]}]}}]}
+    (tmp_path / "s.json").write_text(json.dumps(scene))
+    src = tmp_path / "a.cpp"
+    src.write_text(ANIM_SELFTEST)
+    exe = tmp_path / "a"
+    host = bld.HOST
+    subprocess.run(["g++", "-O1", "-std=c++17", "-I", str(host), "-I", str(bld.INCLUDE), str(src),
+                    str(host / "boundary_objects.cpp"), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe), str(tmp_path / "s.json")], capture_output=True, text=True, check=True).stdout
+    rows = [l.split() for l in out.strip().splitlines()]
+    assert rows[0][0] == "init" and len(rows) == 3 * 7
+    got = {}
+    for r in rows:
+        got.setdefault(float(r[1]), []).append((int(r[2]), int(r[3]), np.array(r[4:16], float), float(r[16])))
+    # static sphere: the same record at every time
+    exp = _inv_rows([0.5, 0.4, 0.5], [0, 0, 1], 0.0, 0.7)
+    for t, recs in got.items():
+        assert recs[0][0] == 1 and recs[0][1] == 0
+        np.testing.assert_allclose(recs[0][2], exp, atol=1e-6)
+        assert abs(recs[0][3] - 0.7) < 1e-7
+    # rotating box: linear angle in frames 2..6, periodic afterwards, static before frame 2
+    def box_angle(t):
+        f, frac = int(t), t - int(t)
+        if f < 2:
+            return None
+        if f > 6:
+            f = (f - 2) % 4 + 2
+        return np.radians(90.0 * ((f + frac) - 2))
+    for t, recs in got.items():
+        tr, dyn, m, sc = recs[1]
+        assert dyn == 1
+        ang = box_angle(t) if t > 0 else None
+        if ang is None:
+            np.testing.assert_allclose(m, _inv_rows([0.5, 0.5, 0.5], [1, 0, 0], 0.0, 1.0), atol=1e-6)
+        else:
+            np.testing.assert_allclose(m, _inv_rows([0.5, 0.5, 0.5], [1, 0, 0], ang, 1.0), atol=2e-6)
+    # cubic translation and scale: keyframe 0 (the object's own: origin, Scale 0.6) and
+    # keyframes 1, 3, 5 (their Scale defaults to 1), zero end slopes
+    xs = [0, 1, 3, 5]
+    ys = np.array([[0, 0, 0], [0.4, 0.5, 0.5], [0.6, 0.5, 0.5], [0.5, 0.45, 0.5]])
+    cs = CubicSpline(xs, ys, bc_type="clamped")
+    css = CubicSpline(xs, [0.6, 1.0, 1.0, 1.0], bc_type="clamped")
+    for t, recs in got.items():
+        if t == 0 or t > 5:
+            continue
+        np.testing.assert_allclose(recs[2][2], _inv_rows(cs(t), [0, 0, 1], 0.0, float(css(t))), atol=2e-6)
+        assert abs(recs[2][3] - float(css(t))) < 1e-6
