@@ -62,7 +62,7 @@ class StepStats(C.Structure):
         ("dt", C.c_double), ("frame_time", C.c_double), ("frame_finished", C.c_uint32),
         ("pcg_iterations", C.c_uint32), ("pcg_residual", C.c_double), ("pcg_success", C.c_uint32),
         ("n_active", C.c_uint32), ("outer_iterations", C.c_uint32), ("zero_phi_cells", C.c_uint32),
-        ("stage_ms", C.c_float * 10), ("device_flags", C.c_uint32),
+        ("stage_ms", C.c_float * 10), ("device_flags", C.c_uint32), ("pcg_kernel_ms", C.c_float),
     ]
 
 

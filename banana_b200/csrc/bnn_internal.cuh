@@ -246,10 +246,12 @@ struct PcgWork {
     float* partMaxF = nullptr;
     double* partMaxD = nullptr;
     int4* rec = nullptr;  // packed grid rows
+    cudaEvent_t ev[2] = {nullptr, nullptr};  // around the persistent launch
 };
 struct PcgOutcome {
     unsigned iterations = 0, outer = 0, success = 0;
     double residual = 0;
+    float kernelMs = 0.f;  // device time of the persistent launches (all inner solves)
 };
 // gridRows: the x neighbours of every row are rows r-1 / r+1 (or none) and the y
 // neighbours lie within 65535 rows (rows of a grid in cell order, at most 65535 cells

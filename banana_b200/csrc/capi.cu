@@ -694,6 +694,7 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st, const HostIo* io = nullp
         st->pcg_success = po.success;
         st->n_active = nrows;
         st->outer_iterations = po.outer;
+        st->pcg_kernel_ms = po.kernelMs;
         st->zero_phi_cells = h->hst->zero_phi;
         st->device_flags = h->hst->flags;
         const int map[10][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 4}, {4, 5}, {5, 6}, {6, 7}, {7, 8}, {8, 9}, {0, 9}};

@@ -628,6 +628,8 @@ int pcg_reserve(PcgWork& w, int n, bool fp64) {
         BNN_CUDA_CHECK(cudaMalloc(&w.partMaxD, nch * sizeof(double)));
         w.cap = cap;
     }
+    for(auto& e : w.ev)
+        if(!e) BNN_CUDA_CHECK(cudaEventCreate(&e));
     if(fp64 && !w.x64) {
         BNN_CUDA_CHECK(cudaMalloc(&w.x64, w.cap * sizeof(double)));
         BNN_CUDA_CHECK(cudaMalloc(&w.r64, w.cap * sizeof(double)));
@@ -641,6 +643,8 @@ int pcg_reserve(PcgWork& w, int n, bool fp64) {
 }
 
 void pcg_release(PcgWork& w) {
+    for(auto& e : w.ev)
+        if(e) cudaEventDestroy(e);
     for(void* p : {(void*)w.rec, (void*)w.x, (void*)w.r, (void*)w.z, (void*)w.s0, (void*)w.s1, (void*)w.q, (void*)w.d32, (void*)w.r32,
                    (void*)w.part, (void*)w.partMaxF, (void*)w.partMaxD, (void*)w.x64, (void*)w.r64, (void*)w.z64,
                    (void*)w.s064, (void*)w.s164, (void*)w.q64, (void*)w.inv64, (void*)w.gs})
@@ -687,10 +691,16 @@ static int pcg_solve_t(PcgWork& w, int n, const float* rhsF, const float* diag, 
     // grids of concurrent solves (several solver handles on several host threads) must
     // fit the GPU together, or blocks of one could wait for SMs held by another's barrier
     CoopShare share(grid * (kShareUnits / perSMv), numSM * kShareUnits);
+    if(w.ev[0]) BNN_CUDA_CHECK(cudaEventRecord(w.ev[0], s));
     BNN_CUDA_CHECK(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kLanes), args, 0, s));
     bnn_note_launch();
+    if(w.ev[1]) BNN_CUDA_CHECK(cudaEventRecord(w.ev[1], s));
     BNN_CUDA_CHECK(cudaMemcpyAsync(hst, dst, sizeof(DevState), cudaMemcpyDeviceToHost, s));
     BNN_CUDA_CHECK(cudaStreamSynchronize(s));
+    if(w.ev[0] && w.ev[1]) {
+        float ms = 0.f;
+        if(cudaEventElapsedTime(&ms, w.ev[0], w.ev[1]) == cudaSuccess) out.kernelMs = ms;
+    }
     if(hst->flags & BNN_FLAG_TIMEOUT) { bnn_set_error("PCG grid barrier timed out"); return BNN_ERR_TIMEOUT; }
     out.iterations = hst->iter;
     out.success = hst->success;
@@ -739,6 +749,7 @@ int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const floa
     BNN_CUDA_CHECK(cudaStreamSynchronize(s));
     const double bmax = hst->outer_bmax;
     unsigned total = 0, outer = 0;
+    float kernelMs = 0.f;
     const unsigned maxOuter = 60;
     double res = bmax;
     bool ok = bmax < (double)FLT_MIN;
@@ -750,6 +761,7 @@ int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const floa
                                 w.s1, w.q, w.partMaxF, dst, hst, s, inner);
         if(rc != BNN_OK) return rc;
         total += inner.iterations;
+        kernelMs += inner.kernelMs;
         { k_ir_accumulate<<<nb, 256, 0, s>>>(n, w.x64, w.d32); bnn_note_launch(); }
         { k_ir_residual<<<nch, kLanes, 0, s>>>(n, rhs, w.x64, w.r64, diag, nbr, coef, (double)(-(1.0f * dt)), w.partMaxD, dst); bnn_note_launch(); }
         BNN_CUDA_CHECK(cudaMemcpyAsync(hst, dst, sizeof(DevState), cudaMemcpyDeviceToHost, s));
@@ -761,6 +773,7 @@ int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const floa
     if(!ok && res < (double)outerTol * bmax) ok = true;
     out.iterations = total;
     out.outer = outer;
+    out.kernelMs = kernelMs;
     out.residual = res;
     out.success = ok ? 1 : 0;
     { k_d64_to_f32<<<nb, 256, 0, s>>>(n, w.x64, pressure); bnn_note_launch(); }

@@ -250,7 +250,10 @@ def run_ours(args, ws, rank, local):
     rows = [s["n_active"] for s in stats]
     pcg_bytes = sum(52.0 * s["n_active"] * s["pcg_iterations"] for s in stats)
     peak, peak_kind = _peaks()
-    pcg_ms = stage_tot["pcg"]
+    # the persistent launch alone (CUDA events around it on the solver's stream); the pcg
+    # stage also holds the row packing and the host's read of the solve's outcome
+    pcg_kernel_ms = sum(s["pcg_kernel_ms"] for s in stats)
+    pcg_ms = pcg_kernel_ms if pcg_kernel_ms > 0 else stage_tot["pcg"]
     achieved = pcg_bytes / (pcg_ms * 1e-3) / 1e9 if pcg_ms > 0 else 0.0
     F = 3 * (N_GRID + 5) * (N_GRID + 4) ** 2
     C = (N_GRID + 4) ** 3
@@ -308,6 +311,7 @@ def run_ours(args, ws, rank, local):
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clk,
             "detail": {"pcg_iterations_per_step": iters / args.steps, "active_rows_mean": float(np.mean(rows)),
+                       "pcg_kernel_ms_per_step": pcg_kernel_ms / args.steps,
                        "stage_ms_per_step": {k: v / args.steps for k, v in stage_tot.items()},
                        "stage_gbs": stage_gbs},
         }

@@ -114,6 +114,7 @@ typedef struct bnn_step_stats {
     float    stage_ms[10];
     uint32_t device_flags;     /* bit 0: particle outside the grid, bit 1: fluid in the
                                   outer cell ring, bit 2: PCG hit MaxCGIteration */
+    float    pcg_kernel_ms;    /* device time of the persistent PCG launch(es) alone */
 } bnn_step_stats;
 
 typedef struct bnn_flip bnn_flip;
