@@ -213,6 +213,7 @@ struct DevState {
     unsigned pad0;
     double outer_res, outer_bmax;
     int bbox[6];            // min x,y,z and max x,y,z of the particles' (clamped) cells
+    unsigned nlarge;        // cells with more than 16 particles, listed for k_sort_large
 };
 
 #define BNN_FLAG_OUT_OF_GRID   1u
@@ -246,6 +247,7 @@ struct PcgWork {
     float* partMaxF = nullptr;
     double* partMaxD = nullptr;
     int4* rec = nullptr;  // packed grid rows
+    float4* coefRow = nullptr;  // packed rows' off-diagonal values (2 per row)
     cudaEvent_t ev[2] = {nullptr, nullptr};  // around the persistent launch
 };
 struct PcgOutcome {
@@ -256,8 +258,8 @@ struct PcgOutcome {
 // gridRows: the x neighbours of every row are rows r-1 / r+1 (or none) and the y
 // neighbours lie within 65535 rows (rows of a grid in cell order, at most 65535 cells
 // along x); the solve then reads the packed 16-byte row records.
-// coef (optional, compact rows only): six planes of off-diagonal values in the order of
-// nbr (face weights != 1); without it every off-diagonal is -dt.
+// coef (optional): six planes of off-diagonal values in the order of nbr (face weights
+// != 1); without it every off-diagonal is -dt.
 int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const float* invd, const int32_t* nbr,
               const float* coef, bool gridRows, float dt, int mode, float tol, unsigned maxIter, float innerTol,
               float outerTol, float* pressure, double* x64out, DevState* dst, DevState* hst, cudaStream_t s,

@@ -27,11 +27,10 @@ void launch_advect(int n, float* p6, size_t stride, const float* const* U, const
                    uint32_t* cellOf, uint32_t* slot, uint32_t* count, DevState* st, int* bboxPart, cudaStream_t s);
 void launch_cell_histogram(int n, const float* p6, size_t stride, const GridDesc& g, uint32_t* cellOf, uint32_t* slot,
                            uint32_t* count, DevState* st, cudaStream_t s);
-void launch_sort_finish(int n, size_t ncells, const uint32_t* cellOf, const uint32_t* slot, const uint32_t* cellStart,
+void launch_sort_finish(int n, size_t ncells, uint32_t* cellOf, uint32_t* slot, const uint32_t* cellStart,
                         uint32_t* order, uint32_t* count, const float* src6, float* dst6, const uint32_t* idSrc,
                         uint32_t* idDst, const float* cSrc, float* cDst, float* g3, float4* rec, const GridDesc& g,
-                        size_t stride,
-                        cudaStream_t s);
+                        size_t stride, DevState* st, cudaStream_t s);
 void launch_p2g(const GridDesc& g, const uint32_t* cellStart, const float* g3, const float* p6, const float* C9,
                 const float4* rec, size_t stride, float* const* out, uint8_t* const* valid, bool affine,
                 const DevState* st, cudaStream_t s);
@@ -568,7 +567,7 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st, const HostIo* io = nullp
     const int nxt = 1 - h->cur;
     launch_sort_finish(n, h->C, h->cellOf, h->slot, h->cellStart, h->order, h->count, h->p6[h->cur], h->p6[nxt],
                        h->ids[h->cur], h->ids[nxt], affine ? h->C9[h->cur] : nullptr, affine ? h->C9[nxt] : nullptr,
-                       h->g3, h->rec, g, h->cap, s);
+                       h->g3, h->rec, g, h->cap, h->dst, s);
     h->cur = nxt;
     if(h->P.correct_position && n > 0) {
         // PIC_Solver::advanceFrame: correctParticlePositions right after moveParticles
@@ -587,7 +586,7 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st, const HostIo* io = nullp
         const int nxt2 = 1 - h->cur;
         launch_sort_finish(n, h->C, h->cellOf, h->slot, h->cellStart, h->order, h->count, h->p6[h->cur], h->p6[nxt2],
                            h->ids[h->cur], h->ids[nxt2], affine ? h->C9[h->cur] : nullptr,
-                           affine ? h->C9[nxt2] : nullptr, h->g3, h->rec, g, h->cap, s);
+                           affine ? h->C9[nxt2] : nullptr, h->g3, h->rec, g, h->cap, h->dst, s);
         h->cur = nxt2;
     }
     cudaEventRecord(h->ev[2], s);
@@ -795,7 +794,7 @@ extern "C" int bnn_flip_anisotropic_kernels(bnn_flip* h, const bnn_aniso_params*
     const int nxt = 1 - h->cur;
     launch_sort_finish(n, h->C, h->cellOf, h->slot, h->cellStart, h->order, h->count, h->p6[h->cur], h->p6[nxt],
                        h->ids[h->cur], h->ids[nxt], affine ? h->C9[h->cur] : nullptr, affine ? h->C9[nxt] : nullptr,
-                       h->g3, h->rec, g, h->cap, s);
+                       h->g3, h->rec, g, h->cap, h->dst, s);
     h->cur = nxt;
     const size_t cap = h->cap;
     if(!h->aniso) BNN_CUDA_CHECK(cudaMalloc(&h->aniso, (12 * cap + 4) * sizeof(float)));

@@ -415,8 +415,11 @@ __device__ __forceinline__ void sort_bucket_regs(uint32_t* __restrict__ order, c
         if((uint32_t)q < cnt) order[b + q] = s[q];
 }
 
+// Buckets of up to 16 particles are sorted in registers; larger ones (particles crowding
+// into a cell, e.g. against a boundary) are listed for k_sort_large.
 __global__ void k_sort_buckets(int ncells, const uint32_t* __restrict__ cellStart, uint32_t* __restrict__ order,
-                               const uint32_t* __restrict__ ids, uint32_t* __restrict__ count) {
+                               const uint32_t* __restrict__ ids, uint32_t* __restrict__ count,
+                               uint32_t* __restrict__ largeList, DevState* st) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if(c >= ncells) return;
     const uint32_t b = cellStart[c], e = cellStart[c + 1];
@@ -425,12 +428,37 @@ __global__ void k_sort_buckets(int ncells, const uint32_t* __restrict__ cellStar
     if(cnt < 2) return;
     if(cnt <= 8) { sort_bucket_regs<8>(order, ids, b, cnt); return; }
     if(cnt <= 16) { sort_bucket_regs<16>(order, ids, b, cnt); return; }
-    for(uint32_t i = b + 1; i < e; ++i) {
-        const uint32_t src = order[i];
-        const uint32_t key = ids[src];
-        uint32_t j = i;
-        while(j > b && ids[order[j - 1]] > key) { order[j] = order[j - 1]; --j; }
-        order[j] = src;
+    largeList[atomicAdd(&st->nlarge, 1u)] = (uint32_t)c;
+}
+
+// One block per listed bucket: every particle's place is the number of particles of the
+// bucket with a smaller id (ids are distinct), counted against keys staged in shared
+// memory.  tmp[b, e) holds the bucket's unsorted order while it is rewritten.
+__global__ void __launch_bounds__(256) k_sort_large(const uint32_t* __restrict__ cellStart, uint32_t* __restrict__ order,
+                                                    const uint32_t* __restrict__ ids, uint32_t* __restrict__ tmp,
+                                                    const uint32_t* __restrict__ largeList, const DevState* st) {
+    __shared__ uint32_t sk[1024];
+    const unsigned nl = st->nlarge;
+    for(unsigned l = blockIdx.x; l < nl; l += gridDim.x) {
+        const uint32_t c = largeList[l];
+        const uint32_t b = cellStart[c], cnt = cellStart[c + 1] - b;
+        for(uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) tmp[b + i] = order[b + i];
+        __syncthreads();
+        for(uint32_t ib = 0; ib < cnt; ib += blockDim.x) {
+            const uint32_t i = ib + threadIdx.x;
+            const uint32_t v = i < cnt ? tmp[b + i] : 0u;
+            const uint32_t key = i < cnt ? ids[v] : 0u;
+            uint32_t rank = 0;
+            for(uint32_t jb = 0; jb < cnt; jb += 1024) {
+                const uint32_t m = min(1024u, cnt - jb);
+                __syncthreads();
+                for(uint32_t j = threadIdx.x; j < m; j += blockDim.x) sk[j] = ids[tmp[b + jb + j]];
+                __syncthreads();
+                for(uint32_t j = 0; j < m; ++j) rank += sk[j] < key ? 1u : 0u;
+            }
+            if(i < cnt) order[b + rank] = v;
+        }
+        __syncthreads();
     }
 }
 
@@ -1293,12 +1321,16 @@ void launch_cell_histogram(int n, const float* p6, size_t stride, const GridDesc
     if(n == 0) return;
     { k_cell_histogram<<<nblk(n), 256, 0, s>>>(n, p6, p6 + stride, p6 + 2 * stride, g, cellOf, slot, count, st); bnn_note_launch(); }
 }
-void launch_sort_finish(int n, size_t ncells, const uint32_t* cellOf, const uint32_t* slot, const uint32_t* cellStart,
+// cellOf and slot are free once the index is scattered: slot lists the crowded buckets,
+// cellOf holds their unsorted order while k_sort_large rewrites them
+void launch_sort_finish(int n, size_t ncells, uint32_t* cellOf, uint32_t* slot, const uint32_t* cellStart,
                         uint32_t* order, uint32_t* count, const float* src6, float* dst6, const uint32_t* idSrc,
                         uint32_t* idDst, const float* cSrc, float* cDst, float* g3, float4* rec, const GridDesc& g,
-                        size_t stride, cudaStream_t s) {
+                        size_t stride, DevState* st, cudaStream_t s) {
     if(n > 0) { k_scatter_index<<<nblk(n), 256, 0, s>>>(n, cellOf, slot, cellStart, order); bnn_note_launch(); }
-    { k_sort_buckets<<<nblk(ncells), 256, 0, s>>>((int)ncells, cellStart, order, idSrc, count); bnn_note_launch(); }
+    cudaMemsetAsync(&st->nlarge, 0, sizeof(unsigned), s);
+    { k_sort_buckets<<<nblk(ncells), 256, 0, s>>>((int)ncells, cellStart, order, idSrc, count, slot, st); bnn_note_launch(); }
+    if(n > 16) { k_sort_large<<<2 * 148, 256, 0, s>>>(cellStart, order, idSrc, cellOf, slot, st); bnn_note_launch(); }
     if(n > 0)
         { k_gather_particles<<<nblk(n), 256, 0, s>>>(n, order, src6, dst6, idSrc, idDst, cSrc, cDst, g3, rec, g, stride); bnn_note_launch(); }
 }

@@ -4,8 +4,9 @@
 // Rows are the fluid cells in linear-cell order.  Per row: diag (float), 1/diag, and six
 // neighbour row indices in ascending column order (-z,-y,-x,+x,+y,+z; -1 = none), stored
 // as six planes nbr[q*n + r].  With face weights 1 every off-diagonal equals -dt, so the
-// matrix is never materialised; with solid boundaries (weights below 1) six planes of
-// off-diagonal values coef[q*n + r] ride along with the compact rows.
+// matrix is never materialised; with solid boundaries (weights below 1) the off-diagonal
+// values ride along: six planes coef[q*n + r] with the compact rows, or two float4 per
+// row (k_pack_coef) with the packed ones.
 //
 // Rows of a grid (rows numbered in cell order) are also packed into one 16-byte record
 // each: the x neighbours are always rows r-1 / r+1, so they become two flag bits, the y
@@ -185,7 +186,8 @@ template<class VT> struct PcgArgs {
     const VT* invd;
     const int32_t* nbr;
     const int4* rec;
-    const float* coef;  // compact rows only: off-diagonal values (nullptr: all negoff)
+    const float* coef;  // compact rows: off-diagonal planes (nullptr: all negoff)
+    const float4* coefRow;  // packed rows with coefficients: 2 float4 per row (6 used)
     VT negoff;
     VT tolFactor;
     unsigned maxIter;
@@ -204,7 +206,7 @@ __device__ __forceinline__ VT s_val(const VT* z, const VT* sOld, VT beta, bool f
 #ifndef BNN_PCG_MIN_BLOCKS
 #define BNN_PCG_MIN_BLOCKS 4
 #endif
-template<class VT, bool PACKED>
+template<class VT, bool PACKED, bool COEF = false>
 __global__ void __launch_bounds__(kLanes, BNN_PCG_MIN_BLOCKS) k_pcg_persistent(PcgArgs<VT> a) {
     __shared__ double smd[kLanes];
     __shared__ VT smv[kLanes];
@@ -346,7 +348,18 @@ __global__ void __launch_bounds__(kLanes, BNN_PCG_MIN_BLOCKS) k_pcg_persistent(P
                         if(lane != 31) s7[4] = dn;
                     }
                     VT t = VT(0);
-                    if constexpr(PACKED) {
+                    if constexpr(PACKED && COEF) {
+                        // the row's off-diagonals in slot order (-z, -y, -x | +x, +y, +z)
+                        const size_t e = base + (size_t)(g0 + u) * kLanes;
+                        const size_t ee = e < (size_t)n ? e : 0;
+                        const float4 c0 = __ldg(a.coefRow + 2 * ee), c1 = __ldg(a.coefRow + 2 * ee + 1);
+                        const VT co[7] = {(VT)c0.x, (VT)c0.y, (VT)c0.z, VT(0), (VT)c0.w, (VT)c1.x, (VT)c1.y};
+#pragma unroll
+                        for(int q = 0; q < 3; ++q) if(has[u][q]) t += co[q] * s7[q];
+                        if(dg[u] != 0.f) t += (VT)dg[u] * s7[3];
+#pragma unroll
+                        for(int q = 4; q < 7; ++q) if(has[u][q]) t += co[q] * s7[q];
+                    } else if constexpr(PACKED) {
 #pragma unroll
                         for(int q = 0; q < 3; ++q) if(has[u][q]) t += negoff * s7[q];
                         if(dg[u] != 0.f) t += (VT)dg[u] * s7[3];
@@ -569,6 +582,16 @@ __global__ void k_pack_rows(int n, const float* __restrict__ diag, const int32_t
     v.w = __float_as_int(diag[r]);
     rec[r] = v;
 }
+// The off-diagonal planes of the rows as 2 float4 per row (6 values, plane order)
+__global__ void k_pack_coef(int n, const float* __restrict__ coef, float4* __restrict__ out) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if(r >= n) return;
+    float c[6];
+#pragma unroll
+    for(int q = 0; q < 6; ++q) c[q] = coef[(size_t)q * n + r];
+    out[2 * (size_t)r] = make_float4(c[0], c[1], c[2], c[3]);
+    out[2 * (size_t)r + 1] = make_float4(c[4], c[5], 0.f, 0.f);
+}
 
 // ---------------------------------------------------------------------------------
 // Host driver
@@ -582,7 +605,7 @@ struct CoopState {
     std::mutex mu;
     std::condition_variable cv;
     int numSM = 0;
-    int perSM[4] = {0, 0, 0, 0};
+    int perSM[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     long long held = 0;
 };
 static CoopState g_coop;
@@ -645,7 +668,7 @@ int pcg_reserve(PcgWork& w, int n, bool fp64) {
 void pcg_release(PcgWork& w) {
     for(auto& e : w.ev)
         if(e) cudaEventDestroy(e);
-    for(void* p : {(void*)w.rec, (void*)w.x, (void*)w.r, (void*)w.z, (void*)w.s0, (void*)w.s1, (void*)w.q, (void*)w.d32, (void*)w.r32,
+    for(void* p : {(void*)w.rec, (void*)w.coefRow, (void*)w.x, (void*)w.r, (void*)w.z, (void*)w.s0, (void*)w.s1, (void*)w.q, (void*)w.d32, (void*)w.r32,
                    (void*)w.part, (void*)w.partMaxF, (void*)w.partMaxD, (void*)w.x64, (void*)w.r64, (void*)w.z64,
                    (void*)w.s064, (void*)w.s164, (void*)w.q64, (void*)w.inv64, (void*)w.gs})
         if(p) cudaFree(p);
@@ -656,13 +679,15 @@ void pcg_release(PcgWork& w) {
 // the solution is left in x.
 template<class VT>
 static int pcg_solve_t(PcgWork& w, int n, const float* rhsF, const float* diag, const VT* invd, const int32_t* nbr,
-                       const int4* rec, const float* coef, VT negoff, VT tolFactor, unsigned maxIter, VT* x, VT* r, VT* z, VT* s0, VT* s1, VT* q,
+                       const int4* rec, const float* coef, const float4* coefRow, VT negoff, VT tolFactor, unsigned maxIter, VT* x, VT* r, VT* z, VT* s0, VT* s1, VT* q,
                        VT* partMax, DevState* dst, DevState* hst, cudaStream_t s, PcgOutcome& out) {
     out = PcgOutcome();
     if(n == 0) { out.success = 1; return BNN_OK; }
     const int nch = (n + kChunk - 1) / kChunk;
-    const int ti = (sizeof(VT) == 8 ? 1 : 0) + (rec ? 2 : 0);
-    const void* kern = rec ? (const void*)k_pcg_persistent<VT, true> : (const void*)k_pcg_persistent<VT, false>;
+    const bool packedCoef = rec && coefRow;
+    const int ti = (sizeof(VT) == 8 ? 1 : 0) + (rec ? 2 : 0) + (packedCoef ? 4 : 0);
+    const void* kern = packedCoef ? (const void*)k_pcg_persistent<VT, true, true>
+                                  : (rec ? (const void*)k_pcg_persistent<VT, true> : (const void*)k_pcg_persistent<VT, false>);
     int numSM = 0, perSMv = 0;
     {
         std::lock_guard<std::mutex> lk(g_coop.mu);
@@ -682,7 +707,7 @@ static int pcg_solve_t(PcgWork& w, int n, const float* rhsF, const float* diag, 
     const int perBlock = (nch + cap - 1) / cap;           // chunks per block
     const int grid = (nch + perBlock - 1) / perBlock;     // balanced: every block the same count
     PcgArgs<VT> a;
-    a.n = n; a.rhsF = rhsF; a.diag = diag; a.invd = invd; a.nbr = nbr; a.rec = rec; a.coef = coef; a.negoff = negoff; a.tolFactor = tolFactor;
+    a.n = n; a.rhsF = rhsF; a.diag = diag; a.invd = invd; a.nbr = nbr; a.rec = rec; a.coef = coef; a.coefRow = coefRow; a.negoff = negoff; a.tolFactor = tolFactor;
     a.maxIter = maxIter; a.x = x; a.r = r; a.z = z; a.s0 = s0; a.s1 = s1; a.q = q;
     a.part0 = w.part; a.part1 = w.part + w.nchCap; a.part2 = w.part + 2 * (size_t)w.nchCap; a.partMax = partMax;
     a.st = dst; a.gs = w.gs;
@@ -719,13 +744,19 @@ int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const floa
     const unsigned nch = (unsigned)((n + kChunk - 1) / kChunk);
     out = PcgOutcome();
     const int4* rec = nullptr;
-    if(coef) gridRows = false;  // the packed records carry no off-diagonal values
+    const float4* coefRow = nullptr;
     if(gridRows && n > 0) {
         { k_pack_rows<<<nb, 256, 0, s>>>(n, diag, nbr, w.rec); bnn_note_launch(); }
         rec = w.rec;
+        if(coef) {
+            // off-diagonal values ride along as 2 float4 per row
+            if(!w.coefRow) BNN_CUDA_CHECK(cudaMalloc(&w.coefRow, 2 * (size_t)w.cap * sizeof(float4)));
+            { k_pack_coef<<<nb, 256, 0, s>>>(n, coef, w.coefRow); bnn_note_launch(); }
+            coefRow = w.coefRow;
+        }
     }
     if(mode == BNN_PCG_FP32) {
-        rc = pcg_solve_t<float>(w, n, rhs, diag, invd, nbr, rec, coef, -(1.0f * dt), tol, maxIter, w.x, w.r, w.z, w.s0, w.s1,
+        rc = pcg_solve_t<float>(w, n, rhs, diag, invd, nbr, rec, coef, coefRow, -(1.0f * dt), tol, maxIter, w.x, w.r, w.z, w.s0, w.s1,
                                 w.q, w.partMaxF, dst, hst, s, out);
         if(rc != BNN_OK) return rc;
         if(n > 0) BNN_CUDA_CHECK(cudaMemcpyAsync(pressure, w.x, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
@@ -734,7 +765,7 @@ int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const floa
     }
     if(mode == BNN_PCG_FP64) {
         if(n > 0) { k_inv_diag64<<<nb, 256, 0, s>>>(n, diag, w.inv64); bnn_note_launch(); }
-        rc = pcg_solve_t<double>(w, n, rhs, diag, w.inv64, nbr, rec, coef, -(double)(1.0f * dt), (double)tol, maxIter, w.x64,
+        rc = pcg_solve_t<double>(w, n, rhs, diag, w.inv64, nbr, rec, coef, coefRow, -(double)(1.0f * dt), (double)tol, maxIter, w.x64,
                                  w.r64, w.z64, w.s064, w.s164, w.q64, w.partMaxD, dst, hst, s, out);
         if(rc != BNN_OK) return rc;
         if(n > 0) { k_d64_to_f32<<<nb, 256, 0, s>>>(n, w.x64, pressure); bnn_note_launch(); }
@@ -757,7 +788,7 @@ int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const floa
         if(res < (double)outerTol * bmax) { ok = true; break; }
         { k_ir_to_f32<<<nb, 256, 0, s>>>(n, w.r64, w.r32); bnn_note_launch(); }
         PcgOutcome inner;
-        rc = pcg_solve_t<float>(w, n, w.r32, diag, invd, nbr, rec, coef, -(1.0f * dt), innerTol, maxIter, w.d32, w.r, w.z, w.s0,
+        rc = pcg_solve_t<float>(w, n, w.r32, diag, invd, nbr, rec, coef, coefRow, -(1.0f * dt), innerTol, maxIter, w.d32, w.r, w.z, w.s0,
                                 w.s1, w.q, w.partMaxF, dst, hst, s, inner);
         if(rc != BNN_OK) return rc;
         total += inner.iterations;

@@ -23,6 +23,9 @@ Other workloads (`--workload`, one JSON line each, not the headline):
   pcg     standalone Jacobi PCG (bnn_pcg_solve_7pt) on the 102 x 153 x 102 box of fluid
           cells the 256^3 dam break starts with (1,591,812 rows), a fixed number of
           iterations (`--steps`); for profiling the solver alone.
+  boundary the 256^3 dam break in a box container that turns about z before every
+          sub-step (a dynamic boundary object: boundary SDF and face weights recomputed,
+          weighted pressure system with per-face off-diagonals, grid velocity constraint).
   aniso   anisotropic kernels (AnisotropicKernelGenerator, the "AniKernel" frame output)
           of the 256^3 dam break after one sub-step: particles/s of the kernel pass, and
           end to end through bnn_flip_anisotropic_kernels into host arrays.
@@ -598,6 +601,69 @@ def run_aniso(args, ws, rank, local):
     return 0
 
 
+def run_boundary(args, ws, rank, local):
+    """Dam break with a dynamic boundary object: a box container of half-size 0.55 about the
+    domain's centre turns about z by 0.2 degrees before every sub-step (update_grid each
+    time, in the timed region, as the reference recomputes the boundary SDF whenever a
+    dynamic object moved).  It cuts the domain's vertical edges, so the boundary SDF, the
+    face weights below 1 and the solid part of the fluid SDF all take part; the fluid starts
+    inside it."""
+    torch, dist = _torch_dist(ws, local)
+    from banana_b200 import capi, scenes
+
+    cfg = scenes.dam_break_params(N_GRID)
+    pos, vel = scenes.dam_break(N_GRID)
+    n = len(pos)
+    g = capi.FlipSolver(cfg)
+    g.set_particles(pos, vel)
+    stream = torch.cuda.ExternalStream(g.stream_ptr())
+
+    def box(k):
+        return capi.boundary_object("box", (-0.55, -0.55, -0.55), (0.55, 0.55, 0.55), translation=(0.5, 0.5, 0.5),
+                                    axis_angle=(0.0, 0.0, 1.0, np.radians(0.2 * k)), dynamic=True)
+
+    k = 0
+    for _ in range(args.warmup):
+        g.set_boundaries([box(k)])
+        g.step()
+        k += 1
+    torch.cuda.synchronize()
+    launches0 = capi.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    stats = []
+    for _ in range(args.steps):
+        g.set_boundaries([box(k)])
+        stats.append(g.step())
+        k += 1
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    launches = capi.launch_count() - launches0
+    if rank == 0:
+        pk = sum(s["pcg_kernel_ms"] for s in stats) / args.steps
+        it = sum(s["pcg_iterations"] for s in stats) / args.steps
+        rows = float(np.mean([s["n_active"] for s in stats]))
+        line = {"metric": f"particle-steps/s at {N_GRID}^3 FLIP with a turning box container", "value": n / (ms * 1e-3),
+                "unit": "particle-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms, "higher_is_better": True, "scaling": "replicas", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic (seeded dam break, seed 42)",
+                "config": {"workload": f"boundary_dam_break_{N_GRID}", "particles": n,
+                           "boundary": "box container of half-size 0.55 about (0.5, 0.5, 0.5) turning 0.2 deg "
+                                       "about z per sub-step"},
+                "detail": {"pcg_iterations_per_step": it, "active_rows_mean": rows, "pcg_kernel_ms_per_step": pk,
+                           "pcg_us_per_iteration": 1e3 * pk / it if it else None,
+                           "stage_ms_per_step": {key: sum(s["stage_ms"][key] for s in stats) / args.steps
+                                                 for key in capi.STAGES}},
+                "gpu_launches": int(launches)}
+        print(json.dumps(line), flush=True)
+    g.close()
+    if ws > 1:
+        dist.destroy_process_group()
+    return 0
+
+
 def _box_system(nx, ny, nz, seed=1):
     """7-point system on a full box of cells in cell order (the layout of a grid)."""
     n = nx * ny * nz
@@ -717,7 +783,7 @@ def main():
     ap.add_argument("--grid", type=int, default=N_GRID, help="fluid-domain resolution (profiling of smaller cases)")
     ap.add_argument("--ref-precond", choices=["jacobi", "ic0"], default="jacobi",
                     help="reference arm: Jacobi (the configs) or the reference's default symmetric MIC(0)")
-    ap.add_argument("--workload", choices=["flip", "batch", "serve", "nsearch", "pcg", "fp64err", "aniso"], default="flip")
+    ap.add_argument("--workload", choices=["flip", "batch", "serve", "nsearch", "pcg", "fp64err", "aniso", "boundary"], default="flip")
     ap.add_argument("--workers", type=int, default=0, help="batch/serve: host threads stepping scenes (0 = auto)")
     ap.add_argument("--requests", type=int, default=100, help="serve: number of requests")
     ap.add_argument("--req-steps", type=int, default=200, help="serve: sub-steps per request")
@@ -739,6 +805,8 @@ def main():
         return run_fp64err(args, ws, rank, local)
     if args.workload == "aniso":
         return run_aniso(args, ws, rank, local)
+    if args.workload == "boundary":
+        return run_boundary(args, ws, rank, local)
     return run_ours(args, ws, rank, local)
 
 

@@ -1,5 +1,6 @@
-"""Edge cases of the sub-step against the oracle: no particles, a single particle, and
-particles that start on or outside the domain box (the box projection brings them in).
+"""Edge cases of the sub-step against the oracle: no particles, a single particle,
+particles that start on or outside the domain box (the box projection brings them in),
+and cells crowded with hundreds of particles.
 Every particle and grid field must agree bit for bit after every sub-step."""
 import numpy as np
 import pytest
@@ -56,3 +57,15 @@ def test_particles_on_and_outside_the_box(bnn, oracle_mod):
     g = _run(bnn, oracle_mod, p, v, 4)
     pg, _ = g.get_particles()
     assert np.all(pg >= 0.0) and np.all(pg <= 1.0)
+
+
+def test_crowded_cells(bnn, oracle_mod):
+    """Hundreds of particles in a few cells (the cell sort's large-bucket path), among the
+    dam block"""
+    pos, vel = scenes.dam_break(16)
+    rng = np.random.default_rng(3)
+    pile = (np.array([0.71, 0.2, 0.63]) + rng.uniform(0, 0.02, size=(400, 3))).astype(np.float32)
+    pile2 = (np.array([0.3, 0.8, 0.8]) + rng.uniform(0, 0.05, size=(2500, 3))).astype(np.float32)
+    p = np.concatenate([pos, pile, pile2]).astype(np.float32)
+    v = np.concatenate([vel, np.zeros_like(pile), np.zeros_like(pile2)]).astype(np.float32)
+    _run(bnn, oracle_mod, p, v, 4)
