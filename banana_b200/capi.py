@@ -232,7 +232,7 @@ def make_params(cfg: dict) -> Params:
     p.pcg_mode = cfg.get("pcg_mode", 0)
     p.preconditioner = cfg.get("preconditioner", 0)
     p.refine_tolerance = cfg.get("refine_tolerance", 1e-8)
-    p.refine_inner_tolerance = cfg.get("refine_inner_tolerance", 1e-3)
+    p.refine_inner_tolerance = cfg.get("refine_inner_tolerance", 1e-2)
     p.apply_gravity = cfg.get("apply_gravity", 1)
     p.max_particles = cfg.get("max_particles", 0)
     p.correct_position = cfg.get("correct_position", 0)

@@ -206,8 +206,20 @@ __device__ __forceinline__ VT s_val(const VT* z, const VT* sOld, VT beta, bool f
 #ifndef BNN_PCG_MIN_BLOCKS
 #define BNN_PCG_MIN_BLOCKS 4
 #endif
+#ifndef BNN_PCG_MIN_BLOCKS_F64
+#define BNN_PCG_MIN_BLOCKS_F64 3
+#endif
+// resident blocks per SM the register budget is sized for: 4 for FP32 vectors; FP64 ones
+// and rows with off-diagonal values run faster at 3 (fewer spills: FP64 47.7 against
+// 53.6 us per iteration at 1.59M rows, rows with values 38.5 against 40.0)
+#ifndef BNN_PCG_MIN_BLOCKS_COEF
+#define BNN_PCG_MIN_BLOCKS_COEF 3
+#endif
+template<class VT, bool COEF> constexpr int pcg_min_blocks() {
+    return sizeof(VT) == 8 ? BNN_PCG_MIN_BLOCKS_F64 : (COEF ? BNN_PCG_MIN_BLOCKS_COEF : BNN_PCG_MIN_BLOCKS);
+}
 template<class VT, bool PACKED, bool COEF = false>
-__global__ void __launch_bounds__(kLanes, BNN_PCG_MIN_BLOCKS) k_pcg_persistent(PcgArgs<VT> a) {
+__global__ void __launch_bounds__(kLanes, pcg_min_blocks<VT, COEF>()) k_pcg_persistent(PcgArgs<VT> a) {
     __shared__ double smd[kLanes];
     __shared__ VT smv[kLanes];
     const int n = a.n;

@@ -77,7 +77,7 @@ struct SimulationParameters {
     // GPU-only choices (no reference counterpart): precision of the pressure solve
     int pcgMode = BNN_PCG_FP32;
     float refineTolerance = 1e-8f;
-    float refineInnerTolerance = 1e-3f;
+    float refineInnerTolerance = 1e-2f;  // measured best at 256^3 (1e-3: 0.69 G, 1e-2: 0.72 G particle-steps/s)
 };
 
 // ParticleSimulationData (ParticleSolverData.h:178-241): AoS vec3 host arrays

@@ -81,7 +81,7 @@ def dam_break_params(n: int, **over) -> dict:
              n_expand_cells=2, cfl_factor=1.0, min_timestep=1e-6, max_timestep=float(np.float32(1.0) / np.float32(30.0)),
              frame_duration=float(np.float32(1.0 / 30.0)), pic_flip_ratio=0.97, cg_relative_tolerance=1e-6,
              max_cg_iteration=5000, advection_steps=1, solver_kind=0, pcg_mode=0, preconditioner=0,
-             refine_tolerance=1e-8, refine_inner_tolerance=1e-3, apply_gravity=1, correct_position=0,
+             refine_tolerance=1e-8, refine_inner_tolerance=1e-2, apply_gravity=1, correct_position=0,
              repulsive_force_stiffness=50.0, ratio_cell_size_p_radius=2.0)
     p.update(over)
     return p

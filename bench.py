@@ -61,10 +61,17 @@ WORKLOAD = "flip_dam_break_256"
 PCG_TRAFFIC_PER_ITER = 931.7e6 / 300
 
 
-def _config(pcg_mode: str):
+def _config(pcg_mode: str, cfg: dict | None = None, pcg_text: str | None = None):
+    if pcg_text is not None:
+        pcg = pcg_text
+    elif pcg_mode == "refined":
+        pcg = (f"Jacobi, FP32 inner to {cfg['refine_inner_tolerance'] if cfg else 1e-2:g} / FP64 outer refined to "
+               f"{cfg['refine_tolerance'] if cfg else 1e-8:g} max-norm rel")
+    else:
+        pcg = f"Jacobi, {pcg_mode}, tol {cfg['cg_relative_tolerance'] if cfg else 1e-6:g} max-norm rel"
     return {"workload": WORKLOAD, "grid": f"{N_GRID}^3 (+2 padding cells per side = {N_GRID + 4}^3 stored)",
             "particles": None, "block": [0.4, 0.6, 0.4], "particles_per_cell": 8, "seed": 42,
-            "solver": "FLIP", "pic_flip_ratio": 0.97, "cfl": 1.0, "pcg": f"Jacobi, {pcg_mode}, tol 1e-6 max-norm rel",
+            "solver": "FLIP", "pic_flip_ratio": 0.97, "cfl": 1.0, "pcg": pcg,
             "step": "one advanceFrame sub-step", "l2_policy": "inputs larger than L2 (particles 306 MB, faces 212 MB)",
             "parallelism": "replicas"}
 
@@ -187,8 +194,9 @@ def run_reference(args, ws, rank):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": steps, "warmup": w_done,
             "ms_per_step": dt * 1e3 / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded dam break, seed 42)", "impl": "reference",
-            "config": dict(_config("reference order FP32" + (", symmetric MIC(0) preconditioner (the reference "
-                                                             "default)" if precond else "")), particles=len(pos)),
+            "config": dict(_config("fp32", pcg_text=("symmetric MIC(0) preconditioner (the reference default)"
+                                                     if precond else "Jacobi") + ", reference order FP32, tol 1e-6 "
+                                                    "max-norm rel"), particles=len(pos)),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": f"{steps} full sub-steps of the 256^3 scene after {w_done} untimed "
                                        f"(oracle port of the reference CPU solver, OpenMP, {threads} threads)"},
@@ -215,6 +223,10 @@ def run_ours(args, ws, rank, local):
 
     pcg_mode = args.pcg_mode
     cfg = scenes.dam_break_params(N_GRID, pcg_mode={"fp32": 0, "fp64": 1, "refined": 2}[pcg_mode])
+    if args.inner_tol is not None:
+        cfg["refine_inner_tolerance"] = args.inner_tol
+    if args.tol is not None:
+        cfg["cg_relative_tolerance"] = args.tol
     pos, vel = scenes.dam_break(N_GRID)
     npart = len(pos)
     solver = FlipSolver(cfg)
@@ -302,7 +314,7 @@ def run_ours(args, ws, rank, local):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded dam break, seed 42)",
-            "config": dict(_config(pcg_mode), particles=npart),
+            "config": dict(_config(pcg_mode, cfg), particles=npart),
             "roofline": {"bound": "hbm", "kernel": "k_pcg_persistent (whole Jacobi PCG solve, one launch per step)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
@@ -392,7 +404,7 @@ def run_batch(args, ws, rank, local):
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scenes, seed 11)",
                 "config": {"workload": "batch_256_scenes", "scenes": len(specs), "scenes_rank0": len(mine),
                            "particles_rank0": npart, "res_choices": [32, 48, 64, 96, 128], "cell_size": "1/64",
-                           "pcg": "Jacobi, refined FP32 inner / FP64 outer to 1e-8, inner 1e-3",
+                           "pcg": "Jacobi, refined FP32 inner / FP64 outer to 1e-8, inner 1e-2",
                            "worker_threads": args.workers or "min(16, cores)", "parallelism": f"scenes/{ws} ranks"},
                 "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
                 "e2e": {"value": tot_ps / e2e_t, "unit": UNIT, "h2d_bytes_per_step": 24 * npart / args.steps,
@@ -778,6 +790,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--pcg-mode", choices=["fp32", "fp64", "refined"], default="fp32")
+    ap.add_argument("--inner-tol", type=float, default=None, help="refined PCG: inner (FP32) relative tolerance")
+    ap.add_argument("--tol", type=float, default=None,
+                    help="fp32 / fp64 PCG: relative tolerance (the refined mode's outer tolerance is 1e-8)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--grid", type=int, default=N_GRID, help="fluid-domain resolution (profiling of smaller cases)")
