@@ -88,7 +88,8 @@ typedef struct bnn_params {
     int32_t  pcg_mode;               /* BNN_PCG_* */
     int32_t  preconditioner;         /* BNN_PRECOND_* */
     float    refine_tolerance;       /* BNN_PCG_REFINED: outer max-norm relative tolerance */
-    float    refine_inner_tolerance; /* BNN_PCG_REFINED: inner FP32 relative tolerance */
+    float    refine_inner_tolerance; /* BNN_PCG_REFINED: inner FP32 relative tolerance (1e-2 is
+                                        fastest on the 256^3 dam break to an outer 1e-8) */
     int32_t  apply_gravity;          /* GlobalParameters ApplyGravity (default 1) */
     uint32_t max_particles;          /* particle capacity; 0 = size to the first set_particles */
     int32_t  correct_position;       /* CorrectPosition (default 0): neighbour-spring pass after
