@@ -387,6 +387,23 @@ def run_batch(args, ws, rank, local):
     t_dl = time.perf_counter() - t_dl
     clk = clocks.stop()
     launches = capi.launch_count() - launches0
+    b.close()
+    # the same scenes one at a time (one worker thread: each scene's sub-step runs alone
+    # on the GPU before the next one starts), for the batching's gain
+    b1 = FlipBatch(worker_threads=1)
+    for cfg, pos, vel in built:
+        b1.add_scene(cfg, pos, vel)
+    b1.step()
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    ps1 = 0
+    seq_steps = 2
+    for _ in range(seq_steps):
+        ps1 += b1.step()["particle_steps"]
+    torch.cuda.synchronize()
+    t1 = time.perf_counter() - t1
+    b1.close()
+    seq_value = ps1 / t1
     tot_ps = ps
     t_max = te
     e2e_t = te + t_up + t_dl
@@ -411,9 +428,11 @@ def run_batch(args, ws, rank, local):
                         "d2h_bytes_per_step": 24 * npart / args.steps,
                         "api": "bnn_batch_add_scene (upload) + steps + bnn_batch_get_scene (download), wall clock"},
                 "gpu_launches": int(launches), "clocks": clk,
-                "detail": {"pcg_iterations_per_step": iters / args.steps, "timing": "host wall clock per batch step"}}
+                "detail": {"pcg_iterations_per_step": iters / args.steps, "timing": "host wall clock per batch step",
+                           "one_scene_at_a_time": {"value": seq_value, "ms_per_step": t1 * 1e3 / seq_steps,
+                                                   "note": "rank 0's scenes, one worker thread, same accuracy"},
+                           "batched_over_one_at_a_time": (ps / te) / seq_value}}
         print(json.dumps(line), flush=True)
-    b.close()
     if ws > 1:
         dist.destroy_process_group()
     return 0
