@@ -224,6 +224,23 @@ __global__ void __launch_bounds__(256) k_bbox_final(int nparts, const int* __res
 // PIC_Solver::moveParticles (PIC_Solver.cpp:353-373) with trace_rk2 (:1137-1144), then the
 // particle's cell id and its arrival slot in the cell histogram (the first half of the
 // counting sort).
+// Cell histogram slot of a particle with one atomic per cell and warp: lanes holding the
+// same cell (most of a warp, the particles being in cell order from the last sort) take
+// consecutive slots from their leader's atomicAdd.  The order of slots inside a cell is
+// arbitrary either way: every bucket is sorted by particle id afterwards.  c = ~0u: no
+// particle in this lane.  All 32 lanes of the warp must call it.
+__device__ __forceinline__ void histogram_slot(uint32_t c, int p, uint32_t* __restrict__ count,
+                                               uint32_t* __restrict__ slot) {
+    const unsigned peers = __match_any_sync(0xffffffffu, c);
+    if(c == 0xffffffffu) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if(lane == leader) base = atomicAdd(count + c, (unsigned)__popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    slot[p] = base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
+}
+
 __global__ void __launch_bounds__(256) k_advect(int n, float* __restrict__ px, float* __restrict__ py,
                                                 float* __restrict__ pz, const float* __restrict__ u,
                                                 const float* __restrict__ v, const float* __restrict__ w, GridDesc g,
@@ -232,6 +249,7 @@ __global__ void __launch_bounds__(256) k_advect(int n, float* __restrict__ px, f
                                                 DevState* st, int* __restrict__ bboxPart) {
     int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {INT_MIN, INT_MIN, INT_MIN};
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t c = 0xffffffffu;
     if(p < n) {
         float x = px[p], y = py[p], z = pz[p];
         for(int s = 0; s < steps; ++s) {
@@ -250,14 +268,13 @@ __global__ void __launch_bounds__(256) k_advect(int n, float* __restrict__ px, f
         px[p] = x; py[p] = y; pz[p] = z;
         bool outside;
         int cc[3];
-        const uint32_t c = cell_linear(g, (x - g.bmin[0]) / g.dx, (y - g.bmin[1]) / g.dx, (z - g.bmin[2]) / g.dx,
-                                       outside, cc);
+        c = cell_linear(g, (x - g.bmin[0]) / g.dx, (y - g.bmin[1]) / g.dx, (z - g.bmin[2]) / g.dx, outside, cc);
         if(outside) atomicOr(&st->flags, BNN_FLAG_OUT_OF_GRID);
         cellOf[p] = c;
-        slot[p] = atomicAdd(count + c, 1u);
 #pragma unroll
         for(int d = 0; d < 3; ++d) { mn[d] = cc[d]; mx[d] = cc[d]; }
     }
+    histogram_slot(c, p, count, slot);
     bbox_block_partial(bboxPart, mn, mx);
 }
 
@@ -344,16 +361,21 @@ __global__ void __launch_bounds__(256) k_rebin(int n, const float* __restrict__ 
                                                uint32_t* __restrict__ cellOf, uint32_t* __restrict__ slot,
                                                uint32_t* __restrict__ count, DevState* st) {
     int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {INT_MIN, INT_MIN, INT_MIN};
-    for(int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
-        bool outside;
-        int cc[3];
-        const uint32_t c = cell_linear(g, (px[p] - g.bmin[0]) / g.dx, (py[p] - g.bmin[1]) / g.dx,
-                                       (pz[p] - g.bmin[2]) / g.dx, outside, cc);
-        if(outside) atomicOr(&st->flags, BNN_FLAG_OUT_OF_GRID);
-        cellOf[p] = c;
-        slot[p] = atomicAdd(count + c, 1u);
+    // the trip count is the same for the whole block (histogram_slot needs every lane)
+    for(int p0 = blockIdx.x * blockDim.x; p0 < n; p0 += gridDim.x * blockDim.x) {
+        const int p = p0 + threadIdx.x;
+        uint32_t c = 0xffffffffu;
+        if(p < n) {
+            bool outside;
+            int cc[3];
+            c = cell_linear(g, (px[p] - g.bmin[0]) / g.dx, (py[p] - g.bmin[1]) / g.dx, (pz[p] - g.bmin[2]) / g.dx,
+                            outside, cc);
+            if(outside) atomicOr(&st->flags, BNN_FLAG_OUT_OF_GRID);
+            cellOf[p] = c;
 #pragma unroll
-        for(int d = 0; d < 3; ++d) { mn[d] = min(mn[d], cc[d]); mx[d] = max(mx[d], cc[d]); }
+            for(int d = 0; d < 3; ++d) { mn[d] = min(mn[d], cc[d]); mx[d] = max(mx[d], cc[d]); }
+        }
+        histogram_slot(c, p, count, slot);
     }
     bbox_block_reduce(st, mn, mx);
 }
