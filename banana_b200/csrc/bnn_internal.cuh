@@ -232,8 +232,7 @@ cudaError_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, size_t n, void
 
 // pcg.cu
 struct GridSync {
-    unsigned count;  // blocks arrived at the current barrier
-    unsigned gen;    // barrier generation
+    unsigned count;  // arrivals at the current barrier (top bit: barriers passed, mod 2)
 };
 struct PcgWork {
     int cap = 0;

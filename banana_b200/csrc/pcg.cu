@@ -81,10 +81,6 @@ constexpr unsigned kSpinLimit = 1u << 24;  // ~seconds of polling before a barri
 #ifndef BNN_BARRIER_SLEEP_NS
 #define BNN_BARRIER_SLEEP_NS 0
 #endif
-#ifndef BNN_PCG_ROW_GROUP
-#define BNN_PCG_ROW_GROUP 2
-#endif
-constexpr int kRowGroup = BNN_PCG_ROW_GROUP;  // rows whose loads are in flight together
 
 // Canonical 256-lane tree (lane t of the chunk owns v; levels 128, 64, 32 then a warp
 // shuffle tree), with one shared-memory staging step: warp 0 forms the three upper
@@ -119,24 +115,61 @@ __device__ __forceinline__ void block_sum_max_256(double v, VT m, double* sm, VT
 }
 
 // Reduce the chunk partials (sum in canonical order, and max) and give the result to
-// every thread of the block.
+// every thread of the block.  A thread's partials (chunks t, t + 256, ...) are loaded four
+// at a time before they are added in chunk order; warp 0 forms the block result and lane 0
+// publishes it in its own shared slot, so one block barrier separates it from the readers
+// (the next write of the slot comes after the next reduction's first barrier, which every
+// reader reaches only after reading).
 template<class VT>
 __device__ __forceinline__ void reduce_partials_bcast(const double* part, const VT* pmax, int nch, double* sm, VT* smm,
                                                       double& sum, VT& mx) {
+    __shared__ double sSum;
+    __shared__ VT sMax;
+    constexpr int U = 4;
     double acc = 0.0;
     VT m = VT(0);
-    for(int c = threadIdx.x; c < nch; c += kLanes) {
-        acc = acc + __ldcg(part + c);
-        if(pmax) { const VT o = __ldcg(pmax + c); m = m > o ? m : o; }
+    for(int c0 = threadIdx.x; c0 < nch; c0 += U * kLanes) {
+        double p[U];
+        VT o[U];
+#pragma unroll
+        for(int u = 0; u < U; ++u) {
+            const int c = c0 + u * kLanes;
+            p[u] = c < nch ? __ldcg(part + c) : 0.0;
+            o[u] = (pmax && c < nch) ? __ldcg(pmax + c) : VT(0);
+        }
+#pragma unroll
+        for(int u = 0; u < U; ++u)
+            if(c0 + u * kLanes < nch) {
+                acc = acc + p[u];
+                if(pmax) m = m > o[u] ? m : o[u];
+            }
     }
-    double s = 0.0;
-    VT x = VT(0);
-    block_sum_max_256<VT>(acc, m, sm, smm, s, x, pmax != nullptr);
-    if(threadIdx.x == 0) { sm[0] = s; smm[0] = x; }
+    const int t = threadIdx.x;
+    sm[t] = acc;
+    if(pmax) smm[t] = m;
     __syncthreads();
-    sum = sm[0];
-    mx = smm[0];
+    if(t < 32) {
+        // the association of block_sum_max_256
+        const double a0 = sm[t] + sm[t + 128];
+        const double a1 = sm[t + 64] + sm[t + 192];
+        const double a2 = sm[t + 32] + sm[t + 160];
+        const double a3 = sm[t + 96] + sm[t + 224];
+        double c = (a0 + a1) + (a2 + a3);
+#pragma unroll
+        for(int off = 16; off > 0; off >>= 1) c = c + __shfl_down_sync(0xffffffffu, c, off);
+        VT x = VT(0);
+        if(pmax) {
+            x = smm[t];
+#pragma unroll
+            for(int q = 1; q < 8; ++q) { const VT o = smm[t + 32 * q]; x = x > o ? x : o; }
+#pragma unroll
+            for(int off = 16; off > 0; off >>= 1) { const VT o = __shfl_down_sync(0xffffffffu, x, off); x = x > o ? x : o; }
+        }
+        if(t == 0) { sSum = c; sMax = x; }
+    }
     __syncthreads();
+    sum = sSum;
+    mx = sMax;
 }
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
@@ -145,27 +178,27 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
     return v;
 }
 
-__device__ __forceinline__ unsigned atom_add_release_u32(unsigned* p, unsigned v) {
-    unsigned old;
-    asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
-    return old;
+__device__ __forceinline__ void red_add_release_u32(unsigned* p, unsigned v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" : : "l"(p), "r"(v) : "memory");
 }
 
-// Grid-wide barrier with a bounded wait (sense reversal on one word): block 0 adds
-// 2^31 - (nblocks - 1), every other block adds 1, so the word's top bit flips exactly
-// when the last block arrives and its low bits return to where they were.  Arrival is a
-// release, the poll an acquire, so each block's writes before the barrier are visible to
-// every block after it.  Returns false (and sets the timeout flag) when the wait gave up.
-__device__ __forceinline__ bool grid_barrier(GridSync* gs, unsigned nblocks, unsigned& gen, unsigned* flags) {
+// Grid-wide barrier with a bounded wait (sense reversal on one word, zeroed before the
+// launch): block 0 adds 2^31 - (nblocks - 1), every other block adds 1, so the word's top
+// bit flips exactly when the last block arrives and its low bits return to where they
+// were.  After the b-th barrier the top bit is b & 1; each block counts its barriers in
+// `sense`, so the arrival is a fire-and-forget reduction (release) and the poll (acquire)
+// starts at once.  Each block's writes before the barrier are visible to every block
+// after it.  Returns false (and sets the timeout flag) when the wait gave up.
+__device__ __forceinline__ bool grid_barrier(GridSync* gs, unsigned nblocks, unsigned& sense, unsigned* flags) {
     __shared__ int sOk;
-    (void)gen;
+    sense ^= 1u;
     __syncthreads();
     if(threadIdx.x == 0) {
         int ok = 1;
         const unsigned add = blockIdx.x == 0 ? 0x80000000u - (nblocks - 1u) : 1u;
-        const unsigned old = atom_add_release_u32(&gs->count, add);
+        red_add_release_u32(&gs->count, add);
         unsigned spins = 0;
-        while(((ld_acquire_u32(&gs->count) ^ old) & 0x80000000u) == 0u) {
+        while((ld_acquire_u32(&gs->count) >> 31) != sense) {
             if(++spins > kSpinLimit) {
                 ok = 0;
                 atomicOr(flags, BNN_FLAG_TIMEOUT);
@@ -203,29 +236,47 @@ __device__ __forceinline__ VT s_val(const VT* z, const VT* sOld, VT beta, bool f
     return first ? __ldcg(z + e) : __ldcg(z + e) + beta * __ldcg(sOld + e);
 }
 
+// Resident blocks per SM the register budget is sized for, and rows per lane whose loads
+// are in flight together in the SpMV phase (a divisor of kPerLane).  Two blocks of 256
+// threads with four rows in flight beat four blocks with two: the same loads in flight per
+// SM, fewer blocks at every grid barrier (1.59M rows, us per iteration: FP32 vectors 24.9
+// against 25.8, FP64 47.0 against 48.2 at three blocks with two rows).  Rows with
+// off-diagonal values keep three blocks with two rows (38.5 us; two blocks with four rows
+// spill and take 42.6).
 #ifndef BNN_PCG_MIN_BLOCKS
-#define BNN_PCG_MIN_BLOCKS 4
+#define BNN_PCG_MIN_BLOCKS 2
+#endif
+#ifndef BNN_PCG_ROW_GROUP
+#define BNN_PCG_ROW_GROUP 4
 #endif
 #ifndef BNN_PCG_MIN_BLOCKS_F64
-#define BNN_PCG_MIN_BLOCKS_F64 3
+#define BNN_PCG_MIN_BLOCKS_F64 2
 #endif
-// resident blocks per SM the register budget is sized for: 4 for FP32 vectors; FP64 ones
-// and rows with off-diagonal values run faster at 3 (fewer spills: FP64 47.7 against
-// 53.6 us per iteration at 1.59M rows, rows with values 38.5 against 40.0)
+#ifndef BNN_PCG_ROW_GROUP_F64
+#define BNN_PCG_ROW_GROUP_F64 4
+#endif
 #ifndef BNN_PCG_MIN_BLOCKS_COEF
 #define BNN_PCG_MIN_BLOCKS_COEF 3
+#endif
+#ifndef BNN_PCG_ROW_GROUP_COEF
+#define BNN_PCG_ROW_GROUP_COEF 2
 #endif
 template<class VT, bool COEF> constexpr int pcg_min_blocks() {
     return sizeof(VT) == 8 ? BNN_PCG_MIN_BLOCKS_F64 : (COEF ? BNN_PCG_MIN_BLOCKS_COEF : BNN_PCG_MIN_BLOCKS);
 }
+template<class VT, bool COEF> constexpr int pcg_row_group() {
+    return sizeof(VT) == 8 ? BNN_PCG_ROW_GROUP_F64 : (COEF ? BNN_PCG_ROW_GROUP_COEF : BNN_PCG_ROW_GROUP);
+}
 template<class VT, bool PACKED, bool COEF = false>
 __global__ void __launch_bounds__(kLanes, pcg_min_blocks<VT, COEF>()) k_pcg_persistent(PcgArgs<VT> a) {
+    constexpr int kRowGroup = pcg_row_group<VT, COEF>();
+    static_assert(kPerLane % kRowGroup == 0, "row groups must tile a lane's rows");
     __shared__ double smd[kLanes];
     __shared__ VT smv[kLanes];
     const int n = a.n;
     const int nch = (n + kChunk - 1) / kChunk;
     const unsigned nb = gridDim.x;
-    unsigned gen = ld_acquire_u32(&a.gs->gen);
+    unsigned sense = 0;  // barriers passed, mod 2
     unsigned* flags = &a.st->flags;
     VT* __restrict__ xR = a.x;
     VT* __restrict__ rR = a.r;
@@ -263,7 +314,7 @@ __global__ void __launch_bounds__(kLanes, pcg_min_blocks<VT, COEF>()) k_pcg_pers
         block_sum_max_256<VT>(acc, m, smd, smv, bs, bm, true);
         if(threadIdx.x == 0) { a.part0[c] = bs; a.partMax[c] = bm; }
     }
-    if(!grid_barrier(a.gs, nb, gen, flags)) return;
+    if(!grid_barrier(a.gs, nb, sense, flags)) return;
     double rho;
     VT resid;
     reduce_partials_bcast<VT>(a.part0, a.partMax, nch, smd, smv, rho, resid);
@@ -408,7 +459,7 @@ __global__ void __launch_bounds__(kLanes, pcg_min_blocks<VT, COEF>()) k_pcg_pers
             if(threadIdx.x == 0) a.part1[c] = bs;
         }
         TMARK(0);
-        if(!grid_barrier(a.gs, nb, gen, flags)) return;
+        if(!grid_barrier(a.gs, nb, sense, flags)) return;
         TMARK(1);
         double tmp;
         VT unused2;
@@ -456,7 +507,7 @@ __global__ void __launch_bounds__(kLanes, pcg_min_blocks<VT, COEF>()) k_pcg_pers
             if(threadIdx.x == 0) { a.part2[c] = bs; a.partMax[c] = bm; }
         }
         TMARK(3);
-        if(!grid_barrier(a.gs, nb, gen, flags)) return;
+        if(!grid_barrier(a.gs, nb, sense, flags)) return;
         TMARK(4);
         double rhoNew;
         reduce_partials_bcast<VT>(a.part2, a.partMax, nch, smd, smv, rhoNew, resid);
