@@ -29,7 +29,7 @@ EXPORTS = [
     "bnn_flip_create", "bnn_flip_destroy", "bnn_flip_grid_dims", "bnn_flip_set_particles", "bnn_flip_get_particles",
     "bnn_flip_num_particles", "bnn_flip_get_grid", "bnn_flip_step", "bnn_flip_advance_frame",
     "bnn_flip_device_particles", "bnn_flip_step_host", "bnn_flip_stream", "bnn_cell_sort", "bnn_cell_sort_noalloc", "bnn_z_sort", "bnn_neighbors",
-    "bnn_pcg_solve_7pt", "bnn_version", "bnn_last_error", "bnn_launch_count",
+    "bnn_pcg_solve_7pt", "bnn_pcg_barrier_probe", "bnn_version", "bnn_last_error", "bnn_launch_count",
     "bnn_flip_device_bytes", "bnn_scene_bytes_estimate", "bnn_flip_set_grid",
     "bnn_batch_create", "bnn_batch_destroy", "bnn_batch_add_scene", "bnn_batch_remove_scene", "bnn_batch_step",
     "bnn_batch_scene_info", "bnn_batch_get_scene", "bnn_batch_memory",
@@ -167,6 +167,7 @@ def load() -> C.CDLL:
     L.bnn_neighbors.argtypes = [vp, C.c_uint32, C.c_float, vp, vp, C.c_uint64, u64p, vp]
     L.bnn_pcg_solve_7pt.argtypes = [C.c_uint32, fp, i32p, C.c_float, fp, C.c_float, C.c_uint32, C.c_int32, C.c_float,
                                     dp, C.POINTER(PcgStats)]
+    L.bnn_pcg_barrier_probe.argtypes = [C.c_float, i32p, fp]
     L.bnn_flip_device_bytes.argtypes = [vp, u64p]
     L.bnn_flip_set_grid.argtypes = [vp, C.c_int32, fp, C.c_size_t]
     L.bnn_scene_bytes_estimate.argtypes = [C.POINTER(Params), C.c_uint32, u64p]
@@ -397,6 +398,16 @@ def pcg_solve_7pt(diag, nbr, offdiag, rhs, tol, max_iter, mode="fp32", inner_tol
     if rc not in (BNN_OK, 3):
         raise BnnError(rc, "bnn_pcg_solve_7pt")
     return x[:n], {f: getattr(st, f) for f, _ in PcgStats._fields_}
+
+
+def pcg_barrier_probe(limit_seconds: float = 0.05):
+    """Self-test of the bounded PCG barrier wait (bnn_pcg_barrier_probe): one block waits at
+    a barrier sized for two until the wait gives up.  Returns (status, elapsed_ms); status
+    is STATUS_CODE["TIMEOUT"] when the wait gave up as designed."""
+    st = C.c_int32(-1)
+    ms = C.c_float(0.0)
+    check(load().bnn_pcg_barrier_probe(C.c_float(limit_seconds), C.byref(st), C.byref(ms)), "bnn_pcg_barrier_probe")
+    return int(st.value), float(ms.value)
 
 
 def scene_bytes_estimate(cfg: dict, n: int) -> int:

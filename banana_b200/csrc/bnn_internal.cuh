@@ -264,6 +264,8 @@ int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const floa
               float outerTol, float* pressure, double* x64out, DevState* dst, DevState* hst, cudaStream_t s,
               PcgOutcome& out);
 int pcg_reserve(PcgWork& w, int n, bool fp64);
+// one block waits at a barrier sized for two until the bounded wait gives up
+int pcg_barrier_probe(float limitSeconds, int* barrierStatus, float* elapsedMs);
 // Cell grid of the anisotropic-kernel pass (aniso.cu)
 struct AnisoGrid {
     int G[3];

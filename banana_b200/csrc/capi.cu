@@ -841,6 +841,17 @@ extern "C" int bnn_flip_advance_frame(bnn_flip* h, uint32_t* substeps) {
 // ---------------------------------------------------------------------------------
 // Standalone PCG on a 7-point system
 // ---------------------------------------------------------------------------------
+extern "C" int bnn_pcg_barrier_probe(float limit_seconds, int32_t* barrier_status, float* elapsed_ms) {
+    if(!barrier_status || !elapsed_ms || !(limit_seconds > 0.f && limit_seconds <= 10.f)) return BNN_ERR_INVALID_ARGUMENT;
+    int st = BNN_OK;
+    float ms = 0.f;
+    const int rc = bnn::pcg_barrier_probe(limit_seconds, &st, &ms);
+    if(rc != BNN_OK) return rc;
+    *barrier_status = st;
+    *elapsed_ms = ms;
+    return BNN_OK;
+}
+
 extern "C" int bnn_pcg_solve_7pt(uint32_t n, const float* diag, const int32_t* nbr, float offdiag, const float* rhs,
                                  float tol, uint32_t max_iter, int32_t mode, float inner_tol, double* x_out,
                                  bnn_pcg_stats* stats) {

@@ -77,7 +77,14 @@ template<class VT> __device__ __forceinline__ VT reduce_max_t(const VT* part, in
 // blocks hold bit-identical scalars and take the same branch without a broadcast.  Data
 // written by other blocks is read with ld.global.cg (L2), never through a stale L1 line.
 // ---------------------------------------------------------------------------------
-constexpr unsigned kSpinLimit = 1u << 24;  // ~seconds of polling before a barrier gives up
+// A barrier wait gives up once it has polled minSpins times and ns more of wall time
+// (%globaltimer) have passed, or after maxSpins polls whatever the clock says.  Counting
+// polls as well as time keeps a solve that the GPU time-slices away from giving up early.
+struct BarrierLimit {
+    unsigned long long ns;
+    unsigned minSpins, maxSpins;
+};
+__host__ __device__ constexpr BarrierLimit solve_barrier_limit() { return {1000000000ull, 1u << 20, 1u << 26}; }
 #ifndef BNN_BARRIER_SLEEP_NS
 #define BNN_BARRIER_SLEEP_NS 0
 #endif
@@ -189,7 +196,14 @@ __device__ __forceinline__ void red_add_release_u32(unsigned* p, unsigned v) {
 // `sense`, so the arrival is a fire-and-forget reduction (release) and the poll (acquire)
 // starts at once.  Each block's writes before the barrier are visible to every block
 // after it.  Returns false (and sets the timeout flag) when the wait gave up.
-__device__ __forceinline__ bool grid_barrier(GridSync* gs, unsigned nblocks, unsigned& sense, unsigned* flags) {
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ bool grid_barrier(GridSync* gs, unsigned nblocks, unsigned& sense, unsigned* flags,
+                                             BarrierLimit lim) {
     __shared__ int sOk;
     sense ^= 1u;
     __syncthreads();
@@ -198,8 +212,11 @@ __device__ __forceinline__ bool grid_barrier(GridSync* gs, unsigned nblocks, uns
         const unsigned add = blockIdx.x == 0 ? 0x80000000u - (nblocks - 1u) : 1u;
         red_add_release_u32(&gs->count, add);
         unsigned spins = 0;
+        unsigned long long t0 = 0;
         while((ld_acquire_u32(&gs->count) >> 31) != sense) {
-            if(++spins > kSpinLimit) {
+            ++spins;
+            if(spins == lim.minSpins) t0 = global_ns();
+            if(spins >= lim.maxSpins || (spins > lim.minSpins && (spins & 255u) == 0u && global_ns() - t0 >= lim.ns)) {
                 ok = 0;
                 atomicOr(flags, BNN_FLAG_TIMEOUT);
                 break;
@@ -314,7 +331,7 @@ __global__ void __launch_bounds__(kLanes, pcg_min_blocks<VT, COEF>()) k_pcg_pers
         block_sum_max_256<VT>(acc, m, smd, smv, bs, bm, true);
         if(threadIdx.x == 0) { a.part0[c] = bs; a.partMax[c] = bm; }
     }
-    if(!grid_barrier(a.gs, nb, sense, flags)) return;
+    if(!grid_barrier(a.gs, nb, sense, flags, solve_barrier_limit())) return;
     double rho;
     VT resid;
     reduce_partials_bcast<VT>(a.part0, a.partMax, nch, smd, smv, rho, resid);
@@ -459,7 +476,7 @@ __global__ void __launch_bounds__(kLanes, pcg_min_blocks<VT, COEF>()) k_pcg_pers
             if(threadIdx.x == 0) a.part1[c] = bs;
         }
         TMARK(0);
-        if(!grid_barrier(a.gs, nb, sense, flags)) return;
+        if(!grid_barrier(a.gs, nb, sense, flags, solve_barrier_limit())) return;
         TMARK(1);
         double tmp;
         VT unused2;
@@ -507,7 +524,7 @@ __global__ void __launch_bounds__(kLanes, pcg_min_blocks<VT, COEF>()) k_pcg_pers
             if(threadIdx.x == 0) { a.part2[c] = bs; a.partMax[c] = bm; }
         }
         TMARK(3);
-        if(!grid_barrier(a.gs, nb, sense, flags)) return;
+        if(!grid_barrier(a.gs, nb, sense, flags, solve_barrier_limit())) return;
         TMARK(4);
         double rhoNew;
         reduce_partials_bcast<VT>(a.part2, a.partMax, nch, smd, smv, rhoNew, resid);
@@ -872,6 +889,53 @@ int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const floa
     out.success = ok ? 1 : 0;
     { k_d64_to_f32<<<nb, 256, 0, s>>>(n, w.x64, pressure); bnn_note_launch(); }
     if(x64out) BNN_CUDA_CHECK(cudaMemcpyAsync(x64out, w.x64, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    return BNN_OK;
+}
+
+// ---- self-test of the bounded barrier wait -------------------------------------------
+// One block arrives at a barrier sized for two blocks, so the wait can only end by giving
+// up; out[0] = 1 when it gave up, out[1] = the block's polling time in ns.
+__global__ void k_barrier_probe(GridSync* gs, unsigned* flags, BarrierLimit lim, unsigned long long* out) {
+    unsigned sense = 0;
+    const unsigned long long t0 = global_ns();
+    const bool passed = grid_barrier(gs, 2u, sense, flags, lim);
+    if(threadIdx.x == 0) {
+        out[0] = passed ? 0ull : 1ull;
+        out[1] = global_ns() - t0;
+    }
+}
+
+int pcg_barrier_probe(float limitSeconds, int* barrierStatus, float* elapsedMs) {
+    GridSync* gs = nullptr;
+    unsigned* flags = nullptr;
+    unsigned long long* out = nullptr;
+    int rc = BNN_OK;
+    auto chk = [&](cudaError_t e) { if(e != cudaSuccess && rc == BNN_OK) { bnn_set_error(cudaGetErrorString(e)); rc = e == cudaErrorMemoryAllocation ? BNN_ERR_OUT_OF_MEMORY : BNN_ERR_CUDA; } };
+    chk(cudaMalloc(&gs, sizeof(GridSync)));
+    chk(cudaMalloc(&flags, sizeof(unsigned)));
+    chk(cudaMalloc(&out, 2 * sizeof(unsigned long long)));
+    unsigned long long h[2] = {0, 0};
+    unsigned hf = 0;
+    if(rc == BNN_OK) {
+        chk(cudaMemset(gs, 0, sizeof(GridSync)));
+        chk(cudaMemset(flags, 0, sizeof(unsigned)));
+    }
+    if(rc == BNN_OK) {
+        // 4096 polls, then limitSeconds of time; 2^26 polls at most whatever the clock says
+        const BarrierLimit lim = {(unsigned long long)((double)limitSeconds * 1e9), 1u << 12, 1u << 26};
+        k_barrier_probe<<<1, kLanes>>>(gs, flags, lim, out);
+        bnn_note_launch();
+        chk(cudaGetLastError());
+        chk(cudaDeviceSynchronize());
+        chk(cudaMemcpy(h, out, sizeof(h), cudaMemcpyDeviceToHost));
+        chk(cudaMemcpy(&hf, flags, sizeof(hf), cudaMemcpyDeviceToHost));
+    }
+    cudaFree(gs);
+    cudaFree(flags);
+    cudaFree(out);
+    if(rc != BNN_OK) return rc;
+    *barrierStatus = (h[0] == 1ull && (hf & BNN_FLAG_TIMEOUT)) ? BNN_ERR_TIMEOUT : BNN_OK;
+    *elapsedMs = (float)((double)h[1] * 1e-6);
     return BNN_OK;
 }
 

@@ -247,6 +247,14 @@ typedef struct bnn_pcg_stats {
 int bnn_pcg_solve_7pt(uint32_t n, const float* diag, const int32_t* nbr, float offdiag, const float* rhs, float tol,
                       uint32_t max_iter, int32_t mode, float inner_tol, double* x_out, bnn_pcg_stats* stats);
 
+/* Self-test of the bounded wait of the PCG grid barrier (no counterpart in the reference,
+ * whose solver has no device-side waits).  One block waits at a barrier sized for two
+ * blocks, so the wait can only end by giving up: after 4096 polls and limit_seconds
+ * (0 < limit_seconds <= 10) of wall time, the limit a solve uses being 1 s.
+ * *barrier_status receives BNN_ERR_TIMEOUT when the wait gave up as designed, *elapsed_ms
+ * how long the block polled.  The device stays usable afterwards. */
+int bnn_pcg_barrier_probe(float limit_seconds, int32_t* barrier_status, float* elapsed_ms);
+
 /* Library version / last CUDA error text / number of kernels this library has launched
  * in this process (diagnostics; no counterpart in the reference). */
 /* ---- boundary objects ------------------------------------------------------------- */

@@ -85,6 +85,10 @@ def test_validation_needs_no_gpu(lib):
         capi.STATUS_CODE["INVALID_ARGUMENT"]
     assert lib.bnn_flip_anisotropic_kernels(None, None, None, None, None) == capi.STATUS_CODE["INVALID_ARGUMENT"]
     assert lib.bnn_flip_set_boundaries(None, None, 0, 1) == capi.STATUS_CODE["INVALID_ARGUMENT"]
+    st, ms = C.c_int32(0), C.c_float(0.0)
+    for lim in (0.0, -1.0, 10.5, float("nan")):
+        assert lib.bnn_pcg_barrier_probe(lim, C.byref(st), C.byref(ms)) == capi.STATUS_CODE["INVALID_ARGUMENT"]
+    assert lib.bnn_pcg_barrier_probe(0.05, None, None) == capi.STATUS_CODE["INVALID_ARGUMENT"]
 
 
 def test_missing_library_fails_loudly(monkeypatch, tmp_path):

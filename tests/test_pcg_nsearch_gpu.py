@@ -123,6 +123,21 @@ def test_pcg_7pt_grid_rows_packed_matches_oracle(bnn, oracle_mod, mode, omode):
             assert np.array_equal(x, xo)
 
 
+def test_barrier_wait_gives_up_and_device_stays_usable(bnn, oracle_mod):
+    """A block waiting at a barrier that nothing completes (sized for two blocks, one
+    launched) gives up after its limit and reports a timeout; the device then solves a
+    system as before."""
+    from banana_b200 import capi
+    status, ms = bnn.pcg_barrier_probe(0.05)
+    assert status == capi.STATUS_CODE["TIMEOUT"]
+    assert 50.0 <= ms < 5000.0, ms
+    nbr, _, diag, off, rhs, (rs, ci, va) = _box_system(12, 10, 8)
+    xo, so = oracle_mod.pcg(rs, ci, va, rhs, 1e-6, 5000, 0)
+    x, st = bnn.pcg_solve_7pt(diag, nbr, off, rhs, 1e-6, 5000)
+    assert st["success"] == 1 and st["iterations"] == so["iterations"]
+    assert np.array_equal(x.astype(np.float32), xo.astype(np.float32))
+
+
 def test_pcg_7pt_rejects_bad_neighbour_index(bnn):
     nbr, _, diag, off, rhs, _ = _box_system(8, 8, 8)
     bad = nbr.copy()
