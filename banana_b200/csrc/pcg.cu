@@ -367,6 +367,15 @@ __global__ void __launch_bounds__(kLanes, pcg_min_blocks<VT, COEF>()) k_pcg_pers
         for(int c = blockIdx.x; c < nch; c += nb) {
             const size_t base = (size_t)c * kChunk + threadIdx.x;
             VT sOut[kPerLane], qOut[kPerLane];
+            // the row records of the whole chunk first: one round trip for all of them
+            int4 recAll[PACKED ? kPerLane : 1];
+            if constexpr(PACKED) {
+#pragma unroll
+                for(int j = 0; j < kPerLane; ++j) {
+                    const size_t e = base + (size_t)j * kLanes;
+                    recAll[j] = __ldg(recR + (e < (size_t)n ? e : 0));
+                }
+            }
 #pragma unroll
             for(int g0 = 0; g0 < kPerLane; g0 += kRowGroup) {
                 int32_t id[kRowGroup][7];
@@ -379,7 +388,7 @@ __global__ void __launch_bounds__(kLanes, pcg_min_blocks<VT, COEF>()) k_pcg_pers
                     const size_t ee = e < (size_t)n ? e : 0;
                     if constexpr(PACKED) {
                         // a row past n reads row 0, whose neighbours are all valid rows
-                        const int4 rr = __ldg(recR + ee);
+                        const int4 rr = recAll[g0 + u];
                         const int dyM = rr.x & 0xffff, dyP = (int)((unsigned)rr.x >> 16);
                         const int dzM = rr.y & 0x7fffffff, dzP = rr.z & 0x7fffffff;
                         const int32_t r0 = (int32_t)ee;
