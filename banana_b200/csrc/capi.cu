@@ -736,9 +736,11 @@ extern "C" int bnn_flip_step_host(bnn_flip* h, float* pos, float* vel, bnn_step_
             launch_scatter_planes(n, 9, h->C9[h->cur], h->ids[h->cur], h->C9[1 - h->cur], cap, s);
             std::swap(h->C9[0], h->C9[1]);
         }
+        // positions first and alone on the link (the advection needs them), then the
+        // velocities, which the step needs only from the sort's gather on
+        BNN_CUDA_CHECK(cudaMemcpyAsync(h->aosStage, pos, 3 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice, s));
         BNN_CUDA_CHECK(cudaEventRecord(h->io[0], s));
         BNN_CUDA_CHECK(cudaStreamWaitEvent(s2, h->io[0], 0));
-        BNN_CUDA_CHECK(cudaMemcpyAsync(h->aosStage, pos, 3 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice, s));
         launch_aos3_to_soa(n, h->aosStage, h->p6[h->cur], h->ids[h->cur], cap, s);
         BNN_CUDA_CHECK(cudaMemcpyAsync(h->aosStage + 3 * cap, vel, 3 * (size_t)n * sizeof(float),
                                        cudaMemcpyHostToDevice, s2));
