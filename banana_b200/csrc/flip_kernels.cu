@@ -700,49 +700,82 @@ __device__ __forceinline__ bool reach_box(const DevState* st, int reach, const i
 // 505-511) to the v component; beyond the region the host has already written the
 // backup 0 and the velocity 0 - gravityDt.  mode 2 (last layer after projection): folds
 // max|u| into the CFL reduction (PIC_Solver.cpp:342-349).
-// The blocks stride over 32 x 8 tiles of the region box only.
-__global__ void __launch_bounds__(256) k_extrapolate(int sx, int sy, int sz, const float* __restrict__ gin,
-                                                     const uint8_t* __restrict__ vin, float* __restrict__ gout,
-                                                     uint8_t* __restrict__ vout, int mode, float* __restrict__ oldOut,
-                                                     float gravityDt, DevState* st) {
-    const int S[3] = {sx, sy, sz};
-    int lo[3], hi[3];
-    float m = 0.f;
-    if(reach_box(st, kExtRegion, S, lo, hi)) {
-        const int tx = (hi[0] - lo[0] + 32) / 32, ty = (hi[1] - lo[1] + 8) / 8, tz = hi[2] - lo[2] + 1;
-        const long long nt = (long long)tx * ty * tz;
-        const size_t sxy = (size_t)sx * sy;
-        for(long long t = blockIdx.x; t < nt; t += gridDim.x) {
-            const int i = lo[0] + (int)(t % tx) * 32 + (int)(threadIdx.x & 31);
-            const int j = lo[1] + (int)((t / tx) % ty) * 8 + (int)(threadIdx.x >> 5);
-            const int k = lo[2] + (int)(t / ((long long)tx * ty));
-            if(i > hi[0] || j > hi[1]) continue;
-            const size_t f = ((size_t)k * sy + j) * sx + i;
-            const int o = bbox_distance(st, i, j, k);
-            float val = gin[f];
-            uint8_t vv = vin[f];
-            if(!vv && o <= kExtFull && i > 0 && i < sx - 1 && j > 0 && j < sy - 1 && k > 0 && k < sz - 1) {
-                float sum = 0.f;
-                unsigned count = 0;
-                if(vin[f + 1]) { sum += gin[f + 1]; ++count; }
-                if(vin[f - 1]) { sum += gin[f - 1]; ++count; }
-                if(vin[f + sx]) { sum += gin[f + sx]; ++count; }
-                if(vin[f - sx]) { sum += gin[f - sx]; ++count; }
-                if(vin[f + sxy]) { sum += gin[f + sxy]; ++count; }
-                if(vin[f - sxy]) { sum += gin[f - sxy]; ++count; }
-                if(count > 0) { val = sum / (float)count; vv = 2; }  // 2: extrapolated in this pass
-            }
-            vout[f] = vv;
-            if(mode == 1) {
-                oldOut[f] = val;
-                gout[f] = val - gravityDt;
-            } else {
-                gout[f] = val;
-            }
-            m = fmaxf(m, fabsf(val));
-        }
+// The blocks stride over 32 x 8 tiles of the region boxes only.
+// The three components go through a layer in one launch: their region tiles form one
+// index space (32-bit tile arithmetic), so the small per-component regions fill the GPU
+// together.
+struct ExtLayer {
+    const float* gin[3];
+    const uint8_t* vin[3];
+    float* gout[3];
+    uint8_t* vout[3];
+    float* oldOut[3];
+    float gdt[3];
+    int S[3][3];
+    int mode;
+};
+
+template<int D>
+__device__ __forceinline__ float ext_tile(const ExtLayer& a, const DevState* st, unsigned t, const int lo[3],
+                                          const int hi[3], unsigned tx, unsigned ty) {
+    const int sx = a.S[D][0], sy = a.S[D][1], sz = a.S[D][2];
+    const int i = lo[0] + (int)(t % tx) * 32 + (int)(threadIdx.x & 31);
+    const int j = lo[1] + (int)((t / tx) % ty) * 8 + (int)(threadIdx.x >> 5);
+    const int k = lo[2] + (int)(t / (tx * ty));
+    if(i > hi[0] || j > hi[1]) return 0.f;
+    const float* __restrict__ gin = a.gin[D];
+    const uint8_t* __restrict__ vin = a.vin[D];
+    const size_t sxy = (size_t)sx * sy;
+    const size_t f = ((size_t)k * sy + j) * sx + i;
+    const int o = bbox_distance(st, i, j, k);
+    float val = gin[f];
+    uint8_t vv = vin[f];
+    if(!vv && o <= kExtFull && i > 0 && i < sx - 1 && j > 0 && j < sy - 1 && k > 0 && k < sz - 1) {
+        float sum = 0.f;
+        unsigned count = 0;
+        if(vin[f + 1]) { sum += gin[f + 1]; ++count; }
+        if(vin[f - 1]) { sum += gin[f - 1]; ++count; }
+        if(vin[f + sx]) { sum += gin[f + sx]; ++count; }
+        if(vin[f - sx]) { sum += gin[f - sx]; ++count; }
+        if(vin[f + sxy]) { sum += gin[f + sxy]; ++count; }
+        if(vin[f - sxy]) { sum += gin[f - sxy]; ++count; }
+        if(count > 0) { val = sum / (float)count; vv = 2; }  // 2: extrapolated in this pass
     }
-    if(mode == 2) {
+    a.vout[D][f] = vv;
+    if(a.mode == 1) {
+        a.oldOut[D][f] = val;
+        a.gout[D][f] = val - a.gdt[D];
+    } else {
+        a.gout[D][f] = val;
+    }
+    return fabsf(val);
+}
+
+__global__ void __launch_bounds__(256, 8) k_extrapolate3(ExtLayer a, DevState* st) {
+    int lo0[3], hi0[3], lo1[3], hi1[3], lo2[3], hi2[3];
+    unsigned tx0 = 1, ty0 = 1, n0 = 0, tx1 = 1, ty1 = 1, n1 = 0, tx2 = 1, ty2 = 1, n2 = 0;
+    if(reach_box(st, kExtRegion, a.S[0], lo0, hi0)) {
+        tx0 = (unsigned)(hi0[0] - lo0[0] + 32) / 32; ty0 = (unsigned)(hi0[1] - lo0[1] + 8) / 8;
+        n0 = tx0 * ty0 * (unsigned)(hi0[2] - lo0[2] + 1);
+    }
+    if(reach_box(st, kExtRegion, a.S[1], lo1, hi1)) {
+        tx1 = (unsigned)(hi1[0] - lo1[0] + 32) / 32; ty1 = (unsigned)(hi1[1] - lo1[1] + 8) / 8;
+        n1 = tx1 * ty1 * (unsigned)(hi1[2] - lo1[2] + 1);
+    }
+    if(reach_box(st, kExtRegion, a.S[2], lo2, hi2)) {
+        tx2 = (unsigned)(hi2[0] - lo2[0] + 32) / 32; ty2 = (unsigned)(hi2[1] - lo2[1] + 8) / 8;
+        n2 = tx2 * ty2 * (unsigned)(hi2[2] - lo2[2] + 1);
+    }
+    const unsigned n01 = n0 + n1, total = n01 + n2;
+    float m = 0.f;
+    for(unsigned t = blockIdx.x; t < total; t += gridDim.x) {
+        float v;
+        if(t < n0) v = ext_tile<0>(a, st, t, lo0, hi0, tx0, ty0);
+        else if(t < n01) v = ext_tile<1>(a, st, t - n0, lo1, hi1, tx1, ty1);
+        else v = ext_tile<2>(a, st, t - n01, lo2, hi2, tx2, ty2);
+        m = fmaxf(m, v);
+    }
+    if(a.mode == 2) {
         __shared__ float sm[8];
         for(int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
         if((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
@@ -1426,23 +1459,24 @@ void launch_maxabs(const float* a, size_t n, unsigned* maxBits, cudaStream_t s) 
 // and v = 0 - gravityDt (A holds 0 there).
 void launch_extrapolate(const GridDesc& g, float* const* A, uint8_t* const* VA, float* const* B, uint8_t* const* VB,
                         int lastMode, float* const* oldOut, float gravityDt, DevState* st, cudaStream_t s) {
-    for(int d = 0; d < 3; ++d) {
-        int sx = face_sx(g, d), sy = face_sy(g, d), sz = face_sz(g, d);
-        size_t nf = (size_t)sx * sy * sz;
-        for(int layer = 0; layer < 4; ++layer) {
-            const float* gin = (layer % 2 == 0) ? A[d] : B[d];
-            const uint8_t* vin = (layer % 2 == 0) ? VA[d] : VB[d];
-            float* gout = (layer % 2 == 0) ? B[d] : A[d];
-            uint8_t* vout = (layer % 2 == 0) ? VB[d] : VA[d];
-            int mode = layer == 3 ? lastMode : 0;
-            float gdt = (mode == 1 && d == 1) ? gravityDt : 0.f;
-            if(mode == 1) {
+    for(int layer = 0; layer < 4; ++layer) {
+        ExtLayer a;
+        a.mode = layer == 3 ? lastMode : 0;
+        for(int d = 0; d < 3; ++d) {
+            a.S[d][0] = face_sx(g, d); a.S[d][1] = face_sy(g, d); a.S[d][2] = face_sz(g, d);
+            const size_t nf = (size_t)a.S[d][0] * a.S[d][1] * a.S[d][2];
+            a.gin[d] = (layer % 2 == 0) ? A[d] : B[d];
+            a.vin[d] = (layer % 2 == 0) ? VA[d] : VB[d];
+            a.gout[d] = (layer % 2 == 0) ? B[d] : A[d];
+            a.vout[d] = (layer % 2 == 0) ? VB[d] : VA[d];
+            a.oldOut[d] = oldOut ? oldOut[d] : nullptr;
+            a.gdt[d] = (a.mode == 1 && d == 1) ? gravityDt : 0.f;
+            if(a.mode == 1) {
                 cudaMemsetAsync(oldOut[d], 0, nf * sizeof(float), s);
-                if(gdt != 0.f) { k_fill<<<kRegionBlocks, 256, 0, s>>>(gout, nf, 0.f - gdt); bnn_note_launch(); }
+                if(a.gdt[d] != 0.f) { k_fill<<<kRegionBlocks, 256, 0, s>>>(a.gout[d], nf, 0.f - a.gdt[d]); bnn_note_launch(); }
             }
-            { k_extrapolate<<<kRegionBlocks, 256, 0, s>>>(sx, sy, sz, gin, vin, gout, vout, mode,
-                                                         oldOut ? oldOut[d] : nullptr, gdt, st); bnn_note_launch(); }
         }
+        { k_extrapolate3<<<kRegionBlocks, 256, 0, s>>>(a, st); bnn_note_launch(); }
     }
 }
 void launch_fluid_sdf(const GridDesc& g, const uint32_t* cellStart, const float4* rec, size_t stride, float* phi,
