@@ -77,19 +77,61 @@ def _config(pcg_mode: str, cfg: dict | None = None, pcg_text: str | None = None)
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region"""
+    """SM clocks and clock-event (throttle) reasons sampled during the timed region: NVML
+    every 20 ms on the GPU this process computes on (matched by UUID), else nvidia-smi
+    every 200 ms.  Read-only: nothing here changes a GPU setting."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits (nvmlClocksEventReason*)
+    REASON_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+                   "hw_thermal_slowdown": 0x40, "hw_power_brake_slowdown": 0x80}
 
     def __init__(self, gpu: int):
         self.gpu = gpu
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.f = None
         self.p = None
+        self.nvml = None
+        self.samples = []
+        self.stop_evt = None
+        self.thread = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        try:
+            uuid = str(torch.cuda.get_device_properties(self.gpu).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
 
     def start(self):
         try:
+            import threading
+            nv, h = self._nvml_handle()
+            reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            self.nvml = nv
+            self.stop_evt = threading.Event()
+
+            def run():
+                while not self.stop_evt.is_set():
+                    try:
+                        self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), mx, int(reasons(h))))
+                    except Exception:
+                        pass
+                    self.stop_evt.wait(0.02)
+
+            self.thread = threading.Thread(target=run, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.nvml = None
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
                                        "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
                                       stderr=subprocess.DEVNULL)
@@ -97,6 +139,14 @@ class ClockSampler:
             self.p = None
 
     def stop(self) -> dict:
+        if self.nvml is not None:
+            self.stop_evt.set()
+            self.thread.join(timeout=5)
+            sm = [float(c) for c, _, _ in self.samples]
+            mx = [float(m) for _, m, _ in self.samples]
+            reasons = {name for _, _, bits in self.samples for name, b in self.REASON_BITS.items() if bits & b}
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                    "reasons": sorted(reasons), "samples": len(sm), "source": "nvml, 20 ms"}
         if self.p is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.p.terminate()
@@ -120,7 +170,7 @@ class ClockSampler:
                     reasons.add(name)
         os.unlink(self.f.name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
 def _peaks():
