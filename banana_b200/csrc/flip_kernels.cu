@@ -700,7 +700,7 @@ __device__ __forceinline__ bool reach_box(const DevState* st, int reach, const i
 // 505-511) to the v component; beyond the region the host has already written the
 // backup 0 and the velocity 0 - gravityDt.  mode 2 (last layer after projection): folds
 // max|u| into the CFL reduction (PIC_Solver.cpp:342-349).
-// The blocks stride over 32 x 8 tiles of the region boxes only.
+// The blocks stride over tiles of 8 rows of the region boxes only.
 // The three components go through a layer in one launch: their region tiles form one
 // index space (32-bit tile arithmetic), so the small per-component regions fill the GPU
 // together.
@@ -715,65 +715,88 @@ struct ExtLayer {
     int mode;
 };
 
+// The region box of component D (faces within kExtRegion of the occupied-cell box bb,
+// clamped to the array; reach_box) and its tile count: tiles are 8 rows (j) of one k plane.
 template<int D>
-__device__ __forceinline__ float ext_tile(const ExtLayer& a, const DevState* st, unsigned t, const int lo[3],
-                                          const int hi[3], unsigned tx, unsigned ty) {
+__device__ __forceinline__ unsigned ext_box(const ExtLayer& a, const int bb[6], int lo[3], int hi[3], unsigned& ty) {
+#pragma unroll
+    for(int d = 0; d < 3; ++d) {
+        lo[d] = max(bb[d] - kExtRegion, 0);
+        hi[d] = min(bb[3 + d] + kExtRegion, a.S[D][d] - 1);
+        if(hi[d] < lo[d]) { ty = 1; return 0u; }
+    }
+    ty = (unsigned)(hi[1] - lo[1] + 8) / 8;
+    return ty * (unsigned)(hi[2] - lo[2] + 1);
+}
+
+// One tile, each of its rows walked along x by one warp; returns max |value| written.
+template<int D>
+__device__ __forceinline__ float ext_tile(const ExtLayer& a, unsigned t, const int bb[6]) {
+    int lo[3], hi[3];
+    unsigned ty;
+    ext_box<D>(a, bb, lo, hi, ty);
     const int sx = a.S[D][0], sy = a.S[D][1], sz = a.S[D][2];
-    const int i = lo[0] + (int)(t % tx) * 32 + (int)(threadIdx.x & 31);
-    const int j = lo[1] + (int)((t / tx) % ty) * 8 + (int)(threadIdx.x >> 5);
-    const int k = lo[2] + (int)(t / (tx * ty));
-    if(i > hi[0] || j > hi[1]) return 0.f;
+    const int j = lo[1] + (int)(t % ty) * 8 + (int)(threadIdx.x >> 5);
+    const int k = lo[2] + (int)(t / ty);
+    if(j > hi[1]) return 0.f;
     const float* __restrict__ gin = a.gin[D];
     const uint8_t* __restrict__ vin = a.vin[D];
     const size_t sxy = (size_t)sx * sy;
-    const size_t f = ((size_t)k * sy + j) * sx + i;
-    const int o = bbox_distance(st, i, j, k);
-    float val = gin[f];
-    uint8_t vv = vin[f];
-    if(!vv && o <= kExtFull && i > 0 && i < sx - 1 && j > 0 && j < sy - 1 && k > 0 && k < sz - 1) {
-        float sum = 0.f;
-        unsigned count = 0;
-        if(vin[f + 1]) { sum += gin[f + 1]; ++count; }
-        if(vin[f - 1]) { sum += gin[f - 1]; ++count; }
-        if(vin[f + sx]) { sum += gin[f + sx]; ++count; }
-        if(vin[f - sx]) { sum += gin[f - sx]; ++count; }
-        if(vin[f + sxy]) { sum += gin[f + sxy]; ++count; }
-        if(vin[f - sxy]) { sum += gin[f - sxy]; ++count; }
-        if(count > 0) { val = sum / (float)count; vv = 2; }  // 2: extrapolated in this pass
+    const size_t rowBase = ((size_t)k * sy + j) * sx;
+    // bbox_distance split: the row's distance along y and z, then x per face
+    const int ojk = max(max(max(bb[1] - j, j - bb[4]), max(bb[2] - k, k - bb[5])), 0);
+    const bool interiorJK = j > 0 && j < sy - 1 && k > 0 && k < sz - 1;
+    float m = 0.f;
+    for(int i = lo[0] + (int)(threadIdx.x & 31); i <= hi[0]; i += 32) {
+        const size_t f = rowBase + i;
+        const int o = max(ojk, max(bb[0] - i, i - bb[3]));
+        float val = gin[f];
+        uint8_t vv = vin[f];
+        if(!vv && o <= kExtFull && interiorJK && i > 0 && i < sx - 1) {
+            float sum = 0.f;
+            unsigned count = 0;
+            if(vin[f + 1]) { sum += gin[f + 1]; ++count; }
+            if(vin[f - 1]) { sum += gin[f - 1]; ++count; }
+            if(vin[f + sx]) { sum += gin[f + sx]; ++count; }
+            if(vin[f - sx]) { sum += gin[f - sx]; ++count; }
+            if(vin[f + sxy]) { sum += gin[f + sxy]; ++count; }
+            if(vin[f - sxy]) { sum += gin[f - sxy]; ++count; }
+            if(count > 0) { val = sum / (float)count; vv = 2; }  // 2: extrapolated in this pass
+        }
+        a.vout[D][f] = vv;
+        if(a.mode == 1) {
+            a.oldOut[D][f] = val;
+            a.gout[D][f] = val - a.gdt[D];
+        } else {
+            a.gout[D][f] = val;
+        }
+        m = fmaxf(m, fabsf(val));
     }
-    a.vout[D][f] = vv;
-    if(a.mode == 1) {
-        a.oldOut[D][f] = val;
-        a.gout[D][f] = val - a.gdt[D];
-    } else {
-        a.gout[D][f] = val;
-    }
-    return fabsf(val);
+    return m;
 }
 
 __global__ void __launch_bounds__(256, 8) k_extrapolate3(ExtLayer a, DevState* st) {
-    int lo0[3], hi0[3], lo1[3], hi1[3], lo2[3], hi2[3];
-    unsigned tx0 = 1, ty0 = 1, n0 = 0, tx1 = 1, ty1 = 1, n1 = 0, tx2 = 1, ty2 = 1, n2 = 0;
-    if(reach_box(st, kExtRegion, a.S[0], lo0, hi0)) {
-        tx0 = (unsigned)(hi0[0] - lo0[0] + 32) / 32; ty0 = (unsigned)(hi0[1] - lo0[1] + 8) / 8;
-        n0 = tx0 * ty0 * (unsigned)(hi0[2] - lo0[2] + 1);
-    }
-    if(reach_box(st, kExtRegion, a.S[1], lo1, hi1)) {
-        tx1 = (unsigned)(hi1[0] - lo1[0] + 32) / 32; ty1 = (unsigned)(hi1[1] - lo1[1] + 8) / 8;
-        n1 = tx1 * ty1 * (unsigned)(hi1[2] - lo1[2] + 1);
-    }
-    if(reach_box(st, kExtRegion, a.S[2], lo2, hi2)) {
-        tx2 = (unsigned)(hi2[0] - lo2[0] + 32) / 32; ty2 = (unsigned)(hi2[1] - lo2[1] + 8) / 8;
-        n2 = tx2 * ty2 * (unsigned)(hi2[2] - lo2[2] + 1);
-    }
-    const unsigned n01 = n0 + n1, total = n01 + n2;
+    int bb[6];
+#pragma unroll
+    for(int q = 0; q < 6; ++q) bb[q] = st->bbox[q];
     float m = 0.f;
-    for(unsigned t = blockIdx.x; t < total; t += gridDim.x) {
-        float v;
-        if(t < n0) v = ext_tile<0>(a, st, t, lo0, hi0, tx0, ty0);
-        else if(t < n01) v = ext_tile<1>(a, st, t - n0, lo1, hi1, tx1, ty1);
-        else v = ext_tile<2>(a, st, t - n01, lo2, hi2, tx2, ty2);
-        m = fmaxf(m, v);
+    if(bb[3] >= bb[0]) {  // no particles: nothing changes
+        unsigned n0, n1, n2;
+        {
+            int lo[3], hi[3];
+            unsigned ty;
+            n0 = ext_box<0>(a, bb, lo, hi, ty);
+            n1 = ext_box<1>(a, bb, lo, hi, ty);
+            n2 = ext_box<2>(a, bb, lo, hi, ty);
+        }
+        const unsigned n01 = n0 + n1, total = n01 + n2;
+        for(unsigned t = blockIdx.x; t < total; t += gridDim.x) {
+            float v;
+            if(t < n0) v = ext_tile<0>(a, t, bb);
+            else if(t < n01) v = ext_tile<1>(a, t - n0, bb);
+            else v = ext_tile<2>(a, t - n01, bb);
+            m = fmaxf(m, v);
+        }
     }
     if(a.mode == 2) {
         __shared__ float sm[8];
