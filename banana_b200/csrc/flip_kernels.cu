@@ -999,33 +999,36 @@ __global__ void __launch_bounds__(256) k_update_velocity(GridDesc g, const DevSt
     const int S[3] = {g.G[0] + (D == 0), g.G[1] + (D == 1), g.G[2] + (D == 2)};
     int lo[3], hi[3];
     if(!reach_box(st, 2, S, lo, hi)) return;
-    const int tx = (hi[0] - lo[0] + 32) / 32, ty = (hi[1] - lo[1] + 8) / 8, tz = hi[2] - lo[2] + 1;
-    const long long nt = (long long)tx * ty * tz;
+    // tiles of 8 rows (j) of one k plane; a warp walks its row along x
+    const unsigned ty = (unsigned)(hi[1] - lo[1] + 8) / 8, nt = ty * (unsigned)(hi[2] - lo[2] + 1);
     const int amax = g.G[D];
-    for(long long t = blockIdx.x; t < nt; t += gridDim.x) {
-        const int i = lo[0] + (int)(t % tx) * 32 + (int)(threadIdx.x & 31);
-        const int j = lo[1] + (int)((t / tx) % ty) * 8 + (int)(threadIdx.x >> 5);
-        const int k = lo[2] + (int)(t / ((long long)tx * ty));
-        if(i > hi[0] || j > hi[1]) continue;
-        const size_t f = ((size_t)k * S[1] + j) * S[0] + i;
-        const int a = D == 0 ? i : (D == 1 ? j : k);
-        float out = 0.f;
-        uint8_t vv = 0;
-        if(a > 0 && a < amax) {
-            const size_t c = ((size_t)k * g.G[1] + j) * g.G[0] + i;
-            const size_t step = D == 0 ? 1 : (D == 1 ? (size_t)g.G[0] : (size_t)g.G[0] * g.G[1]);
-            const size_t cm = c - step;
-            const float pc = phi[c], pm = phi[cm];
-            if((pc < 0.f || pm < 0.f) && (!weight || weight[f] > 0.f)) {
-                const float prc = pc < 0.f ? pressure[aidx[c]] : 0.f;
-                const float prm = pm < 0.f ? pressure[aidx[cm]] : 0.f;
-                const float th = smax(0.01f, fraction_inside(pm, pc));
-                out = velIn[f] - dt * (prc - prm) / th;
-                vv = 1;
+    const size_t step = D == 0 ? 1 : (D == 1 ? (size_t)g.G[0] : (size_t)g.G[0] * g.G[1]);
+    for(unsigned t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int j = lo[1] + (int)(t % ty) * 8 + (int)(threadIdx.x >> 5);
+        const int k = lo[2] + (int)(t / ty);
+        if(j > hi[1]) continue;
+        const size_t fRow = ((size_t)k * S[1] + j) * S[0];
+        const size_t cRow = ((size_t)k * g.G[1] + j) * g.G[0];
+        for(int i = lo[0] + (int)(threadIdx.x & 31); i <= hi[0]; i += 32) {
+            const size_t f = fRow + i;
+            const int a = D == 0 ? i : (D == 1 ? j : k);
+            float out = 0.f;
+            uint8_t vv = 0;
+            if(a > 0 && a < amax) {
+                const size_t c = cRow + i;
+                const size_t cm = c - step;
+                const float pc = phi[c], pm = phi[cm];
+                if((pc < 0.f || pm < 0.f) && (!weight || weight[f] > 0.f)) {
+                    const float prc = pc < 0.f ? pressure[aidx[c]] : 0.f;
+                    const float prm = pm < 0.f ? pressure[aidx[cm]] : 0.f;
+                    const float th = smax(0.01f, fraction_inside(pm, pc));
+                    out = velIn[f] - dt * (prc - prm) / th;
+                    vv = 1;
+                }
             }
+            velOut[f] = out;
+            validOut[f] = vv;
         }
-        velOut[f] = out;
-        validOut[f] = vv;
     }
 }
 
