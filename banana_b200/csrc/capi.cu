@@ -149,7 +149,10 @@ static void free_particles(bnn_flip* h) {
 static int reserve_particles(bnn_flip* h, uint32_t n) {
     if(n <= h->cap) return BNN_OK;
     free_particles(h);
-    uint32_t cap = n;
+    // a multiple of 64, so every plane of every particle array starts 256-byte aligned
+    const uint64_t cap64 = ((uint64_t)n + 63u) & ~(uint64_t)63u;
+    if(cap64 > 0xffffffffull) { bnn_set_error("too many particles"); return BNN_ERR_INVALID_ARGUMENT; }
+    uint32_t cap = (uint32_t)cap64;
     size_t st = cap;
     for(int b = 0; b < 2; ++b) {
         BNN_CUDA_CHECK(cudaMalloc(&h->p6[b], 6 * st * sizeof(float)));
@@ -158,7 +161,8 @@ static int reserve_particles(bnn_flip* h, uint32_t n) {
             BNN_CUDA_CHECK(cudaMalloc(&h->C9[b], 9 * st * sizeof(float)));
     }
     BNN_CUDA_CHECK(cudaMalloc(&h->g3, 3 * st * sizeof(float)));
-    BNN_CUDA_CHECK(cudaMalloc(&h->rec, 4 * st * sizeof(float4)));
+    // two spare records: the gathers load records in aligned pairs
+    BNN_CUDA_CHECK(cudaMalloc(&h->rec, (4 * st + 2) * sizeof(float4)));
     BNN_CUDA_CHECK(cudaMalloc(&h->bboxPart, 6 * ((st + 255) / 256) * sizeof(int)));
     BNN_CUDA_CHECK(cudaMalloc(&h->cellOf, st * sizeof(uint32_t)));
     BNN_CUDA_CHECK(cudaMalloc(&h->slot, st * sizeof(uint32_t)));

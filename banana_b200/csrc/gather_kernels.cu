@@ -3,7 +3,7 @@
 // Both read one 16-byte record per candidate particle, written by the sort's gather
 // (flip_kernels.cu, k_gather_particles): the P2G stencil record of the component, or the
 // position.  Tuned on B200 at 256^3 (12.7M particles): 32 x 8 threads per block, columns
-// of 4 outputs, particle loads issued 2 at a time.
+// of 4 outputs, particle records loaded in aligned pairs (one 256-bit load per pair).
 //
 // One thread owns a column of kCol consecutive outputs (faces of one component, or cells)
 // along one axis, on one or two rows of the third axis; the 32 lanes of a warp own 32
@@ -33,9 +33,6 @@ namespace {
 #ifndef BNN_COL_ROWS
 #define BNN_COL_ROWS 8
 #endif
-#ifndef BNN_COL_BATCH
-#define BNN_COL_BATCH 2
-#endif
 #ifndef BNN_P2G_RPT
 #define BNN_P2G_RPT 1
 #endif
@@ -45,11 +42,19 @@ namespace {
 constexpr int kCol = BNN_COL_LEN;     // outputs per thread along the column axis
 constexpr int kLx = 32;               // threads along x
 constexpr int kLr = BNN_COL_ROWS;     // threads along the row axis
-constexpr int kBatch = BNN_COL_BATCH; // particles whose loads are issued together
 // outputs per thread along the row axis: the SDF's cheap candidates gain from sharing
 // rows between two outputs, P2G's heavier ones do not
 constexpr int kRptP2G = BNN_P2G_RPT;
 constexpr int kRptSdf = BNN_SDF_RPT;
+
+// Records q0 and q0 + 1 (q0 even) in one 256-bit load.  The record planes start on
+// 32-byte boundaries (the particle capacity, their stride, is a multiple of 64) and hold
+// two spare records past the last plane, so a pair never leaves the allocation.
+__device__ __forceinline__ void ldg_pair(const float4* p, float4& a, float4& b) {
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+        : "l"(p));
+}
 
 // Does [lo, hi] (per axis) meet the occupied-cell box grown by one cell?
 __device__ __forceinline__ bool near_particles(const DevState* st, const int lo[3], const int hi[3]) {
@@ -119,15 +124,15 @@ __global__ void __launch_bounds__(kLx * kLr) k_p2g_col(GridDesc g, const DevStat
         const uint32_t b = __ldg(cellStart + base + xlo), e = __ldg(cellStart + base + xhi + 1);
         const uint32_t c1 = __ldg(cellStart + base + min(xlo + 1, xhi + 1));
         const uint32_t c2 = __ldg(cellStart + base + min(xlo + 2, xhi + 1));
-        // Particles are taken kBatch at a time: all loads first, then the arithmetic.  A
-        // particle that does not reach an output adds +0 to its sums, which leaves them
-        // unchanged (they start at +0 and can never become -0), so no branch is needed.
-        for(uint32_t q0 = b; q0 < e; q0 += kBatch) {
-            float4 L[kBatch];
+        // Particles are taken in aligned pairs (one 256-bit load; the pair may start one
+        // record before b and end one after e - 1, those slots being masked).  A particle
+        // that does not reach an output adds +0 to its sums, which leaves them unchanged
+        // (they start at +0 and can never become -0), so no branch is needed.
+        for(uint32_t q0 = b & ~1u; q0 < e; q0 += 2) {
+            float4 L[2];
+            ldg_pair(recD + q0, L[0], L[1]);
 #pragma unroll
-            for(int w = 0; w < kBatch; ++w) L[w] = __ldg(recD + min(q0 + (uint32_t)w, e - 1u));
-#pragma unroll
-            for(int w = 0; w < kBatch; ++w) {
+            for(int w = 0; w < 2; ++w) {
                 const uint32_t q = q0 + (uint32_t)w;
                 const int cx = xlo + (q >= c1 ? 1 : 0) + (q >= c2 ? 1 : 0);
                 const float ex = L[w].x, ey = L[w].y, ez = L[w].z;
@@ -137,7 +142,7 @@ __global__ void __launch_bounds__(kLx * kLr) k_p2g_col(GridDesc g, const DevStat
                 const int sr = rr + (__float_as_int(eR) >> 31);
                 const int sa = ca + (__float_as_int(eA) >> 31);
                 const float fi = fabsf(ex), fr = fabsf(eR), fa = fabsf(eA);
-                const bool reach = (q < e) && (si == i || si == i - 1);
+                const bool reach = (q >= b && q < e) && (si == i || si == i - 1);
                 const float wx = (si == i) ? (1.0f - fi) : fi;
 #pragma unroll
                 for(int ddr = -2; ddr <= 0; ++ddr) {
@@ -237,15 +242,15 @@ __global__ void __launch_bounds__(kLx * kLr) k_fluid_sdf_col(GridDesc g, const D
             if(jj < 0 || jj > g.G[1] - 1 || xlo > xhi) continue;
             const size_t base = ((size_t)kk * g.G[1] + jj) * g.G[0];
             const uint32_t b = __ldg(cellStart + base + xlo), e = __ldg(cellStart + base + xhi + 1);
-            for(uint32_t q0 = b; q0 < e; q0 += kBatch) {
-                float4 L[kBatch];
+            for(uint32_t q0 = b & ~1u; q0 < e; q0 += 2) {
+                float4 L[2];
+                ldg_pair(pos + q0, L[0], L[1]);
 #pragma unroll
-                for(int w = 0; w < kBatch; ++w) L[w] = __ldg(pos + min(q0 + (uint32_t)w, e - 1u));
-#pragma unroll
-                for(int w = 0; w < kBatch; ++w) {
+                for(int w = 0; w < 2; ++w) {
                     const float ddx = sxw - L[w].x;
                     const float dxx = ddx * ddx;
-                    bool reach = q0 + (uint32_t)w < e;
+                    const uint32_t q = q0 + (uint32_t)w;
+                    bool reach = q >= b && q < e;
                     int ci = 0, cj = 0, ck = 0;
                     if(exact) {
                         // the particle's own cell (Grid::getGridCoordinate, truncated) and its
