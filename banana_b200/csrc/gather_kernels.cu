@@ -3,7 +3,8 @@
 // Both read one 16-byte record per candidate particle, written by the sort's gather
 // (flip_kernels.cu, k_gather_particles): the P2G stencil record of the component, or the
 // position.  Tuned on B200 at 256^3 (12.7M particles): 32 x 8 threads per block, columns
-// of 4 outputs, particle records loaded in aligned pairs (one 256-bit load per pair).
+// of 4 outputs, particle records loaded in aligned pairs (one 256-bit load per pair), a
+// register budget for 4 blocks per SM (no spills).
 //
 // One thread owns a column of kCol consecutive outputs (faces of one component, or cells)
 // along one axis, on one or two rows of the third axis; the 32 lanes of a warp own 32
@@ -72,7 +73,7 @@ __device__ __forceinline__ bool near_particles(const DevState* st, const int lo[
 // is z for u and v faces and y for w faces (never the component's own axis); the other
 // non-x axis is the thread-row axis.
 template<int D>
-__global__ void __launch_bounds__(kLx * kLr) k_p2g_col(GridDesc g, const DevState* __restrict__ st,
+__global__ void __launch_bounds__(kLx * kLr, 4) k_p2g_col(GridDesc g, const DevState* __restrict__ st,
                                                        const uint32_t* __restrict__ cellStart,
                                                        const float4* __restrict__ rec, size_t stride,
                                                        float* __restrict__ out, uint8_t* __restrict__ valid) {
@@ -200,7 +201,7 @@ __global__ void __launch_bounds__(kLx * kLr) k_p2g_col(GridDesc g, const DevStat
 // The column axis is z.  The range test against the particle's own cell only matters for
 // a particle outside the grid (its own cell differs from the clamped cell it is sorted
 // into); the advection flags that case and the test is then made for every candidate.
-__global__ void __launch_bounds__(kLx * kLr) k_fluid_sdf_col(GridDesc g, const DevState* __restrict__ st,
+__global__ void __launch_bounds__(kLx * kLr, 4) k_fluid_sdf_col(GridDesc g, const DevState* __restrict__ st,
                                                              const uint32_t* __restrict__ cellStart,
                                                              const float4* __restrict__ pos, float* __restrict__ phi) {
     const int i = blockIdx.x * kLx + threadIdx.x;
