@@ -28,7 +28,7 @@ void launch_advect(int n, float* p6, size_t stride, const float* const* U, const
 void launch_cell_histogram(int n, const float* p6, size_t stride, const GridDesc& g, uint32_t* cellOf, uint32_t* slot,
                            uint32_t* count, DevState* st, cudaStream_t s);
 void launch_sort_finish(int n, size_t ncells, uint32_t* cellOf, uint32_t* slot, const uint32_t* cellStart,
-                        uint32_t* order, uint32_t* count, const float* src6, float* dst6, const uint32_t* idSrc,
+                        uint32_t* order, uint32_t* key, uint32_t* count, const float* src6, float* dst6, const uint32_t* idSrc,
                         uint32_t* idDst, const float* cSrc, float* cDst, float* g3, float4* rec, const GridDesc& g,
                         size_t stride, DevState* st, cudaStream_t s);
 void launch_p2g(const GridDesc& g, const uint32_t* cellStart, const float* g3, const float* p6, const float* C9,
@@ -92,7 +92,7 @@ struct bnn_flip {
     int cur = 0;
     float* g3 = nullptr;    // grid coordinates (APIC / AFLIP P2G)
     float4* rec = nullptr;  // per-particle gather records: 3 P2G stencil planes + positions
-    uint32_t *cellOf = nullptr, *slot = nullptr, *order = nullptr;
+    uint32_t *cellOf = nullptr, *slot = nullptr, *order = nullptr, *key = nullptr;
     int* bboxPart = nullptr;  // per-block occupied-cell boxes of the advection
     uint32_t *count = nullptr, *cellStart = nullptr;
     void* scanWs = nullptr;
@@ -139,9 +139,9 @@ static void free_particles(bnn_flip* h) {
         cudaFree(h->p6[b]); cudaFree(h->ids[b]); cudaFree(h->C9[b]);
         h->p6[b] = nullptr; h->ids[b] = nullptr; h->C9[b] = nullptr;
     }
-    cudaFree(h->g3); cudaFree(h->rec); cudaFree(h->bboxPart); cudaFree(h->cellOf); cudaFree(h->slot); cudaFree(h->order); cudaFree(h->aosStage);
+    cudaFree(h->g3); cudaFree(h->rec); cudaFree(h->bboxPart); cudaFree(h->cellOf); cudaFree(h->slot); cudaFree(h->order); cudaFree(h->key); cudaFree(h->aosStage);
     cudaFree(h->aniso);
-    h->g3 = nullptr; h->rec = nullptr; h->bboxPart = nullptr; h->cellOf = h->slot = h->order = nullptr; h->aosStage = nullptr;
+    h->g3 = nullptr; h->rec = nullptr; h->bboxPart = nullptr; h->cellOf = h->slot = h->order = h->key = nullptr; h->aosStage = nullptr;
     h->aniso = nullptr;
     h->cap = 0;
 }
@@ -167,6 +167,7 @@ static int reserve_particles(bnn_flip* h, uint32_t n) {
     BNN_CUDA_CHECK(cudaMalloc(&h->cellOf, st * sizeof(uint32_t)));
     BNN_CUDA_CHECK(cudaMalloc(&h->slot, st * sizeof(uint32_t)));
     BNN_CUDA_CHECK(cudaMalloc(&h->order, st * sizeof(uint32_t)));
+    BNN_CUDA_CHECK(cudaMalloc(&h->key, st * sizeof(uint32_t)));
     BNN_CUDA_CHECK(cudaMalloc(&h->aosStage, 6 * st * sizeof(float)));
     h->cap = cap;
     return BNN_OK;
@@ -296,7 +297,7 @@ static uint64_t device_bytes(const bnn_flip* h) {
     for(int d = 0; d < 3; ++d) b += (uint64_t)h->F[d] * 14u;                       // U, B, O + 2 valid
     b += (uint64_t)h->C * 20u + 8u + scan_workspace_bytes(h->C);                   // count..aidx
     const bool affine = h->P.solver_kind == BNN_SOLVER_APIC || h->P.solver_kind == BNN_SOLVER_AFLIP;
-    b += (uint64_t)h->cap * (168u + (affine ? 72u : 0u));                          // particle arrays
+    b += (uint64_t)h->cap * (172u + (affine ? 72u : 0u));                          // particle arrays
     b += (uint64_t)h->rowCap * 44u;                                                // rows
     b += (uint64_t)h->pcg.cap * (48u + (h->pcg.x64 ? 56u : 0u)) + (uint64_t)h->pcg.nchCap * 40u;
     return b;
@@ -318,7 +319,7 @@ extern "C" int bnn_scene_bytes_estimate(const bnn_params* params, uint32_t n, ui
     const bool affine = params->solver_kind == BNN_SOLVER_APIC || params->solver_kind == BNN_SOLVER_AFLIP;
     const bool fp64 = params->pcg_mode != BNN_PCG_FP32;
     const uint64_t rows = n < C ? n : C;
-    *bytes = F * 14u + C * 24u + (uint64_t)n * (168u + (affine ? 72u : 0u)) + rows * 44u +
+    *bytes = F * 14u + C * 24u + (uint64_t)n * (172u + (affine ? 72u : 0u)) + rows * 44u +
              (rows * 5u / 4u + 4096u) * (48u + (fp64 ? 56u : 0u));
     return BNN_OK;
 }
@@ -569,7 +570,7 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st, const HostIo* io = nullp
     BNN_CUDA_CHECK(exclusive_scan_u32(h->count, h->cellStart, h->C, h->scanWs, s));
     if(io && io->velPending) BNN_CUDA_CHECK(cudaStreamWaitEvent(s, h->io[1], 0));
     const int nxt = 1 - h->cur;
-    launch_sort_finish(n, h->C, h->cellOf, h->slot, h->cellStart, h->order, h->count, h->p6[h->cur], h->p6[nxt],
+    launch_sort_finish(n, h->C, h->cellOf, h->slot, h->cellStart, h->order, h->key, h->count, h->p6[h->cur], h->p6[nxt],
                        h->ids[h->cur], h->ids[nxt], affine ? h->C9[h->cur] : nullptr, affine ? h->C9[nxt] : nullptr,
                        h->g3, h->rec, g, h->cap, h->dst, s);
     h->cur = nxt;
@@ -588,7 +589,7 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st, const HostIo* io = nullp
         launch_rebin(n, h->p6[h->cur], h->cap, g, h->cellOf, h->slot, h->count, h->dst, s);
         BNN_CUDA_CHECK(exclusive_scan_u32(h->count, h->cellStart, h->C, h->scanWs, s));
         const int nxt2 = 1 - h->cur;
-        launch_sort_finish(n, h->C, h->cellOf, h->slot, h->cellStart, h->order, h->count, h->p6[h->cur], h->p6[nxt2],
+        launch_sort_finish(n, h->C, h->cellOf, h->slot, h->cellStart, h->order, h->key, h->count, h->p6[h->cur], h->p6[nxt2],
                            h->ids[h->cur], h->ids[nxt2], affine ? h->C9[h->cur] : nullptr,
                            affine ? h->C9[nxt2] : nullptr, h->g3, h->rec, g, h->cap, h->dst, s);
         h->cur = nxt2;
@@ -798,7 +799,7 @@ extern "C" int bnn_flip_anisotropic_kernels(bnn_flip* h, const bnn_aniso_params*
     launch_rebin(n, h->p6[h->cur], h->cap, g, h->cellOf, h->slot, h->count, h->dst, s);
     BNN_CUDA_CHECK(exclusive_scan_u32(h->count, h->cellStart, h->C, h->scanWs, s));
     const int nxt = 1 - h->cur;
-    launch_sort_finish(n, h->C, h->cellOf, h->slot, h->cellStart, h->order, h->count, h->p6[h->cur], h->p6[nxt],
+    launch_sort_finish(n, h->C, h->cellOf, h->slot, h->cellStart, h->order, h->key, h->count, h->p6[h->cur], h->p6[nxt],
                        h->ids[h->cur], h->ids[nxt], affine ? h->C9[h->cur] : nullptr, affine ? h->C9[nxt] : nullptr,
                        h->g3, h->rec, g, h->cap, h->dst, s);
     h->cur = nxt;

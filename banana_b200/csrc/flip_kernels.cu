@@ -398,12 +398,17 @@ __global__ void k_cell_histogram(int n, const float* __restrict__ px, const floa
     slot[p] = atomicAdd(count + c, 1u);
 }
 
-// Counting-sort scatter: position of particle p = cellStart[cell] + arrival slot
+// Counting-sort scatter: position of particle p = cellStart[cell] + arrival slot; the
+// particle's id goes to the same position of key, so the bucket sort reads its keys
+// contiguously instead of gathering them through order.
 __global__ void k_scatter_index(int n, const uint32_t* __restrict__ cellOf, const uint32_t* __restrict__ slot,
-                                const uint32_t* __restrict__ cellStart, uint32_t* __restrict__ order) {
+                                const uint32_t* __restrict__ cellStart, const uint32_t* __restrict__ ids,
+                                uint32_t* __restrict__ order, uint32_t* __restrict__ key) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if(p >= n) return;
-    order[cellStart[cellOf[p]] + slot[p]] = (uint32_t)p;
+    const uint32_t pos = cellStart[cellOf[p]] + slot[p];
+    order[pos] = (uint32_t)p;
+    key[pos] = ids[p];
 }
 
 // Arrival slots come from atomics, so each cell's bucket is put back into ascending
@@ -415,13 +420,14 @@ __global__ void k_scatter_index(int n, const uint32_t* __restrict__ cellOf, cons
 // issued at once, then an odd-even transposition network (the ids are distinct, padding
 // sorts last) puts them in order; larger buckets use an insertion sort in memory.
 template<int N>
-__device__ __forceinline__ void sort_bucket_regs(uint32_t* __restrict__ order, const uint32_t* __restrict__ ids,
+__device__ __forceinline__ void sort_bucket_regs(uint32_t* __restrict__ order, const uint32_t* __restrict__ key,
                                                  uint32_t b, uint32_t cnt) {
     uint32_t s[N], k[N];
 #pragma unroll
-    for(int q = 0; q < N; ++q) s[q] = (uint32_t)q < cnt ? order[b + q] : 0u;
-#pragma unroll
-    for(int q = 0; q < N; ++q) k[q] = (uint32_t)q < cnt ? __ldg(ids + s[q]) : 0xffffffffu;
+    for(int q = 0; q < N; ++q) {
+        s[q] = (uint32_t)q < cnt ? order[b + q] : 0u;
+        k[q] = (uint32_t)q < cnt ? key[b + q] : 0xffffffffu;
+    }
 #pragma unroll
     for(int round = 0; round < N; ++round) {
 #pragma unroll
@@ -440,7 +446,7 @@ __device__ __forceinline__ void sort_bucket_regs(uint32_t* __restrict__ order, c
 // Buckets of up to 16 particles are sorted in registers; larger ones (particles crowding
 // into a cell, e.g. against a boundary) are listed for k_sort_large.
 __global__ void k_sort_buckets(int ncells, const uint32_t* __restrict__ cellStart, uint32_t* __restrict__ order,
-                               const uint32_t* __restrict__ ids, uint32_t* __restrict__ count,
+                               const uint32_t* __restrict__ key, uint32_t* __restrict__ count,
                                uint32_t* __restrict__ largeList, DevState* st) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if(c >= ncells) return;
@@ -448,8 +454,8 @@ __global__ void k_sort_buckets(int ncells, const uint32_t* __restrict__ cellStar
     count[c] = 0u;
     const uint32_t cnt = e - b;
     if(cnt < 2) return;
-    if(cnt <= 8) { sort_bucket_regs<8>(order, ids, b, cnt); return; }
-    if(cnt <= 16) { sort_bucket_regs<16>(order, ids, b, cnt); return; }
+    if(cnt <= 8) { sort_bucket_regs<8>(order, key, b, cnt); return; }
+    if(cnt <= 16) { sort_bucket_regs<16>(order, key, b, cnt); return; }
     largeList[atomicAdd(&st->nlarge, 1u)] = (uint32_t)c;
 }
 
@@ -1405,12 +1411,12 @@ void launch_cell_histogram(int n, const float* p6, size_t stride, const GridDesc
 // cellOf and slot are free once the index is scattered: slot lists the crowded buckets,
 // cellOf holds their unsorted order while k_sort_large rewrites them
 void launch_sort_finish(int n, size_t ncells, uint32_t* cellOf, uint32_t* slot, const uint32_t* cellStart,
-                        uint32_t* order, uint32_t* count, const float* src6, float* dst6, const uint32_t* idSrc,
+                        uint32_t* order, uint32_t* key, uint32_t* count, const float* src6, float* dst6, const uint32_t* idSrc,
                         uint32_t* idDst, const float* cSrc, float* cDst, float* g3, float4* rec, const GridDesc& g,
                         size_t stride, DevState* st, cudaStream_t s) {
-    if(n > 0) { k_scatter_index<<<nblk(n), 256, 0, s>>>(n, cellOf, slot, cellStart, order); bnn_note_launch(); }
+    if(n > 0) { k_scatter_index<<<nblk(n), 256, 0, s>>>(n, cellOf, slot, cellStart, idSrc, order, key); bnn_note_launch(); }
     cudaMemsetAsync(&st->nlarge, 0, sizeof(unsigned), s);
-    { k_sort_buckets<<<nblk(ncells), 256, 0, s>>>((int)ncells, cellStart, order, idSrc, count, slot, st); bnn_note_launch(); }
+    { k_sort_buckets<<<nblk(ncells), 256, 0, s>>>((int)ncells, cellStart, order, key, count, slot, st); bnn_note_launch(); }
     if(n > 16) { k_sort_large<<<2 * 148, 256, 0, s>>>(cellStart, order, idSrc, cellOf, slot, st); bnn_note_launch(); }
     if(n > 0)
         { k_gather_particles<<<nblk(n), 256, 0, s>>>(n, order, src6, dst6, idSrc, idDst, cSrc, cDst, g3, rec, g, stride); bnn_note_launch(); }
