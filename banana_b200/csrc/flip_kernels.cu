@@ -241,7 +241,7 @@ __device__ __forceinline__ void histogram_slot(uint32_t c, int p, uint32_t* __re
     slot[p] = base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
 }
 
-__global__ void __launch_bounds__(256) k_advect(int n, float* __restrict__ px, float* __restrict__ py,
+__global__ void __launch_bounds__(256, 6) k_advect(int n, float* __restrict__ px, float* __restrict__ py,
                                                 float* __restrict__ pz, const float* __restrict__ u,
                                                 const float* __restrict__ v, const float* __restrict__ w, GridDesc g,
                                                 float sub, int steps, uint32_t* __restrict__ cellOf,
@@ -445,7 +445,7 @@ __device__ __forceinline__ void sort_bucket_regs(uint32_t* __restrict__ order, c
 
 // Buckets of up to 16 particles are sorted in registers; larger ones (particles crowding
 // into a cell, e.g. against a boundary) are listed for k_sort_large.
-__global__ void k_sort_buckets(int ncells, const uint32_t* __restrict__ cellStart, uint32_t* __restrict__ order,
+__global__ void __launch_bounds__(256, 6) k_sort_buckets(int ncells, const uint32_t* __restrict__ cellStart, uint32_t* __restrict__ order,
                                const uint32_t* __restrict__ key, uint32_t* __restrict__ count,
                                uint32_t* __restrict__ largeList, DevState* st) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
