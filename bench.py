@@ -56,9 +56,9 @@ METRIC = "particle-steps/s at 256^3 FLIP (1e-6 rel residual)"
 UNIT = "particle-steps/s"
 WORKLOAD = "flip_dam_break_256"
 # DRAM bytes (read + write) per PCG iteration of k_pcg_persistent at 1.59M rows, from the ncu
-# capture summarised in profiles/k_pcg_persistent_box_1591812_rows.md (1,054.0 MB over 300
+# capture summarised in profiles/k_pcg_persistent_box_1591812_rows.md (835.7 MB over 300
 # iterations); a launch's traffic is this times its iterations
-PCG_TRAFFIC_PER_ITER = 1054.0e6 / 300
+PCG_TRAFFIC_PER_ITER = 835.7e6 / 300
 
 
 def _config(pcg_mode: str, cfg: dict | None = None, pcg_text: str | None = None):
