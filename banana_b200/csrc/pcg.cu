@@ -255,11 +255,10 @@ __device__ __forceinline__ VT s_val(const VT* z, const VT* sOld, VT beta, bool f
 
 // Resident blocks per SM the register budget is sized for, and rows per lane whose loads
 // are in flight together in the SpMV phase (a divisor of kPerLane).  With the chunk's row
-// records loaded before its neighbour loads, FP32 vectors run best at three blocks of two
-// rows (1.59M rows: 22.9 us per iteration against 23.5 at two blocks of four rows and 23.9
-// at two blocks of two).  FP64 vectors run best at two blocks with four rows (44.6 against
-// 45.6 at three blocks with two); rows with off-diagonal values at three blocks with two
-// rows (38.5 us; two blocks with four rows spill and take 42.6).
+// records loaded before its neighbour loads, three blocks of two rows run best for every
+// vector type (1.59M rows, us per iteration: FP32 22.9 against 23.5 at two blocks of four
+// rows and 23.9 at two blocks of two; FP64 42.1 against 44.5 and 46.8; rows with
+// off-diagonal values 38.5 against 42.6 at two blocks of four rows, which spill).
 #ifndef BNN_PCG_MIN_BLOCKS
 #define BNN_PCG_MIN_BLOCKS 3
 #endif
@@ -267,10 +266,10 @@ __device__ __forceinline__ VT s_val(const VT* z, const VT* sOld, VT beta, bool f
 #define BNN_PCG_ROW_GROUP 2
 #endif
 #ifndef BNN_PCG_MIN_BLOCKS_F64
-#define BNN_PCG_MIN_BLOCKS_F64 2
+#define BNN_PCG_MIN_BLOCKS_F64 3
 #endif
 #ifndef BNN_PCG_ROW_GROUP_F64
-#define BNN_PCG_ROW_GROUP_F64 4
+#define BNN_PCG_ROW_GROUP_F64 2
 #endif
 #ifndef BNN_PCG_MIN_BLOCKS_COEF
 #define BNN_PCG_MIN_BLOCKS_COEF 3
