@@ -252,7 +252,8 @@ int bnn_pcg_solve_7pt(uint32_t n, const float* diag, const int32_t* nbr, float o
  * blocks, so the wait can only end by giving up: after 4096 polls and limit_seconds
  * (0 < limit_seconds <= 10) of wall time, the limit a solve uses being 1 s.
  * *barrier_status receives BNN_ERR_TIMEOUT when the wait gave up as designed, *elapsed_ms
- * how long the block polled.  The device stays usable afterwards. */
+ * how long the block polled.  The device stays usable afterwards.  The probe runs on the
+ * default stream and synchronizes the device, so it is not for use while solves run. */
 int bnn_pcg_barrier_probe(float limit_seconds, int32_t* barrier_status, float* elapsed_ms);
 
 /* Library version / last CUDA error text / number of kernels this library has launched
