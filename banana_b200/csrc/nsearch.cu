@@ -410,13 +410,13 @@ extern "C" int bnn_neighbors(const float* pos_dev, uint32_t n, float radius, uin
 // ---------------------------------------------------------------------------------
 // Cell sort without any device allocation.
 //
-// Some callers cannot allocate device memory at the moment they need a sort: code that
-// runs while a CUDA graph is being captured (cudaMalloc is not capturable), code inside
-// a host callback or a custom allocator's hook, or an embedding application that
-// pre-reserves all device memory and forbids further allocation.  For them this entry
-// point works entirely in a fixed scratch array compiled into the library: every GPU
-// that loads the library holds kNoAllocScratchBytes (about 21 MiB) until the process
-// exits.  Limits: at most kNoAllocMaxPoints points and kNoAllocMaxCells grid cells.
+// Some callers cannot allocate device memory at the moment they need a sort: an
+// application whose own pool allocator has already reserved all device memory, or a loop
+// on a latency budget in which cudaMalloc / cudaFree would synchronise the device and
+// stall the work queued on other streams.  For them this entry point works entirely in a
+// fixed scratch array compiled into the library: every GPU that loads the library holds
+// kNoAllocScratchBytes (about 21 MiB) until the process exits.  Limits: at most
+// kNoAllocMaxPoints points and kNoAllocMaxCells grid cells.
 // ---------------------------------------------------------------------------------
 namespace {
 constexpr uint32_t kNoAllocMaxPoints = 1u << 20;  // 1,048,576 points
@@ -439,16 +439,40 @@ static __device__ __align__(256) unsigned char g_cellSortScratch[kNoAllocScratch
 
 namespace {
 std::mutex g_noallocMutex;
-void* g_noallocPtr[64] = {};  // device address of g_cellSortScratch, per device ordinal
+// device address of g_cellSortScratch per device ordinal, and the id of the context it
+// was resolved in (a reset device gets a new context, in which the module -- and so the
+// array -- can sit at another address)
+void* g_noallocPtr[64] = {};
+unsigned long long g_noallocCtx[64] = {};
 
-// First call on a device: resolve the scratch array's device address with that device
-// current.  The host-side symbol is only a stand-in and must never reach a kernel.
+// Id of the current context (cuCtxGetId through the runtime's driver entry point, so the
+// library does not link libcuda); 0 when the driver cannot tell.
+unsigned long long current_context_id() {
+    using GetId = int (*)(void*, unsigned long long*);  // CUresult cuCtxGetId(CUcontext, unsigned long long*)
+    static GetId fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if(cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) != cudaSuccess ||
+           q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return (GetId)f;
+    }();
+    unsigned long long id = 0;
+    if(fn && fn(nullptr, &id) != 0) id = 0;
+    return id;
+}
+
+// First call on a device (or in a new context of it): resolve the scratch array's device
+// address with that device current.  The host-side symbol is only a stand-in and must
+// never reach a kernel.
 int noalloc_scratch(unsigned char** out) {
     int dev = 0;
     BNN_CUDA_CHECK(cudaGetDevice(&dev));
     if(dev < 0 || dev >= 64) return BNN_ERR_NOT_SUPPORTED;
+    // 0 before the runtime made a context current: resolve (which makes it current)
+    const unsigned long long ctx = current_context_id();
     std::lock_guard<std::mutex> lock(g_noallocMutex);
-    if(!g_noallocPtr[dev]) {
+    if(!g_noallocPtr[dev] || ctx == 0 || g_noallocCtx[dev] != ctx) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_cellSortScratch);
         if(e != cudaSuccess || !p) {
@@ -456,6 +480,7 @@ int noalloc_scratch(unsigned char** out) {
             return BNN_ERR_CUDA;
         }
         g_noallocPtr[dev] = p;
+        g_noallocCtx[dev] = current_context_id();
     }
     *out = (unsigned char*)g_noallocPtr[dev];
     return BNN_OK;

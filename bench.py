@@ -55,8 +55,8 @@ N_GRID = 256
 METRIC = "particle-steps/s at 256^3 FLIP (1e-6 rel residual)"
 UNIT = "particle-steps/s"
 WORKLOAD = "flip_dam_break_256"
-# DRAM bytes (read + write) per PCG iteration of k_pcg_persistent at 1.59M rows, from the ncu
-# capture summarised in profiles/k_pcg_persistent_box_1591812_rows.md (835.7 MB over 300
+# DRAM bytes (read + write) per PCG iteration of k_pcg_persistent at 1.59M rows, from an ncu
+# capture of the standalone solve at that row count (`--workload pcg`: 835.7 MB over 300
 # iterations); a launch's traffic is this times its iterations
 PCG_TRAFFIC_PER_ITER = 835.7e6 / 300
 
@@ -181,6 +181,32 @@ def _peaks():
     return 6650.0, "fallback"
 
 
+def stage_bytes(npart: int, G: int, rows: float, iters: float) -> dict:
+    """Algorithmic bytes of one sub-step's stages (each array touched once per stage, FP32):
+    Np particles, C = G^3 cells, F = 3 (G+1) G^2 faces, A active rows, K PCG iterations.
+    The G2P and the next move share one entry (the particle pass: grid-to-particle blend,
+    RK2 advection, box projection); extrapolation counts 10 F per call (4 layers fused),
+    the first call with the 4 F backup of the FLIP old velocities."""
+    C = float(G) ** 3
+    F = 3.0 * (G + 1) * float(G) ** 2
+    Np, A = float(npart), float(rows)
+    return {"sort": 72.0 * Np + 12.0 * C, "p2g": 24.0 * Np + 5.0 * F, "extrapolate": 10.0 * F + 4.0 * F,
+            "fluid_sdf": 12.0 * Np + 4.0 * C, "system": 8.0 * C + 28.0 * A, "pcg": 52.0 * A * iters,
+            "update": 9.0 * F + 4.0 * A + 10.0 * F, "move+g2p": 48.0 * Np + 8.0 * F}
+
+
+def _stage_gbs(npart, G, stats, stage_tot):
+    """Achieved GB/s of each stage: its algorithmic bytes (stage_bytes, with the measured
+    rows and PCG iterations of every step) over its CUDA-event time."""
+    tot = {}
+    for s in stats:
+        for k, b in stage_bytes(npart, G, s["n_active"], s["pcg_iterations"]).items():
+            tot[k] = tot.get(k, 0.0) + b
+    ms = dict(stage_tot)
+    ms["move+g2p"] = stage_tot["move"] + stage_tot["g2p"]
+    return {k: (tot[k] / (ms[k] * 1e-3) / 1e9 if ms.get(k, 0) > 0 else None) for k in tot}
+
+
 def _dist():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -244,9 +270,11 @@ def run_reference(args, ws, rank):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": steps, "warmup": w_done,
             "ms_per_step": dt * 1e3 / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded dam break, seed 42)", "impl": "reference",
-            "config": dict(_config("fp32", pcg_text=("symmetric MIC(0) preconditioner (the reference default)"
-                                                     if precond else "Jacobi") + ", reference order FP32, tol 1e-6 "
-                                                    "max-norm rel"), particles=len(pos)),
+            "config": dict(_config("fp32", cfg) if not precond else
+                           _config("fp32", pcg_text="symmetric MIC(0) preconditioner (the reference default), "
+                                                    f"fp32, tol {cfg['cg_relative_tolerance']:g} max-norm rel"),
+                           particles=len(pos)),
+            "arithmetic": "reference order: FP32 accumulators, serial left-to-right reductions per thread",
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": f"{steps} full sub-steps of the {N_GRID}^3 scene after {w_done} untimed "
                                        f"(oracle port of the reference CPU solver, OpenMP, {threads} threads)"},
@@ -320,13 +348,7 @@ def run_ours(args, ws, rank, local):
     pcg_kernel_ms = sum(s["pcg_kernel_ms"] for s in stats)
     pcg_ms = pcg_kernel_ms if pcg_kernel_ms > 0 else stage_tot["pcg"]
     achieved = pcg_bytes / (pcg_ms * 1e-3) / 1e9 if pcg_ms > 0 else 0.0
-    F = 3 * (N_GRID + 5) * (N_GRID + 4) ** 2
-    C = (N_GRID + 4) ** 3
-    stage_bytes = {"move": 36.0 * npart + 0.0, "sort": 80.0 * npart + 16.0 * C, "p2g": 28.0 * npart + 5.0 * F,
-                   "extrapolate": 4 * 10.0 * F + 4.0 * F, "fluid_sdf": 24.0 * npart + 4.0 * C + 8.0 * C,
-                   "g2p": 36.0 * npart + 8.0 * F}
-    stage_gbs = {k: (stage_bytes[k] * args.steps / (stage_tot[k] * 1e-3) / 1e9 if stage_tot[k] > 0 else None)
-                 for k in stage_bytes}
+    stage_gbs = _stage_gbs(npart, N_GRID + 4, stats, stage_tot)
 
     # end to end: host arrays in pinned memory, H2D + step + D2H per step
     e2e = None
@@ -851,6 +873,25 @@ def run_fp64err(args, ws, rank, local):
     return 0
 
 
+def _spawn_ranks(n: int) -> int:
+    """`--gpus N` (N > 1) run without a launcher: start N ranks of this same command on this
+    node with torch.distributed.run (rendezvous on 127.0.0.1, a free port) and return the
+    launcher's exit status."""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), str(Path(__file__).resolve())] + sys.argv[1:]
+    p = subprocess.Popen(cmd, start_new_session=True)
+    try:
+        return p.wait(timeout=3600)
+    except subprocess.TimeoutExpired:
+        os.killpg(p.pid, 9)
+        p.wait()
+        return 124
+
+
 def main():
     global N_GRID, METRIC, WORKLOAD
     ap = argparse.ArgumentParser()
@@ -873,7 +914,12 @@ def main():
     ap.add_argument("--req-steps", type=int, default=200, help="serve: sub-steps per request")
     ap.add_argument("--time-limit", type=float, default=240.0, help="serve: stop after this many seconds")
     args = ap.parse_args()
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        return _spawn_ranks(args.gpus)
     ws, rank, local = _dist()
+    if ws != args.gpus:
+        print(f"bench.py: --gpus {args.gpus} but the launcher started {ws} ranks", file=sys.stderr)
+        return 2
     N_GRID = args.grid
     if N_GRID != 256:
         # a smaller (profiling) case names its own size

@@ -206,16 +206,19 @@ int bnn_cell_sort(const float* pos_dev, uint32_t n, const float bmin[3], float c
                   uint32_t* cell_id_dev, uint32_t* sorted_idx_dev, uint32_t* cell_start_dev, uint32_t* out_of_range,
                   void* stream);
 
-/* The same cell sort (same outputs, bit for bit) without allocating any device memory:
- * for callers that cannot call cudaMalloc at the point they need the sort -- code that
- * runs while a CUDA graph is being captured, code inside a host callback or an
- * allocator hook, or an application that has reserved all device memory up front.  No
- * counterpart in the reference (its Grid sort is host code).  Scratch lives in a fixed
- * array compiled into the library (about 21 MiB held on every GPU that loads it until
- * the process exits); limits n <= 1,048,576 points and <= 2,097,152 cells, larger sizes
- * return BNN_ERR_CAPACITY.  The first call on a device looks up the array's device
- * address, so make that first call before any stream capture.  All calls share the one
- * array: calls that overlap on the GPU (several streams or host threads at once) race
+/* The same cell sort (same outputs, bit for bit) without allocating any device memory.
+ * No counterpart in the reference (its Grid sort is host code).  It is for callers that
+ * cannot call cudaMalloc when they need a sort: an application whose own pool allocator
+ * has already reserved all device memory (a further cudaMalloc would fail or steal from
+ * the pool), or a loop on a latency budget where cudaMalloc / cudaFree would synchronise
+ * the device and stall work queued on other streams.  The caller still passes the inputs
+ * and outputs; the sort's scratch lives in a fixed array compiled into the library
+ * (about 21 MiB, held on every GPU that loads the library until the process exits).
+ * Limits: n <= 1,048,576 points and <= 2,097,152 cells; larger sizes return
+ * BNN_ERR_CAPACITY.  The first call on a device (and the first after that device's
+ * context was reset) looks up the array's device address, so make that first call before
+ * any stream capture.  Every call uses the one array, which keeps the previous call's
+ * contents: calls that overlap on the GPU (several streams or host threads at once) race
  * and must be serialised by the caller.  Synchronises `stream` before returning. */
 int bnn_cell_sort_noalloc(const float* pos_dev, uint32_t n, const float bmin[3], float cell_size,
                           const int32_t ncells[3], uint32_t* cell_id_dev, uint32_t* sorted_idx_dev,

@@ -11,7 +11,9 @@ import re
 import sys
 from pathlib import Path
 
-src = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference") / "BananaCore/Banana/Grid/_Grid.Test.hpp"
+if len(sys.argv) != 2:
+    sys.exit(f"usage: python {sys.argv[0]} <reference tree>")
+src = Path(sys.argv[1]) / "BananaCore/Banana/Grid/_Grid.Test.hpp"
 text = src.read_text()
 grid = re.search(r"Grid<3, Real> grid\(Vec3r\((\S+)\), Vec3r\((\S+)\), ([0-9.]+)f\)", text)
 ncells = [int(v) for v in re.findall(r"grid\.getNCells\(\)\[\d\] == (\d+)", text)]

@@ -11,7 +11,9 @@ import re
 import sys
 from pathlib import Path
 
-src = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference") / "BananaCore/Banana/NeighborSearch/Morton/Morton3D_LUTs.h"
+if len(sys.argv) != 2:
+    sys.exit(f"usage: python {sys.argv[0]} <reference tree>")
+src = Path(sys.argv[1]) / "BananaCore/Banana/NeighborSearch/Morton/Morton3D_LUTs.h"
 text = src.read_text()
 out = {"source": "BananaCore/Banana/NeighborSearch/Morton/Morton3D_LUTs.h"}
 for axis in "xyz":
