@@ -247,6 +247,12 @@ struct PcgWork {
     double* partMaxD = nullptr;
     int4* rec = nullptr;  // packed grid rows
     float4* coefRow = nullptr;  // packed rows' off-diagonal values (2 per row)
+    // single-reduction solve: row records {r, w, s, 1/diag} (double-buffered; FP32 as
+    // float4, FP64 as 4 doubles) and the partials of both sums and the max (double-buffered)
+    float4* st32[2] = {nullptr, nullptr};
+    double* st64[2] = {nullptr, nullptr};
+    double* cgPart = nullptr;  // [2][2][nchCap]
+    double* cgMax = nullptr;   // [2][nchCap]
     cudaEvent_t ev[2] = {nullptr, nullptr};  // around the persistent launch
 };
 struct PcgOutcome {

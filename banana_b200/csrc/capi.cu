@@ -31,9 +31,13 @@ void launch_sort_finish(int n, size_t ncells, uint32_t* cellOf, uint32_t* slot, 
                         uint32_t* order, uint32_t* key, uint32_t* count, const float* src6, float* dst6, const uint32_t* idSrc,
                         uint32_t* idDst, const float* cSrc, float* cDst, float* g3, float4* rec, const GridDesc& g,
                         size_t stride, DevState* st, cudaStream_t s);
-void launch_p2g(const GridDesc& g, const uint32_t* cellStart, const float* g3, const float* p6, const float* C9,
-                const float4* rec, size_t stride, float* const* out, uint8_t* const* valid, bool affine,
-                const DevState* st, cudaStream_t s);
+void launch_p2g_affine(const GridDesc& g, const uint32_t* cellStart, const float* g3, const float* p6,
+                       const float* C9, size_t stride, float* const* out, uint8_t* const* valid, cudaStream_t s);
+// gather_kernels.cu
+void launch_p2g_sdf(const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float4* rec,
+                    size_t stride, float* const* out, uint8_t* const* valid, float* phi, cudaStream_t s);
+void launch_fluid_sdf_tile(const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float4* rec,
+                           size_t stride, float* phi, cudaStream_t s);
 void launch_advect_grid(const GridDesc& g, float** U, float** B, float dt, cudaStream_t s);
 void launch_maxabs(const float* a, size_t n, unsigned* maxBits, cudaStream_t s);
 void launch_correct_positions(int n, const GridDesc& g, const float* p6, size_t stride, const uint32_t* ids,
@@ -43,8 +47,6 @@ void launch_rebin(int n, const float* p6, size_t stride, const GridDesc& g, uint
                   uint32_t* count, DevState* st, cudaStream_t s);
 void launch_extrapolate(const GridDesc& g, float* const* A, uint8_t* const* VA, float* const* B, uint8_t* const* VB,
                         int lastMode, float* const* oldOut, float gravityDt, DevState* st, cudaStream_t s);
-void launch_fluid_sdf(const GridDesc& g, const uint32_t* cellStart, const float4* rec, size_t stride, float* phi,
-                      const DevState* st, cudaStream_t s);
 void launch_active_flags(const GridDesc& g, const float* phi, uint32_t* flag, DevState* st, cudaStream_t s);
 void launch_active_rows(size_t nc, const uint32_t* flag, const uint32_t* idx, uint32_t* rowCell, cudaStream_t s);
 void launch_build_rows(const GridDesc& g, int nrows, const uint32_t* rowCell, const float* phi, const uint32_t* aidx,
@@ -215,7 +217,9 @@ extern "C" int bnn_flip_create(const bnn_params* params, bnn_flip** out) {
     const bnn_params& P = *params;
     if(!(P.cell_size > 0.f) || P.advection_steps == 0) return BNN_ERR_INVALID_ARGUMENT;
     if(P.solver_kind < 0 || P.solver_kind > 3) return BNN_ERR_NOT_SUPPORTED;
-    if(P.pcg_mode < 0 || P.pcg_mode > 2 || P.preconditioner != BNN_PRECOND_JACOBI) return BNN_ERR_NOT_SUPPORTED;
+    if((P.pcg_mode & ~(BNN_PCG_MODE_MASK | BNN_PCG_TWO_REDUCTIONS)) != 0 || (P.pcg_mode & BNN_PCG_MODE_MASK) > 2 ||
+       P.preconditioner != BNN_PRECOND_JACOBI)
+        return BNN_ERR_NOT_SUPPORTED;
     for(int d = 0; d < 3; ++d) if(!(P.box_max[d] > P.box_min[d])) return BNN_ERR_INVALID_ARGUMENT;
     auto* h = new bnn_flip();
     h->P = P;
@@ -317,7 +321,7 @@ extern "C" int bnn_scene_bytes_estimate(const bnn_params* params, uint32_t n, ui
     const uint64_t C = G[0] * G[1] * G[2];
     const uint64_t F = (G[0] + 1) * G[1] * G[2] + G[0] * (G[1] + 1) * G[2] + G[0] * G[1] * (G[2] + 1);
     const bool affine = params->solver_kind == BNN_SOLVER_APIC || params->solver_kind == BNN_SOLVER_AFLIP;
-    const bool fp64 = params->pcg_mode != BNN_PCG_FP32;
+    const bool fp64 = (params->pcg_mode & BNN_PCG_MODE_MASK) != BNN_PCG_FP32;
     const uint64_t rows = n < C ? n : C;
     *bytes = F * 14u + C * 24u + (uint64_t)n * (172u + (affine ? 72u : 0u)) + rows * 44u +
              (rows * 5u / 4u + 4096u) * (48u + (fp64 ? 56u : 0u));
@@ -608,9 +612,12 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st, const HostIo* io = nullp
     if(kind == BNN_SOLVER_PIC) {
         // PIC_Solver::advanceVelocity (PIC_Solver.cpp:332-338): the grid velocity is advected
         launch_advect_grid(g, h->U, h->B, substep, s);
+    } else if(affine) {
+        launch_p2g_affine(g, h->cellStart, h->g3, h->p6[h->cur], h->C9[h->cur], h->cap, h->U, h->VA, s);
     } else {
-        launch_p2g(g, h->cellStart, h->g3, h->p6[h->cur], affine ? h->C9[h->cur] : nullptr, h->rec, h->cap, h->U,
-                   h->VA, affine, h->dst, s);
+        // FLIP: the three components and the fluid SDF in one pass over the particles (the
+        // SDF reads positions only, so it is final here already)
+        launch_p2g_sdf(g, h->dst, h->cellStart, h->rec, h->cap, h->U, h->VA, h->phi, s);
     }
     cudaEventRecord(h->ev[3], s);
     const float gdt = h->P.apply_gravity ? 9.81f * substep : 0.f;
@@ -633,7 +640,7 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st, const HostIo* io = nullp
     }
     cudaEventRecord(h->ev[4], s);
     // pressure projection (PIC_Solver.cpp:533-539)
-    launch_fluid_sdf(g, h->cellStart, h->rec, h->cap, h->phi, h->dst, s);
+    if(kind != BNN_SOLVER_FLIP) launch_fluid_sdf_tile(g, h->dst, h->cellStart, h->rec, h->cap, h->phi, s);
     if(h->gridBoundary) launch_solid_extend(g, h->nodeSdf, h->phi, s);
     cudaEventRecord(h->ev[5], s);
     launch_active_flags(g, h->phi, h->flag, h->dst, s);
@@ -862,7 +869,9 @@ extern "C" int bnn_pcg_barrier_probe(float limit_seconds, int32_t* barrier_statu
 extern "C" int bnn_pcg_solve_7pt(uint32_t n, const float* diag, const int32_t* nbr, float offdiag, const float* rhs,
                                  float tol, uint32_t max_iter, int32_t mode, float inner_tol, double* x_out,
                                  bnn_pcg_stats* stats) {
-    if(!diag || !nbr || !rhs || !x_out || mode < 0 || mode > 2) return BNN_ERR_INVALID_ARGUMENT;
+    if(!diag || !nbr || !rhs || !x_out || (mode & ~(BNN_PCG_MODE_MASK | BNN_PCG_TWO_REDUCTIONS)) != 0 ||
+       (mode & BNN_PCG_MODE_MASK) > 2)
+        return BNN_ERR_INVALID_ARGUMENT;
     if(!(offdiag <= 0.f)) return BNN_ERR_INVALID_ARGUMENT;
     cudaStream_t s;
     BNN_CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
@@ -918,7 +927,7 @@ extern "C" int bnn_pcg_solve_7pt(uint32_t n, const float* diag, const int32_t* n
     if(rc == BNN_OK) chk(cudaMemsetAsync(dst, 0, sizeof(DevState), s));
     if(rc == BNN_OK) chk(cudaStreamSynchronize(s));
     PcgOutcome po;
-    if(rc == BNN_OK) rc = pcg_reserve(w, (int)n, mode != BNN_PCG_FP32);  // outside the timed region
+    if(rc == BNN_OK) rc = pcg_reserve(w, (int)n, (mode & BNN_PCG_MODE_MASK) != BNN_PCG_FP32);  // outside the timed region
     if(rc == BNN_OK) {
         cudaEventRecord(e0, s);
         rc = pcg_solve(w, (int)n, dRhs, dDiag, dInv, dNbr, nullptr, gridRows, dt, mode, tol, max_iter, inner_tol, tol, dP, dX,

@@ -837,49 +837,6 @@ __global__ void k_fill(float* __restrict__ a, size_t n, float v) {
 }
 
 // ----------------------------------------------------------------------------------
-// Fluid SDF
-// ----------------------------------------------------------------------------------
-// PIC_Solver::computeFluidSDF (PIC_Solver.cpp:601-652) as a gather per cell over the
-// particles of the 3x3x3 neighbouring cells: phi = min(3 dx, min_p |x_c - x_p| - r_sdf),
-// with the particle's own clamped 3x3x3 range test.  min is exact, so this equals the
-// reference's scatter with locks.
-__global__ void __launch_bounds__(256) k_fluid_sdf(GridDesc g, const uint32_t* __restrict__ cellStart,
-                                                   const float* __restrict__ gxs, const float* __restrict__ gys,
-                                                   const float* __restrict__ gzs, const float* __restrict__ pxs,
-                                                   const float* __restrict__ pys, const float* __restrict__ pzs,
-                                                   float* __restrict__ phi) {
-    const size_t nc = (size_t)g.G[0] * g.G[1] * g.G[2];
-    const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if(c >= nc) return;
-    const int i = (int)(c % g.G[0]);
-    const int j = (int)((c / g.G[0]) % g.G[1]);
-    const int k = (int)(c / ((size_t)g.G[0] * g.G[1]));
-    // Grid::getWorldCoordinate(i + 0.5, j + 0.5, k + 0.5) (Grid.h:186-194)
-    const float sxw = ((float)i + 0.5f) * g.dx + g.bmin[0];
-    const float syw = ((float)j + 0.5f) * g.dx + g.bmin[1];
-    const float szw = ((float)k + 0.5f) * g.dx + g.bmin[2];
-    float ph = g.dx * 3.0f;
-    const int xlo = max(i - 1, 0), xhi = min(i + 1, g.G[0] - 1);
-    for(int kk = max(k - 1, 0); kk <= min(k + 1, g.G[2] - 1); ++kk) {
-        for(int jj = max(j - 1, 0); jj <= min(j + 1, g.G[1] - 1); ++jj) {
-            const size_t row = ((size_t)kk * g.G[1] + jj) * g.G[0];
-            const uint32_t b = __ldg(cellStart + row + xlo), e = __ldg(cellStart + row + xhi + 1);
-            for(uint32_t q = b; q < e; ++q) {
-                // the particle's own cell and its clamped 3x3x3 range (PIC_Solver.cpp:633-635)
-                const int ci = (int)__ldg(gxs + q), cj = (int)__ldg(gys + q), ck = (int)__ldg(gzs + q);
-                if(i < max(ci - 1, 0) || i > min(ci + 1, g.G[0] - 1)) continue;
-                if(j < max(cj - 1, 0) || j > min(cj + 1, g.G[1] - 1)) continue;
-                if(k < max(ck - 1, 0) || k > min(ck + 1, g.G[2] - 1)) continue;
-                const float d = sqrtf(length2f(sxw - __ldg(pxs + q), syw - __ldg(pys + q), szw - __ldg(pzs + q)));
-                const float val = d - g.sdfRadius;
-                if(val < ph) ph = val;
-            }
-        }
-    }
-    phi[c] = ph;
-}
-
-// ----------------------------------------------------------------------------------
 // Pressure system
 // ----------------------------------------------------------------------------------
 // Active-cell flags for PIC_Solver::computeSystem's numbering loop (PIC_Solver.cpp:706-712)
@@ -1421,33 +1378,19 @@ void launch_sort_finish(int n, size_t ncells, uint32_t* cellOf, uint32_t* slot, 
     if(n > 0)
         { k_gather_particles<<<nblk(n), 256, 0, s>>>(n, order, src6, dst6, idSrc, idDst, cSrc, cDst, g3, rec, g, stride); bnn_note_launch(); }
 }
-void launch_p2g_col(const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float4* rec,
-                    size_t stride, float* const* out, uint8_t* const* valid, cudaStream_t s);
-void launch_fluid_sdf_col(const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float4* rec,
-                          size_t stride, float* phi, cudaStream_t s);
-
-void launch_p2g(const GridDesc& g, const uint32_t* cellStart, const float* g3, const float* p6, const float* C9,
-                const float4* rec, size_t stride, float* const* out, uint8_t* const* valid, bool affine,
-                const DevState* st, cudaStream_t s) {
-    if(!affine) {
-        launch_p2g_col(g, st, cellStart, rec, stride, out, valid, s);
-        return;
-    }
+// APIC / AFLIP P2G (the affine momentum term), one launch per component; FLIP's P2G is
+// the tiled pass of gather_kernels.cu
+void launch_p2g_affine(const GridDesc& g, const uint32_t* cellStart, const float* g3, const float* p6,
+                       const float* C9, size_t stride, float* const* out, uint8_t* const* valid, cudaStream_t s) {
     const float *gx = g3, *gy = g3 + stride, *gz = g3 + 2 * stride;
     const float *px = p6, *py = p6 + stride, *pz = p6 + 2 * stride;
     for(int d = 0; d < 3; ++d) {
         size_t nf = (size_t)face_sx(g, d) * face_sy(g, d) * face_sz(g, d);
         const float* vd = p6 + (3 + d) * stride;
-        const float* Cd = C9 ? C9 + (size_t)(3 * d) * stride : nullptr;
-        if(affine) {
-            if(d == 0) { k_p2g<0, true><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[0], valid[0]); bnn_note_launch(); }
-            if(d == 1) { k_p2g<1, true><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[1], valid[1]); bnn_note_launch(); }
-            if(d == 2) { k_p2g<2, true><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[2], valid[2]); bnn_note_launch(); }
-        } else {
-            if(d == 0) { k_p2g<0, false><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[0], valid[0]); bnn_note_launch(); }
-            if(d == 1) { k_p2g<1, false><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[1], valid[1]); bnn_note_launch(); }
-            if(d == 2) { k_p2g<2, false><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[2], valid[2]); bnn_note_launch(); }
-        }
+        const float* Cd = C9 + (size_t)(3 * d) * stride;
+        if(d == 0) { k_p2g<0, true><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[0], valid[0]); bnn_note_launch(); }
+        if(d == 1) { k_p2g<1, true><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[1], valid[1]); bnn_note_launch(); }
+        if(d == 2) { k_p2g<2, true><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[2], valid[2]); bnn_note_launch(); }
     }
 }
 // PIC grid advection of all three components; U[d] / B[d] are swapped after each one
@@ -1510,10 +1453,6 @@ void launch_extrapolate(const GridDesc& g, float* const* A, uint8_t* const* VA, 
         }
         { k_extrapolate3<<<kRegionBlocks, 256, 0, s>>>(a, st); bnn_note_launch(); }
     }
-}
-void launch_fluid_sdf(const GridDesc& g, const uint32_t* cellStart, const float4* rec, size_t stride, float* phi,
-                      const DevState* st, cudaStream_t s) {
-    launch_fluid_sdf_col(g, st, cellStart, rec, stride, phi, s);
 }
 void launch_active_flags(const GridDesc& g, const float* phi, uint32_t* flag, DevState* st, cudaStream_t s) {
     size_t nc = (size_t)g.G[0] * g.G[1] * g.G[2];

@@ -1,324 +1,379 @@
-// Column gathers for P2G (non-affine) and the fluid SDF.
+// P2G (non-affine FLIP) and the fluid SDF in one tiled pass over the cell-sorted particles.
 //
-// Both read one 16-byte record per candidate particle, written by the sort's gather
-// (flip_kernels.cu, k_gather_particles): the P2G stencil record of the component, or the
-// position.  Tuned on B200 at 256^3 (12.7M particles): 32 x 8 threads per block, columns
-// of 4 outputs, particle records loaded in aligned pairs (one 256-bit load per pair), a
-// register budget for 4 blocks per SM (no spills).
+// FLIP_Solver::mapParticles2Grid (FLIP_Solver.cpp:57-95) splats every particle onto the 8
+// faces of its trilinear stencil per component with CAS float atomics, so the reference
+// has no fixed summation order.  Here each face's sums are formed in one fixed two-level
+// order, independent of the launch shape:
+//   1. per cell and per face the cell's particles can reach, a partial sum over the cell's
+//      particles in id order (particles are sorted by (cell, id));
+//   2. per face, the partials of its candidate cells added in (y, z, x)-major cell order:
+//      two cells along the component's own axis, three along the others.
+// Both sums start at +0.  The products are the reference's: weight = wx * wy * wz left to
+// right (ArrayHelpers::getCoordinatesAndWeights, ArrayHelpers.cpp:50-76), momentum =
+// weight * v.  The oracle's canonical mode (mapP2GCanonical) sums in the same order.
 //
-// One thread owns a column of kCol consecutive outputs (faces of one component, or cells)
-// along one axis, on one or two rows of the third axis; the 32 lanes of a warp own 32
-// consecutive x positions, so their particle loads fall on a few cache lines.  A face or cell only receives from particles of the
-// cells one step around it, so the thread walks the cell rows around its whole column
-// once (kCol + 2 rows along the column axis instead of 3 per output) and hands every
-// particle to the outputs of the column it can reach.  Rows are walked in linear cell
-// order (z outer, y inner) and particles in sorted order inside a row, so every output
-// sees its particles in exactly the order of the serial reference loop over cell-sorted
-// particles: the sums are bit-identical to the per-output gathers in flip_kernels.cu.
+// The fluid SDF (PIC_Solver::computeFluidSDF, PIC_Solver.cpp:601-652) rides along: per cell
+// the minimum squared distance of its particles to each of the 27 neighbouring cell
+// centres, then per cell the minimum over its 27 neighbours' partials.  min is exact, so
+// this equals the reference's locked scatter bit for bit; sqrtf (correctly rounded) and the
+// radius subtraction are non-decreasing, so one square root per cell gives the minimum of
+// the per-particle distances.
 //
-// The fluid SDF keeps the minimum squared distance instead of the minimum distance:
-// sqrtf (correctly rounded) and the subtraction of the particle radius are both
-// non-decreasing, so min(sqrtf(d2) - r) == sqrtf(min d2) - r exactly, and one square root
-// per cell replaces one per candidate particle.
+// Work layout.  A block owns a tile of kTX x kTZ face columns (x, z) and walks kYC face
+// layers along y, the gravity axis (Earth gravity is -y, ParticleSolverData.cpp:196-200):
+// a liquid piles up in the cells above the floor, and walking y makes every such crowded
+// layer one layer that all columns of every tile share, instead of a long serial walk
+// inside the few tiles that hold the floor.  For each cell layer it needs, the block first
+// forms the partials of the (kTX + 2) x (kTZ + 2) cells that can reach the tile (a 1-cell
+// halo) into shared memory, one component at a time, then every thread adds the partials
+// its faces need to register accumulators for the three face layers the cell layer
+// reaches.  Each particle record is therefore read once per block (plus the halo) instead
+// of once per candidate face, and the weight of a particle is formed once per reached slot.
 //
-// Thread blocks whose column box lies more than one cell away from every particle (the
-// occupied-cell bounding box is reduced during advection) only write the empty values.
+// Input: one 16-byte record per particle and component, written by the sort's gather
+// (flip_kernels.cu, k_gather_particles): plane D < 3 holds {e_x, e_y, e_z, v_D}, e_a the
+// stencil fraction along axis a with the sign bit set when the stencil's base index is the
+// particle's (sorted) cell - 1 instead of the cell itself; plane 3 holds the position.
 #include "bnn_internal.cuh"
+
+#include <atomic>
 
 namespace bnn {
 
 namespace {
-#ifndef BNN_COL_LEN
-#define BNN_COL_LEN 4
+#ifndef BNN_TILE_X
+#define BNN_TILE_X 32
 #endif
-#ifndef BNN_COL_ROWS
-#define BNN_COL_ROWS 8
+#ifndef BNN_TILE_Z
+#define BNN_TILE_Z 8
 #endif
-#ifndef BNN_P2G_RPT
-#define BNN_P2G_RPT 1
+#ifndef BNN_TILE_Y
+#define BNN_TILE_Y 16
 #endif
-#ifndef BNN_SDF_RPT
-#define BNN_SDF_RPT 2
-#endif
-constexpr int kCol = BNN_COL_LEN;     // outputs per thread along the column axis
-constexpr int kLx = 32;               // threads along x
-constexpr int kLr = BNN_COL_ROWS;     // threads along the row axis
-// outputs per thread along the row axis: the SDF's cheap candidates gain from sharing
-// rows between two outputs, P2G's heavier ones do not
-constexpr int kRptP2G = BNN_P2G_RPT;
-constexpr int kRptSdf = BNN_SDF_RPT;
+constexpr int kTX = BNN_TILE_X;            // face columns per block along x (one warp)
+constexpr int kTZ = BNN_TILE_Z;            // ... along z
+constexpr int kYC = BNN_TILE_Y;            // face layers per block along y (the walk)
+constexpr int kThreads = kTX * kTZ;
+constexpr int kHX = kTX + 2, kHZ = kTZ + 2;
+constexpr int kNH = kHX * kHZ;             // cells of one layer whose partials the tile needs
+constexpr int kPartials = 36;              // 18 face slots x (momentum, weight); the SDF has 27
+constexpr size_t kSmemBytes = sizeof(float) * kPartials * kNH;
 
-// Records q0 and q0 + 1 (q0 even) in one 256-bit load.  The record planes start on
-// 32-byte boundaries (the particle capacity, their stride, is a multiple of 64) and hold
-// two spare records past the last plane, so a pair never leaves the allocation.
-__device__ __forceinline__ void ldg_pair(const float4* p, float4& a, float4& b) {
-    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-        : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
-        : "l"(p));
+// Weights along one axis of a component's stencil, by face offset from the particle's
+// cell.  The component's own axis: offsets {0, +1}, the base is always the cell.  Other
+// axes: offsets {-1, 0, +1}; base cell - 1 (sign bit set) reaches offsets -1, 0, base cell
+// reaches 0, +1.  Unreached offsets weigh exactly 0.
+__device__ __forceinline__ void own_axis(float e, float w[2]) {
+    w[0] = 1.0f - e;
+    w[1] = e;
+}
+__device__ __forceinline__ void side_axis(float e, float w[3]) {
+    const bool low = __float_as_int(e) < 0;
+    const float f = fabsf(e);
+    const float a = 1.0f - f;
+    w[0] = low ? a : 0.0f;
+    w[1] = low ? f : a;
+    w[2] = low ? 0.0f : f;
 }
 
-// Does [lo, hi] (per axis) meet the occupied-cell box grown by one cell?
-__device__ __forceinline__ bool near_particles(const DevState* st, const int lo[3], const int hi[3]) {
+struct TileArgs {
+    GridDesc g;
+    const DevState* st;
+    const uint32_t* cellStart;
+    const float4* rec;  // plane stride `stride`
+    size_t stride;
+    float* out[3];
+    uint8_t* valid[3];
+    float* phi;
+};
+
+// Does the cell box [lo, hi] meet the occupied-cell box?
+__device__ __forceinline__ bool meets_particles(const DevState* st, const int lo[3], const int hi[3]) {
 #pragma unroll
     for(int d = 0; d < 3; ++d) {
         const int bl = st->bbox[d], bh = st->bbox[3 + d];
-        if(bh < bl) return false;  // no particles
-        if(hi[d] < bl - 1 || lo[d] > bh + 1) return false;
+        if(bh < bl) return false;
+        if(hi[d] < bl || lo[d] > bh) return false;
     }
     return true;
 }
+
+// Partials of component D for halo cell h of cell layer cy into sm (slot-major planes).
+template<int D>
+__device__ __forceinline__ void cell_partials(const TileArgs& a, int x0, int z0, int cy, int h, float* __restrict__ sm) {
+    constexpr int NX = D == 0 ? 2 : 3, NY = D == 1 ? 2 : 3, NZ = D == 2 ? 2 : 3;
+    constexpr int NS = NX * NY * NZ;
+    float S[NS], W[NS];
+#pragma unroll
+    for(int s = 0; s < NS; ++s) { S[s] = 0.0f; W[s] = 0.0f; }
+    const int cx = x0 - 1 + h % kHX, cz = z0 - 1 + h / kHX;
+    if(cx >= 0 && cx < a.g.G[0] && cz >= 0 && cz < a.g.G[2]) {
+        const size_t c = ((size_t)cz * a.g.G[1] + cy) * a.g.G[0] + cx;
+        const uint32_t b = __ldg(a.cellStart + c), e = __ldg(a.cellStart + c + 1);
+        const float4* __restrict__ recD = a.rec + (size_t)D * a.stride;
+        for(uint32_t q = b; q < e; ++q) {
+            const float4 L = __ldg(recD + q);
+            float wx[NX], wy[NY], wz[NZ];
+            if constexpr(D == 0) own_axis(L.x, wx); else side_axis(L.x, wx);
+            if constexpr(D == 1) own_axis(L.y, wy); else side_axis(L.y, wy);
+            if constexpr(D == 2) own_axis(L.z, wz); else side_axis(L.z, wz);
+#pragma unroll
+            for(int ix = 0; ix < NX; ++ix)
+#pragma unroll
+                for(int iy = 0; iy < NY; ++iy) {
+                    const float wxy = wx[ix] * wy[iy];
+#pragma unroll
+                    for(int iz = 0; iz < NZ; ++iz) {
+                        const int s = (ix * NY + iy) * NZ + iz;
+                        const float w = wxy * wz[iz];
+                        S[s] = S[s] + w * L.w;
+                        W[s] = W[s] + w;
+                    }
+                }
+        }
+    }
+#pragma unroll
+    for(int s = 0; s < NS; ++s) {
+        sm[(2 * s) * kNH + h] = S[s];
+        sm[(2 * s + 1) * kNH + h] = W[s];
+    }
+}
+
+// The face (x0 + tx, z0 + tz) of component D adds the partials of its candidate cells of
+// this layer, cells in ascending (z, x) order, into its accumulators for face layers
+// cy - 1 + j.
+template<int D>
+__device__ __forceinline__ void pull_partials(const float* __restrict__ sm, int tx, int tz, float aS[3], float aW[3]) {
+    constexpr int NX = D == 0 ? 2 : 3, NY = D == 1 ? 2 : 3, NZ = D == 2 ? 2 : 3;
+#pragma unroll
+    for(int izc = 0; izc < NZ; ++izc) {        // cell z = face z - 1 + izc
+        const int oz = 1 - izc;                  // face offset from that cell
+        const int iz = D == 2 ? oz : oz + 1;
+#pragma unroll
+        for(int ixc = 0; ixc < NX; ++ixc) {
+            const int ox = 1 - ixc;
+            const int ix = D == 0 ? ox : ox + 1;
+            const int h = (tz + izc) * kHX + (tx + ixc);
+#pragma unroll
+            for(int j = (D == 1 ? 1 : 0); j < 3; ++j) {
+                const int oy = j - 1;
+                const int iy = D == 1 ? oy : oy + 1;
+                const int s = (ix * NY + iy) * NZ + iz;
+                aS[j] = aS[j] + sm[(2 * s) * kNH + h];
+                aW[j] = aW[j] + sm[(2 * s + 1) * kNH + h];
+            }
+        }
+    }
+}
+
+// Minimum squared distance from the particles of halo cell h (layer cy) to the centres of
+// the 27 cells around it.  exact: a particle outside the grid (sorted into the clamped
+// cell) reaches only the clamped 3x3x3 range of its own cell (PIC_Solver.cpp:633-635).
+__device__ __forceinline__ void sdf_partials(const TileArgs& a, int x0, int z0, int cy, int h, bool exact,
+                                             float* __restrict__ sm) {
+    const float inf = __int_as_float(0x7f800000);
+    float m[27];
+#pragma unroll
+    for(int s = 0; s < 27; ++s) m[s] = inf;
+    const GridDesc& g = a.g;
+    const int cx = x0 - 1 + h % kHX, cz = z0 - 1 + h / kHX;
+    if(cx >= 0 && cx < g.G[0] && cz >= 0 && cz < g.G[2]) {
+        const size_t c = ((size_t)cz * g.G[1] + cy) * g.G[0] + cx;
+        const uint32_t b = __ldg(a.cellStart + c), e = __ldg(a.cellStart + c + 1);
+        const float4* __restrict__ pos = a.rec + 3 * a.stride;
+        // Grid::getWorldCoordinate(i + 0.5, ...) (Grid.h:186-194) of the 27 target cells
+        float sx[3], sy[3], sz[3];
+#pragma unroll
+        for(int o = 0; o < 3; ++o) {
+            sx[o] = ((float)(cx - 1 + o) + 0.5f) * g.dx + g.bmin[0];
+            sy[o] = ((float)(cy - 1 + o) + 0.5f) * g.dx + g.bmin[1];
+            sz[o] = ((float)(cz - 1 + o) + 0.5f) * g.dx + g.bmin[2];
+        }
+        for(uint32_t q = b; q < e; ++q) {
+            const float4 L = __ldg(pos + q);
+            float dxx[3], dyy[3], dzz[3];
+#pragma unroll
+            for(int o = 0; o < 3; ++o) {
+                const float ddx = sx[o] - L.x, ddy = sy[o] - L.y, ddz = sz[o] - L.z;
+                dxx[o] = ddx * ddx;
+                dyy[o] = ddy * ddy;
+                dzz[o] = ddz * ddz;
+            }
+            bool okx[3] = {true, true, true}, oky[3] = {true, true, true}, okz[3] = {true, true, true};
+            if(exact) {
+                const int ci = (int)((L.x - g.bmin[0]) / g.dx);
+                const int cj = (int)((L.y - g.bmin[1]) / g.dx);
+                const int ck = (int)((L.z - g.bmin[2]) / g.dx);
+#pragma unroll
+                for(int o = 0; o < 3; ++o) {
+                    const int tx = cx - 1 + o, ty = cy - 1 + o, tz = cz - 1 + o;
+                    okx[o] = !(tx < max(ci - 1, 0) || tx > min(ci + 1, g.G[0] - 1));
+                    oky[o] = !(ty < max(cj - 1, 0) || ty > min(cj + 1, g.G[1] - 1));
+                    okz[o] = !(tz < max(ck - 1, 0) || tz > min(ck + 1, g.G[2] - 1));
+                }
+            }
+#pragma unroll
+            for(int iz = 0; iz < 3; ++iz)
+#pragma unroll
+                for(int iy = 0; iy < 3; ++iy)
+#pragma unroll
+                    for(int ix = 0; ix < 3; ++ix) {
+                        const float d2 = (dxx[ix] + dyy[iy]) + dzz[iz];  // glm::length2: (x*x + y*y) + z*z
+                        const int s = (iz * 3 + iy) * 3 + ix;
+                        m[s] = fminf(m[s], (okx[ix] && oky[iy] && okz[iz]) ? d2 : inf);
+                    }
+        }
+    }
+#pragma unroll
+    for(int s = 0; s < 27; ++s) sm[s * kNH + h] = m[s];
+}
+
+// Cell (x0 + tx, cy - 1 + j, z0 + tz) takes the minimum over its 9 neighbours of this layer.
+__device__ __forceinline__ void pull_sdf(const float* __restrict__ sm, int tx, int tz, float aM[3]) {
+#pragma unroll
+    for(int izc = 0; izc < 3; ++izc)
+#pragma unroll
+        for(int ixc = 0; ixc < 3; ++ixc) {
+            const int h = (tz + izc) * kHX + (tx + ixc);
+            const int ix = 2 - ixc, iz = 2 - izc;  // offset (target - source) + 1
+#pragma unroll
+            for(int j = 0; j < 3; ++j) {
+                const int s = (iz * 3 + j) * 3 + ix;
+                aM[j] = fminf(aM[j], sm[s * kNH + h]);
+            }
+        }
+}
+
+template<int D>
+__device__ __forceinline__ void write_face(const TileArgs& a, int fx, int fy, int fz, float S, float W) {
+    const int sx = a.g.G[0] + (D == 0), sy = a.g.G[1] + (D == 1), sz = a.g.G[2] + (D == 2);
+    if(fx >= sx || fy >= sy || fz < 0 || fz >= sz) return;
+    const size_t f = ((size_t)fz * sy + fy) * sx + fx;
+    const bool ok = W > FLT_MIN;
+    a.out[D][f] = ok ? S / W : S;
+    a.valid[D][f] = ok ? 1 : 0;
+}
+
+__device__ __forceinline__ void write_phi(const TileArgs& a, int fx, int fy, int fz, float m) {
+    const GridDesc& g = a.g;
+    if(fx >= g.G[0] || fy >= g.G[1] || fz < 0 || fz >= g.G[2]) return;
+    const float empty = g.dx * 3.0f;
+    float ph = empty;
+    if(m != __int_as_float(0x7f800000)) {
+        const float val = sqrtf(m) - g.sdfRadius;
+        if(val < ph) ph = val;
+    }
+    a.phi[((size_t)fz * g.G[1] + fy) * g.G[0] + fx] = ph;
+}
 } // namespace
 
-// FLIP_Solver::mapParticles2Grid (FLIP_Solver.cpp:57-95) for component D.  The column axis
-// is z for u and v faces and y for w faces (never the component's own axis); the other
-// non-x axis is the thread-row axis.
-template<int D>
-__global__ void __launch_bounds__(kLx * kLr, 4) k_p2g_col(GridDesc g, const DevState* __restrict__ st,
-                                                       const uint32_t* __restrict__ cellStart,
-                                                       const float4* __restrict__ rec, size_t stride,
-                                                       float* __restrict__ out, uint8_t* __restrict__ valid) {
-    constexpr int A = (D == 2) ? 1 : 2;  // column axis
-    constexpr int R = (D == 2) ? 2 : 1;  // thread-row axis
-    const int sz[3] = {g.G[0] + (D == 0), g.G[1] + (D == 1), g.G[2] + (D == 2)};
-    const int i = blockIdx.x * kLx + threadIdx.x;
-    const int r0 = (blockIdx.y * kLr + threadIdx.y) * kRptP2G;  // rows r0 .. r0 + kRptP2G - 1
-    const int a0 = blockIdx.z * kCol;
-    auto face_index = [&](int ur, int u) {
-        const int r = r0 + ur;
-        const int fy = (A == 1) ? a0 + u : r, fz = (A == 2) ? a0 + u : r;
-        return ((size_t)fz * sz[1] + fy) * sz[0] + i;
-    };
+// P2G: the three face components and the fluid SDF (FLIP); otherwise the fluid SDF alone.
+template<bool P2G>
+__global__ void __launch_bounds__(kThreads, 3) k_p2g_sdf_tile(TileArgs a) {
+    extern __shared__ float sm[];
+    const GridDesc& g = a.g;
+    const int tx = threadIdx.x, tz = threadIdx.y, t = tz * kTX + tx;
+    const int x0 = blockIdx.x * kTX, z0 = blockIdx.y * kTZ;
+    const int yA = blockIdx.z * kYC, yB = min(yA + kYC, g.G[1] + 1);  // face layers [yA, yB)
+    const int fx = x0 + tx, fz = z0 + tz;
     {
-        int lo[3], hi[3];
-        lo[0] = blockIdx.x * kLx; hi[0] = lo[0] + kLx - 1;
-        lo[R] = blockIdx.y * kLr * kRptP2G; hi[R] = lo[R] + kLr * kRptP2G - 1;
-        lo[A] = a0; hi[A] = a0 + kCol - 1;
-        if(!near_particles(st, lo, hi)) {
-            if(i < sz[0]) {
-#pragma unroll
-                for(int ur = 0; ur < kRptP2G; ++ur)
-#pragma unroll
-                    for(int u = 0; u < kCol; ++u)
-                        if(r0 + ur < sz[R] && a0 + u < sz[A]) { out[face_index(ur, u)] = 0.f; valid[face_index(ur, u)] = 0; }
-            }
-            return;
-        }
-    }
-    float S[kRptP2G][kCol], W[kRptP2G][kCol];
-#pragma unroll
-    for(int ur = 0; ur < kRptP2G; ++ur)
-#pragma unroll
-        for(int u = 0; u < kCol; ++u) { S[ur][u] = 0.f; W[ur][u] = 0.f; }
-    const int xlo = max(i - 1, 0), xhi = min(D == 0 ? i : i + 1, g.G[0] - 1);
-    const float4* __restrict__ recD = rec + (size_t)D * stride;
-
-    // one cell row: A coordinate a0 - 1 + t, R coordinate r0 - 1 + dr.  A face at row
-    // offset ur / column offset u is reached from rows dr in {ur, ur+1, ur+2} (one row
-    // fewer along the component's own axis) and t in {u, u+1, u+2}.
-    auto row = [&](int t, int dr) __attribute__((always_inline)) {
-        const int ca = a0 - 1 + t, rr = r0 - 1 + dr;
-        if(ca < 0 || ca > g.G[A] - 1 || rr < 0 || rr > g.G[R] - 1) return;
-        if(xlo > xhi) return;
-        const int kk = (A == 2) ? ca : rr, jj = (A == 1) ? ca : rr;
-        const size_t base = ((size_t)kk * g.G[1] + jj) * g.G[0];
-        // the row segment holds cells xlo..xhi (at most 3): c1, c2 split it by cell
-        const uint32_t b = __ldg(cellStart + base + xlo), e = __ldg(cellStart + base + xhi + 1);
-        const uint32_t c1 = __ldg(cellStart + base + min(xlo + 1, xhi + 1));
-        const uint32_t c2 = __ldg(cellStart + base + min(xlo + 2, xhi + 1));
-        // Particles are taken in aligned pairs (one 256-bit load; the pair may start one
-        // record before b and end one after e - 1, those slots being masked).  A particle
-        // that does not reach an output adds +0 to its sums, which leaves them unchanged
-        // (they start at +0 and can never become -0), so no branch is needed.
-        for(uint32_t q0 = b & ~1u; q0 < e; q0 += 2) {
-            float4 L[2];
-            ldg_pair(recD + q0, L[0], L[1]);
-#pragma unroll
-            for(int w = 0; w < 2; ++w) {
-                const uint32_t q = q0 + (uint32_t)w;
-                const int cx = xlo + (q >= c1 ? 1 : 0) + (q >= c2 ? 1 : 0);
-                const float ex = L[w].x, ey = L[w].y, ez = L[w].z;
-                const float eR = (R == 1) ? ey : ez, eA = (A == 1) ? ey : ez;
-                // sign bit set: stencil base = cell - 1
-                const int si = cx + (__float_as_int(ex) >> 31);
-                const int sr = rr + (__float_as_int(eR) >> 31);
-                const int sa = ca + (__float_as_int(eA) >> 31);
-                const float fi = fabsf(ex), fr = fabsf(eR), fa = fabsf(eA);
-                const bool reach = (q >= b && q < e) && (si == i || si == i - 1);
-                const float wx = (si == i) ? (1.0f - fi) : fi;
-#pragma unroll
-                for(int ddr = -2; ddr <= 0; ++ddr) {
-                    const int ur = dr + ddr;
-                    if(ur < 0 || ur >= kRptP2G) continue;
-                    const int fr_ = r0 + ur;
-                    const bool okR = reach && (sr == fr_ || sr == fr_ - 1);
-                    const float wr = (sr == fr_) ? (1.0f - fr) : fr;
-                    const float wxr = wx * wr;  // (wx * wy) when the column axis is z
-#pragma unroll
-                    for(int du = -1; du <= 1; ++du) {
-                        const int u = t - 1 + du;
-                        if(u < 0 || u >= kCol) continue;
-                        const int fa_ = a0 + u;
-                        const bool ok = okR && (sa == fa_ || sa == fa_ - 1);
-                        const float wa = (sa == fa_) ? (1.0f - fa) : fa;
-                        // weight = wx * wy * wz, multiplied left to right
-                        const float wgt = (A == 2) ? wxr * wa : (wx * wa) * wr;
-                        const float m = wgt * L[w].w;
-                        S[ur][u] = S[ur][u] + (ok ? m : 0.f);
-                        W[ur][u] = W[ur][u] + (ok ? wgt : 0.f);
-                    }
+        const int lo[3] = {x0 - 1, yA - 1, z0 - 1}, hi[3] = {x0 + kTX, yB, z0 + kTZ};
+        if(!meets_particles(a.st, lo, hi)) {
+            // no particle reaches the tile: empty faces and cells
+            for(int fy = yA; fy < yB; ++fy) {
+                if constexpr(P2G) {
+                    write_face<0>(a, fx, fy, fz, 0.0f, 0.0f);
+                    write_face<1>(a, fx, fy, fz, 0.0f, 0.0f);
+                    write_face<2>(a, fx, fy, fz, 0.0f, 0.0f);
                 }
-            }
-        }
-    };
-    // rows in linear cell order: z outer, y inner
-    constexpr int NR = kRptP2G + (R == D ? 1 : 2);  // row offsets dr = 0 .. NR-1
-    if(A == 2) {
-#pragma unroll
-        for(int t = 0; t < kCol + 2; ++t)
-#pragma unroll
-            for(int dr = 0; dr < NR; ++dr) row(t, dr);
-    } else {
-#pragma unroll
-        for(int dr = 0; dr < NR; ++dr)
-#pragma unroll
-            for(int t = 0; t < kCol + 2; ++t) row(t, dr);
-    }
-    if(i < sz[0]) {
-#pragma unroll
-        for(int ur = 0; ur < kRptP2G; ++ur)
-#pragma unroll
-            for(int u = 0; u < kCol; ++u) {
-                if(r0 + ur >= sz[R] || a0 + u >= sz[A]) continue;
-                const bool ok = W[ur][u] > FLT_MIN;
-                out[face_index(ur, u)] = ok ? S[ur][u] / W[ur][u] : S[ur][u];
-                valid[face_index(ur, u)] = ok ? 1 : 0;
-            }
-    }
-}
-
-// PIC_Solver::computeFluidSDF (PIC_Solver.cpp:601-652): phi of a cell = min(3 dx,
-// min over the particles whose clamped 3x3x3 cell range holds it of |x_cell - x_p| - r).
-// The column axis is z.  The range test against the particle's own cell only matters for
-// a particle outside the grid (its own cell differs from the clamped cell it is sorted
-// into); the advection flags that case and the test is then made for every candidate.
-__global__ void __launch_bounds__(kLx * kLr, 4) k_fluid_sdf_col(GridDesc g, const DevState* __restrict__ st,
-                                                             const uint32_t* __restrict__ cellStart,
-                                                             const float4* __restrict__ pos, float* __restrict__ phi) {
-    const int i = blockIdx.x * kLx + threadIdx.x;
-    const int j0 = (blockIdx.y * kLr + threadIdx.y) * kRptSdf;  // cells j0 .. j0 + kRptSdf - 1
-    const int k0 = blockIdx.z * kCol;
-    const float empty = g.dx * 3.0f;
-    auto cell_index = [&](int uj, int u) { return ((size_t)(k0 + u) * g.G[1] + (j0 + uj)) * g.G[0] + i; };
-    {
-        const int lo[3] = {(int)(blockIdx.x * kLx), (int)(blockIdx.y * kLr * kRptSdf), k0};
-        const int hi[3] = {lo[0] + kLx - 1, lo[1] + kLr * kRptSdf - 1, k0 + kCol - 1};
-        if(!near_particles(st, lo, hi)) {
-            if(i < g.G[0]) {
-#pragma unroll
-                for(int uj = 0; uj < kRptSdf; ++uj)
-#pragma unroll
-                    for(int u = 0; u < kCol; ++u)
-                        if(j0 + uj < g.G[1] && k0 + u < g.G[2]) phi[cell_index(uj, u)] = empty;
+                write_phi(a, fx, fy, fz, __int_as_float(0x7f800000));
             }
             return;
         }
     }
-    const bool exact = (st->flags & BNN_FLAG_OUT_OF_GRID) != 0u;
+    const bool exact = (a.st->flags & BNN_FLAG_OUT_OF_GRID) != 0u;
     const float inf = __int_as_float(0x7f800000);
-    // Grid::getWorldCoordinate(i + 0.5, j + 0.5, k + 0.5) (Grid.h:186-194)
-    const float sxw = ((float)i + 0.5f) * g.dx + g.bmin[0];
-    float m[kRptSdf][kCol];
-#pragma unroll
-    for(int uj = 0; uj < kRptSdf; ++uj)
-#pragma unroll
-        for(int u = 0; u < kCol; ++u) m[uj][u] = inf;
-    const int xlo = max(i - 1, 0), xhi = min(i + 1, g.G[0] - 1);
-#pragma unroll
-    for(int t = 0; t < kCol + 2; ++t) {
-        const int kk = k0 - 1 + t;
-        if(kk < 0 || kk > g.G[2] - 1) continue;
-#pragma unroll
-        for(int dj = 0; dj < kRptSdf + 2; ++dj) {
-            const int jj = j0 - 1 + dj;
-            if(jj < 0 || jj > g.G[1] - 1 || xlo > xhi) continue;
-            const size_t base = ((size_t)kk * g.G[1] + jj) * g.G[0];
-            const uint32_t b = __ldg(cellStart + base + xlo), e = __ldg(cellStart + base + xhi + 1);
-            for(uint32_t q0 = b & ~1u; q0 < e; q0 += 2) {
-                float4 L[2];
-                ldg_pair(pos + q0, L[0], L[1]);
-#pragma unroll
-                for(int w = 0; w < 2; ++w) {
-                    const float ddx = sxw - L[w].x;
-                    const float dxx = ddx * ddx;
-                    const uint32_t q = q0 + (uint32_t)w;
-                    bool reach = q >= b && q < e;
-                    int ci = 0, cj = 0, ck = 0;
-                    if(exact) {
-                        // the particle's own cell (Grid::getGridCoordinate, truncated) and its
-                        // clamped 3x3x3 range (PIC_Solver.cpp:633-635)
-                        ci = (int)((L[w].x - g.bmin[0]) / g.dx);
-                        cj = (int)((L[w].y - g.bmin[1]) / g.dx);
-                        ck = (int)((L[w].z - g.bmin[2]) / g.dx);
-                        reach = reach && !(i < max(ci - 1, 0) || i > min(ci + 1, g.G[0] - 1));
-                    }
-#pragma unroll
-                    for(int ddj = -2; ddj <= 0; ++ddj) {
-                        const int uj = dj + ddj;
-                        if(uj < 0 || uj >= kRptSdf) continue;
-                        const int j = j0 + uj;
-                        const float syw = ((float)j + 0.5f) * g.dx + g.bmin[1];
-                        const float ddy = syw - L[w].y;
-                        const float dxy = dxx + ddy * ddy;
-                        const bool okJ = reach && !(exact && (j < max(cj - 1, 0) || j > min(cj + 1, g.G[1] - 1)));
-#pragma unroll
-                        for(int du = -1; du <= 1; ++du) {
-                            const int u = t - 1 + du;
-                            if(u < 0 || u >= kCol) continue;
-                            const int k = k0 + u;
-                            const bool ok = okJ && !(exact && (k < max(ck - 1, 0) || k > min(ck + 1, g.G[2] - 1)));
-                            const float ddz = (((float)k + 0.5f) * g.dx + g.bmin[2]) - L[w].z;
-                            const float d2 = dxy + ddz * ddz;  // glm::length2: (x*x + y*y) + z*z
-                            m[uj][u] = fminf(m[uj][u], ok ? d2 : inf);
-                        }
-                    }
+    // accumulators of face layers cy - 1 + j (v, whose own axis is the walk, uses j = 1, 2)
+    float uS[3] = {0.f, 0.f, 0.f}, uW[3] = {0.f, 0.f, 0.f};
+    float vS[3] = {0.f, 0.f, 0.f}, vW[3] = {0.f, 0.f, 0.f};
+    float wS[3] = {0.f, 0.f, 0.f}, wW[3] = {0.f, 0.f, 0.f};
+    float aM[3] = {inf, inf, inf};
+    for(int cy = yA - 1; cy <= yB; ++cy) {
+        if(cy >= 0 && cy < g.G[1]) {
+            if constexpr(P2G) {
+                for(int h = t; h < kNH; h += kThreads) cell_partials<0>(a, x0, z0, cy, h, sm);
+                __syncthreads();
+                pull_partials<0>(sm, tx, tz, uS, uW);
+                __syncthreads();
+                if(cy < yB) {
+                    for(int h = t; h < kNH; h += kThreads) cell_partials<1>(a, x0, z0, cy, h, sm);
+                    __syncthreads();
+                    pull_partials<1>(sm, tx, tz, vS, vW);
+                    __syncthreads();
                 }
+                for(int h = t; h < kNH; h += kThreads) cell_partials<2>(a, x0, z0, cy, h, sm);
+                __syncthreads();
+                pull_partials<2>(sm, tx, tz, wS, wW);
+                __syncthreads();
             }
+            for(int h = t; h < kNH; h += kThreads) sdf_partials(a, x0, z0, cy, h, exact, sm);
+            __syncthreads();
+            pull_sdf(sm, tx, tz, aM);
+            __syncthreads();
         }
-    }
-    if(i < g.G[0]) {
-#pragma unroll
-        for(int uj = 0; uj < kRptSdf; ++uj)
-#pragma unroll
-            for(int u = 0; u < kCol; ++u) {
-                if(j0 + uj >= g.G[1] || k0 + u >= g.G[2]) continue;
-                float ph = empty;
-                if(m[uj][u] != inf) {
-                    const float val = sqrtf(m[uj][u]) - g.sdfRadius;
-                    if(val < ph) ph = val;
-                }
-                phi[cell_index(uj, u)] = ph;
+        // face / cell layer cy - 1 is complete for u, w and the SDF, face layer cy for v
+        if(cy - 1 >= yA && cy - 1 < yB) {
+            if constexpr(P2G) {
+                write_face<0>(a, fx, cy - 1, fz, uS[0], uW[0]);
+                write_face<2>(a, fx, cy - 1, fz, wS[0], wW[0]);
             }
+            write_phi(a, fx, cy - 1, fz, aM[0]);
+        }
+        if constexpr(P2G) {
+            if(cy >= yA && cy < yB) write_face<1>(a, fx, cy, fz, vS[1], vW[1]);
+        }
+        uS[0] = uS[1]; uS[1] = uS[2]; uS[2] = 0.f;
+        uW[0] = uW[1]; uW[1] = uW[2]; uW[2] = 0.f;
+        wS[0] = wS[1]; wS[1] = wS[2]; wS[2] = 0.f;
+        wW[0] = wW[1]; wW[1] = wW[2]; wW[2] = 0.f;
+        vS[1] = vS[2]; vS[2] = 0.f;
+        vW[1] = vW[2]; vW[2] = 0.f;
+        aM[0] = aM[1]; aM[1] = aM[2]; aM[2] = inf;
     }
 }
 
-static dim3 col_grid(int sx, int sr, int sa, int rpt) {
-    return dim3((unsigned)((sx + kLx - 1) / kLx), (unsigned)((sr + kLr * rpt - 1) / (kLr * rpt)),
-                (unsigned)((sa + kCol - 1) / kCol));
+static dim3 tile_grid(const GridDesc& g) {
+    return dim3((unsigned)((g.G[0] + 1 + kTX - 1) / kTX), (unsigned)((g.G[2] + 1 + kTZ - 1) / kTZ),
+                (unsigned)((g.G[1] + 1 + kYC - 1) / kYC));
 }
 
-void launch_p2g_col(const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float4* rec,
-                    size_t stride, float* const* out, uint8_t* const* valid, cudaStream_t s) {
-    const dim3 blk(kLx, kLr);
-    // u, v: rows along y, columns along z; w: rows along z, columns along y
-    { k_p2g_col<0><<<col_grid(g.G[0] + 1, g.G[1], g.G[2], kRptP2G), blk, 0, s>>>(g, st, cellStart, rec, stride, out[0], valid[0]); bnn_note_launch(); }
-    { k_p2g_col<1><<<col_grid(g.G[0], g.G[1] + 1, g.G[2], kRptP2G), blk, 0, s>>>(g, st, cellStart, rec, stride, out[1], valid[1]); bnn_note_launch(); }
-    { k_p2g_col<2><<<col_grid(g.G[0], g.G[2] + 1, g.G[1], kRptP2G), blk, 0, s>>>(g, st, cellStart, rec, stride, out[2], valid[2]); bnn_note_launch(); }
+// The dynamic shared memory above the 48 KB default is opted into once per device.
+template<bool P2G>
+static void launch_tile(const TileArgs& a, cudaStream_t s) {
+    static std::atomic<uint64_t> configured{0};  // bit per device ordinal
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const uint64_t bit = 1ull << (dev & 63);
+    if(!(configured.load(std::memory_order_acquire) & bit)) {
+        cudaFuncSetAttribute(k_p2g_sdf_tile<P2G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+        configured.fetch_or(bit, std::memory_order_acq_rel);
+    }
+    k_p2g_sdf_tile<P2G><<<tile_grid(a.g), dim3(kTX, kTZ), kSmemBytes, s>>>(a);
+    bnn_note_launch();
 }
 
-void launch_fluid_sdf_col(const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float4* rec,
-                          size_t stride, float* phi, cudaStream_t s) {
-    { k_fluid_sdf_col<<<col_grid(g.G[0], g.G[1], g.G[2], kRptSdf), dim3(kLx, kLr), 0, s>>>(g, st, cellStart, rec + 3 * stride,
-                                                                               phi); bnn_note_launch(); }
+// FLIP P2G of the three components together with the fluid SDF
+void launch_p2g_sdf(const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float4* rec,
+                    size_t stride, float* const* out, uint8_t* const* valid, float* phi, cudaStream_t s) {
+    TileArgs a{g, st, cellStart, rec, stride, {out[0], out[1], out[2]}, {valid[0], valid[1], valid[2]}, phi};
+    launch_tile<true>(a, s);
+}
+
+// The fluid SDF alone (APIC / AFLIP / PIC)
+void launch_fluid_sdf_tile(const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float4* rec,
+                           size_t stride, float* phi, cudaStream_t s) {
+    TileArgs a{g, st, cellStart, rec, stride, {nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}, phi};
+    launch_tile<false>(a, s);
 }
 
 } // namespace bnn

@@ -566,6 +566,402 @@ __global__ void __launch_bounds__(kLanes, pcg_min_blocks<VT, COEF>()) k_pcg_pers
     }
 }
 
+// ---------------------------------------------------------------------------------
+// Single-reduction PCG (Chronopoulos & Gear, 1989): the same Krylov iterates as
+// PCGSolver::solve_precond (PCGSolver.cpp:143-199) in exact arithmetic, with both inner
+// products of an iteration formed in one reduction, so one grid barrier per iteration
+// instead of two.  With u = D^-1 r and w = A u:
+//   gamma_i = (r_i, u_i), delta_i = (w_i, u_i)
+//   beta_i  = gamma_i / gamma_{i-1},  alpha_i = gamma_i / (delta_i - beta_i gamma_i / alpha_{i-1})
+//   p_i = u_i + beta_i p_{i-1},  s_i = w_i + beta_i s_{i-1}   (s_i = A p_i)
+//   x_{i+1} = x_i + alpha_i p_i,  r_{i+1} = r_i - alpha_i s_i,  then u_{i+1}, w_{i+1}
+// (the denominator is (p_i, A p_i); the first iteration takes beta = 0, alpha = gamma/delta).
+// w_{i+1} = A u_{i+1} needs the neighbours' new u.  Instead of a second barrier, a row
+// recomputes each neighbour's new u from the neighbour's old record {r, w, s, 1/diag}
+// with the exact operations the neighbour uses for itself, so both agree bit for bit.  The
+// records are double-buffered (read one, write the other), and so are the chunk partials
+// (a block may start the next iteration while another still reads this one's partials).
+// Per row and iteration: its own record, p and x, one record per y / z neighbour; the x
+// neighbours' u come from the adjacent lanes by shuffles (packed rows).  Scalars are
+// formed in FP64 from the canonical FP64 sums and rounded to the vector type.
+// ---------------------------------------------------------------------------------
+template<class VT> struct alignas(4 * sizeof(VT)) RowState {
+    VT r, w, s, inv;
+};
+template<class VT> __device__ __forceinline__ RowState<VT> ld_state(const RowState<VT>* p) {
+    RowState<VT> o;
+    if constexpr(sizeof(VT) == 4) {
+        const float4 v = __ldcg(reinterpret_cast<const float4*>(p));
+        o.r = v.x; o.w = v.y; o.s = v.z; o.inv = v.w;
+    } else {
+        const double2 a = __ldcg(reinterpret_cast<const double2*>(p));
+        const double2 b = __ldcg(reinterpret_cast<const double2*>(p) + 1);
+        o.r = a.x; o.w = a.y; o.s = b.x; o.inv = b.y;
+    }
+    return o;
+}
+template<class VT> __device__ __forceinline__ void st_state(RowState<VT>* p, VT r, VT w, VT s, VT inv) {
+    if constexpr(sizeof(VT) == 4) {
+        *reinterpret_cast<float4*>(p) = make_float4(r, w, s, inv);
+    } else {
+        reinterpret_cast<double2*>(p)[0] = make_double2(r, w);
+        reinterpret_cast<double2*>(p)[1] = make_double2(s, inv);
+    }
+}
+// The new preconditioned residual of a row from its old record: the row's own update
+// written out (s_i = w_i + beta s_{i-1}, r_{i+1} = r_i - alpha s_i, u_{i+1} = r_{i+1} / diag).
+template<class VT> __device__ __forceinline__ VT u_next(const RowState<VT>& o, VT alpha, VT beta, bool first) {
+    const VT s = first ? o.w : o.w + beta * o.s;
+    const VT r = o.r + (-alpha) * s;
+    return o.inv * r;
+}
+
+template<class VT> struct Cg1Args {
+    int n;
+    const float* rhsF;
+    const float* diag;
+    const VT* invd;
+    const int32_t* nbr;
+    const int4* rec;
+    const float* coef;
+    const float4* coefRow;
+    VT negoff;
+    VT tolFactor;
+    unsigned maxIter;
+    VT *x, *p;
+    RowState<VT>* st[2];
+    double* part;  // [set 0/1][gamma, delta][nchCap]
+    double* pmax;  // [set 0/1][nchCap]
+    int nchCap;
+    DevState* dst;
+    GridSync* gs;
+};
+
+// Two canonical 256-lane sums and a max in one block pass (association of
+// block_sum_max_256); valid in thread 0.
+__device__ __forceinline__ void block_sum2_max_256(double a, double b, double m, double* sa, double* sb, double* sm,
+                                                   double& ra, double& rb, double& rm) {
+    const int t = threadIdx.x;
+    sa[t] = a; sb[t] = b; sm[t] = m;
+    __syncthreads();
+    if(t < 32) {
+        double c[2];
+#pragma unroll
+        for(int k = 0; k < 2; ++k) {
+            const double* sx = k == 0 ? sa : sb;
+            const double a0 = sx[t] + sx[t + 128];
+            const double a1 = sx[t + 64] + sx[t + 192];
+            const double a2 = sx[t + 32] + sx[t + 160];
+            const double a3 = sx[t + 96] + sx[t + 224];
+            double v = (a0 + a1) + (a2 + a3);
+#pragma unroll
+            for(int off = 16; off > 0; off >>= 1) v = v + __shfl_down_sync(0xffffffffu, v, off);
+            c[k] = v;
+        }
+        double x = sm[t];
+#pragma unroll
+        for(int q = 1; q < 8; ++q) { const double o = sm[t + 32 * q]; x = x > o ? x : o; }
+#pragma unroll
+        for(int off = 16; off > 0; off >>= 1) { const double o = __shfl_down_sync(0xffffffffu, x, off); x = x > o ? x : o; }
+        ra = c[0]; rb = c[1]; rm = x;
+    }
+    __syncthreads();
+}
+
+// The chunk partials of both sums (canonical order) and their max, to every thread.
+__device__ __forceinline__ void reduce_partials2_bcast(const double* pa, const double* pb, const double* pm, int nch,
+                                                       double* sa, double* sb, double* sm, double& ra, double& rb,
+                                                       double& rm) {
+    __shared__ double sRes[3];
+    constexpr int U = 4;
+    double acc0 = 0.0, acc1 = 0.0, m = 0.0;
+    for(int c0 = threadIdx.x; c0 < nch; c0 += U * kLanes) {
+        double x0[U], x1[U], xm[U];
+#pragma unroll
+        for(int u = 0; u < U; ++u) {
+            const int c = c0 + u * kLanes;
+            x0[u] = c < nch ? __ldcg(pa + c) : 0.0;
+            x1[u] = c < nch ? __ldcg(pb + c) : 0.0;
+            xm[u] = c < nch ? __ldcg(pm + c) : 0.0;
+        }
+#pragma unroll
+        for(int u = 0; u < U; ++u)
+            if(c0 + u * kLanes < nch) {
+                acc0 = acc0 + x0[u];
+                acc1 = acc1 + x1[u];
+                m = m > xm[u] ? m : xm[u];
+            }
+    }
+    double r0 = 0.0, r1 = 0.0, r2 = 0.0;
+    block_sum2_max_256(acc0, acc1, m, sa, sb, sm, r0, r1, r2);
+    if(threadIdx.x == 0) { sRes[0] = r0; sRes[1] = r1; sRes[2] = r2; }
+    __syncthreads();
+    ra = sRes[0]; rb = sRes[1]; rm = sRes[2];
+    __syncthreads();
+}
+
+// Rows whose loads a lane keeps in flight together in the single-reduction kernel (each
+// row holds seven 4-value records)
+#ifndef BNN_CG1_ROW_GROUP
+#define BNN_CG1_ROW_GROUP 1
+#endif
+#ifndef BNN_CG1_MIN_BLOCKS
+#define BNN_CG1_MIN_BLOCKS 3
+#endif
+#ifndef BNN_CG1_MIN_BLOCKS_F64
+#define BNN_CG1_MIN_BLOCKS_F64 2
+#endif
+template<class VT> constexpr int cg1_row_group() { return sizeof(VT) == 8 ? 1 : BNN_CG1_ROW_GROUP; }
+template<class VT> constexpr int cg1_min_blocks() { return sizeof(VT) == 8 ? BNN_CG1_MIN_BLOCKS_F64 : BNN_CG1_MIN_BLOCKS; }
+
+template<class VT, bool PACKED, bool COEF>
+__global__ void __launch_bounds__(kLanes, cg1_min_blocks<VT>()) k_pcg_cg1(Cg1Args<VT> a) {
+    constexpr int kRowGroup = cg1_row_group<VT>();
+    __shared__ double sa[kLanes], sb[kLanes], smx[kLanes];
+    const int n = a.n;
+    const int nch = (n + kChunk - 1) / kChunk;
+    const unsigned nb = gridDim.x;
+    unsigned sense = 0;
+    unsigned* flags = &a.dst->flags;
+    const int lane = threadIdx.x & 31;
+    const VT negoff = a.negoff;
+
+    // neighbour rows of row ee in slot order (-z,-y,-x,self,+x,+y,+z); a missing one reads
+    // the row itself (masked by has)
+    auto neighbours = [&](size_t ee, const int4& rr, int32_t id[7], bool has[7], float& dg) {
+        if constexpr(PACKED) {
+            const int dyM = rr.x & 0xffff, dyP = (int)((unsigned)rr.x >> 16);
+            const int dzM = rr.y & 0x7fffffff, dzP = rr.z & 0x7fffffff;
+            const int32_t r0 = (int32_t)ee;
+            has[0] = dzM != 0; id[0] = r0 - dzM;
+            has[1] = dyM != 0; id[1] = r0 - dyM;
+            has[2] = rr.y < 0; id[2] = (lane == 0 && rr.y < 0) ? r0 - 1 : r0;
+            has[3] = true; id[3] = r0;
+            has[4] = rr.z < 0; id[4] = (lane == 31 && rr.z < 0) ? r0 + 1 : r0;
+            has[5] = dyP != 0; id[5] = r0 + dyP;
+            has[6] = dzP != 0; id[6] = r0 + dzP;
+            dg = __int_as_float(rr.w);
+        } else {
+#pragma unroll
+            for(int q = 0; q < 6; ++q) {
+                const int32_t v = __ldg(a.nbr + (size_t)q * n + ee);
+                const int slot = q < 3 ? q : q + 1;
+                has[slot] = v >= 0;
+                id[slot] = v >= 0 ? v : (int32_t)ee;
+            }
+            id[3] = (int32_t)ee;
+            has[3] = true;
+            dg = __ldg(a.diag + ee);
+        }
+    };
+    // (A v) of a row from its seven slot values, summed in slot order (FixedSparseMatrix::
+    // multiply, SparseMatrix.cpp:222-235: column-sorted)
+    auto apply_row = [&](size_t ee, const bool has[7], float dg, const VT v7[7]) {
+        VT t = VT(0);
+        if constexpr(COEF) {
+            VT co[7];
+            if constexpr(PACKED) {
+                const float4 c0 = __ldg(a.coefRow + 2 * ee), c1 = __ldg(a.coefRow + 2 * ee + 1);
+                co[0] = (VT)c0.x; co[1] = (VT)c0.y; co[2] = (VT)c0.z; co[3] = VT(0);
+                co[4] = (VT)c0.w; co[5] = (VT)c1.x; co[6] = (VT)c1.y;
+            } else {
+#pragma unroll
+                for(int q = 0; q < 7; ++q) co[q] = q == 3 ? VT(0) : (VT)__ldg(a.coef + (size_t)(q < 3 ? q : q - 1) * n + ee);
+            }
+#pragma unroll
+            for(int q = 0; q < 3; ++q) if(has[q]) t += co[q] * v7[q];
+            if(dg != 0.f) t += (VT)dg * v7[3];
+#pragma unroll
+            for(int q = 4; q < 7; ++q) if(has[q]) t += co[q] * v7[q];
+        } else {
+#pragma unroll
+            for(int q = 0; q < 3; ++q) if(has[q]) t += negoff * v7[q];
+            if(dg != 0.f) t += (VT)dg * v7[3];
+#pragma unroll
+            for(int q = 4; q < 7; ++q) if(has[q]) t += negoff * v7[q];
+        }
+        return t;
+    };
+
+    // ---- init: r = b, x = 0, u = D^-1 b, w = A u; gamma, delta, max|r| (set 0)
+    for(int c = blockIdx.x; c < nch; c += nb) {
+        const size_t base = (size_t)c * kChunk + threadIdx.x;
+        double g = 0.0, d = 0.0, m = 0.0;
+#pragma unroll 2
+        for(int j = 0; j < kPerLane; ++j) {
+            const size_t e = base + (size_t)j * kLanes;
+            const size_t ee = e < (size_t)n ? e : 0;
+            int32_t id[7];
+            bool has[7];
+            float dg;
+            int4 rr = make_int4(0, 0, 0, 0);
+            if constexpr(PACKED) rr = __ldg(a.rec + ee);
+            neighbours(ee, rr, id, has, dg);
+            VT u7[7];
+#pragma unroll
+            for(int q = 0; q < 7; ++q) {
+                const bool load = !PACKED || (q != 2 && q != 4) || (q == 2 && lane == 0) || (q == 4 && lane == 31);
+                u7[q] = load ? __ldg(a.invd + id[q]) * (VT)__ldg(a.rhsF + id[q]) : VT(0);
+            }
+            if constexpr(PACKED) {
+                const VT up = __shfl_up_sync(0xffffffffu, u7[3], 1);
+                const VT dn = __shfl_down_sync(0xffffffffu, u7[3], 1);
+                if(lane != 0) u7[2] = up;
+                if(lane != 31) u7[4] = dn;
+            }
+            const VT wv = apply_row(ee, has, dg, u7);
+            if(e < (size_t)n) {
+                const VT rv = (VT)a.rhsF[e];
+                a.x[e] = VT(0);
+                st_state(a.st[0] + e, rv, wv, VT(0), __ldg(a.invd + e));
+                g = g + (double)u7[3] * (double)rv;
+                d = d + (double)wv * (double)u7[3];
+                const double ab = (double)vabs(rv);
+                m = m > ab ? m : ab;
+            }
+        }
+        double bg, bd, bm;
+        block_sum2_max_256(g, d, m, sa, sb, smx, bg, bd, bm);
+        if(threadIdx.x == 0) { a.part[c] = bg; a.part[(size_t)a.nchCap + c] = bd; a.pmax[c] = bm; }
+    }
+    if(!grid_barrier(a.gs, nb, sense, flags, solve_barrier_limit())) return;
+    double gamma, delta, rmax;
+    reduce_partials2_bcast(a.part, a.part + a.nchCap, a.pmax, nch, sa, sb, smx, gamma, delta, rmax);
+    VT resid = (VT)rmax;
+    const VT tolFactor = fmax(a.tolFactor, VT(1e-30));
+    unsigned iter = 0, success = 0;
+    bool done = false;
+    VT tol = VT(0);
+    if(resid < (VT)FLT_MIN) {
+        done = true;
+        success = 1;
+    } else {
+        tol = tolFactor * resid;
+        if(gamma < (double)FLT_MIN || isnan(gamma)) done = true;
+    }
+    if(a.maxIter == 0) done = true;
+    bool first = true;
+    double gammaOld = 0.0, a64Old = 0.0;
+    int cur = 0, set = 1;
+    while(!done) {
+        // alpha_i, beta_i; a denominator (p, A p) below FLT_MIN ends the solve as
+        // PCGSolver's (p, s) check does (PCGSolver.cpp:173-176)
+        double b64 = 0.0, den = delta;
+        if(!first) {
+            b64 = gamma / gammaOld;
+            den = delta - (b64 * gamma) / a64Old;
+        }
+        if(den < (double)FLT_MIN) {
+            ++iter;
+            success = 1;
+            break;
+        }
+        const double a64 = gamma / den;
+        const VT alpha = (VT)a64, beta = (VT)b64;
+        const RowState<VT>* __restrict__ sIn = a.st[cur];
+        RowState<VT>* __restrict__ sOut = a.st[1 - cur];
+        double* __restrict__ pg = a.part + (size_t)set * 2 * a.nchCap;
+        double* __restrict__ pd = pg + a.nchCap;
+        double* __restrict__ pm = a.pmax + (size_t)set * a.nchCap;
+        for(int c = blockIdx.x; c < nch; c += nb) {
+            const size_t base = (size_t)c * kChunk + threadIdx.x;
+            int4 recAll[PACKED ? kPerLane : 1];
+            if constexpr(PACKED) {
+#pragma unroll
+                for(int j = 0; j < kPerLane; ++j) {
+                    const size_t e = base + (size_t)j * kLanes;
+                    recAll[j] = __ldg(a.rec + (e < (size_t)n ? e : 0));
+                }
+            }
+            double g = 0.0, d = 0.0, m = 0.0;
+#pragma unroll
+            for(int g0 = 0; g0 < kPerLane; g0 += kRowGroup) {
+                int32_t id[kRowGroup][7];
+                bool has[kRowGroup][7];
+                float dg[kRowGroup];
+                size_t rowE[kRowGroup];
+#pragma unroll
+                for(int u = 0; u < kRowGroup; ++u) {
+                    const size_t e = base + (size_t)(g0 + u) * kLanes;
+                    rowE[u] = e < (size_t)n ? e : 0;
+                    neighbours(rowE[u], PACKED ? recAll[g0 + u] : make_int4(0, 0, 0, 0), id[u], has[u], dg[u]);
+                }
+                RowState<VT> S[kRowGroup][7];
+                VT pOld[kRowGroup], xOld[kRowGroup];
+#pragma unroll
+                for(int u = 0; u < kRowGroup; ++u) {
+#pragma unroll
+                    for(int q = 0; q < 7; ++q) {
+                        const bool load = !PACKED || (q != 2 && q != 4) || (q == 2 && lane == 0) || (q == 4 && lane == 31);
+                        if(load) S[u][q] = ld_state(sIn + id[u][q]);
+                        else S[u][q] = RowState<VT>{VT(0), VT(0), VT(0), VT(0)};
+                    }
+                    pOld[u] = first ? VT(0) : __ldcg(a.p + rowE[u]);
+                    xOld[u] = __ldcg(a.x + rowE[u]);
+                }
+#pragma unroll
+                for(int u = 0; u < kRowGroup; ++u) {
+                    const RowState<VT>& o = S[u][3];
+                    const VT uOld = o.inv * o.r;
+                    const VT pNew = first ? uOld : uOld + beta * pOld[u];
+                    const VT sNew = first ? o.w : o.w + beta * o.s;
+                    const VT xNew = xOld[u] + alpha * pNew;
+                    const VT rNew = o.r + (-alpha) * sNew;
+                    VT u7[7];
+#pragma unroll
+                    for(int q = 0; q < 7; ++q) u7[q] = q == 3 ? o.inv * rNew : u_next(S[u][q], alpha, beta, first);
+                    if constexpr(PACKED) {
+                        const VT up = __shfl_up_sync(0xffffffffu, u7[3], 1);
+                        const VT dn = __shfl_down_sync(0xffffffffu, u7[3], 1);
+                        if(lane != 0) u7[2] = up;
+                        if(lane != 31) u7[4] = dn;
+                    }
+                    const VT wNew = apply_row(rowE[u], has[u], dg[u], u7);
+                    const size_t e = base + (size_t)(g0 + u) * kLanes;
+                    if(e < (size_t)n) {
+                        st_state(sOut + e, rNew, wNew, sNew, o.inv);
+                        a.p[e] = pNew;
+                        a.x[e] = xNew;
+                        g = g + (double)u7[3] * (double)rNew;
+                        d = d + (double)wNew * (double)u7[3];
+                        const double ab = (double)vabs(rNew);
+                        m = m > ab ? m : ab;
+                    }
+                }
+            }
+            double bg, bd, bm;
+            block_sum2_max_256(g, d, m, sa, sb, smx, bg, bd, bm);
+            if(threadIdx.x == 0) { pg[c] = bg; pd[c] = bd; pm[c] = bm; }
+        }
+        if(!grid_barrier(a.gs, nb, sense, flags, solve_barrier_limit())) return;
+        double gNew, dNew, mNew;
+        reduce_partials2_bcast(pg, pd, pm, nch, sa, sb, smx, gNew, dNew, mNew);
+        resid = (VT)mNew;
+        ++iter;
+        if(resid < tol) {
+            success = 1;
+            break;
+        }
+        if(iter >= a.maxIter) {
+            if(blockIdx.x == 0 && threadIdx.x == 0) atomicOr(flags, BNN_FLAG_PCG_MAXITER);
+            break;
+        }
+        gammaOld = gamma;
+        gamma = gNew;
+        delta = dNew;
+        a64Old = a64;
+        cur = 1 - cur;
+        set = 1 - set;
+        first = false;
+    }
+    if(blockIdx.x == 0 && threadIdx.x == 0) {
+        a.dst->iter = iter;
+        a.dst->success = success;
+        a.dst->done = 1;
+        Sc<VT>::set_resid(a.dst, resid);
+    }
+}
+
 // ---- iterative refinement helpers -------------------------------------------------
 // x64 = 0, r64 = b, outer_bmax = outer_res = max|b|
 __global__ void __launch_bounds__(kLanes) k_ir_init(int n, const float* __restrict__ b, double* __restrict__ x64,
@@ -693,7 +1089,7 @@ struct CoopState {
     std::mutex mu;
     std::condition_variable cv;
     int numSM = 0;
-    int perSM[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int perSM[16] = {};
     long long held = 0;
 };
 static CoopState g_coop;
@@ -741,6 +1137,14 @@ int pcg_reserve(PcgWork& w, int n, bool fp64) {
     }
     for(auto& e : w.ev)
         if(!e) BNN_CUDA_CHECK(cudaEventCreate(&e));
+    if(!w.st32[0]) {
+        // single-reduction solve: double-buffered row records and partials
+        for(int b = 0; b < 2; ++b) BNN_CUDA_CHECK(cudaMalloc(&w.st32[b], w.cap * sizeof(float4)));
+        BNN_CUDA_CHECK(cudaMalloc(&w.cgPart, 4 * (size_t)w.nchCap * sizeof(double)));
+        BNN_CUDA_CHECK(cudaMalloc(&w.cgMax, 2 * (size_t)w.nchCap * sizeof(double)));
+    }
+    if(fp64 && !w.st64[0])
+        for(int b = 0; b < 2; ++b) BNN_CUDA_CHECK(cudaMalloc(&w.st64[b], w.cap * 4 * sizeof(double)));
     if(fp64 && !w.x64) {
         BNN_CUDA_CHECK(cudaMalloc(&w.x64, w.cap * sizeof(double)));
         BNN_CUDA_CHECK(cudaMalloc(&w.r64, w.cap * sizeof(double)));
@@ -758,7 +1162,8 @@ void pcg_release(PcgWork& w) {
         if(e) cudaEventDestroy(e);
     for(void* p : {(void*)w.rec, (void*)w.coefRow, (void*)w.x, (void*)w.r, (void*)w.z, (void*)w.s0, (void*)w.s1, (void*)w.q, (void*)w.d32, (void*)w.r32,
                    (void*)w.part, (void*)w.partMaxF, (void*)w.partMaxD, (void*)w.x64, (void*)w.r64, (void*)w.z64,
-                   (void*)w.s064, (void*)w.s164, (void*)w.q64, (void*)w.inv64, (void*)w.gs})
+                   (void*)w.s064, (void*)w.s164, (void*)w.q64, (void*)w.inv64, (void*)w.gs, (void*)w.st32[0],
+                   (void*)w.st32[1], (void*)w.st64[0], (void*)w.st64[1], (void*)w.cgPart, (void*)w.cgMax})
         if(p) cudaFree(p);
     w = PcgWork();
 }
@@ -768,14 +1173,21 @@ void pcg_release(PcgWork& w) {
 template<class VT>
 static int pcg_solve_t(PcgWork& w, int n, const float* rhsF, const float* diag, const VT* invd, const int32_t* nbr,
                        const int4* rec, const float* coef, const float4* coefRow, VT negoff, VT tolFactor, unsigned maxIter, VT* x, VT* r, VT* z, VT* s0, VT* s1, VT* q,
-                       VT* partMax, DevState* dst, DevState* hst, cudaStream_t s, PcgOutcome& out) {
+                       VT* partMax, bool twoReductions, DevState* dst, DevState* hst, cudaStream_t s, PcgOutcome& out) {
     out = PcgOutcome();
     if(n == 0) { out.success = 1; return BNN_OK; }
     const int nch = (n + kChunk - 1) / kChunk;
     const bool packedCoef = rec && coefRow;
-    const int ti = (sizeof(VT) == 8 ? 1 : 0) + (rec ? 2 : 0) + (packedCoef ? 4 : 0);
-    const void* kern = packedCoef ? (const void*)k_pcg_persistent<VT, true, true>
-                                  : (rec ? (const void*)k_pcg_persistent<VT, true> : (const void*)k_pcg_persistent<VT, false>);
+    // kernel variant: bit 0 FP64, bit 1 packed rows, bit 2 coefficients, bit 3 single reduction
+    const int ti = (sizeof(VT) == 8 ? 1 : 0) + (rec ? 2 : 0) + ((coef || coefRow) ? 4 : 0) + (twoReductions ? 0 : 8);
+    const void* kern;
+    if(twoReductions)
+        kern = packedCoef ? (const void*)k_pcg_persistent<VT, true, true>
+                          : (rec ? (const void*)k_pcg_persistent<VT, true> : (const void*)k_pcg_persistent<VT, false>);
+    else if(rec)
+        kern = coefRow ? (const void*)k_pcg_cg1<VT, true, true> : (const void*)k_pcg_cg1<VT, true, false>;
+    else
+        kern = coef ? (const void*)k_pcg_cg1<VT, false, true> : (const void*)k_pcg_cg1<VT, false, false>;
     int numSM = 0, perSMv = 0;
     {
         std::lock_guard<std::mutex> lk(g_coop.mu);
@@ -799,8 +1211,14 @@ static int pcg_solve_t(PcgWork& w, int n, const float* rhsF, const float* diag, 
     a.maxIter = maxIter; a.x = x; a.r = r; a.z = z; a.s0 = s0; a.s1 = s1; a.q = q;
     a.part0 = w.part; a.part1 = w.part + w.nchCap; a.part2 = w.part + 2 * (size_t)w.nchCap; a.partMax = partMax;
     a.st = dst; a.gs = w.gs;
+    Cg1Args<VT> c;
+    c.n = n; c.rhsF = rhsF; c.diag = diag; c.invd = invd; c.nbr = nbr; c.rec = rec; c.coef = coef; c.coefRow = coefRow;
+    c.negoff = negoff; c.tolFactor = tolFactor; c.maxIter = maxIter; c.x = x; c.p = s0;
+    for(int b = 0; b < 2; ++b)
+        c.st[b] = sizeof(VT) == 8 ? (RowState<VT>*)(void*)w.st64[b] : (RowState<VT>*)(void*)w.st32[b];
+    c.part = w.cgPart; c.pmax = w.cgMax; c.nchCap = w.nchCap; c.dst = dst; c.gs = w.gs;
     BNN_CUDA_CHECK(cudaMemsetAsync(&w.gs->count, 0, sizeof(unsigned), s));
-    void* args[] = {&a};
+    void* args[] = {twoReductions ? (void*)&a : (void*)&c};
     // grids of concurrent solves (several solver handles on several host threads) must
     // fit the GPU together, or blocks of one could wait for SMs held by another's barrier
     CoopShare share(grid * (kShareUnits / perSMv), numSM * kShareUnits);
@@ -821,11 +1239,14 @@ static int pcg_solve_t(PcgWork& w, int n, const float* rhsF, const float* diag, 
     return BNN_OK;
 }
 
-// mode: BNN_PCG_FP32 / FP64 / REFINED.  Pressure written to `pressure` (float, n).
+// mode: BNN_PCG_FP32 / FP64 / REFINED, optionally with BNN_PCG_TWO_REDUCTIONS.  Pressure
+// written to `pressure` (float, n).
 int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const float* invd, const int32_t* nbr,
-              const float* coef, bool gridRows, float dt, int mode, float tol, unsigned maxIter, float innerTol,
+              const float* coef, bool gridRows, float dt, int modeFlags, float tol, unsigned maxIter, float innerTol,
               float outerTol, float* pressure, double* x64out, DevState* dst, DevState* hst, cudaStream_t s,
               PcgOutcome& out) {
+    const int mode = modeFlags & BNN_PCG_MODE_MASK;
+    const bool two = (modeFlags & BNN_PCG_TWO_REDUCTIONS) != 0;
     int rc = pcg_reserve(w, n, mode != BNN_PCG_FP32);
     if(rc != BNN_OK) return rc;
     const unsigned nb = (unsigned)((n + 255) / 256);
@@ -845,7 +1266,7 @@ int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const floa
     }
     if(mode == BNN_PCG_FP32) {
         rc = pcg_solve_t<float>(w, n, rhs, diag, invd, nbr, rec, coef, coefRow, -(1.0f * dt), tol, maxIter, w.x, w.r, w.z, w.s0, w.s1,
-                                w.q, w.partMaxF, dst, hst, s, out);
+                                w.q, w.partMaxF, two, dst, hst, s, out);
         if(rc != BNN_OK) return rc;
         if(n > 0) BNN_CUDA_CHECK(cudaMemcpyAsync(pressure, w.x, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
         if(x64out && n > 0) { k_f32_to_f64<<<nb, 256, 0, s>>>(n, w.x, x64out); bnn_note_launch(); }
@@ -854,7 +1275,7 @@ int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const floa
     if(mode == BNN_PCG_FP64) {
         if(n > 0) { k_inv_diag64<<<nb, 256, 0, s>>>(n, diag, w.inv64); bnn_note_launch(); }
         rc = pcg_solve_t<double>(w, n, rhs, diag, w.inv64, nbr, rec, coef, coefRow, -(double)(1.0f * dt), (double)tol, maxIter, w.x64,
-                                 w.r64, w.z64, w.s064, w.s164, w.q64, w.partMaxD, dst, hst, s, out);
+                                 w.r64, w.z64, w.s064, w.s164, w.q64, w.partMaxD, two, dst, hst, s, out);
         if(rc != BNN_OK) return rc;
         if(n > 0) { k_d64_to_f32<<<nb, 256, 0, s>>>(n, w.x64, pressure); bnn_note_launch(); }
         if(x64out && n > 0)
@@ -877,7 +1298,7 @@ int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const floa
         { k_ir_to_f32<<<nb, 256, 0, s>>>(n, w.r64, w.r32); bnn_note_launch(); }
         PcgOutcome inner;
         rc = pcg_solve_t<float>(w, n, w.r32, diag, invd, nbr, rec, coef, coefRow, -(1.0f * dt), innerTol, maxIter, w.d32, w.r, w.z, w.s0,
-                                w.s1, w.q, w.partMaxF, dst, hst, s, inner);
+                                w.s1, w.q, w.partMaxF, two, dst, hst, s, inner);
         if(rc != BNN_OK) return rc;
         total += inner.iterations;
         kernelMs += inner.kernelMs;

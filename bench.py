@@ -61,6 +61,15 @@ WORKLOAD = "flip_dam_break_256"
 PCG_TRAFFIC_PER_ITER = 835.7e6 / 300
 
 
+PCG_MODE = {"fp32": 0, "fp64": 1, "refined": 2}
+
+
+def _pcg_flags(args) -> int:
+    """BNN_PCG_TWO_REDUCTIONS when the PCGSolver step order (two reductions per iteration)
+    is asked for; the default is the single-reduction form of the same iteration"""
+    return 0x10 if getattr(args, "pcg_steps", "single") == "two" else 0
+
+
 def _config(pcg_mode: str, cfg: dict | None = None, pcg_text: str | None = None):
     if pcg_text is not None:
         pcg = pcg_text
@@ -185,13 +194,14 @@ def stage_bytes(npart: int, G: int, rows: float, iters: float) -> dict:
     """Algorithmic bytes of one sub-step's stages (each array touched once per stage, FP32):
     Np particles, C = G^3 cells, F = 3 (G+1) G^2 faces, A active rows, K PCG iterations.
     The G2P and the next move share one entry (the particle pass: grid-to-particle blend,
-    RK2 advection, box projection); extrapolation counts 10 F per call (4 layers fused),
-    the first call with the 4 F backup of the FLIP old velocities."""
+    RK2 advection, box projection), and so do P2G and the fluid SDF (one tiled pass over
+    the particles); extrapolation counts 10 F per call (4 layers fused), the first call
+    with the 4 F backup of the FLIP old velocities."""
     C = float(G) ** 3
     F = 3.0 * (G + 1) * float(G) ** 2
     Np, A = float(npart), float(rows)
-    return {"sort": 72.0 * Np + 12.0 * C, "p2g": 24.0 * Np + 5.0 * F, "extrapolate": 10.0 * F + 4.0 * F,
-            "fluid_sdf": 12.0 * Np + 4.0 * C, "system": 8.0 * C + 28.0 * A, "pcg": 52.0 * A * iters,
+    return {"sort": 72.0 * Np + 12.0 * C, "p2g+fluid_sdf": (24.0 * Np + 5.0 * F) + (12.0 * Np + 4.0 * C),
+            "extrapolate": 10.0 * F + 4.0 * F, "system": 8.0 * C + 28.0 * A, "pcg": 52.0 * A * iters,
             "update": 9.0 * F + 4.0 * A + 10.0 * F, "move+g2p": 48.0 * Np + 8.0 * F}
 
 
@@ -204,6 +214,7 @@ def _stage_gbs(npart, G, stats, stage_tot):
             tot[k] = tot.get(k, 0.0) + b
     ms = dict(stage_tot)
     ms["move+g2p"] = stage_tot["move"] + stage_tot["g2p"]
+    ms["p2g+fluid_sdf"] = stage_tot["p2g"] + stage_tot["fluid_sdf"]
     return {k: (tot[k] / (ms[k] * 1e-3) / 1e9 if ms.get(k, 0) > 0 else None) for k in tot}
 
 
@@ -300,7 +311,7 @@ def run_ours(args, ws, rank, local):
             dist.barrier()
 
     pcg_mode = args.pcg_mode
-    cfg = scenes.dam_break_params(N_GRID, pcg_mode={"fp32": 0, "fp64": 1, "refined": 2}[pcg_mode])
+    cfg = scenes.dam_break_params(N_GRID, pcg_mode={"fp32": 0, "fp64": 1, "refined": 2}[pcg_mode] | _pcg_flags(args))
     if args.inner_tol is not None:
         cfg["refine_inner_tolerance"] = args.inner_tol
     if args.tol is not None:
@@ -511,56 +522,34 @@ def run_batch(args, ws, rank, local):
 
 
 def run_serve(args, ws, rank, local):
-    """Poisson request stream: each request is a scene that runs 200 sub-steps."""
+    """Poisson request stream: each request is a scene that runs 200 sub-steps, served by
+    banana_b200.serving.SceneServer (admission against the HBM budget, continuous
+    batching)."""
     torch, dist = _torch_dist(ws, local)
-    from banana_b200 import BnnError, FlipBatch, capi, scenes
+    from banana_b200 import FlipBatch, capi, scenes
+    from banana_b200.serving import Request, SceneServer
 
     reqs = scenes.serve_requests(args.requests)
-    mine = [q for k, q in enumerate(reqs) if k % ws == rank]
+    mine = [(k, q) for k, q in enumerate(reqs) if k % ws == rank]
     budget = int(150e9)
     b = FlipBatch(hbm_budget_bytes=budget, worker_threads=args.workers)
-    steps_per_req = args.req_steps
-    queue = list(mine)
-    live = {}
-    done_lat, step_lat = [], []
-    ps = 0
+    server = SceneServer(b)
+    stream = []
+    for k, q in mine:
+        cfg, pos, vel = scenes.batch_scene(q)
+        stream.append(Request(k, cfg, pos, vel, args.req_steps, q["t"]))
     launches0 = capi.launch_count()
     clocks = ClockSampler(local)
     clocks.start()
     t0 = time.perf_counter()
-    while queue or live:
-        now = time.perf_counter() - t0
-        if now > args.time_limit:
-            break  # bounded run: report what completed
-        while queue and queue[0]["t"] <= now:
-            q = queue[0]
-            cfg, pos, vel = scenes.batch_scene(q)
-            try:
-                sid = b.add_scene(cfg, pos, vel)
-            except BnnError as e:
-                if e.code != 8:
-                    raise
-                break  # over budget: wait for a running request to finish
-            live[sid] = q
-            queue.pop(0)
-        if not live:
-            time.sleep(max(0.0, min(queue[0]["t"] - now, 0.05)))
-            continue
-        st = b.step()
-        step_lat.append(st["wall_ms"])
-        ps += st["particle_steps"]
-        for sid in list(live):
-            if b.scene_info(sid)["steps"] >= steps_per_req:
-                b.get_scene(sid)
-                done_lat.append(time.perf_counter() - t0 - live[sid]["t"])
-                b.remove_scene(sid)
-                del live[sid]
+    results = server.run(stream, time_limit=args.time_limit)
     te = time.perf_counter() - t0
     clk = clocks.stop()
     launches = capi.launch_count() - launches0
-    tot = ps
+    summ = server.stats.summary(results, te)
+    tot = server.stats.particle_steps
     if ws > 1:
-        v = torch.tensor([ps], dtype=torch.float64, device="cuda")
+        v = torch.tensor([tot], dtype=torch.float64, device="cuda")
         dist.all_reduce(v)
         tot = float(v.item())
         t = torch.tensor([te], dtype=torch.float64, device="cuda")
@@ -568,16 +557,18 @@ def run_serve(args, ws, rank, local):
         te = float(t.item())
     if rank == 0:
         line = {"metric": "served particle-steps/s, Poisson dam-break requests", "value": tot / te, "unit": UNIT,
-                "n_gpus": ws, "steps": len(step_lat), "warmup": 0, "ms_per_step": float(np.mean(step_lat)),
+                "n_gpus": ws, "steps": summ["batch_steps"], "warmup": 0,
+                "ms_per_step": float(np.mean(server.stats.step_ms)) if server.stats.step_ms else None,
                 "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded request stream, seed 13)",
                 "config": {"workload": "serve_poisson", "requests": len(reqs), "rate_per_s": 20,
-                           "res": "cubic, log-uniform 32..192", "steps_per_request": steps_per_req,
-                           "hbm_budget_gb": 150, "pcg": "refined FP32 to 1e-8", "parallelism": f"requests/{ws} ranks"},
-                "completed_requests": len(done_lat),
-                "request_latency_s": {"p50": float(np.percentile(done_lat, 50)) if done_lat else None,
-                                      "p99": float(np.percentile(done_lat, 99)) if done_lat else None},
-                "step_latency_ms": {"p50": float(np.percentile(step_lat, 50)), "p99": float(np.percentile(step_lat, 99))},
+                           "res": "cubic, log-uniform 32..192", "steps_per_request": args.req_steps,
+                           "hbm_budget_gb": 150, "pcg": "refined FP32 to 1e-8", "parallelism": f"requests/{ws} ranks",
+                           "time_limit_s": args.time_limit},
+                "completed_requests": summ["completed"], "admitted_requests": summ["admitted"],
+                "waits_for_memory": summ["waits_for_memory"], "max_running": summ["max_running"],
+                "request_latency_s": summ["request_latency_s"], "queue_wait_s": summ["queue_wait_s"],
+                "step_latency_ms": summ["step_latency_ms"], "seconds": te,
                 "gpu_launches": int(launches), "clocks": clk}
         print(json.dumps(line), flush=True)
     b.close()
@@ -793,9 +784,9 @@ def run_pcg(args, ws, rank, local):
     diag, nbr, off, rhs = _box_system(102, 153, 102)
     n = len(rhs)
     for _ in range(args.warmup):
-        pcg_solve_7pt(diag, nbr, off, rhs, 1e-30, args.steps, mode=args.pcg_mode)
+        pcg_solve_7pt(diag, nbr, off, rhs, 1e-30, args.steps, mode=PCG_MODE[args.pcg_mode] | _pcg_flags(args))
     launches0 = capi.launch_count()
-    _, st = pcg_solve_7pt(diag, nbr, off, rhs, 1e-30, args.steps, mode=args.pcg_mode)
+    _, st = pcg_solve_7pt(diag, nbr, off, rhs, 1e-30, args.steps, mode=PCG_MODE[args.pcg_mode] | _pcg_flags(args))
     launches = capi.launch_count() - launches0
     it = max(st["iterations"], 1)
     us = 1e3 * st["ms"] / it
@@ -806,7 +797,8 @@ def run_pcg(args, ws, rank, local):
                 "n_gpus": 1, "steps": it, "warmup": args.warmup, "ms_per_step": st["ms"], "higher_is_better": False,
                 "scaling": "replicas", "vs_baseline": None, "dtype": args.pcg_mode,
                 "data": "synthetic (box of fluid cells, random rhs, seed 1)",
-                "config": {"workload": "pcg_box_102x153x102", "rows": n, "pcg": f"Jacobi, {args.pcg_mode}",
+                "config": {"workload": "pcg_box_102x153x102", "rows": n,
+                           "pcg": f"Jacobi, {args.pcg_mode}, {args.pcg_steps} reduction step order",
                            "layout": "grid rows (packed 16-byte records)"},
                 "roofline": {"bound": "hbm", "kernel": "k_pcg_persistent", "achieved": achieved, "peak": peak,
                              "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
@@ -900,6 +892,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--pcg-mode", choices=["fp32", "fp64", "refined"], default="fp32")
+    ap.add_argument("--pcg-steps", choices=["single", "two"], default="single",
+                    help="PCG iteration form: single reduction (default) or PCGSolver's two-reduction order")
     ap.add_argument("--inner-tol", type=float, default=None, help="refined PCG: inner (FP32) relative tolerance")
     ap.add_argument("--tol", type=float, default=None,
                     help="fp32 / fp64 PCG: relative tolerance (the refined mode's outer tolerance is 1e-8)")

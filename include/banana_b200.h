@@ -52,6 +52,13 @@ extern "C" {
 #define BNN_PCG_FP32      0  /* FP32 vectors, FP64 dot/norm reductions */
 #define BNN_PCG_FP64      1  /* FP64 vectors and reductions */
 #define BNN_PCG_REFINED   2  /* FP32 inner PCG + FP64 outer residual (iterative refinement) */
+#define BNN_PCG_MODE_MASK 0x0f
+/* OR-ed into a BNN_PCG_* mode: take PCGSolver::solve_precond's own step order (two inner
+ * products formed one after the other, PCGSolver.cpp:143-199: two grid-wide reductions per
+ * iteration).  Without it the solve uses the single-reduction form of the same iteration
+ * (Chronopoulos & Gear: both inner products in one reduction), which gives the same
+ * iterates up to rounding. */
+#define BNN_PCG_TWO_REDUCTIONS 0x10
 
 #define BNN_PRECOND_JACOBI 0 /* PCGSolver::JACOBI (PCGSolver.cpp:232-237,273-284) */
 
@@ -85,7 +92,7 @@ typedef struct bnn_params {
     uint32_t max_cg_iteration;       /* MaxCGIteration */
     uint32_t advection_steps;        /* AdvectionSteps (default 1) */
     int32_t  solver_kind;            /* BNN_SOLVER_* */
-    int32_t  pcg_mode;               /* BNN_PCG_* */
+    int32_t  pcg_mode;               /* BNN_PCG_*, optionally | BNN_PCG_TWO_REDUCTIONS */
     int32_t  preconditioner;         /* BNN_PRECOND_* */
     float    refine_tolerance;       /* BNN_PCG_REFINED: outer max-norm relative tolerance */
     float    refine_inner_tolerance; /* BNN_PCG_REFINED: inner FP32 relative tolerance (1e-2 is
@@ -230,9 +237,12 @@ int bnn_z_sort(const float* pos_dev, uint32_t n, float radius, uint64_t* zvalue_
 
 /* NeighborSearch::find_neighbors for one self-searching point set (NeighborSearch.cpp:
  * 219-226, query3D :530-692): neighbours of each point are all other points with
- * |x-y|^2 < r^2.  Output CSR: offsets_dev (n+1), idx_dev (capacity entries), each list
- * sorted ascending.  *total receives the entry count; BNN_ERR_CAPACITY when it exceeds
- * capacity (offsets are still written). */
+ * |x-y|^2 < r^2.  Output CSR: offsets_dev (n+1), idx_dev (capacity entries).  A list holds
+ * its points in the order the 27 cells around the point are visited (z, y, x major; a
+ * cell's points in sorted-index order), deterministic but not ascending -- the
+ * reference's own order depends on its thread schedule, so lists compare as sets.
+ * *total receives the entry count; BNN_ERR_CAPACITY when it exceeds capacity (offsets are
+ * still written). */
 int bnn_neighbors(const float* pos_dev, uint32_t n, float radius, uint64_t* offsets_dev, uint32_t* idx_dev,
                   uint64_t capacity, uint64_t* total, void* stream);
 

@@ -29,12 +29,16 @@
 //    * REDUCE_CANONICAL : FP64 accumulation in fixed 2048-element chunks, 256 lanes per
 //                         chunk, each lane summing 8 strided elements, then a halving
 //                         tree; chunk partials reduced the same way.  This is the order
-//                         the CUDA kernels use, so the two agree bit for bit.
+//                         the CUDA kernels use, so the two agree bit for bit (FLIP's P2G
+//                         also takes the kernels' order in this mode, below).
 //  Particles are re-ordered by a stable counting sort on the cell index before each
 //  P2G (the reference's Grid::collectIndexToCells + getParticleIdxSortedByCell +
-//  sortData, run on one thread, BananaCore/Banana/Grid/Grid.cpp:92-114,283-309), which
-//  fixes the order in which P2G sums.  particle ids travel with the particles so the
-//  caller always sees the original order.
+//  sortData, run on one thread, BananaCore/Banana/Grid/Grid.cpp:92-114,283-309).  In the
+//  reference mode P2G then sums serially in that particle order (the reference on one
+//  thread); in the canonical mode FLIP's P2G sums each face in the CUDA kernel's
+//  two-level order (per-cell partials in id order, added in (y, z, x)-major cell order;
+//  see mapP2GCanonical).  particle ids travel with the particles so the caller always sees
+//  the original order.
 //
 //  Compile with -ffp-contract=off (no fused multiply-add): every float operation is
 //  then a single IEEE-rounded operation, as in the reference built for SSE.
@@ -124,6 +128,9 @@ template<class T> struct Arr3 {
 // ----------------------------------------------------------------------------------
 static constexpr int kChunk = 2048;
 static constexpr int kLanes = 256;
+// pcg_mode: BNN_PCG_* in the low bits, the flag for PCGSolver's two-reduction step order
+static constexpr int kPcgModeMask = 0x0f;
+static constexpr int kPcgTwoReductions = 0x10;
 
 static double tree256(double* s) {
     for(int off = kLanes / 2; off > 0; off >>= 1)
@@ -199,7 +206,8 @@ struct orc_params {
     uint32_t max_cg_iteration;      // MaxCGIteration
     uint32_t advection_steps;       // AdvectionSteps
     int32_t  reduce_mode;           // 0 reference order, 1 canonical FP64 order
-    int32_t  pcg_mode;              // 0 FP32 vectors, 1 FP64 vectors, 2 FP32 inner + FP64 refinement
+    int32_t  pcg_mode;              // 0 FP32 vectors, 1 FP64 vectors, 2 FP32 inner + FP64 refinement;
+                                    // | 0x10: two-reduction step order (else single reduction)
     int32_t  preconditioner;        // 0 Jacobi, 1 MICCL0, 2 MICCL0_SYMMETRIC
     float    refine_tolerance;      // outer tolerance for pcg_mode 2 (max-norm, relative)
     float    refine_inner_tolerance;// inner FP32 tolerance for pcg_mode 2
@@ -447,12 +455,80 @@ static PCGResult pcg_canonical(const CSR& A, const std::vector<float>& vals, con
     return out;
 }
 
+// The single-reduction form of the same Jacobi PCG (Chronopoulos & Gear) with the CUDA
+// kernel's arithmetic: u = D^-1 r, w = A u, gamma = (r, u) and delta = (w, u) in one
+// canonical FP64 reduction; beta = gamma / gamma_old and alpha = gamma / (delta -
+// beta gamma / alpha_old) in FP64, rounded to VT; p = u + beta p, s = w + beta s,
+// x += alpha p, r -= alpha s.  Same iterates as pcg_canonical in exact arithmetic
+// (PCGSolver::solve_precond, PCGSolver.cpp:143-199), same stopping rule on max|r|.
+template<class VT>
+static PCGResult pcg_canonical_cg1(const CSR& A, const std::vector<float>& vals, const std::vector<float>& diag,
+                                   const std::vector<VT>& rhs, std::vector<VT>& x, VT tolFactor, uint32_t maxIters) {
+    PCGResult out;
+    const size_t n = A.n;
+    tolFactor = std::fmax(tolFactor, VT(1e-30));
+    x.assign(n, 0);
+    std::vector<VT> r = rhs, u(n), w(n), p(n, VT(0)), s(n, VT(0)), inv(n);
+    for(size_t i = 0; i < n; ++i) inv[i] = diag[i] != 0 ? VT(1.0) / (VT)diag[i] : VT(0);
+    for(size_t i = 0; i < n; ++i) u[i] = inv[i] * r[i];
+    spmv(A, vals, u.data(), w.data(), 1);
+    VT resid = max_abs(r.data(), n);
+    out.residual = resid;
+    double gamma = dot_canonical(u.data(), r.data(), n);
+    double delta = dot_canonical(w.data(), u.data(), n);
+    if(resid < (VT)std::numeric_limits<float>::min()) { out.success = true; return out; }
+    const VT tol = tolFactor * resid;
+    if(gamma < (double)std::numeric_limits<float>::min() || std::isnan(gamma)) { out.success = false; return out; }
+    double gammaOld = 0.0, a64Old = 0.0;
+    bool first = true;
+    for(uint32_t it = 0; it < maxIters; ++it) {
+        double b64 = 0.0, den = delta;
+        if(!first) {
+            b64 = gamma / gammaOld;
+            den = delta - (b64 * gamma) / a64Old;
+        }
+        if(den < (double)std::numeric_limits<float>::min()) { out.iterations = it + 1; out.success = true; return out; }
+        const double a64 = gamma / den;
+        const VT alpha = (VT)a64, beta = (VT)b64;
+        for(size_t i = 0; i < n; ++i) {
+            const VT uOld = inv[i] * r[i];
+            p[i] = first ? uOld : uOld + beta * p[i];
+            s[i] = first ? w[i] : w[i] + beta * s[i];
+            x[i] = x[i] + alpha * p[i];
+            r[i] = r[i] + (-alpha) * s[i];
+            u[i] = inv[i] * r[i];
+        }
+        spmv(A, vals, u.data(), w.data(), 1);
+        resid = max_abs(r.data(), n);
+        out.residual = resid;
+        const double gNew = dot_canonical(u.data(), r.data(), n);
+        const double dNew = dot_canonical(w.data(), u.data(), n);
+        if(resid < tol) { out.iterations = it + 1; out.success = true; return out; }
+        gammaOld = gamma;
+        gamma = gNew;
+        delta = dNew;
+        a64Old = a64;
+        first = false;
+    }
+    out.iterations = maxIters; out.success = false;
+    return out;
+}
+
+// The canonical solve of either form: the single-reduction one unless twoReductions.
+template<class VT>
+static PCGResult pcg_canonical_any(const CSR& A, const std::vector<float>& vals, const std::vector<float>& diag,
+                                   const std::vector<VT>& rhs, std::vector<VT>& x, VT tolFactor, uint32_t maxIters,
+                                   bool twoReductions) {
+    return twoReductions ? pcg_canonical<VT>(A, vals, diag, rhs, x, tolFactor, maxIters)
+                         : pcg_canonical_cg1<VT>(A, vals, diag, rhs, x, tolFactor, maxIters);
+}
+
 // Mixed-precision iterative refinement: FP64 outer residual and solution, FP32 inner
 // Jacobi PCG (canonical arithmetic) on the residual.  Stops when
 // max|b - A x| < outerTol * max|b|.
 static PCGResult pcg_refined(const CSR& A, const std::vector<float>& vals, const std::vector<float>& diag,
                              const std::vector<float>& rhs, std::vector<double>& x, float innerTol, double outerTol,
-                             uint32_t maxIters, uint32_t maxOuter = 60) {
+                             uint32_t maxIters, bool twoReductions, uint32_t maxOuter = 60) {
     PCGResult out;
     size_t n = A.n;
     std::vector<double> vals64(vals.begin(), vals.end());
@@ -467,7 +543,7 @@ static PCGResult pcg_refined(const CSR& A, const std::vector<float>& vals, const
     while(!ok && outer < maxOuter) {
         if(res < outerTol * bmax) { ok = true; break; }
         for(size_t i = 0; i < n; ++i) r32[i] = (float)r64[i];
-        PCGResult inner = pcg_canonical<float>(A, vals, diag, r32, d, innerTol, maxIters);
+        PCGResult inner = pcg_canonical_any<float>(A, vals, diag, r32, d, innerTol, maxIters, twoReductions);
         total += inner.iterations;
         for(size_t i = 0; i < n; ++i) x[i] = x[i] + (double)d[i];
         spmv(A, vals64, x.data(), ax.data(), 1);
@@ -983,6 +1059,93 @@ public:
         w[7] = fi * fj * fk;
     }
 
+    // FLIP P2G with the sums in the canonical two-level order of the CUDA kernel: for every
+    // face, the particles of each candidate cell (two along the component's own axis, three
+    // along the others, clamped to the grid) are summed in id order into a per-cell
+    // partial, and the face adds its candidate cells' partials in (y, z, x)-major cell
+    // order, both sums starting at +0.  The products are those of mapP2G
+    // (getCoordinatesAndWeights, ArrayHelpers.cpp:50-76, weight = wx * wy * wz left to
+    // right, momentum = weight * v); only the association of the sums differs from the
+    // reference's serial loop, whose CAS-atomic parallel form (FLIP_Solver.cpp:57-95,
+    // AtomicOperations.h:31-49) has no fixed order.  Needs the particles sorted by
+    // (cell, id).  Faces are independent, so this runs on any number of threads with the
+    // same result.
+    void mapP2GCanonical() {
+        const size_t n = pos.size(), C = (size_t)G[0] * G[1] * G[2];
+        std::vector<uint32_t> start(C + 1, 0);
+        for(size_t p = 0; p < n; ++p) start[cellLinear(pos[p]) + 1]++;
+        for(size_t c = 0; c < C; ++c) start[c + 1] += start[c];
+        // stencil base index and fraction of every particle, component and axis
+        std::vector<int> base(n * 9);
+        std::vector<R> frac(n * 9);
+#pragma omp parallel for schedule(static) if(nthreads() > 1)
+        for(long long p = 0; p < (long long)n; ++p) {
+            R g[3];
+            gridCoord(pos[p], g);
+            for(int d = 0; d < 3; ++d)
+                for(int a = 0; a < 3; ++a) {
+                    const int size = G[a] + (a == d ? 1 : 0);
+                    int i; R f;
+                    get_barycentric(g[a] - (a == d ? R(0) : R(0.5)), i, f, 0, size);
+                    base[(size_t)p * 9 + d * 3 + a] = i;
+                    frac[(size_t)p * 9 + d * 3 + a] = f;
+                }
+        }
+        for(int d = 0; d < 3; ++d) {
+            Arr3<R>& out = u[d];
+            Arr3<R>& wsum = tmp[d];
+            std::fill(valid[d].d.begin(), valid[d].d.end(), 0);
+            const int sx = out.sx, sy = out.sy, sz = out.sz;
+#pragma omp parallel for schedule(static) if(nthreads() > 1)
+            for(long long li = 0; li < (long long)out.size(); ++li) {
+                const int f[3] = {(int)(li % sx), (int)((li / sx) % sy), (int)(li / ((long long)sx * sy))};
+                int lo[3], hi[3];
+                for(int a = 0; a < 3; ++a) {
+                    lo[a] = std::max(f[a] - 1, 0);
+                    hi[a] = std::min(a == d ? f[a] : f[a] + 1, G[a] - 1);
+                }
+                R S = R(0), W = R(0);
+                for(int cy = lo[1]; cy <= hi[1]; ++cy)
+                    for(int cz = lo[2]; cz <= hi[2]; ++cz)
+                        for(int cx = lo[0]; cx <= hi[0]; ++cx) {
+                            const size_t c = ((size_t)cz * G[1] + cy) * G[0] + cx;
+                            R PS = R(0), PW = R(0);
+                            for(uint32_t q = start[c]; q < start[c + 1]; ++q) {
+                                const int* b = &base[(size_t)q * 9 + d * 3];
+                                const R* fr = &frac[(size_t)q * 9 + d * 3];
+                                R w3[3];
+                                bool reach = true;
+                                for(int a = 0; a < 3; ++a) {
+                                    if(f[a] == b[a]) w3[a] = R(1.0) - fr[a];
+                                    else if(f[a] == b[a] + 1) w3[a] = fr[a];
+                                    else reach = false;
+                                }
+                                if(!reach) continue;
+                                const R w = w3[0] * w3[1] * w3[2];
+                                PS = PS + w * vel[q][d];
+                                PW = PW + w;
+                            }
+                            S = S + PS;
+                            W = W + PW;
+                        }
+                out.d[li] = S;
+                wsum.d[li] = W;
+            }
+#pragma omp parallel for schedule(static) if(nthreads() > 1)
+            for(long long i = 0; i < (long long)out.size(); ++i) {
+                R w = wsum.d[i];
+                if(w > std::numeric_limits<R>::min()) { out.d[i] /= w; valid[d].d[i] = 1; }
+            }
+        }
+    }
+
+    // Which P2G the step runs: FLIP in the canonical mode takes the two-level order above;
+    // every other case the reference's serial loop.
+    void splatParticles() {
+        if(P.solver_kind == 0 && P.reduce_mode == 1 && (P.sort_each_step || P.correct_position)) mapP2GCanonical();
+        else mapP2G();
+    }
+
     // FLIP_Solver::mapParticles2Grid (FLIP_Solver.cpp:57-95); APIC adds the affine term
     // (APIC_Solver.cpp:53-91).  Serial in particle-array order.
     void mapP2G() {
@@ -1222,18 +1385,21 @@ public:
         }
         std::vector<float> valsF(Avals.begin(), Avals.end());
         std::vector<float> rhsF(rhs.begin(), rhs.end());
-        if(P.pcg_mode == 0) {
+        const int mode = P.pcg_mode & kPcgModeMask;
+        const bool two = (P.pcg_mode & kPcgTwoReductions) != 0;
+        if(mode == 0) {
             std::vector<float> x;
-            lastSolve = pcg_canonical<float>(A, valsF, Adiag, rhsF, x, (float)tolf, P.max_cg_iteration);
+            lastSolve = pcg_canonical_any<float>(A, valsF, Adiag, rhsF, x, (float)tolf, P.max_cg_iteration, two);
             for(size_t i = 0; i < x.size(); ++i) pressure[i] = (R)x[i];
-        } else if(P.pcg_mode == 1) {
+        } else if(mode == 1) {
             std::vector<double> x, r64(rhsF.begin(), rhsF.end());
-            lastSolve = pcg_canonical<double>(A, valsF, Adiag, r64, x, (double)P.cg_relative_tolerance, P.max_cg_iteration);
+            lastSolve = pcg_canonical_any<double>(A, valsF, Adiag, r64, x, (double)P.cg_relative_tolerance,
+                                                  P.max_cg_iteration, two);
             for(size_t i = 0; i < x.size(); ++i) pressure[i] = (R)(float)x[i];
         } else {
             std::vector<double> x;
             lastSolve = pcg_refined(A, valsF, Adiag, rhsF, x, P.refine_inner_tolerance, (double)P.refine_tolerance,
-                                    P.max_cg_iteration);
+                                    P.max_cg_iteration, two);
             for(size_t i = 0; i < x.size(); ++i) pressure[i] = (R)(float)x[i];
         }
     }
@@ -1359,7 +1525,7 @@ public:
         // PIC_Solver::advanceVelocity (PIC_Solver.cpp:332-338): advect the grid velocity,
         // gravity, projection, extrapolation; the particles only carry the fluid SDF
         if(kind == 3) advectGrid(substep);
-        else mapP2G();
+        else splatParticles();
         double t3 = now();
         if(kind != 1 && kind != 3) {
             extrapolateAll(); // APIC goes straight to gravity (APIC_Solver.cpp:42-49)
@@ -1572,8 +1738,8 @@ int orc_step(void* hp, orc_step_stats* st) {
 // for analytic checks of the transfer
 int orc_p2g_only(void* hp) {
     auto* h = (orc_handle*)hp;
-    if(h->dbl) { h->d->sortParticlesByCell(); h->d->mapP2G(); }
-    else { h->f->sortParticlesByCell(); h->f->mapP2G(); }
+    if(h->dbl) { h->d->sortParticlesByCell(); h->d->splatParticles(); }
+    else { h->f->sortParticlesByCell(); h->f->splatParticles(); }
     return 0;
 }
 
@@ -1594,7 +1760,8 @@ void orc_get_system(void* hp, uint32_t* rowStart, uint32_t* colIndex, float* val
 
 // Standalone PCG on a CSR system (rows column-sorted), in the chosen arithmetic.
 // mode: 0 canonical FP32, 1 canonical FP64, 2 refined, 3 reference FP32 (precond 0/1/2),
-// 4 reference FP64.
+// 4 reference FP64; modes 0-2 take the single-reduction form unless kPcgTwoReductions is
+// OR-ed in.
 int orc_pcg(uint32_t n, const uint32_t* rowStart, const uint32_t* colIndex, const float* vals, const float* rhs,
             float tol, uint32_t maxIter, int mode, int precond, float innerTol, double* x_out, uint32_t* iters,
             double* resid, uint32_t* outer) {
@@ -1608,15 +1775,17 @@ int orc_pcg(uint32_t n, const uint32_t* rowStart, const uint32_t* colIndex, cons
         for(uint32_t j = rowStart[r]; j < rowStart[r + 1]; ++j) if(colIndex[j] == r) diag[r] = vals[j];
     std::vector<float> b(rhs, rhs + n);
     PCGResult res;
+    const bool two = (mode & kPcgTwoReductions) != 0;
+    mode &= kPcgModeMask;
     if(mode == 0) {
-        std::vector<float> x; res = pcg_canonical<float>(A, v, diag, b, x, tol, maxIter);
+        std::vector<float> x; res = pcg_canonical_any<float>(A, v, diag, b, x, tol, maxIter, two);
         for(uint32_t i = 0; i < n; ++i) x_out[i] = x[i];
     } else if(mode == 1) {
         std::vector<double> x, b64(b.begin(), b.end());
-        res = pcg_canonical<double>(A, v, diag, b64, x, (double)tol, maxIter);
+        res = pcg_canonical_any<double>(A, v, diag, b64, x, (double)tol, maxIter, two);
         for(uint32_t i = 0; i < n; ++i) x_out[i] = x[i];
     } else if(mode == 2) {
-        std::vector<double> x; res = pcg_refined(A, v, diag, b, x, innerTol, (double)tol, maxIter);
+        std::vector<double> x; res = pcg_refined(A, v, diag, b, x, innerTol, (double)tol, maxIter, two);
         for(uint32_t i = 0; i < n; ++i) x_out[i] = x[i];
     } else if(mode == 3) {
         std::vector<float> x; res = pcg_reference<float>(A, v, b, x, tol, maxIter, precond, 1);
