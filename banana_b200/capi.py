@@ -20,9 +20,9 @@ STATUS = {0: "OK", 1: "INVALID_ARGUMENT", 2: "OUT_OF_MEMORY", 3: "PCG_NOT_CONVER
 STATUS_CODE = {v: k for k, v in STATUS.items()}
 SOLVER_KIND = {"FLIP": 0, "APIC": 1, "AFLIP": 2, "PIC": 3}
 PCG_MODE = {"fp32": 0, "fp64": 1, "refined": 2}
-# OR-ed into a PCG mode: PCGSolver::solve_precond's two-reduction step order instead of the
-# default single-reduction form (include/banana_b200.h BNN_PCG_TWO_REDUCTIONS)
-PCG_TWO_REDUCTIONS = 0x10
+# OR-ed into a PCG mode: the single-reduction form of the iteration instead of the default
+# PCGSolver::solve_precond step order (include/banana_b200.h BNN_PCG_SINGLE_REDUCTION)
+PCG_SINGLE_REDUCTION = 0x10
 FIELD = {"u": 0, "v": 1, "w": 2, "phi": 3, "pressure": 4, "old_u": 5, "old_v": 6, "old_w": 7, "active": 8,
          "weight_u": 9, "weight_v": 10, "weight_w": 11, "boundary_sdf": 12}
 GEOMETRY = {"box": 0, "sphere": 1}

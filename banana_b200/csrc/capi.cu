@@ -217,7 +217,7 @@ extern "C" int bnn_flip_create(const bnn_params* params, bnn_flip** out) {
     const bnn_params& P = *params;
     if(!(P.cell_size > 0.f) || P.advection_steps == 0) return BNN_ERR_INVALID_ARGUMENT;
     if(P.solver_kind < 0 || P.solver_kind > 3) return BNN_ERR_NOT_SUPPORTED;
-    if((P.pcg_mode & ~(BNN_PCG_MODE_MASK | BNN_PCG_TWO_REDUCTIONS)) != 0 || (P.pcg_mode & BNN_PCG_MODE_MASK) > 2 ||
+    if((P.pcg_mode & ~(BNN_PCG_MODE_MASK | BNN_PCG_SINGLE_REDUCTION)) != 0 || (P.pcg_mode & BNN_PCG_MODE_MASK) > 2 ||
        P.preconditioner != BNN_PRECOND_JACOBI)
         return BNN_ERR_NOT_SUPPORTED;
     for(int d = 0; d < 3; ++d) if(!(P.box_max[d] > P.box_min[d])) return BNN_ERR_INVALID_ARGUMENT;
@@ -869,7 +869,7 @@ extern "C" int bnn_pcg_barrier_probe(float limit_seconds, int32_t* barrier_statu
 extern "C" int bnn_pcg_solve_7pt(uint32_t n, const float* diag, const int32_t* nbr, float offdiag, const float* rhs,
                                  float tol, uint32_t max_iter, int32_t mode, float inner_tol, double* x_out,
                                  bnn_pcg_stats* stats) {
-    if(!diag || !nbr || !rhs || !x_out || (mode & ~(BNN_PCG_MODE_MASK | BNN_PCG_TWO_REDUCTIONS)) != 0 ||
+    if(!diag || !nbr || !rhs || !x_out || (mode & ~(BNN_PCG_MODE_MASK | BNN_PCG_SINGLE_REDUCTION)) != 0 ||
        (mode & BNN_PCG_MODE_MASK) > 2)
         return BNN_ERR_INVALID_ARGUMENT;
     if(!(offdiag <= 0.f)) return BNN_ERR_INVALID_ARGUMENT;

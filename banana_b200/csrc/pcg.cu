@@ -1239,14 +1239,14 @@ static int pcg_solve_t(PcgWork& w, int n, const float* rhsF, const float* diag, 
     return BNN_OK;
 }
 
-// mode: BNN_PCG_FP32 / FP64 / REFINED, optionally with BNN_PCG_TWO_REDUCTIONS.  Pressure
+// mode: BNN_PCG_FP32 / FP64 / REFINED, optionally with BNN_PCG_SINGLE_REDUCTION.  Pressure
 // written to `pressure` (float, n).
 int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const float* invd, const int32_t* nbr,
               const float* coef, bool gridRows, float dt, int modeFlags, float tol, unsigned maxIter, float innerTol,
               float outerTol, float* pressure, double* x64out, DevState* dst, DevState* hst, cudaStream_t s,
               PcgOutcome& out) {
     const int mode = modeFlags & BNN_PCG_MODE_MASK;
-    const bool two = (modeFlags & BNN_PCG_TWO_REDUCTIONS) != 0;
+    const bool two = (modeFlags & BNN_PCG_SINGLE_REDUCTION) == 0;
     int rc = pcg_reserve(w, n, mode != BNN_PCG_FP32);
     if(rc != BNN_OK) return rc;
     const unsigned nb = (unsigned)((n + 255) / 256);

@@ -65,9 +65,9 @@ PCG_MODE = {"fp32": 0, "fp64": 1, "refined": 2}
 
 
 def _pcg_flags(args) -> int:
-    """BNN_PCG_TWO_REDUCTIONS when the PCGSolver step order (two reductions per iteration)
-    is asked for; the default is the single-reduction form of the same iteration"""
-    return 0x10 if getattr(args, "pcg_steps", "single") == "two" else 0
+    """BNN_PCG_SINGLE_REDUCTION when the single-reduction form is asked for; the default is
+    PCGSolver's step order (two reductions per iteration)"""
+    return 0x10 if getattr(args, "pcg_steps", "two") == "single" else 0
 
 
 def _config(pcg_mode: str, cfg: dict | None = None, pcg_text: str | None = None):
@@ -504,7 +504,7 @@ def run_batch(args, ws, rank, local):
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scenes, seed 11)",
                 "config": {"workload": "batch_256_scenes", "scenes": len(specs), "scenes_rank0": len(mine),
                            "particles_rank0": npart, "res_choices": [32, 48, 64, 96, 128], "cell_size": "1/64",
-                           "pcg": "Jacobi, refined FP32 inner / FP64 outer to 1e-8, inner 1e-2",
+                           "pcg": "Jacobi, refined FP32 inner / FP64 outer to 1e-6, inner 1e-2",
                            "worker_threads": args.workers or "min(16, cores)", "parallelism": f"scenes/{ws} ranks"},
                 "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
                 "e2e": {"value": tot_ps / e2e_t, "unit": UNIT, "h2d_bytes_per_step": 24 * npart / args.steps,
@@ -563,7 +563,7 @@ def run_serve(args, ws, rank, local):
                 "data": "synthetic (seeded request stream, seed 13)",
                 "config": {"workload": "serve_poisson", "requests": len(reqs), "rate_per_s": 20,
                            "res": "cubic, log-uniform 32..192", "steps_per_request": args.req_steps,
-                           "hbm_budget_gb": 150, "pcg": "refined FP32 to 1e-8", "parallelism": f"requests/{ws} ranks",
+                           "hbm_budget_gb": 150, "pcg": "refined FP32 to 1e-6", "parallelism": f"requests/{ws} ranks",
                            "time_limit_s": args.time_limit},
                 "completed_requests": summ["completed"], "admitted_requests": summ["admitted"],
                 "waits_for_memory": summ["waits_for_memory"], "max_running": summ["max_running"],
@@ -892,8 +892,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--pcg-mode", choices=["fp32", "fp64", "refined"], default="fp32")
-    ap.add_argument("--pcg-steps", choices=["single", "two"], default="single",
-                    help="PCG iteration form: single reduction (default) or PCGSolver's two-reduction order")
+    ap.add_argument("--pcg-steps", choices=["single", "two"], default="two",
+                    help="PCG iteration form: PCGSolver's two-reduction order (default) or single reduction")
     ap.add_argument("--inner-tol", type=float, default=None, help="refined PCG: inner (FP32) relative tolerance")
     ap.add_argument("--tol", type=float, default=None,
                     help="fp32 / fp64 PCG: relative tolerance (the refined mode's outer tolerance is 1e-8)")

@@ -53,12 +53,12 @@ extern "C" {
 #define BNN_PCG_FP64      1  /* FP64 vectors and reductions */
 #define BNN_PCG_REFINED   2  /* FP32 inner PCG + FP64 outer residual (iterative refinement) */
 #define BNN_PCG_MODE_MASK 0x0f
-/* OR-ed into a BNN_PCG_* mode: take PCGSolver::solve_precond's own step order (two inner
- * products formed one after the other, PCGSolver.cpp:143-199: two grid-wide reductions per
- * iteration).  Without it the solve uses the single-reduction form of the same iteration
- * (Chronopoulos & Gear: both inner products in one reduction), which gives the same
- * iterates up to rounding. */
-#define BNN_PCG_TWO_REDUCTIONS 0x10
+/* OR-ed into a BNN_PCG_* mode: the single-reduction form of the same iteration (Chronopoulos
+ * & Gear: both inner products of an iteration in one grid-wide reduction, the same iterates
+ * up to rounding).  Without it the solve takes PCGSolver::solve_precond's own step order
+ * (PCGSolver.cpp:143-199: the two inner products one after the other, two reductions per
+ * iteration). */
+#define BNN_PCG_SINGLE_REDUCTION 0x10
 
 #define BNN_PRECOND_JACOBI 0 /* PCGSolver::JACOBI (PCGSolver.cpp:232-237,273-284) */
 
@@ -92,7 +92,7 @@ typedef struct bnn_params {
     uint32_t max_cg_iteration;       /* MaxCGIteration */
     uint32_t advection_steps;        /* AdvectionSteps (default 1) */
     int32_t  solver_kind;            /* BNN_SOLVER_* */
-    int32_t  pcg_mode;               /* BNN_PCG_*, optionally | BNN_PCG_TWO_REDUCTIONS */
+    int32_t  pcg_mode;               /* BNN_PCG_*, optionally | BNN_PCG_SINGLE_REDUCTION */
     int32_t  preconditioner;         /* BNN_PRECOND_* */
     float    refine_tolerance;       /* BNN_PCG_REFINED: outer max-norm relative tolerance */
     float    refine_inner_tolerance; /* BNN_PCG_REFINED: inner FP32 relative tolerance (1e-2 is

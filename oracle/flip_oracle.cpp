@@ -128,9 +128,9 @@ template<class T> struct Arr3 {
 // ----------------------------------------------------------------------------------
 static constexpr int kChunk = 2048;
 static constexpr int kLanes = 256;
-// pcg_mode: BNN_PCG_* in the low bits, the flag for PCGSolver's two-reduction step order
+// pcg_mode: BNN_PCG_* in the low bits, the flag for the single-reduction form
 static constexpr int kPcgModeMask = 0x0f;
-static constexpr int kPcgTwoReductions = 0x10;
+static constexpr int kPcgSingleReduction = 0x10;
 
 static double tree256(double* s) {
     for(int off = kLanes / 2; off > 0; off >>= 1)
@@ -207,7 +207,7 @@ struct orc_params {
     uint32_t advection_steps;       // AdvectionSteps
     int32_t  reduce_mode;           // 0 reference order, 1 canonical FP64 order
     int32_t  pcg_mode;              // 0 FP32 vectors, 1 FP64 vectors, 2 FP32 inner + FP64 refinement;
-                                    // | 0x10: two-reduction step order (else single reduction)
+                                    // | 0x10: single-reduction form (else PCGSolver's step order)
     int32_t  preconditioner;        // 0 Jacobi, 1 MICCL0, 2 MICCL0_SYMMETRIC
     float    refine_tolerance;      // outer tolerance for pcg_mode 2 (max-norm, relative)
     float    refine_inner_tolerance;// inner FP32 tolerance for pcg_mode 2
@@ -514,7 +514,8 @@ static PCGResult pcg_canonical_cg1(const CSR& A, const std::vector<float>& vals,
     return out;
 }
 
-// The canonical solve of either form: the single-reduction one unless twoReductions.
+// The canonical solve of either form: PCGSolver's two-reduction step order, or the
+// single-reduction one.
 template<class VT>
 static PCGResult pcg_canonical_any(const CSR& A, const std::vector<float>& vals, const std::vector<float>& diag,
                                    const std::vector<VT>& rhs, std::vector<VT>& x, VT tolFactor, uint32_t maxIters,
@@ -1386,7 +1387,7 @@ public:
         std::vector<float> valsF(Avals.begin(), Avals.end());
         std::vector<float> rhsF(rhs.begin(), rhs.end());
         const int mode = P.pcg_mode & kPcgModeMask;
-        const bool two = (P.pcg_mode & kPcgTwoReductions) != 0;
+        const bool two = (P.pcg_mode & kPcgSingleReduction) == 0;
         if(mode == 0) {
             std::vector<float> x;
             lastSolve = pcg_canonical_any<float>(A, valsF, Adiag, rhsF, x, (float)tolf, P.max_cg_iteration, two);
@@ -1760,8 +1761,8 @@ void orc_get_system(void* hp, uint32_t* rowStart, uint32_t* colIndex, float* val
 
 // Standalone PCG on a CSR system (rows column-sorted), in the chosen arithmetic.
 // mode: 0 canonical FP32, 1 canonical FP64, 2 refined, 3 reference FP32 (precond 0/1/2),
-// 4 reference FP64; modes 0-2 take the single-reduction form unless kPcgTwoReductions is
-// OR-ed in.
+// 4 reference FP64; modes 0-2 take PCGSolver's two-reduction step order unless
+// kPcgSingleReduction is OR-ed in.
 int orc_pcg(uint32_t n, const uint32_t* rowStart, const uint32_t* colIndex, const float* vals, const float* rhs,
             float tol, uint32_t maxIter, int mode, int precond, float innerTol, double* x_out, uint32_t* iters,
             double* resid, uint32_t* outer) {
@@ -1775,7 +1776,7 @@ int orc_pcg(uint32_t n, const uint32_t* rowStart, const uint32_t* colIndex, cons
         for(uint32_t j = rowStart[r]; j < rowStart[r + 1]; ++j) if(colIndex[j] == r) diag[r] = vals[j];
     std::vector<float> b(rhs, rhs + n);
     PCGResult res;
-    const bool two = (mode & kPcgTwoReductions) != 0;
+    const bool two = (mode & kPcgSingleReduction) == 0;
     mode &= kPcgModeMask;
     if(mode == 0) {
         std::vector<float> x; res = pcg_canonical_any<float>(A, v, diag, b, x, tol, maxIter, two);

@@ -65,8 +65,8 @@ def test_flip_32_bitexact_30_steps(bnn, oracle_mod):
         _compare_step(g, o, s)
 
 
-def test_flip_32_two_reductions_bitexact(bnn, oracle_mod):
-    """The same scene with PCGSolver's two-reduction step order in the solve"""
+def test_flip_32_single_reduction_bitexact(bnn, oracle_mod):
+    """The same scene with the single-reduction form of the solve"""
     g, o = _pair(bnn, oracle_mod, 32, pcg_mode=0x10)
     for s in range(12):
         _compare_step(g, o, s)

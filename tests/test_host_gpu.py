@@ -8,6 +8,7 @@ import pytest
 
 from banana_b200 import build as bld
 from banana_b200 import scenes
+from oracle import bnn_reader
 from tests.bnn_format import matrix_values, read_bnn, values
 from tests.host_scene import dam_break_scene, read_particles
 
@@ -79,6 +80,14 @@ def test_memory_state_resume_and_bnn_frames(bnn, tmp_path):
     st_n, st, _ = read_bnn(data / "state" / "frame.0002.bnn")
     assert np.array_equal(values(st["particle_position"]).reshape(-1, 3), p2)
     assert list(values(st["grid_resolution"])) == [n + 4] * 3
+    # the same files through the restatement of the reference's own reader
+    rn, rfixed, rpart = bnn_reader.read(data / "straight" / "frame.0003.bnn")
+    assert rn == cnt
+    assert np.array_equal(bnn_reader.particle_attribute(rn, rpart, "particle_position"), dec)
+    assert list(bnn_reader.particle_attribute(rn, rpart, "object_index")) == [0] * cnt
+    sn, sfixed, spart = bnn_reader.read(data / "state" / "frame.0002.bnn")
+    assert np.array_equal(bnn_reader.particle_attribute(sn, spart, "particle_position"), p2)
+    assert list(bnn_reader.fixed_attribute(sfixed, "grid_resolution")) == [n + 4] * 3
 
 
 def test_anikernel_frame_output(bnn, tmp_path):
@@ -109,6 +118,10 @@ def test_anikernel_frame_output(bnn, tmp_path):
     K, klo, khi, _ = matrix_values(attrs["anisotropic_kernel"])
     assert klo == mat.min() and khi == mat.max()
     assert np.abs(K - mat).max() <= (khi - klo) / 65535 * 1.01
+    # the reference's reader (restated) decodes the same kernels
+    rn, _, rpart = bnn_reader.read(data / "ani" / "frame.0001.bnn")
+    assert np.array_equal(bnn_reader.particle_attribute(rn, rpart, "anisotropic_kernel", matrix_dim=3), K)
+    assert np.array_equal(bnn_reader.particle_attribute(rn, rpart, "particle_position"), dec)
 
 
 def test_driver_boundary_objects(bnn, tmp_path):
@@ -149,3 +162,41 @@ def test_driver_boundary_objects(bnn, tmp_path):
     q = p2.astype(np.float64) - 0.5
     local = np.stack([c * q[:, 0] + s * q[:, 1], -s * q[:, 0] + c * q[:, 1], q[:, 2]], 1)
     assert np.all(np.abs(local) <= 0.45 + 2.0 / n)
+
+
+def test_reference_scene_through_the_drop_in(bnn, tmp_path):
+    """The reference's own FLIP3D_2DamBreak scene (Applications/QtApps/ParticleSimulation/
+    Scenes, with only "Solver" changed to FLIP_GPU_3DSolver; tests/golden/scenes) through the
+    factory, loadScene and doFrameSimulation: two box generators, position correction,
+    two advection steps, frame files written under the scene's own DataPath (relative to
+    the working directory here) and readable by the reference's reader."""
+    import json
+    from pathlib import Path
+    exe = bld.build_host()
+    scene = Path(__file__).resolve().parent / "golden" / "scenes" / "FLIP3D_2DamBreak.json"
+    sc = json.loads(scene.read_text())
+    assert sc["GlobalParameters"]["Solver"] == "FLIP_GPU_3DSolver"
+    out = tmp_path / "p.f32"
+    r = subprocess.run([str(exe), str(scene), "--frames", "2", "--out", str(out)], capture_output=True, text=True,
+                       timeout=600, cwd=tmp_path)
+    assert r.returncode == 0, r.stderr[-2000:]
+    head = json.loads(r.stdout.splitlines()[0])
+    assert head["solver"] == "FLIP_GPU_3DSolver"
+    frames = [json.loads(l) for l in r.stdout.splitlines()[1:] if l.startswith("{")]
+    assert [f["frame"] for f in frames] == [1, 2] and all(f["substeps"] >= 1 for f in frames)
+    pos, vel = read_particles(out)
+    assert len(pos) == head["particles"] > 0
+    lo = np.array(sc["SimulationParameters"]["SimulationDomainBox"]["BoxMin"], np.float32)
+    hi = np.array(sc["SimulationParameters"]["SimulationDomainBox"]["BoxMax"], np.float32)
+    assert np.all(pos >= lo - 1e-6) and np.all(pos <= hi + 1e-6)
+    assert np.all(np.isfinite(vel))
+    g = sc["GlobalParameters"]
+    frame = tmp_path / g["DataPath"] / g["FrameDataFolder"] / "frame.0002.bnn"
+    n, fixed, part = bnn_reader.read(frame)
+    assert n == len(pos)
+    # the scene asks for "anisotropic_kernel" and "object_index", but the reference's
+    # saveFrameData tests the names "AniKernel" and "ObjectIndex" (PIC_Solver.cpp:240-255),
+    # so, as there, the frame holds the particle radius and positions only
+    assert sorted(fixed) == ["particle_radius"] and sorted(part) == ["particle_position"]
+    p = bnn_reader.particle_attribute(n, part, "particle_position")
+    assert np.abs(p - pos).max() <= (pos.max(0) - pos.min(0)).max() / 65535 * 1.01

@@ -38,17 +38,17 @@ def _system(oracle_mod, n=32, steps=3):
     return (rs, ci, va, rhs), diag, nbr, off
 
 
-TWO = 0x10  # BNN_PCG_TWO_REDUCTIONS: PCGSolver's two-reduction step order
+SINGLE = 0x10  # BNN_PCG_SINGLE_REDUCTION: both inner products in one reduction
 
 
-@pytest.mark.parametrize("two", [0, TWO], ids=["single_reduction", "two_reductions"])
+@pytest.mark.parametrize("form", [0, SINGLE], ids=["two_reductions", "single_reduction"])
 @pytest.mark.parametrize("mode,omode", [("fp32", 0), ("fp64", 1), ("refined", 2)])
-def test_pcg_7pt_matches_oracle(bnn, oracle_mod, mode, omode, two):
+def test_pcg_7pt_matches_oracle(bnn, oracle_mod, mode, omode, form):
     (rs, ci, va, rhs), diag, nbr, off = _system(oracle_mod)
     tol = 1e-8 if mode == "refined" else 1e-6
-    m = bnn.capi.PCG_MODE[mode] | two
+    m = bnn.capi.PCG_MODE[mode] | form
     x, st = bnn.pcg_solve_7pt(diag, nbr, off, rhs, tol, 5000, mode=m, inner_tol=1e-3)
-    xo, so = oracle_mod.pcg(rs, ci, va, rhs, tol, 5000, omode | two, inner_tol=1e-3)
+    xo, so = oracle_mod.pcg(rs, ci, va, rhs, tol, 5000, omode | form, inner_tol=1e-3)
     assert st["success"] == 1 and so["success"]
     assert st["iterations"] == so["iterations"]
     if mode == "fp32":
@@ -110,18 +110,18 @@ def _box_system(nx=40, ny=36, nz=30, holes=0.08, seed=5):
     return nbr, compact, diag, -dt, rhs, (np.array(rs), np.array(ci), np.array(va, np.float32))
 
 
-@pytest.mark.parametrize("two", [0, TWO], ids=["single_reduction", "two_reductions"])
+@pytest.mark.parametrize("form", [0, SINGLE], ids=["two_reductions", "single_reduction"])
 @pytest.mark.parametrize("mode,omode", [("fp32", 0), ("fp64", 1), ("refined", 2)])
-def test_pcg_7pt_grid_rows_packed_matches_oracle(bnn, oracle_mod, mode, omode, two):
+def test_pcg_7pt_grid_rows_packed_matches_oracle(bnn, oracle_mod, mode, omode, form):
     """Grid-ordered rows take the packed-record solve (x neighbours by warp shuffle); the
     compact layout of the same system takes the general one.  Both equal the oracle, in
     either step order."""
     nbr, compact, diag, off, rhs, (rs, ci, va) = _box_system()
     tol = 1e-8 if mode == "refined" else 1e-6
-    xo, so = oracle_mod.pcg(rs, ci, va, rhs, tol, 5000, omode | two, inner_tol=1e-3)
+    xo, so = oracle_mod.pcg(rs, ci, va, rhs, tol, 5000, omode | form, inner_tol=1e-3)
     assert so["success"]
     for layout in (nbr, compact):
-        x, st = bnn.pcg_solve_7pt(diag, layout, off, rhs, tol, 5000, mode=bnn.capi.PCG_MODE[mode] | two,
+        x, st = bnn.pcg_solve_7pt(diag, layout, off, rhs, tol, 5000, mode=bnn.capi.PCG_MODE[mode] | form,
                                   inner_tol=1e-3)
         assert st["success"] == 1
         assert st["iterations"] == so["iterations"]
