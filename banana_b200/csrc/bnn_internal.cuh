@@ -214,6 +214,19 @@ struct DevState {
     double outer_res, outer_bmax;
     int bbox[6];            // min x,y,z and max x,y,z of the particles' (clamped) cells
     unsigned nlarge;        // cells with more than 16 particles, listed for k_sort_large
+    // the next sub-step, when its particle move ran at the end of this one (k_g2p_move)
+    float next_dt;          // its size (PIC_Solver::advanceFrame's substep)
+    unsigned next_flags;    // flags its move raised (BNN_FLAG_OUT_OF_GRID)
+};
+
+// What the fused grid-to-particle + move pass needs to size the next sub-step
+// (PIC_Solver::timestepCFL + advanceFrame's clipping, PIC_Solver.cpp:284-290,342-349) on
+// the device: the frame time after this sub-step and the parameters.
+struct NextStep {
+    float frameTime;        // frameLocalTime after this sub-step (before the new-frame wrap)
+    float frameDuration;
+    float cfl, minDt, maxDt;
+    int advSteps;
 };
 
 #define BNN_FLAG_OUT_OF_GRID   1u

@@ -28,9 +28,9 @@ void launch_advect(int n, float* p6, size_t stride, const float* const* U, const
 void launch_cell_histogram(int n, const float* p6, size_t stride, const GridDesc& g, uint32_t* cellOf, uint32_t* slot,
                            uint32_t* count, DevState* st, cudaStream_t s);
 void launch_sort_finish(int n, size_t ncells, uint32_t* cellOf, uint32_t* slot, const uint32_t* cellStart,
-                        uint32_t* order, uint32_t* key, uint32_t* count, const float* src6, float* dst6, const uint32_t* idSrc,
-                        uint32_t* idDst, const float* cSrc, float* cDst, float* g3, float4* rec, const GridDesc& g,
-                        size_t stride, DevState* st, cudaStream_t s);
+                        uint32_t* order, uint32_t* key, uint32_t* count, const float* src6, const float* srcPos,
+                        float* dst6, const uint32_t* idSrc, uint32_t* idDst, const float* cSrc, float* cDst, float* g3,
+                        float4* rec, const GridDesc& g, size_t stride, DevState* st, cudaStream_t s);
 void launch_p2g_affine(const GridDesc& g, const uint32_t* cellStart, const float* g3, const float* p6,
                        const float* C9, size_t stride, float* const* out, uint8_t* const* valid, cudaStream_t s);
 // gather_kernels.cu
@@ -73,6 +73,10 @@ void launch_cells_from_rows(size_t nc, const float* phi, const uint32_t* aidx, c
                             cudaStream_t s);
 void launch_add_scalar(float* a, size_t n, float v, cudaStream_t s);
 void launch_step_reset(DevState* st, cudaStream_t s);
+void launch_step_reset_moved(DevState* st, cudaStream_t s);
+void launch_g2p_move(int n, const GridDesc& g, float* p6, size_t stride, const float* const* U, const float* const* O,
+                     float ratio, const NextStep& ns, float* moved, uint32_t* cellOf, uint32_t* slot, uint32_t* count,
+                     DevState* st, int* bboxPart, cudaStream_t s);
 
 // pcg.cu
 } // namespace bnn
@@ -134,6 +138,13 @@ struct bnn_flip {
     cudaEvent_t io[3] = {};
     unsigned maxvelBits = 0; // max|u| of the current grid (for the next CFL)
     unsigned long long substepIndex = 0;  // sub-steps taken (keys the position-correction jitter)
+    // FLIP: the next sub-step's particle move runs at the end of this one (k_g2p_move); its
+    // positions, cell ids, histogram and occupied-cell box then wait for the next sub-step,
+    // which must use premovedDt as its size.  Anything that changes the particles, the grid
+    // velocities or the boundaries in between drops it (the next sub-step moves as usual).
+    float* moved = nullptr;  // 3 planes, stride cap
+    bool premoved = false;
+    float premovedDt = 0.f;
 };
 
 static void free_particles(bnn_flip* h) {
@@ -142,9 +153,10 @@ static void free_particles(bnn_flip* h) {
         h->p6[b] = nullptr; h->ids[b] = nullptr; h->C9[b] = nullptr;
     }
     cudaFree(h->g3); cudaFree(h->rec); cudaFree(h->bboxPart); cudaFree(h->cellOf); cudaFree(h->slot); cudaFree(h->order); cudaFree(h->key); cudaFree(h->aosStage);
-    cudaFree(h->aniso);
+    cudaFree(h->aniso); cudaFree(h->moved);
     h->g3 = nullptr; h->rec = nullptr; h->bboxPart = nullptr; h->cellOf = h->slot = h->order = h->key = nullptr; h->aosStage = nullptr;
-    h->aniso = nullptr;
+    h->aniso = nullptr; h->moved = nullptr;
+    h->premoved = false;
     h->cap = 0;
 }
 
@@ -171,6 +183,7 @@ static int reserve_particles(bnn_flip* h, uint32_t n) {
     BNN_CUDA_CHECK(cudaMalloc(&h->order, st * sizeof(uint32_t)));
     BNN_CUDA_CHECK(cudaMalloc(&h->key, st * sizeof(uint32_t)));
     BNN_CUDA_CHECK(cudaMalloc(&h->aosStage, 6 * st * sizeof(float)));
+    if(h->P.solver_kind == BNN_SOLVER_FLIP) BNN_CUDA_CHECK(cudaMalloc(&h->moved, 3 * st * sizeof(float)));
     h->cap = cap;
     return BNN_OK;
 }
@@ -301,7 +314,7 @@ static uint64_t device_bytes(const bnn_flip* h) {
     for(int d = 0; d < 3; ++d) b += (uint64_t)h->F[d] * 14u;                       // U, B, O + 2 valid
     b += (uint64_t)h->C * 20u + 8u + scan_workspace_bytes(h->C);                   // count..aidx
     const bool affine = h->P.solver_kind == BNN_SOLVER_APIC || h->P.solver_kind == BNN_SOLVER_AFLIP;
-    b += (uint64_t)h->cap * (172u + (affine ? 72u : 0u));                          // particle arrays
+    b += (uint64_t)h->cap * (172u + (affine ? 72u : 0u) + (h->moved ? 12u : 0u));  // particle arrays
     b += (uint64_t)h->rowCap * 44u;                                                // rows
     b += (uint64_t)h->pcg.cap * (48u + (h->pcg.x64 ? 56u : 0u)) + (uint64_t)h->pcg.nchCap * 40u;
     return b;
@@ -323,7 +336,8 @@ extern "C" int bnn_scene_bytes_estimate(const bnn_params* params, uint32_t n, ui
     const bool affine = params->solver_kind == BNN_SOLVER_APIC || params->solver_kind == BNN_SOLVER_AFLIP;
     const bool fp64 = (params->pcg_mode & BNN_PCG_MODE_MASK) != BNN_PCG_FP32;
     const uint64_t rows = n < C ? n : C;
-    *bytes = F * 14u + C * 24u + (uint64_t)n * (172u + (affine ? 72u : 0u)) + rows * 44u +
+    const bool flip = params->solver_kind == BNN_SOLVER_FLIP;
+    *bytes = F * 14u + C * 24u + (uint64_t)n * (172u + (affine ? 72u : 0u) + (flip ? 12u : 0u)) + rows * 44u +
              (rows * 5u / 4u + 4096u) * (48u + (fp64 ? 56u : 0u));
     return BNN_OK;
 }
@@ -375,6 +389,7 @@ extern "C" int bnn_flip_set_particles(bnn_flip* h, const float* pos, const float
     if(rc != BNN_OK) return rc;
     h->n = n;
     h->cur = 0;
+    h->premoved = false;
     if(n) {
         rc = upload_particles(h, pos, vel, n);
         if(rc != BNN_OK) return rc;
@@ -407,6 +422,7 @@ extern "C" int bnn_flip_get_particles(bnn_flip* h, float* pos, float* vel) {
 
 extern "C" int bnn_flip_device_particles(bnn_flip* h, float** p6, uint32_t** ids) {
     if(!h) return BNN_ERR_INVALID_ARGUMENT;
+    h->premoved = false;  // the caller may change the particles through these pointers
     if(p6) *p6 = h->p6[h->cur];
     if(ids) *ids = h->ids[h->cur];
     return BNN_OK;
@@ -417,6 +433,7 @@ extern "C" int bnn_flip_device_particles(bnn_flip* h, float** p6, uint32_t** ids
 extern "C" int bnn_flip_set_grid(bnn_flip* h, int32_t field, const float* in, size_t count) {
     if(!h || !in || field < BNN_FIELD_U || field > BNN_FIELD_W) return BNN_ERR_INVALID_ARGUMENT;
     if(count != h->F[field]) return BNN_ERR_INVALID_ARGUMENT;
+    h->premoved = false;
     BNN_CUDA_CHECK(cudaMemcpyAsync(h->U[field], in, count * sizeof(float), cudaMemcpyHostToDevice, h->s));
     BNN_CUDA_CHECK(cudaMemsetAsync(&h->dst->maxvel_bits, 0, sizeof(unsigned), h->s));
     for(int d = 0; d < 3; ++d) launch_maxabs(h->U[d], h->F[d], &h->dst->maxvel_bits, h->s);
@@ -481,6 +498,7 @@ extern "C" int bnn_flip_get_grid(bnn_flip* h, int32_t field, float* out, size_t 
 extern "C" int bnn_flip_set_boundaries(bnn_flip* h, const bnn_boundary_object* objs, uint32_t n,
                                        int32_t update_grid) {
     if(!h || (n && !objs) || n >= (uint32_t)kMaxBoundaryObjects) return BNN_ERR_INVALID_ARGUMENT;
+    h->premoved = false;  // the next move must see these objects
     std::vector<BObj> list;
     BObj box{};
     box.geometry = 0;
@@ -564,17 +582,29 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st, const HostIo* io = nullp
     const int kind = h->P.solver_kind;
     const bool affine = kind == BNN_SOLVER_APIC || kind == BNN_SOLVER_AFLIP;
     const int n = (int)h->n;
+    // the move already ran at the end of the last sub-step: with the size computed there
+    const bool moved = h->premoved && n > 0;
+    h->premoved = false;
+    if(moved && substep != h->premovedDt) {
+        bnn_set_error("sub-step size of the fused move differs from the host's");
+        return BNN_ERR_DEVICE_CHECK;
+    }
 
     cudaEventRecord(h->ev[0], s);
-    launch_step_reset(h->dst, s);
-    // moveParticles + counting sort (histogram while advecting)
-    launch_advect(n, h->p6[h->cur], h->cap, h->U, g, sub, (int)h->P.advection_steps, h->cellOf, h->slot, h->count,
-                  h->dst, h->bboxPart, s);
+    if(moved) {
+        launch_step_reset_moved(h->dst, s);
+    } else {
+        launch_step_reset(h->dst, s);
+        // moveParticles + counting sort (histogram while advecting)
+        launch_advect(n, h->p6[h->cur], h->cap, h->U, g, sub, (int)h->P.advection_steps, h->cellOf, h->slot, h->count,
+                      h->dst, h->bboxPart, s);
+    }
     cudaEventRecord(h->ev[1], s);
     BNN_CUDA_CHECK(exclusive_scan_u32(h->count, h->cellStart, h->C, h->scanWs, s));
     if(io && io->velPending) BNN_CUDA_CHECK(cudaStreamWaitEvent(s, h->io[1], 0));
     const int nxt = 1 - h->cur;
-    launch_sort_finish(n, h->C, h->cellOf, h->slot, h->cellStart, h->order, h->key, h->count, h->p6[h->cur], h->p6[nxt],
+    launch_sort_finish(n, h->C, h->cellOf, h->slot, h->cellStart, h->order, h->key, h->count, h->p6[h->cur],
+                       moved ? h->moved : nullptr, h->p6[nxt],
                        h->ids[h->cur], h->ids[nxt], affine ? h->C9[h->cur] : nullptr, affine ? h->C9[nxt] : nullptr,
                        h->g3, h->rec, g, h->cap, h->dst, s);
     h->cur = nxt;
@@ -593,7 +623,7 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st, const HostIo* io = nullp
         launch_rebin(n, h->p6[h->cur], h->cap, g, h->cellOf, h->slot, h->count, h->dst, s);
         BNN_CUDA_CHECK(exclusive_scan_u32(h->count, h->cellStart, h->C, h->scanWs, s));
         const int nxt2 = 1 - h->cur;
-        launch_sort_finish(n, h->C, h->cellOf, h->slot, h->cellStart, h->order, h->key, h->count, h->p6[h->cur], h->p6[nxt2],
+        launch_sort_finish(n, h->C, h->cellOf, h->slot, h->cellStart, h->order, h->key, h->count, h->p6[h->cur], nullptr, h->p6[nxt2],
                            h->ids[h->cur], h->ids[nxt2], affine ? h->C9[h->cur] : nullptr,
                            affine ? h->C9[nxt2] : nullptr, h->g3, h->rec, g, h->cap, h->dst, s);
         h->cur = nxt2;
@@ -685,10 +715,25 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st, const HostIo* io = nullp
         for(int d = 0; d < 3; ++d) launch_maxabs(h->U[d], h->F[d], &h->dst->maxvel_bits, s);
     }
     cudaEventRecord(h->ev[8], s);
-    // PIC_Solver leaves the particle velocities alone (no grid-to-particle transfer)
-    if(kind != BNN_SOLVER_PIC)
+    // PIC_Solver leaves the particle velocities alone (no grid-to-particle transfer).  FLIP
+    // steps driven from device-resident particles also move the particles for the next
+    // sub-step here (k_g2p_move); a step on caller arrays (bnn_flip_step_host) does not,
+    // since the next call brings new particle data.
+    const bool fuse = kind == BNN_SOLVER_FLIP && n > 0 && !io && h->moved;
+    if(fuse) {
+        NextStep ns;
+        ns.frameTime = h->frameTime + substep;
+        ns.frameDuration = h->frameDuration;
+        ns.cfl = h->P.cfl_factor;
+        ns.minDt = h->P.min_timestep;
+        ns.maxDt = h->P.max_timestep;
+        ns.advSteps = (int)h->P.advection_steps;
+        launch_g2p_move(n, g, h->p6[h->cur], h->cap, h->U, h->O, h->P.pic_flip_ratio, ns, h->moved, h->cellOf, h->slot,
+                        h->count, h->dst, h->bboxPart, s);
+    } else if(kind != BNN_SOLVER_PIC) {
         launch_g2p(n, g, h->p6[h->cur], h->cap, h->U, h->O, h->P.pic_flip_ratio, kind, affine ? h->C9[h->cur] : nullptr,
                    s);
+    }
     cudaEventRecord(h->ev[9], s);
     BNN_CUDA_CHECK(cudaGetLastError());
     BNN_CUDA_CHECK(cudaMemcpyAsync(h->hst, h->dst, sizeof(DevState), cudaMemcpyDeviceToHost, s));
@@ -696,6 +741,10 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st, const HostIo* io = nullp
     h->maxvelBits = h->hst->maxvel_bits;
     h->frameTime += substep;
     ++h->substepIndex;
+    if(fuse) {
+        h->premoved = true;
+        h->premovedDt = h->hst->next_dt;
+    }
     if(st) {
         st->dt = substep;
         st->frame_time = h->frameTime;
@@ -740,6 +789,7 @@ extern "C" int bnn_flip_step_host(bnn_flip* h, float* pos, float* vel, bnn_step_
     const int n = (int)h->n;
     const size_t cap = h->cap;
     HostIo io;
+    h->premoved = false;  // new particle data from the caller
     if(n) {
         cudaStream_t s = h->s, s2 = h->s2;
         if(h->C9[h->cur]) {
@@ -803,10 +853,11 @@ extern "C" int bnn_flip_anisotropic_kernels(bnn_flip* h, const bnn_aniso_params*
     if(n == 0) return BNN_OK;
     cudaStream_t s = h->s;
     const bool affine = h->P.solver_kind == BNN_SOLVER_APIC || h->P.solver_kind == BNN_SOLVER_AFLIP;
+    h->premoved = false;  // the re-sort below reuses the move's buffers
     launch_rebin(n, h->p6[h->cur], h->cap, g, h->cellOf, h->slot, h->count, h->dst, s);
     BNN_CUDA_CHECK(exclusive_scan_u32(h->count, h->cellStart, h->C, h->scanWs, s));
     const int nxt = 1 - h->cur;
-    launch_sort_finish(n, h->C, h->cellOf, h->slot, h->cellStart, h->order, h->key, h->count, h->p6[h->cur], h->p6[nxt],
+    launch_sort_finish(n, h->C, h->cellOf, h->slot, h->cellStart, h->order, h->key, h->count, h->p6[h->cur], nullptr, h->p6[nxt],
                        h->ids[h->cur], h->ids[nxt], affine ? h->C9[h->cur] : nullptr, affine ? h->C9[nxt] : nullptr,
                        h->g3, h->rec, g, h->cap, h->dst, s);
     h->cur = nxt;

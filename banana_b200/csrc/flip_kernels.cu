@@ -501,16 +501,20 @@ __global__ void __launch_bounds__(256) k_sort_large(const uint32_t* __restrict__
 //        plane 3: the position {x, y, z, 0} for the fluid SDF.
 // One 16-byte load per candidate particle then replaces four scattered 4-byte loads.
 __global__ void k_gather_particles(int n, const uint32_t* __restrict__ order, const float* __restrict__ src6,
-                                   float* __restrict__ dst6, const uint32_t* __restrict__ idSrc,
-                                   uint32_t* __restrict__ idDst, const float* __restrict__ cSrc,
-                                   float* __restrict__ cDst, float* __restrict__ g3, float4* __restrict__ rec,
-                                   GridDesc g, size_t stride) {
+                                   const float* __restrict__ srcPos, float* __restrict__ dst6,
+                                   const uint32_t* __restrict__ idSrc, uint32_t* __restrict__ idDst,
+                                   const float* __restrict__ cSrc, float* __restrict__ cDst, float* __restrict__ g3,
+                                   float4* __restrict__ rec, GridDesc g, size_t stride) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if(i >= n) return;
     const uint32_t s = order[i];
     float v6[6];
+    // positions from srcPos when the move wrote them apart (k_g2p_move), else from src6
 #pragma unroll
-    for(int q = 0; q < 6; ++q) { v6[q] = src6[q * stride + s]; dst6[q * stride + i] = v6[q]; }
+    for(int q = 0; q < 6; ++q) {
+        v6[q] = q < 3 ? srcPos[q * stride + s] : src6[q * stride + s];
+        dst6[q * stride + i] = v6[q];
+    }
     idDst[i] = idSrc[s];
     float gc[3];
 #pragma unroll
@@ -1268,6 +1272,102 @@ __global__ void __launch_bounds__(256) k_g2p(int n, GridDesc g, const float* __r
 }
 
 // ----------------------------------------------------------------------------------
+// FLIP grid-to-particle transfer fused with the next sub-step's particle move
+// ----------------------------------------------------------------------------------
+// The next sub-step's size (PIC_Solver::advanceFrame, PIC_Solver.cpp:280-290, with
+// timestepCFL, :342-349) from max|u| of the final grid of this sub-step, in the float
+// operations the host uses (timestep_cfl in capi.cu): every thread forms the same value.
+__device__ __forceinline__ float next_substep(unsigned maxvelBits, const NextStep& ns, float dx) {
+    float ft = ns.frameTime;
+    if(ft >= ns.frameDuration) ft = 0.f;  // a new frame starts
+    const float m = __uint_as_float(maxvelBits);
+    float maxVel = FLT_MIN;
+    maxVel = (maxVel < m) ? m : maxVel;
+    float ts = maxVel > FLT_MIN ? ns.cfl * (dx / maxVel) : FLT_MAX;
+    if(ts < ns.minDt) ts = ns.minDt;
+    else if(ts > ns.maxDt) ts = ns.maxDt;
+    const float remaining = ns.frameDuration - ft;
+    if(ft + ts >= ns.frameDuration) ts = remaining;
+    else if(ft + 1.5f * ts >= ns.frameDuration) ts = remaining * 0.5f;
+    return ts;
+}
+
+// FLIP_Solver::mapGrid2Particles (FLIP_Solver.cpp:99-111), then the next sub-step's
+// PIC_Solver::moveParticles (PIC_Solver.cpp:353-373) and the first half of its counting
+// sort: both read the same grid (the next sub-step starts from this one's velocities), and
+// the move's first RK2 stage is the grid velocity the transfer has just interpolated at
+// the particle.  The particle keeps its position of this sub-step (what callers read
+// between sub-steps); the moved position goes to `moved`, and the next sub-step's sort
+// gathers from there.  Identical arithmetic to k_g2p followed by k_advect.
+__global__ void __launch_bounds__(256, 4) k_g2p_move(int n, GridDesc g, float* __restrict__ p6, size_t stride,
+                                                  const float* __restrict__ u, const float* __restrict__ v,
+                                                  const float* __restrict__ w, const float* __restrict__ ou,
+                                                  const float* __restrict__ ov, const float* __restrict__ ow,
+                                                  float ratio, NextStep ns, float* __restrict__ moved,
+                                                  uint32_t* __restrict__ cellOf, uint32_t* __restrict__ slot,
+                                                  uint32_t* __restrict__ count, DevState* st,
+                                                  int* __restrict__ bboxPart) {
+    int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {INT_MIN, INT_MIN, INT_MIN};
+    const float substep = next_substep(st->maxvel_bits, ns, g.dx);
+    const float sub = substep / (float)ns.advSteps;
+    if(blockIdx.x == 0 && threadIdx.x == 0) st->next_dt = substep;
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t c = 0xffffffffu;
+    if(p < n) {
+        float x = p6[p], y = p6[stride + p], z = p6[2 * stride + p];
+        float gx = (x - g.bmin[0]) / g.dx, gy = (y - g.bmin[1]) / g.dx, gz = (z - g.bmin[2]) / g.dx;
+        float gv[3];
+        vel_from_grid(g, u, v, w, gx, gy, gz, gv);
+        {
+            const int G0 = g.G[0], G1 = g.G[1], G2 = g.G[2];
+            float dg[3];
+            dg[0] = interp_face_diff(u, ou, G0 + 1, G1, G2, gx, gy - 0.5f, gz - 0.5f);
+            dg[1] = interp_face_diff(v, ov, G0, G1 + 1, G2, gx - 0.5f, gy, gz - 0.5f);
+            dg[2] = interp_face_diff(w, ow, G0, G1, G2 + 1, gx - 0.5f, gy - 0.5f, gz);
+            float* vel3 = p6 + 3 * stride;
+#pragma unroll
+            for(int d = 0; d < 3; ++d) {
+                const float pv = vel3[d * stride + p];
+                vel3[d * stride + p] = (1.0f - ratio) * gv[d] + ratio * (pv + dg[d]);
+            }
+        }
+        for(int s = 0; s < ns.advSteps; ++s) {
+            if(s > 0) {
+                gx = (x - g.bmin[0]) / g.dx; gy = (y - g.bmin[1]) / g.dx; gz = (z - g.bmin[2]) / g.dx;
+                vel_from_grid(g, u, v, w, gx, gy, gz, gv);
+            }
+            const float h = 0.5f * sub;
+            const float mxp = x + h * gv[0], myp = y + h * gv[1], mzp = z + h * gv[2];
+            gx = (mxp - g.bmin[0]) / g.dx; gy = (myp - g.bmin[1]) / g.dx; gz = (mzp - g.bmin[2]) / g.dx;
+            float gm[3];
+            vel_from_grid(g, u, v, w, gx, gy, gz, gm);
+            x = x + sub * gm[0];
+            y = y + sub * gm[1];
+            z = z + sub * gm[2];
+            constrain_particle(g, x, y, z);
+        }
+        moved[p] = x; moved[stride + p] = y; moved[2 * stride + p] = z;
+        bool outside;
+        int cc[3];
+        c = cell_linear(g, (x - g.bmin[0]) / g.dx, (y - g.bmin[1]) / g.dx, (z - g.bmin[2]) / g.dx, outside, cc);
+        if(outside) atomicOr(&st->next_flags, BNN_FLAG_OUT_OF_GRID);
+        cellOf[p] = c;
+#pragma unroll
+        for(int d = 0; d < 3; ++d) { mn[d] = cc[d]; mx[d] = cc[d]; }
+    }
+    histogram_slot(c, p, count, slot);
+    bbox_block_partial(bboxPart, mn, mx);
+}
+
+// Start of a sub-step whose move already ran: the move's flags and occupied-cell box stay
+__global__ void k_step_reset_moved(DevState* st) {
+    st->flags = st->next_flags;
+    st->next_flags = 0u;
+    st->zero_phi = 0u;
+    st->maxvel_bits = 0u;
+}
+
+// ----------------------------------------------------------------------------------
 // Particle I/O
 // ----------------------------------------------------------------------------------
 __global__ void k_aos_to_soa(int n, const float* __restrict__ pos, const float* __restrict__ vel,
@@ -1368,15 +1468,16 @@ void launch_cell_histogram(int n, const float* p6, size_t stride, const GridDesc
 // cellOf and slot are free once the index is scattered: slot lists the crowded buckets,
 // cellOf holds their unsorted order while k_sort_large rewrites them
 void launch_sort_finish(int n, size_t ncells, uint32_t* cellOf, uint32_t* slot, const uint32_t* cellStart,
-                        uint32_t* order, uint32_t* key, uint32_t* count, const float* src6, float* dst6, const uint32_t* idSrc,
-                        uint32_t* idDst, const float* cSrc, float* cDst, float* g3, float4* rec, const GridDesc& g,
-                        size_t stride, DevState* st, cudaStream_t s) {
+                        uint32_t* order, uint32_t* key, uint32_t* count, const float* src6, const float* srcPos,
+                        float* dst6, const uint32_t* idSrc, uint32_t* idDst, const float* cSrc, float* cDst, float* g3,
+                        float4* rec, const GridDesc& g, size_t stride, DevState* st, cudaStream_t s) {
     if(n > 0) { k_scatter_index<<<nblk(n), 256, 0, s>>>(n, cellOf, slot, cellStart, idSrc, order, key); bnn_note_launch(); }
     cudaMemsetAsync(&st->nlarge, 0, sizeof(unsigned), s);
     { k_sort_buckets<<<nblk(ncells), 256, 0, s>>>((int)ncells, cellStart, order, key, count, slot, st); bnn_note_launch(); }
     if(n > 16) { k_sort_large<<<2 * 148, 256, 0, s>>>(cellStart, order, idSrc, cellOf, slot, st); bnn_note_launch(); }
     if(n > 0)
-        { k_gather_particles<<<nblk(n), 256, 0, s>>>(n, order, src6, dst6, idSrc, idDst, cSrc, cDst, g3, rec, g, stride); bnn_note_launch(); }
+        { k_gather_particles<<<nblk(n), 256, 0, s>>>(n, order, src6, srcPos ? srcPos : src6, dst6, idSrc, idDst, cSrc, cDst,
+                                                    g3, rec, g, stride); bnn_note_launch(); }
 }
 // APIC / AFLIP P2G (the affine momentum term), one launch per component; FLIP's P2G is
 // the tiled pass of gather_kernels.cu
@@ -1540,6 +1641,20 @@ void launch_soa3_to_aos(int n, const float* soa3, const uint32_t* ids, float* ao
 }
 void launch_add_scalar(float* a, size_t n, float v, cudaStream_t s) { { k_add_scalar<<<nblk(n), 256, 0, s>>>(a, n, v); bnn_note_launch(); } }
 void launch_step_reset(DevState* st, cudaStream_t s) { { k_step_reset<<<1, 1, 0, s>>>(st); bnn_note_launch(); } }
+void launch_step_reset_moved(DevState* st, cudaStream_t s) { { k_step_reset_moved<<<1, 1, 0, s>>>(st); bnn_note_launch(); } }
+// FLIP grid-to-particle transfer + the next sub-step's move; the occupied-cell box is
+// rebuilt for the next sub-step
+void launch_g2p_move(int n, const GridDesc& g, float* p6, size_t stride, const float* const* U, const float* const* O,
+                     float ratio, const NextStep& ns, float* moved, uint32_t* cellOf, uint32_t* slot, uint32_t* count,
+                     DevState* st, int* bboxPart, cudaStream_t s) {
+    { k_bbox_reset<<<1, 1, 0, s>>>(st); bnn_note_launch(); }
+    if(n == 0) return;
+    const unsigned blocks = nblk(n);
+    { k_g2p_move<<<blocks, 256, 0, s>>>(n, g, p6, stride, U[0], U[1], U[2], O[0], O[1], O[2], ratio, ns, moved, cellOf,
+                                       slot, count, st, bboxPart); bnn_note_launch(); }
+    const unsigned fb = blocks < 148u * 4u * 256u ? (blocks + 255u) / 256u : 148u * 4u;
+    { k_bbox_final<<<fb, 256, 0, s>>>((int)blocks, bboxPart, st); bnn_note_launch(); }
+}
 void launch_cells_from_rows(size_t nc, const float* phi, const uint32_t* aidx, const float* pr, float* out, int active,
                             cudaStream_t s) {
     { k_cells_from_rows<<<nblk(nc), 256, 0, s>>>(nc, phi, aidx, pr, out, active); bnn_note_launch(); }

@@ -23,12 +23,14 @@
 // layers along y, the gravity axis (Earth gravity is -y, ParticleSolverData.cpp:196-200):
 // a liquid piles up in the cells above the floor, and walking y makes every such crowded
 // layer one layer that all columns of every tile share, instead of a long serial walk
-// inside the few tiles that hold the floor.  For each cell layer it needs, the block first
-// forms the partials of the (kTX + 2) x (kTZ + 2) cells that can reach the tile (a 1-cell
-// halo) into shared memory, one component at a time, then every thread adds the partials
-// its faces need to register accumulators for the three face layers the cell layer
-// reaches.  Each particle record is therefore read once per block (plus the halo) instead
-// of once per candidate face, and the weight of a particle is formed once per reached slot.
+// inside the few tiles that hold the floor.  A block has one thread per cell of its tile
+// and the tile's 1-cell halo (warps are rows of 32 cells along x: 30 interior columns and a
+// halo cell each side).  For each cell layer it needs, every thread forms its cell's
+// partials into shared memory, one component at a time, then the interior threads add the
+// partials their faces need to register accumulators for the three face layers the cell
+// layer reaches.  Each particle record is therefore read once per block (plus the halo)
+// instead of once per candidate face, the weight of a particle is formed once per reached
+// slot, and no thread forms two cells' partials while the rest of the block waits.
 //
 // Input: one 16-byte record per particle and component, written by the sort's gather
 // (flip_kernels.cu, k_gather_particles): plane D < 3 holds {e_x, e_y, e_z, v_D}, e_a the
@@ -37,25 +39,29 @@
 #include "bnn_internal.cuh"
 
 #include <atomic>
+#include <climits>
 
 namespace bnn {
 
 namespace {
-#ifndef BNN_TILE_X
-#define BNN_TILE_X 32
-#endif
 #ifndef BNN_TILE_Z
-#define BNN_TILE_Z 8
+#define BNN_TILE_Z 6
 #endif
 #ifndef BNN_TILE_Y
-#define BNN_TILE_Y 16
+#define BNN_TILE_Y 8
 #endif
-constexpr int kTX = BNN_TILE_X;            // face columns per block along x (one warp)
-constexpr int kTZ = BNN_TILE_Z;            // ... along z
-constexpr int kYC = BNN_TILE_Y;            // face layers per block along y (the walk)
-constexpr int kThreads = kTX * kTZ;
-constexpr int kHX = kTX + 2, kHZ = kTZ + 2;
-constexpr int kNH = kHX * kHZ;             // cells of one layer whose partials the tile needs
+#ifndef BNN_TILE_MIN_BLOCKS
+#define BNN_TILE_MIN_BLOCKS (768 / (32 * (BNN_TILE_Z + 2)))
+#endif
+// A thread per cell of the tile plus its 1-cell halo: a warp is one row of 32 cells along x
+// (30 interior columns and one halo cell each side), kTZ + 2 rows along z.  Every thread
+// forms the partials of exactly one cell, and the interior threads own the faces.
+constexpr int kHX = 32, kTX = kHX - 2;      // cells per row, interior face columns along x
+constexpr int kTZ = BNN_TILE_Z;              // interior face columns along z
+constexpr int kHZ = kTZ + 2;
+constexpr int kYC = BNN_TILE_Y;              // face layers per block along y (the walk)
+constexpr int kThreads = kHX * kHZ;
+constexpr int kNH = kHX * kHZ;               // cells of one layer whose partials the tile needs
 constexpr int kPartials = 36;              // 18 face slots x (momentum, weight); the SDF has 27
 constexpr size_t kSmemBytes = sizeof(float) * kPartials * kNH;
 
@@ -269,13 +275,15 @@ __device__ __forceinline__ void write_phi(const TileArgs& a, int fx, int fy, int
 
 // P2G: the three face components and the fluid SDF (FLIP); otherwise the fluid SDF alone.
 template<bool P2G>
-__global__ void __launch_bounds__(kThreads, 3) k_p2g_sdf_tile(TileArgs a) {
+__global__ void __launch_bounds__(kThreads, BNN_TILE_MIN_BLOCKS) k_p2g_sdf_tile(TileArgs a) {
     extern __shared__ float sm[];
     const GridDesc& g = a.g;
-    const int tx = threadIdx.x, tz = threadIdx.y, t = tz * kTX + tx;
+    const int t = threadIdx.y * kHX + threadIdx.x;        // this thread's halo cell
+    const int tx = threadIdx.x - 1, tz = threadIdx.y - 1;  // interior column (faces) or halo
+    const bool owner = tx >= 0 && tx < kTX && tz >= 0 && tz < kTZ;
     const int x0 = blockIdx.x * kTX, z0 = blockIdx.y * kTZ;
     const int yA = blockIdx.z * kYC, yB = min(yA + kYC, g.G[1] + 1);  // face layers [yA, yB)
-    const int fx = x0 + tx, fz = z0 + tz;
+    const int fx = owner ? x0 + tx : INT_MAX, fz = owner ? z0 + tz : INT_MAX;
     {
         const int lo[3] = {x0 - 1, yA - 1, z0 - 1}, hi[3] = {x0 + kTX, yB, z0 + kTZ};
         if(!meets_particles(a.st, lo, hi)) {
@@ -301,24 +309,24 @@ __global__ void __launch_bounds__(kThreads, 3) k_p2g_sdf_tile(TileArgs a) {
     for(int cy = yA - 1; cy <= yB; ++cy) {
         if(cy >= 0 && cy < g.G[1]) {
             if constexpr(P2G) {
-                for(int h = t; h < kNH; h += kThreads) cell_partials<0>(a, x0, z0, cy, h, sm);
+                cell_partials<0>(a, x0, z0, cy, t, sm);
                 __syncthreads();
-                pull_partials<0>(sm, tx, tz, uS, uW);
+                if(owner) pull_partials<0>(sm, tx, tz, uS, uW);
                 __syncthreads();
                 if(cy < yB) {
-                    for(int h = t; h < kNH; h += kThreads) cell_partials<1>(a, x0, z0, cy, h, sm);
+                    cell_partials<1>(a, x0, z0, cy, t, sm);
                     __syncthreads();
-                    pull_partials<1>(sm, tx, tz, vS, vW);
+                    if(owner) pull_partials<1>(sm, tx, tz, vS, vW);
                     __syncthreads();
                 }
-                for(int h = t; h < kNH; h += kThreads) cell_partials<2>(a, x0, z0, cy, h, sm);
+                cell_partials<2>(a, x0, z0, cy, t, sm);
                 __syncthreads();
-                pull_partials<2>(sm, tx, tz, wS, wW);
+                if(owner) pull_partials<2>(sm, tx, tz, wS, wW);
                 __syncthreads();
             }
-            for(int h = t; h < kNH; h += kThreads) sdf_partials(a, x0, z0, cy, h, exact, sm);
+            sdf_partials(a, x0, z0, cy, t, exact, sm);
             __syncthreads();
-            pull_sdf(sm, tx, tz, aM);
+            if(owner) pull_sdf(sm, tx, tz, aM);
             __syncthreads();
         }
         // face / cell layer cy - 1 is complete for u, w and the SDF, face layer cy for v
@@ -346,6 +354,7 @@ static dim3 tile_grid(const GridDesc& g) {
     return dim3((unsigned)((g.G[0] + 1 + kTX - 1) / kTX), (unsigned)((g.G[2] + 1 + kTZ - 1) / kTZ),
                 (unsigned)((g.G[1] + 1 + kYC - 1) / kYC));
 }
+static_assert(kHX == 32, "a warp is one row of halo cells");
 
 // The dynamic shared memory above the 48 KB default is opted into once per device.
 template<bool P2G>
@@ -358,7 +367,7 @@ static void launch_tile(const TileArgs& a, cudaStream_t s) {
         cudaFuncSetAttribute(k_p2g_sdf_tile<P2G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
         configured.fetch_or(bit, std::memory_order_acq_rel);
     }
-    k_p2g_sdf_tile<P2G><<<tile_grid(a.g), dim3(kTX, kTZ), kSmemBytes, s>>>(a);
+    k_p2g_sdf_tile<P2G><<<tile_grid(a.g), dim3(kHX, kHZ), kSmemBytes, s>>>(a);
     bnn_note_launch();
 }
 

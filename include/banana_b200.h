@@ -153,7 +153,8 @@ int bnn_flip_step(bnn_flip* h, bnn_step_stats* stats);
 /* PIC_Solver::advanceFrame: sub-steps until FrameDuration is reached. */
 int bnn_flip_advance_frame(bnn_flip* h, uint32_t* substeps);
 /* Device pointers of the particle arrays (SoA x,y,z,vx,vy,vz, current sorted order),
- * valid until the next step; lets a caller keep data on the device. */
+ * valid until the next step; lets a caller keep data on the device (and change it: the
+ * next step then moves the particles from what the arrays hold). */
 int bnn_flip_device_particles(bnn_flip* h, float** xyz_vxyz_dev, uint32_t** ids_dev);
 /* The cudaStream_t every kernel of this handle is launched on (for events / ordering). */
 int bnn_flip_stream(bnn_flip* h, void** stream);
