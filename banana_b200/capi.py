@@ -37,7 +37,7 @@ EXPORTS = [
     "bnn_batch_create", "bnn_batch_destroy", "bnn_batch_add_scene", "bnn_batch_remove_scene", "bnn_batch_step",
     "bnn_batch_scene_info", "bnn_batch_get_scene", "bnn_batch_memory",
     "bnn_aniso_default_params", "bnn_anisotropic_kernels", "bnn_flip_anisotropic_kernels",
-    "bnn_flip_set_boundaries",
+    "bnn_flip_set_boundaries", "bnn_tile_shapes", "bnn_set_tile_shape", "bnn_tile_tuning",
 ]
 
 
@@ -69,13 +69,18 @@ class StepStats(C.Structure):
     ]
 
 
+BATCH_STAGED = 0      # BNN_BATCH_STAGED: one launch per stage over the scenes it takes
+BATCH_PER_SCENE = 1   # BNN_BATCH_PER_SCENE: every scene on its own stream
+
+
 class BatchParams(C.Structure):
-    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("worker_threads", C.c_uint32)]
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("worker_threads", C.c_uint32), ("step_mode", C.c_uint32)]
 
 
 class BatchStats(C.Structure):
     _fields_ = [("scenes", C.c_uint32), ("failed", C.c_uint32), ("particle_steps", C.c_uint64),
-                ("pcg_iterations", C.c_uint64), ("wall_ms", C.c_double), ("max_scene_ms", C.c_double)]
+                ("pcg_iterations", C.c_uint64), ("wall_ms", C.c_double), ("max_scene_ms", C.c_double),
+                ("staged_scenes", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 class PcgStats(C.Structure):
@@ -183,6 +188,9 @@ def load() -> C.CDLL:
     L.bnn_batch_get_scene.argtypes = [vp, C.c_uint32, fp, fp]
     L.bnn_batch_memory.argtypes = [vp, u64p, u64p]
     L.bnn_flip_set_boundaries.argtypes = [vp, C.POINTER(BoundaryObject), C.c_uint32, C.c_int32]
+    L.bnn_tile_shapes.argtypes = [i32p, i32p, C.c_int32]
+    L.bnn_set_tile_shape.argtypes = [C.c_int32]
+    L.bnn_tile_tuning.argtypes = [C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]
     L.bnn_aniso_default_params.argtypes = [C.c_float, C.POINTER(AnisoParams)]
     L.bnn_anisotropic_kernels.argtypes = [vp, C.c_uint32, C.POINTER(AnisoParams), vp, vp, C.POINTER(AnisoStats), vp]
     L.bnn_flip_anisotropic_kernels.argtypes = [vp, C.POINTER(AnisoParams), fp, fp, C.POINTER(AnisoStats)]
@@ -195,6 +203,32 @@ def load() -> C.CDLL:
             getattr(L, name).restype = C.c_int
     _lib = L
     return L
+
+
+def tile_shapes() -> list:
+    """(tz, yc) of every tile shape of the FLIP P2G + fluid SDF pass (bnn_tile_shapes)."""
+    L = load()
+    n = int(L.bnn_tile_shapes(None, None, 0))
+    tz, yc = (C.c_int32 * n)(), (C.c_int32 * n)()
+    L.bnn_tile_shapes(tz, yc, n)
+    return [(int(tz[i]), int(yc[i])) for i in range(n)]
+
+
+def set_tile_shape(shape: int) -> None:
+    """Use one tile shape for every launch of the process (-1: tune per launch kind)."""
+    L = load()
+    check(L.bnn_set_tile_shape(int(shape)), "bnn_set_tile_shape")
+
+
+def tile_tuning() -> list:
+    """The tuner's choices so far, one dict per tuned launch kind (bnn_tile_tuning)."""
+    import json
+    L = load()
+    need = C.c_size_t()
+    L.bnn_tile_tuning(None, 0, C.byref(need))
+    buf = C.create_string_buffer(int(need.value))
+    check(L.bnn_tile_tuning(buf, len(buf), C.byref(need)), "bnn_tile_tuning")
+    return [json.loads(line) for line in buf.value.decode().splitlines() if line.strip()]
 
 
 def launch_count() -> int:
@@ -425,9 +459,9 @@ class FlipBatch:
     """Many independent scenes on one GPU (bnn_batch_*): every scene computes what a lone
     FlipSolver computes; step() advances all of them by one sub-step."""
 
-    def __init__(self, hbm_budget_bytes: int = 0, worker_threads: int = 0):
+    def __init__(self, hbm_budget_bytes: int = 0, worker_threads: int = 0, step_mode: int = BATCH_STAGED):
         self.L = load()
-        bp = BatchParams(int(hbm_budget_bytes), int(worker_threads))
+        bp = BatchParams(int(hbm_budget_bytes), int(worker_threads), int(step_mode))
         h = C.c_void_p()
         check(self.L.bnn_batch_create(C.byref(bp), C.byref(h)), "bnn_batch_create")
         self.h = h
@@ -472,6 +506,7 @@ class FlipBatch:
         st = StepStats()
         rc = self.L.bnn_batch_scene_info(self.h, int(sid), C.byref(n), C.byref(steps), C.byref(st))
         d = {f: getattr(st, f) for f, _ in StepStats._fields_ if f != "stage_ms"}
+        d["stage_ms"] = dict(zip(STAGES, list(st.stage_ms)))
         d.update(n=int(n.value), steps=int(steps.value), status=int(rc))
         return d
 

@@ -2,15 +2,19 @@
 //
 // Every scene is a full solver handle (its own grids, particles, pressure system and CUDA
 // stream), so each scene computes exactly what a lone bnn_flip_step computes.  A step of
-// the batch advances every live scene by one sub-step: a pool of host worker threads
-// takes the scenes (longest first, to the least loaded worker) and steps them on their
-// own streams, so the kernels of many small scenes run side by side and fill the GPU
-// that one small scene leaves mostly idle.  Scenes are admitted against a device-memory
-// budget with bnn_scene_bytes_estimate.
+// the batch advances every live scene by one sub-step:
+// * the scenes the staged step takes (batch_step.cu) advance together on the batch's own
+//   stream, one kernel launch per stage of the sub-step over all of them;
+// * the others (and all of them in BNN_BATCH_PER_SCENE mode) are stepped by a pool of host
+//   worker threads (longest first, to the least loaded worker), each scene on its own
+//   stream, so the kernels of many small scenes run side by side.
+// Both run at the same time; the cooperative PCG launches of the two share the GPU through
+// pcg.cu's occupancy accounting.  Scenes are admitted against a device-memory budget with
+// bnn_scene_bytes_estimate.
 //
 // The reference runs one scene per ParticleSolver object (ParticleSolver.h:39-105); a
 // batch is what a server holding many such objects does, with the objects on one GPU.
-#include "bnn_internal.cuh"
+#include "batch_step.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -38,6 +42,8 @@ struct Scene {
 
 struct bnn_batch {
     int device = 0;
+    uint32_t mode = BNN_BATCH_STAGED;
+    BatchStepWork staged;
     uint64_t budget = 0;
     uint64_t admitted = 0;
     uint32_t nextId = 1;
@@ -90,6 +96,11 @@ extern "C" int bnn_batch_create(const bnn_batch_params* params, bnn_batch** out)
     auto* b = new bnn_batch();
     BNN_CUDA_CHECK(cudaGetDevice(&b->device));
     b->budget = params ? params->hbm_budget_bytes : 0;
+    b->mode = params ? params->step_mode : BNN_BATCH_STAGED;
+    if(b->mode != BNN_BATCH_STAGED && b->mode != BNN_BATCH_PER_SCENE) {
+        delete b;
+        return BNN_ERR_INVALID_ARGUMENT;
+    }
     int nw = params && params->worker_threads ? (int)params->worker_threads : 0;
     if(nw <= 0) {
         const unsigned hc = std::thread::hardware_concurrency();
@@ -110,6 +121,7 @@ extern "C" int bnn_batch_destroy(bnn_batch* b) {
     }
     b->cvWork.notify_all();
     for(auto& t : b->threads) t.join();
+    batch_step_release(b->staged);
     for(auto& s : b->scenes) bnn_flip_destroy(s->h);
     delete b;
     return BNN_OK;
@@ -157,15 +169,16 @@ extern "C" int bnn_batch_remove_scene(bnn_batch* b, uint32_t id) {
 extern "C" int bnn_batch_step(bnn_batch* b, bnn_batch_stats* stats) {
     if(!b) return BNN_ERR_INVALID_ARGUMENT;
     const auto t0 = std::chrono::steady_clock::now();
+    std::vector<Scene*> staged, rest;
+    for(auto& s : b->scenes)
+        (b->mode == BNN_BATCH_STAGED && batch_step_eligible(s->h) ? staged : rest).push_back(s.get());
     {
         std::unique_lock<std::mutex> lk(b->mu);
         // longest processing time first: biggest scene to the least loaded worker
-        std::vector<Scene*> order;
-        for(auto& s : b->scenes) order.push_back(s.get());
-        std::stable_sort(order.begin(), order.end(), [](const Scene* x, const Scene* y) { return x->estimate > y->estimate; });
+        std::stable_sort(rest.begin(), rest.end(), [](const Scene* x, const Scene* y) { return x->estimate > y->estimate; });
         std::vector<uint64_t> load(b->nworkers, 0);
         for(auto& w : b->work) w.clear();
-        for(Scene* s : order) {
+        for(Scene* s : rest) {
             const int w = (int)(std::min_element(load.begin(), load.end()) - load.begin());
             b->work[w].push_back(s);
             load[w] += s->estimate;
@@ -174,14 +187,34 @@ extern "C" int bnn_batch_step(bnn_batch* b, bnn_batch_stats* stats) {
         ++b->gen;
     }
     b->cvWork.notify_all();
+    int batchRc = BNN_OK;
+    if(!staged.empty()) {
+        // the staged scenes on this thread, meanwhile
+        const int ns = (int)staged.size();
+        std::vector<bnn_flip*> hs(ns);
+        std::vector<int> rcs(ns);
+        std::vector<bnn_step_stats> sts(ns);
+        for(int i = 0; i < ns; ++i) hs[i] = staged[i]->h;
+        const auto t1 = std::chrono::steady_clock::now();
+        batchRc = batch_substep(b->staged, hs.data(), ns, rcs.data(), sts.data());
+        const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t1).count();
+        for(int i = 0; i < ns; ++i) {
+            Scene* sc = staged[i];
+            sc->status = batchRc != BNN_OK ? batchRc : rcs[i];
+            sc->last = sts[i];
+            sc->ms = ms;
+            if(sc->status == BNN_OK) ++sc->steps;
+        }
+    }
     {
         std::unique_lock<std::mutex> lk(b->mu);
         b->cvDone.wait(lk, [&] { return b->pending == 0; });
     }
     const double wall = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    int rc = BNN_OK;
+    int rc = batchRc;
     bnn_batch_stats st{};
     st.wall_ms = wall;
+    st.staged_scenes = (uint32_t)staged.size();
     for(auto& s : b->scenes) {
         ++st.scenes;
         if(s->status != BNN_OK) {

@@ -96,6 +96,32 @@ __device__ __forceinline__ float reduce_partials_max(const float* part, int nch,
     return block_max_256(acc, sm);
 }
 
+// Block coordinates a kernel body works in: its own launch's (blockIdx.x, gridDim.x), or,
+// in a batched launch over many scenes (batch_step.cu), the block's place within its
+// scene's share of the launch.
+struct Blk {
+    unsigned x, n;
+};
+__device__ __forceinline__ Blk own_blk() { return Blk{blockIdx.x, gridDim.x}; }
+
+// The segment (scene) a block of a batched launch belongs to: prefix[s] <= b < prefix[s+1],
+// prefix[0] = 0, prefix[nseg] = the launch's blocks (segments with no blocks are skipped).
+__device__ __forceinline__ int seg_of(const unsigned* __restrict__ prefix, int nseg, unsigned b) {
+    int lo = 0, hi = nseg;
+    while(hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if(__ldg(prefix + mid) <= b) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+// The block's segment and its place within the segment's blocks
+__device__ __forceinline__ Blk seg_blk(const unsigned* __restrict__ prefix, int nseg, int& s) {
+    s = seg_of(prefix, nseg, blockIdx.x);
+    const unsigned b0 = __ldg(prefix + s);
+    return Blk{blockIdx.x - b0, __ldg(prefix + s + 1) - b0};
+}
+
 // ----------------------------------------------------------------------------------
 // Scalar helpers, same semantics as the reference's MathHelpers
 // ----------------------------------------------------------------------------------
@@ -236,12 +262,81 @@ struct NextStep {
 #define BNN_FLAG_TIMEOUT       16u
 
 // ----------------------------------------------------------------------------------
+// One scene of a batched sub-step (batch_step.cu): what its stage kernels read.  The
+// batched kernels run the same bodies as a lone scene's kernels, each block on the scene
+// and block coordinates its place in the launch gives it (seg_blk).
+// ----------------------------------------------------------------------------------
+struct BScene {
+    GridDesc g;
+    int n;                  // particles
+    int nrows;              // pressure rows (known after the system's numbering)
+    int advSteps;
+    int moved;              // the move already ran at the end of the last sub-step
+    size_t cap;             // particle plane stride
+    size_t C;               // cells
+    float sub, substep, gdt;
+    float ratio;            // PIC_FLIP_ratio
+    NextStep ns;            // the next sub-step (fused move)
+    float *p6cur, *p6nxt, *movedPos;
+    uint32_t *idcur, *idnxt;
+    float4* rec;
+    uint32_t *cellOf, *slot, *order, *key, *count, *cellStart;
+    int* bboxPart;
+    float* U[3];
+    float* B[3];
+    float* O[3];
+    uint8_t* VA[3];
+    uint8_t* VB[3];
+    float* phi;
+    uint32_t *flag, *aidx, *rowCell;
+    float *rhs, *diag, *invd, *pressure;
+    int32_t* nbr;
+    DevState* dst;
+};
+// Stages of the batched sub-step (flip_kernels.cu), one launch each over all scenes
+enum class BatchStage {
+    StepReset, BboxReset, Advect, BboxFinal, ScatterIndex, SortBuckets, SortLarge, Gather, FillBackup, FillUpdate,
+    Extrapolate, ActiveFlags, ActiveRows, BuildRows, UpdateU, UpdateV, UpdateW, G2PMove
+};
+void launch_batch_stage(BatchStage stage, const BScene* S, const unsigned* P, int ns, unsigned blocks, cudaStream_t s,
+                        int pass = 0, int layer = 0);
+void launch_batch_gather_rows(const BScene* S, int ns, unsigned* out, cudaStream_t s);
+void launch_batch_gather_state(const BScene* S, int ns, DevState* out, cudaStream_t s);
+// The FLIP P2G + fluid SDF pass of all scenes (gather_kernels.cu): per-scene argument
+// records (p2g_tile_args, p2g_tile_args_bytes() each) and the tile prefix P
+// in each tile shape (launch_p2g_sdf_batch picks one: P[shape] and tiles[shape] are the
+// tile prefix and total of every shape, cells the batch's total cells)
+constexpr int kTileShapes = 6;
+unsigned p2g_sdf_tiles(const GridDesc& g, int shape);
+size_t p2g_tile_args_bytes();
+void p2g_tile_args(void* out, const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float4* rec,
+                   size_t stride, float* const U[3], uint8_t* const valid[3], float* phi);
+void launch_p2g_sdf_batch(const void* args, const unsigned* const* P, const unsigned* tiles, int ns, uint64_t cells,
+                          cudaStream_t s);
+// The tile-shape tuner (gather_kernels.cu): force a shape for every launch (-1: tune), the
+// dimensions of a shape, and the table of tuned choices as JSON lines
+int tile_shape_set(int shape);
+void tile_shape_dims(int shape, int* tz, int* yc);
+
+// ----------------------------------------------------------------------------------
 // Host-side launchers (defined in the .cu files)
 // ----------------------------------------------------------------------------------
 // scan.cu
 size_t scan_workspace_bytes(size_t n);
 // exclusive scan of n uint32 into out[0..n], out[n] = total; ws from scan_workspace_bytes
 cudaError_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, size_t n, void* ws, cudaStream_t s);
+// Many independent exclusive scans in three launches: segment q scans in[0..n) into
+// out[0..n] with workspace ws (scan_workspace_bytes(n)).  tiles[q] is the prefix of the
+// segments' 2048-element tile counts (at least 1 each; tiles[nseg] = totalTiles), in
+// device memory.
+struct ScanSeg {
+    const uint32_t* in;
+    uint32_t* out;
+    uint32_t* ws;
+    size_t n;
+};
+cudaError_t batched_exclusive_scan_u32(const ScanSeg* segs, const unsigned* tiles, int nseg, unsigned totalTiles,
+                                       cudaStream_t s);
 
 // pcg.cu
 struct GridSync {
@@ -283,6 +378,32 @@ int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const floa
               float outerTol, float* pressure, double* x64out, DevState* dst, DevState* hst, cudaStream_t s,
               PcgOutcome& out);
 int pcg_reserve(PcgWork& w, int n, bool fp64);
+// One scene's system in a batched refined solve (BNN_PCG_REFINED, two-reduction steps,
+// rows of a grid, face weights 1): what pcg_solve would be called with, and its outcome.
+struct BatchSolveItem {
+    PcgWork* w;
+    int n;
+    const float *rhs, *diag, *invd;
+    const int32_t* nbr;
+    float dt, innerTol, outerTol;
+    unsigned maxIter;
+    float* pressure;
+    DevState* dst;
+    PcgOutcome out;
+};
+// Device tables of the batched solve, kept between calls (grown on demand)
+struct BatchPcgCtx {
+    int cap = 0;
+    size_t upBytes = 0, blobBytes = 0;
+    void* dev = nullptr;       // device tables, reports, barrier
+    void* host = nullptr;      // pinned mirror of the uploaded part, then the reports
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+};
+// The refined solves of many scenes, each stage one launch over the scenes still
+// refining: every scene gets exactly what pcg_solve gives it alone.  Returns BNN status;
+// items[i].out holds each scene's outcome, its pressure is written.
+int pcg_solve_batch_refined(BatchPcgCtx& ctx, BatchSolveItem* items, int count, cudaStream_t s);
+void pcg_batch_release(BatchPcgCtx& ctx);
 // one block waits at a barrier sized for two until the bounded wait gives up
 int pcg_barrier_probe(float limitSeconds, int* barrierStatus, float* elapsedMs);
 // Cell grid of the anisotropic-kernel pass (aniso.cu)

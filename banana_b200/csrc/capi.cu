@@ -83,69 +83,7 @@ void launch_g2p_move(int n, const GridDesc& g, float* p6, size_t stride, const f
 
 using namespace bnn;
 
-struct bnn_flip {
-    bnn_params P{};
-    GridDesc g{};
-    size_t C = 0;      // cells
-    size_t F[3] = {};  // faces per component
-    float frameDuration = 0.f, frameTime = 0.f;
-    uint32_t n = 0, cap = 0;
-    cudaStream_t s = nullptr;
-    // particles: SoA (x,y,z,vx,vy,vz) with stride cap; ping-pong for the sort
-    float* p6[2] = {nullptr, nullptr};
-    uint32_t* ids[2] = {nullptr, nullptr};
-    float* C9[2] = {nullptr, nullptr};
-    int cur = 0;
-    float* g3 = nullptr;    // grid coordinates (APIC / AFLIP P2G)
-    float4* rec = nullptr;  // per-particle gather records: 3 P2G stencil planes + positions
-    uint32_t *cellOf = nullptr, *slot = nullptr, *order = nullptr, *key = nullptr;
-    int* bboxPart = nullptr;  // per-block occupied-cell boxes of the advection
-    uint32_t *count = nullptr, *cellStart = nullptr;
-    void* scanWs = nullptr;
-    float* aosStage = nullptr;
-    float* aniso = nullptr;  // anisotropic-kernel output: centres 3 cap, matrices 9 cap, 2 counters
-    // boundary objects beyond the domain box (g.obj points at objDev)
-    BObj* objDev = nullptr;
-    bool gridBoundary = false;  // a dynamic object exists: node SDF, weights, constraint
-    float* nodeSdf = nullptr;   // (G+1)^3
-    float* W[3] = {};           // face weights
-    float* coef = nullptr;      // off-diagonal values of the rows (6 planes, coefCap rows)
-    int coefCap = 0;
-    // faces
-    float* U[3] = {};
-    float* B[3] = {};
-    float* O[3] = {};
-    uint8_t* VA[3] = {};
-    uint8_t* VB[3] = {};
-    // cells
-    float* phi = nullptr;
-    uint32_t* flag = nullptr;
-    uint32_t* aidx = nullptr; // C+1
-    float* cellTmp = nullptr;
-    // rows
-    int rowCap = 0;
-    uint32_t nRows = 0;
-    uint32_t* rowCell = nullptr;
-    float *rhs = nullptr, *diag = nullptr, *invd = nullptr, *pressure = nullptr;
-    int32_t* nbr = nullptr;
-    PcgWork pcg;
-    DevState* dst = nullptr;
-    DevState* hst = nullptr;
-    cudaEvent_t ev[11] = {};
-    // host transfers of bnn_flip_step_host that overlap the step: a copy stream and its
-    // events (stream idle, velocities on the device, positions final)
-    cudaStream_t s2 = nullptr;
-    cudaEvent_t io[3] = {};
-    unsigned maxvelBits = 0; // max|u| of the current grid (for the next CFL)
-    unsigned long long substepIndex = 0;  // sub-steps taken (keys the position-correction jitter)
-    // FLIP: the next sub-step's particle move runs at the end of this one (k_g2p_move); its
-    // positions, cell ids, histogram and occupied-cell box then wait for the next sub-step,
-    // which must use premovedDt as its size.  Anything that changes the particles, the grid
-    // velocities or the boundaries in between drops it (the next sub-step moves as usual).
-    float* moved = nullptr;  // 3 planes, stride cap
-    bool premoved = false;
-    float premovedDt = 0.f;
-};
+#include "flip_handle.cuh"
 
 static void free_particles(bnn_flip* h) {
     for(int b = 0; b < 2; ++b) {
@@ -185,21 +123,6 @@ static int reserve_particles(bnn_flip* h, uint32_t n) {
     BNN_CUDA_CHECK(cudaMalloc(&h->aosStage, 6 * st * sizeof(float)));
     if(h->P.solver_kind == BNN_SOLVER_FLIP) BNN_CUDA_CHECK(cudaMalloc(&h->moved, 3 * st * sizeof(float)));
     h->cap = cap;
-    return BNN_OK;
-}
-
-static int reserve_rows(bnn_flip* h, uint32_t n) {
-    if((int)n <= h->rowCap) return BNN_OK;
-    cudaFree(h->rowCell); cudaFree(h->rhs); cudaFree(h->diag); cudaFree(h->invd); cudaFree(h->pressure); cudaFree(h->nbr);
-    int cap = (int)(n * 1.25) + 1024;
-    if((size_t)cap > h->C) cap = (int)h->C;
-    BNN_CUDA_CHECK(cudaMalloc(&h->rowCell, cap * sizeof(uint32_t)));
-    BNN_CUDA_CHECK(cudaMalloc(&h->rhs, cap * sizeof(float)));
-    BNN_CUDA_CHECK(cudaMalloc(&h->diag, cap * sizeof(float)));
-    BNN_CUDA_CHECK(cudaMalloc(&h->invd, cap * sizeof(float)));
-    BNN_CUDA_CHECK(cudaMalloc(&h->pressure, cap * sizeof(float)));
-    BNN_CUDA_CHECK(cudaMalloc(&h->nbr, 6 * (size_t)cap * sizeof(int32_t)));
-    h->rowCap = cap;
     return BNN_OK;
 }
 
@@ -422,7 +345,10 @@ extern "C" int bnn_flip_get_particles(bnn_flip* h, float* pos, float* vel) {
 
 extern "C" int bnn_flip_device_particles(bnn_flip* h, float** p6, uint32_t** ids) {
     if(!h) return BNN_ERR_INVALID_ARGUMENT;
-    h->premoved = false;  // the caller may change the particles through these pointers
+    {
+        const int rc = drop_premove(h);  // the caller may change the particles through these pointers
+        if(rc != BNN_OK) return rc;
+    }
     if(p6) *p6 = h->p6[h->cur];
     if(ids) *ids = h->ids[h->cur];
     return BNN_OK;
@@ -433,7 +359,10 @@ extern "C" int bnn_flip_device_particles(bnn_flip* h, float** p6, uint32_t** ids
 extern "C" int bnn_flip_set_grid(bnn_flip* h, int32_t field, const float* in, size_t count) {
     if(!h || !in || field < BNN_FIELD_U || field > BNN_FIELD_W) return BNN_ERR_INVALID_ARGUMENT;
     if(count != h->F[field]) return BNN_ERR_INVALID_ARGUMENT;
-    h->premoved = false;
+    {
+        const int rc = drop_premove(h);
+        if(rc != BNN_OK) return rc;
+    }
     BNN_CUDA_CHECK(cudaMemcpyAsync(h->U[field], in, count * sizeof(float), cudaMemcpyHostToDevice, h->s));
     BNN_CUDA_CHECK(cudaMemsetAsync(&h->dst->maxvel_bits, 0, sizeof(unsigned), h->s));
     for(int d = 0; d < 3; ++d) launch_maxabs(h->U[d], h->F[d], &h->dst->maxvel_bits, h->s);
@@ -498,7 +427,10 @@ extern "C" int bnn_flip_get_grid(bnn_flip* h, int32_t field, float* out, size_t 
 extern "C" int bnn_flip_set_boundaries(bnn_flip* h, const bnn_boundary_object* objs, uint32_t n,
                                        int32_t update_grid) {
     if(!h || (n && !objs) || n >= (uint32_t)kMaxBoundaryObjects) return BNN_ERR_INVALID_ARGUMENT;
-    h->premoved = false;  // the next move must see these objects
+    {
+        const int rc = drop_premove(h);  // the next move must see these objects
+        if(rc != BNN_OK) return rc;
+    }
     std::vector<BObj> list;
     BObj box{};
     box.geometry = 0;
@@ -548,18 +480,6 @@ extern "C" int bnn_flip_set_boundaries(bnn_flip* h, const bnn_boundary_object* o
     return BNN_OK;
 }
 
-// PIC_Solver::timestepCFL (PIC_Solver.cpp:342-349) from max|u| of the current grid
-static float timestep_cfl(const bnn_flip* h) {
-    float m;
-    std::memcpy(&m, &h->maxvelBits, 4);
-    float maxVel = FLT_MIN;
-    maxVel = (maxVel < m) ? m : maxVel;
-    float ts = maxVel > FLT_MIN ? h->P.cfl_factor * (h->g.dx / maxVel) : FLT_MAX;
-    if(ts < h->P.min_timestep) return h->P.min_timestep;
-    if(ts > h->P.max_timestep) return h->P.max_timestep;
-    return ts;
-}
-
 // Host arrays of bnn_flip_step_host whose transfers overlap the step: the main stream waits
 // for the velocity upload only where the sort first gathers velocities, and the positions
 // go back to the host on the copy stream as soon as they are final (after the sort), while
@@ -572,23 +492,19 @@ struct HostIo {
 static int run_substep(bnn_flip* h, bnn_step_stats* st, const HostIo* io = nullptr) {
     cudaStream_t s = h->s;
     const GridDesc& g = h->g;
-    if(h->frameTime >= h->frameDuration) h->frameTime = 0.f;
-    // PIC_Solver::advanceFrame sub-step size (PIC_Solver.cpp:284-290)
-    float substep = timestep_cfl(h);
-    const float remaining = h->frameDuration - h->frameTime;
-    if(h->frameTime + substep >= h->frameDuration) substep = remaining;
-    else if(h->frameTime + 1.5f * substep >= h->frameDuration) substep = remaining * 0.5f;
+    const float substep = begin_substep(h);
     const float sub = substep / (float)h->P.advection_steps;
     const int kind = h->P.solver_kind;
     const bool affine = kind == BNN_SOLVER_APIC || kind == BNN_SOLVER_AFLIP;
     const int n = (int)h->n;
     // the move already ran at the end of the last sub-step: with the size computed there
     const bool moved = h->premoved && n > 0;
-    h->premoved = false;
     if(moved && substep != h->premovedDt) {
+        drop_premove(h);
         bnn_set_error("sub-step size of the fused move differs from the host's");
         return BNN_ERR_DEVICE_CHECK;
     }
+    h->premoved = false;
 
     cudaEventRecord(h->ev[0], s);
     if(moved) {
@@ -789,7 +705,10 @@ extern "C" int bnn_flip_step_host(bnn_flip* h, float* pos, float* vel, bnn_step_
     const int n = (int)h->n;
     const size_t cap = h->cap;
     HostIo io;
-    h->premoved = false;  // new particle data from the caller
+    {
+        const int rc = drop_premove(h);  // new particle data from the caller
+        if(rc != BNN_OK) return rc;
+    }
     if(n) {
         cudaStream_t s = h->s, s2 = h->s2;
         if(h->C9[h->cur]) {
@@ -853,7 +772,8 @@ extern "C" int bnn_flip_anisotropic_kernels(bnn_flip* h, const bnn_aniso_params*
     if(n == 0) return BNN_OK;
     cudaStream_t s = h->s;
     const bool affine = h->P.solver_kind == BNN_SOLVER_APIC || h->P.solver_kind == BNN_SOLVER_AFLIP;
-    h->premoved = false;  // the re-sort below reuses the move's buffers
+    rc = drop_premove(h);  // the re-sort below reuses the move's buffers
+    if(rc != BNN_OK) return rc;
     launch_rebin(n, h->p6[h->cur], h->cap, g, h->cellOf, h->slot, h->count, h->dst, s);
     BNN_CUDA_CHECK(exclusive_scan_u32(h->count, h->cellStart, h->C, h->scanWs, s));
     const int nxt = 1 - h->cur;
@@ -906,6 +826,27 @@ extern "C" int bnn_flip_advance_frame(bnn_flip* h, uint32_t* substeps) {
 // ---------------------------------------------------------------------------------
 // Standalone PCG on a 7-point system
 // ---------------------------------------------------------------------------------
+namespace bnn {
+std::string tile_tuning_report();
+}
+extern "C" int bnn_tile_shapes(int32_t* tz, int32_t* yc, int32_t cap) {
+    for(int k = 0; k < kTileShapes && k < cap; ++k) {
+        int a = 0, b = 0;
+        tile_shape_dims(k, &a, &b);
+        if(tz) tz[k] = a;
+        if(yc) yc[k] = b;
+    }
+    return kTileShapes;
+}
+extern "C" int bnn_set_tile_shape(int32_t shape) { return tile_shape_set(shape); }
+extern "C" int bnn_tile_tuning(char* buf, size_t cap, size_t* needed) {
+    const std::string r = tile_tuning_report();
+    if(needed) *needed = r.size() + 1;
+    if(!buf || cap < r.size() + 1) return BNN_ERR_CAPACITY;
+    std::memcpy(buf, r.c_str(), r.size() + 1);
+    return BNN_OK;
+}
+
 extern "C" int bnn_pcg_barrier_probe(float limit_seconds, int32_t* barrier_status, float* elapsed_ms) {
     if(!barrier_status || !elapsed_ms || !(limit_seconds > 0.f && limit_seconds <= 10.f)) return BNN_ERR_INVALID_ARGUMENT;
     int st = BNN_OK;

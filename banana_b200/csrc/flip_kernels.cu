@@ -184,8 +184,8 @@ __device__ __forceinline__ void bbox_block_reduce(DevState* st, int mn[3], int m
     }
 }
 
-// The block's box written to part[6 * blockIdx.x ...] (min x,y,z, max x,y,z), no atomics
-__device__ __forceinline__ void bbox_block_partial(int* __restrict__ part, int mn[3], int mx[3]) {
+// The block's box written to part[6 * bx ...] (min x,y,z, max x,y,z), no atomics
+__device__ __forceinline__ void bbox_block_partial(int* __restrict__ part, unsigned bx, int mn[3], int mx[3]) {
     __shared__ int sm[2][3][32];
 #pragma unroll
     for(int d = 0; d < 3; ++d)
@@ -203,19 +203,22 @@ __device__ __forceinline__ void bbox_block_partial(int* __restrict__ part, int m
         const int d = threadIdx.x;
         int a = INT_MAX, b = INT_MIN;
         for(int q = 0; q < nw; ++q) { a = min(a, sm[0][d][q]); b = max(b, sm[1][d][q]); }
-        part[6 * blockIdx.x + d] = a;
-        part[6 * blockIdx.x + 3 + d] = b;
+        part[6 * bx + d] = a;
+        part[6 * bx + 3 + d] = b;
     }
 }
 
 // Folds the per-block boxes into DevState::bbox
-__global__ void __launch_bounds__(256) k_bbox_final(int nparts, const int* __restrict__ part, DevState* st) {
+__device__ __forceinline__ void bbox_final_body(Blk blk, int nparts, const int* __restrict__ part, DevState* st) {
     int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {INT_MIN, INT_MIN, INT_MIN};
-    for(int q = blockIdx.x * blockDim.x + threadIdx.x; q < nparts; q += gridDim.x * blockDim.x) {
+    for(int q = blk.x * blockDim.x + threadIdx.x; q < nparts; q += blk.n * blockDim.x) {
 #pragma unroll
         for(int d = 0; d < 3; ++d) { mn[d] = min(mn[d], part[6 * q + d]); mx[d] = max(mx[d], part[6 * q + 3 + d]); }
     }
     bbox_block_reduce(st, mn, mx);
+}
+__global__ void __launch_bounds__(256) k_bbox_final(int nparts, const int* __restrict__ part, DevState* st) {
+    bbox_final_body(own_blk(), nparts, part, st);
 }
 
 // ----------------------------------------------------------------------------------
@@ -241,14 +244,14 @@ __device__ __forceinline__ void histogram_slot(uint32_t c, int p, uint32_t* __re
     slot[p] = base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
 }
 
-__global__ void __launch_bounds__(256, 6) k_advect(int n, float* __restrict__ px, float* __restrict__ py,
-                                                float* __restrict__ pz, const float* __restrict__ u,
-                                                const float* __restrict__ v, const float* __restrict__ w, GridDesc g,
-                                                float sub, int steps, uint32_t* __restrict__ cellOf,
-                                                uint32_t* __restrict__ slot, uint32_t* __restrict__ count,
-                                                DevState* st, int* __restrict__ bboxPart) {
+__device__ __forceinline__ void advect_body(Blk blk, int n, float* __restrict__ px, float* __restrict__ py,
+                                            float* __restrict__ pz, const float* __restrict__ u,
+                                            const float* __restrict__ v, const float* __restrict__ w,
+                                            const GridDesc& g, float sub, int steps, uint32_t* __restrict__ cellOf,
+                                            uint32_t* __restrict__ slot, uint32_t* __restrict__ count, DevState* st,
+                                            int* __restrict__ bboxPart) {
     int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {INT_MIN, INT_MIN, INT_MIN};
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int p = blk.x * blockDim.x + threadIdx.x;
     uint32_t c = 0xffffffffu;
     if(p < n) {
         float x = px[p], y = py[p], z = pz[p];
@@ -275,7 +278,15 @@ __global__ void __launch_bounds__(256, 6) k_advect(int n, float* __restrict__ px
         for(int d = 0; d < 3; ++d) { mn[d] = cc[d]; mx[d] = cc[d]; }
     }
     histogram_slot(c, p, count, slot);
-    bbox_block_partial(bboxPart, mn, mx);
+    bbox_block_partial(bboxPart, blk.x, mn, mx);
+}
+__global__ void __launch_bounds__(256, 6) k_advect(int n, float* __restrict__ px, float* __restrict__ py,
+                                                float* __restrict__ pz, const float* __restrict__ u,
+                                                const float* __restrict__ v, const float* __restrict__ w, GridDesc g,
+                                                float sub, int steps, uint32_t* __restrict__ cellOf,
+                                                uint32_t* __restrict__ slot, uint32_t* __restrict__ count,
+                                                DevState* st, int* __restrict__ bboxPart) {
+    advect_body(own_blk(), n, px, py, pz, u, v, w, g, sub, steps, cellOf, slot, count, st, bboxPart);
 }
 
 // ----------------------------------------------------------------------------------
@@ -401,14 +412,21 @@ __global__ void k_cell_histogram(int n, const float* __restrict__ px, const floa
 // Counting-sort scatter: position of particle p = cellStart[cell] + arrival slot; the
 // particle's id goes to the same position of key, so the bucket sort reads its keys
 // contiguously instead of gathering them through order.
-__global__ void k_scatter_index(int n, const uint32_t* __restrict__ cellOf, const uint32_t* __restrict__ slot,
-                                const uint32_t* __restrict__ cellStart, const uint32_t* __restrict__ ids,
-                                uint32_t* __restrict__ order, uint32_t* __restrict__ key) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void scatter_index_body(Blk blk, int n, const uint32_t* __restrict__ cellOf,
+                                                   const uint32_t* __restrict__ slot,
+                                                   const uint32_t* __restrict__ cellStart,
+                                                   const uint32_t* __restrict__ ids, uint32_t* __restrict__ order,
+                                                   uint32_t* __restrict__ key) {
+    const int p = blk.x * blockDim.x + threadIdx.x;
     if(p >= n) return;
     const uint32_t pos = cellStart[cellOf[p]] + slot[p];
     order[pos] = (uint32_t)p;
     key[pos] = ids[p];
+}
+__global__ void k_scatter_index(int n, const uint32_t* __restrict__ cellOf, const uint32_t* __restrict__ slot,
+                                const uint32_t* __restrict__ cellStart, const uint32_t* __restrict__ ids,
+                                uint32_t* __restrict__ order, uint32_t* __restrict__ key) {
+    scatter_index_body(own_blk(), n, cellOf, slot, cellStart, ids, order, key);
 }
 
 // Arrival slots come from atomics, so each cell's bucket is put back into ascending
@@ -445,10 +463,11 @@ __device__ __forceinline__ void sort_bucket_regs(uint32_t* __restrict__ order, c
 
 // Buckets of up to 16 particles are sorted in registers; larger ones (particles crowding
 // into a cell, e.g. against a boundary) are listed for k_sort_large.
-__global__ void __launch_bounds__(256, 6) k_sort_buckets(int ncells, const uint32_t* __restrict__ cellStart, uint32_t* __restrict__ order,
-                               const uint32_t* __restrict__ key, uint32_t* __restrict__ count,
-                               uint32_t* __restrict__ largeList, DevState* st) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void sort_buckets_body(Blk blk, int ncells, const uint32_t* __restrict__ cellStart,
+                                                  uint32_t* __restrict__ order, const uint32_t* __restrict__ key,
+                                                  uint32_t* __restrict__ count, uint32_t* __restrict__ largeList,
+                                                  DevState* st) {
+    const int c = blk.x * blockDim.x + threadIdx.x;
     if(c >= ncells) return;
     const uint32_t b = cellStart[c], e = cellStart[c + 1];
     count[c] = 0u;
@@ -458,16 +477,22 @@ __global__ void __launch_bounds__(256, 6) k_sort_buckets(int ncells, const uint3
     if(cnt <= 16) { sort_bucket_regs<16>(order, key, b, cnt); return; }
     largeList[atomicAdd(&st->nlarge, 1u)] = (uint32_t)c;
 }
+__global__ void __launch_bounds__(256, 6) k_sort_buckets(int ncells, const uint32_t* __restrict__ cellStart, uint32_t* __restrict__ order,
+                               const uint32_t* __restrict__ key, uint32_t* __restrict__ count,
+                               uint32_t* __restrict__ largeList, DevState* st) {
+    sort_buckets_body(own_blk(), ncells, cellStart, order, key, count, largeList, st);
+}
 
 // One block per listed bucket: every particle's place is the number of particles of the
 // bucket with a smaller id (ids are distinct), counted against keys staged in shared
 // memory.  tmp[b, e) holds the bucket's unsorted order while it is rewritten.
-__global__ void __launch_bounds__(256) k_sort_large(const uint32_t* __restrict__ cellStart, uint32_t* __restrict__ order,
-                                                    const uint32_t* __restrict__ ids, uint32_t* __restrict__ tmp,
-                                                    const uint32_t* __restrict__ largeList, const DevState* st) {
+__device__ __forceinline__ void sort_large_body(Blk blk, const uint32_t* __restrict__ cellStart,
+                                                uint32_t* __restrict__ order, const uint32_t* __restrict__ ids,
+                                                uint32_t* __restrict__ tmp, const uint32_t* __restrict__ largeList,
+                                                const DevState* st) {
     __shared__ uint32_t sk[1024];
     const unsigned nl = st->nlarge;
-    for(unsigned l = blockIdx.x; l < nl; l += gridDim.x) {
+    for(unsigned l = blk.x; l < nl; l += blk.n) {
         const uint32_t c = largeList[l];
         const uint32_t b = cellStart[c], cnt = cellStart[c + 1] - b;
         for(uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) tmp[b + i] = order[b + i];
@@ -489,6 +514,11 @@ __global__ void __launch_bounds__(256) k_sort_large(const uint32_t* __restrict__
         __syncthreads();
     }
 }
+__global__ void __launch_bounds__(256) k_sort_large(const uint32_t* __restrict__ cellStart, uint32_t* __restrict__ order,
+                                                    const uint32_t* __restrict__ ids, uint32_t* __restrict__ tmp,
+                                                    const uint32_t* __restrict__ largeList, const DevState* st) {
+    sort_large_body(own_blk(), cellStart, order, ids, tmp, largeList, st);
+}
 
 // Apply the permutation to the particle arrays and emit what the gathers read per
 // particle (all from Grid::getGridCoordinate, Grid.h:197):
@@ -500,12 +530,13 @@ __global__ void __launch_bounds__(256) k_sort_large(const uint32_t* __restrict__
 //        clamped the same way and fractions are never -0;
 //        plane 3: the position {x, y, z, 0} for the fluid SDF.
 // One 16-byte load per candidate particle then replaces four scattered 4-byte loads.
-__global__ void k_gather_particles(int n, const uint32_t* __restrict__ order, const float* __restrict__ src6,
-                                   const float* __restrict__ srcPos, float* __restrict__ dst6,
-                                   const uint32_t* __restrict__ idSrc, uint32_t* __restrict__ idDst,
-                                   const float* __restrict__ cSrc, float* __restrict__ cDst, float* __restrict__ g3,
-                                   float4* __restrict__ rec, GridDesc g, size_t stride) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void gather_particles_body(Blk blk, int n, const uint32_t* __restrict__ order,
+                                                      const float* __restrict__ src6, const float* __restrict__ srcPos,
+                                                      float* __restrict__ dst6, const uint32_t* __restrict__ idSrc,
+                                                      uint32_t* __restrict__ idDst, const float* __restrict__ cSrc,
+                                                      float* __restrict__ cDst, float* __restrict__ g3,
+                                                      float4* __restrict__ rec, const GridDesc& g, size_t stride) {
+    const int i = blk.x * blockDim.x + threadIdx.x;
     if(i >= n) return;
     const uint32_t s = order[i];
     float v6[6];
@@ -546,6 +577,13 @@ __global__ void k_gather_particles(int n, const uint32_t* __restrict__ order, co
             rec[D * stride + i] = make_float4(e[0], e[1], e[2], v6[3 + D]);
         }
     }
+}
+__global__ void k_gather_particles(int n, const uint32_t* __restrict__ order, const float* __restrict__ src6,
+                                   const float* __restrict__ srcPos, float* __restrict__ dst6,
+                                   const uint32_t* __restrict__ idSrc, uint32_t* __restrict__ idDst,
+                                   const float* __restrict__ cSrc, float* __restrict__ cDst, float* __restrict__ g3,
+                                   float4* __restrict__ rec, GridDesc g, size_t stride) {
+    gather_particles_body(own_blk(), n, order, src6, srcPos, dst6, idSrc, idDst, cSrc, cDst, g3, rec, g, stride);
 }
 
 // ----------------------------------------------------------------------------------
@@ -785,7 +823,7 @@ __device__ __forceinline__ float ext_tile(const ExtLayer& a, unsigned t, const i
     return m;
 }
 
-__global__ void __launch_bounds__(256, 8) k_extrapolate3(ExtLayer a, DevState* st) {
+__device__ __forceinline__ void extrapolate3_body(Blk blk, const ExtLayer& a, DevState* st) {
     int bb[6];
 #pragma unroll
     for(int q = 0; q < 6; ++q) bb[q] = st->bbox[q];
@@ -800,7 +838,7 @@ __global__ void __launch_bounds__(256, 8) k_extrapolate3(ExtLayer a, DevState* s
             n2 = ext_box<2>(a, bb, lo, hi, ty);
         }
         const unsigned n01 = n0 + n1, total = n01 + n2;
-        for(unsigned t = blockIdx.x; t < total; t += gridDim.x) {
+        for(unsigned t = blk.x; t < total; t += blk.n) {
             float v;
             if(t < n0) v = ext_tile<0>(a, t, bb);
             else if(t < n01) v = ext_tile<1>(a, t - n0, bb);
@@ -819,6 +857,7 @@ __global__ void __launch_bounds__(256, 8) k_extrapolate3(ExtLayer a, DevState* s
         }
     }
 }
+__global__ void __launch_bounds__(256, 8) k_extrapolate3(ExtLayer a, DevState* st) { extrapolate3_body(own_blk(), a, st); }
 
 // max |a| over an array, folded into *maxBits (float bits of a non-negative value order
 // like the unsigned integers)
@@ -836,18 +875,19 @@ __global__ void __launch_bounds__(256) k_maxabs(const float* __restrict__ a, siz
     }
 }
 
-__global__ void k_fill(float* __restrict__ a, size_t n, float v) {
-    for(size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) a[i] = v;
+__device__ __forceinline__ void fill_body(Blk blk, float* __restrict__ a, size_t n, float v) {
+    for(size_t i = (size_t)blk.x * blockDim.x + threadIdx.x; i < n; i += (size_t)blk.n * blockDim.x) a[i] = v;
 }
+__global__ void k_fill(float* __restrict__ a, size_t n, float v) { fill_body(own_blk(), a, n, v); }
 
 // ----------------------------------------------------------------------------------
 // Pressure system
 // ----------------------------------------------------------------------------------
 // Active-cell flags for PIC_Solver::computeSystem's numbering loop (PIC_Solver.cpp:706-712)
-__global__ void k_active_flags(GridDesc g, const float* __restrict__ phi, uint32_t* __restrict__ flag,
-                               DevState* st) {
+__device__ __forceinline__ void active_flags_body(Blk blk, const GridDesc& g, const float* __restrict__ phi,
+                                                  uint32_t* __restrict__ flag, DevState* st) {
     const size_t nc = (size_t)g.G[0] * g.G[1] * g.G[2];
-    const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t c = (size_t)blk.x * blockDim.x + threadIdx.x;
     if(c >= nc) return;
     const float p = phi[c];
     flag[c] = p < 0.f ? 1u : 0u;
@@ -858,12 +898,20 @@ __global__ void k_active_flags(GridDesc g, const float* __restrict__ phi, uint32
         if(i > 0 && i < g.G[0] - 1 && j > 0 && j < g.G[1] - 1 && k > 0 && k < g.G[2] - 1) atomicAdd(&st->zero_phi, 1u);
     }
 }
+__global__ void k_active_flags(GridDesc g, const float* __restrict__ phi, uint32_t* __restrict__ flag,
+                               DevState* st) {
+    active_flags_body(own_blk(), g, phi, flag, st);
+}
 
-__global__ void k_active_rows(size_t nc, const uint32_t* __restrict__ flag, const uint32_t* __restrict__ idx,
-                              uint32_t* __restrict__ rowCell) {
-    const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void active_rows_body(Blk blk, size_t nc, const uint32_t* __restrict__ flag,
+                                                 const uint32_t* __restrict__ idx, uint32_t* __restrict__ rowCell) {
+    const size_t c = (size_t)blk.x * blockDim.x + threadIdx.x;
     if(c >= nc) return;
     if(flag[c]) rowCell[idx[c]] = (uint32_t)c;
+}
+__global__ void k_active_rows(size_t nc, const uint32_t* __restrict__ flag, const uint32_t* __restrict__ idx,
+                              uint32_t* __restrict__ rowCell) {
+    active_rows_body(own_blk(), nc, flag, idx, rowCell);
 }
 
 // One row of PIC_Solver::computeSystem (PIC_Solver.cpp:794-891) for a static scene
@@ -872,13 +920,15 @@ __global__ void k_active_rows(size_t nc, const uint32_t* __restrict__ flag, cons
 // neighbours.  Neighbours are stored in ascending column order (-z,-y,-x,+x,+y,+z), the
 // order FixedSparseMatrix::multiply sums them in (SparseMatrix.cpp:222-235).
 template<bool WEIGHTED>
-__global__ void k_build_rows(GridDesc g, int nrows, const uint32_t* __restrict__ rowCell,
-                             const float* __restrict__ phi, const uint32_t* __restrict__ aidx,
-                             const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w,
-                             const float* __restrict__ wu, const float* __restrict__ wv, const float* __restrict__ ww,
-                             float dt, float* __restrict__ rhs, float* __restrict__ diag, float* __restrict__ invdiag,
-                             int32_t* __restrict__ nbr, float* __restrict__ coef, DevState* st) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void build_rows_body(Blk blk, const GridDesc& g, int nrows, const uint32_t* __restrict__ rowCell,
+                                                const float* __restrict__ phi, const uint32_t* __restrict__ aidx,
+                                                const float* __restrict__ u, const float* __restrict__ v,
+                                                const float* __restrict__ w, const float* __restrict__ wu,
+                                                const float* __restrict__ wv, const float* __restrict__ ww, float dt,
+                                                float* __restrict__ rhs, float* __restrict__ diag,
+                                                float* __restrict__ invdiag, int32_t* __restrict__ nbr,
+                                                float* __restrict__ coef, DevState* st) {
+    const int r = blk.x * blockDim.x + threadIdx.x;
     if(r >= nrows) return;
     const uint32_t c = rowCell[r];
     const int G0 = g.G[0], G1 = g.G[1], G2 = g.G[2];
@@ -945,6 +995,16 @@ __global__ void k_build_rows(GridDesc g, int nrows, const uint32_t* __restrict__
 #pragma unroll
         for(int q = 0; q < 6; ++q) coef[(size_t)q * nrows + r] = co[q];
 }
+template<bool WEIGHTED>
+__global__ void k_build_rows(GridDesc g, int nrows, const uint32_t* __restrict__ rowCell,
+                             const float* __restrict__ phi, const uint32_t* __restrict__ aidx,
+                             const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w,
+                             const float* __restrict__ wu, const float* __restrict__ wv, const float* __restrict__ ww,
+                             float dt, float* __restrict__ rhs, float* __restrict__ diag, float* __restrict__ invdiag,
+                             int32_t* __restrict__ nbr, float* __restrict__ coef, DevState* st) {
+    build_rows_body<WEIGHTED>(own_blk(), g, nrows, rowCell, phi, aidx, u, v, w, wu, wv, ww, dt, rhs, diag, invdiag, nbr,
+                              coef, st);
+}
 
 // ----------------------------------------------------------------------------------
 // Pressure update
@@ -956,13 +1016,11 @@ __global__ void k_build_rows(GridDesc g, int nrows, const uint32_t* __restrict__
 // within one cell of the occupied-cell box, so only faces within 2 of it can be valid:
 // the blocks stride over that box and the host zeroes the output arrays beforehand.
 template<int D>
-__global__ void __launch_bounds__(256) k_update_velocity(GridDesc g, const DevState* __restrict__ st,
-                                                         const float* __restrict__ phi,
-                                                         const uint32_t* __restrict__ aidx,
-                                                         const float* __restrict__ pressure, float dt,
-                                                         const float* __restrict__ velIn, float* __restrict__ velOut,
-                                                         uint8_t* __restrict__ validOut,
-                                                         const float* __restrict__ weight) {
+__device__ __forceinline__ void update_velocity_body(Blk blk, const GridDesc& g, const DevState* __restrict__ st,
+                                                     const float* __restrict__ phi, const uint32_t* __restrict__ aidx,
+                                                     const float* __restrict__ pressure, float dt,
+                                                     const float* __restrict__ velIn, float* __restrict__ velOut,
+                                                     uint8_t* __restrict__ validOut, const float* __restrict__ weight) {
     const int S[3] = {g.G[0] + (D == 0), g.G[1] + (D == 1), g.G[2] + (D == 2)};
     int lo[3], hi[3];
     if(!reach_box(st, 2, S, lo, hi)) return;
@@ -970,7 +1028,7 @@ __global__ void __launch_bounds__(256) k_update_velocity(GridDesc g, const DevSt
     const unsigned ty = (unsigned)(hi[1] - lo[1] + 8) / 8, nt = ty * (unsigned)(hi[2] - lo[2] + 1);
     const int amax = g.G[D];
     const size_t step = D == 0 ? 1 : (D == 1 ? (size_t)g.G[0] : (size_t)g.G[0] * g.G[1]);
-    for(unsigned t = blockIdx.x; t < nt; t += gridDim.x) {
+    for(unsigned t = blk.x; t < nt; t += blk.n) {
         const int j = lo[1] + (int)(t % ty) * 8 + (int)(threadIdx.x >> 5);
         const int k = lo[2] + (int)(t / ty);
         if(j > hi[1]) continue;
@@ -997,6 +1055,16 @@ __global__ void __launch_bounds__(256) k_update_velocity(GridDesc g, const DevSt
             validOut[f] = vv;
         }
     }
+}
+template<int D>
+__global__ void __launch_bounds__(256) k_update_velocity(GridDesc g, const DevState* __restrict__ st,
+                                                         const float* __restrict__ phi,
+                                                         const uint32_t* __restrict__ aidx,
+                                                         const float* __restrict__ pressure, float dt,
+                                                         const float* __restrict__ velIn, float* __restrict__ velOut,
+                                                         uint8_t* __restrict__ validOut,
+                                                         const float* __restrict__ weight) {
+    update_velocity_body<D>(own_blk(), g, st, phi, aidx, pressure, dt, velIn, velOut, validOut, weight);
 }
 
 // ----------------------------------------------------------------------------------
@@ -1299,19 +1367,19 @@ __device__ __forceinline__ float next_substep(unsigned maxvelBits, const NextSte
 // the particle.  The particle keeps its position of this sub-step (what callers read
 // between sub-steps); the moved position goes to `moved`, and the next sub-step's sort
 // gathers from there.  Identical arithmetic to k_g2p followed by k_advect.
-__global__ void __launch_bounds__(256, 4) k_g2p_move(int n, GridDesc g, float* __restrict__ p6, size_t stride,
-                                                  const float* __restrict__ u, const float* __restrict__ v,
-                                                  const float* __restrict__ w, const float* __restrict__ ou,
-                                                  const float* __restrict__ ov, const float* __restrict__ ow,
-                                                  float ratio, NextStep ns, float* __restrict__ moved,
-                                                  uint32_t* __restrict__ cellOf, uint32_t* __restrict__ slot,
-                                                  uint32_t* __restrict__ count, DevState* st,
-                                                  int* __restrict__ bboxPart) {
+__device__ __forceinline__ void g2p_move_body(Blk blk, int n, const GridDesc& g, float* __restrict__ p6, size_t stride,
+                                              const float* __restrict__ u, const float* __restrict__ v,
+                                              const float* __restrict__ w, const float* __restrict__ ou,
+                                              const float* __restrict__ ov, const float* __restrict__ ow, float ratio,
+                                              const NextStep& ns, float* __restrict__ moved,
+                                              uint32_t* __restrict__ cellOf, uint32_t* __restrict__ slot,
+                                              uint32_t* __restrict__ count, DevState* st,
+                                              int* __restrict__ bboxPart) {
     int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {INT_MIN, INT_MIN, INT_MIN};
     const float substep = next_substep(st->maxvel_bits, ns, g.dx);
     const float sub = substep / (float)ns.advSteps;
-    if(blockIdx.x == 0 && threadIdx.x == 0) st->next_dt = substep;
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if(blk.x == 0 && threadIdx.x == 0) st->next_dt = substep;
+    const int p = blk.x * blockDim.x + threadIdx.x;
     uint32_t c = 0xffffffffu;
     if(p < n) {
         float x = p6[p], y = p6[stride + p], z = p6[2 * stride + p];
@@ -1356,7 +1424,17 @@ __global__ void __launch_bounds__(256, 4) k_g2p_move(int n, GridDesc g, float* _
         for(int d = 0; d < 3; ++d) { mn[d] = cc[d]; mx[d] = cc[d]; }
     }
     histogram_slot(c, p, count, slot);
-    bbox_block_partial(bboxPart, mn, mx);
+    bbox_block_partial(bboxPart, blk.x, mn, mx);
+}
+__global__ void __launch_bounds__(256, 4) k_g2p_move(int n, GridDesc g, float* __restrict__ p6, size_t stride,
+                                                  const float* __restrict__ u, const float* __restrict__ v,
+                                                  const float* __restrict__ w, const float* __restrict__ ou,
+                                                  const float* __restrict__ ov, const float* __restrict__ ow,
+                                                  float ratio, NextStep ns, float* __restrict__ moved,
+                                                  uint32_t* __restrict__ cellOf, uint32_t* __restrict__ slot,
+                                                  uint32_t* __restrict__ count, DevState* st,
+                                                  int* __restrict__ bboxPart) {
+    g2p_move_body(own_blk(), n, g, p6, stride, u, v, w, ou, ov, ow, ratio, ns, moved, cellOf, slot, count, st, bboxPart);
 }
 
 // Start of a sub-step whose move already ran: the move's flags and occupied-cell box stay
@@ -1440,11 +1518,173 @@ __global__ void k_add_scalar(float* __restrict__ a, size_t n, float v) {
 
 __global__ void k_step_reset(DevState* st) {
     st->flags = 0u;
+    st->next_flags = 0u;
     st->zero_phi = 0u;
     st->maxvel_bits = 0u;
     for(int d = 0; d < 3; ++d) { st->bbox[d] = INT_MAX; st->bbox[3 + d] = INT_MIN; }
 }
 
+
+// ----------------------------------------------------------------------------------
+// Batched stages: one launch over all scenes of a batch (batch_step.cu).  Each block finds
+// its scene and its block within the scene's share of the launch (seg_blk over the
+// per-scene block prefix P) and runs the lone kernel's body there, on that scene's arrays.
+// ----------------------------------------------------------------------------------
+__global__ void kb_step_reset(const BScene* __restrict__ S, int ns) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if(q >= ns) return;
+    DevState* st = S[q].dst;
+    st->flags = S[q].moved ? st->next_flags : 0u;
+    st->next_flags = 0u;
+    st->zero_phi = 0u;
+    st->maxvel_bits = 0u;
+    st->nlarge = 0u;
+    if(!S[q].moved)
+        for(int d = 0; d < 3; ++d) { st->bbox[d] = INT_MAX; st->bbox[3 + d] = INT_MIN; }
+}
+__global__ void __launch_bounds__(256, 4) kb_advect(const BScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
+    int q;
+    const Blk b = seg_blk(P, ns, q);
+    const BScene& c = S[q];
+    advect_body(b, c.n, c.p6cur, c.p6cur + c.cap, c.p6cur + 2 * c.cap, c.U[0], c.U[1], c.U[2], c.g, c.sub, c.advSteps,
+                c.cellOf, c.slot, c.count, c.dst, c.bboxPart);
+}
+// one block per scene: the occupied-cell box from the advection's per-block boxes
+__global__ void __launch_bounds__(256) kb_bbox_final(const BScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
+    int q;
+    const Blk b = seg_blk(P, ns, q);
+    const BScene& c = S[q];
+    bbox_final_body(b, (c.n + 255) / 256, c.bboxPart, c.dst);
+}
+__global__ void kb_scatter_index(const BScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
+    int q;
+    const Blk b = seg_blk(P, ns, q);
+    const BScene& c = S[q];
+    scatter_index_body(b, c.n, c.cellOf, c.slot, c.cellStart, c.idcur, c.order, c.key);
+}
+__global__ void __launch_bounds__(256, 4) kb_sort_buckets(const BScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
+    int q;
+    const Blk b = seg_blk(P, ns, q);
+    const BScene& c = S[q];
+    sort_buckets_body(b, (int)c.C, c.cellStart, c.order, c.key, c.count, c.slot, c.dst);
+}
+__global__ void __launch_bounds__(256) kb_sort_large(const BScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
+    int q;
+    const Blk b = seg_blk(P, ns, q);
+    const BScene& c = S[q];
+    sort_large_body(b, c.cellStart, c.order, c.idcur, c.cellOf, c.slot, c.dst);
+}
+__global__ void kb_gather_particles(const BScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
+    int q;
+    const Blk b = seg_blk(P, ns, q);
+    const BScene& c = S[q];
+    gather_particles_body(b, c.n, c.order, c.p6cur, c.moved ? c.movedPos : c.p6cur, c.p6nxt, c.idcur, c.idnxt, nullptr,
+                          nullptr, nullptr, c.rec, c.g, c.cap);
+}
+// Before the last layer after P2G: the FLIP backup starts at 0 and v at 0 - g dt (the
+// values every face beyond the layer's region keeps; launch_extrapolate mode 1)
+__global__ void kb_fill_backup(const BScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
+    int q;
+    const Blk b = seg_blk(P, ns, q);
+    const BScene& c = S[q];
+    for(int d = 0; d < 3; ++d) {
+        const size_t nf = (size_t)face_sx(c.g, d) * face_sy(c.g, d) * face_sz(c.g, d);
+        fill_body(b, c.O[d], nf, 0.f);
+        if(d == 1 && c.gdt != 0.f) fill_body(b, c.U[1], nf, 0.f - c.gdt);
+    }
+}
+// Before the pressure update: its output arrays start at 0 / invalid
+__global__ void kb_fill_update(const BScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
+    int q;
+    const Blk b = seg_blk(P, ns, q);
+    const BScene& c = S[q];
+    for(int d = 0; d < 3; ++d) {
+        const size_t nf = (size_t)face_sx(c.g, d) * face_sy(c.g, d) * face_sz(c.g, d);
+        fill_body(b, c.B[d], nf, 0.f);
+        for(size_t i = (size_t)b.x * blockDim.x + threadIdx.x; i < nf; i += (size_t)b.n * blockDim.x) c.VB[d][i] = 0;
+    }
+}
+// Extrapolation layer `layer` of pass 1 (after P2G: U -> B -> U ..., backup and gravity on
+// the last layer) or pass 2 (after the pressure update: B -> U -> B ..., the CFL maximum on
+// the last layer), as launch_extrapolate builds them
+__global__ void __launch_bounds__(256, 4) kb_extrapolate(const BScene* __restrict__ S, const unsigned* __restrict__ P,
+                                                         int ns, int pass, int layer) {
+    int q;
+    const Blk b = seg_blk(P, ns, q);
+    const BScene& c = S[q];
+    ExtLayer a;
+    const bool even = layer % 2 == 0;
+    a.mode = layer == 3 ? pass : 0;
+    for(int d = 0; d < 3; ++d) {
+        a.S[d][0] = face_sx(c.g, d); a.S[d][1] = face_sy(c.g, d); a.S[d][2] = face_sz(c.g, d);
+        float* A = pass == 1 ? c.U[d] : c.B[d];
+        uint8_t* VA_ = pass == 1 ? c.VA[d] : c.VB[d];
+        float* Bv = pass == 1 ? c.B[d] : c.U[d];
+        uint8_t* VB_ = pass == 1 ? c.VB[d] : c.VA[d];
+        a.gin[d] = even ? A : Bv;
+        a.vin[d] = even ? VA_ : VB_;
+        a.gout[d] = even ? Bv : A;
+        a.vout[d] = even ? VB_ : VA_;
+        a.oldOut[d] = pass == 1 ? c.O[d] : nullptr;
+        a.gdt[d] = (a.mode == 1 && d == 1) ? c.gdt : 0.f;
+    }
+    extrapolate3_body(b, a, c.dst);
+}
+__global__ void kb_active_flags(const BScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
+    int q;
+    const Blk b = seg_blk(P, ns, q);
+    const BScene& c = S[q];
+    active_flags_body(b, c.g, c.phi, c.flag, c.dst);
+}
+__global__ void kb_active_rows(const BScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
+    int q;
+    const Blk b = seg_blk(P, ns, q);
+    const BScene& c = S[q];
+    active_rows_body(b, c.C, c.flag, c.aidx, c.rowCell);
+}
+__global__ void kb_build_rows(const BScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
+    int q;
+    const Blk b = seg_blk(P, ns, q);
+    const BScene& c = S[q];
+    build_rows_body<false>(b, c.g, c.nrows, c.rowCell, c.phi, c.aidx, c.U[0], c.U[1], c.U[2], nullptr, nullptr, nullptr,
+                           c.substep, c.rhs, c.diag, c.invd, c.nbr, nullptr, c.dst);
+}
+template<int D>
+__global__ void __launch_bounds__(256) kb_update_velocity(const BScene* __restrict__ S, const unsigned* __restrict__ P,
+                                                          int ns) {
+    int q;
+    const Blk b = seg_blk(P, ns, q);
+    const BScene& c = S[q];
+    update_velocity_body<D>(b, c.g, c.dst, c.phi, c.aidx, c.pressure, c.substep, c.U[D], c.B[D], c.VB[D], nullptr);
+}
+// one thread per scene: the occupied-cell box of the fused move starts empty
+__global__ void kb_bbox_reset(const BScene* __restrict__ S, int ns) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if(q >= ns) return;
+    DevState* st = S[q].dst;
+    for(int d = 0; d < 3; ++d) { st->bbox[d] = INT_MAX; st->bbox[3 + d] = INT_MIN; }
+}
+// the fused grid-to-particle transfer + next move, on the final velocities of this
+// sub-step (the pass-2 extrapolation leaves them in B)
+__global__ void __launch_bounds__(256, 3) kb_g2p_move(const BScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
+    int q;
+    const Blk b = seg_blk(P, ns, q);
+    const BScene& c = S[q];
+    g2p_move_body(b, c.n, c.g, c.p6nxt, c.cap, c.B[0], c.B[1], c.B[2], c.O[0], c.O[1], c.O[2], c.ratio, c.ns, c.movedPos,
+                  c.cellOf, c.slot, c.count, c.dst, c.bboxPart);
+}
+// one thread per scene: its pressure rows (the active-cell numbering's total)
+__global__ void kb_gather_rows(const BScene* __restrict__ S, int ns, unsigned* __restrict__ out) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if(q < ns) out[q] = S[q].aidx[S[q].C];
+}
+__global__ void kb_gather_state(const BScene* __restrict__ S, int ns, DevState* __restrict__ out) {
+    const int q = blockIdx.x;
+    if(q >= ns) return;
+    const unsigned* src = (const unsigned*)S[q].dst;
+    unsigned* dst = (unsigned*)(out + q);
+    for(int i = threadIdx.x; i < (int)(sizeof(DevState) / 4); i += blockDim.x) dst[i] = src[i];
+}
 
 // ----------------------------------------------------------------------------------
 // Launchers
@@ -1655,6 +1895,45 @@ void launch_g2p_move(int n, const GridDesc& g, float* p6, size_t stride, const f
     const unsigned fb = blocks < 148u * 4u * 256u ? (blocks + 255u) / 256u : 148u * 4u;
     { k_bbox_final<<<fb, 256, 0, s>>>((int)blocks, bboxPart, st); bnn_note_launch(); }
 }
+// Batched stages (kernels above): `blocks` = P[ns], the launch's total
+void launch_batch_stage(BatchStage stage, const BScene* S, const unsigned* P, int ns, unsigned blocks, cudaStream_t s,
+                        int pass, int layer) {
+    if(ns == 0) return;
+    const unsigned per = (unsigned)((ns + 127) / 128);
+    switch(stage) {
+    case BatchStage::StepReset: kb_step_reset<<<per, 128, 0, s>>>(S, ns); break;
+    case BatchStage::BboxReset: kb_bbox_reset<<<per, 128, 0, s>>>(S, ns); break;
+    default:
+        if(blocks == 0) return;
+        switch(stage) {
+        case BatchStage::Advect: kb_advect<<<blocks, 256, 0, s>>>(S, P, ns); break;
+        case BatchStage::BboxFinal: kb_bbox_final<<<blocks, 256, 0, s>>>(S, P, ns); break;
+        case BatchStage::ScatterIndex: kb_scatter_index<<<blocks, 256, 0, s>>>(S, P, ns); break;
+        case BatchStage::SortBuckets: kb_sort_buckets<<<blocks, 256, 0, s>>>(S, P, ns); break;
+        case BatchStage::SortLarge: kb_sort_large<<<blocks, 256, 0, s>>>(S, P, ns); break;
+        case BatchStage::Gather: kb_gather_particles<<<blocks, 256, 0, s>>>(S, P, ns); break;
+        case BatchStage::FillBackup: kb_fill_backup<<<blocks, 256, 0, s>>>(S, P, ns); break;
+        case BatchStage::FillUpdate: kb_fill_update<<<blocks, 256, 0, s>>>(S, P, ns); break;
+        case BatchStage::Extrapolate: kb_extrapolate<<<blocks, 256, 0, s>>>(S, P, ns, pass, layer); break;
+        case BatchStage::ActiveFlags: kb_active_flags<<<blocks, 256, 0, s>>>(S, P, ns); break;
+        case BatchStage::ActiveRows: kb_active_rows<<<blocks, 256, 0, s>>>(S, P, ns); break;
+        case BatchStage::BuildRows: kb_build_rows<<<blocks, 256, 0, s>>>(S, P, ns); break;
+        case BatchStage::UpdateU: kb_update_velocity<0><<<blocks, 256, 0, s>>>(S, P, ns); break;
+        case BatchStage::UpdateV: kb_update_velocity<1><<<blocks, 256, 0, s>>>(S, P, ns); break;
+        case BatchStage::UpdateW: kb_update_velocity<2><<<blocks, 256, 0, s>>>(S, P, ns); break;
+        case BatchStage::G2PMove: kb_g2p_move<<<blocks, 256, 0, s>>>(S, P, ns); break;
+        default: return;
+        }
+    }
+    bnn_note_launch();
+}
+void launch_batch_gather_rows(const BScene* S, int ns, unsigned* out, cudaStream_t s) {
+    if(ns) { kb_gather_rows<<<(ns + 127) / 128, 128, 0, s>>>(S, ns, out); bnn_note_launch(); }
+}
+void launch_batch_gather_state(const BScene* S, int ns, DevState* out, cudaStream_t s) {
+    if(ns) { kb_gather_state<<<ns, 128, 0, s>>>(S, ns, out); bnn_note_launch(); }
+}
+
 void launch_cells_from_rows(size_t nc, const float* phi, const uint32_t* aidx, const float* pr, float* out, int active,
                             cudaStream_t s) {
     { k_cells_from_rows<<<nblk(nc), 256, 0, s>>>(nc, phi, aidx, pr, out, active); bnn_note_launch(); }

@@ -39,31 +39,41 @@
 #include "bnn_internal.cuh"
 
 #include <atomic>
+#include <cfloat>
 #include <climits>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
 
 namespace bnn {
 
 namespace {
-#ifndef BNN_TILE_Z
-#define BNN_TILE_Z 6
-#endif
-#ifndef BNN_TILE_Y
-#define BNN_TILE_Y 8
-#endif
-#ifndef BNN_TILE_MIN_BLOCKS
-#define BNN_TILE_MIN_BLOCKS (768 / (32 * (BNN_TILE_Z + 2)))
-#endif
 // A thread per cell of the tile plus its 1-cell halo: a warp is one row of 32 cells along x
-// (30 interior columns and one halo cell each side), kTZ + 2 rows along z.  Every thread
-// forms the partials of exactly one cell, and the interior threads own the faces.
+// (30 interior columns and one halo cell each side), TZ + 2 rows along z.  Every thread
+// forms the partials of exactly one cell, and the interior threads own the faces.  A block
+// walks YC face layers along y.  The shape changes only which block forms which sums, not
+// the sums: every shape gives the same bits, so the tuner (tile_tuner) may pick any.
 constexpr int kHX = 32, kTX = kHX - 2;      // cells per row, interior face columns along x
-constexpr int kTZ = BNN_TILE_Z;              // interior face columns along z
-constexpr int kHZ = kTZ + 2;
-constexpr int kYC = BNN_TILE_Y;              // face layers per block along y (the walk)
-constexpr int kThreads = kHX * kHZ;
-constexpr int kNH = kHX * kHZ;               // cells of one layer whose partials the tile needs
 constexpr int kPartials = 36;              // 18 face slots x (momentum, weight); the SDF has 27
-constexpr size_t kSmemBytes = sizeof(float) * kPartials * kNH;
+template<int TZ, int YC>
+struct Shape {
+    static constexpr int kTZ = TZ;             // interior face columns along z
+    static constexpr int kHZ = TZ + 2;
+    static constexpr int kYC = YC;             // face layers per block along y (the walk)
+    static constexpr int kNH = kHX * kHZ;      // cells of one layer whose partials the tile needs
+    static constexpr int kThreads = kNH;
+    static constexpr int kMinBlocks = 768 / kThreads > 0 ? 768 / kThreads : 1;
+    static constexpr size_t kSmemBytes = sizeof(float) * kPartials * kNH;
+};
+// The shapes the tuner chooses from (index = bnn tile-shape id); 0 is the default
+using S0 = Shape<6, 8>;
+using S1 = Shape<4, 8>;
+using S2 = Shape<6, 4>;
+using S3 = Shape<4, 4>;
+using S4 = Shape<6, 16>;
+using S5 = Shape<8, 8>;
 
 // Weights along one axis of a component's stencil, by face offset from the particle's
 // cell.  The component's own axis: offsets {0, +1}, the base is always the cell.  Other
@@ -105,8 +115,9 @@ __device__ __forceinline__ bool meets_particles(const DevState* st, const int lo
 }
 
 // Partials of component D for halo cell h of cell layer cy into sm (slot-major planes).
-template<int D>
+template<int D, class SH>
 __device__ __forceinline__ void cell_partials(const TileArgs& a, int x0, int z0, int cy, int h, float* __restrict__ sm) {
+    constexpr int kNH = SH::kNH;
     constexpr int NX = D == 0 ? 2 : 3, NY = D == 1 ? 2 : 3, NZ = D == 2 ? 2 : 3;
     constexpr int NS = NX * NY * NZ;
     float S[NS], W[NS];
@@ -148,8 +159,9 @@ __device__ __forceinline__ void cell_partials(const TileArgs& a, int x0, int z0,
 // The face (x0 + tx, z0 + tz) of component D adds the partials of its candidate cells of
 // this layer, cells in ascending (z, x) order, into its accumulators for face layers
 // cy - 1 + j.
-template<int D>
+template<int D, class SH>
 __device__ __forceinline__ void pull_partials(const float* __restrict__ sm, int tx, int tz, float aS[3], float aW[3]) {
+    constexpr int kNH = SH::kNH;
     constexpr int NX = D == 0 ? 2 : 3, NY = D == 1 ? 2 : 3, NZ = D == 2 ? 2 : 3;
 #pragma unroll
     for(int izc = 0; izc < NZ; ++izc) {        // cell z = face z - 1 + izc
@@ -175,8 +187,10 @@ __device__ __forceinline__ void pull_partials(const float* __restrict__ sm, int 
 // Minimum squared distance from the particles of halo cell h (layer cy) to the centres of
 // the 27 cells around it.  exact: a particle outside the grid (sorted into the clamped
 // cell) reaches only the clamped 3x3x3 range of its own cell (PIC_Solver.cpp:633-635).
+template<class SH>
 __device__ __forceinline__ void sdf_partials(const TileArgs& a, int x0, int z0, int cy, int h, bool exact,
                                              float* __restrict__ sm) {
+    constexpr int kNH = SH::kNH;
     const float inf = __int_as_float(0x7f800000);
     float m[27];
 #pragma unroll
@@ -235,7 +249,9 @@ __device__ __forceinline__ void sdf_partials(const TileArgs& a, int x0, int z0, 
 }
 
 // Cell (x0 + tx, cy - 1 + j, z0 + tz) takes the minimum over its 9 neighbours of this layer.
+template<class SH>
 __device__ __forceinline__ void pull_sdf(const float* __restrict__ sm, int tx, int tz, float aM[3]) {
+    constexpr int kNH = SH::kNH;
 #pragma unroll
     for(int izc = 0; izc < 3; ++izc)
 #pragma unroll
@@ -274,15 +290,31 @@ __device__ __forceinline__ void write_phi(const TileArgs& a, int fx, int fy, int
 } // namespace
 
 // P2G: the three face components and the fluid SDF (FLIP); otherwise the fluid SDF alone.
-template<bool P2G>
-__global__ void __launch_bounds__(kThreads, BNN_TILE_MIN_BLOCKS) k_p2g_sdf_tile(TileArgs a) {
+// Which tile a block works on: its own launch's block index, or one given to it (a scene's
+// tile in a batched launch).  Reading blockIdx keeps the indices out of registers.
+struct OwnTile {
+    __device__ __forceinline__ unsigned x() const { return blockIdx.x; }
+    __device__ __forceinline__ unsigned z() const { return blockIdx.y; }
+    __device__ __forceinline__ unsigned y() const { return blockIdx.z; }
+};
+struct GivenTile {
+    unsigned bx, bz, by;
+    __device__ __forceinline__ unsigned x() const { return bx; }
+    __device__ __forceinline__ unsigned z() const { return bz; }
+    __device__ __forceinline__ unsigned y() const { return by; }
+};
+
+// One block of the pass: tile (x, z) of face columns, y-chunk y
+template<bool P2G, class SH, class Tile>
+__device__ __forceinline__ void tile_body(const TileArgs& a, const Tile tile) {
+    constexpr int kTZ = SH::kTZ, kYC = SH::kYC;
     extern __shared__ float sm[];
     const GridDesc& g = a.g;
     const int t = threadIdx.y * kHX + threadIdx.x;        // this thread's halo cell
     const int tx = threadIdx.x - 1, tz = threadIdx.y - 1;  // interior column (faces) or halo
     const bool owner = tx >= 0 && tx < kTX && tz >= 0 && tz < kTZ;
-    const int x0 = blockIdx.x * kTX, z0 = blockIdx.y * kTZ;
-    const int yA = blockIdx.z * kYC, yB = min(yA + kYC, g.G[1] + 1);  // face layers [yA, yB)
+    const int x0 = (int)tile.x() * kTX, z0 = (int)tile.z() * kTZ;
+    const int yA = (int)tile.y() * kYC, yB = min(yA + kYC, g.G[1] + 1);  // face layers [yA, yB)
     const int fx = owner ? x0 + tx : INT_MAX, fz = owner ? z0 + tz : INT_MAX;
     {
         const int lo[3] = {x0 - 1, yA - 1, z0 - 1}, hi[3] = {x0 + kTX, yB, z0 + kTZ};
@@ -309,24 +341,24 @@ __global__ void __launch_bounds__(kThreads, BNN_TILE_MIN_BLOCKS) k_p2g_sdf_tile(
     for(int cy = yA - 1; cy <= yB; ++cy) {
         if(cy >= 0 && cy < g.G[1]) {
             if constexpr(P2G) {
-                cell_partials<0>(a, x0, z0, cy, t, sm);
+                cell_partials<0, SH>(a, x0, z0, cy, t, sm);
                 __syncthreads();
-                if(owner) pull_partials<0>(sm, tx, tz, uS, uW);
+                if(owner) pull_partials<0, SH>(sm, tx, tz, uS, uW);
                 __syncthreads();
                 if(cy < yB) {
-                    cell_partials<1>(a, x0, z0, cy, t, sm);
+                    cell_partials<1, SH>(a, x0, z0, cy, t, sm);
                     __syncthreads();
-                    if(owner) pull_partials<1>(sm, tx, tz, vS, vW);
+                    if(owner) pull_partials<1, SH>(sm, tx, tz, vS, vW);
                     __syncthreads();
                 }
-                cell_partials<2>(a, x0, z0, cy, t, sm);
+                cell_partials<2, SH>(a, x0, z0, cy, t, sm);
                 __syncthreads();
-                if(owner) pull_partials<2>(sm, tx, tz, wS, wW);
+                if(owner) pull_partials<2, SH>(sm, tx, tz, wS, wW);
                 __syncthreads();
             }
-            sdf_partials(a, x0, z0, cy, t, exact, sm);
+            sdf_partials<SH>(a, x0, z0, cy, t, exact, sm);
             __syncthreads();
-            if(owner) pull_sdf(sm, tx, tz, aM);
+            if(owner) pull_sdf<SH>(sm, tx, tz, aM);
             __syncthreads();
         }
         // face / cell layer cy - 1 is complete for u, w and the SDF, face layer cy for v
@@ -349,40 +381,248 @@ __global__ void __launch_bounds__(kThreads, BNN_TILE_MIN_BLOCKS) k_p2g_sdf_tile(
         aM[0] = aM[1]; aM[1] = aM[2]; aM[2] = inf;
     }
 }
+template<bool P2G, class SH>
+__global__ void __launch_bounds__(SH::kThreads, SH::kMinBlocks) k_p2g_sdf_tile(const __grid_constant__ TileArgs a) {
+    tile_body<P2G, SH>(a, OwnTile{});
+}
 
-static dim3 tile_grid(const GridDesc& g) {
-    return dim3((unsigned)((g.G[0] + 1 + kTX - 1) / kTX), (unsigned)((g.G[2] + 1 + kTZ - 1) / kTZ),
-                (unsigned)((g.G[1] + 1 + kYC - 1) / kYC));
+// Batched: the tiles of all scenes of a batch in one launch (P: per-scene tile prefix);
+// a block's flat tile index within its scene maps to (x, z, y) as in tile_grid
+template<class SH>
+__global__ void __launch_bounds__(SH::kThreads, SH::kMinBlocks) kb_p2g_sdf_tile(const TileArgs* __restrict__ A,
+                                                                            const unsigned* __restrict__ P, int ns) {
+    int q;
+    const Blk b = seg_blk(P, ns, q);
+    const TileArgs& a = A[q];
+    const unsigned gx = (unsigned)((a.g.G[0] + 1 + kTX - 1) / kTX);
+    const unsigned gz = (unsigned)((a.g.G[2] + 1 + SH::kTZ - 1) / SH::kTZ);
+    tile_body<true, SH>(a, GivenTile{b.x % gx, (b.x / gx) % gz, b.x / (gx * gz)});
 }
 static_assert(kHX == 32, "a warp is one row of halo cells");
 
-// The dynamic shared memory above the 48 KB default is opted into once per device.
-template<bool P2G>
-static void launch_tile(const TileArgs& a, cudaStream_t s) {
-    static std::atomic<uint64_t> configured{0};  // bit per device ordinal
+template<class SH> static dim3 tile_grid_of(const GridDesc& g) {
+    return dim3((unsigned)((g.G[0] + 1 + kTX - 1) / kTX), (unsigned)((g.G[2] + 1 + SH::kTZ - 1) / SH::kTZ),
+                (unsigned)((g.G[1] + 1 + SH::kYC - 1) / SH::kYC));
+}
+
+// The dynamic shared memory above the 48 KB default is opted into once per kernel and device
+template<class K> static void opt_in_smem(K* kern, size_t bytes, std::atomic<uint64_t>& configured) {
     int dev = 0;
     cudaGetDevice(&dev);
     const uint64_t bit = 1ull << (dev & 63);
     if(!(configured.load(std::memory_order_acquire) & bit)) {
-        cudaFuncSetAttribute(k_p2g_sdf_tile<P2G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
         configured.fetch_or(bit, std::memory_order_acq_rel);
     }
-    k_p2g_sdf_tile<P2G><<<tile_grid(a.g), dim3(kHX, kHZ), kSmemBytes, s>>>(a);
+}
+template<bool P2G, class SH> static void launch_tile_sh(const TileArgs& a, cudaStream_t s) {
+    static std::atomic<uint64_t> configured{0};
+    opt_in_smem(k_p2g_sdf_tile<P2G, SH>, SH::kSmemBytes, configured);
+    k_p2g_sdf_tile<P2G, SH><<<tile_grid_of<SH>(a.g), dim3(kHX, SH::kHZ), SH::kSmemBytes, s>>>(a);
     bnn_note_launch();
+}
+template<class SH>
+static void launch_batch_sh(const TileArgs* A, const unsigned* P, int ns, unsigned tiles, cudaStream_t s) {
+    static std::atomic<uint64_t> configured{0};
+    opt_in_smem(kb_p2g_sdf_tile<SH>, SH::kSmemBytes, configured);
+    kb_p2g_sdf_tile<SH><<<tiles, dim3(kHX, SH::kHZ), SH::kSmemBytes, s>>>(A, P, ns);
+    bnn_note_launch();
+}
+
+// ---- shapes and their tuner -----------------------------------------------------------
+// The tuner times every shape on the live pass the first time it meets a kind of launch
+// (a resolution bucket of a lone scene: ceil((G + 1) / 32) cells per axis; for a batch, the
+// scene count and total cells in powers of two) and keeps the fastest for it.  The pass is
+// a pure function of the sorted particles (it writes every face and cell of its outputs and
+// reads none of them), so the timing runs leave exactly what one run leaves, and since all
+// shapes give the same bits the choice never changes a result.
+constexpr int kShapeDims[kTileShapes][2] = {{S0::kTZ, S0::kYC}, {S1::kTZ, S1::kYC}, {S2::kTZ, S2::kYC},
+                                            {S3::kTZ, S3::kYC}, {S4::kTZ, S4::kYC}, {S5::kTZ, S5::kYC}};
+
+static dim3 tile_grid(const GridDesc& g, int shape) {
+    switch(shape) {
+    case 1: return tile_grid_of<S1>(g);
+    case 2: return tile_grid_of<S2>(g);
+    case 3: return tile_grid_of<S3>(g);
+    case 4: return tile_grid_of<S4>(g);
+    case 5: return tile_grid_of<S5>(g);
+    default: return tile_grid_of<S0>(g);
+    }
+}
+static void launch_p2g_shape(int shape, const TileArgs& a, cudaStream_t s) {
+    switch(shape) {
+    case 1: launch_tile_sh<true, S1>(a, s); break;
+    case 2: launch_tile_sh<true, S2>(a, s); break;
+    case 3: launch_tile_sh<true, S3>(a, s); break;
+    case 4: launch_tile_sh<true, S4>(a, s); break;
+    case 5: launch_tile_sh<true, S5>(a, s); break;
+    default: launch_tile_sh<true, S0>(a, s); break;
+    }
+}
+static void launch_batch_shape(int shape, const TileArgs* A, const unsigned* P, int ns, unsigned tiles, cudaStream_t s) {
+    if(tiles == 0) return;
+    switch(shape) {
+    case 1: launch_batch_sh<S1>(A, P, ns, tiles, s); break;
+    case 2: launch_batch_sh<S2>(A, P, ns, tiles, s); break;
+    case 3: launch_batch_sh<S3>(A, P, ns, tiles, s); break;
+    case 4: launch_batch_sh<S4>(A, P, ns, tiles, s); break;
+    case 5: launch_batch_sh<S5>(A, P, ns, tiles, s); break;
+    default: launch_batch_sh<S0>(A, P, ns, tiles, s); break;
+    }
+}
+
+namespace {
+struct TuneEntry {
+    int shape = 0;
+    float us[kTileShapes] = {};
+};
+struct Tuner {
+    std::mutex mu;
+    std::map<uint64_t, TuneEntry> table;
+    int forced = -1;  // bnn_set_tile_shape
+};
+Tuner& tuner() {
+    static Tuner t;
+    return t;
+}
+inline uint64_t log2_bucket(uint64_t x) {
+    uint64_t b = 0;
+    while((1ull << b) < x && b < 63) ++b;
+    return b;
+}
+uint64_t scene_key(const GridDesc& g) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    uint64_t k = (uint64_t)(dev & 0xff) << 56;
+    for(int a = 0; a < 3; ++a) k |= (uint64_t)(((g.G[a] + 1 + 31) / 32) & 0xffff) << (16 * a);
+    return k;
+}
+// The shape for key, or -1 when it still has to be tuned
+int lookup(uint64_t key) {
+    Tuner& t = tuner();
+    std::lock_guard<std::mutex> lk(t.mu);
+    if(t.forced >= 0) return t.forced;
+    auto it = t.table.find(key);
+    return it == t.table.end() ? -1 : it->second.shape;
+}
+// Times launch(shape) for every shape (best of two rounds) on stream s and records the
+// fastest under key; the stream is synchronised.
+template<class F> int tune(uint64_t key, cudaStream_t s, F launch) {
+    constexpr int kRounds = 2;
+    cudaEvent_t ev[kRounds][kTileShapes + 1];
+    for(auto& r : ev)
+        for(auto& e : r) cudaEventCreate(&e);
+    for(int r = 0; r < kRounds; ++r) {
+        cudaEventRecord(ev[r][0], s);
+        for(int v = 0; v < kTileShapes; ++v) {
+            launch(v);
+            cudaEventRecord(ev[r][v + 1], s);
+        }
+    }
+    cudaEventSynchronize(ev[kRounds - 1][kTileShapes]);
+    TuneEntry e;
+    for(int v = 0; v < kTileShapes; ++v) {
+        float best = FLT_MAX;
+        for(int r = 0; r < kRounds; ++r) {
+            float ms = FLT_MAX;
+            if(cudaEventElapsedTime(&ms, ev[r][v], ev[r][v + 1]) != cudaSuccess) ms = FLT_MAX;
+            best = ms < best ? ms : best;
+        }
+        e.us[v] = best * 1000.f;
+        if(e.us[v] < e.us[e.shape]) e.shape = v;
+    }
+    for(auto& r : ev)
+        for(auto& ee : r) cudaEventDestroy(ee);
+    Tuner& t = tuner();
+    std::lock_guard<std::mutex> lk(t.mu);
+    t.table[key] = e;
+    return e.shape;
+}
+} // namespace
+
+int tile_shape_set(int shape) {
+    if(shape < -1 || shape >= kTileShapes) return BNN_ERR_INVALID_ARGUMENT;
+    Tuner& t = tuner();
+    std::lock_guard<std::mutex> lk(t.mu);
+    t.forced = shape;
+    return BNN_OK;
+}
+void tile_shape_dims(int shape, int* tz, int* yc) {
+    *tz = kShapeDims[shape][0];
+    *yc = kShapeDims[shape][1];
+}
+// One JSON object per tuned launch kind, one per line
+std::string tile_tuning_report() {
+    Tuner& t = tuner();
+    std::lock_guard<std::mutex> lk(t.mu);
+    std::string out;
+    char buf[512];
+    for(const auto& kv : t.table) {
+        const uint64_t k = kv.first;
+        const bool batch = (k >> 48) & 1;
+        int n = 0;
+        if(batch)
+            n = std::snprintf(buf, sizeof buf, "{\"kind\": \"batch\", \"scenes_le\": %llu, \"cells_le\": %llu",
+                              1ull << ((k >> 24) & 0x3f), 1ull << (k & 0x3f));
+        else
+            n = std::snprintf(buf, sizeof buf, "{\"kind\": \"scene\", \"cells_per_axis_le\": [%d, %d, %d]",
+                              (int)(k & 0xffff) * 32 - 1, (int)((k >> 16) & 0xffff) * 32 - 1,
+                              (int)((k >> 32) & 0xffff) * 32 - 1);
+        out.append(buf, (size_t)n);
+        const int sh = kv.second.shape;
+        n = std::snprintf(buf, sizeof buf, ", \"shape\": %d, \"tz\": %d, \"yc\": %d, \"us\": [", sh, kShapeDims[sh][0],
+                          kShapeDims[sh][1]);
+        out.append(buf, (size_t)n);
+        for(int v = 0; v < kTileShapes; ++v) {
+            n = std::snprintf(buf, sizeof buf, "%s%.1f", v ? ", " : "", kv.second.us[v]);
+            out.append(buf, (size_t)n);
+        }
+        out += "]}\n";
+    }
+    return out;
 }
 
 // FLIP P2G of the three components together with the fluid SDF
 void launch_p2g_sdf(const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float4* rec,
                     size_t stride, float* const* out, uint8_t* const* valid, float* phi, cudaStream_t s) {
-    TileArgs a{g, st, cellStart, rec, stride, {out[0], out[1], out[2]}, {valid[0], valid[1], valid[2]}, phi};
-    launch_tile<true>(a, s);
+    const TileArgs a{g, st, cellStart, rec, stride, {out[0], out[1], out[2]}, {valid[0], valid[1], valid[2]}, phi};
+    const uint64_t key = scene_key(g);
+    int shape = lookup(key);
+    if(shape < 0) shape = tune(key, s, [&](int v) { launch_p2g_shape(v, a, s); });
+    else launch_p2g_shape(shape, a, s);
 }
 
-// The fluid SDF alone (APIC / AFLIP / PIC)
+// Tiles of one scene's P2G + SDF pass in a shape (the batched launch's share of the scene)
+unsigned p2g_sdf_tiles(const GridDesc& g, int shape) {
+    const dim3 d = tile_grid(g, shape);
+    return d.x * d.y * d.z;
+}
+// Size of the per-scene argument record the batched launch reads, and its host-side fill
+size_t p2g_tile_args_bytes() { return sizeof(TileArgs); }
+void p2g_tile_args(void* out, const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float4* rec,
+                   size_t stride, float* const U[3], uint8_t* const valid[3], float* phi) {
+    TileArgs a{g, st, cellStart, rec, stride, {U[0], U[1], U[2]}, {valid[0], valid[1], valid[2]}, phi};
+    memcpy(out, &a, sizeof a);
+}
+// The batch's P2G + SDF pass: P[shape] is the tile prefix of the scenes in that shape,
+// tiles[shape] its total (host copy); tuned per batch kind like a lone scene's pass
+void launch_p2g_sdf_batch(const void* args, const unsigned* const* P, const unsigned* tiles, int ns, uint64_t cells,
+                          cudaStream_t s) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const uint64_t key = ((uint64_t)(dev & 0xff) << 56) | (1ull << 48) | (log2_bucket((uint64_t)ns) << 24) |
+                         log2_bucket(cells);
+    const TileArgs* A = (const TileArgs*)args;
+    int shape = lookup(key);
+    if(shape < 0) shape = tune(key, s, [&](int v) { launch_batch_shape(v, A, P[v], ns, tiles[v], s); });
+    else launch_batch_shape(shape, A, P[shape], ns, tiles[shape], s);
+}
+
+// The fluid SDF alone (APIC / AFLIP / PIC), in the default shape
 void launch_fluid_sdf_tile(const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float4* rec,
                            size_t stride, float* phi, cudaStream_t s) {
-    TileArgs a{g, st, cellStart, rec, stride, {nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}, phi};
-    launch_tile<false>(a, s);
+    const TileArgs a{g, st, cellStart, rec, stride, {nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}, phi};
+    launch_tile_sh<false, S0>(a, s);
 }
 
 } // namespace bnn

@@ -25,6 +25,7 @@
 
 #include <condition_variable>
 #include <cstdio>
+#include <cstring>
 #include <mutex>
 #include <vector>
 
@@ -962,13 +963,333 @@ __global__ void __launch_bounds__(kLanes, cg1_min_blocks<VT>()) k_pcg_cg1(Cg1Arg
     }
 }
 
+// ---------------------------------------------------------------------------------
+// Batched persistent PCG: the Jacobi systems of many scenes (FP32 vectors, grid rows in
+// packed records, face weights 1) in one cooperative launch.  A scene's rows are cut into
+// the same 2048-row chunks as in a lone solve, and the chunks of all scenes are numbered
+// one after another; a block owns a contiguous range of them, so it meets only a few
+// scenes.  After each grid barrier a block reduces the partials of each of its scenes in
+// the canonical order over that scene's chunks alone, so every scene gets exactly the
+// scalars, iterates and iteration count of a lone k_pcg_persistent solve.  Scenes that have
+// finished skip their chunks; the loop ends, for all blocks at the same barrier, when a
+// counter of unfinished scenes (decremented by the block owning a scene's first chunk)
+// reads 0 right after the first barrier of an iteration -- no scene can finish between
+// the last decrement before that barrier and the read.
+// ---------------------------------------------------------------------------------
+constexpr int kBatchSlots = 64;  // scenes a block's chunk range may touch
+struct BatchPcgScene {
+    int n;                     // rows
+    const float* rhsF;
+    const float* invd;
+    const int4* rec;
+    float negoff;              // -(1 * dt)
+    float tolFactor;
+    unsigned maxIter;
+    float *x, *r, *z, *s0, *s1, *q;
+    double *part0, *part1, *part2;
+    float* partMax;
+    DevState* dst;             // iterations, success and residual go here
+};
+struct BatchPcgArgs {
+    const BatchPcgScene* sc;
+    const unsigned* cp;        // chunk prefix over scenes (ns + 1)
+    int ns;
+    unsigned total;            // chunks of all scenes
+    unsigned perBlock;         // chunks per block
+    GridSync* gs;
+    unsigned* remaining;       // unfinished scenes
+    unsigned* flags;           // BNN_FLAG_TIMEOUT
+};
+
+__global__ void __launch_bounds__(kLanes, pcg_min_blocks<float, false>()) k_pcg_batch(BatchPcgArgs a) {
+    constexpr int kRowGroup = pcg_row_group<float, false>();
+    __shared__ double smd[kLanes];
+    __shared__ float smv[kLanes];
+    __shared__ double sRho[kBatchSlots];
+    __shared__ float sTol[kBatchSlots], sResid[kBatchSlots], sAlpha[kBatchSlots], sBeta[kBatchSlots];
+    __shared__ unsigned sIter[kBatchSlots];
+    __shared__ int sState[kBatchSlots];  // 0 iterating, 1 finished, 2 no solve
+    const unsigned nb = gridDim.x;
+    unsigned sense = 0;
+    const int lane = threadIdx.x & 31;
+    const unsigned c0 = min(blockIdx.x * a.perBlock, a.total), c1 = min(c0 + a.perBlock, a.total);
+    const int sFirst = c0 < c1 ? seg_of(a.cp, a.ns, c0) : 0;
+    const int nslots = c0 < c1 ? seg_of(a.cp, a.ns, c1 - 1) - sFirst + 1 : 0;
+
+    // A scene's result, by the block that owns its first chunk.  The counter of unfinished
+    // scenes is read right after the first barrier of an iteration, so it may only change
+    // between the second barrier and the next first one: a scene finishing between the two
+    // (deferred) is counted off after the second.
+    auto finish = [&](int j, unsigned success, bool deferred) {
+        const int s = sFirst + j;
+        sState[j] = deferred ? 3 : 1;
+        if(threadIdx.x == 0 && __ldg(a.cp + s) >= c0) {
+            DevState* d = a.sc[s].dst;
+            d->iter = sIter[j];
+            d->success = success;
+            d->done = 1;
+            d->resid = sResid[j];
+            d->resid64 = sResid[j];
+            if(!deferred) atomicSub(a.remaining, 1u);
+        }
+    };
+
+    // ---- init: r = rhs, x = 0, z = D^-1 r; partial z.r and max|r|
+    for(unsigned c = c0; c < c1; ++c) {
+        const int s = seg_of(a.cp, a.ns, c);
+        const BatchPcgScene& S = a.sc[s];
+        const int n = S.n;
+        const unsigned lc = c - __ldg(a.cp + s);
+        double acc = 0.0;
+        float m = 0.f;
+        const size_t base = (size_t)lc * kChunk + threadIdx.x;
+#pragma unroll
+        for(int j = 0; j < kPerLane; ++j) {
+            const size_t e = base + (size_t)j * kLanes;
+            if(e < (size_t)n) {
+                const float rv = S.rhsF[e];
+                S.r[e] = rv;
+                S.x[e] = 0.f;
+                const float ab = vabs(rv);
+                m = m > ab ? m : ab;
+                const float zv = __ldg(S.invd + e) * rv;
+                S.z[e] = zv;
+                acc = acc + (double)zv * (double)rv;
+            }
+        }
+        double bs;
+        float bm;
+        block_sum_max_256<float>(acc, m, smd, smv, bs, bm, true);
+        if(threadIdx.x == 0) { S.part0[lc] = bs; S.partMax[lc] = bm; }
+    }
+    if(!grid_barrier(a.gs, nb, sense, a.flags, solve_barrier_limit())) return;
+    for(int j = 0; j < nslots; ++j) {
+        const int s = sFirst + j;
+        const BatchPcgScene& S = a.sc[s];
+        const int nch = (int)(__ldg(a.cp + s + 1) - __ldg(a.cp + s));
+        if(threadIdx.x == 0) { sIter[j] = 0; sState[j] = nch > 0 ? 0 : 2; sBeta[j] = 0.f; }
+        __syncthreads();
+        if(nch == 0) continue;
+        double rho;
+        float resid;
+        reduce_partials_bcast<float>(S.part0, S.partMax, nch, smd, smv, rho, resid);
+        if(threadIdx.x == 0) { sRho[j] = rho; sResid[j] = resid; }
+        const float tolFactor = fmaxf(S.tolFactor, 1e-30f);
+        __syncthreads();
+        if(resid < FLT_MIN) {
+            finish(j, 1u, false);
+        } else {
+            if(threadIdx.x == 0) sTol[j] = tolFactor * resid;
+            if(rho < (double)FLT_MIN || isnan(rho) || S.maxIter == 0) finish(j, 0u, false);
+        }
+        __syncthreads();
+    }
+
+    bool first = true;
+    int parity = 0;  // s0 new / s1 old on even iterations, as the lone solve's swap
+    for(;;) {
+        // ---- phase A: s = z + beta s_old, q = A s, partial s.q
+        for(unsigned c = c0; c < c1; ++c) {
+            const int s = seg_of(a.cp, a.ns, c);
+            const int jslot = s - sFirst;
+            if(sState[jslot] != 0) continue;
+            const BatchPcgScene& S = a.sc[s];
+            const int n = S.n;
+            const unsigned lc = c - __ldg(a.cp + s);
+            const float beta = sBeta[jslot];
+            const float negoff = S.negoff;
+            const float* __restrict__ zR = S.z;
+            const float* __restrict__ sOld = parity ? S.s0 : S.s1;
+            float* __restrict__ sNew = parity ? S.s1 : S.s0;
+            const size_t base = (size_t)lc * kChunk + threadIdx.x;
+            float sOut[kPerLane], qOut[kPerLane];
+            int4 recAll[kPerLane];
+#pragma unroll
+            for(int j = 0; j < kPerLane; ++j) {
+                const size_t e = base + (size_t)j * kLanes;
+                recAll[j] = __ldg(S.rec + (e < (size_t)n ? e : 0));
+            }
+#pragma unroll
+            for(int g0 = 0; g0 < kPerLane; g0 += kRowGroup) {
+                int32_t id[kRowGroup][7];
+                bool has[kRowGroup][7];
+                float dg[kRowGroup];
+#pragma unroll
+                for(int u = 0; u < kRowGroup; ++u) {
+                    const size_t e = base + (size_t)(g0 + u) * kLanes;
+                    const size_t ee = e < (size_t)n ? e : 0;
+                    const int4 rr = recAll[g0 + u];
+                    const int dyM = rr.x & 0xffff, dyP = (int)((unsigned)rr.x >> 16);
+                    const int dzM = rr.y & 0x7fffffff, dzP = rr.z & 0x7fffffff;
+                    const int32_t r0 = (int32_t)ee;
+                    has[u][0] = dzM != 0; id[u][0] = r0 - dzM;
+                    has[u][1] = dyM != 0; id[u][1] = r0 - dyM;
+                    has[u][2] = rr.y < 0; id[u][2] = (lane == 0 && rr.y < 0) ? r0 - 1 : r0;
+                    has[u][3] = true; id[u][3] = r0;
+                    has[u][4] = rr.z < 0; id[u][4] = (lane == 31 && rr.z < 0) ? r0 + 1 : r0;
+                    has[u][5] = dyP != 0; id[u][5] = r0 + dyP;
+                    has[u][6] = dzP != 0; id[u][6] = r0 + dzP;
+                    dg[u] = __int_as_float(rr.w);
+                }
+                float zv[kRowGroup][7], sv[kRowGroup][7];
+#pragma unroll
+                for(int u = 0; u < kRowGroup; ++u)
+#pragma unroll
+                    for(int q = 0; q < 7; ++q) {
+                        const bool load = (q != 2 && q != 4) || (q == 2 && lane == 0) || (q == 4 && lane == 31);
+                        zv[u][q] = load ? __ldcg(zR + id[u][q]) : 0.f;
+                        sv[u][q] = (first || !load) ? 0.f : __ldcg(sOld + id[u][q]);
+                    }
+#pragma unroll
+                for(int u = 0; u < kRowGroup; ++u) {
+                    float s7[7];
+#pragma unroll
+                    for(int q = 0; q < 7; ++q) s7[q] = first ? zv[u][q] : zv[u][q] + beta * sv[u][q];
+                    const float up = __shfl_up_sync(0xffffffffu, s7[3], 1);
+                    const float dn = __shfl_down_sync(0xffffffffu, s7[3], 1);
+                    if(lane != 0) s7[2] = up;
+                    if(lane != 31) s7[4] = dn;
+                    float t = 0.f;
+#pragma unroll
+                    for(int q = 0; q < 3; ++q) if(has[u][q]) t += negoff * s7[q];
+                    if(dg[u] != 0.f) t += dg[u] * s7[3];
+#pragma unroll
+                    for(int q = 4; q < 7; ++q) if(has[u][q]) t += negoff * s7[q];
+                    sOut[g0 + u] = s7[3];
+                    qOut[g0 + u] = t;
+                }
+            }
+            double acc = 0.0;
+#pragma unroll
+            for(int j = 0; j < kPerLane; ++j) {
+                const size_t e = base + (size_t)j * kLanes;
+                if(e < (size_t)n) {
+                    sNew[e] = sOut[j];
+                    S.q[e] = qOut[j];
+                    acc = acc + (double)sOut[j] * (double)qOut[j];
+                }
+            }
+            double bs;
+            float unused;
+            block_sum_max_256<float>(acc, 0.f, smd, smv, bs, unused, false);
+            if(threadIdx.x == 0) S.part1[lc] = bs;
+        }
+        if(!grid_barrier(a.gs, nb, sense, a.flags, solve_barrier_limit())) return;
+        if(ld_acquire_u32(a.remaining) == 0u) break;
+        // alpha of every scene this block works on
+        for(int j = 0; j < nslots; ++j) {
+            if(sState[j] != 0) continue;
+            const int s = sFirst + j;
+            const BatchPcgScene& S = a.sc[s];
+            const int nch = (int)(__ldg(a.cp + s + 1) - __ldg(a.cp + s));
+            double tmp;
+            float unused2;
+            reduce_partials_bcast<float>(S.part1, (const float*)nullptr, nch, smd, smv, tmp, unused2);
+            if(tmp < (double)FLT_MIN) {
+                if(threadIdx.x == 0) ++sIter[j];
+                __syncthreads();
+                finish(j, 1u, true);
+            } else if(threadIdx.x == 0) {
+                sAlpha[j] = (float)(sRho[j] / tmp);
+            }
+            __syncthreads();
+        }
+        // ---- phase B: x += alpha s, r -= alpha q, max|r|, z = D^-1 r, partial z.r
+        for(unsigned c = c0; c < c1; ++c) {
+            const int s = seg_of(a.cp, a.ns, c);
+            const int jslot = s - sFirst;
+            if(sState[jslot] != 0) continue;
+            const BatchPcgScene& S = a.sc[s];
+            const int n = S.n;
+            const unsigned lc = c - __ldg(a.cp + s);
+            const float alpha = sAlpha[jslot];
+            const float* __restrict__ sNew = parity ? S.s1 : S.s0;
+            const size_t base = (size_t)lc * kChunk + threadIdx.x;
+            float xs[kPerLane], ss[kPerLane], rs[kPerLane], qs[kPerLane], is[kPerLane];
+#pragma unroll
+            for(int j = 0; j < kPerLane; ++j) {
+                const size_t e = base + (size_t)j * kLanes;
+                const size_t ee = e < (size_t)n ? e : 0;
+                xs[j] = __ldcg(S.x + ee);
+                ss[j] = __ldcg(sNew + ee);
+                rs[j] = __ldcg(S.r + ee);
+                qs[j] = __ldcg(S.q + ee);
+                is[j] = __ldg(S.invd + ee);
+            }
+            double acc = 0.0;
+            float m = 0.f;
+#pragma unroll
+            for(int j = 0; j < kPerLane; ++j) {
+                const size_t e = base + (size_t)j * kLanes;
+                if(e < (size_t)n) {
+                    S.x[e] = xs[j] + alpha * ss[j];
+                    const float rv = rs[j] + (-alpha) * qs[j];
+                    S.r[e] = rv;
+                    const float ab = vabs(rv);
+                    m = m > ab ? m : ab;
+                    const float zv = is[j] * rv;
+                    S.z[e] = zv;
+                    acc = acc + (double)zv * (double)rv;
+                }
+            }
+            double bs;
+            float bm;
+            block_sum_max_256<float>(acc, m, smd, smv, bs, bm, true);
+            if(threadIdx.x == 0) { S.part2[lc] = bs; S.partMax[lc] = bm; }
+        }
+        if(!grid_barrier(a.gs, nb, sense, a.flags, solve_barrier_limit())) return;
+        for(int j = 0; j < nslots; ++j) {
+            if(sState[j] == 3) {
+                if(threadIdx.x == 0 && __ldg(a.cp + sFirst + j) >= c0) atomicSub(a.remaining, 1u);
+                __syncthreads();
+                if(threadIdx.x == 0) sState[j] = 1;
+                __syncthreads();
+            }
+            if(sState[j] != 0) continue;
+            const int s = sFirst + j;
+            const BatchPcgScene& S = a.sc[s];
+            const int nch = (int)(__ldg(a.cp + s + 1) - __ldg(a.cp + s));
+            double rhoNew;
+            float resid;
+            reduce_partials_bcast<float>(S.part2, S.partMax, nch, smd, smv, rhoNew, resid);
+            if(threadIdx.x == 0) { ++sIter[j]; sResid[j] = resid; }
+            __syncthreads();
+            if(resid < sTol[j]) {
+                finish(j, 1u, false);
+            } else {
+                if(threadIdx.x == 0) {
+                    sBeta[j] = (float)(rhoNew / sRho[j]);
+                    sRho[j] = rhoNew;
+                }
+                __syncthreads();
+                if(sIter[j] >= S.maxIter) {
+                    if(threadIdx.x == 0 && __ldg(a.cp + s) >= c0) atomicOr(&S.dst->flags, BNN_FLAG_PCG_MAXITER);
+                    finish(j, 0u, false);
+                }
+            }
+            __syncthreads();
+        }
+        parity ^= 1;
+        first = false;
+    }
+}
+
 // ---- iterative refinement helpers -------------------------------------------------
+// Last-block-done over a block's share `blk` of a launch (the batched launches give every
+// scene its own share, so the count to reach is the share's, not gridDim.x)
+__device__ __forceinline__ bool last_block_of(unsigned* counter, unsigned nblocks) {
+    __shared__ bool amLast;
+    __threadfence();
+    __syncthreads();
+    if(threadIdx.x == 0) amLast = atomicAdd(counter, 1u) == nblocks - 1;
+    __syncthreads();
+    return amLast;
+}
 // x64 = 0, r64 = b, outer_bmax = outer_res = max|b|
-__global__ void __launch_bounds__(kLanes) k_ir_init(int n, const float* __restrict__ b, double* __restrict__ x64,
-                                                    double* __restrict__ r64, double* __restrict__ partMax,
-                                                    DevState* st) {
+__device__ __forceinline__ void ir_init_body(Blk blk, int n, const float* __restrict__ b, double* __restrict__ x64,
+                                             double* __restrict__ r64, double* __restrict__ partMax, DevState* st) {
     __shared__ double sm[kLanes];
-    const size_t base = (size_t)blockIdx.x * kChunk + threadIdx.x;
+    const size_t base = (size_t)blk.x * kChunk + threadIdx.x;
     double m = 0.0;
     for(int j = 0; j < kPerLane; ++j) {
         const size_t e = base + (size_t)j * kLanes;
@@ -981,11 +1302,16 @@ __global__ void __launch_bounds__(kLanes) k_ir_init(int n, const float* __restri
         }
     }
     const double bm = block_max_t(m, sm);
-    if(threadIdx.x == 0) partMax[blockIdx.x] = bm;
-    if(last_block(&st->counter3)) {
-        const double mx = reduce_max_t(partMax, gridDim.x, sm);
+    if(threadIdx.x == 0) partMax[blk.x] = bm;
+    if(last_block_of(&st->counter3, blk.n)) {
+        const double mx = reduce_max_t(partMax, (int)blk.n, sm);
         if(threadIdx.x == 0) { st->counter3 = 0; st->outer_bmax = mx; st->outer_res = mx; }
     }
+}
+__global__ void __launch_bounds__(kLanes) k_ir_init(int n, const float* __restrict__ b, double* __restrict__ x64,
+                                                    double* __restrict__ r64, double* __restrict__ partMax,
+                                                    DevState* st) {
+    ir_init_body(own_blk(), n, b, x64, r64, partMax, st);
 }
 // r32 = (float) r64
 __global__ void k_ir_to_f32(int n, const double* __restrict__ r64, float* __restrict__ r32) {
@@ -997,14 +1323,13 @@ __global__ void k_ir_accumulate(int n, double* __restrict__ x64, const float* __
     if(e < (size_t)n) x64[e] = x64[e] + (double)d[e];
 }
 // r64 = b - A x64 in FP64, outer_res = max|r64|
-__global__ void __launch_bounds__(kLanes) k_ir_residual(int n, const float* __restrict__ b,
-                                                        const double* __restrict__ x64, double* __restrict__ r64,
-                                                        const float* __restrict__ diag,
-                                                        const int32_t* __restrict__ nbr,
-                                                        const float* __restrict__ coef, double negoff,
-                                                        double* __restrict__ partMax, DevState* st) {
+__device__ __forceinline__ void ir_residual_body(Blk blk, int n, const float* __restrict__ b,
+                                                 const double* __restrict__ x64, double* __restrict__ r64,
+                                                 const float* __restrict__ diag, const int32_t* __restrict__ nbr,
+                                                 const float* __restrict__ coef, double negoff,
+                                                 double* __restrict__ partMax, DevState* st) {
     __shared__ double sm[kLanes];
-    const size_t base = (size_t)blockIdx.x * kChunk + threadIdx.x;
+    const size_t base = (size_t)blk.x * kChunk + threadIdx.x;
     double m = 0.0;
     for(int j = 0; j < kPerLane; ++j) {
         const size_t e = base + (size_t)j * kLanes;
@@ -1029,11 +1354,19 @@ __global__ void __launch_bounds__(kLanes) k_ir_residual(int n, const float* __re
         }
     }
     const double bm = block_max_t(m, sm);
-    if(threadIdx.x == 0) partMax[blockIdx.x] = bm;
-    if(last_block(&st->counter3)) {
-        const double mx = reduce_max_t(partMax, gridDim.x, sm);
+    if(threadIdx.x == 0) partMax[blk.x] = bm;
+    if(last_block_of(&st->counter3, blk.n)) {
+        const double mx = reduce_max_t(partMax, (int)blk.n, sm);
         if(threadIdx.x == 0) { st->counter3 = 0; st->outer_res = mx; }
     }
+}
+__global__ void __launch_bounds__(kLanes) k_ir_residual(int n, const float* __restrict__ b,
+                                                        const double* __restrict__ x64, double* __restrict__ r64,
+                                                        const float* __restrict__ diag,
+                                                        const int32_t* __restrict__ nbr,
+                                                        const float* __restrict__ coef, double negoff,
+                                                        double* __restrict__ partMax, DevState* st) {
+    ir_residual_body(own_blk(), n, b, x64, r64, diag, nbr, coef, negoff, partMax, st);
 }
 __global__ void k_inv_diag64(int n, const float* __restrict__ diag, double* __restrict__ inv) {
     const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1318,6 +1651,320 @@ int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const floa
     out.success = ok ? 1 : 0;
     { k_d64_to_f32<<<nb, 256, 0, s>>>(n, w.x64, pressure); bnn_note_launch(); }
     if(x64out) BNN_CUDA_CHECK(cudaMemcpyAsync(x64out, w.x64, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    return BNN_OK;
+}
+
+// ---------------------------------------------------------------------------------
+// Batched refinement: pcg_solve's BNN_PCG_REFINED loop for many scenes at once.  Every
+// stage is one launch over the scenes still refining (each scene's blocks found through a
+// per-scene block prefix, as the batched step kernels do); the inner FP32 solves of all of
+// them are one k_pcg_batch launch.  The host keeps each scene's outer loop state and
+// takes exactly the decisions the lone loop takes, from the same device values.
+// ---------------------------------------------------------------------------------
+struct IrScene {
+    int n;
+    const float* b;            // right-hand side
+    double *x64, *r64;
+    float *r32, *d32;
+    const float* diag;
+    const int32_t* nbr;
+    int4* rec;                 // packed rows
+    double negoff;             // (double)(-(1 * dt))
+    double* partMax;
+    DevState* st;
+    float* pressure;
+};
+struct IrReport {
+    double res, bmax;
+    unsigned iter, flags;
+};
+// Uploaded with every round's tables: the barrier word and the unfinished-scene counter
+struct BatchHeader {
+    GridSync gs;
+    unsigned remaining;
+    unsigned flags;
+    unsigned pad;
+};
+
+__global__ void kb_pack_rows(const IrScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
+    int q;
+    const Blk b = seg_blk(P, ns, q);
+    const IrScene& c = S[q];
+    const int n = c.n;
+    const int r = b.x * blockDim.x + threadIdx.x;
+    if(r >= n) return;
+    int32_t nb[6];
+#pragma unroll
+    for(int k = 0; k < 6; ++k) nb[k] = c.nbr[(size_t)k * n + r];
+    const unsigned dyM = nb[1] >= 0 ? (unsigned)(r - nb[1]) : 0u, dyP = nb[4] >= 0 ? (unsigned)(nb[4] - r) : 0u;
+    const unsigned dzM = nb[0] >= 0 ? (unsigned)(r - nb[0]) : 0u, dzP = nb[5] >= 0 ? (unsigned)(nb[5] - r) : 0u;
+    int4 v;
+    v.x = (int)(dyM | (dyP << 16));
+    v.y = (int)(dzM | (nb[2] >= 0 ? 0x80000000u : 0u));
+    v.z = (int)(dzP | (nb[3] >= 0 ? 0x80000000u : 0u));
+    v.w = __float_as_int(c.diag[r]);
+    c.rec[r] = v;
+}
+__global__ void __launch_bounds__(kLanes) kb_ir_init(const IrScene* __restrict__ S, const unsigned* __restrict__ P,
+                                                     int ns) {
+    int q;
+    const Blk b = seg_blk(P, ns, q);
+    const IrScene& c = S[q];
+    ir_init_body(b, c.n, c.b, c.x64, c.r64, c.partMax, c.st);
+}
+__global__ void kb_ir_to_f32(const IrScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
+    int q;
+    const Blk b = seg_blk(P, ns, q);
+    const IrScene& c = S[q];
+    const size_t e = (size_t)b.x * blockDim.x + threadIdx.x;
+    if(e < (size_t)c.n) c.r32[e] = (float)c.r64[e];
+}
+__global__ void kb_ir_accumulate(const IrScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
+    int q;
+    const Blk b = seg_blk(P, ns, q);
+    const IrScene& c = S[q];
+    const size_t e = (size_t)b.x * blockDim.x + threadIdx.x;
+    if(e < (size_t)c.n) c.x64[e] = c.x64[e] + (double)c.d32[e];
+}
+__global__ void __launch_bounds__(kLanes) kb_ir_residual(const IrScene* __restrict__ S,
+                                                         const unsigned* __restrict__ P, int ns) {
+    int q;
+    const Blk b = seg_blk(P, ns, q);
+    const IrScene& c = S[q];
+    ir_residual_body(b, c.n, c.b, c.x64, c.r64, c.diag, c.nbr, nullptr, c.negoff, c.partMax, c.st);
+}
+__global__ void kb_ir_finish(const IrScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
+    int q;
+    const Blk b = seg_blk(P, ns, q);
+    const IrScene& c = S[q];
+    const size_t e = (size_t)b.x * blockDim.x + threadIdx.x;
+    if(e < (size_t)c.n) c.pressure[e] = (float)c.x64[e];
+}
+// one thread per scene: what the host's outer loop reads, plus the barrier's flags
+__global__ void kb_ir_report(const IrScene* __restrict__ S, int ns, const BatchHeader* hdr,
+                             IrReport* __restrict__ out) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if(q < ns) {
+        const DevState* st = S[q].st;
+        out[q] = IrReport{st->outer_res, st->outer_bmax, st->iter, st->flags};
+    }
+    if(q == 0) out[ns] = IrReport{0.0, 0.0, 0u, hdr->flags};
+}
+
+namespace {
+// Layout of the context's device blob (the same offsets in the pinned host mirror):
+// header, IrScene[cap], BatchPcgScene[cap], the prefixes of 256-row blocks and of 2048-row
+// chunks (cap + 1 each), then IrReport[cap + 1] (read back, not uploaded).
+struct BatchLayout {
+    size_t hdr, irs, bps, p256, pch, rep, up, total;
+    explicit BatchLayout(int cap) {
+        auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+        const size_t pre = (size_t)(cap + 1) * sizeof(unsigned);
+        hdr = 0;
+        irs = al(sizeof(BatchHeader));
+        bps = irs + al((size_t)cap * sizeof(IrScene));
+        p256 = bps + al((size_t)cap * sizeof(BatchPcgScene));
+        pch = p256 + al(pre);
+        up = pch + al(pre);
+        rep = up;
+        total = rep + al((size_t)(cap + 1) * sizeof(IrReport));
+    }
+};
+} // namespace
+
+static int batch_reserve(BatchPcgCtx& ctx, int count) {
+    if(count <= ctx.cap && ctx.dev) return BNN_OK;
+    pcg_batch_release(ctx);
+    const int cap = count < 64 ? 64 : count + count / 4;
+    const BatchLayout L(cap);
+    BNN_CUDA_CHECK(cudaMalloc(&ctx.dev, L.total));
+    BNN_CUDA_CHECK(cudaMallocHost(&ctx.host, L.total));
+    std::memset(ctx.host, 0, L.total);
+    for(auto& e : ctx.ev) BNN_CUDA_CHECK(cudaEventCreate(&e));
+    ctx.cap = cap;
+    ctx.upBytes = L.up;
+    ctx.blobBytes = L.total;
+    return BNN_OK;
+}
+
+void pcg_batch_release(BatchPcgCtx& ctx) {
+    if(ctx.dev) cudaFree(ctx.dev);
+    if(ctx.host) cudaFreeHost(ctx.host);
+    for(auto& e : ctx.ev)
+        if(e) cudaEventDestroy(e);
+    ctx = BatchPcgCtx();
+}
+
+int pcg_solve_batch_refined(BatchPcgCtx& ctx, BatchSolveItem* items, int count, cudaStream_t s) {
+    constexpr unsigned kMaxOuter = 60;  // pcg_solve's outer limit
+    struct Outer {
+        double bmax = 0, res = 0;
+        unsigned outer = 0, total = 0;
+        bool ok = false, stopped = false;
+        float kernelMs = 0.f;
+    };
+    std::vector<int> live;
+    for(int i = 0; i < count; ++i) {
+        items[i].out = PcgOutcome();
+        if(items[i].n == 0) { items[i].out.success = 1; continue; }
+        const int rc = pcg_reserve(*items[i].w, items[i].n, true);
+        if(rc != BNN_OK) return rc;
+        live.push_back(i);
+    }
+    if(live.empty()) return BNN_OK;
+    int rc = batch_reserve(ctx, (int)live.size());
+    if(rc != BNN_OK) return rc;
+    const BatchLayout L(ctx.cap);
+    char* H = (char*)ctx.host;
+    char* D = (char*)ctx.dev;
+    BatchHeader* hh = (BatchHeader*)(H + L.hdr);
+    IrScene* hirs = (IrScene*)(H + L.irs);
+    BatchPcgScene* hbps = (BatchPcgScene*)(H + L.bps);
+    unsigned* hp256 = (unsigned*)(H + L.p256);
+    unsigned* hpch = (unsigned*)(H + L.pch);
+    const IrReport* hrep = (const IrReport*)(H + L.rep);
+    const IrScene* dirs = (const IrScene*)(D + L.irs);
+    const unsigned* dp256 = (const unsigned*)(D + L.p256);
+    const unsigned* dpch = (const unsigned*)(D + L.pch);
+    BatchHeader* dh = (BatchHeader*)(D + L.hdr);
+    IrReport* drep = (IrReport*)(D + L.rep);
+
+    // this round's tables for the scenes `set` (positions in items), uploaded in one copy
+    auto upload = [&](const std::vector<int>& set) -> cudaError_t {
+        *hh = BatchHeader{GridSync{0u}, (unsigned)set.size(), 0u, 0u};
+        hp256[0] = hpch[0] = 0;
+        for(size_t k = 0; k < set.size(); ++k) {
+            const BatchSolveItem& it = items[set[k]];
+            PcgWork& w = *it.w;
+            const int n = it.n;
+            hirs[k] = IrScene{n, it.rhs, w.x64, w.r64, w.r32, w.d32, it.diag, it.nbr, w.rec,
+                              (double)(-(1.0f * it.dt)), w.partMaxD, it.dst, it.pressure};
+            BatchPcgScene& b = hbps[k];
+            b.n = n; b.rhsF = w.r32; b.invd = it.invd; b.rec = w.rec; b.negoff = -(1.0f * it.dt);
+            b.tolFactor = it.innerTol; b.maxIter = it.maxIter; b.x = w.d32; b.r = w.r; b.z = w.z; b.s0 = w.s0;
+            b.s1 = w.s1; b.q = w.q; b.part0 = w.part; b.part1 = w.part + w.nchCap;
+            b.part2 = w.part + 2 * (size_t)w.nchCap; b.partMax = w.partMaxF; b.dst = it.dst;
+            hp256[k + 1] = hp256[k] + (unsigned)((n + 255) / 256);
+            hpch[k + 1] = hpch[k] + (unsigned)((n + kChunk - 1) / kChunk);
+        }
+        return cudaMemcpyAsync(D, H, L.up, cudaMemcpyHostToDevice, s);
+    };
+    auto report = [&](int ns) -> int {
+        { kb_ir_report<<<(ns + 128) / 128, 128, 0, s>>>(dirs, ns, dh, drep); bnn_note_launch(); }
+        BNN_CUDA_CHECK(cudaMemcpyAsync(H + L.rep, drep, (size_t)(ns + 1) * sizeof(IrReport), cudaMemcpyDeviceToHost, s));
+        BNN_CUDA_CHECK(cudaStreamSynchronize(s));
+        if(hrep[ns].flags & BNN_FLAG_TIMEOUT) { bnn_set_error("batched PCG grid barrier timed out"); return BNN_ERR_TIMEOUT; }
+        return BNN_OK;
+    };
+
+    // outer loop start of every scene: x64 = 0, r64 = b, bmax
+    std::vector<Outer> o(count);
+    const int nl = (int)live.size();
+    BNN_CUDA_CHECK(upload(live));
+    { kb_pack_rows<<<hp256[nl], 256, 0, s>>>(dirs, dp256, nl); bnn_note_launch(); }
+    { kb_ir_init<<<hpch[nl], kLanes, 0, s>>>(dirs, dpch, nl); bnn_note_launch(); }
+    rc = report(nl);
+    if(rc != BNN_OK) return rc;
+    for(int k = 0; k < nl; ++k) {
+        Outer& e = o[live[k]];
+        e.bmax = hrep[k].bmax;
+        e.res = hrep[k].res;
+        e.ok = e.bmax < (double)FLT_MIN;
+    }
+
+    // cooperative grid of the inner solves
+    int numSM = 0, perSMv = 0;
+    {
+        std::lock_guard<std::mutex> lk(g_coop.mu);
+        if(!g_coop.numSM) {
+            int dev = 0;
+            BNN_CUDA_CHECK(cudaGetDevice(&dev));
+            BNN_CUDA_CHECK(cudaDeviceGetAttribute(&g_coop.numSM, cudaDevAttrMultiProcessorCount, dev));
+        }
+        if(!g_coop.perSM[15]) {
+            BNN_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_coop.perSM[15], k_pcg_batch, kLanes, 0));
+            if(g_coop.perSM[15] < 1) { bnn_set_error("batched PCG kernel cannot be resident"); return BNN_ERR_CUDA; }
+        }
+        numSM = g_coop.numSM;
+        perSMv = g_coop.perSM[15];
+    }
+
+    std::vector<int> set;
+    for(;;) {
+        // the lone loop's decisions, scene by scene
+        set.clear();
+        for(int i : live) {
+            Outer& e = o[i];
+            if(e.ok || e.stopped || e.outer >= kMaxOuter) continue;
+            if(e.res < (double)items[i].outerTol * e.bmax) { e.ok = true; continue; }
+            set.push_back(i);
+        }
+        if(set.empty()) break;
+        const int ns = (int)set.size();
+        BNN_CUDA_CHECK(upload(set));
+        { kb_ir_to_f32<<<hp256[ns], 256, 0, s>>>(dirs, dp256, ns); bnn_note_launch(); }
+        const unsigned total = hpch[ns];
+        const unsigned capB = (unsigned)(numSM * perSMv);
+        const unsigned perBlock = (total + capB - 1) / capB;
+        const unsigned grid = (total + perBlock - 1) / perBlock;
+        // every block's chunk range must meet at most kBatchSlots scenes
+        for(unsigned b = 0, k = 0; b < grid; ++b) {
+            const unsigned c0 = b * perBlock, c1 = std::min(c0 + perBlock, total);
+            while(hpch[k + 1] <= c0) ++k;
+            unsigned k1 = k;
+            while(hpch[k1 + 1] < c1) ++k1;
+            if(k1 - k + 1 > (unsigned)kBatchSlots) {
+                bnn_set_error("batched PCG: too many scenes per block");
+                return BNN_ERR_CAPACITY;
+            }
+        }
+        BatchPcgArgs a;
+        a.sc = (const BatchPcgScene*)(D + L.bps);
+        a.cp = dpch;
+        a.ns = ns;
+        a.total = total;
+        a.perBlock = perBlock;
+        a.gs = &dh->gs;
+        a.remaining = &dh->remaining;
+        a.flags = &dh->flags;
+        void* args[] = {(void*)&a};
+        {
+            CoopShare share(grid * (kShareUnits / perSMv), numSM * kShareUnits);
+            BNN_CUDA_CHECK(cudaEventRecord(ctx.ev[0], s));
+            BNN_CUDA_CHECK(cudaLaunchCooperativeKernel((const void*)k_pcg_batch, dim3(grid), dim3(kLanes), args, 0, s));
+            bnn_note_launch();
+            BNN_CUDA_CHECK(cudaEventRecord(ctx.ev[1], s));
+            { kb_ir_accumulate<<<hp256[ns], 256, 0, s>>>(dirs, dp256, ns); bnn_note_launch(); }
+            { kb_ir_residual<<<total, kLanes, 0, s>>>(dirs, dpch, ns); bnn_note_launch(); }
+            rc = report(ns);
+            if(rc != BNN_OK) return rc;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx.ev[0], ctx.ev[1]);
+        for(int k = 0; k < ns; ++k) {
+            Outer& e = o[set[k]];
+            e.total += hrep[k].iter;
+            e.kernelMs += ms;
+            e.res = hrep[k].res;
+            ++e.outer;
+            if(e.total >= items[set[k]].maxIter) e.stopped = true;
+        }
+    }
+    for(int i : live) {
+        Outer& e = o[i];
+        if(!e.ok && e.res < (double)items[i].outerTol * e.bmax) e.ok = true;
+        PcgOutcome& out = items[i].out;
+        out.iterations = e.total;
+        out.outer = e.outer;
+        out.kernelMs = e.kernelMs;
+        out.residual = e.res;
+        out.success = e.ok ? 1 : 0;
+    }
+    // pressure = (float) x64
+    BNN_CUDA_CHECK(upload(live));
+    { kb_ir_finish<<<hp256[nl], 256, 0, s>>>(dirs, dp256, nl); bnn_note_launch(); }
+    BNN_CUDA_CHECK(cudaGetLastError());
+    BNN_CUDA_CHECK(cudaStreamSynchronize(s));
     return BNN_OK;
 }
 

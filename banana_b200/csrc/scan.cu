@@ -94,8 +94,122 @@ template<class TI, class TO> cudaError_t scan_impl(const TI* in, TO* out, size_t
     { k_copy_total<TO><<<1, 1, 0, s>>>(out, n, sumsScan, nb); bnn_note_launch(); }
     return cudaGetLastError();
 }
+
+// ---- batched segments ----------------------------------------------------------------
+// Segment q: tiles tiles[q] .. tiles[q+1]-1 of the launch (at least one, so an empty
+// segment still gets its total 0).  Its tile sums go to ws[0..nb], their scan to
+// ws[nb+1 ..] (the layout scan_impl's first level uses).
+__device__ __forceinline__ void scan_tile_body(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+                                               uint32_t* __restrict__ sums, size_t n, unsigned tile, unsigned ntiles) {
+    __shared__ uint32_t warpTot[kScanThreads / 32];
+    const size_t base = (size_t)tile * kScanTile + (size_t)threadIdx.x * kScanPer;
+    uint32_t v[kScanPer];
+    uint32_t local = 0;
+#pragma unroll
+    for(int j = 0; j < kScanPer; ++j) {
+        size_t e = base + j;
+        v[j] = e < n ? in[e] : 0u;
+        local += v[j];
+    }
+    uint32_t incl = warp_incl_scan(local);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if(lane == 31) warpTot[warp] = incl;
+    __syncthreads();
+    if(warp == 0) {
+        uint32_t w = lane < kScanThreads / 32 ? warpTot[lane] : 0u;
+        uint32_t wi = warp_incl_scan(w);
+        if(lane < kScanThreads / 32) warpTot[lane] = wi - w;
+    }
+    __syncthreads();
+    uint32_t run = warpTot[warp] + incl - local;
+#pragma unroll
+    for(int j = 0; j < kScanPer; ++j) {
+        size_t e = base + j;
+        if(e < n) out[e] = run;
+        run += v[j];
+    }
+    if(threadIdx.x == kScanThreads - 1) {
+        if(ntiles > 1) sums[tile] = run;
+        else out[n] = run;
+    }
+}
+
+__global__ void __launch_bounds__(kScanThreads) kb_scan_tiles(const ScanSeg* __restrict__ segs,
+                                                              const unsigned* __restrict__ tiles, int nseg) {
+    int q;
+    const Blk b = seg_blk(tiles, nseg, q);
+    const ScanSeg sg = segs[q];
+    scan_tile_body(sg.in, sg.out, sg.ws, sg.n, b.x, b.n);
+}
+// Exclusive scan of m <= kScanTile values by one block, continuing from `carry` (updated to
+// the running total; every thread gets it)
+__device__ __forceinline__ void scan_chunk_carry(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+                                                 unsigned m, uint32_t& carry) {
+    __shared__ uint32_t warpTot[kScanThreads / 32];
+    __shared__ uint32_t sTotal;
+    const unsigned base = threadIdx.x * kScanPer;
+    uint32_t v[kScanPer];
+    uint32_t local = 0;
+#pragma unroll
+    for(int j = 0; j < kScanPer; ++j) {
+        v[j] = base + j < m ? in[base + j] : 0u;
+        local += v[j];
+    }
+    const uint32_t incl = warp_incl_scan(local);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if(lane == 31) warpTot[warp] = incl;
+    __syncthreads();
+    if(warp == 0) {
+        const uint32_t w = lane < kScanThreads / 32 ? warpTot[lane] : 0u;
+        const uint32_t wi = warp_incl_scan(w);
+        if(lane < kScanThreads / 32) warpTot[lane] = wi - w;
+        if(lane == kScanThreads / 32 - 1) sTotal = wi;
+    }
+    __syncthreads();
+    uint32_t run = carry + warpTot[warp] + incl - local;
+#pragma unroll
+    for(int j = 0; j < kScanPer; ++j) {
+        if(base + j < m) out[base + j] = run;
+        run += v[j];
+    }
+    carry += sTotal;
+    __syncthreads();
+}
+// one block per segment: scan of its tile sums, and the total
+__global__ void __launch_bounds__(kScanThreads) kb_scan_sums(const ScanSeg* __restrict__ segs,
+                                                             const unsigned* __restrict__ tiles) {
+    const ScanSeg sg = segs[blockIdx.x];
+    const unsigned nb = __ldg(tiles + blockIdx.x + 1) - __ldg(tiles + blockIdx.x);
+    if(nb <= 1) return;
+    uint32_t* sumsScan = sg.ws + (nb + 1);
+    uint32_t carry = 0;
+    for(unsigned b0 = 0; b0 < nb; b0 += kScanTile)
+        scan_chunk_carry(sg.ws + b0, sumsScan + b0, min(nb - b0, (unsigned)kScanTile), carry);
+    if(threadIdx.x == 0) sg.out[sg.n] = carry;
+}
+__global__ void __launch_bounds__(kScanThreads) kb_scan_add(const ScanSeg* __restrict__ segs,
+                                                            const unsigned* __restrict__ tiles, int nseg) {
+    int q;
+    const Blk b = seg_blk(tiles, nseg, q);
+    if(b.n <= 1) return;
+    const ScanSeg sg = segs[q];
+    const uint32_t o = sg.ws[(b.n + 1) + b.x];
+    const size_t base = (size_t)b.x * kScanTile;
+    for(int j = threadIdx.x; j < kScanTile; j += kScanThreads) {
+        size_t e = base + j;
+        if(e < sg.n) sg.out[e] += o;
+    }
+}
 } // namespace
 
+cudaError_t batched_exclusive_scan_u32(const ScanSeg* segs, const unsigned* tiles, int nseg, unsigned totalTiles,
+                                       cudaStream_t s) {
+    if(nseg == 0 || totalTiles == 0) return cudaSuccess;
+    { kb_scan_tiles<<<totalTiles, kScanThreads, 0, s>>>(segs, tiles, nseg); bnn_note_launch(); }
+    { kb_scan_sums<<<(unsigned)nseg, kScanThreads, 0, s>>>(segs, tiles); bnn_note_launch(); }
+    { kb_scan_add<<<totalTiles, kScanThreads, 0, s>>>(segs, tiles, nseg); bnn_note_launch(); }
+    return cudaGetLastError();
+}
 size_t scan_workspace_bytes(size_t n) { return ws_bytes<uint32_t>(n); }
 size_t scan_workspace_bytes_u64(size_t n) { return ws_bytes<unsigned long long>(n); }
 

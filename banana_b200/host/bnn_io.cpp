@@ -1,11 +1,10 @@
 // Banana particle data files (.bnn): see bnn_io.h for the layout.
 #include "bnn_io.h"
 
-#include <sys/stat.h>
-
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <filesystem>
 #include <fstream>
 #include <limits>
 #include <sstream>
@@ -224,12 +223,13 @@ std::string bnn_file_path(const std::string& root, const std::string& folder, co
     return root + "/" + folder + "/" + name + buf;
 }
 
+// FileHelpers::createFolder (FileHelpers.h:43-53) creates every missing folder of the
+// path ("mkdir -p"); so does this
 bool make_output_folder(const std::string& root, const std::string& folder) {
-    mkdir(root.c_str(), 0755);
     const std::string p = root + "/" + folder;
-    mkdir(p.c_str(), 0755);
-    struct stat st;
-    return stat(p.c_str(), &st) == 0 && S_ISDIR(st.st_mode);
+    std::error_code ec;
+    std::filesystem::create_directories(p, ec);
+    return std::filesystem::is_directory(p, ec);
 }
 
 } // namespace bnnhost

@@ -408,7 +408,8 @@ def run_ours(args, ws, rank, local):
                                          "(standalone capture) x iterations per launch; the solve is L2-resident"},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clk,
-            "detail": {"pcg_iterations_per_step": iters / args.steps, "active_rows_mean": float(np.mean(rows)),
+            "detail": {"tile_tuning": capi.tile_tuning(),
+                       "pcg_iterations_per_step": iters / args.steps, "active_rows_mean": float(np.mean(rows)),
                        "pcg_kernel_ms_per_step": pcg_kernel_ms / args.steps,
                        "stage_ms_per_step": {k: v / args.steps for k, v in stage_tot.items()},
                        "stage_gbs": stage_gbs},
@@ -441,7 +442,8 @@ def run_batch(args, ws, rank, local):
         cells = [int(np.floor(f * r + 1e-9)) for f, r in zip(s["block_frac"], s["res"])]
         costs.append(bdist.scene_bytes_per_step(s["res"], 8 * cells[0] * cells[1] * cells[2]))
     mine = bdist.shard_scenes(costs, ws)[rank]
-    b = FlipBatch(worker_threads=args.workers)
+    mode = capi.BATCH_PER_SCENE if args.batch_mode == "per_scene" else capi.BATCH_STAGED
+    b = FlipBatch(worker_threads=args.workers, step_mode=mode)
     built = [scenes.batch_scene(specs[i]) for i in mine]
     npart = sum(len(p) for _, p, _ in built)
     t_up = time.perf_counter()
@@ -455,13 +457,17 @@ def run_batch(args, ws, rank, local):
         dist.barrier()
     torch.cuda.synchronize()
     launches0 = capi.launch_count()
-    lat, ps, iters = [], 0, 0
+    lat, ps, iters, staged = [], 0, 0, 0
+    stage_ms = {k: 0.0 for k in capi.STAGES}
     t0 = time.perf_counter()
     for _ in range(args.steps):
         st = b.step()
         lat.append(st["wall_ms"])
         ps += st["particle_steps"]
         iters += st["pcg_iterations"]
+        staged = max(staged, st["staged_scenes"])
+        for k, v in b.scene_info(ids[0])["stage_ms"].items():
+            stage_ms[k] += v
     torch.cuda.synchronize()
     te = time.perf_counter() - t0
     t_dl = time.perf_counter()
@@ -471,22 +477,26 @@ def run_batch(args, ws, rank, local):
     clk = clocks.stop()
     launches = capi.launch_count() - launches0
     b.close()
-    # the same scenes one at a time (one worker thread: each scene's sub-step runs alone
-    # on the GPU before the next one starts), for the batching's gain
-    b1 = FlipBatch(worker_threads=1)
-    for cfg, pos, vel in built:
-        b1.add_scene(cfg, pos, vel)
-    b1.step()
-    torch.cuda.synchronize()
-    t1 = time.perf_counter()
-    ps1 = 0
-    seq_steps = 2
-    for _ in range(seq_steps):
-        ps1 += b1.step()["particle_steps"]
-    torch.cuda.synchronize()
-    t1 = time.perf_counter() - t1
-    b1.close()
-    seq_value = ps1 / t1
+    # the same scenes one at a time (one worker thread, no staged step: each scene's
+    # sub-step runs alone on the GPU before the next one starts), and each on its own
+    # stream from the worker pool, for the batching's gain
+    def other_mode(workers, step_mode, n_steps=2):
+        bo = FlipBatch(worker_threads=workers, step_mode=step_mode)
+        for cfg, pos, vel in built:
+            bo.add_scene(cfg, pos, vel)
+        bo.step()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        pso = 0
+        for _ in range(n_steps):
+            pso += bo.step()["particle_steps"]
+        torch.cuda.synchronize()
+        t = time.perf_counter() - t
+        bo.close()
+        return pso / t, t * 1e3 / n_steps
+    seq_value, seq_ms = other_mode(1, capi.BATCH_PER_SCENE)
+    pool_value, pool_ms = (other_mode(args.workers, capi.BATCH_PER_SCENE) if mode == capi.BATCH_STAGED
+                           else (ps / te, te * 1e3 / args.steps))
     tot_ps = ps
     t_max = te
     e2e_t = te + t_up + t_dl
@@ -505,15 +515,22 @@ def run_batch(args, ws, rank, local):
                 "config": {"workload": "batch_256_scenes", "scenes": len(specs), "scenes_rank0": len(mine),
                            "particles_rank0": npart, "res_choices": [32, 48, 64, 96, 128], "cell_size": "1/64",
                            "pcg": "Jacobi, refined FP32 inner / FP64 outer to 1e-6, inner 1e-2",
+                           "batch_mode": args.batch_mode, "staged_scenes_rank0": staged,
                            "worker_threads": args.workers or "min(16, cores)", "parallelism": f"scenes/{ws} ranks"},
                 "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
                 "e2e": {"value": tot_ps / e2e_t, "unit": UNIT, "h2d_bytes_per_step": 24 * npart / args.steps,
                         "d2h_bytes_per_step": 24 * npart / args.steps,
                         "api": "bnn_batch_add_scene (upload) + steps + bnn_batch_get_scene (download), wall clock"},
                 "gpu_launches": int(launches), "clocks": clk,
-                "detail": {"pcg_iterations_per_step": iters / args.steps, "timing": "host wall clock per batch step",
-                           "one_scene_at_a_time": {"value": seq_value, "ms_per_step": t1 * 1e3 / seq_steps,
+                "detail": {"tile_tuning": capi.tile_tuning(),
+                           "pcg_iterations_per_step": iters / args.steps, "timing": "host wall clock per batch step",
+                           "stage_ms_per_step": {k: round(v / args.steps, 3) for k, v in stage_ms.items()},
+                           "stage_ms_note": "device time per stage of the staged step (scene 0's record; all "
+                                            "staged scenes share it), or scene 0's own stream in per_scene mode",
+                           "one_scene_at_a_time": {"value": seq_value, "ms_per_step": seq_ms,
                                                    "note": "rank 0's scenes, one worker thread, same accuracy"},
+                           "per_scene_streams": {"value": pool_value, "ms_per_step": pool_ms,
+                                                 "note": "rank 0's scenes, each on its own stream from the worker pool"},
                            "batched_over_one_at_a_time": (ps / te) / seq_value}}
         print(json.dumps(line), flush=True)
     if ws > 1:
@@ -904,6 +921,8 @@ def main():
                     help="reference arm: Jacobi (the configs) or the reference's default symmetric MIC(0)")
     ap.add_argument("--workload", choices=["flip", "batch", "serve", "nsearch", "pcg", "fp64err", "aniso", "boundary"], default="flip")
     ap.add_argument("--workers", type=int, default=0, help="batch/serve: host threads stepping scenes (0 = auto)")
+    ap.add_argument("--batch-mode", choices=["staged", "per_scene"], default="staged",
+                    help="batch/serve: one launch per stage over the scenes (staged) or each scene on its own stream")
     ap.add_argument("--requests", type=int, default=100, help="serve: number of requests")
     ap.add_argument("--req-steps", type=int, default=200, help="serve: sub-steps per request")
     ap.add_argument("--time-limit", type=float, default=240.0, help="serve: stop after this many seconds")

@@ -175,9 +175,18 @@ int bnn_scene_bytes_estimate(const bnn_params* params, uint32_t n, uint64_t* byt
  * driven by one host thread.  No counterpart in the reference, which runs one scene per
  * ParticleSolver object (ParticleSolver.h:39-105). */
 typedef struct bnn_batch bnn_batch;
+/* How bnn_batch_step advances the scenes.  STAGED (the default): the scenes the staged
+ * step takes (FLIP, BNN_PCG_REFINED in its default step order, the domain box as the only
+ * boundary, no position correction, particles present) advance together, one kernel launch
+ * per stage of the sub-step over all of them; the others as in PER_SCENE.  PER_SCENE: every
+ * scene runs bnn_flip_step on its own stream, from a pool of host threads.  Both compute
+ * for every scene exactly what bnn_flip_step computes for it alone. */
+#define BNN_BATCH_STAGED    0
+#define BNN_BATCH_PER_SCENE 1
 typedef struct bnn_batch_params {
     uint64_t hbm_budget_bytes; /* admission budget over bnn_scene_bytes_estimate; 0 = none */
     uint32_t worker_threads;   /* host threads stepping scenes; 0 = min(16, cores) */
+    uint32_t step_mode;        /* BNN_BATCH_STAGED or BNN_BATCH_PER_SCENE */
 } bnn_batch_params;
 typedef struct bnn_batch_stats {
     uint32_t scenes;           /* scenes stepped */
@@ -186,6 +195,8 @@ typedef struct bnn_batch_stats {
     uint64_t pcg_iterations;   /* summed over scenes */
     double   wall_ms;          /* host wall time of the batch step */
     double   max_scene_ms;     /* slowest scene's step */
+    uint32_t staged_scenes;    /* scenes advanced by the staged (one launch per stage) step */
+    uint32_t reserved;
 } bnn_batch_stats;
 int bnn_batch_create(const bnn_batch_params* params, bnn_batch** out);
 int bnn_batch_destroy(bnn_batch* b);
@@ -202,6 +213,22 @@ int bnn_batch_scene_info(bnn_batch* b, uint32_t scene_id, uint32_t* n, uint64_t*
 int bnn_batch_get_scene(bnn_batch* b, uint32_t scene_id, float* pos, float* vel);
 /* Sum of the admitted scenes' estimates and of the bytes they hold now. */
 int bnn_batch_memory(bnn_batch* b, uint64_t* admitted, uint64_t* held);
+
+/* ---- tile shapes of the P2G + fluid SDF pass -------------------------------------
+ * The FLIP pass (P2G of the three face components with the fluid SDF) runs in tiles of
+ * 30 x tz face columns walking yc face layers along y; every shape computes the same bits
+ * (fixed per-cell and per-face summation orders).  By default a tuner times every shape the
+ * first time it meets a kind of launch (a lone scene's resolution bucket, ceil((G + 1) / 32)
+ * cells per axis; a batch's scene count and total cells, in powers of two) and keeps the
+ * fastest.  No counterpart in the reference (its P2G is a serial loop, FLIP_Solver.cpp:57-95). */
+/* Number of shapes; tz[i], yc[i] of each (arrays of at least `cap` entries, may be NULL). */
+int bnn_tile_shapes(int32_t* tz, int32_t* yc, int32_t cap);
+/* Use shape `shape` (0 .. bnn_tile_shapes() - 1) for every launch of the process, or -1 to
+ * tune (the default).  BNN_ERR_INVALID_ARGUMENT outside that range. */
+int bnn_set_tile_shape(int32_t shape);
+/* The tuner's choices as JSON lines, NUL-terminated, into buf (cap bytes); *needed = bytes
+ * the whole text takes with its NUL.  BNN_ERR_CAPACITY when cap is smaller. */
+int bnn_tile_tuning(char* buf, size_t cap, size_t* needed);
 
 /* ---- standalone kernels (device pointers, stream = cudaStream_t or NULL) ---------- */
 

@@ -1,6 +1,7 @@
 """Scene batches (bnn_batch_*): every scene of a batch computes exactly what a lone
-solver handle computes (scenes are stepped concurrently from worker threads, each on its
-own stream), scenes come and go between steps, and admission honours the budget."""
+solver handle computes -- in the staged step (one launch per stage over all the scenes it
+takes) and in the per-scene step (worker threads, each scene on its own stream) -- scenes
+come and go between steps, and admission honours the budget."""
 import numpy as np
 import pytest
 
@@ -16,17 +17,21 @@ SPECS = [
 ]
 
 
-def _lone(bnn, spec, steps):
-    cfg, pos, vel = scenes.batch_scene(spec)
+def _lone(bnn, spec, steps, **over):
+    cfg, pos, vel = scenes.batch_scene(spec, **over)
     s = bnn.FlipSolver(cfg)
     s.set_particles(pos, vel)
     for _ in range(steps):
         s.step()
-    return s.get_particles()
+    out = s.get_particles()
+    s.close()
+    return out
 
 
-def test_batch_scenes_equal_lone_solvers(bnn):
-    b = bnn.FlipBatch(worker_threads=3)
+@pytest.mark.parametrize("mode", ["staged", "per_scene"])
+def test_batch_scenes_equal_lone_solvers(bnn, mode):
+    staged = mode == "staged"
+    b = bnn.FlipBatch(worker_threads=3, step_mode=bnn.capi.BATCH_STAGED if staged else bnn.capi.BATCH_PER_SCENE)
     ids = {}
     for q in range(3):
         cfg, pos, vel = scenes.batch_scene(SPECS[q])
@@ -34,6 +39,7 @@ def test_batch_scenes_equal_lone_solvers(bnn):
     for _ in range(5):
         st = b.step()
         assert st["scenes"] == 3 and st["failed"] == 0
+        assert st["staged_scenes"] == (3 if staged else 0)
     for q in range(3):
         pg, vg = b.get_scene(ids[q])
         pl, vl = _lone(bnn, SPECS[q], 5)
@@ -63,4 +69,31 @@ def test_batch_admission_budget(bnn):
     with pytest.raises(bnn.BnnError) as e:
         b.add_scene(cfg, pos, vel)
     assert e.value.code == 8  # BNN_ERR_CAPACITY
+    b.close()
+
+
+def test_staged_batch_mixed_sizes_and_kinds(bnn):
+    """Scenes of uneven sizes (one with more cells than one 2048 x 2048 scan level holds)
+    beside a scene the staged step does not take (plain FP32 PCG): each equals its lone run."""
+    specs = [{"res": (40, 24, 56), "block_frac": (0.5, 0.5, 0.4), "seed": 11},
+             {"res": (16, 48, 16), "block_frac": (0.6, 0.3, 0.6), "seed": 12},
+             {"res": (168, 160, 160), "block_frac": (0.2, 0.2, 0.2), "seed": 13},
+             {"res": (24, 24, 24), "block_frac": (0.4, 0.6, 0.4), "seed": 14},
+             {"res": (32, 16, 40), "block_frac": (0.3, 0.5, 0.5), "seed": 15}]
+    over = [{}, {}, {}, {"pcg_mode": 0}, {}]
+    steps = 4
+    b = bnn.FlipBatch(worker_threads=2)
+    ids = []
+    for spec, o in zip(specs, over):
+        cfg, pos, vel = scenes.batch_scene(spec, **o)
+        ids.append(b.add_scene(cfg, pos, vel))
+    for _ in range(steps):
+        st = b.step()
+        assert st["failed"] == 0 and st["staged_scenes"] == 4
+    for sid, spec, o in zip(ids, specs, over):
+        pg, vg = b.get_scene(sid)
+        pl, vl = _lone(bnn, spec, steps, **o)
+        assert np.array_equal(pg, pl) and np.array_equal(vg, vl), spec
+        info = b.scene_info(sid)
+        assert info["steps"] == steps and info["pcg_success"] == 1
     b.close()

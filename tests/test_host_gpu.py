@@ -188,7 +188,13 @@ def test_reference_scene_through_the_drop_in(bnn, tmp_path):
     assert len(pos) == head["particles"] > 0
     lo = np.array(sc["SimulationParameters"]["SimulationDomainBox"]["BoxMin"], np.float32)
     hi = np.array(sc["SimulationParameters"]["SimulationDomainBox"]["BoxMax"], np.float32)
-    assert np.all(pos >= lo - 1e-6) and np.all(pos <= hi + 1e-6)
+    # the box projection (BoundaryObject::constrainToBoundary, BoundaryObject.cpp:72-90)
+    # moves a particle along a finite-difference gradient (GeometryObjects.cpp:37-85), which
+    # near the box's edges and corners can leave it a little outside: allow one particle
+    # radius (cell size / RatioCellSizePRadius)
+    radius = sc["SimulationParameters"]["CellSize"] / 2.0
+    excursion = float(max((lo - pos).max(), (pos - hi).max(), 0.0))
+    assert excursion <= radius, excursion
     assert np.all(np.isfinite(vel))
     g = sc["GlobalParameters"]
     frame = tmp_path / g["DataPath"] / g["FrameDataFolder"] / "frame.0002.bnn"
