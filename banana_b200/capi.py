@@ -71,6 +71,7 @@ class StepStats(C.Structure):
 
 BATCH_STAGED = 0      # BNN_BATCH_STAGED: one launch per stage over the scenes it takes
 BATCH_PER_SCENE = 1   # BNN_BATCH_PER_SCENE: every scene on its own stream
+BATCH_NO_GRAPHS = 0x100  # BNN_BATCH_NO_GRAPHS: the staged step without CUDA-graph replay
 
 
 class BatchParams(C.Structure):

@@ -96,8 +96,10 @@ extern "C" int bnn_batch_create(const bnn_batch_params* params, bnn_batch** out)
     auto* b = new bnn_batch();
     BNN_CUDA_CHECK(cudaGetDevice(&b->device));
     b->budget = params ? params->hbm_budget_bytes : 0;
-    b->mode = params ? params->step_mode : BNN_BATCH_STAGED;
-    if(b->mode != BNN_BATCH_STAGED && b->mode != BNN_BATCH_PER_SCENE) {
+    const uint32_t mode = params ? params->step_mode : BNN_BATCH_STAGED;
+    b->mode = mode & 0xffu;
+    b->staged.graphs = (mode & BNN_BATCH_NO_GRAPHS) == 0;
+    if((b->mode != BNN_BATCH_STAGED && b->mode != BNN_BATCH_PER_SCENE) || (mode & ~(0xffu | BNN_BATCH_NO_GRAPHS))) {
         delete b;
         return BNN_ERR_INVALID_ARGUMENT;
     }

@@ -46,7 +46,12 @@ inline unsigned region_tiles(const GridDesc& g, int d) {
     const int sy = g.G[1] + (d == 1 ? 1 : 0), sz = g.G[2] + (d == 2 ? 1 : 0);
     return cdiv((size_t)sy, 8) * (unsigned)sz;
 }
-inline unsigned region_blocks(unsigned tiles) { return std::min(kRegionBlocks, std::max(1u, tiles / 2)); }
+// The stage touches only the faces within reach of the occupied-cell box (a part of the
+// array), and every block of a batched launch pays for finding its scene: a block per 32
+// tiles of the whole array
+inline unsigned region_blocks(unsigned tiles) { return std::min(kRegionBlocks, std::max(1u, tiles / 32)); }
+// Blocks of an element-wise batched stage over n elements (kBatchVirt lone blocks each)
+inline unsigned virt_blocks(size_t n) { return cdiv(cdiv(n, 256), kBatchVirt); }
 
 // Prefix arrays of the step (cap + 1 entries each), in upload order
 enum Pre { PAdvect, PAdvFold, PParticles, PMoveFold, PCells, PSortLarge, PScan, PExtrap, PFill, PUpdU, PUpdV, PUpdW,
@@ -75,6 +80,8 @@ bool batch_step_eligible(const bnn_flip* h) {
 }
 
 void batch_step_release(BatchStepWork& w) {
+    for(auto& g : w.seg)
+        if(g.exec) cudaGraphExecDestroy(g.exec);
     if(w.dev) cudaFree(w.dev);
     if(w.host) cudaFreeHost(w.host);
     for(auto& e : w.ev)
@@ -82,6 +89,37 @@ void batch_step_release(BatchStepWork& w) {
     if(w.s) cudaStreamDestroy(w.s);
     pcg_batch_release(w.pcg);
     w = BatchStepWork();
+}
+
+// Runs a segment of launches: directly, or as a CUDA graph captured from them (again when
+// the launch shapes `sig` changed since the last capture) and replayed.
+template<class F> static int run_segment(StagedGraph& g, const std::vector<uint64_t>& sig, cudaStream_t s,
+                                         bool graph, F body) {
+    if(!graph) return body(false);
+    if(!g.exec || g.sig != sig) {
+        if(g.exec) cudaGraphExecDestroy(g.exec);
+        g.exec = nullptr;
+        const long long l0 = (long long)bnn_launch_count();
+        BNN_CUDA_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        const int rc = body(true);
+        cudaGraph_t cg = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(s, &cg);
+        g.kernels = (long long)bnn_launch_count() - l0;
+        bnn_note_launches(-g.kernels);  // captured, not run
+        if(rc != BNN_OK || e != cudaSuccess) {
+            if(cg) cudaGraphDestroy(cg);
+            if(rc != BNN_OK) return rc;
+            BNN_CUDA_CHECK(e);
+        }
+        const cudaError_t ei = cudaGraphInstantiate(&g.exec, cg, 0);
+        cudaGraphDestroy(cg);
+        if(ei != cudaSuccess) g.exec = nullptr;
+        BNN_CUDA_CHECK(ei);
+        g.sig = sig;
+    }
+    BNN_CUDA_CHECK(cudaGraphLaunch(g.exec, s));
+    bnn_note_launches(g.kernels);
+    return BNN_OK;
 }
 
 static int batch_reserve(BatchStepWork& w, int ns) {
@@ -187,7 +225,7 @@ int batch_substep(BatchStepWork& w, bnn_flip* const* hs, int nsIn, int* rc, bnn_
                       h->phi);
         hSeg[q] = ScanSeg{h->count, h->cellStart, (uint32_t*)h->scanWs, h->C};
         hSeg[ns + q] = ScanSeg{h->flag, h->aidx, (uint32_t*)h->scanWs, h->C};
-        const unsigned pb = cdiv((size_t)c.n, 256);
+        const unsigned pb = virt_blocks((size_t)c.n);
         unsigned tiles[3], ftot = 0;
         size_t fmax = 0;
         for(int d = 0; d < 3; ++d) {
@@ -200,7 +238,7 @@ int batch_substep(BatchStepWork& w, bnn_flip* const* hs, int nsIn, int* rc, bnn_
             moved ? 0u : bbox_fold_blocks(c.n),                // PAdvFold
             pb,                                                // PParticles
             bbox_fold_blocks(c.n),                             // PMoveFold
-            cdiv(h->C, 256),                                   // PCells
+            virt_blocks(h->C),                                 // PCells
             c.n > 16 ? std::min(296u, std::max(2u, cdiv((size_t)c.n, 65536))) : 0u,  // PSortLarge
             cdiv(h->C, 2048),                                  // PScan
             region_blocks(ftot),                               // PExtrap
@@ -213,43 +251,57 @@ int batch_substep(BatchStepWork& w, bnn_flip* const* hs, int nsIn, int* rc, bnn_
     }
     BNN_CUDA_CHECK(cudaMemcpyAsync(D, H, L.up, cudaMemcpyHostToDevice, s));
 
-    // ---- move + counting sort
-    cudaEventRecord(w.ev[0], s);
-    launch_batch_stage(BatchStage::StepReset, dS, nullptr, ns, 0, s);
-    launch_batch_stage(BatchStage::Advect, dS, dP(PAdvect), ns, tot(PAdvect), s);
-    launch_batch_stage(BatchStage::BboxFinal, dS, dP(PAdvFold), ns, tot(PAdvFold), s);
-    cudaEventRecord(w.ev[1], s);
-    BNN_CUDA_CHECK(batched_exclusive_scan_u32(dSeg, dP(PScan), ns, tot(PScan), s));
-    launch_batch_stage(BatchStage::ScatterIndex, dS, dP(PParticles), ns, tot(PParticles), s);
-    launch_batch_stage(BatchStage::SortBuckets, dS, dP(PCells), ns, tot(PCells), s);
-    launch_batch_stage(BatchStage::SortLarge, dS, dP(PSortLarge), ns, tot(PSortLarge), s);
-    launch_batch_stage(BatchStage::Gather, dS, dP(PParticles), ns, tot(PParticles), s);
-    cudaEventRecord(w.ev[2], s);
-    // ---- P2G + fluid SDF
-    {
-        const unsigned* P[kTileShapes];
-        unsigned tiles[kTileShapes];
-        for(int k = 0; k < kTileShapes; ++k) {
-            P[k] = dP(PTiles + k);
-            tiles[k] = tot(PTiles + k);
-        }
-        launch_p2g_sdf_batch(D + L.args, P, tiles, ns, cells, s);
-    }
-    cudaEventRecord(w.ev[3], s);
-    // ---- extrapolate, backup, gravity (FLIP_Solver.cpp:44-47)
-    for(int layer = 0; layer < 4; ++layer) {
-        if(layer == 3) launch_batch_stage(BatchStage::FillBackup, dS, dP(PFill), ns, tot(PFill), s);
-        launch_batch_stage(BatchStage::Extrapolate, dS, dP(PExtrap), ns, tot(PExtrap), s, 1, layer);
-    }
-    cudaEventRecord(w.ev[4], s);
-    cudaEventRecord(w.ev[5], s);
-    // ---- the pressure system's numbering
-    launch_batch_stage(BatchStage::ActiveFlags, dS, dP(PCells), ns, tot(PCells), s);
-    BNN_CUDA_CHECK(batched_exclusive_scan_u32(dSeg + ns, dP(PScan), ns, tot(PScan), s));
+    // ---- segment 1: move, counting sort, P2G + fluid SDF, extrapolation, numbering
+    const int shape = p2g_batch_shape(ns, cells);
+    const bool capture = w.graphs && shape >= 0;  // the tuner synchronises: not inside a capture
     unsigned* dRows = (unsigned*)(D + L.rows);
     const unsigned* hRows = (const unsigned*)(H + L.rows);
-    launch_batch_gather_rows(dS, ns, dRows, s);
-    BNN_CUDA_CHECK(cudaMemcpyAsync(H + L.rows, dRows, (size_t)ns * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    cudaEventRecord(w.ev[0], s);
+    auto seg1 = [&](bool capturing) -> int {
+        auto mark = [&](int k) { capturing ? cudaEventRecordWithFlags(w.ev[k], s, cudaEventRecordExternal)
+                                           : cudaEventRecord(w.ev[k], s); };
+        launch_batch_stage(BatchStage::StepReset, dS, nullptr, ns, 0, s);
+        launch_batch_stage(BatchStage::Advect, dS, dP(PAdvect), ns, tot(PAdvect), s);
+        launch_batch_stage(BatchStage::BboxFinal, dS, dP(PAdvFold), ns, tot(PAdvFold), s);
+        mark(1);
+        BNN_CUDA_CHECK(batched_exclusive_scan_u32(dSeg, dP(PScan), ns, tot(PScan), s));
+        launch_batch_stage(BatchStage::ScatterIndex, dS, dP(PParticles), ns, tot(PParticles), s);
+        launch_batch_stage(BatchStage::SortBuckets, dS, dP(PCells), ns, tot(PCells), s);
+        launch_batch_stage(BatchStage::SortLarge, dS, dP(PSortLarge), ns, tot(PSortLarge), s);
+        launch_batch_stage(BatchStage::Gather, dS, dP(PParticles), ns, tot(PParticles), s);
+        mark(2);
+        {
+            const unsigned* P[kTileShapes];
+            unsigned tiles[kTileShapes];
+            for(int k = 0; k < kTileShapes; ++k) {
+                P[k] = dP(PTiles + k);
+                tiles[k] = tot(PTiles + k);
+            }
+            launch_p2g_sdf_batch(D + L.args, P, tiles, ns, cells, s);
+        }
+        mark(3);
+        // extrapolate, backup, gravity (FLIP_Solver.cpp:44-47)
+        for(int layer = 0; layer < 4; ++layer) {
+            if(layer == 3) launch_batch_stage(BatchStage::FillBackup, dS, dP(PFill), ns, tot(PFill), s);
+            launch_batch_stage(BatchStage::Extrapolate, dS, dP(PExtrap), ns, tot(PExtrap), s, 1, layer);
+        }
+        mark(4);
+        mark(5);
+        // the pressure system's numbering, and its row count per scene to the host
+        launch_batch_stage(BatchStage::ActiveFlags, dS, dP(PCells), ns, tot(PCells), s);
+        BNN_CUDA_CHECK(batched_exclusive_scan_u32(dSeg + ns, dP(PScan), ns, tot(PScan), s));
+        launch_batch_gather_rows(dS, ns, dRows, s);
+        BNN_CUDA_CHECK(cudaMemcpyAsync(H + L.rows, dRows, (size_t)ns * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+        return BNN_OK;
+    };
+    {
+        const std::vector<uint64_t> sig = {(uint64_t)(uintptr_t)w.dev, (uint64_t)w.cap, (uint64_t)ns, (uint64_t)shape,
+                                           tot(PAdvect), tot(PAdvFold), tot(PScan), tot(PParticles), tot(PCells),
+                                           tot(PSortLarge), tot(PTiles + (shape < 0 ? 0 : shape)), tot(PExtrap),
+                                           tot(PFill)};
+        r = run_segment(w.seg[0], sig, s, capture, seg1);
+        if(r != BNN_OK) return r;
+    }
     BNN_CUDA_CHECK(cudaStreamSynchronize(s));
     // rows of every scene, then the table again (row arrays may have moved)
     std::vector<BatchSolveItem> items(ns);
@@ -263,7 +315,7 @@ int batch_substep(BatchStepWork& w, bnn_flip* const* hs, int nsIn, int* rc, bnn_
         c.nrows = (int)nrows;
         c.rowCell = h->rowCell; c.rhs = h->rhs; c.diag = h->diag; c.invd = h->invd; c.pressure = h->pressure;
         c.nbr = h->nbr;
-        hP(PRows)[q + 1] = hP(PRows)[q] + cdiv(nrows, 256);
+        hP(PRows)[q + 1] = hP(PRows)[q] + virt_blocks(nrows);
         BatchSolveItem& it = items[q];
         it.w = &h->pcg;
         it.n = (int)nrows;
@@ -283,24 +335,36 @@ int batch_substep(BatchStepWork& w, bnn_flip* const* hs, int nsIn, int* rc, bnn_
     r = pcg_solve_batch_refined(w.pcg, items.data(), ns, s);
     if(r != BNN_OK) return r;
     cudaEventRecord(w.ev[7], s);
-    // ---- projection, extrapolation of the projected faces, CFL maximum
-    launch_batch_stage(BatchStage::FillUpdate, dS, dP(PFill), ns, tot(PFill), s);
-    launch_batch_stage(BatchStage::UpdateU, dS, dP(PUpdU), ns, tot(PUpdU), s);
-    launch_batch_stage(BatchStage::UpdateV, dS, dP(PUpdV), ns, tot(PUpdV), s);
-    launch_batch_stage(BatchStage::UpdateW, dS, dP(PUpdW), ns, tot(PUpdW), s);
-    for(int layer = 0; layer < 4; ++layer)
-        launch_batch_stage(BatchStage::Extrapolate, dS, dP(PExtrap), ns, tot(PExtrap), s, 2, layer);
-    cudaEventRecord(w.ev[8], s);
-    // ---- grid-to-particle transfer + the next sub-step's move
-    launch_batch_stage(BatchStage::BboxReset, dS, nullptr, ns, 0, s);
-    launch_batch_stage(BatchStage::G2PMove, dS, dP(PParticles), ns, tot(PParticles), s);
-    launch_batch_stage(BatchStage::BboxFinal, dS, dP(PMoveFold), ns, tot(PMoveFold), s);
-    cudaEventRecord(w.ev[9], s);
+    // ---- segment 2: projection, extrapolation of the projected faces, CFL maximum, the
+    // grid-to-particle transfer + the next sub-step's move, the scenes' state to the host
     DevState* dState = (DevState*)(D + L.state);
     const DevState* hState = (const DevState*)(H + L.state);
-    launch_batch_gather_state(dS, ns, dState, s);
+    auto seg2 = [&](bool capturing) -> int {
+        auto mark = [&](int k) { capturing ? cudaEventRecordWithFlags(w.ev[k], s, cudaEventRecordExternal)
+                                           : cudaEventRecord(w.ev[k], s); };
+        launch_batch_stage(BatchStage::FillUpdate, dS, dP(PFill), ns, tot(PFill), s);
+        launch_batch_stage(BatchStage::UpdateU, dS, dP(PUpdU), ns, tot(PUpdU), s);
+        launch_batch_stage(BatchStage::UpdateV, dS, dP(PUpdV), ns, tot(PUpdV), s);
+        launch_batch_stage(BatchStage::UpdateW, dS, dP(PUpdW), ns, tot(PUpdW), s);
+        for(int layer = 0; layer < 4; ++layer)
+            launch_batch_stage(BatchStage::Extrapolate, dS, dP(PExtrap), ns, tot(PExtrap), s, 2, layer);
+        mark(8);
+        launch_batch_stage(BatchStage::BboxReset, dS, nullptr, ns, 0, s);
+        launch_batch_stage(BatchStage::G2PMove, dS, dP(PParticles), ns, tot(PParticles), s);
+        launch_batch_stage(BatchStage::BboxFinal, dS, dP(PMoveFold), ns, tot(PMoveFold), s);
+        mark(9);
+        launch_batch_gather_state(dS, ns, dState, s);
+        BNN_CUDA_CHECK(cudaMemcpyAsync(H + L.state, dState, (size_t)ns * sizeof(DevState), cudaMemcpyDeviceToHost, s));
+        return BNN_OK;
+    };
+    {
+        const std::vector<uint64_t> sig = {(uint64_t)(uintptr_t)w.dev, (uint64_t)w.cap, (uint64_t)ns, tot(PFill),
+                                           tot(PUpdU), tot(PUpdV), tot(PUpdW), tot(PExtrap), tot(PParticles),
+                                           tot(PMoveFold)};
+        r = run_segment(w.seg[1], sig, s, w.graphs, seg2);
+        if(r != BNN_OK) return r;
+    }
     BNN_CUDA_CHECK(cudaGetLastError());
-    BNN_CUDA_CHECK(cudaMemcpyAsync(H + L.state, dState, (size_t)ns * sizeof(DevState), cudaMemcpyDeviceToHost, s));
     BNN_CUDA_CHECK(cudaStreamSynchronize(s));
 
     float stage[10] = {};

@@ -3,8 +3,20 @@
 
 #include "flip_handle.cuh"
 
+#include <vector>
+
+// One captured segment of the staged step: replayed while the launch shapes it was
+// captured with (sig) stay the same
+struct StagedGraph {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<uint64_t> sig;
+    long long kernels = 0;     // kernel launches the segment holds
+};
+
 // Device tables, pinned mirror and stream of the batched step, kept between steps
 struct BatchStepWork {
+    bool graphs = true;        // capture the fixed segments of the step in CUDA graphs
+    StagedGraph seg[2];        // before the pressure-row count, after the pressure solve
     int cap = 0;               // scenes the tables hold
     void* dev = nullptr;
     void* host = nullptr;

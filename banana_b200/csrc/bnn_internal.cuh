@@ -121,6 +121,19 @@ __device__ __forceinline__ Blk seg_blk(const unsigned* __restrict__ prefix, int 
     const unsigned b0 = __ldg(prefix + s);
     return Blk{blockIdx.x - b0, __ldg(prefix + s + 1) - b0};
 }
+// Batched element-wise stages give a block kBatchVirt consecutive blocks of the lone
+// launch's layout (virtual blocks), so the cost of finding the scene is paid once per
+// kBatchVirt blocks of work.  f(Blk) runs the lone body for virtual blocks
+// b.x * kBatchVirt + j below `count` (the scene's lone block count), in order.
+constexpr unsigned kBatchVirt = 8;
+template<class F> __device__ __forceinline__ void virtual_blocks(Blk b, unsigned count, F f) {
+#pragma unroll 1
+    for(unsigned j = 0; j < kBatchVirt; ++j) {
+        const unsigned v = b.x * kBatchVirt + j;
+        if(v >= count) break;
+        f(Blk{v, count});
+    }
+}
 
 // ----------------------------------------------------------------------------------
 // Scalar helpers, same semantics as the reference's MathHelpers
@@ -313,6 +326,10 @@ void p2g_tile_args(void* out, const GridDesc& g, const DevState* st, const uint3
                    size_t stride, float* const U[3], uint8_t* const valid[3], float* phi);
 void launch_p2g_sdf_batch(const void* args, const unsigned* const* P, const unsigned* tiles, int ns, uint64_t cells,
                           cudaStream_t s);
+// The shape launch_p2g_sdf_batch will use for such a batch, or -1 while it is untuned (its
+// next call then times every shape and synchronises the stream); also opts every batched
+// shape into its shared memory, so a launch can be captured into a graph
+int p2g_batch_shape(int ns, uint64_t cells);
 // The tile-shape tuner (gather_kernels.cu): force a shape for every launch (-1: tune), the
 // dimensions of a shape, and the table of tuned choices as JSON lines
 int tile_shape_set(int shape);
@@ -424,8 +441,10 @@ void pcg_release(PcgWork& w);
 extern "C" void bnn_set_error(const char* msg);
 
 // Every kernel launch of the library is followed by bnn_note_launch(): the running total
-// is what bnn_launch_count() reports.
+// is what bnn_launch_count() reports.  Launches captured into a CUDA graph are taken back
+// (bnn_note_launches(-k)) and counted again at every replay (bnn_note_launches(k)).
 void bnn_note_launch();
+void bnn_note_launches(long long k);
 
 #define BNN_CUDA_CHECK(expr)                                                                 \
     do {                                                                                     \

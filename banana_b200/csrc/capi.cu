@@ -16,6 +16,7 @@
 static thread_local std::string g_lastError;
 static std::atomic<unsigned long long> g_launches{0};
 void bnn_note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void bnn_note_launches(long long k) { g_launches.fetch_add((unsigned long long)k, std::memory_order_relaxed); }
 extern "C" uint64_t bnn_launch_count(void) { return g_launches.load(); }
 extern "C" void bnn_set_error(const char* msg) { g_lastError = msg ? msg : ""; }
 extern "C" const char* bnn_last_error(void) { return g_lastError.c_str(); }

@@ -206,6 +206,7 @@ __device__ __forceinline__ void bbox_block_partial(int* __restrict__ part, unsig
         part[6 * bx + d] = a;
         part[6 * bx + 3 + d] = b;
     }
+    __syncthreads();  // sm is free again (batched stages call this once per virtual block)
 }
 
 // Folds the per-block boxes into DevState::bbox
@@ -1542,12 +1543,14 @@ __global__ void kb_step_reset(const BScene* __restrict__ S, int ns) {
     if(!S[q].moved)
         for(int d = 0; d < 3; ++d) { st->bbox[d] = INT_MAX; st->bbox[3 + d] = INT_MIN; }
 }
-__global__ void __launch_bounds__(256, 4) kb_advect(const BScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
+__global__ void __launch_bounds__(256, 3) kb_advect(const BScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
     int q;
     const Blk b = seg_blk(P, ns, q);
     const BScene& c = S[q];
-    advect_body(b, c.n, c.p6cur, c.p6cur + c.cap, c.p6cur + 2 * c.cap, c.U[0], c.U[1], c.U[2], c.g, c.sub, c.advSteps,
-                c.cellOf, c.slot, c.count, c.dst, c.bboxPart);
+    virtual_blocks(b, (unsigned)(c.n + 255) / 256, [&](Blk v) {
+        advect_body(v, c.n, c.p6cur, c.p6cur + c.cap, c.p6cur + 2 * c.cap, c.U[0], c.U[1], c.U[2], c.g, c.sub,
+                    c.advSteps, c.cellOf, c.slot, c.count, c.dst, c.bboxPart);
+    });
 }
 // one block per scene: the occupied-cell box from the advection's per-block boxes
 __global__ void __launch_bounds__(256) kb_bbox_final(const BScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
@@ -1560,13 +1563,15 @@ __global__ void kb_scatter_index(const BScene* __restrict__ S, const unsigned* _
     int q;
     const Blk b = seg_blk(P, ns, q);
     const BScene& c = S[q];
-    scatter_index_body(b, c.n, c.cellOf, c.slot, c.cellStart, c.idcur, c.order, c.key);
+    virtual_blocks(b, (unsigned)(c.n + 255) / 256,
+                   [&](Blk v) { scatter_index_body(v, c.n, c.cellOf, c.slot, c.cellStart, c.idcur, c.order, c.key); });
 }
 __global__ void __launch_bounds__(256, 4) kb_sort_buckets(const BScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
     int q;
     const Blk b = seg_blk(P, ns, q);
     const BScene& c = S[q];
-    sort_buckets_body(b, (int)c.C, c.cellStart, c.order, c.key, c.count, c.slot, c.dst);
+    virtual_blocks(b, (unsigned)((c.C + 255) / 256),
+                   [&](Blk v) { sort_buckets_body(v, (int)c.C, c.cellStart, c.order, c.key, c.count, c.slot, c.dst); });
 }
 __global__ void __launch_bounds__(256) kb_sort_large(const BScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
     int q;
@@ -1578,8 +1583,10 @@ __global__ void kb_gather_particles(const BScene* __restrict__ S, const unsigned
     int q;
     const Blk b = seg_blk(P, ns, q);
     const BScene& c = S[q];
-    gather_particles_body(b, c.n, c.order, c.p6cur, c.moved ? c.movedPos : c.p6cur, c.p6nxt, c.idcur, c.idnxt, nullptr,
-                          nullptr, nullptr, c.rec, c.g, c.cap);
+    virtual_blocks(b, (unsigned)(c.n + 255) / 256, [&](Blk v) {
+        gather_particles_body(v, c.n, c.order, c.p6cur, c.moved ? c.movedPos : c.p6cur, c.p6nxt, c.idcur, c.idnxt,
+                              nullptr, nullptr, nullptr, c.rec, c.g, c.cap);
+    });
 }
 // Before the last layer after P2G: the FLIP backup starts at 0 and v at 0 - g dt (the
 // values every face beyond the layer's region keeps; launch_extrapolate mode 1)
@@ -1634,20 +1641,22 @@ __global__ void kb_active_flags(const BScene* __restrict__ S, const unsigned* __
     int q;
     const Blk b = seg_blk(P, ns, q);
     const BScene& c = S[q];
-    active_flags_body(b, c.g, c.phi, c.flag, c.dst);
+    virtual_blocks(b, (unsigned)((c.C + 255) / 256), [&](Blk v) { active_flags_body(v, c.g, c.phi, c.flag, c.dst); });
 }
 __global__ void kb_active_rows(const BScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
     int q;
     const Blk b = seg_blk(P, ns, q);
     const BScene& c = S[q];
-    active_rows_body(b, c.C, c.flag, c.aidx, c.rowCell);
+    virtual_blocks(b, (unsigned)((c.C + 255) / 256), [&](Blk v) { active_rows_body(v, c.C, c.flag, c.aidx, c.rowCell); });
 }
 __global__ void kb_build_rows(const BScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
     int q;
     const Blk b = seg_blk(P, ns, q);
     const BScene& c = S[q];
-    build_rows_body<false>(b, c.g, c.nrows, c.rowCell, c.phi, c.aidx, c.U[0], c.U[1], c.U[2], nullptr, nullptr, nullptr,
-                           c.substep, c.rhs, c.diag, c.invd, c.nbr, nullptr, c.dst);
+    virtual_blocks(b, (unsigned)(c.nrows + 255) / 256, [&](Blk v) {
+        build_rows_body<false>(v, c.g, c.nrows, c.rowCell, c.phi, c.aidx, c.U[0], c.U[1], c.U[2], nullptr, nullptr,
+                               nullptr, c.substep, c.rhs, c.diag, c.invd, c.nbr, nullptr, c.dst);
+    });
 }
 template<int D>
 __global__ void __launch_bounds__(256) kb_update_velocity(const BScene* __restrict__ S, const unsigned* __restrict__ P,
@@ -1666,12 +1675,14 @@ __global__ void kb_bbox_reset(const BScene* __restrict__ S, int ns) {
 }
 // the fused grid-to-particle transfer + next move, on the final velocities of this
 // sub-step (the pass-2 extrapolation leaves them in B)
-__global__ void __launch_bounds__(256, 3) kb_g2p_move(const BScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
+__global__ void __launch_bounds__(256, 2) kb_g2p_move(const BScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
     int q;
     const Blk b = seg_blk(P, ns, q);
     const BScene& c = S[q];
-    g2p_move_body(b, c.n, c.g, c.p6nxt, c.cap, c.B[0], c.B[1], c.B[2], c.O[0], c.O[1], c.O[2], c.ratio, c.ns, c.movedPos,
-                  c.cellOf, c.slot, c.count, c.dst, c.bboxPart);
+    virtual_blocks(b, (unsigned)(c.n + 255) / 256, [&](Blk v) {
+        g2p_move_body(v, c.n, c.g, c.p6nxt, c.cap, c.B[0], c.B[1], c.B[2], c.O[0], c.O[1], c.O[2], c.ratio, c.ns,
+                      c.movedPos, c.cellOf, c.slot, c.count, c.dst, c.bboxPart);
+    });
 }
 // one thread per scene: its pressure rows (the active-cell numbering's total)
 __global__ void kb_gather_rows(const BScene* __restrict__ S, int ns, unsigned* __restrict__ out) {

@@ -606,12 +606,24 @@ void p2g_tile_args(void* out, const GridDesc& g, const DevState* st, const uint3
 }
 // The batch's P2G + SDF pass: P[shape] is the tile prefix of the scenes in that shape,
 // tiles[shape] its total (host copy); tuned per batch kind like a lone scene's pass
-void launch_p2g_sdf_batch(const void* args, const unsigned* const* P, const unsigned* tiles, int ns, uint64_t cells,
-                          cudaStream_t s) {
+static uint64_t batch_key(int ns, uint64_t cells) {
     int dev = 0;
     cudaGetDevice(&dev);
-    const uint64_t key = ((uint64_t)(dev & 0xff) << 56) | (1ull << 48) | (log2_bucket((uint64_t)ns) << 24) |
-                         log2_bucket(cells);
+    return ((uint64_t)(dev & 0xff) << 56) | (1ull << 48) | (log2_bucket((uint64_t)ns) << 24) | log2_bucket(cells);
+}
+int p2g_batch_shape(int ns, uint64_t cells) {
+    static std::atomic<uint64_t> c0{0}, c1{0}, c2{0}, c3{0}, c4{0}, c5{0};
+    opt_in_smem(kb_p2g_sdf_tile<S0>, S0::kSmemBytes, c0);
+    opt_in_smem(kb_p2g_sdf_tile<S1>, S1::kSmemBytes, c1);
+    opt_in_smem(kb_p2g_sdf_tile<S2>, S2::kSmemBytes, c2);
+    opt_in_smem(kb_p2g_sdf_tile<S3>, S3::kSmemBytes, c3);
+    opt_in_smem(kb_p2g_sdf_tile<S4>, S4::kSmemBytes, c4);
+    opt_in_smem(kb_p2g_sdf_tile<S5>, S5::kSmemBytes, c5);
+    return lookup(batch_key(ns, cells));
+}
+void launch_p2g_sdf_batch(const void* args, const unsigned* const* P, const unsigned* tiles, int ns, uint64_t cells,
+                          cudaStream_t s) {
+    const uint64_t key = batch_key(ns, cells);
     const TileArgs* A = (const TileArgs*)args;
     int shape = lookup(key);
     if(shape < 0) shape = tune(key, s, [&](int v) { launch_batch_shape(v, A, P[v], ns, tiles[v], s); });

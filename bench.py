@@ -494,9 +494,12 @@ def run_batch(args, ws, rank, local):
         t = time.perf_counter() - t
         bo.close()
         return pso / t, t * 1e3 / n_steps
-    seq_value, seq_ms = other_mode(1, capi.BATCH_PER_SCENE)
-    pool_value, pool_ms = (other_mode(args.workers, capi.BATCH_PER_SCENE) if mode == capi.BATCH_STAGED
-                           else (ps / te, te * 1e3 / args.steps))
+    if args.no_compare:
+        seq_value = seq_ms = pool_value = pool_ms = None
+    else:
+        seq_value, seq_ms = other_mode(1, capi.BATCH_PER_SCENE)
+        pool_value, pool_ms = (other_mode(args.workers, capi.BATCH_PER_SCENE) if mode == capi.BATCH_STAGED
+                               else (ps / te, te * 1e3 / args.steps))
     tot_ps = ps
     t_max = te
     e2e_t = te + t_up + t_dl
@@ -531,7 +534,7 @@ def run_batch(args, ws, rank, local):
                                                    "note": "rank 0's scenes, one worker thread, same accuracy"},
                            "per_scene_streams": {"value": pool_value, "ms_per_step": pool_ms,
                                                  "note": "rank 0's scenes, each on its own stream from the worker pool"},
-                           "batched_over_one_at_a_time": (ps / te) / seq_value}}
+                           "batched_over_one_at_a_time": (ps / te) / seq_value if seq_value else None}}
         print(json.dumps(line), flush=True)
     if ws > 1:
         dist.destroy_process_group()
@@ -915,6 +918,8 @@ def main():
     ap.add_argument("--tol", type=float, default=None,
                     help="fp32 / fp64 PCG: relative tolerance (the refined mode's outer tolerance is 1e-8)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="batch: skip the one-at-a-time and per-scene-stream comparison runs")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--grid", type=int, default=N_GRID, help="fluid-domain resolution (profiling of smaller cases)")
     ap.add_argument("--ref-precond", choices=["jacobi", "ic0"], default="jacobi",

@@ -183,10 +183,13 @@ typedef struct bnn_batch bnn_batch;
  * for every scene exactly what bnn_flip_step computes for it alone. */
 #define BNN_BATCH_STAGED    0
 #define BNN_BATCH_PER_SCENE 1
+/* OR-ed into BNN_BATCH_STAGED: launch the staged step's kernels one by one instead of
+ * replaying the CUDA graphs captured from them (same kernels, same results) */
+#define BNN_BATCH_NO_GRAPHS 0x100
 typedef struct bnn_batch_params {
     uint64_t hbm_budget_bytes; /* admission budget over bnn_scene_bytes_estimate; 0 = none */
     uint32_t worker_threads;   /* host threads stepping scenes; 0 = min(16, cores) */
-    uint32_t step_mode;        /* BNN_BATCH_STAGED or BNN_BATCH_PER_SCENE */
+    uint32_t step_mode;        /* BNN_BATCH_STAGED (optionally | BNN_BATCH_NO_GRAPHS) or BNN_BATCH_PER_SCENE */
 } bnn_batch_params;
 typedef struct bnn_batch_stats {
     uint32_t scenes;           /* scenes stepped */

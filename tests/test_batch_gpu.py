@@ -28,10 +28,12 @@ def _lone(bnn, spec, steps, **over):
     return out
 
 
-@pytest.mark.parametrize("mode", ["staged", "per_scene"])
+@pytest.mark.parametrize("mode", ["staged", "staged_no_graphs", "per_scene"])
 def test_batch_scenes_equal_lone_solvers(bnn, mode):
-    staged = mode == "staged"
-    b = bnn.FlipBatch(worker_threads=3, step_mode=bnn.capi.BATCH_STAGED if staged else bnn.capi.BATCH_PER_SCENE)
+    staged = mode.startswith("staged")
+    step_mode = {"staged": bnn.capi.BATCH_STAGED, "per_scene": bnn.capi.BATCH_PER_SCENE,
+                 "staged_no_graphs": bnn.capi.BATCH_STAGED | bnn.capi.BATCH_NO_GRAPHS}[mode]
+    b = bnn.FlipBatch(worker_threads=3, step_mode=step_mode)
     ids = {}
     for q in range(3):
         cfg, pos, vel = scenes.batch_scene(SPECS[q])
