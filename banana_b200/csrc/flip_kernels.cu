@@ -1675,14 +1675,12 @@ __global__ void kb_bbox_reset(const BScene* __restrict__ S, int ns) {
 }
 // the fused grid-to-particle transfer + next move, on the final velocities of this
 // sub-step (the pass-2 extrapolation leaves them in B)
-__global__ void __launch_bounds__(256, 2) kb_g2p_move(const BScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
+__global__ void __launch_bounds__(256, 3) kb_g2p_move(const BScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
     int q;
     const Blk b = seg_blk(P, ns, q);
     const BScene& c = S[q];
-    virtual_blocks(b, (unsigned)(c.n + 255) / 256, [&](Blk v) {
-        g2p_move_body(v, c.n, c.g, c.p6nxt, c.cap, c.B[0], c.B[1], c.B[2], c.O[0], c.O[1], c.O[2], c.ratio, c.ns,
-                      c.movedPos, c.cellOf, c.slot, c.count, c.dst, c.bboxPart);
-    });
+    g2p_move_body(b, c.n, c.g, c.p6nxt, c.cap, c.B[0], c.B[1], c.B[2], c.O[0], c.O[1], c.O[2], c.ratio, c.ns, c.movedPos,
+                  c.cellOf, c.slot, c.count, c.dst, c.bboxPart);
 }
 // one thread per scene: its pressure rows (the active-cell numbering's total)
 __global__ void kb_gather_rows(const BScene* __restrict__ S, int ns, unsigned* __restrict__ out) {

@@ -223,7 +223,7 @@ int bnn_batch_memory(bnn_batch* b, uint64_t* admitted, uint64_t* held);
  * (fixed per-cell and per-face summation orders).  By default a tuner times every shape the
  * first time it meets a kind of launch (a lone scene's resolution bucket, ceil((G + 1) / 32)
  * cells per axis; a batch's scene count and total cells, in powers of two) and keeps the
- * fastest.  No counterpart in the reference (its P2G is a serial loop, FLIP_Solver.cpp:57-95). */
+ * fastest (the default shape 0 unless another is 3% faster).  No counterpart in the reference (its P2G is a serial loop, FLIP_Solver.cpp:57-95). */
 /* Number of shapes; tz[i], yc[i] of each (arrays of at least `cap` entries, may be NULL). */
 int bnn_tile_shapes(int32_t* tz, int32_t* yc, int32_t cap);
 /* Use shape `shape` (0 .. bnn_tile_shapes() - 1) for every launch of the process, or -1 to

@@ -20,7 +20,20 @@ def test_served_requests_equal_lone_runs(bnn):
     # room for the two largest at once, not for all four: later requests wait for memory
     budget = sorted(est)[-1] + sorted(est)[-2] + 1
     batch = bnn.FlipBatch(hbm_budget_bytes=budget, worker_threads=2)
-    srv = SceneServer(batch)
+
+    # the server's clock advances 10 ms per batch step, so arrivals meet the same running
+    # set whatever the GPU's speed: requests 2 and 3 arrive while 0 and 1 still run
+    now = [0.0]
+
+    class Ticking:
+        def __getattr__(self, name):
+            return getattr(batch, name)
+
+        def step(self):
+            now[0] += 0.01
+            return batch.step()
+
+    srv = SceneServer(Ticking(), clock=lambda: now[0])
     reqs = [Request(k, cfg, pos, vel, steps[k], arrival=0.0 if k < 2 else 0.01 * k)
             for k, (cfg, pos, vel) in enumerate(built)]
     results = {r.rid: r for r in srv.run(reqs, time_limit=120.0)}

@@ -1,6 +1,6 @@
 """Tile shapes of the FLIP P2G + fluid SDF pass: every shape gives the same bits (lone
-scenes and the staged batch), and the tuner records a choice per launch kind that is the
-fastest shape it timed."""
+scenes and the staged batch), and the tuner records a choice per launch kind: the fastest
+shape it timed, or the default when none beats it by 3%."""
 import numpy as np
 import pytest
 
@@ -80,4 +80,9 @@ def test_tuner_records_the_fastest_shape(bnn, shapes):
     assert len(rows) == 1, bnn.capi.tile_tuning()
     r = rows[0]
     assert len(r["us"]) == len(shapes) and all(t > 0 for t in r["us"])
-    assert r["us"][r["shape"]] == min(r["us"]) and (r["tz"], r["yc"]) == shapes[r["shape"]]
+    assert (r["tz"], r["yc"]) == shapes[r["shape"]]
+    # the fastest shape, unless it is within 3% of the default's time
+    if r["shape"] == 0:
+        assert min(r["us"]) >= 0.97 * r["us"][0] * (1 - 1e-6)
+    else:
+        assert r["us"][r["shape"]] == min(r["us"]) and r["us"][r["shape"]] < 0.97 * r["us"][0]
