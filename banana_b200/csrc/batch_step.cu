@@ -54,8 +54,9 @@ inline unsigned region_blocks(unsigned tiles) { return std::min(kRegionBlocks, s
 inline unsigned virt_blocks(size_t n) { return cdiv(cdiv(n, 256), kBatchVirt); }
 
 // Prefix arrays of the step (cap + 1 entries each), in upload order
-enum Pre { PAdvect, PAdvFold, PParticles, PMoveFold, PCells, PSortLarge, PScan, PExtrap, PFill, PUpdU, PUpdV, PUpdW,
-           PRows, PTiles, kPre = PTiles + kTileShapes };  // PTiles + k: tiles in tile shape k
+// (PParticles, PCells, PRows: kBatchVirt lone blocks per batched block; PMove: one)
+enum Pre { PAdvect, PAdvFold, PParticles, PMove, PMoveFold, PCells, PSortLarge, PScan, PExtrap, PFill, PUpdU, PUpdV,
+           PUpdW, PRows, PTiles, kPre = PTiles + kTileShapes };  // PTiles + k: tiles in tile shape k
 
 struct Layout {
     size_t scenes, args, segs, pre, rows, state, up, total;
@@ -237,6 +238,7 @@ int batch_substep(BatchStepWork& w, bnn_flip* const* hs, int nsIn, int* rc, bnn_
             moved ? 0u : pb,                                   // PAdvect
             moved ? 0u : bbox_fold_blocks(c.n),                // PAdvFold
             pb,                                                // PParticles
+            cdiv((size_t)c.n, 256),                            // PMove
             bbox_fold_blocks(c.n),                             // PMoveFold
             virt_blocks(h->C),                                 // PCells
             c.n > 16 ? std::min(296u, std::max(2u, cdiv((size_t)c.n, 65536))) : 0u,  // PSortLarge
@@ -350,7 +352,7 @@ int batch_substep(BatchStepWork& w, bnn_flip* const* hs, int nsIn, int* rc, bnn_
             launch_batch_stage(BatchStage::Extrapolate, dS, dP(PExtrap), ns, tot(PExtrap), s, 2, layer);
         mark(8);
         launch_batch_stage(BatchStage::BboxReset, dS, nullptr, ns, 0, s);
-        launch_batch_stage(BatchStage::G2PMove, dS, dP(PParticles), ns, tot(PParticles), s);
+        launch_batch_stage(BatchStage::G2PMove, dS, dP(PMove), ns, tot(PMove), s);
         launch_batch_stage(BatchStage::BboxFinal, dS, dP(PMoveFold), ns, tot(PMoveFold), s);
         mark(9);
         launch_batch_gather_state(dS, ns, dState, s);
@@ -359,7 +361,7 @@ int batch_substep(BatchStepWork& w, bnn_flip* const* hs, int nsIn, int* rc, bnn_
     };
     {
         const std::vector<uint64_t> sig = {(uint64_t)(uintptr_t)w.dev, (uint64_t)w.cap, (uint64_t)ns, tot(PFill),
-                                           tot(PUpdU), tot(PUpdV), tot(PUpdW), tot(PExtrap), tot(PParticles),
+                                           tot(PUpdU), tot(PUpdV), tot(PUpdW), tot(PExtrap), tot(PMove),
                                            tot(PMoveFold)};
         r = run_segment(w.seg[1], sig, s, w.graphs, seg2);
         if(r != BNN_OK) return r;

@@ -975,10 +975,17 @@ __global__ void __launch_bounds__(kLanes, cg1_min_blocks<VT>()) k_pcg_cg1(Cg1Arg
 // counter of unfinished scenes (decremented by the block owning a scene's first chunk)
 // reads 0 right after the first barrier of an iteration -- no scene can finish between
 // the last decrement before that barrier and the read.
+// Yield: a second counter holds the chunks of the unfinished scenes.  When it has fallen to
+// yieldBelow (read at the same point), every block leaves at the end of that iteration and
+// the owner of each unfinished scene saves its scalars (iterations, rho, beta, tol, last
+// residual) to the scene's DevState; the host launches the unfinished scenes again with
+// resume set, spread over the whole grid, and they carry on with exactly the iterates they
+// had.  Which of the s buffers is the new one follows from the iteration count (even: s0).
 // ---------------------------------------------------------------------------------
 constexpr int kBatchSlots = 64;  // scenes a block's chunk range may touch
 struct BatchPcgScene {
     int n;                     // rows
+    int resume;                // carry on from the scalars saved at a yield
     const float* rhsF;
     const float* invd;
     const int4* rec;
@@ -998,6 +1005,8 @@ struct BatchPcgArgs {
     unsigned perBlock;         // chunks per block
     GridSync* gs;
     unsigned* remaining;       // unfinished scenes
+    unsigned* active;          // chunks of the unfinished scenes
+    unsigned yieldBelow;       // leave when active has fallen to this (0: never)
     unsigned* flags;           // BNN_FLAG_TIMEOUT
 };
 
@@ -1020,6 +1029,10 @@ __global__ void __launch_bounds__(kLanes, pcg_min_blocks<float, false>()) k_pcg_
     // scenes is read right after the first barrier of an iteration, so it may only change
     // between the second barrier and the next first one: a scene finishing between the two
     // (deferred) is counted off after the second.
+    auto count_off = [&](int s) {
+        atomicSub(a.remaining, 1u);
+        atomicSub(a.active, __ldg(a.cp + s + 1) - __ldg(a.cp + s));
+    };
     auto finish = [&](int j, unsigned success, bool deferred) {
         const int s = sFirst + j;
         sState[j] = deferred ? 3 : 1;
@@ -1030,14 +1043,15 @@ __global__ void __launch_bounds__(kLanes, pcg_min_blocks<float, false>()) k_pcg_
             d->done = 1;
             d->resid = sResid[j];
             d->resid64 = sResid[j];
-            if(!deferred) atomicSub(a.remaining, 1u);
+            if(!deferred) count_off(s);
         }
     };
 
-    // ---- init: r = rhs, x = 0, z = D^-1 r; partial z.r and max|r|
+    // ---- init: r = rhs, x = 0, z = D^-1 r; partial z.r and max|r| (not for a resumed scene)
     for(unsigned c = c0; c < c1; ++c) {
         const int s = seg_of(a.cp, a.ns, c);
         const BatchPcgScene& S = a.sc[s];
+        if(S.resume) continue;
         const int n = S.n;
         const unsigned lc = c - __ldg(a.cp + s);
         double acc = 0.0;
@@ -1067,6 +1081,16 @@ __global__ void __launch_bounds__(kLanes, pcg_min_blocks<float, false>()) k_pcg_
         const int s = sFirst + j;
         const BatchPcgScene& S = a.sc[s];
         const int nch = (int)(__ldg(a.cp + s + 1) - __ldg(a.cp + s));
+        if(S.resume) {
+            // the scalars saved at the yield
+            if(threadIdx.x == 0) {
+                const DevState* d = S.dst;
+                sIter[j] = d->iter; sRho[j] = d->rho; sBeta[j] = d->beta; sTol[j] = d->tol; sResid[j] = d->resid;
+                sState[j] = 0;
+            }
+            __syncthreads();
+            continue;
+        }
         if(threadIdx.x == 0) { sIter[j] = 0; sState[j] = nch > 0 ? 0 : 2; sBeta[j] = 0.f; }
         __syncthreads();
         if(nch == 0) continue;
@@ -1085,8 +1109,8 @@ __global__ void __launch_bounds__(kLanes, pcg_min_blocks<float, false>()) k_pcg_
         __syncthreads();
     }
 
-    bool first = true;
-    int parity = 0;  // s0 new / s1 old on even iterations, as the lone solve's swap
+    // a scene's new s is s0 after an even number of iterations, as the lone solve's swap;
+    // its first iteration (no s yet) is the one with 0 iterations done
     for(;;) {
         // ---- phase A: s = z + beta s_old, q = A s, partial s.q
         for(unsigned c = c0; c < c1; ++c) {
@@ -1099,6 +1123,8 @@ __global__ void __launch_bounds__(kLanes, pcg_min_blocks<float, false>()) k_pcg_
             const float beta = sBeta[jslot];
             const float negoff = S.negoff;
             const float* __restrict__ zR = S.z;
+            const bool parity = (sIter[jslot] & 1u) != 0;
+            const bool first = sIter[jslot] == 0;
             const float* __restrict__ sOld = parity ? S.s0 : S.s1;
             float* __restrict__ sNew = parity ? S.s1 : S.s0;
             const size_t base = (size_t)lc * kChunk + threadIdx.x;
@@ -1176,6 +1202,7 @@ __global__ void __launch_bounds__(kLanes, pcg_min_blocks<float, false>()) k_pcg_
         }
         if(!grid_barrier(a.gs, nb, sense, a.flags, solve_barrier_limit())) return;
         if(ld_acquire_u32(a.remaining) == 0u) break;
+        const bool yieldNow = a.yieldBelow != 0u && ld_acquire_u32(a.active) <= a.yieldBelow;
         // alpha of every scene this block works on
         for(int j = 0; j < nslots; ++j) {
             if(sState[j] != 0) continue;
@@ -1203,7 +1230,7 @@ __global__ void __launch_bounds__(kLanes, pcg_min_blocks<float, false>()) k_pcg_
             const int n = S.n;
             const unsigned lc = c - __ldg(a.cp + s);
             const float alpha = sAlpha[jslot];
-            const float* __restrict__ sNew = parity ? S.s1 : S.s0;
+            const float* __restrict__ sNew = (sIter[jslot] & 1u) ? S.s1 : S.s0;
             const size_t base = (size_t)lc * kChunk + threadIdx.x;
             float xs[kPerLane], ss[kPerLane], rs[kPerLane], qs[kPerLane], is[kPerLane];
 #pragma unroll
@@ -1240,7 +1267,7 @@ __global__ void __launch_bounds__(kLanes, pcg_min_blocks<float, false>()) k_pcg_
         if(!grid_barrier(a.gs, nb, sense, a.flags, solve_barrier_limit())) return;
         for(int j = 0; j < nslots; ++j) {
             if(sState[j] == 3) {
-                if(threadIdx.x == 0 && __ldg(a.cp + sFirst + j) >= c0) atomicSub(a.remaining, 1u);
+                if(threadIdx.x == 0 && __ldg(a.cp + sFirst + j) >= c0) count_off(sFirst + j);
                 __syncthreads();
                 if(threadIdx.x == 0) sState[j] = 1;
                 __syncthreads();
@@ -1269,8 +1296,17 @@ __global__ void __launch_bounds__(kLanes, pcg_min_blocks<float, false>()) k_pcg_
             }
             __syncthreads();
         }
-        parity ^= 1;
-        first = false;
+        if(yieldNow) {
+            // every block leaves here; each unfinished scene's owner saves its scalars
+            for(int j = 0; j < nslots; ++j) {
+                const int s = sFirst + j;
+                if(sState[j] != 0 || threadIdx.x != 0 || __ldg(a.cp + s) < c0) continue;
+                DevState* d = a.sc[s].dst;
+                d->iter = sIter[j]; d->rho = sRho[j]; d->beta = sBeta[j]; d->tol = sTol[j]; d->resid = sResid[j];
+                d->done = 0;
+            }
+            return;
+        }
     }
 }
 
@@ -1676,14 +1712,14 @@ struct IrScene {
 };
 struct IrReport {
     double res, bmax;
-    unsigned iter, flags;
+    unsigned iter, flags, done, pad;
 };
-// Uploaded with every round's tables: the barrier word and the unfinished-scene counter
+// Uploaded with every launch's tables: the barrier word and the unfinished-scene counters
 struct BatchHeader {
     GridSync gs;
     unsigned remaining;
     unsigned flags;
-    unsigned pad;
+    unsigned active;
 };
 
 __global__ void kb_pack_rows(const IrScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
@@ -1746,9 +1782,9 @@ __global__ void kb_ir_report(const IrScene* __restrict__ S, int ns, const BatchH
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if(q < ns) {
         const DevState* st = S[q].st;
-        out[q] = IrReport{st->outer_res, st->outer_bmax, st->iter, st->flags};
+        out[q] = IrReport{st->outer_res, st->outer_bmax, st->iter, st->flags, st->done, 0u};
     }
-    if(q == 0) out[ns] = IrReport{0.0, 0.0, 0u, hdr->flags};
+    if(q == 0) out[ns] = IrReport{0.0, 0.0, 0u, hdr->flags, 0u, 0u};
 }
 
 namespace {
@@ -1829,9 +1865,9 @@ int pcg_solve_batch_refined(BatchPcgCtx& ctx, BatchSolveItem* items, int count, 
     BatchHeader* dh = (BatchHeader*)(D + L.hdr);
     IrReport* drep = (IrReport*)(D + L.rep);
 
-    // this round's tables for the scenes `set` (positions in items), uploaded in one copy
-    auto upload = [&](const std::vector<int>& set) -> cudaError_t {
-        *hh = BatchHeader{GridSync{0u}, (unsigned)set.size(), 0u, 0u};
+    // tables for the scenes `set` (positions in items), uploaded in one copy; resume: the
+    // inner solves carry on from a yield
+    auto upload = [&](const std::vector<int>& set, bool resume = false) -> cudaError_t {
         hp256[0] = hpch[0] = 0;
         for(size_t k = 0; k < set.size(); ++k) {
             const BatchSolveItem& it = items[set[k]];
@@ -1844,9 +1880,11 @@ int pcg_solve_batch_refined(BatchPcgCtx& ctx, BatchSolveItem* items, int count, 
             b.tolFactor = it.innerTol; b.maxIter = it.maxIter; b.x = w.d32; b.r = w.r; b.z = w.z; b.s0 = w.s0;
             b.s1 = w.s1; b.q = w.q; b.part0 = w.part; b.part1 = w.part + w.nchCap;
             b.part2 = w.part + 2 * (size_t)w.nchCap; b.partMax = w.partMaxF; b.dst = it.dst;
+            b.resume = resume ? 1 : 0;
             hp256[k + 1] = hp256[k] + (unsigned)((n + 255) / 256);
             hpch[k + 1] = hpch[k] + (unsigned)((n + kChunk - 1) / kChunk);
         }
+        *hh = BatchHeader{GridSync{0u}, (unsigned)set.size(), 0u, hpch[set.size()]};
         return cudaMemcpyAsync(D, H, L.up, cudaMemcpyHostToDevice, s);
     };
     auto report = [&](int ns) -> int {
@@ -1903,44 +1941,67 @@ int pcg_solve_batch_refined(BatchPcgCtx& ctx, BatchSolveItem* items, int count, 
         const int ns = (int)set.size();
         BNN_CUDA_CHECK(upload(set));
         { kb_ir_to_f32<<<hp256[ns], 256, 0, s>>>(dirs, dp256, ns); bnn_note_launch(); }
-        const unsigned total = hpch[ns];
-        const unsigned capB = (unsigned)(numSM * perSMv);
-        const unsigned perBlock = (total + capB - 1) / capB;
-        const unsigned grid = (total + perBlock - 1) / perBlock;
-        // every block's chunk range must meet at most kBatchSlots scenes
-        for(unsigned b = 0, k = 0; b < grid; ++b) {
-            const unsigned c0 = b * perBlock, c1 = std::min(c0 + perBlock, total);
-            while(hpch[k + 1] <= c0) ++k;
-            unsigned k1 = k;
-            while(hpch[k1 + 1] < c1) ++k1;
-            if(k1 - k + 1 > (unsigned)kBatchSlots) {
-                bnn_set_error("batched PCG: too many scenes per block");
-                return BNN_ERR_CAPACITY;
+        // the inner solves: launched over the whole grid, again for the scenes still
+        // iterating whenever their chunks have fallen to half of a launch's
+        float ms = 0.f;
+        {
+            std::vector<int> part = set;
+            bool resume = false;
+            for(;;) {
+                const int np = (int)part.size();
+                const unsigned total = hpch[np];
+                const unsigned capB = (unsigned)(numSM * perSMv);
+                const unsigned perBlock = (total + capB - 1) / capB;
+                const unsigned grid = (total + perBlock - 1) / perBlock;
+                // every block's chunk range must meet at most kBatchSlots scenes
+                for(unsigned b = 0, k = 0; b < grid; ++b) {
+                    const unsigned c0 = b * perBlock, c1 = std::min(c0 + perBlock, total);
+                    while(hpch[k + 1] <= c0) ++k;
+                    unsigned k1 = k;
+                    while(hpch[k1 + 1] < c1) ++k1;
+                    if(k1 - k + 1 > (unsigned)kBatchSlots) {
+                        bnn_set_error("batched PCG: too many scenes per block");
+                        return BNN_ERR_CAPACITY;
+                    }
+                }
+                BatchPcgArgs a;
+                a.sc = (const BatchPcgScene*)(D + L.bps);
+                a.cp = dpch;
+                a.ns = np;
+                a.total = total;
+                a.perBlock = perBlock;
+                a.gs = &dh->gs;
+                a.remaining = &dh->remaining;
+                a.active = &dh->active;
+                a.yieldBelow = perBlock > 1 ? total / 2 : 0u;
+                a.flags = &dh->flags;
+                void* args[] = {(void*)&a};
+                {
+                    CoopShare share(grid * (kShareUnits / perSMv), numSM * kShareUnits);
+                    BNN_CUDA_CHECK(cudaEventRecord(ctx.ev[0], s));
+                    BNN_CUDA_CHECK(cudaLaunchCooperativeKernel((const void*)k_pcg_batch, dim3(grid), dim3(kLanes), args, 0, s));
+                    bnn_note_launch();
+                    BNN_CUDA_CHECK(cudaEventRecord(ctx.ev[1], s));
+                    rc = report(np);
+                    if(rc != BNN_OK) return rc;
+                }
+                float lm = 0.f;
+                cudaEventElapsedTime(&lm, ctx.ev[0], ctx.ev[1]);
+                ms += lm;
+                std::vector<int> left;
+                for(int k = 0; k < np; ++k)
+                    if(!hrep[k].done) left.push_back(part[k]);
+                if(left.empty()) break;
+                part.swap(left);
+                resume = true;
+                BNN_CUDA_CHECK(upload(part, resume));
             }
         }
-        BatchPcgArgs a;
-        a.sc = (const BatchPcgScene*)(D + L.bps);
-        a.cp = dpch;
-        a.ns = ns;
-        a.total = total;
-        a.perBlock = perBlock;
-        a.gs = &dh->gs;
-        a.remaining = &dh->remaining;
-        a.flags = &dh->flags;
-        void* args[] = {(void*)&a};
-        {
-            CoopShare share(grid * (kShareUnits / perSMv), numSM * kShareUnits);
-            BNN_CUDA_CHECK(cudaEventRecord(ctx.ev[0], s));
-            BNN_CUDA_CHECK(cudaLaunchCooperativeKernel((const void*)k_pcg_batch, dim3(grid), dim3(kLanes), args, 0, s));
-            bnn_note_launch();
-            BNN_CUDA_CHECK(cudaEventRecord(ctx.ev[1], s));
-            { kb_ir_accumulate<<<hp256[ns], 256, 0, s>>>(dirs, dp256, ns); bnn_note_launch(); }
-            { kb_ir_residual<<<total, kLanes, 0, s>>>(dirs, dpch, ns); bnn_note_launch(); }
-            rc = report(ns);
-            if(rc != BNN_OK) return rc;
-        }
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, ctx.ev[0], ctx.ev[1]);
+        BNN_CUDA_CHECK(upload(set));
+        { kb_ir_accumulate<<<hp256[ns], 256, 0, s>>>(dirs, dp256, ns); bnn_note_launch(); }
+        { kb_ir_residual<<<hpch[ns], kLanes, 0, s>>>(dirs, dpch, ns); bnn_note_launch(); }
+        rc = report(ns);
+        if(rc != BNN_OK) return rc;
         for(int k = 0; k < ns; ++k) {
             Outer& e = o[set[k]];
             e.total += hrep[k].iter;
