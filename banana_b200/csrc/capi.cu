@@ -635,8 +635,9 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st, const HostIo* io = nullp
     // PIC_Solver leaves the particle velocities alone (no grid-to-particle transfer).  FLIP
     // steps driven from device-resident particles also move the particles for the next
     // sub-step here (k_g2p_move); a step on caller arrays (bnn_flip_step_host) does not,
-    // since the next call brings new particle data.
-    const bool fuse = kind == BNN_SOLVER_FLIP && n > 0 && !io && h->moved;
+    // since the next call brings new particle data, and neither does a scene with dynamic
+    // boundary objects, which are moved (bnn_flip_set_boundaries) before every sub-step.
+    const bool fuse = kind == BNN_SOLVER_FLIP && n > 0 && !io && h->moved && !h->gridBoundary;
     if(fuse) {
         NextStep ns;
         ns.frameTime = h->frameTime + substep;

@@ -414,6 +414,12 @@ def run_ours(args, ws, rank, local):
                        "stage_ms_per_step": {k: v / args.steps for k, v in stage_tot.items()},
                        "stage_gbs": stage_gbs},
         }
+        if args.per_step:
+            # every timed sub-step (numbered from 1 over the whole run, warm-up included)
+            line["detail"]["per_step"] = [
+                {"step": args.warmup + i + 1, "dt": s["dt"], "pcg_iterations": s["pcg_iterations"],
+                 "n_active": s["n_active"], "stage_ms": {k: round(v, 4) for k, v in s["stage_ms"].items()}}
+                for i, s in enumerate(stats)]
         print(json.dumps(line), flush=True)
     solver.close()
     if ws > 1:
@@ -918,6 +924,8 @@ def main():
     ap.add_argument("--tol", type=float, default=None,
                     help="fp32 / fp64 PCG: relative tolerance (the refined mode's outer tolerance is 1e-8)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--per-step", action="store_true",
+                    help="flip: add every timed sub-step's stage times to the line (detail.per_step)")
     ap.add_argument("--no-compare", action="store_true",
                     help="batch: skip the one-at-a-time and per-scene-stream comparison runs")
     ap.add_argument("--skip-e2e", action="store_true")
