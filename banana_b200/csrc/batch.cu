@@ -93,16 +93,19 @@ static Scene* find_scene(bnn_batch* b, uint32_t id) {
 extern "C" int bnn_batch_create(const bnn_batch_params* params, bnn_batch** out) {
     if(!out) return BNN_ERR_INVALID_ARGUMENT;
     *out = nullptr;
-    auto* b = new bnn_batch();
-    BNN_CUDA_CHECK(cudaGetDevice(&b->device));
-    b->budget = params ? params->hbm_budget_bytes : 0;
     const uint32_t mode = params ? params->step_mode : BNN_BATCH_STAGED;
-    b->mode = mode & 0xffu;
-    b->staged.graphs = (mode & BNN_BATCH_NO_GRAPHS) == 0;
-    if((b->mode != BNN_BATCH_STAGED && b->mode != BNN_BATCH_PER_SCENE) || (mode & ~(0xffu | BNN_BATCH_NO_GRAPHS))) {
-        delete b;
+    if(((mode & 0xffu) != BNN_BATCH_STAGED && (mode & 0xffu) != BNN_BATCH_PER_SCENE) ||
+       (mode & ~(0xffu | BNN_BATCH_NO_GRAPHS))) {
+        bnn_set_error("bnn_batch_create: unknown step_mode");
         return BNN_ERR_INVALID_ARGUMENT;
     }
+    int device = 0;
+    BNN_CUDA_CHECK(cudaGetDevice(&device));
+    auto* b = new bnn_batch();
+    b->device = device;
+    b->budget = params ? params->hbm_budget_bytes : 0;
+    b->mode = mode & 0xffu;
+    b->staged.graphs = (mode & BNN_BATCH_NO_GRAPHS) == 0;
     int nw = params && params->worker_threads ? (int)params->worker_threads : 0;
     if(nw <= 0) {
         const unsigned hc = std::thread::hardware_concurrency();

@@ -128,8 +128,11 @@ __device__ __forceinline__ void cell_partials(const TileArgs& a, int x0, int z0,
         const size_t c = ((size_t)cz * a.g.G[1] + cy) * a.g.G[0] + cx;
         const uint32_t b = __ldg(a.cellStart + c), e = __ldg(a.cellStart + c + 1);
         const float4* __restrict__ recD = a.rec + (size_t)D * a.stride;
+        // the next record is loaded while this one is summed
+        float4 Ln = b < e ? __ldg(recD + b) : make_float4(0.f, 0.f, 0.f, 0.f);
         for(uint32_t q = b; q < e; ++q) {
-            const float4 L = __ldg(recD + q);
+            const float4 L = Ln;
+            if(q + 1 < e) Ln = __ldg(recD + q + 1);
             float wx[NX], wy[NY], wz[NZ];
             if constexpr(D == 0) own_axis(L.x, wx); else side_axis(L.x, wx);
             if constexpr(D == 1) own_axis(L.y, wy); else side_axis(L.y, wy);
@@ -209,8 +212,10 @@ __device__ __forceinline__ void sdf_partials(const TileArgs& a, int x0, int z0, 
             sy[o] = ((float)(cy - 1 + o) + 0.5f) * g.dx + g.bmin[1];
             sz[o] = ((float)(cz - 1 + o) + 0.5f) * g.dx + g.bmin[2];
         }
+        float4 Ln = b < e ? __ldg(pos + b) : make_float4(0.f, 0.f, 0.f, 0.f);
         for(uint32_t q = b; q < e; ++q) {
-            const float4 L = __ldg(pos + q);
+            const float4 L = Ln;
+            if(q + 1 < e) Ln = __ldg(pos + q + 1);
             float dxx[3], dyy[3], dzz[3];
 #pragma unroll
             for(int o = 0; o < 3; ++o) {

@@ -96,3 +96,25 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(capi, "LIB_PATH", tmp_path / "nope.so")
     with pytest.raises(RuntimeError, match="no CPU fallback"):
         capi.load()
+
+
+def test_tile_shape_entry_points(lib):
+    """bnn_tile_shapes / bnn_set_tile_shape / bnn_tile_tuning need no GPU: the shape table,
+    range checks, and the (empty) tuning table with its size protocol."""
+    shapes = capi.tile_shapes()
+    assert len(shapes) == 6 and shapes[0] == (6, 8) and len(set(shapes)) == 6
+    assert lib.bnn_set_tile_shape(len(shapes)) == capi.STATUS_CODE["INVALID_ARGUMENT"]
+    assert lib.bnn_set_tile_shape(-2) == capi.STATUS_CODE["INVALID_ARGUMENT"]
+    assert lib.bnn_set_tile_shape(2) == 0 and lib.bnn_set_tile_shape(-1) == 0
+    need = C.c_size_t()
+    assert lib.bnn_tile_tuning(None, 0, C.byref(need)) == capi.STATUS_CODE["CAPACITY"]
+    assert need.value >= 1
+    assert capi.tile_tuning() == []
+
+
+def test_batch_mode_validation_needs_no_gpu(lib):
+    """bnn_batch_create rejects an unknown step mode before any CUDA call."""
+    h = C.c_void_p()
+    for mode in (2, 0x200, capi.BATCH_PER_SCENE | 0x400):
+        bp = capi.BatchParams(0, 1, mode)
+        assert lib.bnn_batch_create(C.byref(bp), C.byref(h)) == capi.STATUS_CODE["INVALID_ARGUMENT"]
