@@ -241,7 +241,7 @@ int batch_substep(BatchStepWork& w, bnn_flip* const* hs, int nsIn, int* rc, bnn_
             cdiv((size_t)c.n, 256),                            // PMove
             bbox_fold_blocks(c.n),                             // PMoveFold
             virt_blocks(h->C),                                 // PCells
-            c.n > 16 ? std::min(296u, std::max(2u, cdiv((size_t)c.n, 65536))) : 0u,  // PSortLarge
+            c.n > 16 ? std::min(296u, std::max(2u, cdiv((size_t)c.n, 8192))) : 0u,  // PSortLarge
             cdiv(h->C, 2048),                                  // PScan
             region_blocks(ftot),                               // PExtrap
             std::min(kRegionBlocks, cdiv(fmax, 2048)),         // PFill

@@ -450,7 +450,8 @@ def run_batch(args, ws, rank, local):
     mine = bdist.shard_scenes(costs, ws)[rank]
     mode = capi.BATCH_PER_SCENE if args.batch_mode == "per_scene" else capi.BATCH_STAGED
     b = FlipBatch(worker_threads=args.workers, step_mode=mode)
-    built = [scenes.batch_scene(specs[i]) for i in mine]
+    over = {} if args.inner_tol is None else {"refine_inner_tolerance": args.inner_tol}
+    built = [scenes.batch_scene(specs[i], **over) for i in mine]
     npart = sum(len(p) for _, p, _ in built)
     t_up = time.perf_counter()
     ids = [b.add_scene(cfg, pos, vel) for cfg, pos, vel in built]
@@ -523,7 +524,8 @@ def run_batch(args, ws, rank, local):
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scenes, seed 11)",
                 "config": {"workload": "batch_256_scenes", "scenes": len(specs), "scenes_rank0": len(mine),
                            "particles_rank0": npart, "res_choices": [32, 48, 64, 96, 128], "cell_size": "1/64",
-                           "pcg": "Jacobi, refined FP32 inner / FP64 outer to 1e-6, inner 1e-2",
+                           "pcg": "Jacobi, refined FP32 inner / FP64 outer to 1e-6, inner "
+                                  f"{args.inner_tol if args.inner_tol is not None else 1e-2:g}",
                            "batch_mode": args.batch_mode, "staged_scenes_rank0": staged,
                            "worker_threads": args.workers or "min(16, cores)", "parallelism": f"scenes/{ws} ranks"},
                 "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
