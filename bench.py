@@ -318,6 +318,8 @@ def run_ours(args, ws, rank, local):
         cfg["cg_relative_tolerance"] = args.tol
     pos, vel = scenes.dam_break(N_GRID)
     npart = len(pos)
+    if args.tile_shape is not None:
+        capi.set_tile_shape(args.tile_shape)
     solver = FlipSolver(cfg)
     solver.set_particles(pos, vel)
     stream = torch.cuda.ExternalStream(solver.stream_ptr())
@@ -926,6 +928,8 @@ def main():
     ap.add_argument("--tol", type=float, default=None,
                     help="fp32 / fp64 PCG: relative tolerance (the refined mode's outer tolerance is 1e-8)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tile-shape", type=int, default=None,
+                    help="flip: use this P2G tile shape (bnn_set_tile_shape) instead of the tuner's choice")
     ap.add_argument("--per-step", action="store_true",
                     help="flip: add every timed sub-step's stage times to the line (detail.per_step)")
     ap.add_argument("--no-compare", action="store_true",
