@@ -1723,7 +1723,7 @@ void launch_sort_finish(int n, size_t ncells, uint32_t* cellOf, uint32_t* slot, 
     if(n > 0) { k_scatter_index<<<nblk(n), 256, 0, s>>>(n, cellOf, slot, cellStart, idSrc, order, key); bnn_note_launch(); }
     cudaMemsetAsync(&st->nlarge, 0, sizeof(unsigned), s);
     { k_sort_buckets<<<nblk(ncells), 256, 0, s>>>((int)ncells, cellStart, order, key, count, slot, st); bnn_note_launch(); }
-    if(n > 16) { k_sort_large<<<2 * 148, 256, 0, s>>>(cellStart, order, idSrc, cellOf, slot, st); bnn_note_launch(); }
+    if(n > 16) { k_sort_large<<<8 * 148, 256, 0, s>>>(cellStart, order, idSrc, cellOf, slot, st); bnn_note_launch(); }
     if(n > 0)
         { k_gather_particles<<<nblk(n), 256, 0, s>>>(n, order, src6, srcPos ? srcPos : src6, dst6, idSrc, idDst, cSrc, cDst,
                                                     g3, rec, g, stride); bnn_note_launch(); }

@@ -145,12 +145,15 @@ def batch_scene(spec: dict, ppc: int = 8, pcg_mode: int = 2, **over):
     """Parameters and particles of one batch scene (batch_scene_specs / serve_requests):
     domain [0, res/64] per axis with cell size 1/64, a dam-break block of block_frac of
     the domain anchored at the origin, `ppc` particles per cell, FP32 PCG refined to a
-    1e-6 relative residual (FP64-checked), as the batch and serving configurations ask."""
+    1e-6 relative residual (FP64-checked), as the batch and serving configurations ask.
+    The inner FP32 solves stop at 1e-3 of their start residual: two outer rounds reach
+    1e-6 (measured on the 256-scene batch: 1e-2 1.33, 1e-3 1.39, 3e-4 1.28, 1e-4 1.19 G
+    particle-steps/s)."""
     dx = 1.0 / 64.0
     res = spec["res"]
     ext = tuple(r * dx for r in res)
     block = tuple(f * e for f, e in zip(spec["block_frac"], ext))
-    over = dict({"refine_tolerance": 1e-6}, **over)
+    over = dict({"refine_tolerance": 1e-6, "refine_inner_tolerance": 1e-3}, **over)
     cfg = dam_break_params(64, box_max=ext, pcg_mode=pcg_mode, **over)
     pos, vel = dam_break(64, block=block, ppc=ppc, seed=spec["seed"], cell_size=dx)
     return cfg, pos, vel

@@ -527,7 +527,7 @@ def run_batch(args, ws, rank, local):
                 "config": {"workload": "batch_256_scenes", "scenes": len(specs), "scenes_rank0": len(mine),
                            "particles_rank0": npart, "res_choices": [32, 48, 64, 96, 128], "cell_size": "1/64",
                            "pcg": "Jacobi, refined FP32 inner / FP64 outer to 1e-6, inner "
-                                  f"{args.inner_tol if args.inner_tol is not None else 1e-2:g}",
+                                  f"{args.inner_tol if args.inner_tol is not None else 1e-3:g}",
                            "batch_mode": args.batch_mode, "staged_scenes_rank0": staged,
                            "worker_threads": args.workers or "min(16, cores)", "parallelism": f"scenes/{ws} ranks"},
                 "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
@@ -593,7 +593,7 @@ def run_serve(args, ws, rank, local):
                 "data": "synthetic (seeded request stream, seed 13)",
                 "config": {"workload": "serve_poisson", "requests": len(reqs), "rate_per_s": 20,
                            "res": "cubic, log-uniform 32..192", "steps_per_request": args.req_steps,
-                           "hbm_budget_gb": 150, "pcg": "refined FP32 to 1e-6", "parallelism": f"requests/{ws} ranks",
+                           "hbm_budget_gb": 150, "pcg": "refined FP32 (inner 1e-3) to 1e-6", "parallelism": f"requests/{ws} ranks",
                            "time_limit_s": args.time_limit},
                 "completed_requests": summ["completed"], "admitted_requests": summ["admitted"],
                 "waits_for_memory": summ["waits_for_memory"], "max_running": summ["max_running"],
