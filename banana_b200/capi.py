@@ -23,7 +23,6 @@ PCG_MODE = {"fp32": 0, "fp64": 1, "refined": 2}
 # OR-ed into a PCG mode: the single-reduction form of the iteration instead of the default
 # PCGSolver::solve_precond step order (include/banana_b200.h BNN_PCG_SINGLE_REDUCTION)
 PCG_SINGLE_REDUCTION = 0x10
-PCG_CHUNK_SMEM = 0x20  # BNN_PCG_CHUNK_SMEM: chunk-resident SpMV (FP32, reference step order)
 FIELD = {"u": 0, "v": 1, "w": 2, "phi": 3, "pressure": 4, "old_u": 5, "old_v": 6, "old_w": 7, "active": 8,
          "weight_u": 9, "weight_v": 10, "weight_w": 11, "boundary_sdf": 12}
 GEOMETRY = {"box": 0, "sphere": 1}

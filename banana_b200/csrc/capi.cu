@@ -863,8 +863,7 @@ extern "C" int bnn_pcg_barrier_probe(float limit_seconds, int32_t* barrier_statu
 extern "C" int bnn_pcg_solve_7pt(uint32_t n, const float* diag, const int32_t* nbr, float offdiag, const float* rhs,
                                  float tol, uint32_t max_iter, int32_t mode, float inner_tol, double* x_out,
                                  bnn_pcg_stats* stats) {
-    if(!diag || !nbr || !rhs || !x_out ||
-       (mode & ~(BNN_PCG_MODE_MASK | BNN_PCG_SINGLE_REDUCTION | BNN_PCG_CHUNK_SMEM)) != 0 ||
+    if(!diag || !nbr || !rhs || !x_out || (mode & ~(BNN_PCG_MODE_MASK | BNN_PCG_SINGLE_REDUCTION)) != 0 ||
        (mode & BNN_PCG_MODE_MASK) > 2)
         return BNN_ERR_INVALID_ARGUMENT;
     if(!(offdiag <= 0.f)) return BNN_ERR_INVALID_ARGUMENT;

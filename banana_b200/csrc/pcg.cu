@@ -568,256 +568,6 @@ __global__ void __launch_bounds__(kLanes, pcg_min_blocks<VT, COEF>()) k_pcg_pers
 }
 
 // ---------------------------------------------------------------------------------
-// Chunk-resident SpMV (BNN_PCG_CHUNK_SMEM, FP32, two-reduction step order, rows given as
-// neighbour planes): the same iteration as k_pcg_persistent, with phase A reorganised.
-// A block keeps, for the whole solve, the structure of the (at most kSmemChunks) chunks it
-// owns in shared memory: per row and direction a 16-bit code -- no neighbour, a row of the
-// same chunk, or an entry of the chunk's list of rows outside it.  Per iteration it loads
-// z and s_old of its own rows and of the listed outside rows in one round trip, forms
-// s = z + beta s_old once per row into shared memory, and sums q = A s from there in the
-// same slot order (-z, -y, -x, diagonal, +x, +y, +z).  s and q are therefore bit for bit
-// those of k_pcg_persistent; the latency chain of a chunk is one global round trip instead
-// of one per row group.  The saving needs a row numbering in which most neighbours fall in
-// the same 2048-row chunk (bricks of cells, not x-major slabs).
-// ---------------------------------------------------------------------------------
-constexpr int kFarCap = 1024;     // outside rows a chunk lists in shared memory (a 16x16x8 brick has 1024)
-constexpr int kSmemChunks = 2;    // chunks a block may own
-constexpr unsigned short kCodeNone = 0xffffu, kCodeDirect = 0xfffeu, kCodeFar = 0x8000u;
-struct SmemChunk {
-    unsigned short code[6][kChunk];
-    int far[kFarCap];
-    int nfar;
-};
-constexpr size_t kPcgSmemBytes = sizeof(float) * (kChunk + kFarCap) + sizeof(SmemChunk) * kSmemChunks;
-
-__global__ void __launch_bounds__(kLanes, 3) k_pcg_smem(PcgArgs<float> a) {
-    extern __shared__ __align__(16) unsigned char smraw[];
-    float* sS = (float*)smraw;                 // s of the chunk's rows
-    float* sFar = sS + kChunk;                 // s of its listed outside rows
-    SmemChunk* ch = (SmemChunk*)(sFar + kFarCap);
-    __shared__ double smd[kLanes];
-    __shared__ float smv[kLanes];
-    const int n = a.n;
-    const int nch = (n + kChunk - 1) / kChunk;
-    const unsigned nb = gridDim.x;
-    unsigned sense = 0;
-    unsigned* flags = &a.st->flags;
-    const float negoff = a.negoff;
-
-    // ---- the structure of this block's chunks, once
-    for(int c = blockIdx.x, k = 0; c < nch; c += nb, ++k) {
-        SmemChunk& C = ch[k];
-        if(threadIdx.x == 0) C.nfar = 0;
-        __syncthreads();
-        const size_t cbase = (size_t)c * kChunk;
-#pragma unroll 1
-        for(int j = 0; j < kPerLane; ++j) {
-            const int lr = threadIdx.x + j * kLanes;
-            const size_t e = cbase + lr;
-#pragma unroll
-            for(int q = 0; q < 6; ++q) {
-                unsigned short code = kCodeNone;
-                if(e < (size_t)n) {
-                    const int32_t v = __ldg(a.nbr + (size_t)q * n + e);
-                    if(v >= 0) {
-                        if((size_t)v >= cbase && (size_t)v < cbase + kChunk) {
-                            code = (unsigned short)((size_t)v - cbase);
-                        } else {
-                            const int f = atomicAdd(&C.nfar, 1);
-                            if(f < kFarCap) { C.far[f] = v; code = (unsigned short)(kCodeFar | (unsigned)f); }
-                            else code = kCodeDirect;
-                        }
-                    }
-                }
-                C.code[q][lr] = code;
-            }
-        }
-        __syncthreads();
-        if(threadIdx.x == 0 && C.nfar > kFarCap) C.nfar = kFarCap;
-        __syncthreads();
-    }
-
-    // ---- init: r = rhs, x = 0, z = D^-1 r; partial z.r and max|r| (PCGSolver.cpp:151-168)
-    for(int c = blockIdx.x; c < nch; c += nb) {
-        double acc = 0.0;
-        float m = 0.f;
-        const size_t base = (size_t)c * kChunk + threadIdx.x;
-#pragma unroll
-        for(int j = 0; j < kPerLane; ++j) {
-            const size_t e = base + (size_t)j * kLanes;
-            if(e < (size_t)n) {
-                const float rv = a.rhsF[e];
-                a.r[e] = rv;
-                a.x[e] = 0.f;
-                const float ab = vabs(rv);
-                m = m > ab ? m : ab;
-                const float zv = __ldg(a.invd + e) * rv;
-                a.z[e] = zv;
-                acc = acc + (double)zv * (double)rv;
-            }
-        }
-        double bs;
-        float bm;
-        block_sum_max_256<float>(acc, m, smd, smv, bs, bm, true);
-        if(threadIdx.x == 0) { a.part0[c] = bs; a.partMax[c] = bm; }
-    }
-    if(!grid_barrier(a.gs, nb, sense, flags, solve_barrier_limit())) return;
-    double rho;
-    float resid;
-    reduce_partials_bcast<float>(a.part0, a.partMax, nch, smd, smv, rho, resid);
-    const float tolFactor = fmaxf(a.tolFactor, 1e-30f);
-    unsigned iter = 0, success = 0;
-    bool done = false;
-    float tol = 0.f;
-    if(resid < FLT_MIN) {
-        done = true;
-        success = 1;
-    } else {
-        tol = tolFactor * resid;
-        if(rho < (double)FLT_MIN || isnan(rho)) done = true;
-    }
-    if(a.maxIter == 0) done = true;
-
-    float beta = 0.f;
-    bool first = true;
-    float* sOld = a.s1;
-    float* sNew = a.s0;
-    const float* __restrict__ zR = a.z;
-    while(!done) {
-        // ---- phase A: s = z + beta s_old, q = A s, partial s.q (PCGSolver.cpp:173-174,192-193)
-        for(int c = blockIdx.x, k = 0; c < nch; c += nb, ++k) {
-            const SmemChunk& C = ch[k];
-            const size_t base = (size_t)c * kChunk + threadIdx.x;
-            float sOwn[kPerLane], dg[kPerLane];
-            // own rows and listed outside rows: all loads issued together
-#pragma unroll
-            for(int j = 0; j < kPerLane; ++j) {
-                const size_t e = base + (size_t)j * kLanes;
-                const size_t ee = e < (size_t)n ? e : 0;
-                const float zv = __ldcg(zR + ee);
-                const float sv = first ? 0.f : __ldcg(sOld + ee);
-                dg[j] = __ldg(a.diag + ee);
-                sOwn[j] = first ? zv : zv + beta * sv;
-            }
-            for(int f = threadIdx.x; f < C.nfar; f += kLanes) {
-                const int v = C.far[f];
-                const float zv = __ldcg(zR + v);
-                const float sv = first ? 0.f : __ldcg(sOld + v);
-                sFar[f] = first ? zv : zv + beta * sv;
-            }
-#pragma unroll
-            for(int j = 0; j < kPerLane; ++j) sS[threadIdx.x + j * kLanes] = sOwn[j];
-            __syncthreads();
-            double acc = 0.0;
-#pragma unroll
-            for(int j = 0; j < kPerLane; ++j) {
-                const int lr = threadIdx.x + j * kLanes;
-                const size_t e = base + (size_t)j * kLanes;
-                if(e >= (size_t)n) continue;
-                float s6[6];
-                bool has[6];
-#pragma unroll
-                for(int q = 0; q < 6; ++q) {
-                    const unsigned code = C.code[q][lr];
-                    has[q] = code != kCodeNone;
-                    if(code == kCodeNone) s6[q] = 0.f;
-                    else if(code < kCodeFar) s6[q] = sS[code];
-                    else if(code != kCodeDirect) s6[q] = sFar[code & 0x7fffu];
-                    else {
-                        const int32_t v = __ldg(a.nbr + (size_t)q * n + e);
-                        const float zv = __ldcg(zR + v);
-                        const float sv = first ? 0.f : __ldcg(sOld + v);
-                        s6[q] = first ? zv : zv + beta * sv;
-                    }
-                }
-                float t = 0.f;
-#pragma unroll
-                for(int q = 0; q < 3; ++q) if(has[q]) t += negoff * s6[q];
-                if(dg[j] != 0.f) t += dg[j] * sOwn[j];
-#pragma unroll
-                for(int q = 3; q < 6; ++q) if(has[q]) t += negoff * s6[q];
-                sNew[e] = sOwn[j];
-                a.q[e] = t;
-                acc = acc + (double)sOwn[j] * (double)t;
-            }
-            double bs;
-            float unused;
-            block_sum_max_256<float>(acc, 0.f, smd, smv, bs, unused, false);
-            if(threadIdx.x == 0) a.part1[c] = bs;
-        }
-        if(!grid_barrier(a.gs, nb, sense, flags, solve_barrier_limit())) return;
-        double tmp;
-        float unused2;
-        reduce_partials_bcast<float>(a.part1, (const float*)nullptr, nch, smd, smv, tmp, unused2);
-        if(tmp < (double)FLT_MIN) {
-            ++iter;
-            success = 1;
-            break;
-        }
-        const float alpha = (float)(rho / tmp);
-        // ---- phase B: x += alpha s, r -= alpha q, max|r|, z = D^-1 r, partial z.r
-        for(int c = blockIdx.x; c < nch; c += nb) {
-            const size_t base = (size_t)c * kChunk + threadIdx.x;
-            float xs[kPerLane], ss[kPerLane], rs[kPerLane], qs[kPerLane], is[kPerLane];
-#pragma unroll
-            for(int j = 0; j < kPerLane; ++j) {
-                const size_t e = base + (size_t)j * kLanes;
-                const size_t ee = e < (size_t)n ? e : 0;
-                xs[j] = __ldcg(a.x + ee);
-                ss[j] = __ldcg(sNew + ee);
-                rs[j] = __ldcg(a.r + ee);
-                qs[j] = __ldcg(a.q + ee);
-                is[j] = __ldg(a.invd + ee);
-            }
-            double acc = 0.0;
-            float m = 0.f;
-#pragma unroll
-            for(int j = 0; j < kPerLane; ++j) {
-                const size_t e = base + (size_t)j * kLanes;
-                if(e < (size_t)n) {
-                    a.x[e] = xs[j] + alpha * ss[j];
-                    const float rv = rs[j] + (-alpha) * qs[j];
-                    a.r[e] = rv;
-                    const float ab = vabs(rv);
-                    m = m > ab ? m : ab;
-                    const float zv = is[j] * rv;
-                    a.z[e] = zv;
-                    acc = acc + (double)zv * (double)rv;
-                }
-            }
-            double bs;
-            float bm;
-            block_sum_max_256<float>(acc, m, smd, smv, bs, bm, true);
-            if(threadIdx.x == 0) { a.part2[c] = bs; a.partMax[c] = bm; }
-        }
-        if(!grid_barrier(a.gs, nb, sense, flags, solve_barrier_limit())) return;
-        double rhoNew;
-        reduce_partials_bcast<float>(a.part2, a.partMax, nch, smd, smv, rhoNew, resid);
-        ++iter;
-        if(resid < tol) {
-            success = 1;
-            break;
-        }
-        beta = (float)(rhoNew / rho);
-        rho = rhoNew;
-        if(iter >= a.maxIter) {
-            if(blockIdx.x == 0 && threadIdx.x == 0) atomicOr(flags, BNN_FLAG_PCG_MAXITER);
-            break;
-        }
-        float* t = sOld;
-        sOld = sNew;
-        sNew = t;
-        first = false;
-    }
-    if(blockIdx.x == 0 && threadIdx.x == 0) {
-        a.st->iter = iter;
-        a.st->success = success;
-        a.st->done = 1;
-        Sc<float>::set_resid(a.st, resid);
-    }
-}
-
-// ---------------------------------------------------------------------------------
 // Single-reduction PCG (Chronopoulos & Gear, 1989): the same Krylov iterates as
 // PCGSolver::solve_precond (PCGSolver.cpp:143-199) in exact arithmetic, with both inner
 // products of an iteration formed in one reduction, so one grid barrier per iteration
@@ -1787,31 +1537,20 @@ void pcg_release(PcgWork& w) {
     w = PcgWork();
 }
 
-// Slot of a kernel variant in CoopState::perSM: bit 0 FP64, bit 1 packed rows, bit 2
-// coefficients, bit 3 single reduction; 14 the chunk-resident SpMV kernel
-static int chunkSmemIndex(bool f64, bool packed, bool coef, bool two, bool smem) {
-    if(smem && !f64 && !packed && !coef && two) return 14;
-    return (f64 ? 1 : 0) + (packed ? 2 : 0) + (coef ? 4 : 0) + (two ? 0 : 8);
-}
-
 // Runs one PCG solve (VT vectors) as a single cooperative launch.  Returns BNN status;
 // the solution is left in x.
 template<class VT>
 static int pcg_solve_t(PcgWork& w, int n, const float* rhsF, const float* diag, const VT* invd, const int32_t* nbr,
                        const int4* rec, const float* coef, const float4* coefRow, VT negoff, VT tolFactor, unsigned maxIter, VT* x, VT* r, VT* z, VT* s0, VT* s1, VT* q,
-                       VT* partMax, bool twoReductions, bool smemSpmv, DevState* dst, DevState* hst, cudaStream_t s,
-                       PcgOutcome& out) {
+                       VT* partMax, bool twoReductions, DevState* dst, DevState* hst, cudaStream_t s, PcgOutcome& out) {
     out = PcgOutcome();
     if(n == 0) { out.success = 1; return BNN_OK; }
     const int nch = (n + kChunk - 1) / kChunk;
     const bool packedCoef = rec && coefRow;
     // kernel variant: bit 0 FP64, bit 1 packed rows, bit 2 coefficients, bit 3 single reduction
-    const int ti = chunkSmemIndex(sizeof(VT) == 8, rec != nullptr, coef || coefRow, twoReductions, smemSpmv);
+    const int ti = (sizeof(VT) == 8 ? 1 : 0) + (rec ? 2 : 0) + ((coef || coefRow) ? 4 : 0) + (twoReductions ? 0 : 8);
     const void* kern;
-    // the chunk-resident SpMV kernel, when asked for and its shape fits (checked below)
-    bool chunkSmem = smemSpmv && sizeof(VT) == 4 && twoReductions && !rec && !coef;
-    if(chunkSmem) kern = (const void*)k_pcg_smem;
-    else if(twoReductions)
+    if(twoReductions)
         kern = packedCoef ? (const void*)k_pcg_persistent<VT, true, true>
                           : (rec ? (const void*)k_pcg_persistent<VT, true> : (const void*)k_pcg_persistent<VT, false>);
     else if(rec)
@@ -1827,25 +1566,13 @@ static int pcg_solve_t(PcgWork& w, int n, const float* rhsF, const float* diag, 
             BNN_CUDA_CHECK(cudaDeviceGetAttribute(&g_coop.numSM, cudaDevAttrMultiProcessorCount, dev));
         }
         if(!g_coop.perSM[ti]) {
-            const size_t dyn = ti == 14 ? kPcgSmemBytes : 0;
-            if(dyn) BNN_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-            BNN_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_coop.perSM[ti], kern, kLanes, dyn));
+            BNN_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_coop.perSM[ti], kern, kLanes, 0));
             if(g_coop.perSM[ti] < 1) { bnn_set_error("persistent PCG kernel cannot be resident"); return BNN_ERR_CUDA; }
         }
         numSM = g_coop.numSM;
         perSMv = g_coop.perSM[ti];
     }
-    int cap = numSM * perSMv;
-    if(chunkSmem && (nch + cap - 1) / cap > kSmemChunks) {
-        // more chunks per block than its shared memory holds: the general kernel
-        chunkSmem = false;
-        kern = (const void*)k_pcg_persistent<VT, false>;
-        std::lock_guard<std::mutex> lk(g_coop.mu);
-        const int t0 = chunkSmemIndex(sizeof(VT) == 8, false, false, true, false);
-        if(!g_coop.perSM[t0]) BNN_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_coop.perSM[t0], kern, kLanes, 0));
-        perSMv = g_coop.perSM[t0];
-        cap = numSM * perSMv;
-    }
+    const int cap = numSM * perSMv;
     const int perBlock = (nch + cap - 1) / cap;           // chunks per block
     const int grid = (nch + perBlock - 1) / perBlock;     // balanced: every block the same count
     PcgArgs<VT> a;
@@ -1865,7 +1592,7 @@ static int pcg_solve_t(PcgWork& w, int n, const float* rhsF, const float* diag, 
     // fit the GPU together, or blocks of one could wait for SMs held by another's barrier
     CoopShare share(grid * (kShareUnits / perSMv), numSM * kShareUnits);
     if(w.ev[0]) BNN_CUDA_CHECK(cudaEventRecord(w.ev[0], s));
-    BNN_CUDA_CHECK(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kLanes), args, chunkSmem ? kPcgSmemBytes : 0, s));
+    BNN_CUDA_CHECK(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kLanes), args, 0, s));
     bnn_note_launch();
     if(w.ev[1]) BNN_CUDA_CHECK(cudaEventRecord(w.ev[1], s));
     BNN_CUDA_CHECK(cudaMemcpyAsync(hst, dst, sizeof(DevState), cudaMemcpyDeviceToHost, s));
@@ -1889,8 +1616,6 @@ int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const floa
               PcgOutcome& out) {
     const int mode = modeFlags & BNN_PCG_MODE_MASK;
     const bool two = (modeFlags & BNN_PCG_SINGLE_REDUCTION) == 0;
-    const bool smemK = (modeFlags & BNN_PCG_CHUNK_SMEM) != 0;
-    if(smemK) gridRows = false;  // the chunk-resident kernel reads neighbour planes
     int rc = pcg_reserve(w, n, mode != BNN_PCG_FP32);
     if(rc != BNN_OK) return rc;
     const unsigned nb = (unsigned)((n + 255) / 256);
@@ -1910,7 +1635,7 @@ int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const floa
     }
     if(mode == BNN_PCG_FP32) {
         rc = pcg_solve_t<float>(w, n, rhs, diag, invd, nbr, rec, coef, coefRow, -(1.0f * dt), tol, maxIter, w.x, w.r, w.z, w.s0, w.s1,
-                                w.q, w.partMaxF, two, smemK, dst, hst, s, out);
+                                w.q, w.partMaxF, two, dst, hst, s, out);
         if(rc != BNN_OK) return rc;
         if(n > 0) BNN_CUDA_CHECK(cudaMemcpyAsync(pressure, w.x, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
         if(x64out && n > 0) { k_f32_to_f64<<<nb, 256, 0, s>>>(n, w.x, x64out); bnn_note_launch(); }
@@ -1919,7 +1644,7 @@ int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const floa
     if(mode == BNN_PCG_FP64) {
         if(n > 0) { k_inv_diag64<<<nb, 256, 0, s>>>(n, diag, w.inv64); bnn_note_launch(); }
         rc = pcg_solve_t<double>(w, n, rhs, diag, w.inv64, nbr, rec, coef, coefRow, -(double)(1.0f * dt), (double)tol, maxIter, w.x64,
-                                 w.r64, w.z64, w.s064, w.s164, w.q64, w.partMaxD, two, smemK, dst, hst, s, out);
+                                 w.r64, w.z64, w.s064, w.s164, w.q64, w.partMaxD, two, dst, hst, s, out);
         if(rc != BNN_OK) return rc;
         if(n > 0) { k_d64_to_f32<<<nb, 256, 0, s>>>(n, w.x64, pressure); bnn_note_launch(); }
         if(x64out && n > 0)
@@ -1942,7 +1667,7 @@ int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const floa
         { k_ir_to_f32<<<nb, 256, 0, s>>>(n, w.r64, w.r32); bnn_note_launch(); }
         PcgOutcome inner;
         rc = pcg_solve_t<float>(w, n, w.r32, diag, invd, nbr, rec, coef, coefRow, -(1.0f * dt), innerTol, maxIter, w.d32, w.r, w.z, w.s0,
-                                w.s1, w.q, w.partMaxF, two, smemK, dst, hst, s, inner);
+                                w.s1, w.q, w.partMaxF, two, dst, hst, s, inner);
         if(rc != BNN_OK) return rc;
         total += inner.iterations;
         kernelMs += inner.kernelMs;

@@ -59,11 +59,6 @@ extern "C" {
  * (PCGSolver.cpp:143-199: the two inner products one after the other, two reductions per
  * iteration). */
 #define BNN_PCG_SINGLE_REDUCTION 0x10
-/* OR-ed into BNN_PCG_FP32 (reference step order): the same iteration with the SpMV summed
- * from a per-block shared-memory copy of each 2048-row chunk's structure and values (same
- * bits).  It pays off when most neighbours of a row lie in its chunk (rows numbered by
- * bricks of cells); other modes ignore it. */
-#define BNN_PCG_CHUNK_SMEM 0x20
 
 #define BNN_PRECOND_JACOBI 0 /* PCGSolver::JACOBI (PCGSolver.cpp:232-237,273-284) */
 
