@@ -440,6 +440,20 @@ void pcg_release(PcgWork& w);
 
 extern "C" void bnn_set_error(const char* msg);
 
+// Device memory of solver handles (grids, particles, rows, PCG vectors) comes from the
+// device's stream-ordered memory pool: allocating and freeing a scene's arrays then costs
+// neither a driver allocation each nor, on free, a synchronisation of the whole device
+// (what cudaFree does) -- scenes come and go between the steps of a serving batch.  An
+// allocation is usable on every stream when dev_alloc returns; dev_free requires that no
+// work on the memory is pending (every API call that frees ends its streams' work first).
+cudaError_t dev_alloc_bytes(void** p, size_t bytes);
+void dev_free_ptr(void* p);
+template<class T> inline cudaError_t dev_alloc(T** p, size_t bytes) { return dev_alloc_bytes((void**)p, bytes); }
+inline cudaError_t dev_free(const void* p) {
+    dev_free_ptr(const_cast<void*>(p));
+    return cudaSuccess;
+}
+
 // Every kernel launch of the library is followed by bnn_note_launch(): the running total
 // is what bnn_launch_count() reports.  Launches captured into a CUDA graph are taken back
 // (bnn_note_launches(-k)) and counted again at every replay (bnn_note_launches(k)).

@@ -22,6 +22,64 @@ extern "C" void bnn_set_error(const char* msg) { g_lastError = msg ? msg : ""; }
 extern "C" const char* bnn_last_error(void) { return g_lastError.c_str(); }
 extern "C" const char* bnn_version(void) { return "banana_b200 0.1 (sm_100a)"; }
 
+// The pool keeps up to 16 GB of freed memory for reuse instead of handing it back to the
+// driver at every synchronisation; allocations and frees are ordered on the calling
+// thread's default stream, which the handles never queue work on.
+static std::atomic<uint64_t> g_poolSetUp{0};  // bit per device ordinal
+cudaError_t dev_alloc_bytes(void** p, size_t bytes) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if(e != cudaSuccess) return e;
+    const uint64_t bit = 1ull << (dev & 63);
+    if(!(g_poolSetUp.load(std::memory_order_acquire) & bit)) {
+        cudaMemPool_t pool;
+        if(cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            uint64_t keep = 16ull << 30;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        g_poolSetUp.fetch_or(bit, std::memory_order_acq_rel);
+    }
+    e = cudaMallocAsync(p, bytes ? bytes : 1, cudaStreamPerThread);
+    if(e != cudaSuccess) return e;
+    return cudaStreamSynchronize(cudaStreamPerThread);
+}
+void dev_free_ptr(void* p) {
+    if(p) cudaFreeAsync(p, cudaStreamPerThread);
+}
+
+// Pinned host copies of the per-handle device record come from page-sized pinned blocks
+// (cudaHostAlloc is a slow call; a handle needs one small record)
+namespace {
+struct PinnedStates {
+    std::mutex mu;
+    std::vector<bnn::DevState*> freeList;
+};
+PinnedStates& pinned_states() {
+    static PinnedStates p;
+    return p;
+}
+} // namespace
+static cudaError_t pinned_state_alloc(bnn::DevState** out) {
+    PinnedStates& P = pinned_states();
+    std::lock_guard<std::mutex> lk(P.mu);
+    if(P.freeList.empty()) {
+        constexpr int kPer = 64;
+        bnn::DevState* blk = nullptr;
+        const cudaError_t e = cudaHostAlloc(&blk, kPer * sizeof(bnn::DevState), cudaHostAllocDefault);
+        if(e != cudaSuccess) return e;
+        for(int i = kPer - 1; i >= 0; --i) P.freeList.push_back(blk + i);
+    }
+    *out = P.freeList.back();
+    P.freeList.pop_back();
+    return cudaSuccess;
+}
+static void pinned_state_free(bnn::DevState* p) {
+    if(!p) return;
+    PinnedStates& P = pinned_states();
+    std::lock_guard<std::mutex> lk(P.mu);
+    P.freeList.push_back(p);
+}
+
 namespace bnn {
 // flip_kernels.cu
 void launch_advect(int n, float* p6, size_t stride, const float* const* U, const GridDesc& g, float sub, int steps,
@@ -88,11 +146,11 @@ using namespace bnn;
 
 static void free_particles(bnn_flip* h) {
     for(int b = 0; b < 2; ++b) {
-        cudaFree(h->p6[b]); cudaFree(h->ids[b]); cudaFree(h->C9[b]);
+        dev_free(h->p6[b]); dev_free(h->ids[b]); dev_free(h->C9[b]);
         h->p6[b] = nullptr; h->ids[b] = nullptr; h->C9[b] = nullptr;
     }
-    cudaFree(h->g3); cudaFree(h->rec); cudaFree(h->bboxPart); cudaFree(h->cellOf); cudaFree(h->slot); cudaFree(h->order); cudaFree(h->key); cudaFree(h->aosStage);
-    cudaFree(h->aniso); cudaFree(h->moved);
+    dev_free(h->g3); dev_free(h->rec); dev_free(h->bboxPart); dev_free(h->cellOf); dev_free(h->slot); dev_free(h->order); dev_free(h->key); dev_free(h->aosStage);
+    dev_free(h->aniso); dev_free(h->moved);
     h->g3 = nullptr; h->rec = nullptr; h->bboxPart = nullptr; h->cellOf = h->slot = h->order = h->key = nullptr; h->aosStage = nullptr;
     h->aniso = nullptr; h->moved = nullptr;
     h->premoved = false;
@@ -108,21 +166,21 @@ static int reserve_particles(bnn_flip* h, uint32_t n) {
     uint32_t cap = (uint32_t)cap64;
     size_t st = cap;
     for(int b = 0; b < 2; ++b) {
-        BNN_CUDA_CHECK(cudaMalloc(&h->p6[b], 6 * st * sizeof(float)));
-        BNN_CUDA_CHECK(cudaMalloc(&h->ids[b], st * sizeof(uint32_t)));
+        BNN_CUDA_CHECK(dev_alloc(&h->p6[b], 6 * st * sizeof(float)));
+        BNN_CUDA_CHECK(dev_alloc(&h->ids[b], st * sizeof(uint32_t)));
         if(h->P.solver_kind == BNN_SOLVER_APIC || h->P.solver_kind == BNN_SOLVER_AFLIP)
-            BNN_CUDA_CHECK(cudaMalloc(&h->C9[b], 9 * st * sizeof(float)));
+            BNN_CUDA_CHECK(dev_alloc(&h->C9[b], 9 * st * sizeof(float)));
     }
-    BNN_CUDA_CHECK(cudaMalloc(&h->g3, 3 * st * sizeof(float)));
+    BNN_CUDA_CHECK(dev_alloc(&h->g3, 3 * st * sizeof(float)));
     // two spare records: the gathers load records in aligned pairs
-    BNN_CUDA_CHECK(cudaMalloc(&h->rec, (4 * st + 2) * sizeof(float4)));
-    BNN_CUDA_CHECK(cudaMalloc(&h->bboxPart, 6 * ((st + 255) / 256) * sizeof(int)));
-    BNN_CUDA_CHECK(cudaMalloc(&h->cellOf, st * sizeof(uint32_t)));
-    BNN_CUDA_CHECK(cudaMalloc(&h->slot, st * sizeof(uint32_t)));
-    BNN_CUDA_CHECK(cudaMalloc(&h->order, st * sizeof(uint32_t)));
-    BNN_CUDA_CHECK(cudaMalloc(&h->key, st * sizeof(uint32_t)));
-    BNN_CUDA_CHECK(cudaMalloc(&h->aosStage, 6 * st * sizeof(float)));
-    if(h->P.solver_kind == BNN_SOLVER_FLIP) BNN_CUDA_CHECK(cudaMalloc(&h->moved, 3 * st * sizeof(float)));
+    BNN_CUDA_CHECK(dev_alloc(&h->rec, (4 * st + 2) * sizeof(float4)));
+    BNN_CUDA_CHECK(dev_alloc(&h->bboxPart, 6 * ((st + 255) / 256) * sizeof(int)));
+    BNN_CUDA_CHECK(dev_alloc(&h->cellOf, st * sizeof(uint32_t)));
+    BNN_CUDA_CHECK(dev_alloc(&h->slot, st * sizeof(uint32_t)));
+    BNN_CUDA_CHECK(dev_alloc(&h->order, st * sizeof(uint32_t)));
+    BNN_CUDA_CHECK(dev_alloc(&h->key, st * sizeof(uint32_t)));
+    BNN_CUDA_CHECK(dev_alloc(&h->aosStage, 6 * st * sizeof(float)));
+    if(h->P.solver_kind == BNN_SOLVER_FLIP) BNN_CUDA_CHECK(dev_alloc(&h->moved, 3 * st * sizeof(float)));
     h->cap = cap;
     return BNN_OK;
 }
@@ -131,16 +189,16 @@ static void destroy_all(bnn_flip* h) {
     if(!h) return;
     free_particles(h);
     for(int d = 0; d < 3; ++d) {
-        cudaFree(h->U[d]); cudaFree(h->B[d]); cudaFree(h->O[d]); cudaFree(h->VA[d]); cudaFree(h->VB[d]);
+        dev_free(h->U[d]); dev_free(h->B[d]); dev_free(h->O[d]); dev_free(h->VA[d]); dev_free(h->VB[d]);
     }
-    cudaFree(h->count); cudaFree(h->cellStart); cudaFree(h->scanWs); cudaFree(h->phi); cudaFree(h->flag);
-    cudaFree(h->aidx); cudaFree(h->cellTmp);
-    cudaFree(h->rowCell); cudaFree(h->rhs); cudaFree(h->diag); cudaFree(h->invd); cudaFree(h->pressure); cudaFree(h->nbr);
+    dev_free(h->count); dev_free(h->cellStart); dev_free(h->scanWs); dev_free(h->phi); dev_free(h->flag);
+    dev_free(h->aidx); dev_free(h->cellTmp);
+    dev_free(h->rowCell); dev_free(h->rhs); dev_free(h->diag); dev_free(h->invd); dev_free(h->pressure); dev_free(h->nbr);
     pcg_release(h->pcg);
-    cudaFree(h->objDev); cudaFree(h->nodeSdf); cudaFree(h->coef);
-    for(int d = 0; d < 3; ++d) cudaFree(h->W[d]);
-    cudaFree(h->dst);
-    if(h->hst) cudaFreeHost(h->hst);
+    dev_free(h->objDev); dev_free(h->nodeSdf); dev_free(h->coef);
+    for(int d = 0; d < 3; ++d) dev_free(h->W[d]);
+    dev_free(h->dst);
+    pinned_state_free(h->hst);
     for(auto& e : h->ev) if(e) cudaEventDestroy(e);
     for(auto& e : h->io) if(e) cudaEventDestroy(e);
     if(h->s2) cudaStreamDestroy(h->s2);
@@ -195,21 +253,21 @@ extern "C" int bnn_flip_create(const bnn_params* params, bnn_flip** out) {
         }
     };
     for(int d = 0; d < 3; ++d) {
-        ok(cudaMalloc(&h->U[d], h->F[d] * sizeof(float)));
-        ok(cudaMalloc(&h->B[d], h->F[d] * sizeof(float)));
-        ok(cudaMalloc(&h->O[d], h->F[d] * sizeof(float)));
-        ok(cudaMalloc(&h->VA[d], h->F[d]));
-        ok(cudaMalloc(&h->VB[d], h->F[d]));
+        ok(dev_alloc(&h->U[d], h->F[d] * sizeof(float)));
+        ok(dev_alloc(&h->B[d], h->F[d] * sizeof(float)));
+        ok(dev_alloc(&h->O[d], h->F[d] * sizeof(float)));
+        ok(dev_alloc(&h->VA[d], h->F[d]));
+        ok(dev_alloc(&h->VB[d], h->F[d]));
     }
-    ok(cudaMalloc(&h->count, h->C * sizeof(uint32_t)));
-    ok(cudaMalloc(&h->cellStart, (h->C + 1) * sizeof(uint32_t)));
+    ok(dev_alloc(&h->count, h->C * sizeof(uint32_t)));
+    ok(dev_alloc(&h->cellStart, (h->C + 1) * sizeof(uint32_t)));
     size_t ws = scan_workspace_bytes(h->C);
-    if(ws) ok(cudaMalloc(&h->scanWs, ws));
-    ok(cudaMalloc(&h->phi, h->C * sizeof(float)));
-    ok(cudaMalloc(&h->flag, h->C * sizeof(uint32_t)));
-    ok(cudaMalloc(&h->aidx, (h->C + 1) * sizeof(uint32_t)));
-    ok(cudaMalloc(&h->dst, sizeof(DevState)));
-    ok(cudaHostAlloc(&h->hst, sizeof(DevState), cudaHostAllocDefault));
+    if(ws) ok(dev_alloc(&h->scanWs, ws));
+    ok(dev_alloc(&h->phi, h->C * sizeof(float)));
+    ok(dev_alloc(&h->flag, h->C * sizeof(uint32_t)));
+    ok(dev_alloc(&h->aidx, (h->C + 1) * sizeof(uint32_t)));
+    ok(dev_alloc(&h->dst, sizeof(DevState)));
+    ok(pinned_state_alloc(&h->hst));
     for(auto& ev : h->ev) ok(cudaEventCreate(&ev));
     for(auto& ev : h->io) ok(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     ok(cudaStreamCreateWithFlags(&h->s2, cudaStreamNonBlocking));
@@ -404,7 +462,7 @@ extern "C" int bnn_flip_get_grid(bnn_flip* h, int32_t field, float* out, size_t 
     else if(field == BNN_FIELD_PRESSURE || field == BNN_FIELD_ACTIVE) {
         need = h->C;
         if(count < need) return BNN_ERR_INVALID_ARGUMENT;
-        if(!h->cellTmp) BNN_CUDA_CHECK(cudaMalloc(&h->cellTmp, h->C * sizeof(float)));
+        if(!h->cellTmp) BNN_CUDA_CHECK(dev_alloc(&h->cellTmp, h->C * sizeof(float)));
         if(h->nRows == 0 && field == BNN_FIELD_PRESSURE) {
             BNN_CUDA_CHECK(cudaMemsetAsync(h->cellTmp, 0, h->C * sizeof(float), h->s));
         } else {
@@ -456,7 +514,7 @@ extern "C" int bnn_flip_set_boundaries(bnn_flip* h, const bnn_boundary_object* o
         }
     uint32_t nStatic = 1;
     for(uint32_t i = 0; i < n; ++i) nStatic += objs[i].dynamic ? 0u : 1u;
-    if(!h->objDev) BNN_CUDA_CHECK(cudaMalloc(&h->objDev, kMaxBoundaryObjects * sizeof(BObj)));
+    if(!h->objDev) BNN_CUDA_CHECK(dev_alloc(&h->objDev, kMaxBoundaryObjects * sizeof(BObj)));
     BNN_CUDA_CHECK(cudaMemcpyAsync(h->objDev, list.data(), list.size() * sizeof(BObj), cudaMemcpyHostToDevice, h->s));
     if(n == 0) {
         h->g.obj = nullptr;
@@ -471,9 +529,9 @@ extern "C" int bnn_flip_set_boundaries(bnn_flip* h, const bnn_boundary_object* o
     if(anyDynamic && update_grid) {
         h->gridBoundary = true;
         const size_t nn = (size_t)(h->g.G[0] + 1) * (h->g.G[1] + 1) * (h->g.G[2] + 1);
-        if(!h->nodeSdf) BNN_CUDA_CHECK(cudaMalloc(&h->nodeSdf, nn * sizeof(float)));
+        if(!h->nodeSdf) BNN_CUDA_CHECK(dev_alloc(&h->nodeSdf, nn * sizeof(float)));
         for(int d = 0; d < 3; ++d)
-            if(!h->W[d]) BNN_CUDA_CHECK(cudaMalloc(&h->W[d], h->F[d] * sizeof(float)));
+            if(!h->W[d]) BNN_CUDA_CHECK(dev_alloc(&h->W[d], h->F[d] * sizeof(float)));
         launch_boundary_grid(h->g, h->nodeSdf, h->W, h->s);
     }
     BNN_CUDA_CHECK(cudaGetLastError());
@@ -601,10 +659,10 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st, const HostIo* io = nullp
     h->nRows = nrows;
     launch_active_rows(h->C, h->flag, h->aidx, h->rowCell, s);
     if(h->gridBoundary && h->coefCap < h->rowCap) {
-        cudaFree(h->coef);
+        dev_free(h->coef);
         h->coef = nullptr;
         h->coefCap = 0;
-        BNN_CUDA_CHECK(cudaMalloc(&h->coef, 6 * (size_t)h->rowCap * sizeof(float)));
+        BNN_CUDA_CHECK(dev_alloc(&h->coef, 6 * (size_t)h->rowCap * sizeof(float)));
         h->coefCap = h->rowCap;
     }
     launch_build_rows(g, (int)nrows, h->rowCell, h->phi, h->aidx, h->U, h->gridBoundary ? h->W : nullptr, substep,
@@ -784,7 +842,7 @@ extern "C" int bnn_flip_anisotropic_kernels(bnn_flip* h, const bnn_aniso_params*
                        h->g3, h->rec, g, h->cap, h->dst, s);
     h->cur = nxt;
     const size_t cap = h->cap;
-    if(!h->aniso) BNN_CUDA_CHECK(cudaMalloc(&h->aniso, (12 * cap + 4) * sizeof(float)));
+    if(!h->aniso) BNN_CUDA_CHECK(dev_alloc(&h->aniso, (12 * cap + 4) * sizeof(float)));
     float* dC = h->aniso;
     float* dM = h->aniso + 3 * cap;
     unsigned* cnt = (unsigned*)(h->aniso + 12 * cap);

@@ -89,15 +89,15 @@ inline int drop_premove(bnn_flip* h) {
 
 inline int reserve_rows(bnn_flip* h, uint32_t n) {
     if((int)n <= h->rowCap) return BNN_OK;
-    cudaFree(h->rowCell); cudaFree(h->rhs); cudaFree(h->diag); cudaFree(h->invd); cudaFree(h->pressure); cudaFree(h->nbr);
+    dev_free(h->rowCell); dev_free(h->rhs); dev_free(h->diag); dev_free(h->invd); dev_free(h->pressure); dev_free(h->nbr);
     int cap = (int)(n * 1.25) + 1024;
     if((size_t)cap > h->C) cap = (int)h->C;
-    BNN_CUDA_CHECK(cudaMalloc(&h->rowCell, cap * sizeof(uint32_t)));
-    BNN_CUDA_CHECK(cudaMalloc(&h->rhs, cap * sizeof(float)));
-    BNN_CUDA_CHECK(cudaMalloc(&h->diag, cap * sizeof(float)));
-    BNN_CUDA_CHECK(cudaMalloc(&h->invd, cap * sizeof(float)));
-    BNN_CUDA_CHECK(cudaMalloc(&h->pressure, cap * sizeof(float)));
-    BNN_CUDA_CHECK(cudaMalloc(&h->nbr, 6 * (size_t)cap * sizeof(int32_t)));
+    BNN_CUDA_CHECK(dev_alloc(&h->rowCell, cap * sizeof(uint32_t)));
+    BNN_CUDA_CHECK(dev_alloc(&h->rhs, cap * sizeof(float)));
+    BNN_CUDA_CHECK(dev_alloc(&h->diag, cap * sizeof(float)));
+    BNN_CUDA_CHECK(dev_alloc(&h->invd, cap * sizeof(float)));
+    BNN_CUDA_CHECK(dev_alloc(&h->pressure, cap * sizeof(float)));
+    BNN_CUDA_CHECK(dev_alloc(&h->nbr, 6 * (size_t)cap * sizeof(int32_t)));
     h->rowCap = cap;
     return BNN_OK;
 }

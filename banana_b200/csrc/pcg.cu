@@ -1488,40 +1488,40 @@ int pcg_reserve(PcgWork& w, int n, bool fp64) {
         const int cap = (int)(n * 1.25) + 4096;
         const size_t nch = ((size_t)cap + kChunk - 1) / kChunk + 1;
         w.nchCap = (int)nch;
-        BNN_CUDA_CHECK(cudaMalloc(&w.x, cap * sizeof(float)));
-        BNN_CUDA_CHECK(cudaMalloc(&w.r, cap * sizeof(float)));
-        BNN_CUDA_CHECK(cudaMalloc(&w.z, cap * sizeof(float)));
-        BNN_CUDA_CHECK(cudaMalloc(&w.s0, cap * sizeof(float)));
-        BNN_CUDA_CHECK(cudaMalloc(&w.s1, cap * sizeof(float)));
-        BNN_CUDA_CHECK(cudaMalloc(&w.q, cap * sizeof(float)));
-        BNN_CUDA_CHECK(cudaMalloc(&w.d32, cap * sizeof(float)));
-        BNN_CUDA_CHECK(cudaMalloc(&w.r32, cap * sizeof(float)));
-        BNN_CUDA_CHECK(cudaMalloc(&w.rec, cap * sizeof(int4)));
-        BNN_CUDA_CHECK(cudaMalloc(&w.part, 3 * nch * sizeof(double)));
-        BNN_CUDA_CHECK(cudaMalloc(&w.gs, sizeof(GridSync)));
+        BNN_CUDA_CHECK(dev_alloc(&w.x, cap * sizeof(float)));
+        BNN_CUDA_CHECK(dev_alloc(&w.r, cap * sizeof(float)));
+        BNN_CUDA_CHECK(dev_alloc(&w.z, cap * sizeof(float)));
+        BNN_CUDA_CHECK(dev_alloc(&w.s0, cap * sizeof(float)));
+        BNN_CUDA_CHECK(dev_alloc(&w.s1, cap * sizeof(float)));
+        BNN_CUDA_CHECK(dev_alloc(&w.q, cap * sizeof(float)));
+        BNN_CUDA_CHECK(dev_alloc(&w.d32, cap * sizeof(float)));
+        BNN_CUDA_CHECK(dev_alloc(&w.r32, cap * sizeof(float)));
+        BNN_CUDA_CHECK(dev_alloc(&w.rec, cap * sizeof(int4)));
+        BNN_CUDA_CHECK(dev_alloc(&w.part, 3 * nch * sizeof(double)));
+        BNN_CUDA_CHECK(dev_alloc(&w.gs, sizeof(GridSync)));
         BNN_CUDA_CHECK(cudaMemset(w.gs, 0, sizeof(GridSync)));
-        BNN_CUDA_CHECK(cudaMalloc(&w.partMaxF, nch * sizeof(float)));
-        BNN_CUDA_CHECK(cudaMalloc(&w.partMaxD, nch * sizeof(double)));
+        BNN_CUDA_CHECK(dev_alloc(&w.partMaxF, nch * sizeof(float)));
+        BNN_CUDA_CHECK(dev_alloc(&w.partMaxD, nch * sizeof(double)));
         w.cap = cap;
     }
     for(auto& e : w.ev)
         if(!e) BNN_CUDA_CHECK(cudaEventCreate(&e));
     if(!w.st32[0]) {
         // single-reduction solve: double-buffered row records and partials
-        for(int b = 0; b < 2; ++b) BNN_CUDA_CHECK(cudaMalloc(&w.st32[b], w.cap * sizeof(float4)));
-        BNN_CUDA_CHECK(cudaMalloc(&w.cgPart, 4 * (size_t)w.nchCap * sizeof(double)));
-        BNN_CUDA_CHECK(cudaMalloc(&w.cgMax, 2 * (size_t)w.nchCap * sizeof(double)));
+        for(int b = 0; b < 2; ++b) BNN_CUDA_CHECK(dev_alloc(&w.st32[b], w.cap * sizeof(float4)));
+        BNN_CUDA_CHECK(dev_alloc(&w.cgPart, 4 * (size_t)w.nchCap * sizeof(double)));
+        BNN_CUDA_CHECK(dev_alloc(&w.cgMax, 2 * (size_t)w.nchCap * sizeof(double)));
     }
     if(fp64 && !w.st64[0])
-        for(int b = 0; b < 2; ++b) BNN_CUDA_CHECK(cudaMalloc(&w.st64[b], w.cap * 4 * sizeof(double)));
+        for(int b = 0; b < 2; ++b) BNN_CUDA_CHECK(dev_alloc(&w.st64[b], w.cap * 4 * sizeof(double)));
     if(fp64 && !w.x64) {
-        BNN_CUDA_CHECK(cudaMalloc(&w.x64, w.cap * sizeof(double)));
-        BNN_CUDA_CHECK(cudaMalloc(&w.r64, w.cap * sizeof(double)));
-        BNN_CUDA_CHECK(cudaMalloc(&w.z64, w.cap * sizeof(double)));
-        BNN_CUDA_CHECK(cudaMalloc(&w.s064, w.cap * sizeof(double)));
-        BNN_CUDA_CHECK(cudaMalloc(&w.s164, w.cap * sizeof(double)));
-        BNN_CUDA_CHECK(cudaMalloc(&w.q64, w.cap * sizeof(double)));
-        BNN_CUDA_CHECK(cudaMalloc(&w.inv64, w.cap * sizeof(double)));
+        BNN_CUDA_CHECK(dev_alloc(&w.x64, w.cap * sizeof(double)));
+        BNN_CUDA_CHECK(dev_alloc(&w.r64, w.cap * sizeof(double)));
+        BNN_CUDA_CHECK(dev_alloc(&w.z64, w.cap * sizeof(double)));
+        BNN_CUDA_CHECK(dev_alloc(&w.s064, w.cap * sizeof(double)));
+        BNN_CUDA_CHECK(dev_alloc(&w.s164, w.cap * sizeof(double)));
+        BNN_CUDA_CHECK(dev_alloc(&w.q64, w.cap * sizeof(double)));
+        BNN_CUDA_CHECK(dev_alloc(&w.inv64, w.cap * sizeof(double)));
     }
     return BNN_OK;
 }
@@ -1533,7 +1533,7 @@ void pcg_release(PcgWork& w) {
                    (void*)w.part, (void*)w.partMaxF, (void*)w.partMaxD, (void*)w.x64, (void*)w.r64, (void*)w.z64,
                    (void*)w.s064, (void*)w.s164, (void*)w.q64, (void*)w.inv64, (void*)w.gs, (void*)w.st32[0],
                    (void*)w.st32[1], (void*)w.st64[0], (void*)w.st64[1], (void*)w.cgPart, (void*)w.cgMax})
-        if(p) cudaFree(p);
+        if(p) dev_free(p);
     w = PcgWork();
 }
 
@@ -1628,7 +1628,7 @@ int pcg_solve(PcgWork& w, int n, const float* rhs, const float* diag, const floa
         rec = w.rec;
         if(coef) {
             // off-diagonal values ride along as 2 float4 per row
-            if(!w.coefRow) BNN_CUDA_CHECK(cudaMalloc(&w.coefRow, 2 * (size_t)w.cap * sizeof(float4)));
+            if(!w.coefRow) BNN_CUDA_CHECK(dev_alloc(&w.coefRow, 2 * (size_t)w.cap * sizeof(float4)));
             { k_pack_coef<<<nb, 256, 0, s>>>(n, coef, w.coefRow); bnn_note_launch(); }
             coefRow = w.coefRow;
         }
