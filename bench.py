@@ -416,6 +416,9 @@ def run_ours(args, ws, rank, local):
                        "stage_ms_per_step": {k: v / args.steps for k, v in stage_tot.items()},
                        "stage_gbs": stage_gbs},
         }
+        if ws == 1 and N_GRID == 256 and not args.no_extras:
+            solver.close()
+            line["detail"]["more_workloads"] = _more_workloads()
         if args.per_step:
             # every timed sub-step (numbered from 1 over the whole run, warm-up included)
             line["detail"]["per_step"] = [
@@ -807,6 +810,47 @@ def _box_system(nx, ny, nz, seed=1):
     return diag, nbr, -dt, rhs
 
 
+def _more_workloads() -> dict:
+    """The other configurations' headline numbers, measured in the same run (each workload in
+    its own process, after the headline solver has released its memory): the 256-scene
+    batch (config 4), the served Poisson stream (config 5), and the 256^3 step with FP64 PCG
+    and with refined FP32 PCG, both to 1e-8 (config 2's two precision runs)."""
+    import subprocess
+    runs = {
+        "batch_256_scenes": ["--workload", "batch", "--steps", "10", "--warmup", "3"],
+        "serve_poisson": ["--workload", "serve", "--workers", "8"],
+        "fp64_pcg_to_1e-8": ["--pcg-mode", "fp64", "--tol", "1e-8", "--steps", "10", "--warmup", "5",
+                             "--no-cpu-baseline", "--skip-e2e", "--no-extras"],
+        "refined_pcg_to_1e-8": ["--pcg-mode", "refined", "--steps", "10", "--warmup", "5", "--no-cpu-baseline",
+                                "--skip-e2e", "--no-extras"],
+    }
+    keep = ("metric", "value", "unit", "ms_per_step", "steps", "warmup", "latency_ms", "step_latency_ms",
+            "request_latency_s", "queue_wait_s", "completed_requests", "gpu_launches", "clocks", "seconds")
+    out = {"note": "each measured by this bench.py run in a child process (same box, after the headline)"}
+    for name, extra in runs.items():
+        try:
+            r = subprocess.run([sys.executable, os.path.abspath(__file__), *extra], capture_output=True, text=True,
+                               timeout=600, env=dict(os.environ))
+            lines = [json.loads(l) for l in r.stdout.splitlines() if l.startswith("{")]
+            if r.returncode != 0 or not lines:
+                out[name] = {"error": f"exit {r.returncode}: {r.stderr.strip()[-300:]}"}
+                continue
+            d = lines[-1]
+            rec = {k: d[k] for k in keep if k in d}
+            rec["config"] = {k: v for k, v in d.get("config", {}).items() if k in ("workload", "pcg", "scenes", "requests",
+                                                                                  "particles_rank0", "particles")}
+            if d.get("e2e"):
+                rec["e2e"] = {"value": d["e2e"]["value"], "api": d["e2e"].get("api")}
+            det = d.get("detail", {})
+            for k in ("per_scene_streams", "one_scene_at_a_time", "pcg_iterations_per_step", "stage_ms_per_step"):
+                if k in det:
+                    rec[k] = det[k]
+            out[name] = rec
+        except Exception as e:  # noqa: BLE001 -- a failing extra must not take the headline line with it
+            out[name] = {"error": repr(e)[:300]}
+    return out
+
+
 def run_pcg(args, ws, rank, local):
     torch, dist = _torch_dist(ws, local)
     from banana_b200 import capi, pcg_solve_7pt
@@ -930,6 +974,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tile-shape", type=int, default=None,
                     help="flip: use this P2G tile shape (bnn_set_tile_shape) instead of the tuner's choice")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="flip at 256^3 on one GPU: skip the other configurations' runs in detail.more_workloads")
     ap.add_argument("--per-step", action="store_true",
                     help="flip: add every timed sub-step's stage times to the line (detail.per_step)")
     ap.add_argument("--no-compare", action="store_true",
