@@ -172,8 +172,8 @@ static int reserve_particles(bnn_flip* h, uint32_t n) {
             BNN_CUDA_CHECK(dev_alloc(&h->C9[b], 9 * st * sizeof(float)));
     }
     BNN_CUDA_CHECK(dev_alloc(&h->g3, 3 * st * sizeof(float)));
-    // two spare records: the gathers load records in aligned pairs
-    BNN_CUDA_CHECK(dev_alloc(&h->rec, (4 * st + 2) * sizeof(float4)));
+    // per-particle records of the P2G + SDF pass: 3 stencil planes and the positions
+    BNN_CUDA_CHECK(dev_alloc(&h->rec, 4 * st * sizeof(float4)));
     BNN_CUDA_CHECK(dev_alloc(&h->bboxPart, 6 * ((st + 255) / 256) * sizeof(int)));
     BNN_CUDA_CHECK(dev_alloc(&h->cellOf, st * sizeof(uint32_t)));
     BNN_CUDA_CHECK(dev_alloc(&h->slot, st * sizeof(uint32_t)));
