@@ -37,10 +37,11 @@ __device__ __forceinline__ float interp_face(const float* __restrict__ a, int sx
                  lerpf(lerpf(v001, v101, fi), lerpf(v011, v111, fi), fj), fk);
 }
 
-// Same trilinear sample of (a - b), the FLIP velocity change dVels = velocities - oldVels
-// (FLIP_Solver.cpp:115-121) formed tap by tap, as if the difference array existed.
-__device__ __forceinline__ float interp_face_diff(const float* __restrict__ a, const float* __restrict__ o, int sx,
-                                                  int sy, int sz, float px, float py, float pz) {
+// interp_face of a (*val) and the same trilinear sample of (a - o) (*diff), from one load of
+// each tap: the grid velocity and the FLIP velocity change dVels = velocities - oldVels
+// (FLIP_Solver.cpp:115-121), the difference formed tap by tap as if that array existed
+__device__ __forceinline__ void interp_face_pair(const float* __restrict__ a, const float* __restrict__ o, int sx,
+                                                 int sy, int sz, float px, float py, float pz, float* val, float* diff) {
     int i, j, k;
     float fi, fj, fk;
     bary(px, i, fi, sx);
@@ -48,12 +49,17 @@ __device__ __forceinline__ float interp_face_diff(const float* __restrict__ a, c
     bary(pz, k, fk, sz);
     const size_t sxy = (size_t)sx * sy;
     const size_t b = (size_t)k * sxy + (size_t)j * sx + i;
-#define D_(off) (__ldg(a + b + (off)) - __ldg(o + b + (off)))
-    float v000 = D_(0), v100 = D_(1), v010 = D_(sx), v110 = D_(sx + 1);
-    float v001 = D_(sxy), v101 = D_(sxy + 1), v011 = D_(sxy + sx), v111 = D_(sxy + sx + 1);
-#undef D_
-    return lerpf(lerpf(lerpf(v000, v100, fi), lerpf(v010, v110, fi), fj),
-                 lerpf(lerpf(v001, v101, fi), lerpf(v011, v111, fi), fj), fk);
+    const size_t off[8] = {0, 1, (size_t)sx, (size_t)sx + 1, sxy, sxy + 1, sxy + sx, sxy + sx + 1};
+    float va[8], vd[8];
+#pragma unroll
+    for(int t = 0; t < 8; ++t) {
+        va[t] = __ldg(a + b + off[t]);
+        vd[t] = va[t] - __ldg(o + b + off[t]);
+    }
+    *val = lerpf(lerpf(lerpf(va[0], va[1], fi), lerpf(va[2], va[3], fi), fj),
+                 lerpf(lerpf(va[4], va[5], fi), lerpf(va[6], va[7], fi), fj), fk);
+    *diff = lerpf(lerpf(lerpf(vd[0], vd[1], fi), lerpf(vd[2], vd[3], fi), fj),
+                  lerpf(lerpf(vd[4], vd[5], fi), lerpf(vd[6], vd[7], fi), fj), fk);
 }
 
 // PIC_Solver::getVelocityFromGrid(gridPos) (PIC_Solver.cpp:1119-1133)
@@ -1299,15 +1305,16 @@ __global__ void __launch_bounds__(256) k_g2p(int n, GridDesc g, const float* __r
     const float gz = (pos6[2 * stride + p] - g.bmin[2]) / g.dx;
     const int G0 = g.G[0], G1 = g.G[1], G2 = g.G[2];
     float gv[3];
-    vel_from_grid(g, u, v, w, gx, gy, gz, gv);
     if(kind == 1) {
+        vel_from_grid(g, u, v, w, gx, gy, gz, gv);
 #pragma unroll
         for(int d = 0; d < 3; ++d) vel3[d * stride + p] = gv[d];
     } else {
+        // the grid velocity and its change at the particle, from the same taps
         float dg[3];
-        dg[0] = interp_face_diff(u, ou, G0 + 1, G1, G2, gx, gy - 0.5f, gz - 0.5f);
-        dg[1] = interp_face_diff(v, ov, G0, G1 + 1, G2, gx - 0.5f, gy, gz - 0.5f);
-        dg[2] = interp_face_diff(w, ow, G0, G1, G2 + 1, gx - 0.5f, gy - 0.5f, gz);
+        interp_face_pair(u, ou, G0 + 1, G1, G2, gx, gy - 0.5f, gz - 0.5f, &gv[0], &dg[0]);
+        interp_face_pair(v, ov, G0, G1 + 1, G2, gx - 0.5f, gy, gz - 0.5f, &gv[1], &dg[1]);
+        interp_face_pair(w, ow, G0, G1, G2 + 1, gx - 0.5f, gy - 0.5f, gz, &gv[2], &dg[2]);
 #pragma unroll
         for(int d = 0; d < 3; ++d) {
             const float pv = vel3[d * stride + p];
@@ -1386,13 +1393,14 @@ __device__ __forceinline__ void g2p_move_body(Blk blk, int n, const GridDesc& g,
         float x = p6[p], y = p6[stride + p], z = p6[2 * stride + p];
         float gx = (x - g.bmin[0]) / g.dx, gy = (y - g.bmin[1]) / g.dx, gz = (z - g.bmin[2]) / g.dx;
         float gv[3];
-        vel_from_grid(g, u, v, w, gx, gy, gz, gv);
         {
+            // the grid velocity (getVelocityFromGrid) and its change (FLIP_Solver.cpp:125-133)
+            // at the particle, from the same taps
             const int G0 = g.G[0], G1 = g.G[1], G2 = g.G[2];
             float dg[3];
-            dg[0] = interp_face_diff(u, ou, G0 + 1, G1, G2, gx, gy - 0.5f, gz - 0.5f);
-            dg[1] = interp_face_diff(v, ov, G0, G1 + 1, G2, gx - 0.5f, gy, gz - 0.5f);
-            dg[2] = interp_face_diff(w, ow, G0, G1, G2 + 1, gx - 0.5f, gy - 0.5f, gz);
+            interp_face_pair(u, ou, G0 + 1, G1, G2, gx, gy - 0.5f, gz - 0.5f, &gv[0], &dg[0]);
+            interp_face_pair(v, ov, G0, G1 + 1, G2, gx - 0.5f, gy, gz - 0.5f, &gv[1], &dg[1]);
+            interp_face_pair(w, ow, G0, G1, G2 + 1, gx - 0.5f, gy - 0.5f, gz, &gv[2], &dg[2]);
             float* vel3 = p6 + 3 * stride;
 #pragma unroll
             for(int d = 0; d < 3; ++d) {
