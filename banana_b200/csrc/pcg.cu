@@ -555,9 +555,13 @@ __global__ void __launch_bounds__(kLanes, pcg_min_blocks<VT, COEF>()) k_pcg_pers
         first = false;
     }
 #ifdef BNN_PCG_TIMING
-    if(threadIdx.x == 0 && blockIdx.x < 2)
-        printf("blk %d iters %u  cycles/iter: phaseA %.0f bar1 %.0f red1 %.0f phaseB %.0f bar2 %.0f red2 %.0f\n", (int)blockIdx.x, iter,
-               tc[0] / (double)iter, tc[1] / (double)iter, tc[2] / (double)iter, tc[3] / (double)iter, tc[4] / (double)iter, tc[5] / (double)iter);
+    if(threadIdx.x == 0) {
+        unsigned smid;
+        asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+        printf("blk %d sm %u iters %u  cycles/iter: phaseA %.0f bar1 %.0f red1 %.0f phaseB %.0f bar2 %.0f red2 %.0f\n",
+               (int)blockIdx.x, smid, iter, tc[0] / (double)iter, tc[1] / (double)iter, tc[2] / (double)iter,
+               tc[3] / (double)iter, tc[4] / (double)iter, tc[5] / (double)iter);
+    }
 #endif
     if(blockIdx.x == 0 && threadIdx.x == 0) {
         a.st->iter = iter;

@@ -131,6 +131,95 @@ def test_pcg_7pt_grid_rows_packed_matches_oracle(bnn, oracle_mod, mode, omode, f
             assert np.array_equal(x, xo)
 
 
+def _slot_system(nbr, seed):
+    """Diagonal (every missing neighbour counted as a face to air, so the matrix is
+    strictly diagonally dominant), right-hand side and CSR (columns in slot order, the
+    solver's summation order) of a system given as slot neighbours."""
+    rng = np.random.default_rng(seed)
+    n = len(nbr)
+    dt = np.float32(1.0 / 30)
+    cnt = (nbr >= 0).sum(1)
+    diag = (cnt * dt + (6 - cnt) * dt / np.float32(0.5)).astype(np.float32)
+    rhs = (rng.standard_normal(n) * 1e-3).astype(np.float32)
+    rs, ci, va = [0], [], []
+    for q in range(n):
+        for c in nbr[q, :3]:
+            if c >= 0:
+                ci.append(c); va.append(-dt)
+        ci.append(q); va.append(diag[q])
+        for c in nbr[q, 3:]:
+            if c >= 0:
+                ci.append(c); va.append(-dt)
+        rs.append(len(ci))
+    return diag, -dt, rhs, (np.array(rs), np.array(ci), np.array(va, np.float32))
+
+
+def _grid_slots(act):
+    """Slot neighbours (-z,-y,-x,+x,+y,+z) of the active cells of a (z, y, x) mask, rows
+    in cell order."""
+    nz, ny, nx = act.shape
+    row = -np.ones(act.shape, np.int64)
+    row[act] = np.arange(int(act.sum()))
+    k, j, i = np.nonzero(act)
+    r = row[k, j, i]
+    nbr = -np.ones((int(act.sum()), 6), np.int32)
+    for slot, (dk, dj, di) in enumerate([(-1, 0, 0), (0, -1, 0), (0, 0, -1), (0, 0, 1), (0, 1, 0), (1, 0, 0)]):
+        kk, jj, ii = k + dk, j + dj, i + di
+        ok = (kk >= 0) & (kk < nz) & (jj >= 0) & (jj < ny) & (ii >= 0) & (ii < nx)
+        nb = np.full(len(r), -1, np.int64)
+        nb[ok] = row[kk[ok], jj[ok], ii[ok]]
+        nbr[r, slot] = nb
+    return nbr
+
+
+def _layout_system(kind):
+    """Grid-row systems of unusual shape for the packed-record solve: 'box' (a box of
+    cells with holes), 'wide_rows' (z layers of 120 then 2000 cells along x: y neighbours
+    up to ~2000 rows away) and 'unordered_z' (x chains whose z partners are shuffled in
+    blocks of 16 rows: valid grid rows whose -z / +z neighbours are not in row order)."""
+    rng = np.random.default_rng(21)
+    if kind == "box":
+        nbr = _grid_slots(rng.random((30, 36, 40)) > 0.08)
+    elif kind == "wide_rows":
+        act = rng.random((6, 6, 2000)) > 0.08
+        act[:3, :, 120:] = False
+        nbr = _grid_slots(act)
+    else:
+        half = 6 * 2048
+        n = 2 * half
+        nbr = -np.ones((n, 6), np.int32)
+        r = np.arange(n)
+        chain = (r % 64) != 0  # x chains of 64 rows
+        nbr[chain, 2] = r[chain] - 1
+        nxt = np.roll(chain, -1) & (r < n - 1)
+        nbr[nxt, 3] = r[nxt] + 1
+        perm = np.arange(half).reshape(-1, 16)
+        for b in perm:
+            rng.shuffle(b)
+        perm = perm.ravel()
+        nbr[np.arange(half), 5] = half + perm
+        nbr[half + perm, 0] = np.arange(half)
+    return (nbr,) + _slot_system(nbr, 22)
+
+
+@pytest.mark.parametrize("kind", ["box", "wide_rows", "unordered_z"])
+@pytest.mark.parametrize("mode,omode", [("fp32", 0), ("fp64", 1), ("refined", 2)])
+def test_pcg_grid_row_layouts_match_oracle(bnn, oracle_mod, kind, mode, omode):
+    """Grid rows whose y neighbours lie far away, or whose z partners are out of row order,
+    still take the packed-record solve (its x neighbours by warp shuffle, the others by row
+    distance) and equal the oracle bit for bit."""
+    nbr, diag, off, rhs, (rs, ci, va) = _layout_system(kind)
+    tol = 1e-8 if mode == "refined" else 1e-6
+    xo, so = oracle_mod.pcg(rs, ci, va, rhs, tol, 5000, omode, inner_tol=1e-3)
+    assert so["success"]
+    x, st = bnn.pcg_solve_7pt(diag, nbr, off, rhs, tol, 5000, mode=bnn.capi.PCG_MODE[mode], inner_tol=1e-3)
+    assert st["success"] == 1 and st["iterations"] == so["iterations"]
+    if mode == "fp32":
+        assert np.array_equal(x.astype(np.float32), xo.astype(np.float32))
+    else:
+        assert np.array_equal(x, xo)
+
+
 def test_barrier_wait_gives_up_and_device_stays_usable(bnn, oracle_mod):
     """A block waiting at a barrier that nothing completes (sized for two blocks, one
     launched) gives up after its limit and reports a timeout; the device then solves a
