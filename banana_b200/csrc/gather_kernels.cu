@@ -188,10 +188,12 @@ __device__ __forceinline__ void pull_partials(const float* __restrict__ sm, int 
 }
 
 // Minimum squared distance from the particles of halo cell h (layer cy) to the centres of
-// the 27 cells around it.  exact: a particle outside the grid (sorted into the clamped
-// cell) reaches only the clamped 3x3x3 range of its own cell (PIC_Solver.cpp:633-635).
-template<class SH>
-__device__ __forceinline__ void sdf_partials(const TileArgs& a, int x0, int z0, int cy, int h, bool exact,
+// the 27 cells around it.  EXACT (some particle left the grid, so the whole launch takes
+// it): a particle outside the grid (sorted into the clamped cell) reaches only the clamped
+// 3x3x3 range of its own cell (PIC_Solver.cpp:633-635); otherwise every particle reaches
+// all 27 and no per-slot test runs.
+template<class SH, bool EXACT>
+__device__ __forceinline__ void sdf_partials(const TileArgs& a, int x0, int z0, int cy, int h,
                                              float* __restrict__ sm) {
     constexpr int kNH = SH::kNH;
     const float inf = __int_as_float(0x7f800000);
@@ -225,7 +227,7 @@ __device__ __forceinline__ void sdf_partials(const TileArgs& a, int x0, int z0, 
                 dzz[o] = ddz * ddz;
             }
             bool okx[3] = {true, true, true}, oky[3] = {true, true, true}, okz[3] = {true, true, true};
-            if(exact) {
+            if constexpr(EXACT) {
                 const int ci = (int)((L.x - g.bmin[0]) / g.dx);
                 const int cj = (int)((L.y - g.bmin[1]) / g.dx);
                 const int ck = (int)((L.z - g.bmin[2]) / g.dx);
@@ -245,7 +247,8 @@ __device__ __forceinline__ void sdf_partials(const TileArgs& a, int x0, int z0, 
                     for(int ix = 0; ix < 3; ++ix) {
                         const float d2 = (dxx[ix] + dyy[iy]) + dzz[iz];  // glm::length2: (x*x + y*y) + z*z
                         const int s = (iz * 3 + iy) * 3 + ix;
-                        m[s] = fminf(m[s], (okx[ix] && oky[iy] && okz[iz]) ? d2 : inf);
+                        if constexpr(EXACT) m[s] = fminf(m[s], (okx[ix] && oky[iy] && okz[iz]) ? d2 : inf);
+                        else m[s] = fminf(m[s], d2);
                     }
         }
     }
@@ -309,8 +312,9 @@ struct GivenTile {
     __device__ __forceinline__ unsigned y() const { return by; }
 };
 
-// One block of the pass: tile (x, z) of face columns, y-chunk y
-template<bool P2G, class SH, class Tile>
+// One block of the pass: tile (x, z) of face columns, y-chunk y.  EXACT: some particle
+// left the grid (the same for the whole launch; see sdf_partials).
+template<bool P2G, class SH, bool EXACT, class Tile>
 __device__ __forceinline__ void tile_body(const TileArgs& a, const Tile tile) {
     constexpr int kTZ = SH::kTZ, kYC = SH::kYC;
     extern __shared__ float sm[];
@@ -336,7 +340,6 @@ __device__ __forceinline__ void tile_body(const TileArgs& a, const Tile tile) {
             return;
         }
     }
-    const bool exact = (a.st->flags & BNN_FLAG_OUT_OF_GRID) != 0u;
     const float inf = __int_as_float(0x7f800000);
     // accumulators of face layers cy - 1 + j (v, whose own axis is the walk, uses j = 1, 2)
     float uS[3] = {0.f, 0.f, 0.f}, uW[3] = {0.f, 0.f, 0.f};
@@ -361,7 +364,7 @@ __device__ __forceinline__ void tile_body(const TileArgs& a, const Tile tile) {
                 if(owner) pull_partials<2, SH>(sm, tx, tz, wS, wW);
                 __syncthreads();
             }
-            sdf_partials<SH>(a, x0, z0, cy, t, exact, sm);
+            sdf_partials<SH, EXACT>(a, x0, z0, cy, t, sm);
             __syncthreads();
             if(owner) pull_sdf<SH>(sm, tx, tz, aM);
             __syncthreads();
@@ -386,9 +389,16 @@ __device__ __forceinline__ void tile_body(const TileArgs& a, const Tile tile) {
         aM[0] = aM[1]; aM[1] = aM[2]; aM[2] = inf;
     }
 }
+// The rare launch in which some particle left the grid, kept out of line so that its
+// per-slot tests do not weigh on the registers of the common path
+template<bool P2G, class SH, class Tile>
+__device__ __noinline__ void tile_body_exact(const TileArgs& a, const Tile tile) {
+    tile_body<P2G, SH, true>(a, tile);
+}
 template<bool P2G, class SH>
 __global__ void __launch_bounds__(SH::kThreads, SH::kMinBlocks) k_p2g_sdf_tile(const __grid_constant__ TileArgs a) {
-    tile_body<P2G, SH>(a, OwnTile{});
+    if((a.st->flags & BNN_FLAG_OUT_OF_GRID) != 0u) tile_body_exact<P2G, SH>(a, OwnTile{});
+    else tile_body<P2G, SH, false>(a, OwnTile{});
 }
 
 // Batched: the tiles of all scenes of a batch in one launch (P: per-scene tile prefix);
@@ -401,7 +411,9 @@ __global__ void __launch_bounds__(SH::kThreads, SH::kMinBlocks) kb_p2g_sdf_tile(
     const TileArgs& a = A[q];
     const unsigned gx = (unsigned)((a.g.G[0] + 1 + kTX - 1) / kTX);
     const unsigned gz = (unsigned)((a.g.G[2] + 1 + SH::kTZ - 1) / SH::kTZ);
-    tile_body<true, SH>(a, GivenTile{b.x % gx, (b.x / gx) % gz, b.x / (gx * gz)});
+    const GivenTile tile{b.x % gx, (b.x / gx) % gz, b.x / (gx * gz)};
+    if((a.st->flags & BNN_FLAG_OUT_OF_GRID) != 0u) tile_body_exact<true, SH>(a, tile);  // the scene's flag
+    else tile_body<true, SH, false>(a, tile);
 }
 static_assert(kHX == 32, "a warp is one row of halo cells");
 
