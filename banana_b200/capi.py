@@ -81,7 +81,8 @@ class BatchParams(C.Structure):
 class BatchStats(C.Structure):
     _fields_ = [("scenes", C.c_uint32), ("failed", C.c_uint32), ("particle_steps", C.c_uint64),
                 ("pcg_iterations", C.c_uint64), ("wall_ms", C.c_double), ("max_scene_ms", C.c_double),
-                ("staged_scenes", C.c_uint32), ("reserved", C.c_uint32)]
+                ("staged_scenes", C.c_uint32), ("graph_instantiations", C.c_uint16),
+                ("graph_updates", C.c_uint16)]
 
 
 class PcgStats(C.Structure):

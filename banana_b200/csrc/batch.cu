@@ -193,6 +193,8 @@ extern "C" int bnn_batch_step(bnn_batch* b, bnn_batch_stats* stats) {
     }
     b->cvWork.notify_all();
     int batchRc = BNN_OK;
+    unsigned long long inst0 = 0, upd0 = 0;
+    for(const auto& g : b->staged.seg) { inst0 += g.instantiated; upd0 += g.updated; }
     if(!staged.empty()) {
         // the staged scenes on this thread, meanwhile
         const int ns = (int)staged.size();
@@ -220,6 +222,12 @@ extern "C" int bnn_batch_step(bnn_batch* b, bnn_batch_stats* stats) {
     bnn_batch_stats st{};
     st.wall_ms = wall;
     st.staged_scenes = (uint32_t)staged.size();
+    {
+        unsigned long long inst1 = 0, upd1 = 0;
+        for(const auto& g : b->staged.seg) { inst1 += g.instantiated; upd1 += g.updated; }
+        st.graph_instantiations = (uint16_t)(inst1 - inst0);
+        st.graph_updates = (uint16_t)(upd1 - upd0);
+    }
     for(auto& s : b->scenes) {
         ++st.scenes;
         if(s->status != BNN_OK) {

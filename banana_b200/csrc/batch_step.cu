@@ -93,29 +93,49 @@ void batch_step_release(BatchStepWork& w) {
 }
 
 // Runs a segment of launches: directly, or as a CUDA graph captured from them (again when
-// the launch shapes `sig` changed since the last capture) and replayed.
+// the launch shapes `sig` changed since the last capture) and replayed.  A new capture
+// with the same launches in the same order (scenes come and go, block counts change) is
+// written into the existing executable graph (cudaGraphExecUpdate), which costs far less
+// host time than building a new one; only a different sequence of launches is built anew.
 template<class F> static int run_segment(StagedGraph& g, const std::vector<uint64_t>& sig, cudaStream_t s,
                                          bool graph, F body) {
     if(!graph) return body(false);
     if(!g.exec || g.sig != sig) {
-        if(g.exec) cudaGraphExecDestroy(g.exec);
-        g.exec = nullptr;
         const long long l0 = (long long)bnn_launch_count();
         BNN_CUDA_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         const int rc = body(true);
         cudaGraph_t cg = nullptr;
         const cudaError_t e = cudaStreamEndCapture(s, &cg);
-        g.kernels = (long long)bnn_launch_count() - l0;
-        bnn_note_launches(-g.kernels);  // captured, not run
+        const long long kernels = (long long)bnn_launch_count() - l0;
+        bnn_note_launches(-kernels);  // captured, not run
         if(rc != BNN_OK || e != cudaSuccess) {
             if(cg) cudaGraphDestroy(cg);
             if(rc != BNN_OK) return rc;
             BNN_CUDA_CHECK(e);
         }
-        const cudaError_t ei = cudaGraphInstantiate(&g.exec, cg, 0);
+        bool done = false;
+        if(g.exec && kernels == g.kernels) {
+            cudaGraphExecUpdateResultInfo info;
+            if(cudaGraphExecUpdate(g.exec, cg, &info) == cudaSuccess) {
+                done = true;
+                ++g.updated;
+            } else {
+                (void)cudaGetLastError();  // a refused update leaves no error behind
+            }
+        }
+        if(!done) {
+            if(g.exec) cudaGraphExecDestroy(g.exec);
+            g.exec = nullptr;
+            const cudaError_t ei = cudaGraphInstantiate(&g.exec, cg, 0);
+            if(ei != cudaSuccess) {
+                g.exec = nullptr;
+                cudaGraphDestroy(cg);
+                BNN_CUDA_CHECK(ei);
+            }
+            ++g.instantiated;
+        }
         cudaGraphDestroy(cg);
-        if(ei != cudaSuccess) g.exec = nullptr;
-        BNN_CUDA_CHECK(ei);
+        g.kernels = kernels;
         g.sig = sig;
     }
     BNN_CUDA_CHECK(cudaGraphLaunch(g.exec, s));

@@ -11,6 +11,9 @@ struct StagedGraph {
     cudaGraphExec_t exec = nullptr;
     std::vector<uint64_t> sig;
     long long kernels = 0;     // kernel launches the segment holds
+    // new captures so far: built into a new executable graph / written into the existing
+    // one (same launches, other shapes or arguments: cudaGraphExecUpdate)
+    unsigned long long instantiated = 0, updated = 0;
 };
 
 // Device tables, pinned mirror and stream of the batched step, kept between steps

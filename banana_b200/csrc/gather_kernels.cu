@@ -114,19 +114,28 @@ __device__ __forceinline__ bool meets_particles(const DevState* st, const int lo
     return true;
 }
 
-// Partials of component D for halo cell h of cell layer cy into sm (slot-major planes).
+// The particles [b, e) of halo cell h of the current cell layer (none for a halo cell
+// outside the grid), read once per layer for the four passes over them
+__device__ __forceinline__ void cell_range(const TileArgs& a, int x0, int z0, int cy, int h, uint32_t& b, uint32_t& e) {
+    const int cx = x0 - 1 + h % kHX, cz = z0 - 1 + h / kHX;
+    b = e = 0u;
+    if(cx >= 0 && cx < a.g.G[0] && cz >= 0 && cz < a.g.G[2]) {
+        const size_t c = ((size_t)cz * a.g.G[1] + cy) * a.g.G[0] + cx;
+        b = __ldg(a.cellStart + c);
+        e = __ldg(a.cellStart + c + 1);
+    }
+}
+
+// Partials of component D for halo cell h (particles [b, e)) into sm (slot-major planes).
 template<int D, class SH>
-__device__ __forceinline__ void cell_partials(const TileArgs& a, int x0, int z0, int cy, int h, float* __restrict__ sm) {
+__device__ __forceinline__ void cell_partials(const TileArgs& a, int h, uint32_t b, uint32_t e, float* __restrict__ sm) {
     constexpr int kNH = SH::kNH;
     constexpr int NX = D == 0 ? 2 : 3, NY = D == 1 ? 2 : 3, NZ = D == 2 ? 2 : 3;
     constexpr int NS = NX * NY * NZ;
     float S[NS], W[NS];
 #pragma unroll
     for(int s = 0; s < NS; ++s) { S[s] = 0.0f; W[s] = 0.0f; }
-    const int cx = x0 - 1 + h % kHX, cz = z0 - 1 + h / kHX;
-    if(cx >= 0 && cx < a.g.G[0] && cz >= 0 && cz < a.g.G[2]) {
-        const size_t c = ((size_t)cz * a.g.G[1] + cy) * a.g.G[0] + cx;
-        const uint32_t b = __ldg(a.cellStart + c), e = __ldg(a.cellStart + c + 1);
+    {
         const float4* __restrict__ recD = a.rec + (size_t)D * a.stride;
         // the next record is loaded while this one is summed
         float4 Ln = b < e ? __ldg(recD + b) : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -193,8 +202,8 @@ __device__ __forceinline__ void pull_partials(const float* __restrict__ sm, int 
 // 3x3x3 range of its own cell (PIC_Solver.cpp:633-635); otherwise every particle reaches
 // all 27 and no per-slot test runs.
 template<class SH, bool EXACT>
-__device__ __forceinline__ void sdf_partials(const TileArgs& a, int x0, int z0, int cy, int h,
-                                             float* __restrict__ sm) {
+__device__ __forceinline__ void sdf_partials(const TileArgs& a, int x0, int z0, int cy, int h, uint32_t b,
+                                             uint32_t e, float* __restrict__ sm) {
     constexpr int kNH = SH::kNH;
     const float inf = __int_as_float(0x7f800000);
     float m[27];
@@ -202,9 +211,7 @@ __device__ __forceinline__ void sdf_partials(const TileArgs& a, int x0, int z0, 
     for(int s = 0; s < 27; ++s) m[s] = inf;
     const GridDesc& g = a.g;
     const int cx = x0 - 1 + h % kHX, cz = z0 - 1 + h / kHX;
-    if(cx >= 0 && cx < g.G[0] && cz >= 0 && cz < g.G[2]) {
-        const size_t c = ((size_t)cz * g.G[1] + cy) * g.G[0] + cx;
-        const uint32_t b = __ldg(a.cellStart + c), e = __ldg(a.cellStart + c + 1);
+    if(b < e) {
         const float4* __restrict__ pos = a.rec + 3 * a.stride;
         // Grid::getWorldCoordinate(i + 0.5, ...) (Grid.h:186-194) of the 27 target cells
         float sx[3], sy[3], sz[3];
@@ -348,23 +355,25 @@ __device__ __forceinline__ void tile_body(const TileArgs& a, const Tile tile) {
     float aM[3] = {inf, inf, inf};
     for(int cy = yA - 1; cy <= yB; ++cy) {
         if(cy >= 0 && cy < g.G[1]) {
+            uint32_t pb, pe;
+            cell_range(a, x0, z0, cy, t, pb, pe);
             if constexpr(P2G) {
-                cell_partials<0, SH>(a, x0, z0, cy, t, sm);
+                cell_partials<0, SH>(a, t, pb, pe, sm);
                 __syncthreads();
                 if(owner) pull_partials<0, SH>(sm, tx, tz, uS, uW);
                 __syncthreads();
                 if(cy < yB) {
-                    cell_partials<1, SH>(a, x0, z0, cy, t, sm);
+                    cell_partials<1, SH>(a, t, pb, pe, sm);
                     __syncthreads();
                     if(owner) pull_partials<1, SH>(sm, tx, tz, vS, vW);
                     __syncthreads();
                 }
-                cell_partials<2, SH>(a, x0, z0, cy, t, sm);
+                cell_partials<2, SH>(a, t, pb, pe, sm);
                 __syncthreads();
                 if(owner) pull_partials<2, SH>(sm, tx, tz, wS, wW);
                 __syncthreads();
             }
-            sdf_partials<SH, EXACT>(a, x0, z0, cy, t, sm);
+            sdf_partials<SH, EXACT>(a, x0, z0, cy, t, pb, pe, sm);
             __syncthreads();
             if(owner) pull_sdf<SH>(sm, tx, tz, aM);
             __syncthreads();

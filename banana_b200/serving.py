@@ -74,6 +74,8 @@ class ServeStats:
     admitted: int = 0
     waits_for_memory: int = 0                          # admissions refused for the budget
     max_running: int = 0
+    graph_instantiations: int = 0                      # staged-step segments built into new CUDA graphs
+    graph_updates: int = 0                             # ... written into the existing graphs
 
     def summary(self, results: list, seconds: float) -> dict:
         lat = [r.latency for r in results]
@@ -81,6 +83,7 @@ class ServeStats:
         return {"particle_steps_per_s": self.particle_steps / seconds if seconds > 0 else 0.0,
                 "batch_steps": self.batch_steps, "completed": len(results), "admitted": self.admitted,
                 "waits_for_memory": self.waits_for_memory, "max_running": self.max_running,
+                "graph_instantiations": self.graph_instantiations, "graph_updates": self.graph_updates,
                 "step_latency_ms": {"p50": pct(self.step_ms, 50), "p99": pct(self.step_ms, 99)},
                 "request_latency_s": {"p50": pct(lat, 50), "p99": pct(lat, 99)},
                 "queue_wait_s": {"p50": pct([r.wait for r in results], 50),
@@ -136,6 +139,8 @@ class SceneServer:
         self.stats.step_ms.append(float(st["wall_ms"]))
         self.stats.particle_steps += int(st["particle_steps"])
         self.stats.batch_steps += 1
+        self.stats.graph_instantiations += int(st.get("graph_instantiations", 0))
+        self.stats.graph_updates += int(st.get("graph_updates", 0))
         done = []
         for sid in list(self.running):
             q, admitted = self.running[sid]

@@ -447,6 +447,8 @@ def run_batch(args, ws, rank, local):
     torch, dist = _torch_dist(ws, local)
     from banana_b200 import FlipBatch, capi, dist as bdist, scenes
 
+    if args.tile_shape is not None:
+        capi.set_tile_shape(args.tile_shape)
     specs = scenes.batch_scene_specs()
     costs = []
     for s in specs:
@@ -561,6 +563,8 @@ def run_serve(args, ws, rank, local):
     torch, dist = _torch_dist(ws, local)
     from banana_b200 import FlipBatch, capi, scenes
     from banana_b200.serving import Request, SceneServer
+    if args.tile_shape is not None:
+        capi.set_tile_shape(args.tile_shape)
 
     reqs = scenes.serve_requests(args.requests)
     mine = [(k, q) for k, q in enumerate(reqs) if k % ws == rank]
@@ -600,6 +604,8 @@ def run_serve(args, ws, rank, local):
                            "time_limit_s": args.time_limit},
                 "completed_requests": summ["completed"], "admitted_requests": summ["admitted"],
                 "waits_for_memory": summ["waits_for_memory"], "max_running": summ["max_running"],
+                "graphs": {"instantiated": summ["graph_instantiations"], "updated": summ["graph_updates"]},
+                "tile_shapes_tuned": len(capi.tile_tuning()),
                 "request_latency_s": summ["request_latency_s"], "queue_wait_s": summ["queue_wait_s"],
                 "step_latency_ms": summ["step_latency_ms"], "seconds": te,
                 "gpu_launches": int(launches), "clocks": clk}
@@ -973,7 +979,8 @@ def main():
                     help="fp32 / fp64 PCG: relative tolerance (the refined mode's outer tolerance is 1e-8)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tile-shape", type=int, default=None,
-                    help="flip: use this P2G tile shape (bnn_set_tile_shape) instead of the tuner's choice")
+                    help="flip / batch / serve: use this P2G tile shape (bnn_set_tile_shape) instead of the "
+                         "tuner's choice")
     ap.add_argument("--no-extras", action="store_true",
                     help="flip at 256^3 on one GPU: skip the other configurations' runs in detail.more_workloads")
     ap.add_argument("--per-step", action="store_true",

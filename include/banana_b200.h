@@ -199,7 +199,10 @@ typedef struct bnn_batch_stats {
     double   wall_ms;          /* host wall time of the batch step */
     double   max_scene_ms;     /* slowest scene's step */
     uint32_t staged_scenes;    /* scenes advanced by the staged (one launch per stage) step */
-    uint32_t reserved;
+    uint16_t graph_instantiations; /* segments of the staged step captured and built into a new
+                                      CUDA graph in this step (0-2) */
+    uint16_t graph_updates;    /* segments captured again and written into the existing graph
+                                  (same launches, other shapes; 0-2) */
 } bnn_batch_stats;
 int bnn_batch_create(const bnn_batch_params* params, bnn_batch** out);
 int bnn_batch_destroy(bnn_batch* b);

@@ -38,10 +38,18 @@ def test_batch_scenes_equal_lone_solvers(bnn, mode):
     for q in range(3):
         cfg, pos, vel = scenes.batch_scene(SPECS[q])
         ids[q] = b.add_scene(cfg, pos, vel)
+    graphs = []
     for _ in range(5):
         st = b.step()
         assert st["scenes"] == 3 and st["failed"] == 0
         assert st["staged_scenes"] == (3 if staged else 0)
+        graphs.append((st["graph_instantiations"], st["graph_updates"]))
+    if mode == "staged":
+        # both segments built once (the first step tunes the tile shape outside a capture),
+        # then replayed while the scenes stay the same
+        assert sum(i for i, _ in graphs) == 2 and graphs[-1] == (0, 0)
+    else:
+        assert graphs == [(0, 0)] * 5
     for q in range(3):
         pg, vg = b.get_scene(ids[q])
         pl, vl = _lone(bnn, SPECS[q], 5)
@@ -51,9 +59,12 @@ def test_batch_scenes_equal_lone_solvers(bnn, mode):
     b.remove_scene(ids[1])
     cfg, pos, vel = scenes.batch_scene(SPECS[3])
     ids[3] = b.add_scene(cfg, pos, vel)
-    for _ in range(3):
+    for k in range(3):
         st = b.step()
         assert st["scenes"] == 3
+        if mode == "staged" and k == 0:
+            # other scenes, other launch shapes: the segments are captured again
+            assert st["graph_instantiations"] + st["graph_updates"] >= 1
     for q, steps in ((0, 8), (2, 8), (3, 3)):
         pg, _ = b.get_scene(ids[q])
         pl, _ = _lone(bnn, SPECS[q], steps)
