@@ -447,6 +447,8 @@ extern "C" void bnn_set_error(const char* msg);
 // allocation is usable on every stream when dev_alloc returns; dev_free requires that no
 // work on the memory is pending (every API call that frees ends its streams' work first).
 cudaError_t dev_alloc_bytes(void** p, size_t bytes);
+// Sets up this device's stream-ordered memory pool (keeps freed memory for reuse) once
+cudaError_t mem_pool_setup();
 void dev_free_ptr(void* p);
 template<class T> inline cudaError_t dev_alloc(T** p, size_t bytes) { return dev_alloc_bytes((void**)p, bytes); }
 inline cudaError_t dev_free(const void* p) {

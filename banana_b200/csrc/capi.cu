@@ -26,7 +26,7 @@ extern "C" const char* bnn_version(void) { return "banana_b200 0.1 (sm_100a)"; }
 // driver at every synchronisation; allocations and frees are ordered on the calling
 // thread's default stream, which the handles never queue work on.
 static std::atomic<uint64_t> g_poolSetUp{0};  // bit per device ordinal
-cudaError_t dev_alloc_bytes(void** p, size_t bytes) {
+cudaError_t mem_pool_setup() {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if(e != cudaSuccess) return e;
@@ -39,6 +39,11 @@ cudaError_t dev_alloc_bytes(void** p, size_t bytes) {
         }
         g_poolSetUp.fetch_or(bit, std::memory_order_acq_rel);
     }
+    return cudaSuccess;
+}
+cudaError_t dev_alloc_bytes(void** p, size_t bytes) {
+    cudaError_t e = mem_pool_setup();
+    if(e != cudaSuccess) return e;
     e = cudaMallocAsync(p, bytes ? bytes : 1, cudaStreamPerThread);
     if(e != cudaSuccess) return e;
     return cudaStreamSynchronize(cudaStreamPerThread);

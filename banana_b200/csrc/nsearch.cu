@@ -160,8 +160,12 @@ __global__ void k_zvalues(const float* __restrict__ pos, uint32_t n, float inv, 
     z[p] = morton3d(c[0], c[1], c[2]);
 }
 
-__global__ void k_ns_keys(const float* __restrict__ pos, uint32_t n, float inv, int* __restrict__ keys3,
-                          int* __restrict__ kmin, int* __restrict__ kmax) {
+// Hash keys of the points and their box: reduced over the block first, so the six
+// words of the box see one atomic per block instead of one per warp
+__global__ void __launch_bounds__(256) k_ns_keys(const float* __restrict__ pos, uint32_t n, float inv,
+                                                 int* __restrict__ keys3, int* __restrict__ kmin,
+                                                 int* __restrict__ kmax) {
+    __shared__ int sMin[3][8], sMax[3][8];
     const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     int k[3] = {INT_MAX, INT_MAX, INT_MAX}, km[3] = {INT_MIN, INT_MIN, INT_MIN};
     if(p < n) {
@@ -169,6 +173,7 @@ __global__ void k_ns_keys(const float* __restrict__ pos, uint32_t n, float inv, 
 #pragma unroll
         for(int d = 0; d < 3; ++d) { keys3[3 * p + d] = k[d]; km[d] = k[d]; }
     }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
     for(int d = 0; d < 3; ++d) {
         int a = k[d], b = km[d];
@@ -176,7 +181,15 @@ __global__ void k_ns_keys(const float* __restrict__ pos, uint32_t n, float inv, 
             a = min(a, __shfl_xor_sync(0xffffffffu, a, off));
             b = max(b, __shfl_xor_sync(0xffffffffu, b, off));
         }
-        if((threadIdx.x & 31) == 0) { atomicMin(kmin + d, a); atomicMax(kmax + d, b); }
+        if(lane == 0) { sMin[d][w] = a; sMax[d][w] = b; }
+    }
+    __syncthreads();
+    if(threadIdx.x < 3) {
+        const int d = threadIdx.x;
+        int a = INT_MAX, b = INT_MIN;
+        for(int q = 0; q < (int)(blockDim.x >> 5); ++q) { a = min(a, sMin[d][q]); b = max(b, sMax[d][q]); }
+        if(a != INT_MAX) atomicMin(kmin + d, a);
+        if(b != INT_MIN) atomicMax(kmax + d, b);
     }
 }
 
@@ -198,13 +211,11 @@ __global__ void k_gather_pos(const float* __restrict__ pos, const uint32_t* __re
 
 // NeighborSearch::query3D (NeighborSearch.cpp:530-692) per point: every other point of the
 // 27 hash cells with (dx*dx + dy*dy) + dz*dz < r^2.  One thread per point in cell-sorted
-// order, so a warp shares its candidate cells.  pass 0 counts, pass 1 writes.
-template<bool WRITE>
-__global__ void __launch_bounds__(256) k_ns_query(const float4* __restrict__ sp, const uint32_t* __restrict__ scid,
+// order, so a warp shares its candidate cells.  This pass counts each point's neighbours;
+// k_ns_query_write then writes them, visiting the candidates in the same order.
+__global__ void __launch_bounds__(256) k_ns_count(const float4* __restrict__ sp, const uint32_t* __restrict__ scid,
                                                   uint32_t n, const uint32_t* __restrict__ cellStart, int d0, int d1,
-                                                  float r2, uint32_t* __restrict__ counts,
-                                                  const unsigned long long* __restrict__ offsets,
-                                                  uint32_t* __restrict__ idx) {
+                                                  float r2, uint32_t* __restrict__ counts) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if(i >= n) return;
     const float4 a = sp[i];
@@ -212,7 +223,6 @@ __global__ void __launch_bounds__(256) k_ns_query(const float4* __restrict__ sp,
     const uint32_t c = scid[i];
     const size_t plane = (size_t)d0 * d1;
     uint32_t cnt = 0;
-    unsigned long long o = WRITE ? offsets[self] : 0ull;
     for(int dz = -1; dz <= 1; ++dz)
         for(int dy = -1; dy <= 1; ++dy) {
             const size_t row = (size_t)((long long)c + dz * (long long)plane + dy * (long long)d0);
@@ -223,22 +233,96 @@ __global__ void __launch_bounds__(256) k_ns_query(const float4* __restrict__ sp,
                 if(other == self) continue;
                 const float t0 = a.x - q.x, t1 = a.y - q.y, t2 = a.z - q.z;
                 const float l2 = t0 * t0 + t1 * t1 + t2 * t2;
-                if(l2 < r2) {
-                    if(WRITE) idx[o + cnt] = other;
-                    ++cnt;
-                }
+                if(l2 < r2) ++cnt;
             }
         }
-    if(!WRITE) counts[self] = cnt;
+    counts[self] = cnt;
+}
+
+// The writing pass, its stores gathered per warp: each lane appends its
+// neighbours to its own row of a shared-memory buffer, and as soon as one lane's row is
+// full the warp writes every lane's buffered entries out, one lane's entries at a time
+// (lanes k write entry k: consecutive addresses), instead of 32 lanes storing into 32
+// different lists at every candidate.  The lanes walk their candidate ranges in step (the
+// warp's longest range; shorter ones idle), so the warp's votes see every lane.  Each list
+// holds exactly the entries k_ns_count counted, in its visiting order.
+constexpr int kNsBuf = 32;   // entries a lane's buffer row holds
+constexpr int kNsGroup = 4;  // candidates tested between two checks of the rows
+__global__ void __launch_bounds__(256) k_ns_query_write(const float4* __restrict__ sp, const uint32_t* __restrict__ scid,
+                                                        uint32_t n, const uint32_t* __restrict__ cellStart, int d0,
+                                                        int d1, float r2, const unsigned long long* __restrict__ offsets,
+                                                        uint32_t* __restrict__ idx) {
+    __shared__ uint32_t buf[256 / 32][32][kNsBuf + 1];  // +1: a lane's row starts in its own bank
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned full = 0xffffffffu;
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = i < n;
+    const float4 a = live ? sp[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const uint32_t self = __float_as_uint(a.w);
+    const uint32_t c = live ? scid[i] : 0u;
+    const size_t plane = (size_t)d0 * d1;
+    const unsigned long long o = live ? offsets[self] : 0ull;
+    unsigned long long written = 0;  // entries of this lane's list already in idx
+    uint32_t held = 0;               // entries in this lane's buffer row
+    uint32_t* row = buf[warp][lane];
+    auto flush = [&]() {
+        __syncwarp();
+        for(int L = 0; L < 32; ++L) {
+            const uint32_t cntL = __shfl_sync(full, held, L);
+            const unsigned long long dst = __shfl_sync(full, o + written, L);
+            if((uint32_t)lane < cntL) idx[dst + lane] = buf[warp][L][lane];
+        }
+        __syncwarp();
+        written += held;
+        held = 0;
+    };
+    for(int dz = -1; dz <= 1; ++dz)
+        for(int dy = -1; dy <= 1; ++dy) {
+            uint32_t b = 0, e = 0;
+            if(live) {
+                const size_t r = (size_t)((long long)c + dz * (long long)plane + dy * (long long)d0);
+                b = cellStart[r - 1];
+                e = cellStart[r + 2];
+            }
+            const uint32_t len = e - b;
+            uint32_t most = len;
+#pragma unroll
+            for(int off = 16; off > 0; off >>= 1) most = max(most, __shfl_xor_sync(full, most, off));
+            // candidates four at a time (their loads in flight together); a group adds at
+            // most four entries, so the warp writes out before any row could overflow
+            for(uint32_t t = 0; t < most; t += kNsGroup) {
+                float4 q[kNsGroup];
+#pragma unroll
+                for(int u = 0; u < kNsGroup; ++u) q[u] = t + u < len ? sp[b + t + u] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+                for(int u = 0; u < kNsGroup; ++u) {
+                    const uint32_t other = __float_as_uint(q[u].w);
+                    const float t0 = a.x - q[u].x, t1 = a.y - q[u].y, t2 = a.z - q[u].z;
+                    const float l2 = t0 * t0 + t1 * t1 + t2 * t2;
+                    if(t + u < len && other != self && l2 < r2) row[held++] = other;
+                }
+                if(__any_sync(full, held > (uint32_t)(kNsBuf - kNsGroup))) flush();
+            }
+        }
+    if(__any_sync(full, held != 0u)) flush();
 }
 } // namespace
 
 // ---- host helpers -------------------------------------------------------------------
 namespace {
+// Temporary device memory from the device's memory pool, allocated and freed in order on
+// the stream that uses it (no device-wide synchronisation, freed memory reused by the next
+// call)
 struct DevBuf {
     void* p = nullptr;
-    ~DevBuf() { if(p) cudaFree(p); }
-    cudaError_t alloc(size_t b) { return cudaMalloc(&p, b ? b : 1); }
+    cudaStream_t s = nullptr;
+    ~DevBuf() { if(p) cudaFreeAsync(p, s); }
+    cudaError_t alloc(size_t b, cudaStream_t st) {
+        const cudaError_t e = mem_pool_setup();
+        if(e != cudaSuccess) return e;
+        s = st;
+        return cudaMallocAsync(&p, b ? b : 1, st);
+    }
     template<class T> T* as() { return (T*)p; }
 };
 
@@ -248,7 +332,7 @@ template<class K>
 int radix_sort(const K* keys, size_t n, K* keysOut, uint32_t* permOut, cudaStream_t s) {
     if(n == 0) return BNN_OK;
     DevBuf bits, k2, v2, hist, ws;
-    BNN_CUDA_CHECK(bits.alloc(2 * sizeof(unsigned long long)));
+    BNN_CUDA_CHECK(bits.alloc(2 * sizeof(unsigned long long), s));
     unsigned long long init[2] = {0ull, ~0ull};
     BNN_CUDA_CHECK(cudaMemcpyAsync(bits.p, init, sizeof(init), cudaMemcpyHostToDevice, s));
     { k_key_bits<K><<<(unsigned)std::min<size_t>((n + 255) / 256, 4096), 256, 0, s>>>(keys, n, bits.as<unsigned long long>(),
@@ -263,11 +347,11 @@ int radix_sort(const K* keys, size_t n, K* keysOut, uint32_t* permOut, cudaStrea
         hi = 63 - __builtin_clzll(vary);
     }
     const unsigned ntiles = (unsigned)((n + kRTile - 1) / kRTile);
-    BNN_CUDA_CHECK(k2.alloc(n * sizeof(K)));
-    BNN_CUDA_CHECK(v2.alloc(n * sizeof(uint32_t)));
-    BNN_CUDA_CHECK(hist.alloc(((size_t)256 * ntiles + 1) * sizeof(uint32_t)));
+    BNN_CUDA_CHECK(k2.alloc(n * sizeof(K), s));
+    BNN_CUDA_CHECK(v2.alloc(n * sizeof(uint32_t), s));
+    BNN_CUDA_CHECK(hist.alloc(((size_t)256 * ntiles + 1) * sizeof(uint32_t), s));
     size_t wsb = scan_workspace_bytes((size_t)256 * ntiles);
-    if(wsb) BNN_CUDA_CHECK(ws.alloc(wsb));
+    if(wsb) BNN_CUDA_CHECK(ws.alloc(wsb, s));
     std::vector<int> shifts;
     for(int sh = lo; sh <= hi; sh += 8) shifts.push_back(sh);
     // ping-pong so that the last pass lands in keysOut / permOut
@@ -307,22 +391,22 @@ extern "C" int bnn_cell_sort(const float* pos_dev, uint32_t n, const float bmin[
     if(C >= 0xffffffffull) return BNN_ERR_NOT_SUPPORTED;
     cudaStream_t s = (cudaStream_t)stream;
     DevBuf oor, keysSorted;
-    BNN_CUDA_CHECK(oor.alloc(sizeof(unsigned)));
+    BNN_CUDA_CHECK(oor.alloc(sizeof(unsigned), s));
     BNN_CUDA_CHECK(cudaMemsetAsync(oor.p, 0, sizeof(unsigned), s));
     if(n) {
         { k_grid_cell_ids<<<(n + 255) / 256, 256, 0, s>>>(pos_dev, n, bmin[0], bmin[1], bmin[2], cell_size, ncells[0],
                                                          ncells[1], ncells[2], cell_id_dev, oor.as<unsigned>()); bnn_note_launch(); }
-        BNN_CUDA_CHECK(keysSorted.alloc((size_t)n * sizeof(uint32_t)));
+        BNN_CUDA_CHECK(keysSorted.alloc((size_t)n * sizeof(uint32_t), s));
         int rc = radix_sort<uint32_t>(cell_id_dev, n, keysSorted.as<uint32_t>(), sorted_idx_dev, s);
         if(rc != BNN_OK) return rc;
     }
     if(cell_start_dev) {
         DevBuf cnt, ws;
-        BNN_CUDA_CHECK(cnt.alloc(C * sizeof(uint32_t)));
+        BNN_CUDA_CHECK(cnt.alloc(C * sizeof(uint32_t), s));
         BNN_CUDA_CHECK(cudaMemsetAsync(cnt.p, 0, C * sizeof(uint32_t), s));
         if(n) { k_histogram<<<(n + 255) / 256, 256, 0, s>>>(cell_id_dev, n, cnt.as<uint32_t>()); bnn_note_launch(); }
         size_t wsb = scan_workspace_bytes(C);
-        if(wsb) BNN_CUDA_CHECK(ws.alloc(wsb));
+        if(wsb) BNN_CUDA_CHECK(ws.alloc(wsb, s));
         BNN_CUDA_CHECK(exclusive_scan_u32(cnt.as<uint32_t>(), cell_start_dev, C, ws.p, s));
     }
     unsigned h = 0;
@@ -340,7 +424,7 @@ extern "C" int bnn_z_sort(const float* pos_dev, uint32_t n, float radius, uint64
     const float inv = (float)(1.0 / (double)radius);
     { k_zvalues<<<(n + 255) / 256, 256, 0, s>>>(pos_dev, n, inv, (unsigned long long*)zvalue_dev); bnn_note_launch(); }
     DevBuf sorted;
-    BNN_CUDA_CHECK(sorted.alloc((size_t)n * sizeof(unsigned long long)));
+    BNN_CUDA_CHECK(sorted.alloc((size_t)n * sizeof(unsigned long long), s));
     int rc = radix_sort<unsigned long long>((const unsigned long long*)zvalue_dev, n, sorted.as<unsigned long long>(),
                                             perm_dev, s);
     if(rc != BNN_OK) return rc;
@@ -360,8 +444,8 @@ extern "C" int bnn_neighbors(const float* pos_dev, uint32_t n, float radius, uin
     const float inv = (float)(1.0 / (double)radius);
     const float r2 = radius * radius;
     DevBuf keys3, kmm, cid, cidSorted, order, sp, cnt, start, ws, counts, ws64;
-    BNN_CUDA_CHECK(keys3.alloc((size_t)n * 3 * sizeof(int)));
-    BNN_CUDA_CHECK(kmm.alloc(6 * sizeof(int)));
+    BNN_CUDA_CHECK(keys3.alloc((size_t)n * 3 * sizeof(int), s));
+    BNN_CUDA_CHECK(kmm.alloc(6 * sizeof(int), s));
     int init[6] = {INT_MAX, INT_MAX, INT_MAX, INT_MIN, INT_MIN, INT_MIN};
     BNN_CUDA_CHECK(cudaMemcpyAsync(kmm.p, init, sizeof(init), cudaMemcpyHostToDevice, s));
     { k_ns_keys<<<(n + 255) / 256, 256, 0, s>>>(pos_dev, n, inv, keys3.as<int>(), kmm.as<int>(), kmm.as<int>() + 3); bnn_note_launch(); }
@@ -372,26 +456,26 @@ extern "C" int bnn_neighbors(const float* pos_dev, uint32_t n, float radius, uin
     const long long d0 = (long long)hk[3] - hk[0] + 3, d1 = (long long)hk[4] - hk[1] + 3, d2 = (long long)hk[5] - hk[2] + 3;
     const long long V = d0 * d1 * d2;
     if(V > (1ll << 30)) return BNN_ERR_NOT_SUPPORTED;
-    BNN_CUDA_CHECK(cid.alloc((size_t)n * sizeof(uint32_t)));
+    BNN_CUDA_CHECK(cid.alloc((size_t)n * sizeof(uint32_t), s));
     { k_dense_cell<<<(n + 255) / 256, 256, 0, s>>>(keys3.as<int>(), n, kmm.as<int>(), (int)d0, (int)d1, cid.as<uint32_t>()); bnn_note_launch(); }
-    BNN_CUDA_CHECK(cidSorted.alloc((size_t)n * sizeof(uint32_t)));
-    BNN_CUDA_CHECK(order.alloc((size_t)n * sizeof(uint32_t)));
+    BNN_CUDA_CHECK(cidSorted.alloc((size_t)n * sizeof(uint32_t), s));
+    BNN_CUDA_CHECK(order.alloc((size_t)n * sizeof(uint32_t), s));
     int rc = radix_sort<uint32_t>(cid.as<uint32_t>(), n, cidSorted.as<uint32_t>(), order.as<uint32_t>(), s);
     if(rc != BNN_OK) return rc;
-    BNN_CUDA_CHECK(sp.alloc((size_t)n * sizeof(float4)));
+    BNN_CUDA_CHECK(sp.alloc((size_t)n * sizeof(float4), s));
     { k_gather_pos<<<(n + 255) / 256, 256, 0, s>>>(pos_dev, order.as<uint32_t>(), n, sp.as<float4>()); bnn_note_launch(); }
-    BNN_CUDA_CHECK(cnt.alloc((size_t)V * sizeof(uint32_t)));
-    BNN_CUDA_CHECK(start.alloc(((size_t)V + 1) * sizeof(uint32_t)));
+    BNN_CUDA_CHECK(cnt.alloc((size_t)V * sizeof(uint32_t), s));
+    BNN_CUDA_CHECK(start.alloc(((size_t)V + 1) * sizeof(uint32_t), s));
     BNN_CUDA_CHECK(cudaMemsetAsync(cnt.p, 0, (size_t)V * sizeof(uint32_t), s));
     { k_histogram<<<(n + 255) / 256, 256, 0, s>>>(cid.as<uint32_t>(), n, cnt.as<uint32_t>()); bnn_note_launch(); }
     size_t wsb = scan_workspace_bytes((size_t)V);
-    if(wsb) BNN_CUDA_CHECK(ws.alloc(wsb));
+    if(wsb) BNN_CUDA_CHECK(ws.alloc(wsb, s));
     BNN_CUDA_CHECK(exclusive_scan_u32(cnt.as<uint32_t>(), start.as<uint32_t>(), (size_t)V, ws.p, s));
-    BNN_CUDA_CHECK(counts.alloc((size_t)n * sizeof(uint32_t)));
-    { k_ns_query<false><<<(n + 255) / 256, 256, 0, s>>>(sp.as<float4>(), cidSorted.as<uint32_t>(), n, start.as<uint32_t>(),
-                                                       (int)d0, (int)d1, r2, counts.as<uint32_t>(), nullptr, nullptr); bnn_note_launch(); }
+    BNN_CUDA_CHECK(counts.alloc((size_t)n * sizeof(uint32_t), s));
+    { k_ns_count<<<(n + 255) / 256, 256, 0, s>>>(sp.as<float4>(), cidSorted.as<uint32_t>(), n, start.as<uint32_t>(),
+                                                 (int)d0, (int)d1, r2, counts.as<uint32_t>()); bnn_note_launch(); }
     size_t wsb64 = scan_workspace_bytes_u64(n);
-    if(wsb64) BNN_CUDA_CHECK(ws64.alloc(wsb64));
+    if(wsb64) BNN_CUDA_CHECK(ws64.alloc(wsb64, s));
     BNN_CUDA_CHECK(exclusive_scan_u32_to_u64(counts.as<uint32_t>(), (unsigned long long*)offsets_dev, n, ws64.p, s));
     uint64_t tot = 0;
     BNN_CUDA_CHECK(cudaMemcpyAsync(&tot, offsets_dev + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
@@ -399,9 +483,9 @@ extern "C" int bnn_neighbors(const float* pos_dev, uint32_t n, float radius, uin
     if(total) *total = tot;
     if(tot > capacity) return BNN_ERR_CAPACITY;
     if(tot && !idx_dev) return BNN_ERR_INVALID_ARGUMENT;
-    { k_ns_query<true><<<(n + 255) / 256, 256, 0, s>>>(sp.as<float4>(), cidSorted.as<uint32_t>(), n, start.as<uint32_t>(),
-                                                      (int)d0, (int)d1, r2, nullptr,
-                                                      (const unsigned long long*)offsets_dev, idx_dev); bnn_note_launch(); }
+    { k_ns_query_write<<<(n + 255) / 256, 256, 0, s>>>(sp.as<float4>(), cidSorted.as<uint32_t>(), n, start.as<uint32_t>(),
+                                                      (int)d0, (int)d1, r2, (const unsigned long long*)offsets_dev,
+                                                      idx_dev); bnn_note_launch(); }
     BNN_CUDA_CHECK(cudaGetLastError());
     BNN_CUDA_CHECK(cudaStreamSynchronize(s));
     return BNN_OK;
