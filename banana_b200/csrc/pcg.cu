@@ -971,14 +971,17 @@ __global__ void __launch_bounds__(kLanes, cg1_min_blocks<VT>()) k_pcg_cg1(Cg1Arg
 // Batched persistent PCG: the Jacobi systems of many scenes (FP32 vectors, grid rows in
 // packed records, face weights 1) in one cooperative launch.  A scene's rows are cut into
 // the same 2048-row chunks as in a lone solve, and the chunks of all scenes are numbered
-// one after another; a block owns a contiguous range of them, so it meets only a few
-// scenes.  After each grid barrier a block reduces the partials of each of its scenes in
-// the canonical order over that scene's chunks alone, so every scene gets exactly the
-// scalars, iterates and iteration count of a lone k_pcg_persistent solve.  Scenes that have
-// finished skip their chunks; the loop ends, for all blocks at the same barrier, when a
-// counter of unfinished scenes (decremented by the block owning a scene's first chunk)
-// reads 0 right after the first barrier of an iteration -- no scene can finish between
-// the last decrement before that barrier and the read.
+// one after another and striped over the blocks (block b takes chunks b, b + grid, ...),
+// so as scenes finish the chunks of those still iterating stay spread over the whole grid
+// and every block keeps its share of the remaining work.  After each grid barrier a block
+// reduces the partials of each scene it works on, a warp per scene
+// (warp_reduce_partials: the canonical order over that scene's chunks alone), so every
+// scene gets exactly the scalars, iterates and iteration count of a lone
+// k_pcg_persistent solve.  Scenes that have finished skip their chunks; the loop ends, for
+// all blocks at the same barrier, when a counter of unfinished scenes (decremented by the
+// block owning a scene's first chunk) reads 0 right after the first barrier of an
+// iteration -- no scene can finish between the last decrement before that barrier and the
+// read.
 // Yield: a second counter holds the chunks of the unfinished scenes.  When it has fallen to
 // yieldBelow (read at the same point), every block leaves at the end of that iteration and
 // the owner of each unfinished scene saves its scalars (iterations, rho, beta, tol, last
@@ -986,7 +989,49 @@ __global__ void __launch_bounds__(kLanes, cg1_min_blocks<VT>()) k_pcg_cg1(Cg1Arg
 // resume set, spread over the whole grid, and they carry on with exactly the iterates they
 // had.  Which of the s buffers is the new one follows from the iteration count (even: s0).
 // ---------------------------------------------------------------------------------
-constexpr int kBatchSlots = 64;  // scenes a block's chunk range may touch
+constexpr int kBatchSlots = 64;  // scenes a block's chunks may belong to
+
+// reduce_partials_bcast's result (the canonical sum over nch chunk partials and their max)
+// formed by one warp: lane t stands for the block's threads t, t + 32, ..., t + 224 (the
+// threads of block_sum_max_256's first level that lane t of warp 0 combines), each summing
+// its partials t', t' + 256, ... in order, then the same association and shuffle tree.
+// The result is valid in lane 0.
+__device__ __forceinline__ void warp_reduce_partials(const double* part, const float* pmax, int nch, double& sum,
+                                                     float& mx) {
+    const int lane = threadIdx.x & 31;
+    double acc[8];
+    float m[8];
+#pragma unroll
+    for(int v = 0; v < 8; ++v) {
+        acc[v] = 0.0;
+        m[v] = 0.f;
+        for(int c = lane + 32 * v; c < nch; c += kLanes) {
+            acc[v] = acc[v] + __ldcg(part + c);
+            if(pmax) {
+                const float o = __ldcg(pmax + c);
+                m[v] = m[v] > o ? m[v] : o;
+            }
+        }
+    }
+    // virtual threads lane + 32 v: level 128 pairs v with v + 4, level 64 v = 0/2 with 4/6 ...
+    const double a0 = acc[0] + acc[4];
+    const double a1 = acc[2] + acc[6];
+    const double a2 = acc[1] + acc[5];
+    const double a3 = acc[3] + acc[7];
+    double c = (a0 + a1) + (a2 + a3);
+#pragma unroll
+    for(int off = 16; off > 0; off >>= 1) c = c + __shfl_down_sync(0xffffffffu, c, off);
+    float x = 0.f;
+    if(pmax) {
+        x = m[0];
+#pragma unroll
+        for(int q = 1; q < 8; ++q) { const float o = m[q]; x = x > o ? x : o; }
+#pragma unroll
+        for(int off = 16; off > 0; off >>= 1) { const float o = __shfl_down_sync(0xffffffffu, x, off); x = x > o ? x : o; }
+    }
+    sum = c;
+    mx = x;
+}
 struct BatchPcgScene {
     int n;                     // rows
     int resume;                // carry on from the scalars saved at a yield
@@ -1016,48 +1061,70 @@ struct BatchPcgArgs {
 
 __global__ void __launch_bounds__(kLanes, pcg_min_blocks<float, false>()) k_pcg_batch(BatchPcgArgs a) {
     constexpr int kRowGroup = pcg_row_group<float, false>();
+    constexpr int kWarps = kLanes / 32;
     __shared__ double smd[kLanes];
     __shared__ float smv[kLanes];
     __shared__ double sRho[kBatchSlots];
     __shared__ float sTol[kBatchSlots], sResid[kBatchSlots], sAlpha[kBatchSlots], sBeta[kBatchSlots];
     __shared__ unsigned sIter[kBatchSlots];
-    __shared__ int sState[kBatchSlots];  // 0 iterating, 1 finished, 2 no solve
+    // 0 iterating, 1 finished, 2 no solve, 3 finished in this iteration's first half
+    // (counted off after the second barrier)
+    __shared__ int sState[kBatchSlots];
+    __shared__ int sScene[kBatchSlots];
+    __shared__ unsigned char sSlotOf[kBatchSlots];  // slot of the block's k-th chunk
+    __shared__ int sNslots;
     const unsigned nb = gridDim.x;
     unsigned sense = 0;
-    const int lane = threadIdx.x & 31;
-    const unsigned c0 = min(blockIdx.x * a.perBlock, a.total), c1 = min(c0 + a.perBlock, a.total);
-    const int sFirst = c0 < c1 ? seg_of(a.cp, a.ns, c0) : 0;
-    const int nslots = c0 < c1 ? seg_of(a.cp, a.ns, c1 - 1) - sFirst + 1 : 0;
-
-    // A scene's result, by the block that owns its first chunk.  The counter of unfinished
-    // scenes is read right after the first barrier of an iteration, so it may only change
-    // between the second barrier and the next first one: a scene finishing between the two
-    // (deferred) is counted off after the second.
-    auto count_off = [&](int s) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // The block's chunks are blockIdx.x + k nb (k < nmine): striped over the grid, so the
+    // chunks of the scenes still iterating stay spread over all blocks as others finish.
+    // Its slots are the scenes those chunks belong to, in order.
+    const unsigned nmine = blockIdx.x < a.total ? (a.total - 1 - blockIdx.x) / nb + 1 : 0u;
+    if(nmine > (unsigned)kBatchSlots) {  // the host keeps chunks per block within the slot table
+        if(threadIdx.x == 0) atomicOr(a.flags, BNN_FLAG_TIMEOUT);
+        return;
+    }
+    if(threadIdx.x == 0) {
+        int m = 0, last = -1;
+        for(unsigned k = 0; k < nmine; ++k) {
+            const int sc = seg_of(a.cp, a.ns, blockIdx.x + k * nb);
+            if(sc != last) { sScene[m++] = sc; last = sc; }
+            sSlotOf[k] = (unsigned char)(m - 1);
+        }
+        sNslots = m;
+    }
+    __syncthreads();
+    const int nslots = sNslots;
+    // the block owning a scene's first chunk reports its result and counts it off
+    auto owner = [&](int sc) { return __ldg(a.cp + sc) % nb == blockIdx.x; };
+    auto count_off = [&](int sc) {
         atomicSub(a.remaining, 1u);
-        atomicSub(a.active, __ldg(a.cp + s + 1) - __ldg(a.cp + s));
+        atomicSub(a.active, __ldg(a.cp + sc + 1) - __ldg(a.cp + sc));
     };
-    auto finish = [&](int j, unsigned success, bool deferred) {
-        const int s = sFirst + j;
+    // one thread: the scene of slot j is done (deferred: counted off after the second barrier)
+    auto finish1 = [&](int j, unsigned success, bool deferred) {
+        const int sc = sScene[j];
         sState[j] = deferred ? 3 : 1;
-        if(threadIdx.x == 0 && __ldg(a.cp + s) >= c0) {
-            DevState* d = a.sc[s].dst;
+        if(owner(sc)) {
+            DevState* d = a.sc[sc].dst;
             d->iter = sIter[j];
             d->success = success;
             d->done = 1;
             d->resid = sResid[j];
             d->resid64 = sResid[j];
-            if(!deferred) count_off(s);
+            if(!deferred) count_off(sc);
         }
     };
+    auto chunks_of = [&](int sc) { return (int)(__ldg(a.cp + sc + 1) - __ldg(a.cp + sc)); };
 
     // ---- init: r = rhs, x = 0, z = D^-1 r; partial z.r and max|r| (not for a resumed scene)
-    for(unsigned c = c0; c < c1; ++c) {
-        const int s = seg_of(a.cp, a.ns, c);
-        const BatchPcgScene& S = a.sc[s];
+    for(unsigned k = 0; k < nmine; ++k) {
+        const unsigned c = blockIdx.x + k * nb;
+        const int sc = sScene[sSlotOf[k]];
+        const BatchPcgScene& S = a.sc[sc];
         if(S.resume) continue;
         const int n = S.n;
-        const unsigned lc = c - __ldg(a.cp + s);
+        const unsigned lc = c - __ldg(a.cp + sc);
         double acc = 0.0;
         float m = 0.f;
         const size_t base = (size_t)lc * kChunk + threadIdx.x;
@@ -1081,49 +1148,54 @@ __global__ void __launch_bounds__(kLanes, pcg_min_blocks<float, false>()) k_pcg_
         if(threadIdx.x == 0) { S.part0[lc] = bs; S.partMax[lc] = bm; }
     }
     if(!grid_barrier(a.gs, nb, sense, a.flags, solve_barrier_limit())) return;
-    for(int j = 0; j < nslots; ++j) {
-        const int s = sFirst + j;
-        const BatchPcgScene& S = a.sc[s];
-        const int nch = (int)(__ldg(a.cp + s + 1) - __ldg(a.cp + s));
+    // the scenes' first scalars, a warp per slot
+    for(int j = warp; j < nslots; j += kWarps) {
+        const int sc = sScene[j];
+        const BatchPcgScene& S = a.sc[sc];
+        const int nch = chunks_of(sc);
         if(S.resume) {
             // the scalars saved at the yield
-            if(threadIdx.x == 0) {
+            if(lane == 0) {
                 const DevState* d = S.dst;
                 sIter[j] = d->iter; sRho[j] = d->rho; sBeta[j] = d->beta; sTol[j] = d->tol; sResid[j] = d->resid;
                 sState[j] = 0;
             }
-            __syncthreads();
             continue;
         }
-        if(threadIdx.x == 0) { sIter[j] = 0; sState[j] = nch > 0 ? 0 : 2; sBeta[j] = 0.f; }
-        __syncthreads();
-        if(nch == 0) continue;
-        double rho;
-        float resid;
-        reduce_partials_bcast<float>(S.part0, S.partMax, nch, smd, smv, rho, resid);
-        if(threadIdx.x == 0) { sRho[j] = rho; sResid[j] = resid; }
-        const float tolFactor = fmaxf(S.tolFactor, 1e-30f);
-        __syncthreads();
-        if(resid < FLT_MIN) {
-            finish(j, 1u, false);
-        } else {
-            if(threadIdx.x == 0) sTol[j] = tolFactor * resid;
-            if(rho < (double)FLT_MIN || isnan(rho) || S.maxIter == 0) finish(j, 0u, false);
+        double rho = 0.0;
+        float resid = 0.f;
+        if(nch > 0) warp_reduce_partials(S.part0, S.partMax, nch, rho, resid);
+        if(lane == 0) {
+            sIter[j] = 0;
+            sState[j] = nch > 0 ? 0 : 2;
+            sBeta[j] = 0.f;
+            if(nch > 0) {
+                sRho[j] = rho;
+                sResid[j] = resid;
+                const float tolFactor = fmaxf(S.tolFactor, 1e-30f);
+                if(resid < FLT_MIN) {
+                    finish1(j, 1u, false);
+                } else {
+                    sTol[j] = tolFactor * resid;
+                    if(rho < (double)FLT_MIN || isnan(rho) || S.maxIter == 0) finish1(j, 0u, false);
+                }
+            }
         }
-        __syncthreads();
     }
+    __syncthreads();
 
     // a scene's new s is s0 after an even number of iterations, as the lone solve's swap;
     // its first iteration (no s yet) is the one with 0 iterations done
     for(;;) {
         // ---- phase A: s = z + beta s_old, q = A s, partial s.q
-        for(unsigned c = c0; c < c1; ++c) {
-            const int s = seg_of(a.cp, a.ns, c);
-            const int jslot = s - sFirst;
+        for(unsigned k = 0; k < nmine; ++k) {
+            const int jslot = sSlotOf[k];
             if(sState[jslot] != 0) continue;
-            const BatchPcgScene& S = a.sc[s];
+            const unsigned c = blockIdx.x + k * nb;
+            const int sc = sScene[jslot];
+            const BatchPcgScene& S = a.sc[sc];
             const int n = S.n;
-            const unsigned lc = c - __ldg(a.cp + s);
+            const unsigned lc = c - __ldg(a.cp + sc);
             const float beta = sBeta[jslot];
             const float negoff = S.negoff;
             const float* __restrict__ zR = S.z;
@@ -1207,32 +1279,32 @@ __global__ void __launch_bounds__(kLanes, pcg_min_blocks<float, false>()) k_pcg_
         if(!grid_barrier(a.gs, nb, sense, a.flags, solve_barrier_limit())) return;
         if(ld_acquire_u32(a.remaining) == 0u) break;
         const bool yieldNow = a.yieldBelow != 0u && ld_acquire_u32(a.active) <= a.yieldBelow;
-        // alpha of every scene this block works on
-        for(int j = 0; j < nslots; ++j) {
+        // alpha of every scene this block works on, a warp per slot
+        for(int j = warp; j < nslots; j += kWarps) {
             if(sState[j] != 0) continue;
-            const int s = sFirst + j;
-            const BatchPcgScene& S = a.sc[s];
-            const int nch = (int)(__ldg(a.cp + s + 1) - __ldg(a.cp + s));
+            const int sc = sScene[j];
             double tmp;
             float unused2;
-            reduce_partials_bcast<float>(S.part1, (const float*)nullptr, nch, smd, smv, tmp, unused2);
-            if(tmp < (double)FLT_MIN) {
-                if(threadIdx.x == 0) ++sIter[j];
-                __syncthreads();
-                finish(j, 1u, true);
-            } else if(threadIdx.x == 0) {
-                sAlpha[j] = (float)(sRho[j] / tmp);
+            warp_reduce_partials(a.sc[sc].part1, nullptr, chunks_of(sc), tmp, unused2);
+            if(lane == 0) {
+                if(tmp < (double)FLT_MIN) {
+                    ++sIter[j];
+                    finish1(j, 1u, true);
+                } else {
+                    sAlpha[j] = (float)(sRho[j] / tmp);
+                }
             }
-            __syncthreads();
         }
+        __syncthreads();
         // ---- phase B: x += alpha s, r -= alpha q, max|r|, z = D^-1 r, partial z.r
-        for(unsigned c = c0; c < c1; ++c) {
-            const int s = seg_of(a.cp, a.ns, c);
-            const int jslot = s - sFirst;
+        for(unsigned k = 0; k < nmine; ++k) {
+            const int jslot = sSlotOf[k];
             if(sState[jslot] != 0) continue;
-            const BatchPcgScene& S = a.sc[s];
+            const unsigned c = blockIdx.x + k * nb;
+            const int sc = sScene[jslot];
+            const BatchPcgScene& S = a.sc[sc];
             const int n = S.n;
-            const unsigned lc = c - __ldg(a.cp + s);
+            const unsigned lc = c - __ldg(a.cp + sc);
             const float alpha = sAlpha[jslot];
             const float* __restrict__ sNew = (sIter[jslot] & 1u) ? S.s1 : S.s0;
             const size_t base = (size_t)lc * kChunk + threadIdx.x;
@@ -1269,43 +1341,42 @@ __global__ void __launch_bounds__(kLanes, pcg_min_blocks<float, false>()) k_pcg_
             if(threadIdx.x == 0) { S.part2[lc] = bs; S.partMax[lc] = bm; }
         }
         if(!grid_barrier(a.gs, nb, sense, a.flags, solve_barrier_limit())) return;
-        for(int j = 0; j < nslots; ++j) {
+        for(int j = warp; j < nslots; j += kWarps) {
             if(sState[j] == 3) {
-                if(threadIdx.x == 0 && __ldg(a.cp + sFirst + j) >= c0) count_off(sFirst + j);
-                __syncthreads();
-                if(threadIdx.x == 0) sState[j] = 1;
-                __syncthreads();
+                if(lane == 0) {
+                    if(owner(sScene[j])) count_off(sScene[j]);
+                    sState[j] = 1;
+                }
+                continue;
             }
             if(sState[j] != 0) continue;
-            const int s = sFirst + j;
-            const BatchPcgScene& S = a.sc[s];
-            const int nch = (int)(__ldg(a.cp + s + 1) - __ldg(a.cp + s));
+            const int sc = sScene[j];
+            const BatchPcgScene& S = a.sc[sc];
             double rhoNew;
             float resid;
-            reduce_partials_bcast<float>(S.part2, S.partMax, nch, smd, smv, rhoNew, resid);
-            if(threadIdx.x == 0) { ++sIter[j]; sResid[j] = resid; }
-            __syncthreads();
-            if(resid < sTol[j]) {
-                finish(j, 1u, false);
-            } else {
-                if(threadIdx.x == 0) {
+            warp_reduce_partials(S.part2, S.partMax, chunks_of(sc), rhoNew, resid);
+            if(lane == 0) {
+                ++sIter[j];
+                sResid[j] = resid;
+                if(resid < sTol[j]) {
+                    finish1(j, 1u, false);
+                } else {
                     sBeta[j] = (float)(rhoNew / sRho[j]);
                     sRho[j] = rhoNew;
-                }
-                __syncthreads();
-                if(sIter[j] >= S.maxIter) {
-                    if(threadIdx.x == 0 && __ldg(a.cp + s) >= c0) atomicOr(&S.dst->flags, BNN_FLAG_PCG_MAXITER);
-                    finish(j, 0u, false);
+                    if(sIter[j] >= S.maxIter) {
+                        if(owner(sc)) atomicOr(&S.dst->flags, BNN_FLAG_PCG_MAXITER);
+                        finish1(j, 0u, false);
+                    }
                 }
             }
-            __syncthreads();
         }
+        __syncthreads();
         if(yieldNow) {
             // every block leaves here; each unfinished scene's owner saves its scalars
             for(int j = 0; j < nslots; ++j) {
-                const int s = sFirst + j;
-                if(sState[j] != 0 || threadIdx.x != 0 || __ldg(a.cp + s) < c0) continue;
-                DevState* d = a.sc[s].dst;
+                const int sc = sScene[j];
+                if(sState[j] != 0 || threadIdx.x != 0 || !owner(sc)) continue;
+                DevState* d = a.sc[sc].dst;
                 d->iter = sIter[j]; d->rho = sRho[j]; d->beta = sBeta[j]; d->tol = sTol[j]; d->resid = sResid[j];
                 d->done = 0;
             }
@@ -1955,18 +2026,13 @@ int pcg_solve_batch_refined(BatchPcgCtx& ctx, BatchSolveItem* items, int count, 
                 const int np = (int)part.size();
                 const unsigned total = hpch[np];
                 const unsigned capB = (unsigned)(numSM * perSMv);
-                const unsigned perBlock = (total + capB - 1) / capB;
-                const unsigned grid = (total + perBlock - 1) / perBlock;
-                // every block's chunk range must meet at most kBatchSlots scenes
-                for(unsigned b = 0, k = 0; b < grid; ++b) {
-                    const unsigned c0 = b * perBlock, c1 = std::min(c0 + perBlock, total);
-                    while(hpch[k + 1] <= c0) ++k;
-                    unsigned k1 = k;
-                    while(hpch[k1 + 1] < c1) ++k1;
-                    if(k1 - k + 1 > (unsigned)kBatchSlots) {
-                        bnn_set_error("batched PCG: too many scenes per block");
-                        return BNN_ERR_CAPACITY;
-                    }
+                // chunks striped over every resident block; a block's chunks (and so the
+                // scenes it meets) must fit its slot table
+                const unsigned grid = std::min(total, capB);
+                const unsigned perBlock = (total + grid - 1) / grid;
+                if(perBlock > (unsigned)kBatchSlots) {
+                    bnn_set_error("batched PCG: too many chunks per block");
+                    return BNN_ERR_CAPACITY;
                 }
                 BatchPcgArgs a;
                 a.sc = (const BatchPcgScene*)(D + L.bps);
@@ -1977,7 +2043,7 @@ int pcg_solve_batch_refined(BatchPcgCtx& ctx, BatchSolveItem* items, int count, 
                 a.gs = &dh->gs;
                 a.remaining = &dh->remaining;
                 a.active = &dh->active;
-                a.yieldBelow = perBlock > 1 ? total / 2 : 0u;
+                a.yieldBelow = 0u;  // striped chunks stay balanced: no relaunch
                 a.flags = &dh->flags;
                 void* args[] = {(void*)&a};
                 {
