@@ -93,13 +93,14 @@ void launch_cell_histogram(int n, const float* p6, size_t stride, const GridDesc
                            uint32_t* count, DevState* st, cudaStream_t s);
 void launch_sort_finish(int n, size_t ncells, uint32_t* cellOf, uint32_t* slot, const uint32_t* cellStart,
                         uint32_t* order, uint32_t* key, uint32_t* count, const float* src6, const float* srcPos,
-                        float* dst6, const uint32_t* idSrc, uint32_t* idDst, const float* cSrc, float* cDst, float* g3,
+                        float* dst6, const uint32_t* idSrc, uint32_t* idDst, const float* cSrc, float* cDst,
                         float4* rec, const GridDesc& g, size_t stride, DevState* st, cudaStream_t s);
-void launch_p2g_affine(const GridDesc& g, const uint32_t* cellStart, const float* g3, const float* p6,
-                       const float* C9, size_t stride, float* const* out, uint8_t* const* valid, cudaStream_t s);
 // gather_kernels.cu
 void launch_p2g_sdf(const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float4* rec,
                     size_t stride, float* const* out, uint8_t* const* valid, float* phi, cudaStream_t s);
+void launch_p2g_sdf_affine(const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float4* rec,
+                           const float* C9, size_t stride, float* const* out, uint8_t* const* valid, float* phi,
+                           cudaStream_t s);
 void launch_fluid_sdf_tile(const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float4* rec,
                            size_t stride, float* phi, cudaStream_t s);
 void launch_advect_grid(const GridDesc& g, float** U, float** B, float dt, cudaStream_t s);
@@ -154,9 +155,9 @@ static void free_particles(bnn_flip* h) {
         dev_free(h->p6[b]); dev_free(h->ids[b]); dev_free(h->C9[b]);
         h->p6[b] = nullptr; h->ids[b] = nullptr; h->C9[b] = nullptr;
     }
-    dev_free(h->g3); dev_free(h->rec); dev_free(h->bboxPart); dev_free(h->cellOf); dev_free(h->slot); dev_free(h->order); dev_free(h->key); dev_free(h->aosStage);
+    dev_free(h->rec); dev_free(h->bboxPart); dev_free(h->cellOf); dev_free(h->slot); dev_free(h->order); dev_free(h->key); dev_free(h->aosStage);
     dev_free(h->aniso); dev_free(h->moved);
-    h->g3 = nullptr; h->rec = nullptr; h->bboxPart = nullptr; h->cellOf = h->slot = h->order = h->key = nullptr; h->aosStage = nullptr;
+    h->rec = nullptr; h->bboxPart = nullptr; h->cellOf = h->slot = h->order = h->key = nullptr; h->aosStage = nullptr;
     h->aniso = nullptr; h->moved = nullptr;
     h->premoved = false;
     h->cap = 0;
@@ -176,7 +177,6 @@ static int reserve_particles(bnn_flip* h, uint32_t n) {
         if(h->P.solver_kind == BNN_SOLVER_APIC || h->P.solver_kind == BNN_SOLVER_AFLIP)
             BNN_CUDA_CHECK(dev_alloc(&h->C9[b], 9 * st * sizeof(float)));
     }
-    BNN_CUDA_CHECK(dev_alloc(&h->g3, 3 * st * sizeof(float)));
     // per-particle records of the P2G + SDF pass: 3 stencil planes and the positions
     BNN_CUDA_CHECK(dev_alloc(&h->rec, 4 * st * sizeof(float4)));
     BNN_CUDA_CHECK(dev_alloc(&h->bboxPart, 6 * ((st + 255) / 256) * sizeof(int)));
@@ -586,7 +586,7 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st, const HostIo* io = nullp
     launch_sort_finish(n, h->C, h->cellOf, h->slot, h->cellStart, h->order, h->key, h->count, h->p6[h->cur],
                        moved ? h->moved : nullptr, h->p6[nxt],
                        h->ids[h->cur], h->ids[nxt], affine ? h->C9[h->cur] : nullptr, affine ? h->C9[nxt] : nullptr,
-                       h->g3, h->rec, g, h->cap, h->dst, s);
+                       h->rec, g, h->cap, h->dst, s);
     h->cur = nxt;
     if(h->P.correct_position && n > 0) {
         // PIC_Solver::advanceFrame: correctParticlePositions right after moveParticles
@@ -605,7 +605,7 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st, const HostIo* io = nullp
         const int nxt2 = 1 - h->cur;
         launch_sort_finish(n, h->C, h->cellOf, h->slot, h->cellStart, h->order, h->key, h->count, h->p6[h->cur], nullptr, h->p6[nxt2],
                            h->ids[h->cur], h->ids[nxt2], affine ? h->C9[h->cur] : nullptr,
-                           affine ? h->C9[nxt2] : nullptr, h->g3, h->rec, g, h->cap, h->dst, s);
+                           affine ? h->C9[nxt2] : nullptr, h->rec, g, h->cap, h->dst, s);
         h->cur = nxt2;
     }
     cudaEventRecord(h->ev[2], s);
@@ -623,7 +623,8 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st, const HostIo* io = nullp
         // PIC_Solver::advanceVelocity (PIC_Solver.cpp:332-338): the grid velocity is advected
         launch_advect_grid(g, h->U, h->B, substep, s);
     } else if(affine) {
-        launch_p2g_affine(g, h->cellStart, h->g3, h->p6[h->cur], h->C9[h->cur], h->cap, h->U, h->VA, s);
+        // APIC / AFLIP: the same pass with the affine momentum term
+        launch_p2g_sdf_affine(g, h->dst, h->cellStart, h->rec, h->C9[h->cur], h->cap, h->U, h->VA, h->phi, s);
     } else {
         // FLIP: the three components and the fluid SDF in one pass over the particles (the
         // SDF reads positions only, so it is final here already)
@@ -650,7 +651,7 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st, const HostIo* io = nullp
     }
     cudaEventRecord(h->ev[4], s);
     // pressure projection (PIC_Solver.cpp:533-539)
-    if(kind != BNN_SOLVER_FLIP) launch_fluid_sdf_tile(g, h->dst, h->cellStart, h->rec, h->cap, h->phi, s);
+    if(kind == BNN_SOLVER_PIC) launch_fluid_sdf_tile(g, h->dst, h->cellStart, h->rec, h->cap, h->phi, s);
     if(h->gridBoundary) launch_solid_extend(g, h->nodeSdf, h->phi, s);
     cudaEventRecord(h->ev[5], s);
     launch_active_flags(g, h->phi, h->flag, h->dst, s);
@@ -844,7 +845,7 @@ extern "C" int bnn_flip_anisotropic_kernels(bnn_flip* h, const bnn_aniso_params*
     const int nxt = 1 - h->cur;
     launch_sort_finish(n, h->C, h->cellOf, h->slot, h->cellStart, h->order, h->key, h->count, h->p6[h->cur], nullptr, h->p6[nxt],
                        h->ids[h->cur], h->ids[nxt], affine ? h->C9[h->cur] : nullptr, affine ? h->C9[nxt] : nullptr,
-                       h->g3, h->rec, g, h->cap, h->dst, s);
+                       h->rec, g, h->cap, h->dst, s);
     h->cur = nxt;
     const size_t cap = h->cap;
     if(!h->aniso) BNN_CUDA_CHECK(dev_alloc(&h->aniso, (12 * cap + 4) * sizeof(float)));

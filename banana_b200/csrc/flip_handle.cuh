@@ -26,7 +26,6 @@ struct bnn_flip {
     uint32_t* ids[2] = {nullptr, nullptr};
     float* C9[2] = {nullptr, nullptr};
     int cur = 0;
-    float* g3 = nullptr;    // grid coordinates (APIC / AFLIP P2G)
     float4* rec = nullptr;  // per-particle gather records: 3 P2G stencil planes + positions
     uint32_t *cellOf = nullptr, *slot = nullptr, *order = nullptr, *key = nullptr;
     int* bboxPart = nullptr;  // per-block occupied-cell boxes of the advection

@@ -529,7 +529,6 @@ __global__ void __launch_bounds__(256) k_sort_large(const uint32_t* __restrict__
 
 // Apply the permutation to the particle arrays and emit what the gathers read per
 // particle (all from Grid::getGridCoordinate, Grid.h:197):
-//   g3   grid coordinates (SoA; the APIC/AFLIP P2G reads them);
 //   rec  plane D < 3: the P2G stencil record of component D, {ex, ey, ez, v_D}: e_a is the
 //        get_barycentric fraction of axis a (ArrayHelpers.h:95-112), its sign bit set when
 //        the stencil's base index is the particle's (sort) cell - 1 instead of the cell
@@ -541,8 +540,8 @@ __device__ __forceinline__ void gather_particles_body(Blk blk, int n, const uint
                                                       const float* __restrict__ src6, const float* __restrict__ srcPos,
                                                       float* __restrict__ dst6, const uint32_t* __restrict__ idSrc,
                                                       uint32_t* __restrict__ idDst, const float* __restrict__ cSrc,
-                                                      float* __restrict__ cDst, float* __restrict__ g3,
-                                                      float4* __restrict__ rec, const GridDesc& g, size_t stride) {
+                                                      float* __restrict__ cDst, float4* __restrict__ rec,
+                                                      const GridDesc& g, size_t stride) {
     const int i = blk.x * blockDim.x + threadIdx.x;
     if(i >= n) return;
     const uint32_t s = order[i];
@@ -560,114 +559,33 @@ __device__ __forceinline__ void gather_particles_body(Blk blk, int n, const uint
     if(cSrc) {
 #pragma unroll
         for(int q = 0; q < 9; ++q) cDst[q * stride + i] = cSrc[q * stride + s];
-#pragma unroll
-        for(int a = 0; a < 3; ++a) g3[a * stride + i] = gc[a];
     }
     rec[3 * stride + i] = make_float4(v6[0], v6[1], v6[2], 0.f);
-    if(!cSrc) {
-        int cell[3];
+    int cell[3];
+#pragma unroll
+    for(int a = 0; a < 3; ++a) {
+        int c = (int)gc[a];
+        cell[a] = c < 0 ? 0 : (c > g.G[a] - 1 ? g.G[a] - 1 : c);
+    }
+#pragma unroll
+    for(int D = 0; D < 3; ++D) {
+        float e[3];
 #pragma unroll
         for(int a = 0; a < 3; ++a) {
-            int c = (int)gc[a];
-            cell[a] = c < 0 ? 0 : (c > g.G[a] - 1 ? g.G[a] - 1 : c);
+            int si;
+            float fi;
+            bary(gc[a] - (a == D ? 0.f : 0.5f), si, fi, g.G[a] + (a == D ? 1 : 0));
+            e[a] = (si < cell[a]) ? __int_as_float(__float_as_int(fi) | (int)0x80000000) : fi;
         }
-#pragma unroll
-        for(int D = 0; D < 3; ++D) {
-            float e[3];
-#pragma unroll
-            for(int a = 0; a < 3; ++a) {
-                int si;
-                float fi;
-                bary(gc[a] - (a == D ? 0.f : 0.5f), si, fi, g.G[a] + (a == D ? 1 : 0));
-                e[a] = (si < cell[a]) ? __int_as_float(__float_as_int(fi) | (int)0x80000000) : fi;
-            }
-            rec[D * stride + i] = make_float4(e[0], e[1], e[2], v6[3 + D]);
-        }
+        rec[D * stride + i] = make_float4(e[0], e[1], e[2], v6[3 + D]);
     }
 }
 __global__ void k_gather_particles(int n, const uint32_t* __restrict__ order, const float* __restrict__ src6,
                                    const float* __restrict__ srcPos, float* __restrict__ dst6,
                                    const uint32_t* __restrict__ idSrc, uint32_t* __restrict__ idDst,
-                                   const float* __restrict__ cSrc, float* __restrict__ cDst, float* __restrict__ g3,
+                                   const float* __restrict__ cSrc, float* __restrict__ cDst,
                                    float4* __restrict__ rec, GridDesc g, size_t stride) {
-    gather_particles_body(own_blk(), n, order, src6, srcPos, dst6, idSrc, idDst, cSrc, cDst, g3, rec, g, stride);
-}
-
-// ----------------------------------------------------------------------------------
-// P2G
-// ----------------------------------------------------------------------------------
-// FLIP_Solver::mapParticles2Grid (FLIP_Solver.cpp:57-95) as a gather: the thread of face
-// f walks the particles of the cells whose particles can reach f (2 cells along the
-// component's axis, 3 along the others), in sorted-array order, keeps those whose
-// trilinear stencil (ArrayHelpers::getCoordinatesAndWeights, ArrayHelpers.cpp:50-76)
-// contains f, and sums w*v and w in that order -- the sums a serial run of the reference
-// P2G over the sorted particle array produces.  APIC/AFLIP add the affine momentum term
-// w * dot(C_d, x_f - x_p) (APIC_Solver.cpp:53-91).
-template<int D, bool AFFINE>
-__global__ void __launch_bounds__(256) k_p2g(GridDesc g, const uint32_t* __restrict__ cellStart,
-                                             const float* __restrict__ gxs, const float* __restrict__ gys,
-                                             const float* __restrict__ gzs, const float* __restrict__ pxs,
-                                             const float* __restrict__ pys, const float* __restrict__ pzs,
-                                             const float* __restrict__ vd, const float* __restrict__ Cd,
-                                             size_t cstride, float* __restrict__ out,
-                                             uint8_t* __restrict__ valid) {
-    const int sx = g.G[0] + (D == 0), sy = g.G[1] + (D == 1), sz = g.G[2] + (D == 2);
-    const size_t nf = (size_t)sx * sy * sz;
-    const size_t f = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if(f >= nf) return;
-    const int i = (int)(f % sx);
-    const int j = (int)((f / sx) % sy);
-    const int k = (int)(f / ((size_t)sx * sy));
-    const int xlo = max(i - 1, 0), xhi = min(D == 0 ? i : i + 1, g.G[0] - 1);
-    const int ylo = max(j - 1, 0), yhi = min(D == 1 ? j : j + 1, g.G[1] - 1);
-    const int zlo = max(k - 1, 0), zhi = min(D == 2 ? k : k + 1, g.G[2] - 1);
-    // world position of the face (Grid::getWorldCoordinate(VecN(idx) + extra), Grid.h:181-184)
-    float fxw = 0.f, fyw = 0.f, fzw = 0.f;
-    if(AFFINE) {
-        fxw = ((float)i + (D == 0 ? 0.f : 0.5f)) * g.dx + g.bmin[0];
-        fyw = ((float)j + (D == 1 ? 0.f : 0.5f)) * g.dx + g.bmin[1];
-        fzw = ((float)k + (D == 2 ? 0.f : 0.5f)) * g.dx + g.bmin[2];
-    }
-    float S = 0.f, W = 0.f;
-    if(xlo <= xhi) {
-        for(int kk = zlo; kk <= zhi; ++kk) {
-            for(int jj = ylo; jj <= yhi; ++jj) {
-                const size_t row = ((size_t)kk * g.G[1] + jj) * g.G[0];
-                const uint32_t b = __ldg(cellStart + row + xlo), e = __ldg(cellStart + row + xhi + 1);
-                for(uint32_t q = b; q < e; ++q) {
-                    const float ax = __ldg(gxs + q) - (D == 0 ? 0.f : 0.5f);
-                    const float ay = __ldg(gys + q) - (D == 1 ? 0.f : 0.5f);
-                    const float az = __ldg(gzs + q) - (D == 2 ? 0.f : 0.5f);
-                    int si, sj, sk;
-                    float fi, fj, fk;
-                    bary(ax, si, fi, sx);
-                    if(si != i && si != i - 1) continue;
-                    bary(ay, sj, fj, sy);
-                    if(sj != j && sj != j - 1) continue;
-                    bary(az, sk, fk, sz);
-                    if(sk != k && sk != k - 1) continue;
-                    const float wx = (si == i) ? (1.0f - fi) : fi;
-                    const float wy = (sj == j) ? (1.0f - fj) : fj;
-                    const float wz = (sk == k) ? (1.0f - fk) : fk;
-                    const float wgt = wx * wy * wz;
-                    float m;
-                    if(AFFINE) {
-                        const float c0 = __ldg(Cd + q), c1 = __ldg(Cd + cstride + q), c2 = __ldg(Cd + 2 * cstride + q);
-                        const float dxp = fxw - __ldg(pxs + q), dyp = fyw - __ldg(pys + q), dzp = fzw - __ldg(pzs + q);
-                        const float dotv = (c0 * dxp + c1 * dyp) + c2 * dzp;
-                        m = wgt * (__ldg(vd + q) + dotv);
-                    } else {
-                        m = wgt * __ldg(vd + q);
-                    }
-                    S = S + m;
-                    W = W + wgt;
-                }
-            }
-        }
-    }
-    const bool ok = W > FLT_MIN;
-    out[f] = ok ? S / W : S;
-    valid[f] = ok ? 1 : 0;
+    gather_particles_body(own_blk(), n, order, src6, srcPos, dst6, idSrc, idDst, cSrc, cDst, rec, g, stride);
 }
 
 // ----------------------------------------------------------------------------------
@@ -1593,7 +1511,7 @@ __global__ void kb_gather_particles(const BScene* __restrict__ S, const unsigned
     const BScene& c = S[q];
     virtual_blocks(b, (unsigned)(c.n + 255) / 256, [&](Blk v) {
         gather_particles_body(v, c.n, c.order, c.p6cur, c.moved ? c.movedPos : c.p6cur, c.p6nxt, c.idcur, c.idnxt,
-                              nullptr, nullptr, nullptr, c.rec, c.g, c.cap);
+                              nullptr, nullptr, c.rec, c.g, c.cap);
     });
 }
 // Before the last layer after P2G: the FLIP backup starts at 0 and v at 0 - g dt (the
@@ -1726,7 +1644,7 @@ void launch_cell_histogram(int n, const float* p6, size_t stride, const GridDesc
 // cellOf holds their unsorted order while k_sort_large rewrites them
 void launch_sort_finish(int n, size_t ncells, uint32_t* cellOf, uint32_t* slot, const uint32_t* cellStart,
                         uint32_t* order, uint32_t* key, uint32_t* count, const float* src6, const float* srcPos,
-                        float* dst6, const uint32_t* idSrc, uint32_t* idDst, const float* cSrc, float* cDst, float* g3,
+                        float* dst6, const uint32_t* idSrc, uint32_t* idDst, const float* cSrc, float* cDst,
                         float4* rec, const GridDesc& g, size_t stride, DevState* st, cudaStream_t s) {
     if(n > 0) { k_scatter_index<<<nblk(n), 256, 0, s>>>(n, cellOf, slot, cellStart, idSrc, order, key); bnn_note_launch(); }
     cudaMemsetAsync(&st->nlarge, 0, sizeof(unsigned), s);
@@ -1734,22 +1652,7 @@ void launch_sort_finish(int n, size_t ncells, uint32_t* cellOf, uint32_t* slot, 
     if(n > 16) { k_sort_large<<<8 * 148, 256, 0, s>>>(cellStart, order, idSrc, cellOf, slot, st); bnn_note_launch(); }
     if(n > 0)
         { k_gather_particles<<<nblk(n), 256, 0, s>>>(n, order, src6, srcPos ? srcPos : src6, dst6, idSrc, idDst, cSrc, cDst,
-                                                    g3, rec, g, stride); bnn_note_launch(); }
-}
-// APIC / AFLIP P2G (the affine momentum term), one launch per component; FLIP's P2G is
-// the tiled pass of gather_kernels.cu
-void launch_p2g_affine(const GridDesc& g, const uint32_t* cellStart, const float* g3, const float* p6,
-                       const float* C9, size_t stride, float* const* out, uint8_t* const* valid, cudaStream_t s) {
-    const float *gx = g3, *gy = g3 + stride, *gz = g3 + 2 * stride;
-    const float *px = p6, *py = p6 + stride, *pz = p6 + 2 * stride;
-    for(int d = 0; d < 3; ++d) {
-        size_t nf = (size_t)face_sx(g, d) * face_sy(g, d) * face_sz(g, d);
-        const float* vd = p6 + (3 + d) * stride;
-        const float* Cd = C9 + (size_t)(3 * d) * stride;
-        if(d == 0) { k_p2g<0, true><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[0], valid[0]); bnn_note_launch(); }
-        if(d == 1) { k_p2g<1, true><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[1], valid[1]); bnn_note_launch(); }
-        if(d == 2) { k_p2g<2, true><<<nblk(nf), 256, 0, s>>>(g, cellStart, gx, gy, gz, px, py, pz, vd, Cd, stride, out[2], valid[2]); bnn_note_launch(); }
-    }
+                                                    rec, g, stride); bnn_note_launch(); }
 }
 // PIC grid advection of all three components; U[d] / B[d] are swapped after each one
 void launch_advect_grid(const GridDesc& g, float** U, float** B, float dt, cudaStream_t s) {

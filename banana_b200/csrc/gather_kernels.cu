@@ -101,6 +101,7 @@ struct TileArgs {
     float* out[3];
     uint8_t* valid[3];
     float* phi;
+    const float* C9;    // APIC / AFLIP: the sorted particles' affine matrices (9 planes, stride `stride`)
 };
 
 // Does the cell box [lo, hi] meet the occupied-cell box?
@@ -127,14 +128,30 @@ __device__ __forceinline__ void cell_range(const TileArgs& a, int x0, int z0, in
 }
 
 // Partials of component D for halo cell h (particles [b, e)) into sm (slot-major planes).
-template<int D, class SH>
-__device__ __forceinline__ void cell_partials(const TileArgs& a, int h, uint32_t b, uint32_t e, float* __restrict__ sm) {
+// AFF (APIC / AFLIP, APIC_Solver.cpp:53-91): a particle's momentum at a face is
+// weight * (v + C_D . (x_face - x_p)), x_face the face's world position
+// (Grid::getWorldCoordinate, Grid.h:181-184), in the reference's association.
+template<int D, class SH, bool AFF = false>
+__device__ __forceinline__ void cell_partials(const TileArgs& a, int h, uint32_t b, uint32_t e, float* __restrict__ sm,
+                                              int x0 = 0, int z0 = 0, int cy = 0) {
     constexpr int kNH = SH::kNH;
     constexpr int NX = D == 0 ? 2 : 3, NY = D == 1 ? 2 : 3, NZ = D == 2 ? 2 : 3;
     constexpr int NS = NX * NY * NZ;
     float S[NS], W[NS];
 #pragma unroll
     for(int s = 0; s < NS; ++s) { S[s] = 0.0f; W[s] = 0.0f; }
+    // AFF: world coordinates of the faces the slots address (slot i along axis a is the face
+    // at offset i from the cell on the component's own axis, i - 1 on the others)
+    float gpx[NX], gpy[NY], gpz[NZ];
+    if constexpr(AFF) {
+        const int cx = x0 - 1 + h % kHX, cz = z0 - 1 + h / kHX;
+#pragma unroll
+        for(int i = 0; i < NX; ++i) gpx[i] = ((float)(cx + (D == 0 ? i : i - 1)) + (D == 0 ? 0.f : 0.5f)) * a.g.dx + a.g.bmin[0];
+#pragma unroll
+        for(int i = 0; i < NY; ++i) gpy[i] = ((float)(cy + (D == 1 ? i : i - 1)) + (D == 1 ? 0.f : 0.5f)) * a.g.dx + a.g.bmin[1];
+#pragma unroll
+        for(int i = 0; i < NZ; ++i) gpz[i] = ((float)(cz + (D == 2 ? i : i - 1)) + (D == 2 ? 0.f : 0.5f)) * a.g.dx + a.g.bmin[2];
+    }
     {
         const float4* __restrict__ recD = a.rec + (size_t)D * a.stride;
         // the next record is loaded while this one is summed
@@ -146,16 +163,37 @@ __device__ __forceinline__ void cell_partials(const TileArgs& a, int h, uint32_t
             if constexpr(D == 0) own_axis(L.x, wx); else side_axis(L.x, wx);
             if constexpr(D == 1) own_axis(L.y, wy); else side_axis(L.y, wy);
             if constexpr(D == 2) own_axis(L.z, wz); else side_axis(L.z, wz);
+            float c0 = 0.f, c1 = 0.f, c2 = 0.f, dxp[NX], dyp[NY], dzp[NZ];
+            if constexpr(AFF) {
+                const float4 P = __ldg(a.rec + 3 * a.stride + q);
+                const float* __restrict__ Cd = a.C9 + (size_t)(3 * D) * a.stride;
+                c0 = __ldg(Cd + q);
+                c1 = __ldg(Cd + a.stride + q);
+                c2 = __ldg(Cd + 2 * a.stride + q);
+#pragma unroll
+                for(int i = 0; i < NX; ++i) dxp[i] = gpx[i] - P.x;
+#pragma unroll
+                for(int i = 0; i < NY; ++i) dyp[i] = gpy[i] - P.y;
+#pragma unroll
+                for(int i = 0; i < NZ; ++i) dzp[i] = gpz[i] - P.z;
+            }
 #pragma unroll
             for(int ix = 0; ix < NX; ++ix)
 #pragma unroll
                 for(int iy = 0; iy < NY; ++iy) {
                     const float wxy = wx[ix] * wy[iy];
+                    float cxy = 0.f;
+                    if constexpr(AFF) cxy = c0 * dxp[ix] + c1 * dyp[iy];
 #pragma unroll
                     for(int iz = 0; iz < NZ; ++iz) {
                         const int s = (ix * NY + iy) * NZ + iz;
                         const float w = wxy * wz[iz];
-                        S[s] = S[s] + w * L.w;
+                        if constexpr(AFF) {
+                            const float dotv = cxy + c2 * dzp[iz];
+                            S[s] = S[s] + w * (L.w + dotv);
+                        } else {
+                            S[s] = S[s] + w * L.w;
+                        }
                         W[s] = W[s] + w;
                     }
                 }
@@ -320,8 +358,9 @@ struct GivenTile {
 };
 
 // One block of the pass: tile (x, z) of face columns, y-chunk y.  EXACT: some particle
-// left the grid (the same for the whole launch; see sdf_partials).
-template<bool P2G, class SH, bool EXACT, class Tile>
+// left the grid (the same for the whole launch; see sdf_partials).  AFF: APIC / AFLIP
+// momentum (cell_partials).
+template<bool P2G, class SH, bool EXACT, bool AFF = false, class Tile>
 __device__ __forceinline__ void tile_body(const TileArgs& a, const Tile tile) {
     constexpr int kTZ = SH::kTZ, kYC = SH::kYC;
     extern __shared__ float sm[];
@@ -358,17 +397,17 @@ __device__ __forceinline__ void tile_body(const TileArgs& a, const Tile tile) {
             uint32_t pb, pe;
             cell_range(a, x0, z0, cy, t, pb, pe);
             if constexpr(P2G) {
-                cell_partials<0, SH>(a, t, pb, pe, sm);
+                cell_partials<0, SH, AFF>(a, t, pb, pe, sm, x0, z0, cy);
                 __syncthreads();
                 if(owner) pull_partials<0, SH>(sm, tx, tz, uS, uW);
                 __syncthreads();
                 if(cy < yB) {
-                    cell_partials<1, SH>(a, t, pb, pe, sm);
+                    cell_partials<1, SH, AFF>(a, t, pb, pe, sm, x0, z0, cy);
                     __syncthreads();
                     if(owner) pull_partials<1, SH>(sm, tx, tz, vS, vW);
                     __syncthreads();
                 }
-                cell_partials<2, SH>(a, t, pb, pe, sm);
+                cell_partials<2, SH, AFF>(a, t, pb, pe, sm, x0, z0, cy);
                 __syncthreads();
                 if(owner) pull_partials<2, SH>(sm, tx, tz, wS, wW);
                 __syncthreads();
@@ -400,14 +439,14 @@ __device__ __forceinline__ void tile_body(const TileArgs& a, const Tile tile) {
 }
 // The rare launch in which some particle left the grid, kept out of line so that its
 // per-slot tests do not weigh on the registers of the common path
-template<bool P2G, class SH, class Tile>
+template<bool P2G, class SH, bool AFF, class Tile>
 __device__ __noinline__ void tile_body_exact(const TileArgs& a, const Tile tile) {
-    tile_body<P2G, SH, true>(a, tile);
+    tile_body<P2G, SH, true, AFF>(a, tile);
 }
-template<bool P2G, class SH>
+template<bool P2G, class SH, bool AFF = false>
 __global__ void __launch_bounds__(SH::kThreads, SH::kMinBlocks) k_p2g_sdf_tile(const __grid_constant__ TileArgs a) {
-    if((a.st->flags & BNN_FLAG_OUT_OF_GRID) != 0u) tile_body_exact<P2G, SH>(a, OwnTile{});
-    else tile_body<P2G, SH, false>(a, OwnTile{});
+    if((a.st->flags & BNN_FLAG_OUT_OF_GRID) != 0u) tile_body_exact<P2G, SH, AFF>(a, OwnTile{});
+    else tile_body<P2G, SH, false, AFF>(a, OwnTile{});
 }
 
 // Batched: the tiles of all scenes of a batch in one launch (P: per-scene tile prefix);
@@ -421,8 +460,8 @@ __global__ void __launch_bounds__(SH::kThreads, SH::kMinBlocks) kb_p2g_sdf_tile(
     const unsigned gx = (unsigned)((a.g.G[0] + 1 + kTX - 1) / kTX);
     const unsigned gz = (unsigned)((a.g.G[2] + 1 + SH::kTZ - 1) / SH::kTZ);
     const GivenTile tile{b.x % gx, (b.x / gx) % gz, b.x / (gx * gz)};
-    if((a.st->flags & BNN_FLAG_OUT_OF_GRID) != 0u) tile_body_exact<true, SH>(a, tile);  // the scene's flag
-    else tile_body<true, SH, false>(a, tile);
+    if((a.st->flags & BNN_FLAG_OUT_OF_GRID) != 0u) tile_body_exact<true, SH, false>(a, tile);  // the scene's flag
+    else tile_body<true, SH, false, false>(a, tile);
 }
 static_assert(kHX == 32, "a warp is one row of halo cells");
 
@@ -618,6 +657,18 @@ void launch_p2g_sdf(const GridDesc& g, const DevState* st, const uint32_t* cellS
     int shape = lookup(key);
     if(shape < 0) shape = tune(key, s, [&](int v) { launch_p2g_shape(v, a, s); });
     else launch_p2g_shape(shape, a, s);
+}
+
+// APIC / AFLIP: the same pass with the affine momentum term (C9: the sorted particles'
+// affine matrices), in the default tile shape
+void launch_p2g_sdf_affine(const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float4* rec,
+                           const float* C9, size_t stride, float* const* out, uint8_t* const* valid, float* phi,
+                           cudaStream_t s) {
+    const TileArgs a{g, st, cellStart, rec, stride, {out[0], out[1], out[2]}, {valid[0], valid[1], valid[2]}, phi, C9};
+    static std::atomic<uint64_t> configured{0};
+    opt_in_smem(k_p2g_sdf_tile<true, S0, true>, S0::kSmemBytes, configured);
+    k_p2g_sdf_tile<true, S0, true><<<tile_grid_of<S0>(g), dim3(kHX, S0::kHZ), S0::kSmemBytes, s>>>(a);
+    bnn_note_launch();
 }
 
 // Tiles of one scene's P2G + SDF pass in a shape (the batched launch's share of the scene)

@@ -62,6 +62,8 @@ PCG_TRAFFIC_PER_ITER = 835.7e6 / 300
 
 
 PCG_MODE = {"fp32": 0, "fp64": 1, "refined": 2}
+# BNN_SOLVER_*: the headline is FLIP; the others run the same scene through the same step
+SOLVERS = {"flip": 0, "apic": 1, "aflip": 2, "pic": 3}
 
 
 def _pcg_flags(args) -> int:
@@ -316,6 +318,7 @@ def run_ours(args, ws, rank, local):
         cfg["refine_inner_tolerance"] = args.inner_tol
     if args.tol is not None:
         cfg["cg_relative_tolerance"] = args.tol
+    cfg["solver_kind"] = SOLVERS[args.solver]
     pos, vel = scenes.dam_break(N_GRID)
     npart = len(pos)
     if args.tile_shape is not None:
@@ -399,7 +402,8 @@ def run_ours(args, ws, rank, local):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded dam break, seed 42)",
-            "config": dict(_config(pcg_mode, cfg), particles=npart),
+            "config": dict(_config(pcg_mode, cfg), particles=npart, solver=args.solver.upper(),
+                           workload=WORKLOAD if args.solver == "flip" else f"{args.solver}_dam_break_256"),
             "roofline": {"bound": "hbm", "kernel": "k_pcg_persistent (whole Jacobi PCG solve, one launch per step)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
@@ -972,6 +976,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--pcg-mode", choices=["fp32", "fp64", "refined"], default="fp32")
+    ap.add_argument("--solver", choices=list(SOLVERS), default="flip",
+                    help="flip workload: the particle solver (FLIP is the headline; APIC / AFLIP / PIC the "
+                         "reference's other PIC-family solvers on the same scene)")
     ap.add_argument("--pcg-steps", choices=["single", "two"], default="two",
                     help="PCG iteration form: PCGSolver's two-reduction order (default) or single reduction")
     ap.add_argument("--inner-tol", type=float, default=None, help="refined PCG: inner (FP32) relative tolerance")

@@ -1060,18 +1060,20 @@ public:
         w[7] = fi * fj * fk;
     }
 
-    // FLIP P2G with the sums in the canonical two-level order of the CUDA kernel: for every
+    // P2G with the sums in the canonical two-level order of the CUDA kernel: for every
     // face, the particles of each candidate cell (two along the component's own axis, three
     // along the others, clamped to the grid) are summed in id order into a per-cell
     // partial, and the face adds its candidate cells' partials in (y, z, x)-major cell
     // order, both sums starting at +0.  The products are those of mapP2G
     // (getCoordinatesAndWeights, ArrayHelpers.cpp:50-76, weight = wx * wy * wz left to
-    // right, momentum = weight * v); only the association of the sums differs from the
-    // reference's serial loop, whose CAS-atomic parallel form (FLIP_Solver.cpp:57-95,
-    // AtomicOperations.h:31-49) has no fixed order.  Needs the particles sorted by
-    // (cell, id).  Faces are independent, so this runs on any number of threads with the
-    // same result.
+    // right, momentum = weight * v, and for APIC / AFLIP weight * (v + C_d . (x_face - x_p))
+    // with the face's world position, APIC_Solver.cpp:53-91); only the association of the
+    // sums differs from the reference's serial loop, whose CAS-atomic parallel form
+    // (FLIP_Solver.cpp:57-95, AtomicOperations.h:31-49) has no fixed order.  Needs the
+    // particles sorted by (cell, id).  Faces are independent, so this runs on any number of
+    // threads with the same result.
     void mapP2GCanonical() {
+        const bool affine = (P.solver_kind == 1 || P.solver_kind == 2);
         const size_t n = pos.size(), C = (size_t)G[0] * G[1] * G[2];
         std::vector<uint32_t> start(C + 1, 0);
         for(size_t p = 0; p < n; ++p) start[cellLinear(pos[p]) + 1]++;
@@ -1123,7 +1125,19 @@ public:
                                 }
                                 if(!reach) continue;
                                 const R w = w3[0] * w3[1] * w3[2];
-                                PS = PS + w * vel[q][d];
+                                R m;
+                                if(affine) {
+                                    // gpos = grid().getWorldCoordinate(VecN(face) + extra) (Grid.h:181-184)
+                                    R gp[3];
+                                    for(int a = 0; a < 3; ++a) gp[a] = ((R)f[a] + (a == d ? R(0) : R(0.5))) * dx + bmin[a];
+                                    const R* Cq = &Cmat[(size_t)q * 9 + d * 3];
+                                    const R dxp = gp[0] - pos[q].x, dyp = gp[1] - pos[q].y, dzp = gp[2] - pos[q].z;
+                                    const R dotv = (Cq[0] * dxp + Cq[1] * dyp) + Cq[2] * dzp;
+                                    m = w * (vel[q][d] + dotv);
+                                } else {
+                                    m = w * vel[q][d];
+                                }
+                                PS = PS + m;
                                 PW = PW + w;
                             }
                             S = S + PS;
@@ -1140,10 +1154,10 @@ public:
         }
     }
 
-    // Which P2G the step runs: FLIP in the canonical mode takes the two-level order above;
-    // every other case the reference's serial loop.
+    // Which P2G the step runs: FLIP, APIC and AFLIP in the canonical mode take the
+    // two-level order above; every other case the reference's serial loop.
     void splatParticles() {
-        if(P.solver_kind == 0 && P.reduce_mode == 1 && (P.sort_each_step || P.correct_position)) mapP2GCanonical();
+        if(P.solver_kind <= 2 && P.reduce_mode == 1 && (P.sort_each_step || P.correct_position)) mapP2GCanonical();
         else mapP2G();
     }
 
