@@ -140,8 +140,8 @@ void launch_add_scalar(float* a, size_t n, float v, cudaStream_t s);
 void launch_step_reset(DevState* st, cudaStream_t s);
 void launch_step_reset_moved(DevState* st, cudaStream_t s);
 void launch_g2p_move(int n, const GridDesc& g, float* p6, size_t stride, const float* const* U, const float* const* O,
-                     float ratio, const NextStep& ns, float* moved, uint32_t* cellOf, uint32_t* slot, uint32_t* count,
-                     DevState* st, int* bboxPart, cudaStream_t s);
+                     float ratio, int kind, float* C9, const NextStep& ns, float* moved, uint32_t* cellOf,
+                     uint32_t* slot, uint32_t* count, DevState* st, int* bboxPart, cudaStream_t s);
 
 // pcg.cu
 } // namespace bnn
@@ -185,7 +185,8 @@ static int reserve_particles(bnn_flip* h, uint32_t n) {
     BNN_CUDA_CHECK(dev_alloc(&h->order, st * sizeof(uint32_t)));
     BNN_CUDA_CHECK(dev_alloc(&h->key, st * sizeof(uint32_t)));
     BNN_CUDA_CHECK(dev_alloc(&h->aosStage, 6 * st * sizeof(float)));
-    if(h->P.solver_kind == BNN_SOLVER_FLIP) BNN_CUDA_CHECK(dev_alloc(&h->moved, 3 * st * sizeof(float)));
+    // positions moved for the next sub-step by the fused transfer + move (not PIC, which has no transfer)
+    if(h->P.solver_kind != BNN_SOLVER_PIC) BNN_CUDA_CHECK(dev_alloc(&h->moved, 3 * st * sizeof(float)));
     h->cap = cap;
     return BNN_OK;
 }
@@ -323,8 +324,8 @@ extern "C" int bnn_scene_bytes_estimate(const bnn_params* params, uint32_t n, ui
     const bool affine = params->solver_kind == BNN_SOLVER_APIC || params->solver_kind == BNN_SOLVER_AFLIP;
     const bool fp64 = (params->pcg_mode & BNN_PCG_MODE_MASK) != BNN_PCG_FP32;
     const uint64_t rows = n < C ? n : C;
-    const bool flip = params->solver_kind == BNN_SOLVER_FLIP;
-    *bytes = F * 14u + C * 24u + (uint64_t)n * (172u + (affine ? 72u : 0u) + (flip ? 12u : 0u)) + rows * 44u +
+    const bool fused = params->solver_kind != BNN_SOLVER_PIC;
+    *bytes = F * 14u + C * 24u + (uint64_t)n * (172u + (affine ? 72u : 0u) + (fused ? 12u : 0u)) + rows * 44u +
              (rows * 5u / 4u + 4096u) * (48u + (fp64 ? 56u : 0u));
     return BNN_OK;
 }
@@ -696,12 +697,13 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st, const HostIo* io = nullp
         for(int d = 0; d < 3; ++d) launch_maxabs(h->U[d], h->F[d], &h->dst->maxvel_bits, s);
     }
     cudaEventRecord(h->ev[8], s);
-    // PIC_Solver leaves the particle velocities alone (no grid-to-particle transfer).  FLIP
-    // steps driven from device-resident particles also move the particles for the next
-    // sub-step here (k_g2p_move); a step on caller arrays (bnn_flip_step_host) does not,
-    // since the next call brings new particle data, and neither does a scene with dynamic
-    // boundary objects, which are moved (bnn_flip_set_boundaries) before every sub-step.
-    const bool fuse = kind == BNN_SOLVER_FLIP && n > 0 && !io && h->moved && !h->gridBoundary;
+    // PIC_Solver leaves the particle velocities alone (no grid-to-particle transfer).  FLIP,
+    // APIC and AFLIP steps driven from device-resident particles also move the particles for
+    // the next sub-step here (k_g2p_move); a step on caller arrays (bnn_flip_step_host) does
+    // not, since the next call brings new particle data, and neither does a scene with
+    // dynamic boundary objects, which are moved (bnn_flip_set_boundaries) before every
+    // sub-step.
+    const bool fuse = kind != BNN_SOLVER_PIC && n > 0 && !io && h->moved && !h->gridBoundary;
     if(fuse) {
         NextStep ns;
         ns.frameTime = h->frameTime + substep;
@@ -710,7 +712,8 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st, const HostIo* io = nullp
         ns.minDt = h->P.min_timestep;
         ns.maxDt = h->P.max_timestep;
         ns.advSteps = (int)h->P.advection_steps;
-        launch_g2p_move(n, g, h->p6[h->cur], h->cap, h->U, h->O, h->P.pic_flip_ratio, ns, h->moved, h->cellOf, h->slot,
+        launch_g2p_move(n, g, h->p6[h->cur], h->cap, h->U, h->O, h->P.pic_flip_ratio, kind,
+                        affine ? h->C9[h->cur] : nullptr, ns, h->moved, h->cellOf, h->slot,
                         h->count, h->dst, h->bboxPart, s);
     } else if(kind != BNN_SOLVER_PIC) {
         launch_g2p(n, g, h->p6[h->cur], h->cap, h->U, h->O, h->P.pic_flip_ratio, kind, affine ? h->C9[h->cur] : nullptr,

@@ -1286,13 +1286,15 @@ __device__ __forceinline__ float next_substep(unsigned maxvelBits, const NextSte
     return ts;
 }
 
-// FLIP_Solver::mapGrid2Particles (FLIP_Solver.cpp:99-111), then the next sub-step's
-// PIC_Solver::moveParticles (PIC_Solver.cpp:353-373) and the first half of its counting
-// sort: both read the same grid (the next sub-step starts from this one's velocities), and
-// the move's first RK2 stage is the grid velocity the transfer has just interpolated at
-// the particle.  The particle keeps its position of this sub-step (what callers read
-// between sub-steps); the moved position goes to `moved`, and the next sub-step's sort
-// gathers from there.  Identical arithmetic to k_g2p followed by k_advect.
+// FLIP_Solver::mapGrid2Particles (FLIP_Solver.cpp:99-111; KIND 0), APIC_Solver's and
+// AFLIP_Solver's (the velocity and affine matrix of k_g2p; KIND 1, 2), then the next
+// sub-step's PIC_Solver::moveParticles (PIC_Solver.cpp:353-373) and the first half of its
+// counting sort: both read the same grid (the next sub-step starts from this one's
+// velocities), and the move's first RK2 stage is the grid velocity the transfer has just
+// interpolated at the particle.  The particle keeps its position of this sub-step (what
+// callers read between sub-steps); the moved position goes to `moved`, and the next
+// sub-step's sort gathers from there.  Identical arithmetic to k_g2p followed by k_advect.
+template <int KIND>
 __device__ __forceinline__ void g2p_move_body(Blk blk, int n, const GridDesc& g, float* __restrict__ p6, size_t stride,
                                               const float* __restrict__ u, const float* __restrict__ v,
                                               const float* __restrict__ w, const float* __restrict__ ou,
@@ -1300,7 +1302,7 @@ __device__ __forceinline__ void g2p_move_body(Blk blk, int n, const GridDesc& g,
                                               const NextStep& ns, float* __restrict__ moved,
                                               uint32_t* __restrict__ cellOf, uint32_t* __restrict__ slot,
                                               uint32_t* __restrict__ count, DevState* st,
-                                              int* __restrict__ bboxPart) {
+                                              int* __restrict__ bboxPart, float* __restrict__ C9) {
     int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {INT_MIN, INT_MIN, INT_MIN};
     const float substep = next_substep(st->maxvel_bits, ns, g.dx);
     const float sub = substep / (float)ns.advSteps;
@@ -1311,7 +1313,11 @@ __device__ __forceinline__ void g2p_move_body(Blk blk, int n, const GridDesc& g,
         float x = p6[p], y = p6[stride + p], z = p6[2 * stride + p];
         float gx = (x - g.bmin[0]) / g.dx, gy = (y - g.bmin[1]) / g.dx, gz = (z - g.bmin[2]) / g.dx;
         float gv[3];
-        {
+        if(KIND == 1) {
+            vel_from_grid(g, u, v, w, gx, gy, gz, gv);
+#pragma unroll
+            for(int d = 0; d < 3; ++d) p6[(3 + d) * stride + p] = gv[d];
+        } else {
             // the grid velocity (getVelocityFromGrid) and its change (FLIP_Solver.cpp:125-133)
             // at the particle, from the same taps
             const int G0 = g.G[0], G1 = g.G[1], G2 = g.G[2];
@@ -1324,6 +1330,30 @@ __device__ __forceinline__ void g2p_move_body(Blk blk, int n, const GridDesc& g,
             for(int d = 0; d < 3; ++d) {
                 const float pv = vel3[d * stride + p];
                 vel3[d * stride + p] = (1.0f - ratio) * gv[d] + ratio * (pv + dg[d]);
+            }
+        }
+        if(KIND == 1 || KIND == 2) {
+            // the affine matrix as k_g2p forms it
+            const int G0 = g.G[0], G1 = g.G[1], G2 = g.G[2];
+            const float* arrs[3] = {u, v, w};
+            const float* olds[3] = {ou, ov, ow};
+            const int dims[3][3] = {{G0 + 1, G1, G2}, {G0, G1 + 1, G2}, {G0, G1, G2 + 1}};
+            for(int d = 0; d < 3; ++d) {
+                const float ptx = d == 0 ? gx : gx - 0.5f, pty = d == 1 ? gy : gy - 0.5f, ptz = d == 2 ? gz : gz - 0.5f;
+                float gc[3];
+                grad_value(arrs[d], dims[d][0], dims[d][1], dims[d][2], ptx, pty, ptz, g.dx, gc);
+                if(KIND == 1) {
+#pragma unroll
+                    for(int c = 0; c < 3; ++c) C9[(size_t)(d * 3 + c) * stride + p] = gc[c];
+                } else {
+                    float dc[3];
+                    grad_value_diff(arrs[d], olds[d], dims[d][0], dims[d][1], dims[d][2], ptx, pty, ptz, g.dx, dc);
+#pragma unroll
+                    for(int c = 0; c < 3; ++c) {
+                        const size_t o_ = (size_t)(d * 3 + c) * stride + p;
+                        C9[o_] = (1.0f - ratio) * gc[c] + ratio * (C9[o_] + dc[c]);
+                    }
+                }
             }
         }
         for(int s = 0; s < ns.advSteps; ++s) {
@@ -1353,6 +1383,7 @@ __device__ __forceinline__ void g2p_move_body(Blk blk, int n, const GridDesc& g,
     histogram_slot(c, p, count, slot);
     bbox_block_partial(bboxPart, blk.x, mn, mx);
 }
+template <int KIND>
 __global__ void __launch_bounds__(256, 4) k_g2p_move(int n, GridDesc g, float* __restrict__ p6, size_t stride,
                                                   const float* __restrict__ u, const float* __restrict__ v,
                                                   const float* __restrict__ w, const float* __restrict__ ou,
@@ -1360,8 +1391,9 @@ __global__ void __launch_bounds__(256, 4) k_g2p_move(int n, GridDesc g, float* _
                                                   float ratio, NextStep ns, float* __restrict__ moved,
                                                   uint32_t* __restrict__ cellOf, uint32_t* __restrict__ slot,
                                                   uint32_t* __restrict__ count, DevState* st,
-                                                  int* __restrict__ bboxPart) {
-    g2p_move_body(own_blk(), n, g, p6, stride, u, v, w, ou, ov, ow, ratio, ns, moved, cellOf, slot, count, st, bboxPart);
+                                                  int* __restrict__ bboxPart, float* __restrict__ C9) {
+    g2p_move_body<KIND>(own_blk(), n, g, p6, stride, u, v, w, ou, ov, ow, ratio, ns, moved, cellOf, slot, count, st,
+                        bboxPart, C9);
 }
 
 // Start of a sub-step whose move already ran: the move's flags and occupied-cell box stay
@@ -1605,8 +1637,8 @@ __global__ void __launch_bounds__(256, 4) kb_g2p_move(const BScene* __restrict__
     int q;
     const Blk b = seg_blk(P, ns, q);
     const BScene& c = S[q];
-    g2p_move_body(b, c.n, c.g, c.p6nxt, c.cap, c.B[0], c.B[1], c.B[2], c.O[0], c.O[1], c.O[2], c.ratio, c.ns, c.movedPos,
-                  c.cellOf, c.slot, c.count, c.dst, c.bboxPart);
+    g2p_move_body<0>(b, c.n, c.g, c.p6nxt, c.cap, c.B[0], c.B[1], c.B[2], c.O[0], c.O[1], c.O[2], c.ratio, c.ns,
+                     c.movedPos, c.cellOf, c.slot, c.count, c.dst, c.bboxPart, nullptr);
 }
 // one thread per scene: its pressure rows (the active-cell numbering's total)
 __global__ void kb_gather_rows(const BScene* __restrict__ S, int ns, unsigned* __restrict__ out) {
@@ -1805,13 +1837,14 @@ void launch_step_reset_moved(DevState* st, cudaStream_t s) { { k_step_reset_move
 // FLIP grid-to-particle transfer + the next sub-step's move; the occupied-cell box is
 // rebuilt for the next sub-step
 void launch_g2p_move(int n, const GridDesc& g, float* p6, size_t stride, const float* const* U, const float* const* O,
-                     float ratio, const NextStep& ns, float* moved, uint32_t* cellOf, uint32_t* slot, uint32_t* count,
-                     DevState* st, int* bboxPart, cudaStream_t s) {
+                     float ratio, int kind, float* C9, const NextStep& ns, float* moved, uint32_t* cellOf,
+                     uint32_t* slot, uint32_t* count, DevState* st, int* bboxPart, cudaStream_t s) {
     { k_bbox_reset<<<1, 1, 0, s>>>(st); bnn_note_launch(); }
     if(n == 0) return;
     const unsigned blocks = nblk(n);
-    { k_g2p_move<<<blocks, 256, 0, s>>>(n, g, p6, stride, U[0], U[1], U[2], O[0], O[1], O[2], ratio, ns, moved, cellOf,
-                                       slot, count, st, bboxPart); bnn_note_launch(); }
+    auto k = kind == 1 ? k_g2p_move<1> : kind == 2 ? k_g2p_move<2> : k_g2p_move<0>;
+    { k<<<blocks, 256, 0, s>>>(n, g, p6, stride, U[0], U[1], U[2], O[0], O[1], O[2], ratio, ns, moved, cellOf, slot,
+                               count, st, bboxPart, C9); bnn_note_launch(); }
     const unsigned fb = blocks < 148u * 4u * 256u ? (blocks + 255u) / 256u : 148u * 4u;
     { k_bbox_final<<<fb, 256, 0, s>>>((int)blocks, bboxPart, st); bnn_note_launch(); }
 }

@@ -113,7 +113,7 @@ def test_config1_100_steps_positions(bnn, oracle_mod):
     assert np.array_equal(pg, po)
 
 
-@pytest.mark.parametrize("over", [{}, {"solver_kind": 1}, {"solver_kind": 3}, {"correct_position": 1}])
+@pytest.mark.parametrize("over", [{}, {"solver_kind": 1}, {"solver_kind": 2}, {"solver_kind": 3}, {"correct_position": 1}])
 def test_step_host_matches_resident(bnn, over):
     """The end-to-end entry point (host arrays in, host arrays out each step, transfers
     overlapping the step) computes the same step as the device-resident one: the sort key
