@@ -94,7 +94,8 @@ void launch_cell_histogram(int n, const float* p6, size_t stride, const GridDesc
 void launch_sort_finish(int n, size_t ncells, uint32_t* cellOf, uint32_t* slot, const uint32_t* cellStart,
                         uint32_t* order, uint32_t* key, uint32_t* count, const float* src6, const float* srcPos,
                         float* dst6, const uint32_t* idSrc, uint32_t* idDst, const float* cSrc, float* cDst,
-                        float4* rec, const GridDesc& g, size_t stride, DevState* st, cudaStream_t s);
+                        float4* rec, const GridDesc& g, size_t stride, DevState* st, cudaStream_t s,
+                        cudaEvent_t gatherAfter = nullptr);
 // gather_kernels.cu
 void launch_p2g_sdf(const GridDesc& g, const DevState* st, const uint32_t* cellStart, const float4* rec,
                     size_t stride, float* const* out, uint8_t* const* valid, float* phi, cudaStream_t s);
@@ -546,9 +547,11 @@ extern "C" int bnn_flip_set_boundaries(bnn_flip* h, const bnn_boundary_object* o
 }
 
 // Host arrays of bnn_flip_step_host whose transfers overlap the step: the main stream waits
-// for the velocity upload only where the sort first gathers velocities, and the positions
-// go back to the host on the copy stream as soon as they are final (after the sort), while
-// the rest of the step runs.
+// for the velocity upload only where the sort first gathers velocities, and the positions,
+// final after the sort, go back to the host on the copy stream while the rest of the step
+// runs.  Their download is issued after the step's last small device-to-host read before
+// the pressure solve (the active-row count): copies in one direction share a copy engine,
+// so that read would otherwise wait for the whole 12 bytes per particle to cross the link.
 struct HostIo {
     bool velPending = false;  // velocities still being uploaded on s2 (event io[1])
     float* posOut = nullptr;  // host array for the final positions (caller order)
@@ -582,12 +585,13 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st, const HostIo* io = nullp
     }
     cudaEventRecord(h->ev[1], s);
     BNN_CUDA_CHECK(exclusive_scan_u32(h->count, h->cellStart, h->C, h->scanWs, s));
-    if(io && io->velPending) BNN_CUDA_CHECK(cudaStreamWaitEvent(s, h->io[1], 0));
     const int nxt = 1 - h->cur;
+    // the particles' gather is the first reader of the velocities: it alone waits for
+    // their upload (bnn_flip_step_host)
     launch_sort_finish(n, h->C, h->cellOf, h->slot, h->cellStart, h->order, h->key, h->count, h->p6[h->cur],
                        moved ? h->moved : nullptr, h->p6[nxt],
                        h->ids[h->cur], h->ids[nxt], affine ? h->C9[h->cur] : nullptr, affine ? h->C9[nxt] : nullptr,
-                       h->rec, g, h->cap, h->dst, s);
+                       h->rec, g, h->cap, h->dst, s, io && io->velPending ? h->io[1] : nullptr);
     h->cur = nxt;
     if(h->P.correct_position && n > 0) {
         // PIC_Solver::advanceFrame: correctParticlePositions right after moveParticles
@@ -616,8 +620,6 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st, const HostIo* io = nullp
         BNN_CUDA_CHECK(cudaEventRecord(h->io[2], s));
         BNN_CUDA_CHECK(cudaStreamWaitEvent(h->s2, h->io[2], 0));
         launch_soa3_to_aos(n, h->p6[h->cur], h->ids[h->cur], h->aosStage, h->cap, h->s2);
-        BNN_CUDA_CHECK(cudaMemcpyAsync(io->posOut, h->aosStage, 3 * (size_t)n * sizeof(float), cudaMemcpyDeviceToHost,
-                                       h->s2));
     }
     // P2G
     if(kind == BNN_SOLVER_PIC) {
@@ -661,6 +663,9 @@ static int run_substep(bnn_flip* h, bnn_step_stats* st, const HostIo* io = nullp
     BNN_CUDA_CHECK(cudaMemcpyAsync(&h->hst->n_active, h->aidx + h->C, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     BNN_CUDA_CHECK(cudaStreamSynchronize(s));
     nrows = h->hst->n_active;
+    if(io && io->posOut && n > 0)
+        BNN_CUDA_CHECK(cudaMemcpyAsync(io->posOut, h->aosStage, 3 * (size_t)n * sizeof(float), cudaMemcpyDeviceToHost,
+                                       h->s2));
     int rc = reserve_rows(h, nrows);
     if(rc != BNN_OK) return rc;
     h->nRows = nrows;

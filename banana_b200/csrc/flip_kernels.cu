@@ -1677,11 +1677,14 @@ void launch_cell_histogram(int n, const float* p6, size_t stride, const GridDesc
 void launch_sort_finish(int n, size_t ncells, uint32_t* cellOf, uint32_t* slot, const uint32_t* cellStart,
                         uint32_t* order, uint32_t* key, uint32_t* count, const float* src6, const float* srcPos,
                         float* dst6, const uint32_t* idSrc, uint32_t* idDst, const float* cSrc, float* cDst,
-                        float4* rec, const GridDesc& g, size_t stride, DevState* st, cudaStream_t s) {
+                        float4* rec, const GridDesc& g, size_t stride, DevState* st, cudaStream_t s,
+                        cudaEvent_t gatherAfter) {
     if(n > 0) { k_scatter_index<<<nblk(n), 256, 0, s>>>(n, cellOf, slot, cellStart, idSrc, order, key); bnn_note_launch(); }
     cudaMemsetAsync(&st->nlarge, 0, sizeof(unsigned), s);
     { k_sort_buckets<<<nblk(ncells), 256, 0, s>>>((int)ncells, cellStart, order, key, count, slot, st); bnn_note_launch(); }
     if(n > 16) { k_sort_large<<<8 * 148, 256, 0, s>>>(cellStart, order, idSrc, cellOf, slot, st); bnn_note_launch(); }
+    // src6's velocity planes may still be arriving on another stream until this event
+    if(gatherAfter) cudaStreamWaitEvent(s, gatherAfter, 0);
     if(n > 0)
         { k_gather_particles<<<nblk(n), 256, 0, s>>>(n, order, src6, srcPos ? srcPos : src6, dst6, idSrc, idDst, cSrc, cDst,
                                                     rec, g, stride); bnn_note_launch(); }
