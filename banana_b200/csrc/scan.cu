@@ -3,6 +3,9 @@
 // block layout.
 #include "bnn_internal.cuh"
 
+#include <cstdint>
+#include <type_traits>
+
 namespace bnn {
 
 namespace {
@@ -69,6 +72,123 @@ template<class TO> __global__ void k_scan_add(TO* __restrict__ out, const TO* __
 
 template<class TO> __global__ void k_copy_total(TO* out, size_t n, const TO* sumsScan, size_t nb) { out[n] = sumsScan[nb]; }
 
+// ---- reduce-then-scan of 32-bit inputs -----------------------------------------------
+// Three launches for any n: the tile sums (one 16384-element tile per block), their scan,
+// and the tiles' scans with the tile offsets added.  The last pass reads its tile again,
+// from L2 for arrays up to a few tens of MB (the cell histograms, the active-cell flags),
+// so DRAM sees about one read and one write of the array.  Every load and store is 16
+// bytes: tile element (j * kRtsThreads + t) * 4 + c belongs to thread t, load j, lane c
+// of the vector, so each warp instruction moves 512 contiguous bytes.
+constexpr int kRtsThreads = 512;
+constexpr int kRtsVec = 8;
+constexpr int kRtsTile = kRtsThreads * kRtsVec * 4;
+constexpr int kRtsWarps = kRtsThreads / 32;
+
+__device__ __forceinline__ void rts_load(const uint32_t* __restrict__ in, size_t n, size_t tb, uint4 q[kRtsVec]) {
+#pragma unroll
+    for(int j = 0; j < kRtsVec; ++j) {
+        const size_t e = tb + ((size_t)j * kRtsThreads + threadIdx.x) * 4;
+        if(e + 4 <= n) {
+            q[j] = *reinterpret_cast<const uint4*>(in + e);
+        } else {
+            q[j].x = e < n ? in[e] : 0u;
+            q[j].y = e + 1 < n ? in[e + 1] : 0u;
+            q[j].z = e + 2 < n ? in[e + 2] : 0u;
+            q[j].w = 0u;
+        }
+    }
+}
+
+template<class TO> __device__ __forceinline__ TO quad_sum(const uint4& v) {
+    return (TO)v.x + (TO)v.y + (TO)v.z + (TO)v.w;
+}
+
+template<class TO>
+__global__ void __launch_bounds__(kRtsThreads) k_rts_sums(const uint32_t* __restrict__ in, TO* __restrict__ sums,
+                                                          size_t n) {
+    __shared__ TO wsum[kRtsWarps];
+    uint4 q[kRtsVec];
+    rts_load(in, n, (size_t)blockIdx.x * kRtsTile, q);
+    TO t = 0;
+#pragma unroll
+    for(int j = 0; j < kRtsVec; ++j) t += quad_sum<TO>(q[j]);
+#pragma unroll
+    for(int off = 16; off > 0; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if(lane == 0) wsum[warp] = t;
+    __syncthreads();
+    if(warp == 0) {
+        TO v = lane < kRtsWarps ? wsum[lane] : (TO)0;
+#pragma unroll
+        for(int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        if(lane == 0) sums[blockIdx.x] = v;
+    }
+}
+
+template<class TO> __device__ __forceinline__ void store_quad(TO* __restrict__ out, size_t e, size_t n, TO a, TO b,
+                                                              TO c, TO d);
+template<> __device__ __forceinline__ void store_quad<uint32_t>(uint32_t* __restrict__ out, size_t e, size_t n,
+                                                                uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+    if(e + 4 <= n) {
+        *reinterpret_cast<uint4*>(out + e) = make_uint4(a, b, c, d);
+    } else {
+        if(e < n) out[e] = a;
+        if(e + 1 < n) out[e + 1] = b;
+        if(e + 2 < n) out[e + 2] = c;
+    }
+}
+template<> __device__ __forceinline__ void store_quad<unsigned long long>(unsigned long long* __restrict__ out, size_t e,
+                                                                          size_t n, unsigned long long a,
+                                                                          unsigned long long b, unsigned long long c,
+                                                                          unsigned long long d) {
+    if(e + 4 <= n) {
+        *reinterpret_cast<ulonglong2*>(out + e) = make_ulonglong2(a, b);
+        *reinterpret_cast<ulonglong2*>(out + e + 2) = make_ulonglong2(c, d);
+    } else {
+        if(e < n) out[e] = a;
+        if(e + 1 < n) out[e + 1] = b;
+        if(e + 2 < n) out[e + 2] = c;
+    }
+}
+
+// offs: the exclusive scan of the tile sums, offs[gridDim.x] the total (written to out[n])
+template<class TO>
+__global__ void __launch_bounds__(kRtsThreads) k_rts_final(const uint32_t* __restrict__ in, TO* __restrict__ out,
+                                                           const TO* __restrict__ offs, size_t n) {
+    __shared__ TO part[kRtsVec * kRtsWarps];  // warp totals in tile order: load j, then warp
+    const size_t tb = (size_t)blockIdx.x * kRtsTile;
+    uint4 q[kRtsVec];
+    rts_load(in, n, tb, q);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    TO sum[kRtsVec], inc[kRtsVec];
+#pragma unroll
+    for(int j = 0; j < kRtsVec; ++j) {
+        sum[j] = quad_sum<TO>(q[j]);
+        inc[j] = warp_incl_scan(sum[j]);
+        if(lane == 31) part[j * kRtsWarps + warp] = inc[j];
+    }
+    __syncthreads();
+    if(warp == 0) {
+        constexpr int kPer = kRtsVec * kRtsWarps / 32;
+        TO v[kPer];
+        TO loc = 0;
+#pragma unroll
+        for(int k = 0; k < kPer; ++k) { v[k] = part[lane * kPer + k]; loc += v[k]; }
+        TO run = warp_incl_scan(loc) - loc;
+#pragma unroll
+        for(int k = 0; k < kPer; ++k) { part[lane * kPer + k] = run; run += v[k]; }
+    }
+    __syncthreads();
+    const TO base = offs[blockIdx.x];
+#pragma unroll
+    for(int j = 0; j < kRtsVec; ++j) {
+        const TO r = base + part[j * kRtsWarps + warp] + inc[j] - sum[j];
+        const TO r1 = r + (TO)q[j].x, r2 = r1 + (TO)q[j].y, r3 = r2 + (TO)q[j].z;
+        store_quad<TO>(out, tb + ((size_t)j * kRtsThreads + threadIdx.x) * 4, n, r, r1, r2, r3);
+    }
+    if(blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = offs[gridDim.x];
+}
+
 template<class TO> size_t ws_bytes(size_t n) {
     size_t nb = (n + kScanTile - 1) / kScanTile;
     if(nb <= 1) return 0;
@@ -81,6 +201,19 @@ template<class TI, class TO> cudaError_t scan_impl(const TI* in, TO* out, size_t
     if(n == 0) return cudaMemsetAsync(out, 0, sizeof(TO), s);
     if(nb == 1) {
         { k_scan_tile<TI, TO><<<1, kScanThreads, 0, s>>>(in, out, nullptr, n); bnn_note_launch(); }
+        return cudaGetLastError();
+    }
+    if(std::is_same<TI, uint32_t>::value && ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15u) == 0) {
+        // reduce-then-scan: fewer tiles than the scan below, so its workspace holds them
+        const size_t nt = (n + kRtsTile - 1) / kRtsTile;
+        TO* sums = (TO*)ws;
+        TO* sumsScan = sums + (nt + 1);
+        const size_t here = ((nt + 1) * 2 * sizeof(TO) + 255) & ~size_t(255);
+        const uint32_t* in32 = reinterpret_cast<const uint32_t*>(in);
+        { k_rts_sums<TO><<<(unsigned)nt, kRtsThreads, 0, s>>>(in32, sums, n); bnn_note_launch(); }
+        cudaError_t e = scan_impl<TO, TO>(sums, sumsScan, nt, (char*)ws + here, s);
+        if(e != cudaSuccess) return e;
+        { k_rts_final<TO><<<(unsigned)nt, kRtsThreads, 0, s>>>(in32, out, sumsScan, n); bnn_note_launch(); }
         return cudaGetLastError();
     }
     TO* sums = (TO*)ws;

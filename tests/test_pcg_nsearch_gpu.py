@@ -270,6 +270,33 @@ def test_cell_sort_bitexact(bnn, oracle_mod):
     assert np.array_equal(gst.cpu().numpy().view(np.uint32), start)
 
 
+@pytest.mark.parametrize("nc,cell", [((3, 5, 7), 0.34), ((17, 33, 41), 1 / 16.5), ((129, 130, 131), 1 / 128)],
+                         ids=["105_cells", "23001_cells", "2196870_cells"])
+def test_cell_sort_grid_sizes_bitexact(bnn, oracle_mod, nc, cell):
+    """Cell starts (the exclusive prefix sum of the cell counts, total last) on grids of one
+    scan tile, of a few tiles with a ragged end, and of many tiles"""
+    pts = scenes.point_cloud(150_000, seed=11)
+    bmin = np.zeros(3, np.float32)
+    nc = np.array(nc, np.int32)
+    cid, srt, start, oor = oracle_mod.cell_sort(pts, bmin, np.float32(cell), nc)
+    L = bnn.load()
+    p = _dev(pts)
+    n = len(pts)
+    gc = torch.zeros(n, dtype=torch.int32, device="cuda")
+    gs = torch.zeros(n, dtype=torch.int32, device="cuda")
+    gst = torch.full((int(nc.prod()) + 1,), -1, dtype=torch.int32, device="cuda")
+    o = C.c_uint32()
+    rc = L.bnn_cell_sort(C.c_void_p(p.data_ptr()), n, bmin.ctypes.data_as(C.POINTER(C.c_float)), float(np.float32(cell)),
+                         nc.ctypes.data_as(C.POINTER(C.c_int32)), C.c_void_p(gc.data_ptr()), C.c_void_p(gs.data_ptr()),
+                         C.c_void_p(gst.data_ptr()), C.byref(o), None)
+    torch.cuda.synchronize()
+    assert rc == 0
+    assert o.value == oor
+    assert np.array_equal(gc.cpu().numpy().view(np.uint32), cid)
+    assert np.array_equal(gs.cpu().numpy().view(np.uint32), srt)
+    assert np.array_equal(gst.cpu().numpy().view(np.uint32), start)
+
+
 def test_z_sort_bitexact(bnn, oracle_mod):
     pts = scenes.point_cloud(100_000, seed=3)
     z, perm = oracle_mod.z_sort(pts, np.float32(0.01))
