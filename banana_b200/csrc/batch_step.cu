@@ -244,6 +244,10 @@ int batch_substep(BatchStepWork& w, bnn_flip* const* hs, int nsIn, int* rc, bnn_
         c.dst = h->dst;
         p2g_tile_args(H + L.args + (size_t)q * argBytes, h->g, h->dst, h->cellStart, h->rec, h->cap, h->U, h->VA,
                       h->phi);
+        if(((uintptr_t)h->count | (uintptr_t)h->cellStart | (uintptr_t)h->flag | (uintptr_t)h->aidx) & 15u) {
+            bnn_set_error("batched scan: cell arrays not 16-byte aligned");
+            return BNN_ERR_NOT_SUPPORTED;
+        }
         hSeg[q] = ScanSeg{h->count, h->cellStart, (uint32_t*)h->scanWs, h->C};
         hSeg[ns + q] = ScanSeg{h->flag, h->aidx, (uint32_t*)h->scanWs, h->C};
         const unsigned pb = virt_blocks((size_t)c.n);
@@ -262,7 +266,7 @@ int batch_substep(BatchStepWork& w, bnn_flip* const* hs, int nsIn, int* rc, bnn_
             bbox_fold_blocks(c.n),                             // PMoveFold
             virt_blocks(h->C),                                 // PCells
             c.n > 16 ? std::min(296u, std::max(2u, cdiv((size_t)c.n, 8192))) : 0u,  // PSortLarge
-            cdiv(h->C, 2048),                                  // PScan
+            cdiv(h->C, kScanSegTile),                          // PScan
             region_blocks(ftot),                               // PExtrap
             std::min(kRegionBlocks, cdiv(fmax, 2048)),         // PFill
             region_blocks(tiles[0]), region_blocks(tiles[1]), region_blocks(tiles[2]),  // PUpd*

@@ -343,9 +343,10 @@ size_t scan_workspace_bytes(size_t n);
 // exclusive scan of n uint32 into out[0..n], out[n] = total; ws from scan_workspace_bytes
 cudaError_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, size_t n, void* ws, cudaStream_t s);
 // Many independent exclusive scans in three launches: segment q scans in[0..n) into
-// out[0..n] with workspace ws (scan_workspace_bytes(n)).  tiles[q] is the prefix of the
-// segments' 2048-element tile counts (at least 1 each; tiles[nseg] = totalTiles), in
-// device memory.
+// out[0..n] with workspace ws (scan_workspace_bytes(n)); in and out 16-byte aligned.
+// tiles[q] is the prefix of the segments' kScanSegTile-element tile counts (at least 1
+// each; tiles[nseg] = totalTiles), in device memory.
+constexpr unsigned kScanSegTile = 16384;
 struct ScanSeg {
     const uint32_t* in;
     uint32_t* out;

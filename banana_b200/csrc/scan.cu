@@ -103,12 +103,13 @@ template<class TO> __device__ __forceinline__ TO quad_sum(const uint4& v) {
     return (TO)v.x + (TO)v.y + (TO)v.z + (TO)v.w;
 }
 
+// The sum of tile `tile` to *dst (all threads of the block take part)
 template<class TO>
-__global__ void __launch_bounds__(kRtsThreads) k_rts_sums(const uint32_t* __restrict__ in, TO* __restrict__ sums,
-                                                          size_t n) {
+__device__ __forceinline__ void rts_sums_body(const uint32_t* __restrict__ in, size_t n, size_t tile,
+                                              TO* __restrict__ dst) {
     __shared__ TO wsum[kRtsWarps];
     uint4 q[kRtsVec];
-    rts_load(in, n, (size_t)blockIdx.x * kRtsTile, q);
+    rts_load(in, n, tile * kRtsTile, q);
     TO t = 0;
 #pragma unroll
     for(int j = 0; j < kRtsVec; ++j) t += quad_sum<TO>(q[j]);
@@ -121,8 +122,14 @@ __global__ void __launch_bounds__(kRtsThreads) k_rts_sums(const uint32_t* __rest
         TO v = lane < kRtsWarps ? wsum[lane] : (TO)0;
 #pragma unroll
         for(int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-        if(lane == 0) sums[blockIdx.x] = v;
+        if(lane == 0) *dst = v;
     }
+}
+
+template<class TO>
+__global__ void __launch_bounds__(kRtsThreads) k_rts_sums(const uint32_t* __restrict__ in, TO* __restrict__ sums,
+                                                          size_t n) {
+    rts_sums_body(in, n, blockIdx.x, sums + blockIdx.x);
 }
 
 template<class TO> __device__ __forceinline__ void store_quad(TO* __restrict__ out, size_t e, size_t n, TO a, TO b,
@@ -151,12 +158,13 @@ template<> __device__ __forceinline__ void store_quad<unsigned long long>(unsign
     }
 }
 
-// offs: the exclusive scan of the tile sums, offs[gridDim.x] the total (written to out[n])
+// Exclusive scan of tile `tile` plus `base` into out; `totalOut`, if given, gets base plus
+// the tile's sum
 template<class TO>
-__global__ void __launch_bounds__(kRtsThreads) k_rts_final(const uint32_t* __restrict__ in, TO* __restrict__ out,
-                                                           const TO* __restrict__ offs, size_t n) {
+__device__ __forceinline__ void rts_final_body(const uint32_t* __restrict__ in, TO* __restrict__ out, TO base,
+                                               size_t n, size_t tile, TO* __restrict__ totalOut) {
     __shared__ TO part[kRtsVec * kRtsWarps];  // warp totals in tile order: load j, then warp
-    const size_t tb = (size_t)blockIdx.x * kRtsTile;
+    const size_t tb = tile * kRtsTile;
     uint4 q[kRtsVec];
     rts_load(in, n, tb, q);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -174,19 +182,26 @@ __global__ void __launch_bounds__(kRtsThreads) k_rts_final(const uint32_t* __res
         TO loc = 0;
 #pragma unroll
         for(int k = 0; k < kPer; ++k) { v[k] = part[lane * kPer + k]; loc += v[k]; }
-        TO run = warp_incl_scan(loc) - loc;
+        const TO li = warp_incl_scan(loc);
+        TO run = li - loc;
 #pragma unroll
         for(int k = 0; k < kPer; ++k) { part[lane * kPer + k] = run; run += v[k]; }
+        if(totalOut && lane == 31) *totalOut = base + li;
     }
     __syncthreads();
-    const TO base = offs[blockIdx.x];
 #pragma unroll
     for(int j = 0; j < kRtsVec; ++j) {
         const TO r = base + part[j * kRtsWarps + warp] + inc[j] - sum[j];
         const TO r1 = r + (TO)q[j].x, r2 = r1 + (TO)q[j].y, r3 = r2 + (TO)q[j].z;
         store_quad<TO>(out, tb + ((size_t)j * kRtsThreads + threadIdx.x) * 4, n, r, r1, r2, r3);
     }
-    if(blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = offs[gridDim.x];
+}
+
+// offs: the exclusive scan of the tile sums; the last tile writes the total to out[n]
+template<class TO>
+__global__ void __launch_bounds__(kRtsThreads, sizeof(TO) == 4 ? 2 : 1) k_rts_final(const uint32_t* __restrict__ in, TO* __restrict__ out,
+                                                           const TO* __restrict__ offs, size_t n) {
+    rts_final_body(in, out, offs[blockIdx.x], n, blockIdx.x, blockIdx.x == gridDim.x - 1 ? out + n : nullptr);
 }
 
 template<class TO> size_t ws_bytes(size_t n) {
@@ -229,50 +244,18 @@ template<class TI, class TO> cudaError_t scan_impl(const TI* in, TO* out, size_t
 }
 
 // ---- batched segments ----------------------------------------------------------------
-// Segment q: tiles tiles[q] .. tiles[q+1]-1 of the launch (at least one, so an empty
-// segment still gets its total 0).  Its tile sums go to ws[0..nb], their scan to
-// ws[nb+1 ..] (the layout scan_impl's first level uses).
-__device__ __forceinline__ void scan_tile_body(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
-                                               uint32_t* __restrict__ sums, size_t n, unsigned tile, unsigned ntiles) {
-    __shared__ uint32_t warpTot[kScanThreads / 32];
-    const size_t base = (size_t)tile * kScanTile + (size_t)threadIdx.x * kScanPer;
-    uint32_t v[kScanPer];
-    uint32_t local = 0;
-#pragma unroll
-    for(int j = 0; j < kScanPer; ++j) {
-        size_t e = base + j;
-        v[j] = e < n ? in[e] : 0u;
-        local += v[j];
-    }
-    uint32_t incl = warp_incl_scan(local);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if(lane == 31) warpTot[warp] = incl;
-    __syncthreads();
-    if(warp == 0) {
-        uint32_t w = lane < kScanThreads / 32 ? warpTot[lane] : 0u;
-        uint32_t wi = warp_incl_scan(w);
-        if(lane < kScanThreads / 32) warpTot[lane] = wi - w;
-    }
-    __syncthreads();
-    uint32_t run = warpTot[warp] + incl - local;
-#pragma unroll
-    for(int j = 0; j < kScanPer; ++j) {
-        size_t e = base + j;
-        if(e < n) out[e] = run;
-        run += v[j];
-    }
-    if(threadIdx.x == kScanThreads - 1) {
-        if(ntiles > 1) sums[tile] = run;
-        else out[n] = run;
-    }
-}
-
-__global__ void __launch_bounds__(kScanThreads) kb_scan_tiles(const ScanSeg* __restrict__ segs,
-                                                              const unsigned* __restrict__ tiles, int nseg) {
+// Segment q: tiles tiles[q] .. tiles[q+1]-1 of the launch, kScanSegTile elements each (at
+// least one, so an empty segment still gets its total 0).  Its tile sums go to ws[0..nb],
+// their scan to ws[nb+1 ..] (the layout of scan_impl's first level).
+static_assert(kRtsTile == kScanSegTile, "segment tiles are the reduce-then-scan tiles");
+// tile sums of every segment of more than one tile
+__global__ void __launch_bounds__(kRtsThreads) kb_rts_sums(const ScanSeg* __restrict__ segs,
+                                                           const unsigned* __restrict__ tiles, int nseg) {
     int q;
     const Blk b = seg_blk(tiles, nseg, q);
+    if(b.n <= 1) return;
     const ScanSeg sg = segs[q];
-    scan_tile_body(sg.in, sg.out, sg.ws, sg.n, b.x, b.n);
+    rts_sums_body<uint32_t>(sg.in, sg.n, b.x, sg.ws + b.x);
 }
 // Exclusive scan of m <= kScanTile values by one block, continuing from `carry` (updated to
 // the running total; every thread gets it)
@@ -320,27 +303,23 @@ __global__ void __launch_bounds__(kScanThreads) kb_scan_sums(const ScanSeg* __re
         scan_chunk_carry(sg.ws + b0, sumsScan + b0, min(nb - b0, (unsigned)kScanTile), carry);
     if(threadIdx.x == 0) sg.out[sg.n] = carry;
 }
-__global__ void __launch_bounds__(kScanThreads) kb_scan_add(const ScanSeg* __restrict__ segs,
+// the tiles' scans from their offsets (kb_scan_sums); a one-tile segment writes its total
+__global__ void __launch_bounds__(kRtsThreads, 2) kb_rts_final(const ScanSeg* __restrict__ segs,
                                                             const unsigned* __restrict__ tiles, int nseg) {
     int q;
     const Blk b = seg_blk(tiles, nseg, q);
-    if(b.n <= 1) return;
     const ScanSeg sg = segs[q];
-    const uint32_t o = sg.ws[(b.n + 1) + b.x];
-    const size_t base = (size_t)b.x * kScanTile;
-    for(int j = threadIdx.x; j < kScanTile; j += kScanThreads) {
-        size_t e = base + j;
-        if(e < sg.n) sg.out[e] += o;
-    }
+    const uint32_t base = b.n > 1 ? sg.ws[(b.n + 1) + b.x] : 0u;
+    rts_final_body<uint32_t>(sg.in, sg.out, base, sg.n, b.x, b.n == 1 ? sg.out + sg.n : nullptr);
 }
 } // namespace
 
 cudaError_t batched_exclusive_scan_u32(const ScanSeg* segs, const unsigned* tiles, int nseg, unsigned totalTiles,
                                        cudaStream_t s) {
     if(nseg == 0 || totalTiles == 0) return cudaSuccess;
-    { kb_scan_tiles<<<totalTiles, kScanThreads, 0, s>>>(segs, tiles, nseg); bnn_note_launch(); }
+    { kb_rts_sums<<<totalTiles, kRtsThreads, 0, s>>>(segs, tiles, nseg); bnn_note_launch(); }
     { kb_scan_sums<<<(unsigned)nseg, kScanThreads, 0, s>>>(segs, tiles); bnn_note_launch(); }
-    { kb_scan_add<<<totalTiles, kScanThreads, 0, s>>>(segs, tiles, nseg); bnn_note_launch(); }
+    { kb_rts_final<<<totalTiles, kRtsThreads, 0, s>>>(segs, tiles, nseg); bnn_note_launch(); }
     return cudaGetLastError();
 }
 size_t scan_workspace_bytes(size_t n) { return ws_bytes<uint32_t>(n); }
