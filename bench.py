@@ -465,7 +465,11 @@ def run_batch(args, ws, rank, local):
     built = [scenes.batch_scene(specs[i], **over) for i in mine]
     npart = sum(len(p) for _, p, _ in built)
     t_up = time.perf_counter()
-    ids = [b.add_scene(cfg, pos, vel) for cfg, pos, vel in built]
+    ids, add_ms = [], []
+    for cfg, pos, vel in built:
+        ta = time.perf_counter()
+        ids.append(b.add_scene(cfg, pos, vel))
+        add_ms.append((time.perf_counter() - ta) * 1e3)
     t_up = time.perf_counter() - t_up
     for _ in range(args.warmup):
         b.step()
@@ -542,7 +546,10 @@ def run_batch(args, ws, rank, local):
                 "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
                 "e2e": {"value": tot_ps / e2e_t, "unit": UNIT, "h2d_bytes_per_step": 24 * npart / args.steps,
                         "d2h_bytes_per_step": 24 * npart / args.steps,
-                        "api": "bnn_batch_add_scene (upload) + steps + bnn_batch_get_scene (download), wall clock"},
+                        "api": "bnn_batch_add_scene (upload) + steps + bnn_batch_get_scene (download), wall clock",
+                        "upload_s": t_up, "download_s": t_dl,
+                        "add_scene_ms": {"p50": float(np.median(add_ms)), "max": float(np.max(add_ms)),
+                                         "first": add_ms[0]}},
                 "gpu_launches": int(launches), "clocks": clk,
                 "detail": {"tile_tuning": capi.tile_tuning(),
                            "pcg_iterations_per_step": iters / args.steps, "timing": "host wall clock per batch step",
