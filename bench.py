@@ -857,7 +857,8 @@ def _more_workloads() -> dict:
             rec["config"] = {k: v for k, v in d.get("config", {}).items() if k in ("workload", "pcg", "scenes", "requests",
                                                                                   "particles_rank0", "particles")}
             if d.get("e2e"):
-                rec["e2e"] = {"value": d["e2e"]["value"], "api": d["e2e"].get("api")}
+                rec["e2e"] = {k: d["e2e"].get(k) for k in ("value", "api", "upload_s", "download_s", "add_scene_ms")
+                              if k in d["e2e"]}
             det = d.get("detail", {})
             for k in ("per_scene_streams", "one_scene_at_a_time", "pcg_iterations_per_step", "stage_ms_per_step"):
                 if k in det:
