@@ -28,11 +28,15 @@ __device__ __forceinline__ float interp_face(const float* __restrict__ a, int sx
     bary(px, i, fi, sx);
     bary(py, j, fj, sy);
     bary(pz, k, fk, sz);
-    const size_t sxy = (size_t)sx * sy;
-    const size_t b = (size_t)k * sxy + (size_t)j * sx + i;
-    float v000 = __ldg(a + b), v100 = __ldg(a + b + 1), v010 = __ldg(a + b + sx), v110 = __ldg(a + b + sx + 1);
-    float v001 = __ldg(a + b + sxy), v101 = __ldg(a + b + sxy + 1), v011 = __ldg(a + b + sxy + sx),
-          v111 = __ldg(a + b + sxy + sx + 1);
+    // a face array holds fewer than 2^32 entries (cells < 2^31, at least 3 along x): the tap
+    // index in 32 bits, then one pointer per stencil row
+    const unsigned usx = (unsigned)sx, sxy = usx * (unsigned)sy;
+    const float* r00 = a + ((unsigned)k * sxy + (unsigned)j * usx + (unsigned)i);
+    const float* r10 = r00 + usx;
+    const float* r01 = r00 + sxy;
+    const float* r11 = r01 + usx;
+    float v000 = __ldg(r00), v100 = __ldg(r00 + 1), v010 = __ldg(r10), v110 = __ldg(r10 + 1);
+    float v001 = __ldg(r01), v101 = __ldg(r01 + 1), v011 = __ldg(r11), v111 = __ldg(r11 + 1);
     return lerpf(lerpf(lerpf(v000, v100, fi), lerpf(v010, v110, fi), fj),
                  lerpf(lerpf(v001, v101, fi), lerpf(v011, v111, fi), fj), fk);
 }
@@ -47,14 +51,19 @@ __device__ __forceinline__ void interp_face_pair(const float* __restrict__ a, co
     bary(px, i, fi, sx);
     bary(py, j, fj, sy);
     bary(pz, k, fk, sz);
-    const size_t sxy = (size_t)sx * sy;
-    const size_t b = (size_t)k * sxy + (size_t)j * sx + i;
-    const size_t off[8] = {0, 1, (size_t)sx, (size_t)sx + 1, sxy, sxy + 1, sxy + sx, sxy + sx + 1};
+    // 32-bit tap index, then one pointer per stencil row (as interp_face)
+    const unsigned usx = (unsigned)sx, sxy = usx * (unsigned)sy;
+    const unsigned b = (unsigned)k * sxy + (unsigned)j * usx + (unsigned)i;
+    const unsigned rows[4] = {0u, usx, sxy, sxy + usx};
     float va[8], vd[8];
 #pragma unroll
-    for(int t = 0; t < 8; ++t) {
-        va[t] = __ldg(a + b + off[t]);
-        vd[t] = va[t] - __ldg(o + b + off[t]);
+    for(int r = 0; r < 4; ++r) {
+        const float* pa = a + (b + rows[r]);
+        const float* po = o + (b + rows[r]);
+        va[2 * r] = __ldg(pa);
+        vd[2 * r] = va[2 * r] - __ldg(po);
+        va[2 * r + 1] = __ldg(pa + 1);
+        vd[2 * r + 1] = va[2 * r + 1] - __ldg(po + 1);
     }
     *val = lerpf(lerpf(lerpf(va[0], va[1], fi), lerpf(va[2], va[3], fi), fj),
                  lerpf(lerpf(va[4], va[5], fi), lerpf(va[6], va[7], fi), fj), fk);
@@ -1184,9 +1193,10 @@ __device__ __forceinline__ void grad_value_t(const float* __restrict__ a, const 
     bary(px, i, fi, sx);
     bary(py, j, fj, sy);
     bary(pz, k, fk, sz);
-    const size_t sxy = (size_t)sx * sy;
-    const size_t b = (size_t)k * sxy + (size_t)j * sx + i;
-    const size_t offs[8] = {0, sxy, (size_t)sx, sxy + sx, 1, sxy + 1, (size_t)sx + 1, sxy + sx + 1};
+    // 32-bit tap index (as interp_face)
+    const unsigned usx = (unsigned)sx, sxy = usx * (unsigned)sy;
+    const unsigned b = (unsigned)k * sxy + (unsigned)j * usx + (unsigned)i;
+    const unsigned offs[8] = {0u, sxy, usx, sxy + usx, 1u, sxy + 1u, usx + 1u, sxy + usx + 1u};
     float vv[8]; // v000, v001, v010, v011, v100, v101, v110, v111
 #pragma unroll
     for(int q = 0; q < 8; ++q) vv[q] = DIFF ? a[b + offs[q]] - o[b + offs[q]] : a[b + offs[q]];
