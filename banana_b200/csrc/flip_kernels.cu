@@ -1643,7 +1643,7 @@ __global__ void kb_bbox_reset(const BScene* __restrict__ S, int ns) {
 }
 // the fused grid-to-particle transfer + next move, on the final velocities of this
 // sub-step (the pass-2 extrapolation leaves them in B)
-__global__ void __launch_bounds__(256, 4) kb_g2p_move(const BScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
+__global__ void __launch_bounds__(256, 3) kb_g2p_move(const BScene* __restrict__ S, const unsigned* __restrict__ P, int ns) {
     int q;
     const Blk b = seg_blk(P, ns, q);
     const BScene& c = S[q];
