@@ -86,8 +86,12 @@ struct BarrierLimit {
     unsigned minSpins, maxSpins;
 };
 __host__ __device__ constexpr BarrierLimit solve_barrier_limit() { return {1000000000ull, 1u << 20, 1u << 26}; }
+// Pause between polls of the barrier word: fewer acquire loads queue at the word's L2
+// slice behind the arrivals (1.59M-row solve, us per iteration: 22.59 without a pause,
+// 22.42-22.46 at 32 or 100 ns, 22.74 at 256, 22.83-22.92 at 1000; a relaxed poll followed
+// by one acquire fence: 23.24)
 #ifndef BNN_BARRIER_SLEEP_NS
-#define BNN_BARRIER_SLEEP_NS 0
+#define BNN_BARRIER_SLEEP_NS 100
 #endif
 
 // Canonical 256-lane tree (lane t of the chunk owns v; levels 128, 64, 32 then a warp
